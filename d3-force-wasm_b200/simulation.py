@@ -1,0 +1,638 @@
+"""d3-force's simulation and force API over the engine's C ABI.
+
+A Python restatement of d3-force-wasm's facade: ``src/simulation.js`` (alpha
+schedule, force order, tick loop, phyllotaxis start), ``src/core.js``
+(`Context` copy-in / copy-out, `Slot` binding, the fast-mode SEED draw) and the
+force facades ``src/{manyBody,link,collide,center,x,y,radial}.js`` (accessor
+evaluation into the core's arrays). Names, defaults and arithmetic follow those
+files; nodes are a `Nodes` structure of f64 arrays instead of JS objects, with
+NaN standing for a missing (null / undefined) field.
+"""
+
+import math
+
+import numpy as np
+
+from . import core as C
+
+INITIAL_RADIUS = 10.0
+INITIAL_ANGLE = math.pi * (3 - math.sqrt(5))  # simulation.js:14-15
+
+
+class Nodes:
+    """Node table: x, y, vx, vy, fx, fy as f64[n]; NaN = field not set."""
+
+    def __init__(self, n=0, x=None, y=None, vx=None, vy=None, fx=None, fy=None):
+        self.n = n
+        nan = lambda: np.full(n, np.nan)  # noqa: E731
+        self.x = np.array(x, np.float64) if x is not None else nan()
+        self.y = np.array(y, np.float64) if y is not None else nan()
+        self.vx = np.array(vx, np.float64) if vx is not None else nan()
+        self.vy = np.array(vy, np.float64) if vy is not None else nan()
+        self.fx = np.array(fx, np.float64) if fx is not None else nan()
+        self.fy = np.array(fy, np.float64) if fy is not None else nan()
+
+    def __len__(self):
+        return self.n
+
+    def fixed_bits(self):
+        """src/core.js:130: (fx != null) | (fy != null) << 1."""
+        return ((~np.isnan(self.fx)).astype(np.uint8) | ((~np.isnan(self.fy)).astype(np.uint8) << 1))
+
+
+def _constant(v):
+    return lambda *_: v
+
+
+def _accessor(v):
+    return v if callable(v) else _constant(float(v))
+
+
+class Context:
+    """src/core.js:89-164: one simulation handle in the core per node table."""
+
+    def __init__(self, core):
+        self.core = core
+        self.h = core.sim_create()
+        if not self.h:
+            raise C.CoreError(C.OUT_OF_MEMORY)
+        self.n = 0
+        self.live = False
+        self.precision = None  # None = exact; {"order", "opening"} = fast
+        self.host_random = None  # callback for randomSource(); None = device LCG
+        self._cb = None
+
+    def resize(self, n):
+        if n != self.n:
+            C.check(self.core.sim_set_node_count(self.h, n))
+            self.n = n
+
+    def view(self, which, n):
+        return self.core.f64_view(self.core.sim_ptr(self.h, which), n)
+
+    def copy_in(self, nodes):
+        """src/core.js:121-131, then one host-to-device sync."""
+        n = len(nodes)
+        self.resize(n)
+        core, h = self.core, self.h
+        for which, arr in ((C.PTR_X, nodes.x), (C.PTR_Y, nodes.y), (C.PTR_VX, nodes.vx),
+                           (C.PTR_VY, nodes.vy), (C.PTR_FX, nodes.fx), (C.PTR_FY, nodes.fy)):
+            if n:
+                self.view(which, n)[:] = arr
+        if n:
+            core.u8_view(core.sim_ptr(h, C.PTR_FIXED), n)[:] = nodes.fixed_bits()
+        C.check(core.sim_sync_in(h))
+
+    def copy_out(self, nodes):
+        """src/core.js:133-141, after one device-to-host sync."""
+        n = self.n
+        C.check(self.core.sim_sync_out(self.h))
+        if n:
+            nodes.x[:] = self.view(C.PTR_X, n)
+            nodes.y[:] = self.view(C.PTR_Y, n)
+            nodes.vx[:] = self.view(C.PTR_VX, n)
+            nodes.vy[:] = self.view(C.PTR_VY, n)
+
+    def set_random(self, fn):
+        """None: the device LCG; else a Python callable drawn in d3's order."""
+        if fn is None:
+            self._cb = None
+            self.host_random = None
+            return
+        self._cb = C.RANDOM_FN(lambda _ctx: float(fn()))
+        self.host_random = fn
+        C.check(self.core.sim_set_random(self.h, self._cb, None))
+
+    def close(self):
+        if self.h:
+            self.core.sim_destroy(self.h)
+            self.h = 0
+
+
+class Slot:
+    """src/core.js:174-232: a native force's handle in the core."""
+
+    def __init__(self, kind):
+        self.kind = kind
+        self.ctx = None
+        self.fh = 0
+        self.m = 0
+
+    def bind(self, ctx, n):
+        if ctx is not self.ctx:
+            if self.ctx is not None:
+                self.ctx.core.force_destroy(self.ctx.h, self.fh)
+            self.fh = ctx.core.force_create(ctx.h, self.kind)
+            if not self.fh:
+                raise C.CoreError(C.OUT_OF_MEMORY)
+            self.ctx = ctx
+            self.m = 0
+        ctx.resize(n)
+
+    def count(self, m):
+        C.check(self.ctx.core.force_set_count(self.ctx.h, self.fh, m))
+        self.m = m
+
+    def f64(self, which, m):
+        return self.ctx.core.f64_view(self.ctx.core.force_ptr(self.ctx.h, self.fh, which), m)
+
+    def u32(self, which, m):
+        return self.ctx.core.u32_view(self.ctx.core.force_ptr(self.ctx.h, self.fh, which), m)
+
+    def scalar(self, which, v):
+        self.ctx.core.force_set_scalar(self.ctx.h, self.fh, which, float(v))
+
+    def run(self, alpha, random=None):
+        """src/core.js:213-231: PRECISION, fast-mode ORDER / OPENING and SEED."""
+        ctx = self.ctx
+        fast = ctx.precision
+        self.scalar(C.PRECISION, 1 if fast else 0)
+        if fast:
+            self.scalar(C.ORDER, fast["order"])
+            self.scalar(C.OPENING, fast["opening"])
+            # With the device LCG the core draws SEED itself at force_run.
+            if ctx.host_random is not None and self.kind in (C.MANY_BODY, C.LINK, C.COLLIDE):
+                self.scalar(C.SEED, ctx.host_random())
+        C.check(ctx.core.force_run(ctx.h, self.fh, alpha))
+
+
+class Force:
+    kind = None
+
+    def __init__(self):
+        self.slot = Slot(self.kind)
+        self.nodes = None
+        self.ctx = None
+
+    def initialize(self, nodes, ctx):
+        self.nodes = nodes
+        self.ctx = ctx
+        self._initialize()
+
+    def _initialize(self):
+        self.slot.bind(self.ctx, len(self.nodes))
+
+    def __call__(self, alpha):
+        self._push()
+        self.slot.run(alpha)
+
+    def _push(self):
+        pass
+
+
+class ForceManyBody(Force):
+    """src/manyBody.js: strength -30, distanceMin 1, distanceMax inf, theta 0.9."""
+
+    kind = C.MANY_BODY
+
+    def __init__(self):
+        super().__init__()
+        self._strength = _constant(-30.0)
+        self.distance_min2 = 1.0
+        self.distance_max2 = math.inf
+        self.theta2 = 0.81
+
+    def _initialize(self):
+        n = len(self.nodes)
+        self.slot.bind(self.ctx, n)
+        self.slot.count(n)
+        a = self.slot.f64(C.F0, n)
+        for i in range(n):
+            a[i] = float(self._strength(i))
+
+    def _push(self):
+        self.slot.scalar(C.THETA2, self.theta2)
+        self.slot.scalar(C.DISTANCE_MIN2, self.distance_min2)
+        self.slot.scalar(C.DISTANCE_MAX2, self.distance_max2)
+
+    def strength(self, s):
+        self._strength = _accessor(s)
+        if self.nodes is not None:
+            self._initialize()
+        return self
+
+    def distanceMin(self, d):
+        self.distance_min2 = d * d
+        return self
+
+    def distanceMax(self, d):
+        self.distance_max2 = d * d
+        return self
+
+    def theta(self, t):
+        self.theta2 = t * t
+        return self
+
+
+class ForceLink(Force):
+    """src/link.js: links as node indices; degree count, bias, default
+    strength 1 / min(count[source], count[target]), distance 30."""
+
+    kind = C.LINK
+
+    def __init__(self, source=(), target=()):
+        super().__init__()
+        self.source = np.asarray(source, np.int64)
+        self.target = np.asarray(target, np.int64)
+        self._strength = None  # default strength
+        self._distance = _constant(30.0)
+        self._iterations = 1
+        self.count = None
+        self.bias = None
+
+    def _initialize(self):
+        n, m = len(self.nodes), len(self.source)
+        src, tgt = self.source, self.target
+        count = np.zeros(n, np.int64)
+        np.add.at(count, src, 1)
+        np.add.at(count, tgt, 1)
+        self.count = count
+        cs = count[src].astype(np.float64)
+        ct = count[tgt].astype(np.float64)
+        self.bias = cs / (cs + ct)  # link.js:56-58
+        self.slot.bind(self.ctx, n)
+        self.slot.count(m)
+        if m:
+            self.slot.u32(C.SOURCE, m)[:] = src.astype(np.uint32)
+            self.slot.u32(C.TARGET, m)[:] = tgt.astype(np.uint32)
+            self.slot.f64(C.F2, m)[:] = self.bias
+        self._write_strength()
+        self._write_distance()
+
+    def _write_strength(self):
+        m = len(self.source)
+        if self.nodes is None or not m:
+            return
+        if self._strength is None:  # link.js:30-32
+            cs = self.count[self.source].astype(np.float64)
+            ct = self.count[self.target].astype(np.float64)
+            vals = 1.0 / np.minimum(cs, ct)
+        else:
+            vals = np.array([float(self._strength(i)) for i in range(m)])
+        self.slot.f64(C.F0, m)[:] = vals
+
+    def _write_distance(self):
+        m = len(self.source)
+        if self.nodes is None or not m:
+            return
+        self.slot.f64(C.F1, m)[:] = np.array([float(self._distance(i)) for i in range(m)])
+
+    def _push(self):
+        self.slot.scalar(C.ITERATIONS, self._iterations)
+
+    def iterations(self, k):
+        self._iterations = float(k)
+        return self
+
+    def strength(self, s):
+        self._strength = _accessor(s)
+        self._write_strength()
+        return self
+
+    def distance(self, d):
+        self._distance = _accessor(d)
+        self._write_distance()
+        return self
+
+
+class ForceCollide(Force):
+    """src/collide.js: radius 1, strength 1, iterations 1; alpha ignored."""
+
+    kind = C.COLLIDE
+
+    def __init__(self, radius=None):
+        super().__init__()
+        self._radius = _accessor(1.0 if radius is None else radius)
+        self._strength = 1.0
+        self._iterations = 1.0
+
+    def _initialize(self):
+        n = len(self.nodes)
+        self.slot.bind(self.ctx, n)
+        self.slot.count(n)
+        a = self.slot.f64(C.F0, n)
+        for i in range(n):
+            a[i] = float(self._radius(i))
+
+    def __call__(self, alpha):
+        self._push()
+        self.slot.run(0.0)
+
+    def _push(self):
+        self.slot.scalar(C.STRENGTH, self._strength)
+        self.slot.scalar(C.ITERATIONS, self._iterations)
+
+    def radius(self, r):
+        self._radius = _accessor(r)
+        if self.nodes is not None:
+            self._initialize()
+        return self
+
+    def strength(self, s):
+        self._strength = float(s)
+        return self
+
+    def iterations(self, k):
+        self._iterations = float(k)
+        return self
+
+
+class ForceCenter(Force):
+    """src/center.js"""
+
+    kind = C.CENTER
+
+    def __init__(self, x=0.0, y=0.0):
+        super().__init__()
+        self.cx, self.cy, self._strength = float(x), float(y), 1.0
+
+    def __call__(self, alpha):
+        self._push()
+        self.slot.run(0.0)
+
+    def _push(self):
+        self.slot.scalar(C.CX, self.cx)
+        self.slot.scalar(C.CY, self.cy)
+        self.slot.scalar(C.STRENGTH, self._strength)
+
+    def strength(self, s):
+        self._strength = float(s)
+        return self
+
+
+class _ForceAxis(Force):
+    """src/x.js, src/y.js: strength 0.1, target 0 (NaN target -> strength 0)."""
+
+    def __init__(self, target=0.0):
+        super().__init__()
+        self._target = _accessor(target)
+        self._strength = _constant(0.1)
+
+    def _initialize(self):
+        n = len(self.nodes)
+        tz = np.array([float(self._target(i)) for i in range(n)])
+        st = np.array([0.0 if math.isnan(tz[i]) else float(self._strength(i)) for i in range(n)])
+        self.slot.bind(self.ctx, n)
+        self.slot.count(n)
+        if n:
+            self.slot.f64(C.F0, n)[:] = st
+            self.slot.f64(C.F1, n)[:] = tz
+
+    def strength(self, s):
+        self._strength = _accessor(s)
+        if self.nodes is not None:
+            self._initialize()
+        return self
+
+
+class ForceX(_ForceAxis):
+    kind = C.X
+
+
+class ForceY(_ForceAxis):
+    kind = C.Y
+
+
+class ForceRadial(Force):
+    """src/radial.js"""
+
+    kind = C.RADIAL
+
+    def __init__(self, radius, x=0.0, y=0.0):
+        super().__init__()
+        self._radius = _accessor(radius)
+        self._strength = _constant(0.1)
+        self.cx, self.cy = float(x), float(y)
+
+    def _initialize(self):
+        n = len(self.nodes)
+        rz = np.array([float(self._radius(i)) for i in range(n)])
+        st = np.array([0.0 if math.isnan(rz[i]) else float(self._strength(i)) for i in range(n)])
+        self.slot.bind(self.ctx, n)
+        self.slot.count(n)
+        if n:
+            self.slot.f64(C.F0, n)[:] = st
+            self.slot.f64(C.F1, n)[:] = rz
+
+    def _push(self):
+        self.slot.scalar(C.CX, self.cx)
+        self.slot.scalar(C.CY, self.cy)
+
+
+def d3_lcg(seed=1):
+    """src/lcg.js: d3's LCG as a Python callable (for host-side draws)."""
+    state = [seed & 0xFFFFFFFF]
+
+    def rnd():
+        state[0] = (1664525 * state[0] + 1013904223) % 4294967296
+        return state[0] / 4294967296
+
+    return rnd
+
+
+class Simulation:
+    """src/simulation.js:17-215 over a core."""
+
+    def __init__(self, nodes, core):
+        self.core = core
+        self._nodes = nodes
+        self._alpha = 1.0
+        self._alpha_min = 0.001
+        self._alpha_decay = 1 - math.pow(self._alpha_min, 1 / 300)
+        self._alpha_target = 0.0
+        self._velocity_decay = 0.6
+        self._forces = {}  # insertion order = Map order
+        self._random = None  # None = d3's lcg() on the device
+        self._precision = "exact"
+        self.ctx = Context(core)
+        self.ctx.set_random(None)
+        C.check(core.sim_set_lcg(self.ctx.h, 1))
+        self._initialize_nodes()
+
+    # simulation.js:91-105
+    def _initialize_nodes(self):
+        nd = self._nodes
+        for i in range(nd.n):
+            if not math.isnan(nd.fx[i]):
+                nd.x[i] = nd.fx[i]
+            if not math.isnan(nd.fy[i]):
+                nd.y[i] = nd.fy[i]
+            if math.isnan(nd.x[i]) or math.isnan(nd.y[i]):
+                radius = INITIAL_RADIUS * math.sqrt(0.5 + i)
+                angle = i * INITIAL_ANGLE
+                nd.x[i] = radius * math.cos(angle)
+                nd.y[i] = radius * math.sin(angle)
+            if math.isnan(nd.vx[i]) or math.isnan(nd.vy[i]):
+                nd.vx[i] = nd.vy[i] = 0.0
+        self.ctx.resize(nd.n)
+
+    def tick(self, iterations=1):
+        """simulation.js:49-89, one force_run per force per tick."""
+        if not (0 < iterations):
+            return self
+        ctx = self.ctx
+        ctx.copy_in(self._nodes)
+        ctx.live = True
+        try:
+            for _ in range(int(iterations)):
+                self._alpha += (self._alpha_target - self._alpha) * self._alpha_decay
+                for f in self._forces.values():
+                    f(self._alpha)
+                C.check(self.core.sim_integrate(ctx.h, self._velocity_decay))
+        finally:
+            ctx.live = False
+            ctx.copy_out(self._nodes)
+        return self
+
+    def run(self, ticks):
+        """`ticks` ticks in one engine call (sim_tick); bitwise the same as
+        `ticks` calls of tick(1). Needs the device LCG random source; with a
+        randomSource() callback it falls back to tick(ticks)."""
+        if self._random is not None:
+            return self.tick(ticks)
+        ctx = self.ctx
+        ctx.copy_in(self._nodes)
+        forces = list(self._forces.values())
+        for f in forces:
+            f._push()
+            s = f.slot
+            s.scalar(C.PRECISION, 1 if ctx.precision else 0)
+            if ctx.precision:
+                s.scalar(C.ORDER, ctx.precision["order"])
+                s.scalar(C.OPENING, ctx.precision["opening"])
+        # collide and center get alpha 0 from the facade and ignore it in the
+        # core, so one alpha per tick for every force is equivalent.
+        order = (C._U32 * max(1, len(forces)))(*[f.slot.fh for f in forces])
+        alpha = C._F64(self._alpha)
+        C.check(self.core.sim_tick(ctx.h, int(ticks), alpha, self._alpha_target,
+                                   self._alpha_decay, self._velocity_decay, order, len(forces)))
+        self._alpha = alpha.value
+        ctx.copy_out(self._nodes)
+        return self
+
+    def nodes(self, nodes=None):
+        if nodes is None:
+            return self._nodes
+        self._nodes = nodes
+        self._initialize_nodes()
+        for f in self._forces.values():
+            f.initialize(self._nodes, self.ctx)
+        return self
+
+    def alpha(self, a=None):
+        if a is None:
+            return self._alpha
+        self._alpha = float(a)
+        return self
+
+    def alphaMin(self, a=None):
+        if a is None:
+            return self._alpha_min
+        self._alpha_min = float(a)
+        return self
+
+    def alphaDecay(self, a=None):
+        if a is None:
+            return self._alpha_decay
+        self._alpha_decay = float(a)
+        return self
+
+    def alphaTarget(self, a=None):
+        if a is None:
+            return self._alpha_target
+        self._alpha_target = float(a)
+        return self
+
+    def velocityDecay(self, a=None):
+        if a is None:
+            return 1 - self._velocity_decay
+        self._velocity_decay = 1 - float(a)
+        return self
+
+    def randomSource(self, fn=None):
+        """simulation.js:149-151: a callable drawn for every jiggle, in d3's order."""
+        if fn is None:
+            return self._random
+        self._random = fn
+        self.ctx.set_random(fn)
+        for f in self._forces.values():
+            f.initialize(self._nodes, self.ctx)
+        return self
+
+    def force(self, name, f="__get__"):
+        if f == "__get__":
+            return self._forces.get(name)
+        if f is None:
+            self._forces.pop(name, None)
+        else:
+            f.initialize(self._nodes, self.ctx)
+            self._forces[name] = f
+        return self
+
+    def precision(self, mode=None, order=None, opening=None):
+        """simulation.js:187-200"""
+        if mode is None:
+            return self._precision
+        if mode not in ("exact", "fast"):
+            raise ValueError('precision must be "exact" or "fast"')
+        self._precision = mode
+        if mode == "fast":
+            o = order if order else 8
+            self.ctx.precision = {"order": min(24, max(1, round(float(o)))),
+                                  "opening": max(1.01, float(opening) if opening else 1.5)}
+        else:
+            self.ctx.precision = None
+        return self
+
+    def find(self, x, y, radius=None):
+        """simulation.js:157-178 (host side, on the current node table)."""
+        nd = self._nodes
+        r2 = math.inf if radius is None else radius * radius
+        closest = None
+        for i in range(nd.n):
+            dx, dy = x - nd.x[i], y - nd.y[i]
+            d2 = dx * dx + dy * dy
+            if d2 < r2:
+                closest, r2 = i, d2
+        return closest
+
+    def close(self):
+        self.ctx.close()
+
+
+def forceSimulation(nodes=None, core=None):
+    if core is None:
+        from . import cuda_core
+
+        core = cuda_core()
+    if nodes is None:
+        nodes = Nodes(0)
+    return Simulation(nodes, core)
+
+
+def forceManyBody():
+    return ForceManyBody()
+
+
+def forceLink(source=(), target=()):
+    return ForceLink(source, target)
+
+
+def forceCollide(radius=None):
+    return ForceCollide(radius)
+
+
+def forceCenter(x=0.0, y=0.0):
+    return ForceCenter(x, y)
+
+
+def forceX(x=0.0):
+    return ForceX(x)
+
+
+def forceY(y=0.0):
+    return ForceY(y)
+
+
+def forceRadial(radius, x=0.0, y=0.0):
+    return ForceRadial(radius, x, y)

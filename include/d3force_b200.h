@@ -1,0 +1,144 @@
+/* d3force_b200.h — C ABI of the B200 d3-force tick engine.
+ *
+ * The export set mirrors the core of d3-force-wasm (`src/core/root.zig`):
+ * flat C-style calls that take a simulation handle plus integers or f64 and
+ * return an i32 status or an index. Handles are 1-based with slot reuse.
+ * Pointers returned by `sim_ptr` / `force_ptr` / `tree_info` are host
+ * addresses of pinned host mirrors of the device arrays (the reference
+ * returned wasm linear-memory offsets); they stay valid until the next call
+ * that returns D3_GROWN or resizes the simulation.
+ *
+ * Residency: the device copy is the working copy. Host writes through the
+ * mirrors reach the device at `sim_sync_in` (or, in D3_SYNC_PER_CALL mode,
+ * at the start of every force_run / sim_integrate); results reach the mirrors
+ * at `sim_sync_out` (or after every call in D3_SYNC_PER_CALL mode).
+ *
+ * Threading: one caller thread per simulation; not reentrant (as the
+ * reference, root.zig: single caller thread, `random` called back on it).
+ */
+#ifndef D3FORCE_B200_H
+#define D3FORCE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes: root.zig:16-25 (`Status`). */
+enum {
+  D3_OK = 0,
+  D3_GROWN = 1,
+  D3_ARENA_FULL = 2,
+  D3_RNG_EXHAUSTED = 3,
+  D3_BAD_HANDLE = -1,
+  D3_OUT_OF_MEMORY = -2,
+  D3_BAD_ARGUMENT = -3,
+  D3_WORKER_FAILED = -4 /* a device-side bounded wait expired */
+};
+
+/* Force kinds: force.zig:8 (`Kind`). */
+enum { D3_CENTER = 0, D3_COLLIDE, D3_LINK, D3_MANY_BODY, D3_RADIAL, D3_X, D3_Y };
+
+/* Scalar slots: force.zig:13 (`Scalar`). */
+enum {
+  D3_STRENGTH = 0, D3_CX, D3_CY, D3_THETA2, D3_DISTANCE_MIN2, D3_DISTANCE_MAX2,
+  D3_ITERATIONS, D3_PRECISION, D3_ORDER, D3_OPENING, D3_SEED, D3_SCALARS
+};
+
+/* Array slots: force.zig:21 (`Array`). Per kind: many_body f0 strength;
+ * collide f0 radius; x, y f0 strength, f1 target; radial f0 strength,
+ * f1 radius; link f0 strength, f1 distance, f2 bias, source, target. */
+enum { D3_F0 = 0, D3_F1, D3_F2, D3_SOURCE, D3_TARGET };
+
+/* sim_ptr selectors: sim.zig:14 (`Ptr`). */
+enum {
+  D3_PTR_X = 0, D3_PTR_Y, D3_PTR_VX, D3_PTR_VY, D3_PTR_FX, D3_PTR_FY,
+  D3_PTR_FIXED, D3_PTR_PERM, D3_PTR_RNG_BUF, D3_PTR_SNAP
+};
+
+/* ---- Exports with a counterpart in root.zig ---------------------------- */
+
+/* root.zig:65 `sim_create`: a new empty simulation; 0 on failure. */
+uint32_t sim_create(void);
+/* root.zig:80 `sim_destroy`. */
+int32_t sim_destroy(uint32_t h);
+/* root.zig:88 `sim_set_node_count`: OK, GROWN (mirrors moved) or OUT_OF_MEMORY.
+ * Node-sized force arrays follow the count, padded with NaN (sim.zig:59-73). */
+int32_t sim_set_node_count(uint32_t h, uint32_t n);
+/* root.zig:94 `sim_ptr`: host mirror of x, y, vx, vy, fx, fy (f64[n]),
+ * fixed (u8[n], bit 0 = fx set, bit 1 = fy set), perm (u32[m] after a tree
+ * build), snap (f64[4n] after sim_snapshot). 0 when empty. */
+uintptr_t sim_ptr(uint32_t h, uint32_t which);
+/* root.zig:147 `force_create`: a force of `kind`; 0 on failure. */
+uint32_t force_create(uint32_t h, uint32_t kind);
+/* root.zig:163 `force_destroy`. */
+int32_t force_destroy(uint32_t h, uint32_t fh);
+/* root.zig:174 `force_set_count`: resizes every array of the force to
+ * `count` (nodes, or links for link); new floats NaN, new indices 0.
+ * Always returns GROWN (force.zig:65-82). */
+int32_t force_set_count(uint32_t h, uint32_t fh, uint32_t count);
+/* root.zig:181 `force_ptr`: host mirror of f0, f1, f2 (f64), source, target (u32). */
+uintptr_t force_ptr(uint32_t h, uint32_t fh, uint32_t which);
+/* root.zig:188 `force_set_scalar` / root.zig:196 `force_get_scalar`. */
+int32_t force_set_scalar(uint32_t h, uint32_t fh, uint32_t which, double v);
+double force_get_scalar(uint32_t h, uint32_t fh, uint32_t which);
+/* root.zig:211 `force_run`: applies the force with `alpha`. Exact kernels,
+ * or fast kernels when PRECISION == 1 and n >= 2000 (root.zig:219-248).
+ * BAD_ARGUMENT for a node-sized force with count < n or a link index >= n. */
+int32_t force_run(uint32_t h, uint32_t fh, double alpha);
+/* root.zig:250 `sim_integrate`: v *= decay, p += v, or pin to fx / fy. */
+int32_t sim_integrate(uint32_t h, double velocity_decay);
+/* root.zig:205 `sim_snapshot`: saves vx, vy (and x, y) into `snap`. */
+int32_t sim_snapshot(uint32_t h, uint32_t positions);
+/* root.zig:102 `tree_build`: the d3-quadtree-identical tree on positions
+ * (shifted = 0) or on x + vx, y + vy (1). GROWN when tree mirrors moved. */
+int32_t tree_build(uint32_t h, uint32_t shifted);
+/* root.zig:113 `tree_info`: 0 cell count, 1 root, 2 cells (88-byte records:
+ * child[4] u32, first u32, count u32, x0 y0 x1 y1 x y value r f64), 3 extent
+ * (4 x f64), 4 perm, 5 sizeof(cell) = 88, 6 points in the tree. Pointers are
+ * host addresses (the reference returned u32 offsets). */
+uintptr_t tree_info(uint32_t h, uint32_t which);
+/* root.zig:128 `tree_order`: cell indices in d3-quadtree `visit` order
+ * (after = 0) or `visitAfter` order (after = 1) into out[cell count]. */
+int32_t tree_order(uint32_t h, uint32_t after, uint32_t *out);
+
+/* ---- Extensions (no counterpart in root.zig) -------------------------- */
+
+/* Random source for exact-mode jiggle. The reference imports `env.random`
+ * (root.zig:141) and calls it synchronously; here the caller either registers
+ * a callback (called on the caller thread, in d3's draw order) or selects the
+ * built-in d3 LCG (src/lcg.js: a = 1664525, c = 1013904223, m = 2^32) whose
+ * state lives on the device. In LCG mode, force_run of a many_body, link or
+ * collide force with PRECISION == 1 also draws that force's SEED from the
+ * stream first, as the reference facade does before each run
+ * (src/core.js:218-222). */
+typedef double (*d3_random_fn)(void *ctx);
+int32_t sim_set_random(uint32_t h, d3_random_fn fn, void *ctx);
+int32_t sim_set_lcg(uint32_t h, uint32_t state);
+/* The LCG state after every call issued so far (synchronises). */
+uint32_t sim_get_lcg(uint32_t h);
+
+enum { D3_SYNC_EXPLICIT = 0, D3_SYNC_PER_CALL = 1 };
+int32_t sim_set_sync(uint32_t h, uint32_t mode);
+/* Host mirrors -> device (node state, fixed bits, every force's arrays). */
+int32_t sim_sync_in(uint32_t h);
+/* Device -> host mirrors (x, y, vx, vy). */
+int32_t sim_sync_out(uint32_t h);
+
+/* Runs `ticks` ticks of simulation.js:63-79 on the device without returning
+ * to the host: alpha += (alpha_target - alpha) * alpha_decay, then the forces
+ * in `order[0..n_order)` with that alpha, then integrate. `*alpha` is read and
+ * updated. Requires LCG random mode (or no force that may jiggle). */
+int32_t sim_tick(uint32_t h, uint32_t ticks, double *alpha, double alpha_target,
+                 double alpha_decay, double velocity_decay,
+                 const uint32_t *order, uint32_t n_order);
+
+/* Milliseconds of device time of the last sim_tick call (CUDA events). */
+double sim_last_tick_ms(uint32_t h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* D3FORCE_B200_H */

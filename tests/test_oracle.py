@@ -1,0 +1,244 @@
+"""The CPU oracle against the reference's golden vectors and known answers.
+
+Pins: 19 d3-quadtree traces (test/fixtures/tree-traces.json), the fast-mode
+SHA-256 digests of 5 scenarios at ticks 1/10/100/300
+(test/fixtures/fast-golden.json), d3's own known answers (test/d3/*.js,
+tolerance 1e-6 as test/d3/asserts.js:3-15) and the Zig unit tests
+(src/core/tests.zig, sort.zig, hash.zig, fmm.zig).
+"""
+
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+import helpers as H
+
+C = H.C
+pkg = H.pkg
+sc = H.scenarios
+
+TREE_GOLDEN = H.load_tree_golden()
+
+
+@pytest.mark.parametrize("name", sorted(TREE_GOLDEN))
+def test_tree_matches_d3_quadtree_trace(ocore, name):
+    H.check_trace(ocore, name, TREE_GOLDEN[name])
+
+
+def _fast_golden():
+    with open(os.path.join(H.GOLDEN, "fast_golden.json")) as f:
+        return json.load(f)
+
+
+@pytest.mark.parametrize("name", sc.FAST_SCENARIOS)
+def test_fast_mode_matches_golden_digests(ocore, name):
+    golden = _fast_golden()[name]
+    nodes, sim = sc.setup_fast_scenario(pkg, ocore, name)
+    for t in range(1, sc.CHECKPOINTS[-1] + 1):
+        sim.tick()
+        if t in sc.CHECKPOINTS:
+            assert sc.digest(nodes) == golden[str(t)], "tick %d" % t
+    sim.close()
+
+
+def near(a, b, tol=1e-6):
+    return abs(a - b) < tol
+
+
+def node_equal(nodes, i, x, y, vx, vy):
+    return near(nodes.x[i], x) and near(nodes.y[i], y) and near(nodes.vx[i], vx) and near(nodes.vy[i], vy)
+
+
+def test_simulation_phyllotaxis_start(ocore):
+    """test/d3/simulation-test.js:10-17"""
+    sim = pkg.forceSimulation(core=ocore)
+    sim.nodes(pkg.Nodes(3))
+    nd = sim.nodes()
+    assert node_equal(nd, 0, 7.0710678118654755, 0, 0, 0)
+    assert node_equal(nd, 1, -9.03088751750192, 8.27303273571596, 0, 0)
+    assert node_equal(nd, 2, 1.3823220809823638, -15.750847141167634, 0, 0)
+
+
+def test_collide_known_answers(ocore):
+    """test/d3/collide-test.js:5-19"""
+    collide = pkg.forceCollide(1)
+    sim = pkg.forceSimulation(core=ocore).force("collide", collide)
+    sim.nodes(pkg.Nodes(3))
+    sim.tick(10)
+    nd = sim.nodes()
+    assert node_equal(nd, 0, 7.0710678118654755, 0, 0, 0)
+    assert node_equal(nd, 1, -9.03088751750192, 8.27303273571596, 0, 0)
+    assert node_equal(nd, 2, 1.3823220809823638, -15.750847141167634, 0, 0)
+    collide.radius(100)
+    sim.tick(10)
+    assert node_equal(nd, 0, 174.08616723117228, 66.51743051995625, 0.677346615710878, 0.26976816231064354)
+    assert node_equal(nd, 1, -139.73606544743998, 95.69860503079263, -0.5300880593105067, 0.3545632444404687)
+    assert node_equal(nd, 2, -34.9275994083864, -169.69384995620052, -0.1472585564003713, -0.6243314067511122)
+
+
+def test_collide_respects_fixed(ocore):
+    """test/d3/collide-test.js:22-32"""
+    collide = pkg.forceCollide(1)
+    sim = pkg.forceSimulation(core=ocore).force("collide", collide)
+    nd = pkg.Nodes(3, fx=[0, np.nan, np.nan], fy=[0, np.nan, np.nan])
+    sim.nodes(nd)
+    sim.tick(10)
+    assert node_equal(nd, 0, 0, 0, 0, 0)
+    collide.radius(100)
+    sim.tick(10)
+    assert node_equal(nd, 0, 0, 0, 0, 0)
+
+
+def test_collide_jiggles_equal_positions(ocore):
+    """test/d3/collide-test.js:34-44"""
+    sim = pkg.forceSimulation(core=ocore).force("collide", pkg.forceCollide(1))
+    nd = pkg.Nodes(2, x=[0, 0], y=[0, 0])
+    sim.nodes(nd)
+    sim.tick()
+    assert nd.x[0] != nd.x[1] and nd.y[0] != nd.y[1]
+    assert nd.vx[0] == -nd.vx[1] and nd.vy[0] == -nd.vy[1]
+
+
+def test_collide_jiggles_reproducibly(ocore):
+    """test/d3/collide-test.js:46-50"""
+    nd = pkg.Nodes(10, x=[0] * 10, y=[0] * 10)
+    sim = pkg.forceSimulation(core=ocore).nodes(nd).force("collide", pkg.forceCollide())
+    sim.tick(50)
+    assert node_equal(nd, 0, -5.371433857229194, -2.6644608278592576, 0, 0)
+
+
+def test_center_known_answers(ocore):
+    """test/d3/center-test.js:1-22"""
+    sim = pkg.forceSimulation(core=ocore).force("center", pkg.forceCenter(0, 0))
+    nd = pkg.Nodes(3, x=[100, 200, 300], y=[0, 0, 0])
+    sim.nodes(nd)
+    sim.tick()
+    assert node_equal(nd, 0, -100, 0, 0, 0)
+    assert node_equal(nd, 1, 0, 0, 0, 0)
+    assert node_equal(nd, 2, 100, 0, 0, 0)
+    sim2 = pkg.forceSimulation(core=ocore).force("center", pkg.forceCenter())
+    nd2 = pkg.Nodes(3, fx=[0, np.nan, np.nan], fy=[0, np.nan, np.nan])
+    sim2.nodes(nd2)
+    sim2.tick()
+    assert node_equal(nd2, 0, 0, 0, 0, 0)
+
+
+# --- src/core/tests.zig ports ------------------------------------------------
+
+
+def test_tree_empty_and_all_nan(ocore):
+    """tests.zig:16-25"""
+    t = H.trace(ocore, np.array([]), np.array([]))
+    assert t["cells"] == 0
+    t = H.trace(ocore, np.array([np.nan, 1.0]), np.array([0.0, np.nan]))
+    assert t["cells"] == 0 and math.isnan(H.unbits(t["extent"][0]))
+
+
+def test_tree_single_point(ocore):
+    """tests.zig:27-34"""
+    h = H.build_tree(ocore, np.array([3.25]), np.array([-7.5]))
+    t = ocore.tree(h)
+    assert len(t["cells"]) == 1 and list(t["extent"]) == [3, -8, 4, -7]
+    ocore.sim_destroy(h)
+
+
+def test_tree_coincident_chain(ocore):
+    """tests.zig:36-49"""
+    h = H.build_tree(ocore, np.array([1, 1, -0.0, 1]), np.array([2, 2, 5, 2]))
+    t = ocore.tree(h)
+    found = False
+    for c in t["cells"]:
+        if all(int(k) == H.NONE for k in c["child"]) and c["count"] == 3:
+            assert list(t["perm"][c["first"]:c["first"] + 3]) == [0, 1, 3]
+            found = True
+    assert found
+    ocore.sim_destroy(h)
+
+
+def test_tree_two_points(ocore):
+    """tests.zig:51-60"""
+    h = H.build_tree(ocore, np.array([0.0, 1.0]), np.array([0.0, 1.0]))
+    t = ocore.tree(h)
+    assert list(t["extent"]) == [0, 0, 2, 2]
+    r = t["cells"][t["root"]]["child"]
+    assert r[0] != H.NONE and r[3] != H.NONE and r[1] == H.NONE and r[2] == H.NONE
+    ocore.sim_destroy(h)
+
+
+def test_tree_near_duplicates_separate(ocore):
+    """tests.zig:62-76"""
+    h = H.build_tree(ocore, np.array([0, 1024, 0.5, 0.5 + 1e-12]), np.array([0, 1024, 0.25, 0.25]))
+    t = ocore.tree(h)
+    leaves = [c for c in t["cells"] if all(int(k) == H.NONE for k in c["child"])]
+    assert len(leaves) == 4
+    assert min(c["x1"] - c["x0"] for c in leaves) < 2048.0 / 2**32
+    ocore.sim_destroy(h)
+
+
+def test_tree_order_pre_and_post(ocore):
+    """tests.zig:97-116"""
+    h = H.build_tree(ocore, np.array([0, 3, 1, 2, 3.5]), np.array([0, 3, 2, 1, 0.5]))
+    t = ocore.tree(h)
+    n = len(t["cells"])
+    assert list(ocore.order(h, 0)) == list(range(n))
+    after = list(ocore.order(h, 1))
+    assert after[-1] == t["root"]
+    pos = {c: i for i, c in enumerate(after)}
+    for i, c in enumerate(t["cells"]):
+        for ch in c["child"]:
+            if int(ch) != H.NONE:
+                assert pos[int(ch)] < pos[i]
+    ocore.sim_destroy(h)
+
+
+def test_node_sized_arrays_padded_with_nan(ocore):
+    """tests.zig:128-143"""
+    h = ocore.sim_create()
+    fh = ocore.force_create(h, C.X)
+    assert ocore.force_set_count(h, fh, 2) == C.GROWN
+    f0 = ocore.f64_view(ocore.force_ptr(h, fh, C.F0), 2)
+    f1 = ocore.f64_view(ocore.force_ptr(h, fh, C.F1), 2)
+    f0[0], f1[1] = 1, 2
+    assert ocore.sim_set_node_count(h, 5) == C.GROWN
+    f0 = ocore.f64_view(ocore.force_ptr(h, fh, C.F0), 5)
+    f1 = ocore.f64_view(ocore.force_ptr(h, fh, C.F1), 5)
+    assert f0[0] == 1 and f1[1] == 2
+    assert np.isnan(f0[2:]).all() and np.isnan(f1[2:]).all()
+    ocore.sim_destroy(h)
+
+
+def test_bad_link_index_rejected(ocore):
+    """tests.zig:145-161, link.zig:10-12"""
+    h = ocore.sim_create()
+    ocore.sim_set_node_count(h, 3)
+    fh = ocore.force_create(h, C.LINK)
+    ocore.force_set_count(h, fh, 1)
+    ocore.sim_set_node_count(h, 10)
+    ocore.u32_view(ocore.force_ptr(h, fh, C.SOURCE), 1)[0] = 0
+    ocore.u32_view(ocore.force_ptr(h, fh, C.TARGET), 1)[0] = 10
+    ocore.force_set_scalar(h, fh, C.ITERATIONS, 1)
+    assert ocore.force_run(h, fh, 1.0) == C.BAD_ARGUMENT
+    ocore.sim_destroy(h)
+
+
+def test_integrate_fixed_per_axis(ocore):
+    """tests.zig:163-182"""
+    h = ocore.sim_create()
+    ocore.sim_set_node_count(h, 2)
+    v = lambda w: ocore.f64_view(ocore.sim_ptr(h, w), 2)  # noqa: E731
+    v(C.PTR_X)[:] = 1
+    v(C.PTR_Y)[:] = 2
+    v(C.PTR_VX)[:] = 10
+    v(C.PTR_VY)[:] = 20
+    v(C.PTR_FX)[:] = -5
+    v(C.PTR_FY)[:] = -6
+    ocore.u8_view(ocore.sim_ptr(h, C.PTR_FIXED), 2)[:] = [0, 2]
+    ocore.sim_sync_in(h)
+    assert ocore.sim_integrate(h, 0.5) == 0
+    ocore.sim_sync_out(h)
+    assert list(v(C.PTR_X)) == [6, 6] and list(v(C.PTR_VX)) == [5, 5]
+    assert list(v(C.PTR_Y)) == [12, -6] and list(v(C.PTR_VY)) == [10, 0]
+    ocore.sim_destroy(h)

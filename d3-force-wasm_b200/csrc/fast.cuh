@@ -1,0 +1,58 @@
+// fast.cuh — fast mode (precision 'fast', n >= 2000): FMM many-body, uniform
+// grid collide, Jacobi link (fmm.zig, grid.zig, link_fast.zig).
+#pragma once
+
+#include "common.cuh"
+#include "forces.cuh"
+#include "tree.cuh"
+
+namespace d3 {
+
+constexpr uint32_t FAST_MIN_N = 2000;  // fmm.zig:43
+
+struct FastScratch {
+  uint32_t cap = 0;
+  double *seed = nullptr;  // the running force's SEED (f64 bits = hash seed)
+  // grid collide
+  uint64_t *g_keys = nullptr, *g_keys_tmp = nullptr;
+  uint32_t *g_items = nullptr, *g_items_tmp = nullptr, *g_cell_of = nullptr, *g_start = nullptr;
+  uint32_t *g_hist = nullptr, *g_part = nullptr;
+  double *g_box = nullptr;      // per-block partial bounds
+  uint32_t *g_info = nullptr;   // grid geometry: gx, gy, cells, m, active, ticket
+  double *g_geom = nullptr;     // x0, y0, inv_h
+  // FMM
+  void *fmm = nullptr;
+};
+
+int fast_reserve(FastScratch &s, uint32_t n);
+void fast_free(FastScratch &s);
+
+// The per-run SEED: one draw from the device LCG (src/core.js:221), or a
+// value the host drew from the caller's random function.
+void draw_seed(Rng *rng, double *seed, cudaStream_t st);
+void set_seed(double *seed, double value, cudaStream_t st);
+
+// link_fast.zig: CSR adjacency (edge id, TARGET_BIT on the target's entry),
+// rows filled from the back so each row lists its edges in descending order.
+struct FastLink {
+  uint32_t n = 0, m = 0;
+  uint32_t *row = nullptr, *adj = nullptr;
+};
+int fast_link_build(FastLink &c, const uint32_t *src, const uint32_t *tgt, uint32_t m, uint32_t n);
+void fast_link_free(FastLink &c);
+void fast_link(const NodeArrays &a, const LinkArrays &l, const FastLink &c, double alpha,
+               double iterations, const double *seed, cudaStream_t st);
+
+// grid.zig:198-286
+void fast_collide(FastScratch &s, const NodeArrays &a, const double *radii, double strength,
+                  double iterations, const double *seed, cudaStream_t st);
+
+struct FmmParams {
+  double order, opening, dmin2, dmax2, alpha;
+};
+// fmm.zig:247-354. Returns 1 when applied, 0 when the exact kernel must run
+// instead (non-finite extent), < 0 on failure.
+int fmm_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *strengths,
+            const FmmParams &p, const double *seed, uint32_t *status, cudaStream_t st);
+
+}  // namespace d3

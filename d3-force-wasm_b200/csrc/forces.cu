@@ -1,0 +1,711 @@
+// forces.cu — exact-mode forces on the device, bit-exact with d3-force.
+//
+// All arithmetic keeps d3's statement order (no FMA contraction: the file is
+// built with -fmad=false). Traversals are stackless: cells are in d3's visit
+// preorder, so "descend" is c + 1 and "do not descend" is skip[c].
+#include <vector>
+
+#include "forces.cuh"
+#include "scan_sort.cuh"
+
+namespace d3 {
+
+int scratch_reserve(ForceScratch &s, uint32_t n) {
+  if (!s.counters) {
+    D3_CUDA_OK(cudaMalloc(&s.counters, 16 * sizeof(uint32_t)));
+    D3_CUDA_OK(cudaMemset(s.counters, 0, 16 * sizeof(uint32_t)));
+    D3_CUDA_OK(cudaMalloc(&s.center, 2 * sizeof(double)));
+  }
+  if (n <= s.cap && s.cap) return 0;
+  uint32_t cap = n < 1024 ? 1024 : n;
+  cudaFree(s.draws); cudaFree(s.offsets); cudaFree(s.scan_part);
+  D3_CUDA_OK(cudaMalloc(&s.draws, (cap + 1) * 4ull));
+  D3_CUDA_OK(cudaMalloc(&s.offsets, (cap + 1) * 4ull));
+  D3_CUDA_OK(cudaMalloc(&s.scan_part, scan_partial_words(cap + 1) * 4));
+  s.cap = cap;
+  return 0;
+}
+
+void scratch_free(ForceScratch &s) {
+  cudaFree(s.draws); cudaFree(s.offsets); cudaFree(s.scan_part); cudaFree(s.counters);
+  cudaFree(s.center);
+  s = ForceScratch();
+}
+
+// ---------------------------------------------------------------------------
+// Bottom-up passes (visitAfter): the last child to finish computes its parent.
+// ---------------------------------------------------------------------------
+
+__device__ inline double ld_cg(const double *p) { return __ldcg(p); }
+
+// many_body.zig:101-135 (accumulate). Leaf: head position, strength summed
+// over the chain from perm[first + count - 1] down. Internal: children 0..3
+// with a truthy |value|.
+__global__ void k_mb_accumulate(Cell *cells, const uint32_t *parent, uint32_t *counter,
+                                const uint32_t *perm, const double *xs, const double *ys,
+                                const double *strengths, const uint32_t *info) {
+  const uint32_t len = info[1];
+  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < len; c += gridDim.x * blockDim.x) {
+    Cell *q = &cells[c];
+    if (!is_leaf(*q)) continue;
+    uint32_t head = perm[q->first + q->count - 1];
+    double strength = 0;
+    for (uint32_t k = q->first + q->count; k > q->first;) {
+      --k;
+      strength += strengths[perm[k]];
+    }
+    q->x = xs[head];
+    q->y = ys[head];
+    q->value = strength;
+    uint32_t cur = c;
+    for (;;) {
+      uint32_t p = parent[cur];
+      if (p == NONE) break;
+      Cell *pc = &cells[p];
+      uint32_t nch = 0;
+      for (int k = 0; k < 4; ++k) nch += pc->child[k] != NONE;
+      __threadfence();
+      if (atomicAdd(&counter[p], 1u) != nch - 1) break;
+      __threadfence();
+      double st = 0, weight = 0, x = 0, y = 0;
+      for (int k = 0; k < 4; ++k) {
+        uint32_t ch = pc->child[k];
+        if (ch == NONE) continue;
+        double v = ld_cg(&cells[ch].value);
+        double w = fabs(v);
+        if (w > 0) {
+          st += v;
+          weight += w;
+          x += w * ld_cg(&cells[ch].x);
+          y += w * ld_cg(&cells[ch].y);
+        }
+      }
+      pc->x = x / weight;
+      pc->y = y / weight;
+      pc->value = st;
+      cur = p;
+    }
+  }
+}
+
+// collide.zig:117-129 (prepare): leaf radius of its head, internal the largest
+// child radius (strict >, from 0).
+__global__ void k_collide_prep(Cell *cells, const uint32_t *parent, uint32_t *counter,
+                               const uint32_t *perm, const double *radii, const uint32_t *info) {
+  const uint32_t len = info[1];
+  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < len; c += gridDim.x * blockDim.x) {
+    Cell *q = &cells[c];
+    if (!is_leaf(*q)) continue;
+    q->r = radii[perm[q->first + q->count - 1]];
+    uint32_t cur = c;
+    for (;;) {
+      uint32_t p = parent[cur];
+      if (p == NONE) break;
+      Cell *pc = &cells[p];
+      uint32_t nch = 0;
+      for (int k = 0; k < 4; ++k) nch += pc->child[k] != NONE;
+      __threadfence();
+      if (atomicAdd(&counter[p], 1u) != nch - 1) break;
+      __threadfence();
+      double r = 0;
+      for (int k = 0; k < 4; ++k) {
+        uint32_t ch = pc->child[k];
+        if (ch == NONE) continue;
+        double cr = ld_cg(&cells[ch].r);
+        if (cr > r) r = cr;
+      }
+      pc->r = r;
+      cur = p;
+    }
+  }
+}
+
+__global__ void k_zero_counters(uint32_t *counter, const uint32_t *info) {
+  const uint32_t len = info[1];
+  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < len; c += gridDim.x * blockDim.x)
+    counter[c] = 0;
+}
+
+// ---------------------------------------------------------------------------
+// Exact many-body traversal (many_body.zig:176-263)
+// ---------------------------------------------------------------------------
+
+// One target. RECORD: stop accumulating at the first zero delta d3 would
+// jiggle, count the draws it would make, and do not write. Otherwise draws
+// come from the stream at `draw0`.
+template <bool RECORD>
+__device__ inline uint32_t mb_node(const Cell *cells, const uint32_t *skip, const uint32_t *perm,
+                                   uint32_t len, const double *xs, const double *ys,
+                                   double *vxs, double *vys, const double *strengths,
+                                   const ManyBodyParams p, uint32_t i, const Rng *rng,
+                                   uint64_t draw0) {
+  const double nx = xs[i], ny = ys[i];
+  double vx = vxs[i], vy = vys[i];
+  uint32_t draws = 0;
+  bool flagged = false;
+  uint32_t c = 0;
+  while (c < len) {
+    const Cell &q = cells[c];
+    const double value = q.value;
+    if (!(value != 0 && value == value)) {
+      c = skip[c];
+      continue;
+    }
+    double x = q.x - nx, y = q.y - ny;
+    const double w = q.x1 - q.x0;
+    double l = x * x + y * y;
+    if (w * w / p.theta2 < l) {
+      if (l < p.dmax2) {
+        if (RECORD && (x == 0 || y == 0)) {
+          flagged = true;
+          draws += (x == 0) + (y == 0);
+        } else if (!flagged) {
+          if (!RECORD) {
+            if (x == 0) { x = (rng_draw_at(*rng, draw0 + draws++) - 0.5) * 1e-6; l += x * x; }
+            if (y == 0) { y = (rng_draw_at(*rng, draw0 + draws++) - 0.5) * 1e-6; l += y * y; }
+          }
+          if (l < p.dmin2) l = sqrt(p.dmin2 * l);
+          vx += x * value * p.alpha / l;
+          vy += y * value * p.alpha / l;
+        }
+      }
+      c = skip[c];
+      continue;
+    }
+    if (!is_leaf(q)) {
+      c = c + 1;
+      continue;
+    }
+    if (l >= p.dmax2) {
+      c = c + 1;
+      continue;
+    }
+    const uint32_t first = q.first, count = q.count;
+    const uint32_t head = perm[first + count - 1];
+    if (head != i || count > 1) {
+      if (RECORD && (x == 0 || y == 0)) {
+        flagged = true;
+        draws += (x == 0) + (y == 0);
+      } else if (!flagged) {
+        if (!RECORD) {
+          if (x == 0) { x = (rng_draw_at(*rng, draw0 + draws++) - 0.5) * 1e-6; l += x * x; }
+          if (y == 0) { y = (rng_draw_at(*rng, draw0 + draws++) - 0.5) * 1e-6; l += y * y; }
+        }
+        if (l < p.dmin2) l = sqrt(p.dmin2 * l);
+      }
+    }
+    if (!flagged) {
+      for (uint32_t k = first + count; k > first;) {
+        --k;
+        const uint32_t j = perm[k];
+        if (j != i) {
+          const double wj = strengths[j] * p.alpha / l;
+          vx += x * wj;
+          vy += y * wj;
+        }
+      }
+    }
+    c = c + 1;
+  }
+  if (!flagged) {
+    vxs[i] = vx;
+    vys[i] = vy;
+  }
+  return flagged ? draws : 0;
+}
+
+// Record pass over all nodes in Morton order (perm, then the NaN nodes).
+__global__ void __launch_bounds__(128) k_mb_traverse(const Cell *cells, const uint32_t *skip,
+                                                     const uint32_t *perm, const uint32_t *info,
+                                                     const double *xs, const double *ys, double *vxs,
+                                                     double *vys, const double *strengths,
+                                                     ManyBodyParams p, uint32_t n, uint32_t *draws,
+                                                     uint32_t *counters) {
+  const uint32_t pos = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pos >= n) return;
+  const uint32_t len = info[1];
+  const uint32_t i = perm[pos];
+  uint32_t d = len ? mb_node<true>(cells, skip, perm, len, xs, ys, vxs, vys, strengths, p, i,
+                                   nullptr, 0)
+                   : 0;
+  draws[i] = d;
+  if (d) atomicAdd(&counters[1], 1u);
+}
+
+// Flagged nodes again, each from its own offset in the draw stream (the
+// exclusive scan of draws over node index = d3's draw order).
+__global__ void __launch_bounds__(128) k_mb_rerun(const Cell *cells, const uint32_t *skip,
+                                                  const uint32_t *perm, const uint32_t *info,
+                                                  const double *xs, const double *ys, double *vxs,
+                                                  double *vys, const double *strengths,
+                                                  ManyBodyParams p, uint32_t n,
+                                                  const uint32_t *draws, const uint32_t *offsets,
+                                                  const uint32_t *counters, const Rng *rng) {
+  if (counters[1] == 0) return;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || draws[i] == 0) return;
+  mb_node<false>(cells, skip, perm, info[1], xs, ys, vxs, vys, strengths, p, i, rng, offsets[i]);
+}
+
+__global__ void k_rng_advance(Rng *rng, const uint32_t *total) {
+  uint32_t t = *total;
+  if (t == 0) return;
+  if (rng->mode == 0) rng->lcg = lcg_skip(rng->lcg, t);
+  else rng->pos += t;
+}
+
+static void climb_grid(unsigned &blocks, unsigned &threads, uint32_t cap) {
+  threads = 256;
+  blocks = blocks_for(cap, threads);
+  if (blocks > 148 * 16) blocks = 148 * 16;
+}
+
+void many_body_exact(TreeDev &t, const NodeArrays &a, const double *strengths,
+                     const ManyBodyParams &p, Rng *rng, ForceScratch &s, uint32_t *status,
+                     bool host_draws, cudaStream_t st) {
+  const uint32_t n = a.n;
+  tree_build(t, a.x, a.y, n, status, st);
+  if (n == 0) return;
+  unsigned cb, ct;
+  climb_grid(cb, ct, t.cells_cap);
+  k_mb_accumulate<<<cb, ct, 0, st>>>(t.cells, t.parent, t.counter, t.perm, a.x, a.y, strengths,
+                                     t.info);
+  cudaMemsetAsync(s.counters, 0, 2 * sizeof(uint32_t), st);
+  k_mb_traverse<<<blocks_for(n, 128), 128, 0, st>>>(t.cells, t.skip, t.perm, t.info, a.x, a.y,
+                                                    a.vx, a.vy, strengths, p, n, s.draws,
+                                                    s.counters);
+  scan_u32(s.draws, s.offsets, n, s.scan_part, s.counters, st);
+  if (!host_draws) many_body_rerun(t, a, strengths, p, rng, s, st);
+}
+
+void many_body_rerun(TreeDev &t, const NodeArrays &a, const double *strengths,
+                     const ManyBodyParams &p, Rng *rng, ForceScratch &s, cudaStream_t st) {
+  const uint32_t n = a.n;
+  k_mb_rerun<<<blocks_for(n, 128), 128, 0, st>>>(t.cells, t.skip, t.perm, t.info, a.x, a.y, a.vx,
+                                                 a.vy, strengths, p, n, s.draws, s.offsets,
+                                                 s.counters, rng);
+  k_rng_advance<<<1, 1, 0, st>>>(rng, s.counters);
+}
+
+// ---------------------------------------------------------------------------
+// Exact link (link.zig:8-40)
+// ---------------------------------------------------------------------------
+
+int link_plan_build(LinkPlan &plan, const uint32_t *src, const uint32_t *tgt, uint32_t m) {
+  // level(e) = 1 + the largest level of an earlier link sharing a node, so
+  // every link sees exactly the velocities its predecessors wrote.
+  uint32_t nmax = 0;
+  for (uint32_t e = 0; e < m; ++e) {
+    if (src[e] + 1 > nmax) nmax = src[e] + 1;
+    if (tgt[e] + 1 > nmax) nmax = tgt[e] + 1;
+  }
+  std::vector<uint32_t> node_level(nmax, 0), level(m);
+  uint32_t levels = 0;
+  for (uint32_t e = 0; e < m; ++e) {
+    uint32_t l = (node_level[src[e]] > node_level[tgt[e]] ? node_level[src[e]] : node_level[tgt[e]]) + 1;
+    level[e] = l;
+    node_level[src[e]] = l;
+    node_level[tgt[e]] = l;
+    if (l > levels) levels = l;
+  }
+  std::vector<uint32_t> start(levels + 2, 0), order(m > 0 ? m : 1);
+  for (uint32_t e = 0; e < m; ++e) start[level[e]]++;
+  uint32_t run = 0;
+  for (uint32_t l = 0; l <= levels + 1; ++l) {
+    uint32_t c = start[l];
+    start[l] = run;
+    run += c;
+  }
+  std::vector<uint32_t> fill(start.begin(), start.end());
+  for (uint32_t e = 0; e < m; ++e) order[fill[level[e]]++] = e;
+  link_plan_free(plan);
+  D3_CUDA_OK(cudaMalloc(&plan.order, order.size() * 4));
+  D3_CUDA_OK(cudaMalloc(&plan.level_start, start.size() * 4));
+  D3_CUDA_OK(cudaMemcpy(plan.order, order.data(), order.size() * 4, cudaMemcpyHostToDevice));
+  D3_CUDA_OK(cudaMemcpy(plan.level_start, start.data(), start.size() * 4, cudaMemcpyHostToDevice));
+  plan.h_level_start = new uint32_t[start.size()];
+  for (size_t k = 0; k < start.size(); ++k) plan.h_level_start[k] = start[k];
+  plan.m = m;
+  plan.levels = levels;
+  return 0;
+}
+
+void link_plan_free(LinkPlan &plan) {
+  cudaFree(plan.order);
+  cudaFree(plan.level_start);
+  delete[] plan.h_level_start;
+  plan = LinkPlan();
+}
+
+// One link, d3's statement order. Returns false (writing nothing) where d3
+// would draw from `random`.
+__device__ inline bool link_one(double *xs, double *ys, double *vxs, double *vys, const LinkArrays l,
+                                uint32_t e, double alpha) {
+  const uint32_t src = l.source[e], tgt = l.target[e];
+  double x = xs[tgt] + vxs[tgt] - xs[src] - vxs[src];
+  double y = ys[tgt] + vys[tgt] - ys[src] - vys[src];
+  if (x == 0 || x != x || y == 0 || y != y) return false;
+  double len = sqrt(x * x + y * y);
+  len = (len - l.distance[e]) / len * alpha * l.strength[e];
+  x *= len;
+  y *= len;
+  double b = l.bias[e];
+  vxs[tgt] -= x * b;
+  vys[tgt] -= y * b;
+  b = 1 - b;
+  vxs[src] += x * b;
+  vys[src] += y * b;
+  return true;
+}
+
+__global__ void k_link_level(double *xs, double *ys, double *vxs, double *vys, LinkArrays l,
+                             const uint32_t *order, uint32_t lo, uint32_t hi, double alpha,
+                             uint32_t *flag) {
+  uint32_t k = lo + blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= hi) return;
+  if (!link_one(xs, ys, vxs, vys, l, order[k], alpha)) atomicOr(flag, 1u);
+}
+
+__global__ void k_restore_v(double *vx, double *vy, const double *svx, const double *svy, uint32_t n,
+                            const uint32_t *flag) {
+  if (*flag == 0) return;
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  vx[i] = svx[i];
+  vy[i] = svy[i];
+}
+
+__global__ void k_save_v(double *svx, double *svy, const double *vx, const double *vy, uint32_t n) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  svx[i] = vx[i];
+  svy[i] = vy[i];
+}
+
+// link.zig:8-40 on one thread, drawing from the device LCG.
+__global__ void k_link_serial(double *xs, double *ys, double *vxs, double *vys, LinkArrays l,
+                              double alpha, double iterations, Rng *rng, const uint32_t *flag,
+                              uint32_t *status) {
+  if (*flag == 0) return;
+  atomicOr(status, ST_LINK_JIGGLE);
+  uint32_t s = rng->lcg;
+  for (double k = 0; k < iterations; k += 1) {
+    for (uint32_t i = 0; i < l.m; ++i) {
+      const uint32_t src = l.source[i], tgt = l.target[i];
+      double x = xs[tgt] + vxs[tgt] - xs[src] - vxs[src];
+      if (x == 0 || x != x) { s = lcg_step(s); x = (lcg_value(s) - 0.5) * 1e-6; }
+      double y = ys[tgt] + vys[tgt] - ys[src] - vys[src];
+      if (y == 0 || y != y) { s = lcg_step(s); y = (lcg_value(s) - 0.5) * 1e-6; }
+      double len = sqrt(x * x + y * y);
+      len = (len - l.distance[i]) / len * alpha * l.strength[i];
+      x *= len;
+      y *= len;
+      double b = l.bias[i];
+      vxs[tgt] -= x * b;
+      vys[tgt] -= y * b;
+      b = 1 - b;
+      vxs[src] += x * b;
+      vys[src] += y * b;
+    }
+  }
+  rng->lcg = s;
+}
+
+// The same with draws pulled by the host: resumes at (resume[0], resume[1]),
+// stops before a link whose draws are not in the buffer yet.
+__global__ void k_link_serial_host(double *xs, double *ys, double *vxs, double *vys, LinkArrays l,
+                                   double alpha, double iterations, Rng *rng, uint32_t *resume) {
+  uint64_t used = 0, avail = rng->avail - rng->pos;
+  const double *buf = rng->buf + rng->pos;
+  uint32_t it = resume[0], i0 = resume[1];
+  for (double k = (double)it; k < iterations; k += 1, ++it, i0 = 0) {
+    for (uint32_t i = i0; i < l.m; ++i) {
+      const uint32_t src = l.source[i], tgt = l.target[i];
+      double x = xs[tgt] + vxs[tgt] - xs[src] - vxs[src];
+      double y = ys[tgt] + vys[tgt] - ys[src] - vys[src];
+      uint32_t need = (x == 0 || x != x) + (y == 0 || y != y);
+      if (used + need > avail) {
+        resume[0] = it;
+        resume[1] = i;
+        resume[2] = (uint32_t)(used + need - avail);
+        rng->pos += used;
+        return;
+      }
+      if (x == 0 || x != x) x = (buf[used++] - 0.5) * 1e-6;
+      if (y == 0 || y != y) y = (buf[used++] - 0.5) * 1e-6;
+      double len = sqrt(x * x + y * y);
+      len = (len - l.distance[i]) / len * alpha * l.strength[i];
+      x *= len;
+      y *= len;
+      double b = l.bias[i];
+      vxs[tgt] -= x * b;
+      vys[tgt] -= y * b;
+      b = 1 - b;
+      vxs[src] += x * b;
+      vys[src] += y * b;
+    }
+  }
+  resume[2] = 0;
+  rng->pos += used;
+}
+
+void link_exact(const NodeArrays &a, const LinkArrays &l, const LinkPlan &plan, double alpha,
+                double iterations, Rng *rng, uint32_t *flag, cudaStream_t st) {
+  if (l.m == 0) return;
+  const uint32_t n = a.n;
+  cudaMemsetAsync(flag, 0, sizeof(uint32_t), st);
+  k_save_v<<<blocks_for(n, 256), 256, 0, st>>>(a.snap_vx, a.snap_vy, a.vx, a.vy, n);
+  for (double k = 0; k < iterations; k += 1) {
+    for (uint32_t lv = 1; lv <= plan.levels; ++lv) {
+      uint32_t lo = plan.h_level_start[lv], hi = plan.h_level_start[lv + 1];
+      if (hi > lo)
+        k_link_level<<<blocks_for(hi - lo, 128), 128, 0, st>>>(a.x, a.y, a.vx, a.vy, l, plan.order,
+                                                                lo, hi, alpha, flag);
+    }
+  }
+  k_restore_v<<<blocks_for(n, 256), 256, 0, st>>>(a.vx, a.vy, a.snap_vx, a.snap_vy, n, flag);
+}
+
+void link_serial_host(const NodeArrays &a, const LinkArrays &l, double alpha, double iterations,
+                      Rng *rng, uint32_t *resume, cudaStream_t st) {
+  k_link_serial_host<<<1, 1, 0, st>>>(a.x, a.y, a.vx, a.vy, l, alpha, iterations, rng, resume);
+}
+
+// Serial link on the device LCG, after a DAG pass that met a jiggle.
+void link_fallback_lcg(const NodeArrays &a, const LinkArrays &l, double alpha, double iterations,
+                       Rng *rng, const uint32_t *flag, uint32_t *status, cudaStream_t st) {
+  k_link_serial<<<1, 1, 0, st>>>(a.x, a.y, a.vx, a.vy, l, alpha, iterations, rng, flag, status);
+}
+
+// ---------------------------------------------------------------------------
+// Exact collide (collide.zig:17-102), serial node order
+// ---------------------------------------------------------------------------
+
+__global__ void k_shift(const double *x, const double *y, const double *vx, const double *vy,
+                        double *px, double *py, uint32_t n) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  px[i] = x[i] + vx[i];
+  py[i] = y[i] + vy[i];
+}
+
+// The node loop of collide.zig:47-100 from node i0. In host-draw mode a turn
+// first counts its draws (decided by the state at the turn's start) and stops
+// before the turn when the buffer is short.
+__global__ void k_collide_serial(const Cell *cells, const uint32_t *skip, const uint32_t *perm,
+                                 const uint32_t *info, const double *xs, const double *ys, double *vxs,
+                                 double *vys, const double *radii, double strength, uint32_t n,
+                                 Rng *rng, bool host_draws, uint32_t *resume) {
+  const uint32_t len = info[1];
+  if (len == 0) {
+    if (resume) resume[2] = 0;
+    return;
+  }
+  uint32_t s = rng->lcg;
+  uint64_t used = 0, avail = host_draws ? rng->avail - rng->pos : 0;
+  const double *buf = host_draws ? rng->buf + rng->pos : nullptr;
+  uint32_t i0 = resume ? resume[0] : 0;
+  for (uint32_t i = i0; i < n; ++i) {
+    const double ri = radii[i], ri2 = ri * ri;
+    const double xi = xs[i] + vxs[i], yi = ys[i] + vys[i];
+    if (host_draws) {
+      uint32_t need = 0;
+      for (uint32_t c = 0; c < len;) {
+        const Cell &q = cells[c];
+        double r = ri + q.r;
+        if (is_leaf(q)) {
+          uint32_t j = perm[q.first + q.count - 1];
+          if (j > i) {
+            double x = xi - xs[j] - vxs[j], y = yi - ys[j] - vys[j];
+            if (x * x + y * y < r * r) need += (x == 0) + (y == 0);
+          }
+          c = c + 1;
+          continue;
+        }
+        if (q.x0 > xi + r || q.x1 < xi - r || q.y0 > yi + r || q.y1 < yi - r) c = skip[c];
+        else c = c + 1;
+      }
+      if (used + need > avail) {
+        resume[0] = i;
+        resume[2] = (uint32_t)(used + need - avail);
+        rng->pos += used;
+        return;
+      }
+    }
+    for (uint32_t c = 0; c < len;) {
+      const Cell &q = cells[c];
+      double rj = q.r;
+      double r = ri + rj;
+      if (is_leaf(q)) {
+        const uint32_t j = perm[q.first + q.count - 1];
+        if (j > i) {
+          double x = xi - xs[j] - vxs[j];
+          double y = yi - ys[j] - vys[j];
+          double l = x * x + y * y;
+          if (l < r * r) {
+            if (x == 0) {
+              double u;
+              if (host_draws) u = buf[used++]; else { s = lcg_step(s); u = lcg_value(s); }
+              x = (u - 0.5) * 1e-6;
+              l += x * x;
+            }
+            if (y == 0) {
+              double u;
+              if (host_draws) u = buf[used++]; else { s = lcg_step(s); u = lcg_value(s); }
+              y = (u - 0.5) * 1e-6;
+              l += y * y;
+            }
+            l = sqrt(l);
+            l = (r - l) / l * strength;
+            x *= l;
+            y *= l;
+            rj *= rj;
+            r = rj / (ri2 + rj);
+            vxs[i] += x * r;
+            vys[i] += y * r;
+            r = 1 - r;
+            vxs[j] -= x * r;
+            vys[j] -= y * r;
+          }
+        }
+        c = c + 1;
+        continue;
+      }
+      if (q.x0 > xi + r || q.x1 < xi - r || q.y0 > yi + r || q.y1 < yi - r) c = skip[c];
+      else c = c + 1;
+    }
+  }
+  if (host_draws) rng->pos += used;
+  else rng->lcg = s;
+  if (resume) resume[2] = 0;
+}
+
+void shift_positions(const NodeArrays &a, cudaStream_t st) {
+  if (a.n == 0) return;
+  k_shift<<<blocks_for(a.n, 256), 256, 0, st>>>(a.x, a.y, a.vx, a.vy, a.px, a.py, a.n);
+}
+
+void collide_setup(TreeDev &t, const NodeArrays &a, const double *radii, uint32_t *status,
+                   cudaStream_t st) {
+  const uint32_t n = a.n;
+  k_shift<<<blocks_for(n, 256), 256, 0, st>>>(a.x, a.y, a.vx, a.vy, a.px, a.py, n);
+  tree_build(t, a.px, a.py, n, status, st);
+  if (n == 0) return;
+  unsigned cb, ct;
+  climb_grid(cb, ct, t.cells_cap);
+  k_collide_prep<<<cb, ct, 0, st>>>(t.cells, t.parent, t.counter, t.perm, radii, t.info);
+}
+
+void collide_serial(TreeDev &t, const NodeArrays &a, const double *radii, double strength, Rng *rng,
+                    bool host_draws, uint32_t *resume, cudaStream_t st) {
+  if (a.n == 0) return;
+  k_collide_serial<<<1, 1, 0, st>>>(t.cells, t.skip, t.perm, t.info, a.x, a.y, a.vx, a.vy, radii,
+                                    strength, a.n, rng, host_draws, resume);
+}
+
+// ---------------------------------------------------------------------------
+// center, x, y, radial, integrate (simple.zig)
+// ---------------------------------------------------------------------------
+
+// simple.zig:14-31: the sums in index order, one dependent chain per axis.
+__global__ void k_center_sum(const double *x, const double *y, uint32_t n, double *out) {
+  const double *a = threadIdx.x == 0 ? x : y;
+  if (threadIdx.x != 0 && threadIdx.x != 32) return;
+  double s = 0;
+  uint32_t i = 0;
+  for (; i + 8 <= n; i += 8) {
+    double v0 = a[i], v1 = a[i + 1], v2 = a[i + 2], v3 = a[i + 3];
+    double v4 = a[i + 4], v5 = a[i + 5], v6 = a[i + 6], v7 = a[i + 7];
+    s += v0; s += v1; s += v2; s += v3; s += v4; s += v5; s += v6; s += v7;
+  }
+  for (; i < n; ++i) s += a[i];
+  out[threadIdx.x == 0 ? 0 : 1] = s;
+}
+
+__global__ void k_center_apply(double *x, double *y, uint32_t n, const double *sums, double cx,
+                               double cy, double strength) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double nf = (double)n;
+  const double sx = (sums[0] / nf - cx) * strength;
+  const double sy = (sums[1] / nf - cy) * strength;
+  x[i] -= sx;
+  y[i] -= sy;
+}
+
+void center_force(const NodeArrays &a, double cx, double cy, double strength, ForceScratch &s,
+                  cudaStream_t st) {
+  if (a.n == 0) return;
+  k_center_sum<<<1, 64, 0, st>>>(a.x, a.y, a.n, s.center);
+  k_center_apply<<<blocks_for(a.n, 256), 256, 0, st>>>(a.x, a.y, a.n, s.center, cx, cy, strength);
+}
+
+// simple.zig:51-62
+__global__ void k_axis(double *pos, double *v, const double *strength, const double *target,
+                       double alpha, uint32_t n) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  v[i] += (target[i] - pos[i]) * strength[i] * alpha;
+}
+
+void axis_force(const NodeArrays &a, const double *strength, const double *target, double alpha,
+                int dim, cudaStream_t st) {
+  if (a.n == 0) return;
+  k_axis<<<blocks_for(a.n, 256), 256, 0, st>>>(dim ? a.y : a.x, dim ? a.vy : a.vx, strength, target,
+                                               alpha, a.n);
+}
+
+// simple.zig:64-86
+__global__ void k_radial(const double *x, const double *y, double *vx, double *vy,
+                         const double *strength, const double *radius, double cx, double cy,
+                         double alpha, uint32_t n) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double dx = x[i] - cx;
+  if (dx == 0 || dx != dx) dx = 1e-6;
+  double dy = y[i] - cy;
+  if (dy == 0 || dy != dy) dy = 1e-6;
+  double l = sqrt(dx * dx + dy * dy);
+  double k = (radius[i] - l) * strength[i] * alpha / l;
+  vx[i] += dx * k;
+  vy[i] += dy * k;
+}
+
+void radial_force(const NodeArrays &a, const double *strength, const double *radius, double cx,
+                  double cy, double alpha, cudaStream_t st) {
+  if (a.n == 0) return;
+  k_radial<<<blocks_for(a.n, 256), 256, 0, st>>>(a.x, a.y, a.vx, a.vy, strength, radius, cx, cy,
+                                                 alpha, a.n);
+}
+
+// simple.zig:90-123
+__global__ void k_integrate(double *x, double *y, double *vx, double *vy, const double *fx,
+                            const double *fy, const uint8_t *fixed, double decay, uint32_t n) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint8_t f = fixed[i];
+  if ((f & 1) == 0) {
+    double v = vx[i] * decay;
+    vx[i] = v;
+    x[i] += v;
+  } else {
+    x[i] = fx[i];
+    vx[i] = 0;
+  }
+  if ((f & 2) == 0) {
+    double v = vy[i] * decay;
+    vy[i] = v;
+    y[i] += v;
+  } else {
+    y[i] = fy[i];
+    vy[i] = 0;
+  }
+}
+
+void integrate(const NodeArrays &a, double decay, cudaStream_t st) {
+  if (a.n == 0) return;
+  k_integrate<<<blocks_for(a.n, 256), 256, 0, st>>>(a.x, a.y, a.vx, a.vy, a.fx, a.fy, a.fixed, decay,
+                                                    a.n);
+}
+
+}  // namespace d3

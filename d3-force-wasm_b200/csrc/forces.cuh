@@ -1,0 +1,95 @@
+// forces.cuh — exact-mode force kernels and their launch wrappers.
+#pragma once
+
+#include "common.cuh"
+#include "tree.cuh"
+
+namespace d3 {
+
+struct NodeArrays {
+  double *x, *y, *vx, *vy, *fx, *fy;
+  uint8_t *fixed;
+  double *px, *py;     // shifted positions (collide, fast link)
+  double *snap_vx, *snap_vy;
+  uint32_t n;
+};
+
+// Per-simulation device scratch for the force kernels.
+struct ForceScratch {
+  uint32_t cap = 0;
+  uint32_t *draws = nullptr;    // jiggle draws per node (many-body record pass)
+  uint32_t *offsets = nullptr;  // exclusive scan of draws
+  uint32_t *scan_part = nullptr;
+  uint32_t *counters = nullptr; // 0 total draws, 1 flagged, 2.. misc
+  double *center = nullptr;     // 2 sums
+};
+
+int scratch_reserve(ForceScratch &s, uint32_t n);
+void scratch_free(ForceScratch &s);
+
+struct ManyBodyParams {
+  double theta2, dmin2, dmax2, alpha;
+};
+
+// many_body.zig:31-84 on the device. `rng` is device memory; in host-draw
+// mode the caller must run the rerun itself (returns the draws needed via
+// scratch.counters[0] after a sync).
+void many_body_exact(TreeDev &t, const NodeArrays &a, const double *strengths,
+                     const ManyBodyParams &p, Rng *rng, ForceScratch &s, uint32_t *status,
+                     bool host_draws, cudaStream_t st);
+// The rerun of flagged nodes with their draws (after many_body_exact).
+void many_body_rerun(TreeDev &t, const NodeArrays &a, const double *strengths,
+                     const ManyBodyParams &p, Rng *rng, ForceScratch &s, cudaStream_t st);
+
+// Link levels (computed on the host from source/target): links grouped by
+// level so that links sharing a node keep their order (link.zig:8-40).
+struct LinkPlan {
+  uint32_t m = 0, levels = 0;
+  uint32_t *order = nullptr;        // device: link ids grouped by level
+  uint32_t *level_start = nullptr;  // device: levels + 1 offsets
+  uint32_t *h_level_start = nullptr;
+};
+int link_plan_build(LinkPlan &plan, const uint32_t *src, const uint32_t *tgt, uint32_t m);
+void link_plan_free(LinkPlan &plan);
+
+struct LinkArrays {
+  const double *strength, *distance, *bias;
+  const uint32_t *source, *target;
+  uint32_t m;
+};
+
+// Exact link: level-scheduled Gauss-Seidel. A link that meets a zero / NaN
+// delta (where d3 draws from `random`) sets *flag and the pass is undone
+// (velocities restored from the snapshot); the caller then runs a serial pass.
+void link_exact(const NodeArrays &a, const LinkArrays &l, const LinkPlan &plan, double alpha,
+                double iterations, Rng *rng, uint32_t *flag, cudaStream_t st);
+// The serial pass on the device LCG, only when *flag is set.
+void link_fallback_lcg(const NodeArrays &a, const LinkArrays &l, double alpha, double iterations,
+                       Rng *rng, const uint32_t *flag, uint32_t *status, cudaStream_t st);
+// Serial link from (iteration, link) with host draws; returns via resume[]:
+// resume[0] iteration, resume[1] link, resume[2] draws still needed (0 = done).
+void link_serial_host(const NodeArrays &a, const LinkArrays &l, double alpha, double iterations,
+                      Rng *rng, uint32_t *resume, cudaStream_t st);
+
+struct CollideParams {
+  double strength;
+  double iterations;
+};
+// px = x + vx, py = y + vy (sim.zig:129-146).
+void shift_positions(const NodeArrays &a, cudaStream_t st);
+// One collide iteration's set-up: px = x + vx, tree on (px, py), radii per cell.
+void collide_setup(TreeDev &t, const NodeArrays &a, const double *radii, uint32_t *status,
+                   cudaStream_t st);
+// The ordered node loop of one iteration from node resume[0] (serial).
+void collide_serial(TreeDev &t, const NodeArrays &a, const double *radii, double strength, Rng *rng,
+                    bool host_draws, uint32_t *resume, cudaStream_t st);
+
+void center_force(const NodeArrays &a, double cx, double cy, double strength, ForceScratch &s,
+                  cudaStream_t st);
+void axis_force(const NodeArrays &a, const double *strength, const double *target, double alpha,
+                int dim, cudaStream_t st);
+void radial_force(const NodeArrays &a, const double *strength, const double *radius, double cx,
+                  double cy, double alpha, cudaStream_t st);
+void integrate(const NodeArrays &a, double decay, cudaStream_t st);
+
+}  // namespace d3

@@ -1,0 +1,196 @@
+// scan_sort.cu — device-wide exclusive scan and stable LSD radix sort.
+#include "scan_sort.cuh"
+
+namespace d3 {
+
+// ---- exclusive scan --------------------------------------------------------
+
+// Block-wide exclusive scan of one value per thread (blockDim a multiple of
+// 32, at most 1024); the block total goes to *total.
+__device__ inline uint32_t block_exclusive_scan(uint32_t v, uint32_t *sw, uint32_t *total) {
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= (unsigned)o) x += y;
+  }
+  if (lane == 31) sw[warp] = x;
+  __syncthreads();
+  const unsigned nw = blockDim.x >> 5;
+  if (warp == 0) {
+    uint32_t w = lane < nw ? sw[lane] : 0;
+    uint32_t t = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= (unsigned)o) t += y;
+    }
+    if (lane < nw) sw[lane] = t - w;
+    if (lane == nw - 1) sw[32] = t;
+  }
+  __syncthreads();
+  uint32_t r = sw[warp] + x - v;
+  *total = sw[32];
+  __syncthreads();
+  return r;
+}
+
+// Each block scans 4 * blockDim values (4 consecutive per thread).
+__global__ void k_scan_local(const uint32_t *in, uint32_t *out, uint32_t n, uint32_t *partials) {
+  __shared__ uint32_t sw[33];
+  const size_t base = (size_t)blockIdx.x * blockDim.x * 4 + threadIdx.x * 4;
+  uint32_t v[4];
+  uint32_t s = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    v[k] = base + k < n ? in[base + k] : 0;
+    s += v[k];
+  }
+  uint32_t tot;
+  uint32_t ex = block_exclusive_scan(s, sw, &tot);
+  uint32_t run = ex;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (base + k < n) out[base + k] = run;
+    run += v[k];
+  }
+  if (threadIdx.x == 0) partials[blockIdx.x] = tot;
+}
+
+// Scans the block partials in place (one block; loops if many).
+__global__ void k_scan_partials(uint32_t *partials, uint32_t nb, uint32_t *total) {
+  __shared__ uint32_t sw[33];
+  __shared__ uint32_t carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (uint32_t off = 0; off < nb; off += blockDim.x) {
+    uint32_t i = off + threadIdx.x;
+    uint32_t v = i < nb ? partials[i] : 0;
+    uint32_t tot;
+    uint32_t ex = block_exclusive_scan(v, sw, &tot);
+    if (i < nb) partials[i] = carry + ex;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && total) *total = carry;
+}
+
+__global__ void k_scan_add(uint32_t *out, uint32_t n, const uint32_t *partials) {
+  const size_t base = (size_t)blockIdx.x * blockDim.x * 4 + threadIdx.x * 4;
+  uint32_t p = partials[blockIdx.x];
+  if (p == 0) return;
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    if (base + k < n) out[base + k] += p;
+}
+
+void scan_u32(const uint32_t *in, uint32_t *out, uint32_t n, uint32_t *partials, uint32_t *total,
+              cudaStream_t st) {
+  unsigned nb = blocks_for(n, SCAN_BLOCK * 4);
+  k_scan_local<<<nb, SCAN_BLOCK, 0, st>>>(in, out, n, partials);
+  k_scan_partials<<<1, SCAN_BLOCK, 0, st>>>(partials, nb, total);
+  if (nb > 1) k_scan_add<<<nb, SCAN_BLOCK, 0, st>>>(out, n, partials);
+}
+
+// ---- radix sort -------------------------------------------------------------
+
+template <bool PART>
+__device__ inline uint32_t digit_of(uint64_t k, uint32_t v, int shift) {
+  if (PART) return v >> 31;
+  return (uint32_t)(k >> shift) & 255u;
+}
+
+template <bool PART>
+__global__ void __launch_bounds__(SORT_THREADS) k_sort_hist(const uint64_t *keys, const uint32_t *vals,
+                                                            uint32_t n, int shift, uint32_t *hist,
+                                                            uint32_t tiles) {
+  __shared__ uint32_t h[256];
+  for (int d = threadIdx.x; d < 256; d += blockDim.x) h[d] = 0;
+  __syncthreads();
+  const size_t base = (size_t)blockIdx.x * SORT_TILE;
+  for (unsigned k = threadIdx.x; k < SORT_TILE; k += blockDim.x) {
+    size_t i = base + k;
+    if (i < n) atomicAdd(&h[digit_of<PART>(keys[i], vals[i], shift)], 1u);
+  }
+  __syncthreads();
+  for (int d = threadIdx.x; d < 256; d += blockDim.x) hist[(size_t)d * tiles + blockIdx.x] = h[d];
+}
+
+// Stable scatter of one tile: chunks of 256 keys in order; within a chunk a
+// key's rank among equal digits = earlier warps' counts + lanes below it in
+// its warp with the same digit (warp match).
+template <bool PART>
+__global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(const uint64_t *keys, const uint32_t *vals,
+                                                               uint64_t *okeys, uint32_t *ovals,
+                                                               uint32_t n, int shift,
+                                                               const uint32_t *offsets,
+                                                               uint32_t tiles) {
+  __shared__ uint32_t run[256];
+  __shared__ uint32_t wcnt[SORT_THREADS / 32][256];
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int d = threadIdx.x; d < 256; d += blockDim.x) run[d] = offsets[(size_t)d * tiles + blockIdx.x];
+  const size_t base = (size_t)blockIdx.x * SORT_TILE;
+  for (unsigned c = 0; c < SORT_TILE; c += SORT_THREADS) {
+    for (int d = threadIdx.x; d < 256 * (SORT_THREADS / 32); d += blockDim.x) (&wcnt[0][0])[d] = 0;
+    __syncthreads();
+    size_t i = base + c + threadIdx.x;
+    bool valid = i < n;
+    uint64_t k = valid ? keys[i] : 0;
+    uint32_t v = valid ? vals[i] : 0;
+    uint32_t d = valid ? digit_of<PART>(k, v, shift) : 256u + lane;  // invalid lanes never match
+    unsigned peers = __match_any_sync(0xffffffffu, d);
+    unsigned below = __popc(peers & ((1u << lane) - 1));
+    if (valid && below == 0) wcnt[warp][d] = __popc(peers);
+    __syncthreads();
+    uint32_t pos = 0;
+    if (valid) {
+      uint32_t before = 0;
+      for (unsigned w = 0; w < warp; ++w) before += wcnt[w][d];
+      pos = run[d] + before + below;
+      okeys[pos] = k;
+      ovals[pos] = v;
+    }
+    __syncthreads();
+    // advance the running offsets by this chunk's counts
+    for (int dd = threadIdx.x; dd < 256; dd += blockDim.x) {
+      uint32_t t = 0;
+      for (unsigned w = 0; w < SORT_THREADS / 32; ++w) t += wcnt[w][dd];
+      run[dd] += t;
+    }
+    __syncthreads();
+  }
+}
+
+template <bool PART>
+static void sort_pass(const uint64_t *ik, const uint32_t *iv, uint64_t *ok, uint32_t *ov, uint32_t n,
+                      int shift, const SortScratch &s, cudaStream_t st) {
+  uint32_t tiles = (n + SORT_TILE - 1) / SORT_TILE;
+  k_sort_hist<PART><<<tiles, SORT_THREADS, 0, st>>>(ik, iv, n, shift, s.hist, tiles);
+  scan_u32(s.hist, s.hist, 256 * tiles, s.partials, nullptr, st);
+  k_sort_scatter<PART><<<tiles, SORT_THREADS, 0, st>>>(ik, iv, ok, ov, n, shift, s.hist, tiles);
+}
+
+void radix_sort_u64(uint64_t *keys, uint32_t *vals, uint32_t n, int byte_lo, int byte_hi,
+                    bool partition_hi_bit, const SortScratch &s, cudaStream_t st) {
+  if (n == 0) return;
+  uint64_t *ak = keys, *bk = s.keys_tmp;
+  uint32_t *av = vals, *bv = s.vals_tmp;
+  for (int b = byte_lo; b < byte_hi; ++b) {
+    sort_pass<false>(ak, av, bk, bv, n, 8 * b, s, st);
+    uint64_t *tk = ak; ak = bk; bk = tk;
+    uint32_t *tv = av; av = bv; bv = tv;
+  }
+  if (partition_hi_bit) {
+    sort_pass<true>(ak, av, bk, bv, n, 0, s, st);
+    uint64_t *tk = ak; ak = bk; bk = tk;
+    uint32_t *tv = av; av = bv; bv = tv;
+  }
+  if (ak != keys) {
+    cudaMemcpyAsync(keys, ak, (size_t)n * 8, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(vals, av, (size_t)n * 4, cudaMemcpyDeviceToDevice, st);
+  }
+}
+
+}  // namespace d3

@@ -57,6 +57,7 @@ class Context:
         if not self.h:
             raise C.CoreError(C.OUT_OF_MEMORY)
         self.n = 0
+        C.check(core.sim_set_sync(self.h, C.SYNC_EXPLICIT))
         self.live = False
         self.precision = None  # None = exact; {"order", "opening"} = fast
         self.host_random = None  # callback for randomSource(); None = device LCG

@@ -30,6 +30,7 @@ struct DForce {
   bool dirty = false;       // host mirrors may hold writes not yet uploaded
   bool plan_dirty = true;   // link plan / adjacency must be rebuilt
   uint32_t max_index = 0;   // largest source / target + 1 (link)
+  double max_f0 = 0;        // largest f0 (collide: the largest radius)
   LinkPlan plan;
   FastLink csr;             // fast link adjacency (link_fast.zig)
 };
@@ -47,6 +48,7 @@ struct DSim {
   TreeDev tree;
   ForceScratch scratch;
   FastScratch fast;
+  CollideSpec spec;
   std::vector<DForce *> forces;
   // random
   Rng *d_rng = nullptr;
@@ -174,6 +176,12 @@ int upload_force(DSim *s, DForce *f) {
   for (int i = 0; i < k; ++i)
     if (f->count)
       cudaMemcpyAsync(f->d_f[i], f->h_f[i], f->count * 8ull, cudaMemcpyHostToDevice, s->stream);
+  if (f->kind == D3_COLLIDE) {
+    double mx = 0;
+    for (uint32_t i = 0; i < f->count; ++i)
+      if (f->h_f[0][i] > mx) mx = f->h_f[0][i];
+    f->max_f0 = mx;
+  }
   if (f->kind == D3_LINK && f->count) {
     cudaMemcpyAsync(f->d_src, f->h_src, f->count * 4ull, cudaMemcpyHostToDevice, s->stream);
     cudaMemcpyAsync(f->d_tgt, f->h_tgt, f->count * 4ull, cudaMemcpyHostToDevice, s->stream);
@@ -320,7 +328,9 @@ int run_collide(DSim *s, DForce *f) {
     collide_setup(s->tree, a, f->d_f[0], status_word(s), s->stream);
     cudaMemsetAsync(res, 0, 3 * sizeof(uint32_t), s->stream);
     if (!s->host_random) {
-      collide_serial(s->tree, a, f->d_f[0], strength, s->d_rng, false, res, s->stream);
+      const double delta = f->max_f0 > 0 ? f->max_f0 : 1.0;
+      if (collide_parallel(s->tree, a, f->d_f[0], strength, delta, s->d_rng, s->spec, s->stream))
+        collide_serial(s->tree, a, f->d_f[0], strength, s->d_rng, false, res, s->stream);
       continue;
     }
     if (pull_draws(s, 0)) return D3_OUT_OF_MEMORY;
@@ -416,7 +426,8 @@ int ensure_cap(DSim *s, uint32_t n) {
       grow_device(s->d_py, 0, cap, st) || grow_device(s->d_svx, 0, cap, st) ||
       grow_device(s->d_svy, 0, cap, st))
     return -1;
-  if (tree_reserve(s->tree, cap) || scratch_reserve(s->scratch, cap) || fast_reserve(s->fast, cap))
+  if (tree_reserve(s->tree, cap) || scratch_reserve(s->scratch, cap) || fast_reserve(s->fast, cap) ||
+      collide_spec_reserve(s->spec, cap))
     return -1;
   s->cap = cap;
   return 0;
@@ -473,6 +484,7 @@ int32_t sim_destroy(uint32_t h) {
   tree_free(s->tree);
   scratch_free(s->scratch);
   fast_free(s->fast);
+  collide_spec_free(s->spec);
   cudaFree(s->d_rng);
   cudaFreeHost(s->h_rng);
   cudaFree(s->d_words);
@@ -808,6 +820,37 @@ int32_t sim_tick(uint32_t h, uint32_t ticks, double *alpha, double alpha_target,
   cudaEventElapsedTime(&ms, s->ev0, s->ev1);
   s->last_ms = ms;
   return D3_OK;
+}
+
+double sim_stat(uint32_t h, uint32_t which) {
+  DSim *s = get_sim(h);
+  if (!s) return 0;
+  uint32_t spec[8] = {0}, sc[2] = {0}, words[2] = {0};
+  cudaMemcpyAsync(s->h_words + 8, s->spec.counters, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                  s->stream);
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess) return -1;
+  memcpy(spec, s->h_words + 8, sizeof spec);
+  cudaMemcpyAsync(s->h_words + 8, s->scratch.counters, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                  s->stream);
+  cudaMemcpyAsync(s->h_words + 10, s->d_words, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                  s->stream);
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess) return -1;
+  memcpy(sc, s->h_words + 8, sizeof sc);
+  memcpy(words, s->h_words + 10, sizeof words);
+  switch (which) {
+    case 0: return spec[5];
+    case 1: return spec[6];
+    case 2: return spec[7];
+    case 3: return sc[1];
+    case 4: {
+      uint32_t lv = 0;
+      for (DForce *f : s->forces)
+        if (f && f->kind == D3_LINK) lv = f->plan.levels;
+      return lv;
+    }
+    case 5: return words[1] != 0;
+    default: return 0;
+  }
 }
 
 double sim_last_tick_ms(uint32_t h) {

@@ -84,6 +84,26 @@ void collide_setup(TreeDev &t, const NodeArrays &a, const double *radii, uint32_
 void collide_serial(TreeDev &t, const NodeArrays &a, const double *radii, double strength, Rng *rng,
                     bool host_draws, uint32_t *resume, cudaStream_t st);
 
+// Scratch of the parallel exact collide (collide_spec.cu).
+struct CollideSpec {
+  uint32_t cap = 0;
+  uint32_t *rlist = nullptr;
+  uint8_t *rcount = nullptr;
+  uint64_t *wmask = nullptr;
+  uint8_t *state = nullptr;
+  uint32_t *active = nullptr;
+  uint64_t *min_acc = nullptr, *min_wr = nullptr;
+  double *push = nullptr;
+  uint32_t *min_pusher = nullptr;
+  uint32_t *counters = nullptr;  // active, done, fail, jiggle, overflow, rounds, attempts, serial
+};
+int collide_spec_reserve(CollideSpec &s, uint32_t n);
+void collide_spec_free(CollideSpec &s);
+// One iteration's node loop, in parallel and bit-identical to the serial
+// order (after collide_setup). `delta`: the guess margin. LCG random only.
+int collide_parallel(TreeDev &t, const NodeArrays &a, const double *radii, double strength,
+                     double delta, Rng *rng, CollideSpec &s, cudaStream_t st);
+
 void center_force(const NodeArrays &a, double cx, double cy, double strength, ForceScratch &s,
                   cudaStream_t st);
 void axis_force(const NodeArrays &a, const double *strength, const double *target, double alpha,

@@ -137,6 +137,13 @@ int32_t sim_tick(uint32_t h, uint32_t ticks, double *alpha, double alpha_target,
 /* Milliseconds of device time of the last sim_tick call (CUDA events). */
 double sim_last_tick_ms(uint32_t h);
 
+/* Diagnostics of the last force runs (synchronises): 0 rounds of the last
+ * parallel exact collide, 1 its attempts, 2 1 if it fell back to the serial
+ * loop, 3 nodes the last exact many-body traversal flagged for jiggle, 4 link
+ * levels of the last exact link plan, 5 1 if the last exact link pass fell
+ * back to the serial order (a jiggle). */
+double sim_stat(uint32_t h, uint32_t which);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1889,6 +1889,12 @@ double sim_last_tick_ms(uint32_t h) {
   return 0;
 }
 
+double sim_stat(uint32_t h, uint32_t which) {
+  (void)h;
+  (void)which;
+  return 0;
+}
+
 /* Oracle-only: worker threads for the exact many-body record pass (the CPU
  * baseline's stand-in for the reference's thread pool). */
 int32_t oracle_set_threads(uint32_t h, uint32_t k) {

@@ -37,7 +37,10 @@ def run_pair(setup, ocore, gcore, ticks, step=1, check_every=1):
                 d = first_difference(na, nb)
                 assert d is None, "tick %d: %s" % (t, d)
                 assert sa.alpha() == sb.alpha()
-        assert ocore.sim_get_lcg(sa.ctx.h) == gcore.sim_get_lcg(sb.ctx.h), "random stream position"
+        if sa.randomSource() is None:
+            assert ocore.sim_get_lcg(sa.ctx.h) == gcore.sim_get_lcg(sb.ctx.h), "random stream position"
+        else:  # each side drew from its own copy of the caller's function
+            assert sa.randomSource()() == sb.randomSource()(), "random stream position"
     finally:
         sa.close()
         sb.close()

@@ -54,6 +54,24 @@ def test_gpu_exact_collide_coincident_small(ocore, gcore):
                ocore, gcore, 60)
 
 
+def test_gpu_exact_collide_runs_in_parallel(ocore, gcore):
+    """The parallel collide path itself (not its serial fallback) matches."""
+    setup = _defaults(4000, 8000, collide=5)
+    na, sa = setup(ocore)
+    nb, sb = setup(gcore)
+    try:
+        serial_ticks = 0
+        for t in range(30):
+            sa.tick()
+            sb.tick()
+            serial_ticks += int(gcore.sim_stat(sb.ctx.h, 2))
+            assert P.first_difference(na, nb) is None, "tick %d" % (t + 1)
+        assert serial_ticks < 30
+    finally:
+        sa.close()
+        sb.close()
+
+
 def test_gpu_exact_d3_collide_known_answers(ocore, gcore):
     """test/d3/collide-test.js scenarios, every tick bitwise with the oracle."""
     def three(core):

@@ -1,0 +1,281 @@
+#!/usr/bin/env python
+"""Benchmark of the exact d3-force tick on the B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (a "step" = one tick): exact mode, n = 50,000 nodes at d3's
+phyllotaxis start, m = 100,000 links drawn from d3's LCG (no self-loops),
+forceManyBody(-30, theta 0.9) + forceLink(distance 30, default strength) +
+forceCollide(radius 5) + forceCenter(0, 0); 1% of nodes moved onto exact copies
+of other nodes' positions, 1% to offsets below 1e-12 from other nodes, 0.5%
+pinned (fx, fy). Every tick is bit-identical to the CPU oracle (tests/).
+
+`value` is device milliseconds per tick (CUDA events on the engine's stream),
+with L2 flushed between ticks (the working set fits in L2). `e2e` is the same
+metric through the public API (`Simulation.tick`), with the host-to-device copy
+of the node state and the device-to-host read of the result in every step.
+`--impl reference` times the reference algorithm's CPU restatement (the
+oracle: the reference compiles only with zig, which this machine lacks) on all
+host cores. Under torchrun (N > 1) each rank runs an independent replica
+(the exact tick does not shard: ordered link / collide sums and one random
+stream); rank 0 prints the line.
+"""
+
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(n=50000, m=100000, collide_radius=5, coincident=0.01, near=0.01, pinned=0.005)
+WORKLOAD_NAME = ("exact n=50000 m=100000 manyBody(-30,theta .9)+link(30)+collide(5)+center; "
+                 "1% coincident, 1% offsets<1e-12, 0.5% pinned")
+METRIC = "ms/tick: exact 50k bit-exact"
+PHASES = ["mb_tree", "mb_accumulate", "mb_traverse", "link", "collide_tree", "collide_loop",
+          "center", "integrate"]
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    return ap.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)),
+            int(os.environ.get("WORLD_SIZE", 1)))
+
+
+def oracle_ms_per_tick(pkg, sc, threads, warmup, rounds, ticks):
+    """The reference algorithm (oracle) on the host: `warmup` ticks, then the
+    best of `rounds` rounds of `ticks` ticks (bench/threads.js:85-96)."""
+    import oracle
+
+    core = oracle.load(pkg)
+    nodes, sim = sc.setup_exact(pkg, core, **WORKLOAD)
+    core.lib.oracle_set_threads(sim.ctx.h, threads)
+    sim.tick(warmup)
+    best = float("inf")
+    for _ in range(rounds):
+        t0 = time.perf_counter()
+        sim.tick(ticks)
+        best = min(best, (time.perf_counter() - t0) * 1e3 / ticks)
+    sim.close()
+    return best
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.proc = None
+        self.device = device
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(device), "--query-gpu=" + self.QUERY,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, mx, reasons = [], None, set()
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                                "sw_power_cap"), f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def run_ours(args, pkg, sc):
+    rank, local_rank, world = dist_env()
+    if world > 1:
+        os.environ["CUDA_VISIBLE_DEVICES"] = str(local_rank)
+    import torch
+    import torch.distributed as dist
+
+    if world > 1:
+        dist.init_process_group("gloo", timeout=__import__("datetime").timedelta(seconds=300))
+    core = pkg.cuda_core()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+
+    def flush_l2():
+        flush.zero_()
+        torch.cuda.synchronize()
+
+    nodes, sim = sc.setup_exact(pkg, core, **WORKLOAD)
+    h = sim.ctx.h
+    sim.device_begin()
+    for _ in range(args.warmup):
+        flush_l2()
+        sim.device_ticks(1)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(0 if world > 1 else int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0))
+    launches0 = core.sim_stat(h, 6)
+    core.sim_set_profile(h, 1)
+    times = []
+    for _ in range(args.steps):
+        flush_l2()
+        times.append(sim.device_ticks(1))
+    phases = {name: core.sim_stat(h, 100 + k) for k, name in enumerate(PHASES)}
+    core.sim_set_profile(h, 0)
+    launches = int(core.sim_stat(h, 6) - launches0)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = sum(times) / len(times)
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+        ms = float(t.item())
+    sim.device_end()
+    # e2e through the public API: node state in, tick, node state out
+    e2e = []
+    for _ in range(args.e2e_steps):
+        flush_l2()
+        t0 = time.perf_counter()
+        sim.tick(1)
+        e2e.append((time.perf_counter() - t0) * 1e3)
+    n = WORKLOAD["n"]
+    e2e_ms = sum(e2e) / len(e2e)
+    if world > 1:
+        t = torch.tensor([e2e_ms], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    stats = {"collide_rounds": core.sim_stat(h, 0), "collide_attempts": core.sim_stat(h, 1),
+             "collide_serial_fallback": core.sim_stat(h, 2), "link_levels": core.sim_stat(h, 4)}
+    sim.close()
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+    # Roofline of the dominant phase: the exact many-body traversal is the
+    # f64 work; bytes are the HBM traffic of its inputs and outputs per tick.
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    dom = max(phases, key=phases.get)
+    per_tick_ms = {k: v / args.steps for k, v in phases.items()}
+    # algorithmic bytes per launch of the dominant phase (per tick)
+    alg_bytes = {
+        "mb_traverse": n * (4 + 8 * 2 + 8 * 2 * 2 + 8) + 1.75 * n * 112,
+        "collide_loop": n * (8 * 2 + 8 * 2 * 2 + 8) + 1.75 * n * 112,
+        "link": WORKLOAD["m"] * (2 * 4 + 3 * 8) + 4 * WORKLOAD["m"] * 8 * 2,
+    }.get(dom, n * 64.0)
+    achieved = alg_bytes / (per_tick_ms[dom] * 1e-3) / 1e9
+    line = {
+        "metric": METRIC, "value": round(ms, 4), "unit": "ms/tick", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generators of the reference's scenarios)",
+        "config": {"workload": WORKLOAD_NAME, "n": n, "m": WORKLOAD["m"],
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "flushed between timed ticks (256 MB write)", "bit_exact": True},
+        "e2e": {"value": round(e2e_ms, 4), "unit": "ms/tick", "h2d_bytes_per_step": 49 * n,
+                "d2h_bytes_per_step": 32 * n},
+        "gpu_launches": launches,
+        "phase_ms_per_tick": {k: round(v, 4) for k, v in per_tick_ms.items()},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 2),
+                     "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 5),
+                     "traffic": None, "peak_source": "measured" if peaks else "fallback"},
+        "engine_stats": stats,
+        "clocks": clk,
+    }
+    if not args.no_cpu_baseline and world == 1:
+        threads = os.cpu_count() or 1
+        cpu = oracle_ms_per_tick(pkg, sc, threads, warmup=3, rounds=2, ticks=8)
+        line["cpu_baseline"] = {"value": round(cpu, 3), "unit": "ms/tick", "cores": threads,
+                                "kind": "port",
+                                "sample": "3 warm-up ticks then best of 2 rounds x 8 ticks of the "
+                                          "same workload (C restatement of the reference core)"}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_reference(args, pkg, sc):
+    rank, _, world = dist_env()
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    import oracle
+
+    core = oracle.load(pkg)
+    nodes, sim = sc.setup_exact(pkg, core, **WORKLOAD)
+    core.lib.oracle_set_threads(sim.ctx.h, threads)
+    sim.tick(args.warmup)
+    steps = max(1, min(args.steps, 60))
+    t0 = time.perf_counter()
+    sim.tick(steps)
+    ms = (time.perf_counter() - t0) * 1e3 / steps
+    sim.close()
+    line = {
+        "metric": METRIC, "value": round(ms, 3), "unit": "ms/tick", "n_gpus": world,
+        "steps": steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generators of the reference's scenarios)",
+        "config": {"workload": WORKLOAD_NAME, "n": WORKLOAD["n"], "m": WORKLOAD["m"]},
+        "impl": "reference",
+        "cpu_baseline": {"value": round(ms, 3), "unit": "ms/tick", "cores": threads,
+                         "kind": "port",
+                         "sample": "%d warm-up then %d ticks of the workload (C restatement of "
+                                   "the reference core; zig is unavailable)" % (args.warmup, steps)},
+        "e2e": {"value": round(ms, 3), "unit": "ms/tick", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    pkg = importlib.import_module("d3-force-wasm_b200")
+    sc = importlib.import_module("d3-force-wasm_b200.scenarios")
+    if args.impl == "reference":
+        run_reference(args, pkg, sc)
+    else:
+        run_ours(args, pkg, sc)
+
+
+if __name__ == "__main__":
+    main()

@@ -428,6 +428,7 @@ int collide_parallel(TreeDev &t, const NodeArrays &a, const double *radii, doubl
   args.active = s.active; args.min_acc = s.min_acc; args.min_wr = s.min_wr; args.push = s.push;
   args.min_pusher = s.min_pusher; args.counters = s.counters; args.rng = rng;
   void *params[] = {&args};
+  ++g_launches;
   cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_collide_spec, g_spec_blocks,
                                               SPEC_THREADS, params, 0, st);
   return e == cudaSuccess ? 0 : -1;

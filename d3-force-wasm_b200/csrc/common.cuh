@@ -101,6 +101,13 @@ __device__ inline double rng_draw_at(const Rng &r, uint64_t k) {
     }                                                                               \
   } while (0)
 
+// Kernels this library has launched (every launch site goes through
+// D3_LAUNCH); the benchmark reports how many ran in its timed region.
+extern unsigned long long g_launches;
+#define D3_LAUNCH(kernel, ...) \
+  for (int d3_launch_once_ = (++::d3::g_launches, 0); d3_launch_once_ < 1; ++d3_launch_once_) \
+  kernel<<<__VA_ARGS__>>>
+
 inline unsigned blocks_for(size_t n, unsigned threads) {
   size_t b = (n + threads - 1) / threads;
   return b ? (unsigned)b : 1u;

@@ -18,6 +18,10 @@
 
 using namespace d3;
 
+namespace d3 {
+unsigned long long g_launches = 0;
+}
+
 namespace {
 
 struct DForce {
@@ -72,7 +76,58 @@ struct DSim {
   uint32_t h_len = 0, h_root = NONE, h_m = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_ms = 0;
+  // phase timers (sim_set_profile): pending event pairs per phase, totals
+  bool profile = false;
+  std::vector<cudaEvent_t> ev_pool;
+  struct Pending { int phase; cudaEvent_t a, b; };
+  std::vector<Pending> pending;
+  double phase_ms[16] = {0};
+  uint64_t phase_n[16] = {0};
 };
+
+enum Phase { PH_MB_TREE = 0, PH_MB_ACC, PH_MB_TRAVERSE, PH_LINK, PH_COLLIDE_SETUP, PH_COLLIDE_RUN,
+             PH_CENTER, PH_INTEGRATE, PH_FAST_MB, PH_FAST_LINK, PH_FAST_COLLIDE, PH_OTHER };
+
+cudaEvent_t pool_event(DSim *s) {
+  if (!s->ev_pool.empty()) {
+    cudaEvent_t e = s->ev_pool.back();
+    s->ev_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Records the start of a phase on the simulation's stream (no-op unless
+// profiling); returns the event to close it with phase_end.
+cudaEvent_t phase_begin(DSim *s) {
+  if (!s->profile) return nullptr;
+  cudaEvent_t e = pool_event(s);
+  cudaEventRecord(e, s->stream);
+  return e;
+}
+
+void phase_end(DSim *s, int phase, cudaEvent_t a) {
+  if (!a) return;
+  cudaEvent_t b = pool_event(s);
+  cudaEventRecord(b, s->stream);
+  s->pending.push_back({phase, a, b});
+}
+
+void phase_collect(DSim *s) {
+  if (s->pending.empty()) return;
+  cudaStreamSynchronize(s->stream);
+  for (auto &p : s->pending) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, p.a, p.b);
+    s->phase_ms[p.phase] += ms;
+    s->phase_n[p.phase] += 1;
+    s->ev_pool.push_back(p.a);
+    s->ev_pool.push_back(p.b);
+  }
+  s->pending.clear();
+}
 
 std::vector<DSim *> g_sims;
 int g_device_ok = -1;
@@ -274,8 +329,13 @@ int run_many_body(DSim *s, DForce *f, double alpha) {
                    f->scalars[D3_DISTANCE_MAX2], alpha};
   NodeArrays a = nodes_of(s);
   if (!s->host_random) {
+    cudaEvent_t e = phase_begin(s);
     many_body_exact(s->tree, a, f->d_f[0], p, s->d_rng, s->scratch, status_word(s), false,
-                    s->stream);
+                    s->stream, [&](int ph) {
+                      phase_end(s, ph, e);
+                      e = phase_begin(s);
+                    });
+    phase_end(s, PH_MB_TRAVERSE, e);
     return D3_OK;
   }
   many_body_exact(s->tree, a, f->d_f[0], p, s->d_rng, s->scratch, status_word(s), true, s->stream);
@@ -299,11 +359,14 @@ int run_link(DSim *s, DForce *f, double alpha) {
   NodeArrays a = nodes_of(s);
   LinkArrays l{f->d_f[0], f->d_f[1], f->d_f[2], f->d_src, f->d_tgt, f->count};
   const double iterations = f->scalars[D3_ITERATIONS];
+  cudaEvent_t e = phase_begin(s);
   link_exact(a, l, f->plan, alpha, iterations, s->d_rng, link_flag(s), s->stream);
   if (!s->host_random) {
     link_fallback_lcg(a, l, alpha, iterations, s->d_rng, link_flag(s), status_word(s), s->stream);
+    phase_end(s, PH_LINK, e);
     return D3_OK;
   }
+  phase_end(s, PH_LINK, e);
   if (read_words(s)) return D3_WORKER_FAILED;
   if (s->h_words[1] == 0) return D3_OK;
   // Serial pass with exactly the draws it asks for, pulled in d3's order.
@@ -325,12 +388,16 @@ int run_collide(DSim *s, DForce *f) {
   const double strength = f->scalars[D3_STRENGTH], iterations = f->scalars[D3_ITERATIONS];
   uint32_t *res = resume_words(s);
   for (double k = 0; k < iterations; k += 1) {
+    cudaEvent_t e = phase_begin(s);
     collide_setup(s->tree, a, f->d_f[0], status_word(s), s->stream);
     cudaMemsetAsync(res, 0, 3 * sizeof(uint32_t), s->stream);
+    phase_end(s, PH_COLLIDE_SETUP, e);
     if (!s->host_random) {
       const double delta = f->max_f0 > 0 ? f->max_f0 : 1.0;
+      e = phase_begin(s);
       if (collide_parallel(s->tree, a, f->d_f[0], strength, delta, s->d_rng, s->spec, s->stream))
         collide_serial(s->tree, a, f->d_f[0], strength, s->d_rng, false, res, s->stream);
+      phase_end(s, PH_COLLIDE_RUN, e);
       continue;
     }
     if (pull_draws(s, 0)) return D3_OUT_OF_MEMORY;
@@ -361,10 +428,13 @@ int run_force(DSim *s, DForce *f, double alpha) {
     else set_seed(seed_slot, f->scalars[D3_SEED], s->stream);
   }
   switch (f->kind) {
-    case D3_CENTER:
+    case D3_CENTER: {
+      cudaEvent_t e = phase_begin(s);
       center_force(a, f->scalars[D3_CX], f->scalars[D3_CY], f->scalars[D3_STRENGTH], s->scratch,
                    s->stream);
+      phase_end(s, PH_CENTER, e);
       return D3_OK;
+    }
     case D3_X: axis_force(a, f->d_f[0], f->d_f[1], alpha, 0, s->stream); return D3_OK;
     case D3_Y: axis_force(a, f->d_f[0], f->d_f[1], alpha, 1, s->stream); return D3_OK;
     case D3_RADIAL:
@@ -378,7 +448,9 @@ int run_force(DSim *s, DForce *f, double alpha) {
           f->plan_dirty = true;  // the exact plan is rebuilt on its next use
         }
         LinkArrays l{f->d_f[0], f->d_f[1], f->d_f[2], f->d_src, f->d_tgt, f->count};
+        cudaEvent_t e = phase_begin(s);
         fast_link(a, l, f->csr, alpha, f->scalars[D3_ITERATIONS], seed_slot, s->stream);
+        phase_end(s, PH_FAST_LINK, e);
         return D3_OK;
       }
       return run_link(s, f, alpha);
@@ -390,7 +462,9 @@ int run_force(DSim *s, DForce *f, double alpha) {
         fp.dmin2 = f->scalars[D3_DISTANCE_MIN2];
         fp.dmax2 = f->scalars[D3_DISTANCE_MAX2];
         fp.alpha = alpha;
+        cudaEvent_t e = phase_begin(s);
         int r = fmm_run(s->fast, s->tree, a, f->d_f[0], fp, seed_slot, status_word(s), s->stream);
+        phase_end(s, PH_FAST_MB, e);
         if (r == 1) return D3_OK;
         if (r == -3) return D3_BAD_ARGUMENT;
         if (r < 0) return D3_OUT_OF_MEMORY;
@@ -398,8 +472,10 @@ int run_force(DSim *s, DForce *f, double alpha) {
       return run_many_body(s, f, alpha);
     case D3_COLLIDE:
       if (fast_mode(s, f)) {
+        cudaEvent_t e = phase_begin(s);
         fast_collide(s->fast, a, f->d_f[0], f->scalars[D3_STRENGTH], f->scalars[D3_ITERATIONS],
                      seed_slot, s->stream);
+        phase_end(s, PH_FAST_COLLIDE, e);
         return D3_OK;
       }
       return run_collide(s, f);
@@ -811,7 +887,9 @@ int32_t sim_tick(uint32_t h, uint32_t ticks, double *alpha, double alpha_target,
       int r = run_force(s, f, a);
       if (r < 0) return r;
     }
+    cudaEvent_t e = phase_begin(s);
     integrate(nodes_of(s), velocity_decay, s->stream);
+    phase_end(s, PH_INTEGRATE, e);
   }
   cudaEventRecord(s->ev1, s->stream);
   *alpha = a;
@@ -822,9 +900,29 @@ int32_t sim_tick(uint32_t h, uint32_t ticks, double *alpha, double alpha_target,
   return D3_OK;
 }
 
+int32_t sim_set_profile(uint32_t h, uint32_t on) {
+  DSim *s = get_sim(h);
+  if (!s) return D3_BAD_HANDLE;
+  phase_collect(s);
+  s->profile = on != 0;
+  for (int k = 0; k < 16; ++k) {
+    s->phase_ms[k] = 0;
+    s->phase_n[k] = 0;
+  }
+  return D3_OK;
+}
+
 double sim_stat(uint32_t h, uint32_t which) {
   DSim *s = get_sim(h);
   if (!s) return 0;
+  if (which >= 100 && which < 116) {
+    phase_collect(s);
+    return s->phase_ms[which - 100];
+  }
+  if (which >= 200 && which < 216) {
+    phase_collect(s);
+    return (double)s->phase_n[which - 200];
+  }
   uint32_t spec[8] = {0}, sc[2] = {0}, words[2] = {0};
   cudaMemcpyAsync(s->h_words + 8, s->spec.counters, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost,
                   s->stream);
@@ -849,6 +947,7 @@ double sim_stat(uint32_t h, uint32_t which) {
       return lv;
     }
     case 5: return words[1] != 0;
+    case 6: return (double)g_launches;
     default: return 0;
   }
 }

@@ -58,9 +58,9 @@ __global__ void k_draw_seed(Rng *rng, double *seed) {
 
 __global__ void k_set_seed(double *seed, double v) { *seed = v; }
 
-void draw_seed(Rng *rng, double *seed, cudaStream_t st) { k_draw_seed<<<1, 1, 0, st>>>(rng, seed); }
+void draw_seed(Rng *rng, double *seed, cudaStream_t st) { D3_LAUNCH(k_draw_seed, 1, 1, 0, st)(rng, seed); }
 void set_seed(double *seed, double value, cudaStream_t st) {
-  k_set_seed<<<1, 1, 0, st>>>(seed, value);
+  D3_LAUNCH(k_set_seed, 1, 1, 0, st)(seed, value);
 }
 
 __device__ inline uint64_t seed_bits(const double *seed) {
@@ -148,8 +148,8 @@ void fast_link(const NodeArrays &a, const LinkArrays &l, const FastLink &c, doub
                double iterations, const double *seed, cudaStream_t st) {
   const uint32_t n = a.n;
   for (double k = 0; k < iterations; k += 1) {
-    k_shift2<<<blocks_for(n, 256), 256, 0, st>>>(a.x, a.y, a.vx, a.vy, a.px, a.py, n);
-    k_link_sweep<<<blocks_for(n, 128), 128, 0, st>>>(a.px, a.py, a.vx, a.vy, l, c.row, c.adj, alpha,
+    D3_LAUNCH(k_shift2, blocks_for(n, 256), 256, 0, st)(a.x, a.y, a.vx, a.vy, a.px, a.py, n);
+    D3_LAUNCH(k_link_sweep, blocks_for(n, 128), 128, 0, st)(a.px, a.py, a.vx, a.vy, l, c.row, c.adj, alpha,
                                                      seed, n);
   }
 }
@@ -334,13 +334,13 @@ void fast_collide(FastScratch &s, const NodeArrays &a, const double *radii, doub
   if (gb > GRID_BLOCKS_MAX) gb = GRID_BLOCKS_MAX;
   SortScratch ss{s.g_keys_tmp, s.g_items_tmp, s.g_hist, s.g_part};
   for (double k = 0; k < iterations; k += 1) {
-    k_grid_bounds<<<gb, GRID_THREADS, 0, st>>>(a.x, a.y, a.vx, a.vy, a.px, a.py, radii, n, s.g_box,
+    D3_LAUNCH(k_grid_bounds, gb, GRID_THREADS, 0, st)(a.x, a.y, a.vx, a.vy, a.px, a.py, radii, n, s.g_box,
                                                 s.g_info, s.g_geom);
-    k_grid_bin<<<blocks_for(n, 256), 256, 0, st>>>(a.px, a.py, n, s.g_info, s.g_geom, s.g_keys,
+    D3_LAUNCH(k_grid_bin, blocks_for(n, 256), 256, 0, st)(a.px, a.py, n, s.g_info, s.g_geom, s.g_keys,
                                                    s.g_items, s.g_cell_of);
     radix_sort_u64(s.g_keys, s.g_items, n, 0, 4, false, ss, st);
-    k_grid_starts<<<blocks_for(4ull * n + 17, 256), 256, 0, st>>>(s.g_keys, n, s.g_info, s.g_start);
-    k_grid_sweep<<<blocks_for(n, 128), 128, 0, st>>>(a.px, a.py, a.vx, a.vy, radii, strength, seed, n,
+    D3_LAUNCH(k_grid_starts, blocks_for(4ull * n + 17, 256), 256, 0, st)(s.g_keys, n, s.g_info, s.g_start);
+    D3_LAUNCH(k_grid_sweep, blocks_for(n, 128), 128, 0, st)(a.px, a.py, a.vx, a.vy, radii, strength, seed, n,
                                                      s.g_info, s.g_start, s.g_items, s.g_cell_of);
   }
 }

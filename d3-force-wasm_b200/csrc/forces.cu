@@ -262,16 +262,18 @@ static void climb_grid(unsigned &blocks, unsigned &threads, uint32_t cap) {
 
 void many_body_exact(TreeDev &t, const NodeArrays &a, const double *strengths,
                      const ManyBodyParams &p, Rng *rng, ForceScratch &s, uint32_t *status,
-                     bool host_draws, cudaStream_t st) {
+                     bool host_draws, cudaStream_t st, const std::function<void(int)> &mark) {
   const uint32_t n = a.n;
   tree_build(t, a.x, a.y, n, status, st);
+  if (mark) mark(0);
   if (n == 0) return;
   unsigned cb, ct;
   climb_grid(cb, ct, t.cells_cap);
-  k_mb_accumulate<<<cb, ct, 0, st>>>(t.cells, t.parent, t.counter, t.perm, a.x, a.y, strengths,
+  D3_LAUNCH(k_mb_accumulate, cb, ct, 0, st)(t.cells, t.parent, t.counter, t.perm, a.x, a.y, strengths,
                                      t.info);
+  if (mark) mark(1);
   cudaMemsetAsync(s.counters, 0, 2 * sizeof(uint32_t), st);
-  k_mb_traverse<<<blocks_for(n, 128), 128, 0, st>>>(t.cells, t.skip, t.perm, t.info, a.x, a.y,
+  D3_LAUNCH(k_mb_traverse, blocks_for(n, 128), 128, 0, st)(t.cells, t.skip, t.perm, t.info, a.x, a.y,
                                                     a.vx, a.vy, strengths, p, n, s.draws,
                                                     s.counters);
   scan_u32(s.draws, s.offsets, n, s.scan_part, s.counters, st);
@@ -281,10 +283,10 @@ void many_body_exact(TreeDev &t, const NodeArrays &a, const double *strengths,
 void many_body_rerun(TreeDev &t, const NodeArrays &a, const double *strengths,
                      const ManyBodyParams &p, Rng *rng, ForceScratch &s, cudaStream_t st) {
   const uint32_t n = a.n;
-  k_mb_rerun<<<blocks_for(n, 128), 128, 0, st>>>(t.cells, t.skip, t.perm, t.info, a.x, a.y, a.vx,
+  D3_LAUNCH(k_mb_rerun, blocks_for(n, 128), 128, 0, st)(t.cells, t.skip, t.perm, t.info, a.x, a.y, a.vx,
                                                  a.vy, strengths, p, n, s.draws, s.offsets,
                                                  s.counters, rng);
-  k_rng_advance<<<1, 1, 0, st>>>(rng, s.counters);
+  D3_LAUNCH(k_rng_advance, 1, 1, 0, st)(rng, s.counters);
 }
 
 // ---------------------------------------------------------------------------
@@ -454,27 +456,27 @@ void link_exact(const NodeArrays &a, const LinkArrays &l, const LinkPlan &plan, 
   if (l.m == 0) return;
   const uint32_t n = a.n;
   cudaMemsetAsync(flag, 0, sizeof(uint32_t), st);
-  k_save_v<<<blocks_for(n, 256), 256, 0, st>>>(a.snap_vx, a.snap_vy, a.vx, a.vy, n);
+  D3_LAUNCH(k_save_v, blocks_for(n, 256), 256, 0, st)(a.snap_vx, a.snap_vy, a.vx, a.vy, n);
   for (double k = 0; k < iterations; k += 1) {
     for (uint32_t lv = 1; lv <= plan.levels; ++lv) {
       uint32_t lo = plan.h_level_start[lv], hi = plan.h_level_start[lv + 1];
       if (hi > lo)
-        k_link_level<<<blocks_for(hi - lo, 128), 128, 0, st>>>(a.x, a.y, a.vx, a.vy, l, plan.order,
+        D3_LAUNCH(k_link_level, blocks_for(hi - lo, 128), 128, 0, st)(a.x, a.y, a.vx, a.vy, l, plan.order,
                                                                 lo, hi, alpha, flag);
     }
   }
-  k_restore_v<<<blocks_for(n, 256), 256, 0, st>>>(a.vx, a.vy, a.snap_vx, a.snap_vy, n, flag);
+  D3_LAUNCH(k_restore_v, blocks_for(n, 256), 256, 0, st)(a.vx, a.vy, a.snap_vx, a.snap_vy, n, flag);
 }
 
 void link_serial_host(const NodeArrays &a, const LinkArrays &l, double alpha, double iterations,
                       Rng *rng, uint32_t *resume, cudaStream_t st) {
-  k_link_serial_host<<<1, 1, 0, st>>>(a.x, a.y, a.vx, a.vy, l, alpha, iterations, rng, resume);
+  D3_LAUNCH(k_link_serial_host, 1, 1, 0, st)(a.x, a.y, a.vx, a.vy, l, alpha, iterations, rng, resume);
 }
 
 // Serial link on the device LCG, after a DAG pass that met a jiggle.
 void link_fallback_lcg(const NodeArrays &a, const LinkArrays &l, double alpha, double iterations,
                        Rng *rng, const uint32_t *flag, uint32_t *status, cudaStream_t st) {
-  k_link_serial<<<1, 1, 0, st>>>(a.x, a.y, a.vx, a.vy, l, alpha, iterations, rng, flag, status);
+  D3_LAUNCH(k_link_serial, 1, 1, 0, st)(a.x, a.y, a.vx, a.vy, l, alpha, iterations, rng, flag, status);
 }
 
 // ---------------------------------------------------------------------------
@@ -582,24 +584,24 @@ __global__ void k_collide_serial(const Cell *cells, const uint32_t *skip, const 
 
 void shift_positions(const NodeArrays &a, cudaStream_t st) {
   if (a.n == 0) return;
-  k_shift<<<blocks_for(a.n, 256), 256, 0, st>>>(a.x, a.y, a.vx, a.vy, a.px, a.py, a.n);
+  D3_LAUNCH(k_shift, blocks_for(a.n, 256), 256, 0, st)(a.x, a.y, a.vx, a.vy, a.px, a.py, a.n);
 }
 
 void collide_setup(TreeDev &t, const NodeArrays &a, const double *radii, uint32_t *status,
                    cudaStream_t st) {
   const uint32_t n = a.n;
-  k_shift<<<blocks_for(n, 256), 256, 0, st>>>(a.x, a.y, a.vx, a.vy, a.px, a.py, n);
+  D3_LAUNCH(k_shift, blocks_for(n, 256), 256, 0, st)(a.x, a.y, a.vx, a.vy, a.px, a.py, n);
   tree_build(t, a.px, a.py, n, status, st);
   if (n == 0) return;
   unsigned cb, ct;
   climb_grid(cb, ct, t.cells_cap);
-  k_collide_prep<<<cb, ct, 0, st>>>(t.cells, t.parent, t.counter, t.perm, radii, t.info);
+  D3_LAUNCH(k_collide_prep, cb, ct, 0, st)(t.cells, t.parent, t.counter, t.perm, radii, t.info);
 }
 
 void collide_serial(TreeDev &t, const NodeArrays &a, const double *radii, double strength, Rng *rng,
                     bool host_draws, uint32_t *resume, cudaStream_t st) {
   if (a.n == 0) return;
-  k_collide_serial<<<1, 1, 0, st>>>(t.cells, t.skip, t.perm, t.info, a.x, a.y, a.vx, a.vy, radii,
+  D3_LAUNCH(k_collide_serial, 1, 1, 0, st)(t.cells, t.skip, t.perm, t.info, a.x, a.y, a.vx, a.vy, radii,
                                     strength, a.n, rng, host_draws, resume);
 }
 
@@ -636,8 +638,8 @@ __global__ void k_center_apply(double *x, double *y, uint32_t n, const double *s
 void center_force(const NodeArrays &a, double cx, double cy, double strength, ForceScratch &s,
                   cudaStream_t st) {
   if (a.n == 0) return;
-  k_center_sum<<<1, 64, 0, st>>>(a.x, a.y, a.n, s.center);
-  k_center_apply<<<blocks_for(a.n, 256), 256, 0, st>>>(a.x, a.y, a.n, s.center, cx, cy, strength);
+  D3_LAUNCH(k_center_sum, 1, 64, 0, st)(a.x, a.y, a.n, s.center);
+  D3_LAUNCH(k_center_apply, blocks_for(a.n, 256), 256, 0, st)(a.x, a.y, a.n, s.center, cx, cy, strength);
 }
 
 // simple.zig:51-62
@@ -651,7 +653,7 @@ __global__ void k_axis(double *pos, double *v, const double *strength, const dou
 void axis_force(const NodeArrays &a, const double *strength, const double *target, double alpha,
                 int dim, cudaStream_t st) {
   if (a.n == 0) return;
-  k_axis<<<blocks_for(a.n, 256), 256, 0, st>>>(dim ? a.y : a.x, dim ? a.vy : a.vx, strength, target,
+  D3_LAUNCH(k_axis, blocks_for(a.n, 256), 256, 0, st)(dim ? a.y : a.x, dim ? a.vy : a.vx, strength, target,
                                                alpha, a.n);
 }
 
@@ -674,7 +676,7 @@ __global__ void k_radial(const double *x, const double *y, double *vx, double *v
 void radial_force(const NodeArrays &a, const double *strength, const double *radius, double cx,
                   double cy, double alpha, cudaStream_t st) {
   if (a.n == 0) return;
-  k_radial<<<blocks_for(a.n, 256), 256, 0, st>>>(a.x, a.y, a.vx, a.vy, strength, radius, cx, cy,
+  D3_LAUNCH(k_radial, blocks_for(a.n, 256), 256, 0, st)(a.x, a.y, a.vx, a.vy, strength, radius, cx, cy,
                                                  alpha, a.n);
 }
 
@@ -704,7 +706,7 @@ __global__ void k_integrate(double *x, double *y, double *vx, double *vy, const 
 
 void integrate(const NodeArrays &a, double decay, cudaStream_t st) {
   if (a.n == 0) return;
-  k_integrate<<<blocks_for(a.n, 256), 256, 0, st>>>(a.x, a.y, a.vx, a.vy, a.fx, a.fy, a.fixed, decay,
+  D3_LAUNCH(k_integrate, blocks_for(a.n, 256), 256, 0, st)(a.x, a.y, a.vx, a.vy, a.fx, a.fy, a.fixed, decay,
                                                     a.n);
 }
 

@@ -1,6 +1,8 @@
 // forces.cuh — exact-mode force kernels and their launch wrappers.
 #pragma once
 
+#include <functional>
+
 #include "common.cuh"
 #include "tree.cuh"
 
@@ -34,9 +36,12 @@ struct ManyBodyParams {
 // many_body.zig:31-84 on the device. `rng` is device memory; in host-draw
 // mode the caller must run the rerun itself (returns the draws needed via
 // scratch.counters[0] after a sync).
+// `mark(phase)` is called after the tree build (0) and the accumulation (1),
+// so the caller can time the phases.
 void many_body_exact(TreeDev &t, const NodeArrays &a, const double *strengths,
                      const ManyBodyParams &p, Rng *rng, ForceScratch &s, uint32_t *status,
-                     bool host_draws, cudaStream_t st);
+                     bool host_draws, cudaStream_t st,
+                     const std::function<void(int)> &mark = std::function<void(int)>());
 // The rerun of flagged nodes with their draws (after many_body_exact).
 void many_body_rerun(TreeDev &t, const NodeArrays &a, const double *strengths,
                      const ManyBodyParams &p, Rng *rng, ForceScratch &s, cudaStream_t st);

@@ -89,9 +89,9 @@ __global__ void k_scan_add(uint32_t *out, uint32_t n, const uint32_t *partials) 
 void scan_u32(const uint32_t *in, uint32_t *out, uint32_t n, uint32_t *partials, uint32_t *total,
               cudaStream_t st) {
   unsigned nb = blocks_for(n, SCAN_BLOCK * 4);
-  k_scan_local<<<nb, SCAN_BLOCK, 0, st>>>(in, out, n, partials);
-  k_scan_partials<<<1, SCAN_BLOCK, 0, st>>>(partials, nb, total);
-  if (nb > 1) k_scan_add<<<nb, SCAN_BLOCK, 0, st>>>(out, n, partials);
+  D3_LAUNCH(k_scan_local, nb, SCAN_BLOCK, 0, st)(in, out, n, partials);
+  D3_LAUNCH(k_scan_partials, 1, SCAN_BLOCK, 0, st)(partials, nb, total);
+  if (nb > 1) D3_LAUNCH(k_scan_add, nb, SCAN_BLOCK, 0, st)(out, n, partials);
 }
 
 // ---- radix sort -------------------------------------------------------------
@@ -167,9 +167,9 @@ template <bool PART>
 static void sort_pass(const uint64_t *ik, const uint32_t *iv, uint64_t *ok, uint32_t *ov, uint32_t n,
                       int shift, const SortScratch &s, cudaStream_t st) {
   uint32_t tiles = (n + SORT_TILE - 1) / SORT_TILE;
-  k_sort_hist<PART><<<tiles, SORT_THREADS, 0, st>>>(ik, iv, n, shift, s.hist, tiles);
+  D3_LAUNCH(k_sort_hist<PART>, tiles, SORT_THREADS, 0, st)(ik, iv, n, shift, s.hist, tiles);
   scan_u32(s.hist, s.hist, 256 * tiles, s.partials, nullptr, st);
-  k_sort_scatter<PART><<<tiles, SORT_THREADS, 0, st>>>(ik, iv, ok, ov, n, shift, s.hist, tiles);
+  D3_LAUNCH(k_sort_scatter<PART>, tiles, SORT_THREADS, 0, st)(ik, iv, ok, ov, n, shift, s.hist, tiles);
 }
 
 void radix_sort_u64(uint64_t *keys, uint32_t *vals, uint32_t n, int byte_lo, int byte_hi,

@@ -489,18 +489,18 @@ void tree_build(TreeDev &t, const double *xs, const double *ys, uint32_t n, uint
                 cudaStream_t st) {
   unsigned bb = blocks_for(n, BOX_THREADS * 4);
   if (bb > BOX_BLOCKS_MAX) bb = BOX_BLOCKS_MAX;
-  k_box<<<bb, BOX_THREADS, 0, st>>>(xs, ys, n, (BoxPart *)t.box_part, t.extent, t.info);
+  D3_LAUNCH(k_box, bb, BOX_THREADS, 0, st)(xs, ys, n, (BoxPart *)t.box_part, t.extent, t.info);
   if (n == 0) return;
   const unsigned T = 256, B = blocks_for(n, T);
-  k_keys<<<B, T, 0, st>>>(xs, ys, n, t.extent, t.keys, t.sv);
+  D3_LAUNCH(k_keys, B, T, 0, st)(xs, ys, n, t.extent, t.keys, t.sv);
   SortScratch ss{t.keys_tmp, t.sv_tmp, t.hist, t.scan_part};
   radix_sort_u64(t.keys, t.sv, n, 0, 8, true, ss, st);
-  k_runs<<<B, T, 0, st>>>(xs, ys, n, t.keys, t.sv, t.perm, t.lcpx, t.info);
-  k_count<<<B, T, 0, st>>>(xs, ys, t.keys, t.lcpx, t.extent, t.perm, t.perm_tmp, t.frames, t.cnt,
+  D3_LAUNCH(k_runs, B, T, 0, st)(xs, ys, n, t.keys, t.sv, t.perm, t.lcpx, t.info);
+  D3_LAUNCH(k_count, B, T, 0, st)(xs, ys, t.keys, t.lcpx, t.extent, t.perm, t.perm_tmp, t.frames, t.cnt,
                            t.run_end, t.leafd, t.info, n);
   // cells before each start; the total lands in info[1]
   scan_u32(t.cnt, t.base, n, t.scan_part, t.info + 1, st);
-  k_emit<<<B, T, 0, st>>>(xs, ys, t.keys, t.lcpx, t.extent, t.perm, t.perm_tmp, t.frames, t.base,
+  D3_LAUNCH(k_emit, B, T, 0, st)(xs, ys, t.keys, t.lcpx, t.extent, t.perm, t.perm_tmp, t.frames, t.base,
                           t.run_end, t.leafd, t.cells, t.skip, t.parent, t.counter, t.cells_cap,
                           t.info, status);
 }

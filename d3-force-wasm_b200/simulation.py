@@ -491,25 +491,40 @@ class Simulation:
         randomSource() callback it falls back to tick(ticks)."""
         if self._random is not None:
             return self.tick(ticks)
+        self.device_begin()
+        self.device_ticks(ticks)
+        self.device_end()
+        return self
+
+    def device_begin(self):
+        """Node state to the device and every force's scalars pushed, so that
+        device_ticks() can run ticks with no host transfer."""
         ctx = self.ctx
         ctx.copy_in(self._nodes)
-        forces = list(self._forces.values())
-        for f in forces:
+        for f in self._forces.values():
             f._push()
             s = f.slot
             s.scalar(C.PRECISION, 1 if ctx.precision else 0)
             if ctx.precision:
                 s.scalar(C.ORDER, ctx.precision["order"])
                 s.scalar(C.OPENING, ctx.precision["opening"])
-        # collide and center get alpha 0 from the facade and ignore it in the
-        # core, so one alpha per tick for every force is equivalent.
-        order = (C._U32 * max(1, len(forces)))(*[f.slot.fh for f in forces])
+        forces = list(self._forces.values())
+        self._order = (C._U32 * max(1, len(forces)))(*[f.slot.fh for f in forces])
+        self._n_order = len(forces)
+
+    def device_ticks(self, ticks):
+        """`ticks` ticks on the device (sim_tick); returns their device ms.
+        collide and center get alpha 0 from the facade and ignore it in the
+        core, so one alpha per tick for every force is equivalent."""
         alpha = C._F64(self._alpha)
-        C.check(self.core.sim_tick(ctx.h, int(ticks), alpha, self._alpha_target,
-                                   self._alpha_decay, self._velocity_decay, order, len(forces)))
+        C.check(self.core.sim_tick(self.ctx.h, int(ticks), alpha, self._alpha_target,
+                                   self._alpha_decay, self._velocity_decay, self._order,
+                                   self._n_order))
         self._alpha = alpha.value
-        ctx.copy_out(self._nodes)
-        return self
+        return self.core.sim_last_tick_ms(self.ctx.h)
+
+    def device_end(self):
+        self.ctx.copy_out(self._nodes)
 
     def nodes(self, nodes=None):
         if nodes is None:

@@ -141,8 +141,16 @@ double sim_last_tick_ms(uint32_t h);
  * parallel exact collide, 1 its attempts, 2 1 if it fell back to the serial
  * loop, 3 nodes the last exact many-body traversal flagged for jiggle, 4 link
  * levels of the last exact link plan, 5 1 if the last exact link pass fell
- * back to the serial order (a jiggle). */
+ * back to the serial order (a jiggle), 6 kernels this library launched so
+ * far (all simulations); 100 + k milliseconds and 200 + k count of phase k
+ * since sim_set_profile(h, 1): 0 many-body tree, 1 many-body accumulation,
+ * 2 many-body traversal, 3 exact link, 4 collide tree and radii, 5 collide
+ * node loop, 6 center, 7 integrate, 8 fast many-body, 9 fast link, 10 fast
+ * collide. */
 double sim_stat(uint32_t h, uint32_t which);
+/* Phase timers on (1) / off (0); both reset them. CUDA events on the
+ * simulation's stream around each phase. */
+int32_t sim_set_profile(uint32_t h, uint32_t on);
 
 #ifdef __cplusplus
 }

@@ -1895,6 +1895,11 @@ double sim_stat(uint32_t h, uint32_t which) {
   return 0;
 }
 
+int32_t sim_set_profile(uint32_t h, uint32_t on) {
+  (void)on;
+  return get_sim(h) ? D3_OK : D3_BAD_HANDLE;
+}
+
 /* Oracle-only: worker threads for the exact many-body record pass (the CPU
  * baseline's stand-in for the reference's thread pool). */
 int32_t oracle_set_threads(uint32_t h, uint32_t k) {

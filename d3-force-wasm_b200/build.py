@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 OUT = os.path.join(OUT_DIR, "libd3force_b200.so")
-SOURCES = ["engine.cu", "tree.cu", "scan_sort.cu", "forces.cu", "fast.cu", "fmm.cu", "collide_spec.cu"]
+SOURCES = ["engine.cu", "tree.cu", "scan_sort.cu", "forces.cu", "fast.cu", "fmm.cu", "collide_spec.cu", "noalloc.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
          "-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false",

@@ -152,6 +152,30 @@ double sim_stat(uint32_t h, uint32_t which);
  * simulation's stream around each phase. */
 int32_t sim_set_profile(uint32_t h, uint32_t on);
 
+/* ---- Allocation-free entry point (no counterpart in the reference) ------
+ *
+ * For callers that cannot let a library allocate device memory (an engine
+ * that owns and budgets all GPU memory, a frame or control loop where
+ * cudaMalloc would add synchronisation and latency): the exact many-body
+ * force of force_run (d3's Barnes-Hut, bit-identical) on caller-owned device
+ * buffers x, y, vx, vy, strength (f64[n]), with all scratch taken from one
+ * static device array sized for D3_NOALLOC_MAX_NODES nodes, held by every GPU
+ * that loads the library until the process exits. No cudaMalloc / cudaFree is
+ * called. `*lcg_state` (host) is d3's LCG state for jiggle draws, updated on
+ * return. Runs on `stream` (a cudaStream_t; NULL = the default stream) and
+ * returns when the work is done. The first call on each device looks up the
+ * array's device address (set-up), so make it before any stream capture.
+ * Calls share the array: calls that overlap on the GPU (other threads or
+ * streams) race. Returns D3_OK; D3_BAD_ARGUMENT when n exceeds
+ * D3_NOALLOC_MAX_NODES or a pointer is missing; D3_ARENA_FULL when the tree
+ * needs more cells than the array holds (points closer than 2^-32 of the
+ * extent in long chains); D3_WORKER_FAILED on a CUDA error. */
+#define D3_NOALLOC_MAX_NODES 8192u
+int32_t d3_many_body_exact_noalloc(const double *x, const double *y, double *vx, double *vy,
+                                   const double *strength, uint32_t n, double theta2,
+                                   double distance_min2, double distance_max2, double alpha,
+                                   uint32_t *lcg_state, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -66,6 +66,11 @@ struct DSim {
   uint32_t *d_words = nullptr;
   uint32_t *h_words = nullptr;
   cudaStream_t stream = nullptr;
+  // Side stream for work that may run ahead of its place in the tick (the
+  // sums of a center force: they read positions, which nothing before the
+  // first center force of a tick changes).
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_xready = nullptr, ev_sumdone = nullptr;
   uint32_t sync_mode = D3_SYNC_PER_CALL;
   // tree mirrors (tree_info)
   Cell *h_cells = nullptr;
@@ -393,7 +398,12 @@ int run_collide(DSim *s, DForce *f) {
     cudaMemsetAsync(res, 0, 3 * sizeof(uint32_t), s->stream);
     phase_end(s, PH_COLLIDE_SETUP, e);
     if (!s->host_random) {
-      const double delta = f->max_f0 > 0 ? f->max_f0 : 1.0;
+      static const double factor = [] {
+        const char *e = getenv("D3_COLLIDE_DELTA");
+        double v = e ? atof(e) : 0;
+        return v > 0 ? v : 1.0;
+      }();
+      const double delta = (f->max_f0 > 0 ? f->max_f0 : 1.0) * factor;
       e = phase_begin(s);
       if (collide_parallel(s->tree, a, f->d_f[0], strength, delta, s->d_rng, s->spec, s->stream))
         collide_serial(s->tree, a, f->d_f[0], strength, s->d_rng, false, res, s->stream);
@@ -416,7 +426,7 @@ bool fast_mode(const DSim *s, const DForce *f) {
   return f->scalars[D3_PRECISION] == 1 && s->n >= FAST_MIN_N;
 }
 
-int run_force(DSim *s, DForce *f, double alpha) {
+int run_force(DSim *s, DForce *f, double alpha, bool presummed = false) {
   NodeArrays a = nodes_of(s);
   // The facade's per-run SEED draw in fast mode (src/core.js:218-222), from
   // the device LCG when it is the random source.
@@ -430,7 +440,9 @@ int run_force(DSim *s, DForce *f, double alpha) {
   switch (f->kind) {
     case D3_CENTER: {
       cudaEvent_t e = phase_begin(s);
-      center_force(a, f->scalars[D3_CX], f->scalars[D3_CY], f->scalars[D3_STRENGTH], s->scratch,
+      if (presummed) cudaStreamWaitEvent(s->stream, s->ev_sumdone, 0);
+      else center_sum(a, s->scratch, status_word(s), s->stream);
+      center_apply(a, f->scalars[D3_CX], f->scalars[D3_CY], f->scalars[D3_STRENGTH], s->scratch,
                    s->stream);
       phase_end(s, PH_CENTER, e);
       return D3_OK;
@@ -516,10 +528,13 @@ extern "C" {
 uint32_t sim_create(void) {
   if (!device_ok()) return 0;
   DSim *s = new DSim();
-  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking) != cudaSuccess) {
     delete s;
     return 0;
   }
+  cudaEventCreateWithFlags(&s->ev_xready, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&s->ev_sumdone, cudaEventDisableTiming);
   cudaMalloc(&s->d_rng, sizeof(Rng));
   cudaMallocHost(&s->h_rng, sizeof(Rng));
   cudaMalloc(&s->d_words, 16 * sizeof(uint32_t));
@@ -571,6 +586,10 @@ int32_t sim_destroy(uint32_t h) {
   free(s->h_perm);
   cudaEventDestroy(s->ev0);
   cudaEventDestroy(s->ev1);
+  cudaEventDestroy(s->ev_xready);
+  cudaEventDestroy(s->ev_sumdone);
+  cudaStreamSynchronize(s->side);
+  cudaStreamDestroy(s->side);
   cudaStreamDestroy(s->stream);
   delete s;
   g_sims[h - 1] = nullptr;
@@ -879,12 +898,26 @@ int32_t sim_tick(uint32_t h, uint32_t ticks, double *alpha, double alpha_target,
     upload_force(s, f);
     fs.push_back(f);
   }
+  // The first center force's sums only read positions, which no force
+  // before it changes: run them on the side stream from the tick's start.
+  int hoist = -1;
+  for (size_t i = 0; i < fs.size(); ++i)
+    if (fs[i]->kind == D3_CENTER) {
+      hoist = (int)i;
+      break;
+    }
   cudaEventRecord(s->ev0, s->stream);
   double a = *alpha;
   for (uint32_t k = 0; k < ticks; ++k) {
     a += (alpha_target - a) * alpha_decay;
-    for (DForce *f : fs) {
-      int r = run_force(s, f, a);
+    if (hoist >= 0 && s->n) {
+      cudaEventRecord(s->ev_xready, s->stream);
+      cudaStreamWaitEvent(s->side, s->ev_xready, 0);
+      center_sum(nodes_of(s), s->scratch, status_word(s), s->side);
+      cudaEventRecord(s->ev_sumdone, s->side);
+    }
+    for (size_t i = 0; i < fs.size(); ++i) {
+      int r = run_force(s, fs[i], a, (int)i == hoist && s->n);
       if (r < 0) return r;
     }
     cudaEvent_t e = phase_begin(s);
@@ -923,11 +956,11 @@ double sim_stat(uint32_t h, uint32_t which) {
     phase_collect(s);
     return (double)s->phase_n[which - 200];
   }
-  uint32_t spec[8] = {0}, sc[2] = {0}, words[2] = {0};
-  cudaMemcpyAsync(s->h_words + 8, s->spec.counters, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+  uint32_t spec[16] = {0}, sc[2] = {0}, words[2] = {0};
+  cudaMemcpyAsync(s->h_words, s->spec.counters, 16 * sizeof(uint32_t), cudaMemcpyDeviceToHost,
                   s->stream);
   if (cudaStreamSynchronize(s->stream) != cudaSuccess) return -1;
-  memcpy(spec, s->h_words + 8, sizeof spec);
+  memcpy(spec, s->h_words, sizeof spec);
   cudaMemcpyAsync(s->h_words + 8, s->scratch.counters, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost,
                   s->stream);
   cudaMemcpyAsync(s->h_words + 10, s->d_words, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost,
@@ -948,6 +981,20 @@ double sim_stat(uint32_t h, uint32_t which) {
     }
     case 5: return words[1] != 0;
     case 6: return (double)g_launches;
+    case 7: return spec[8];   // collide turns that examined an unguessed head
+    case 8: return spec[9];   // ... that overlapped an unguessed head
+    case 9: return spec[10];  // inactive nodes whose turn would have written
+    case 10: return spec[11]; // turns run from the recorded head list
+    case 11: return spec[12]; // turns that traversed the tree
+    case 12: case 13: case 14: case 15: case 16: case 17: case 18: {
+      // microseconds of the last parallel collide's phases: 12 guess, 13/14
+      // attempt 1 rounds / check, 15/16 attempt 2, 17/18 attempt 3
+      unsigned long long st[16];
+      cudaMemcpy(st, s->spec.stamps, sizeof st, cudaMemcpyDeviceToHost);
+      int k = which - 12;
+      if (!st[k] || !st[k + 1]) return 0;
+      return (double)(st[k + 1] - st[k]) / 1e3;
+    }
     default: return 0;
   }
 }

@@ -3,6 +3,7 @@
 // All arithmetic keeps d3's statement order (no FMA contraction: the file is
 // built with -fmad=false). Traversals are stackless: cells are in d3's visit
 // preorder, so "descend" is c + 1 and "do not descend" is skip[c].
+#include <climits>
 #include <vector>
 
 #include "forces.cuh"
@@ -609,19 +610,258 @@ void collide_serial(TreeDev &t, const NodeArrays &a, const double *radii, double
 // center, x, y, radial, integrate (simple.zig)
 // ---------------------------------------------------------------------------
 
-// simple.zig:14-31: the sums in index order, one dependent chain per axis.
-__global__ void k_center_sum(const double *x, const double *y, uint32_t n, double *out) {
-  const double *a = threadIdx.x == 0 ? x : y;
-  if (threadIdx.x != 0 && threadIdx.x != 32) return;
-  double s = 0;
-  uint32_t i = 0;
-  for (; i + 8 <= n; i += 8) {
-    double v0 = a[i], v1 = a[i + 1], v2 = a[i + 2], v3 = a[i + 3];
-    double v4 = a[i + 4], v5 = a[i + 5], v6 = a[i + 6], v7 = a[i + 7];
-    s += v0; s += v1; s += v2; s += v3; s += v4; s += v5; s += v6; s += v7;
+// simple.zig:14-31: sx += x[i] for i = 0..n-1 (and sy), reproduced exactly
+// in parallel. While the running sum s stays inside one binade [2^e, 2^e+1)
+// (or its negative) and never meets a rounding tie, fl(s + v) = s + R(v) u
+// with u = 2^(e-52) the ulp there and R(v) = v / u rounded to the nearest
+// integer: the chain is an integer prefix sum. One block (a) sums chunks of
+// the input approximately and scans them to guess each chunk's binade, (b)
+// computes per chunk R's total and the min / max of its prefix in that
+// binade, and (c) one thread per axis walks the chunks with the exact s:
+// where s is in the guessed binade and every partial sum provably stays in
+// it, s jumps by total * u (exact); anywhere else it adds the chunk's values
+// one by one, as the reference does.
+constexpr unsigned CSUM_THREADS = 1024;
+// Serial stretches stream the axis through shared memory with bulk async
+// copies (cp.async.bulk, completion on an mbarrier): CSUM_STAGES stages of
+// CSUM_STAGE values per axis in flight, so the dependent add chain reads
+// shared memory instead of waiting on global loads.
+constexpr unsigned CSUM_STAGE = 2048;
+constexpr unsigned CSUM_STAGES = 4;
+constexpr size_t CSUM_DYN_SMEM = 2ull * CSUM_STAGES * CSUM_STAGE * sizeof(double);
+constexpr unsigned long long CSUM_WAIT_NS = 20000000ull;  // 20 ms per copy, far above need
+
+__device__ inline uint32_t smem_addr(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ inline unsigned long long gtimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Stage k (values [k * CSUM_STAGE, ...)) lives in ring slot k % CSUM_STAGES.
+// Each slot records the stage it holds, whether its copy is still pending and
+// how many copies it has completed (the mbarrier phase to wait on). A slot is
+// refilled only after its pending copy has landed; stages the walk skips are
+// never copied. The copy size is rounded down to 16 bytes (the bulk copy
+// granularity); an odd last value is read from global memory.
+struct StageRing {
+  double *buf;     // CSUM_STAGES * CSUM_STAGE values
+  uint64_t *bar;   // CSUM_STAGES mbarriers
+  const double *src;
+  uint32_t n;
+  uint32_t stage[CSUM_STAGES], phase[CSUM_STAGES];
+  bool pending[CSUM_STAGES];
+  bool timeout;
+
+  __device__ uint32_t copied(uint32_t k) const {
+    const uint32_t lo = k * CSUM_STAGE;
+    return lo < n ? ((min(CSUM_STAGE, n - lo) * 8u) & ~15u) / 8u : 0;
   }
-  for (; i < n; ++i) s += a[i];
-  out[threadIdx.x == 0 ? 0 : 1] = s;
+
+  // Waits for slot q's pending copy: a non-blocking test polled against a
+  // time budget, so a wait that cannot end reports instead of spinning.
+  __device__ void settle(uint32_t q) {
+    if (!pending[q]) return;
+    const uint32_t a = smem_addr(&bar[q]), parity = phase[q] & 1u;
+    const unsigned long long t0 = gtimer_ns();
+    for (;;) {
+      uint32_t done;
+      asm volatile(
+          "{ .reg .pred p; mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2; "
+          "selp.u32 %0, 1, 0, p; }"
+          : "=r"(done)
+          : "r"(a), "r"(parity)
+          : "memory");
+      if (done) break;
+      if (gtimer_ns() - t0 > CSUM_WAIT_NS) {
+        timeout = true;
+        break;
+      }
+      __nanosleep(64);
+    }
+    pending[q] = false;
+    ++phase[q];
+  }
+
+  __device__ void issue(uint32_t k) {
+    const uint32_t q = k % CSUM_STAGES;
+    if (stage[q] == k) return;  // already there (or in flight)
+    settle(q);
+    stage[q] = k;
+    const uint32_t cnt = copied(k);
+    if (!cnt) return;
+    const uint32_t bytes = cnt * 8u;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&bar[q])),
+                 "r"(bytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_addr(buf + (size_t)q * CSUM_STAGE)),
+        "l"(src + (size_t)k * CSUM_STAGE), "r"(bytes), "r"(smem_addr(&bar[q]))
+        : "memory");
+    pending[q] = true;
+  }
+
+  __device__ void init(double *b, uint64_t *bars, const double *sp, uint32_t count) {
+    buf = b;
+    bar = bars;
+    src = sp;
+    n = count;
+    timeout = false;
+    for (uint32_t q = 0; q < CSUM_STAGES; ++q) {
+      stage[q] = 0xffffffffu;
+      phase[q] = 0;
+      pending[q] = false;
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar[q])) : "memory");
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    for (uint32_t k = 0; k < CSUM_STAGES; ++k) issue(k);
+  }
+
+  // Value i: its stage is made resident (and the next stages prefetched).
+  __device__ double at(uint32_t i) {
+    const uint32_t k = i / CSUM_STAGE, off = i % CSUM_STAGE;
+    if (off >= copied(k)) return src[i];  // the odd last value
+    const uint32_t q = k % CSUM_STAGES;
+    if (stage[q] != k || pending[q]) {
+      issue(k);
+      settle(q);
+      for (uint32_t j = 1; j < CSUM_STAGES; ++j) issue(k + j);
+    }
+    return buf[(size_t)q * CSUM_STAGE + off];
+  }
+
+  // Every copy still in flight lands before the block may exit.
+  __device__ void drain() {
+    for (uint32_t q = 0; q < CSUM_STAGES; ++q) settle(q);
+  }
+};
+
+constexpr unsigned CSUM_MAX_CHUNKS = 512;
+
+struct CsumChunk {
+  long long total, pmin, pmax;
+  int e;       // binade exponent guess; INT_MIN = add serially
+  int neg;
+};
+
+__device__ inline int binade_of(double s) {
+  int e;
+  frexp(s, &e);  // s = f 2^e, f in [0.5, 1): binade [2^(e-1), 2^e)
+  return e - 1;
+}
+
+__global__ void __launch_bounds__(CSUM_THREADS) k_center_sum(const double *x, const double *y,
+                                                             uint32_t n, double *out,
+                                                             uint32_t *status) {
+  extern __shared__ __align__(128) double ring_buf[];
+  __shared__ __align__(8) uint64_t ring_bar[2][CSUM_STAGES];
+  __shared__ CsumChunk ch[2][CSUM_MAX_CHUNKS];
+  __shared__ double approx[2][CSUM_MAX_CHUNKS];
+  __shared__ double warp_tot[2][32];
+  const uint32_t L = n <= 64 * CSUM_MAX_CHUNKS ? 64 : (n + CSUM_MAX_CHUNKS - 1) / CSUM_MAX_CHUNKS;
+  const uint32_t nc = (n + L - 1) / L;
+  const unsigned t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  // (a) approximate chunk sums, then an exclusive scan of them per axis
+  for (int ax = 0; ax < 2; ++ax) {
+    const double *v = ax ? y : x;
+    double a = 0;
+    if (t < nc)
+      for (uint32_t k = t * L, e = min(n, (t + 1) * L); k < e; ++k) a += v[k];
+    double incl = a;
+    for (int o = 1; o < 32; o <<= 1) {
+      double yv = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= (unsigned)o) incl += yv;
+    }
+    if (lane == 31) warp_tot[ax][warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      double w = warp_tot[ax][lane], wi = w;
+      for (int o = 1; o < 32; o <<= 1) {
+        double yv = __shfl_up_sync(0xffffffffu, wi, o);
+        if (lane >= (unsigned)o) wi += yv;
+      }
+      warp_tot[ax][lane] = wi - w;
+    }
+    __syncthreads();
+    if (t < nc) approx[ax][t] = warp_tot[ax][warp] + incl - a;  // approximate s at chunk start
+    __syncthreads();
+  }
+  // (b) integer summaries in the guessed binade
+  for (int ax = 0; ax < 2; ++ax) {
+    if (t >= nc) continue;
+    const double *v = ax ? y : x;
+    CsumChunk c;
+    c.e = INT_MIN;
+    c.neg = 0;
+    c.total = c.pmin = c.pmax = 0;
+    const double s0 = approx[ax][t];
+    if (s0 != 0 && isfinite(s0)) {
+      const int e = binade_of(s0);
+      const double scale = ldexp(1.0, 52 - e);  // 1 / u
+      long long p = 0, mn = 0, mx = 0;
+      bool ok = e > -1000 && e < 1000;
+      double run = s0;  // approximate running sum, for the binade guess
+      for (uint32_t k = t * L, end = min(n, (t + 1) * L); k < end && ok; ++k) {
+        const double vv = v[k];
+        const double q = vv * scale;  // exact: a power-of-two scaling in range
+        if (!(fabs(q) < 4.0e18)) { ok = false; break; }
+        const double r = rint(q);
+        if (fabs(q - trunc(q)) == 0.5) { ok = false; break; }  // a tie: parity of s decides
+        p += (long long)r;
+        mn = p < mn ? p : mn;
+        mx = p > mx ? p : mx;
+        run += vv;
+        if (binade_of(run) != e || (run < 0) != (s0 < 0)) ok = false;  // likely crossing
+      }
+      if (ok) {
+        c.e = e;
+        c.neg = s0 < 0;
+        c.total = p;
+        c.pmin = mn;
+        c.pmax = mx;
+      }
+    }
+    ch[ax][t] = c;
+  }
+  __syncthreads();
+  // (c) the exact walk, one thread per axis
+  if (t != 0 && t != 32) return;
+  const int ax = t ? 1 : 0;
+  const double *v = ax ? y : x;
+  StageRing ring;
+  ring.init(ring_buf + (size_t)ax * CSUM_STAGES * CSUM_STAGE, ring_bar[ax], v, n);
+  const long long LO = (1ll << 52) + 1, HI = (1ll << 53) - 1;
+  double s = 0;
+  for (uint32_t c = 0; c < nc; ++c) {
+    const CsumChunk k = ch[ax][c];
+    bool fast = false;
+    if (k.e != INT_MIN && s != 0 && isfinite(s) && (s < 0) == (k.neg != 0) && binade_of(s) == k.e) {
+      const double scale = ldexp(1.0, 52 - k.e);
+      long long S = (long long)(fabs(s) * scale);  // exact: s is a multiple of u in [2^52 u, 2^53 u)
+      if (k.neg) {
+        // |s| shrinks by R: partial sums are -(S - P); need S - P within [LO, HI]
+        if (S - k.pmax >= LO && S - k.pmin <= HI) {
+          s = -ldexp((double)(S - k.total), k.e - 52);
+          fast = true;
+        }
+      } else if (S + k.pmin >= LO && S + k.pmax <= HI) {
+        s = ldexp((double)(S + k.total), k.e - 52);
+        fast = true;
+      }
+    }
+    if (!fast) {
+      const uint32_t end = min(n, (c + 1) * L);
+      for (uint32_t i = c * L; i < end; ++i) s += ring.at(i);
+    }
+  }
+  ring.drain();  // no copy may still target shared memory when the block exits
+  if (ring.timeout) atomicOr(status, ST_WAIT_TIMEOUT);
+  out[ax] = s;
 }
 
 __global__ void k_center_apply(double *x, double *y, uint32_t n, const double *sums, double cx,
@@ -635,10 +875,20 @@ __global__ void k_center_apply(double *x, double *y, uint32_t n, const double *s
   y[i] -= sy;
 }
 
-void center_force(const NodeArrays &a, double cx, double cy, double strength, ForceScratch &s,
+void center_sum(const NodeArrays &a, ForceScratch &s, uint32_t *status, cudaStream_t st) {
+  if (a.n == 0) return;
+  static bool attr = [] {
+    cudaFuncSetAttribute(k_center_sum, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)CSUM_DYN_SMEM);
+    return true;
+  }();
+  (void)attr;
+  D3_LAUNCH(k_center_sum, 1, CSUM_THREADS, CSUM_DYN_SMEM, st)(a.x, a.y, a.n, s.center, status);
+}
+
+void center_apply(const NodeArrays &a, double cx, double cy, double strength, ForceScratch &s,
                   cudaStream_t st) {
   if (a.n == 0) return;
-  D3_LAUNCH(k_center_sum, 1, 64, 0, st)(a.x, a.y, a.n, s.center);
   D3_LAUNCH(k_center_apply, blocks_for(a.n, 256), 256, 0, st)(a.x, a.y, a.n, s.center, cx, cy, strength);
 }
 

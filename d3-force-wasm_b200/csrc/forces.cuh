@@ -94,13 +94,16 @@ struct CollideSpec {
   uint32_t cap = 0;
   uint32_t *rlist = nullptr;
   uint8_t *rcount = nullptr;
-  uint64_t *wmask = nullptr;
+  uint64_t *wmask = nullptr, *emask = nullptr;
   uint8_t *state = nullptr;
   uint32_t *active = nullptr;
   uint64_t *min_acc = nullptr, *min_wr = nullptr;
   double *push = nullptr;
-  uint32_t *min_pusher = nullptr;
-  uint32_t *counters = nullptr;  // active, done, fail, jiggle, overflow, rounds, attempts, serial
+  uint32_t *min_pusher = nullptr, *max_pusher = nullptr;
+  uint32_t *vlist = nullptr;
+  uint16_t *vcount = nullptr;
+  uint32_t *counters = nullptr;  // collide_spec.cu C_*
+  unsigned long long *stamps = nullptr;
 };
 int collide_spec_reserve(CollideSpec &s, uint32_t n);
 void collide_spec_free(CollideSpec &s);
@@ -109,7 +112,11 @@ void collide_spec_free(CollideSpec &s);
 int collide_parallel(TreeDev &t, const NodeArrays &a, const double *radii, double strength,
                      double delta, Rng *rng, CollideSpec &s, cudaStream_t st);
 
-void center_force(const NodeArrays &a, double cx, double cy, double strength, ForceScratch &s,
+// simple.zig:14-31 in two steps: the sums of x and y in index order (bit-exact)
+// into s.center, then the shift. The sums only read positions, so the caller
+// may issue them early on another stream.
+void center_sum(const NodeArrays &a, ForceScratch &s, uint32_t *status, cudaStream_t st);
+void center_apply(const NodeArrays &a, double cx, double cy, double strength, ForceScratch &s,
                   cudaStream_t st);
 void axis_force(const NodeArrays &a, const double *strength, const double *target, double alpha,
                 int dim, cudaStream_t st);

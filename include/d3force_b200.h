@@ -142,7 +142,10 @@ double sim_last_tick_ms(uint32_t h);
  * loop, 3 nodes the last exact many-body traversal flagged for jiggle, 4 link
  * levels of the last exact link plan, 5 1 if the last exact link pass fell
  * back to the serial order (a jiggle), 6 kernels this library launched so
- * far (all simulations); 100 + k milliseconds and 200 + k count of phase k
+ * far (all simulations); 7, 8 turns of the last parallel collide that met an
+ * unguessed head / overlap, 9 inactive nodes whose turn would have written,
+ * 10 turns run from the recorded head list, 11 turns that traversed the tree;
+ * 100 + k milliseconds and 200 + k count of phase k
  * since sim_set_profile(h, 1): 0 many-body tree, 1 many-body accumulation,
  * 2 many-body traversal, 3 exact link, 4 collide tree and radii, 5 collide
  * node loop, 6 center, 7 integrate, 8 fast many-body, 9 fast link, 10 fast

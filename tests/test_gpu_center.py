@@ -1,0 +1,47 @@
+"""The exact parallel center sum: bit-identical to the serial index-order sum
+(simple.zig:14-31) on inputs that force its every path: long same-binade runs,
+binade crossings, sums through zero, ties, signed zeros, NaN, huge ranges."""
+
+import numpy as np
+import pytest
+
+import helpers as H
+import parity as P
+
+pkg = H.pkg
+pytestmark = pytest.mark.gpu
+
+
+def _center_only(xs, ys):
+    def setup(core):
+        nd = pkg.Nodes(len(xs), x=xs, y=ys, vx=[0.0] * len(xs), vy=[0.0] * len(xs))
+        sim = pkg.forceSimulation(nd, core=core).force("center", pkg.forceCenter(3.5, -2.25))
+        return nd, sim
+    return setup
+
+
+@pytest.mark.parametrize("case", ["walk", "offset", "ties", "tiny_huge", "zeros_nan", "large"])
+def test_gpu_center_sum_bitwise(ocore, gcore, case):
+    rng = np.random.default_rng(5)
+    n = 50000
+    if case == "walk":
+        xs = rng.normal(0, 2500, n)
+        ys = rng.normal(0, 2500, n)
+    elif case == "offset":
+        xs = 1e5 + rng.normal(0, 10, n)
+        ys = -3e6 + rng.normal(0, 1000, n)
+    elif case == "ties":
+        xs = np.round(rng.normal(0, 1e6, n)) + 0.5
+        ys = np.round(rng.normal(0, 4, n)) * 0.25
+    elif case == "tiny_huge":
+        xs = rng.normal(0, 1, n) * 10.0 ** rng.integers(-12, 12, n)
+        ys = rng.normal(0, 1, n) * 10.0 ** rng.integers(-300, 300, n)
+    elif case == "zeros_nan":
+        xs = np.where(rng.random(n) < 0.5, -0.0, 0.0)
+        ys = rng.normal(0, 1, n)
+        ys[n // 2] = np.nan
+    else:
+        n = 300000
+        xs = rng.normal(0, 1e4, n)
+        ys = rng.uniform(-1, 1, n) * 2.0 ** 40
+    P.run_pair(_center_only(list(xs), list(ys)), ocore, gcore, 3)

@@ -113,3 +113,21 @@ def test_gpu_exact_50k_collide(ocore, gcore):
     """The 50k + collide benchmark workload, bitwise for the first ticks."""
     P.run_pair(_defaults(50000, 100000, collide=5, coincident=0.01, near=0.01, pinned=0.005),
                ocore, gcore, 5)
+
+
+def test_gpu_sim_tick_path_matches(ocore, gcore):
+    """sim_tick (device-resident ticks, center sums overlapped on a side
+    stream) gives the same bits as one force_run per force per tick."""
+    setup = _defaults(5000, 10000, collide=5, coincident=0.01, near=0.01, pinned=0.005)
+    na, sa = setup(ocore)
+    nb, sb = setup(gcore)
+    try:
+        for chunk in (1, 4, 15):
+            sa.tick(chunk)
+            sb.run(chunk)
+            assert P.first_difference(na, nb) is None, "after a run of %d" % chunk
+            assert sa.alpha() == sb.alpha()
+        assert ocore.sim_get_lcg(sa.ctx.h) == gcore.sim_get_lcg(sb.ctx.h)
+    finally:
+        sa.close()
+        sb.close()

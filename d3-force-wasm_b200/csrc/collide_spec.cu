@@ -576,7 +576,9 @@ int collide_parallel(TreeDev &t, const NodeArrays &a, const double *radii, doubl
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_collide_spec, SPEC_THREADS, 0);
-    g_spec_blocks = sms * (per > 4 ? 4 : per);
+    // one block per SM short of full occupancy, so a concurrent one-block
+    // kernel (the center sums on the side stream) never delays the launch
+    g_spec_blocks = sms * (per > 3 ? 3 : (per > 1 ? per - 1 : 1));
     if (g_spec_blocks <= 0) g_spec_blocks = sms;
   }
   SpecArgs args;

@@ -913,7 +913,17 @@ int32_t sim_tick(uint32_t h, uint32_t ticks, double *alpha, double alpha_target,
     if (hoist >= 0 && s->n) {
       cudaEventRecord(s->ev_xready, s->stream);
       cudaStreamWaitEvent(s->side, s->ev_xready, 0);
+      cudaEvent_t e = nullptr;
+      if (s->profile) {
+        e = pool_event(s);
+        cudaEventRecord(e, s->side);
+      }
       center_sum(nodes_of(s), s->scratch, status_word(s), s->side);
+      if (e) {
+        cudaEvent_t b = pool_event(s);
+        cudaEventRecord(b, s->side);
+        s->pending.push_back({PH_OTHER, e, b});
+      }
       cudaEventRecord(s->ev_sumdone, s->side);
     }
     for (size_t i = 0; i < fs.size(); ++i) {

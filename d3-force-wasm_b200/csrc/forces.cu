@@ -722,17 +722,37 @@ struct StageRing {
     for (uint32_t k = 0; k < CSUM_STAGES; ++k) issue(k);
   }
 
-  // Value i: its stage is made resident (and the next stages prefetched).
-  __device__ double at(uint32_t i) {
-    const uint32_t k = i / CSUM_STAGE, off = i % CSUM_STAGE;
-    if (off >= copied(k)) return src[i];  // the odd last value
+  // Makes stage k resident (and prefetches the next stages); returns its
+  // slot's values, indexed so that [k * CSUM_STAGE + j] is value k * STAGE + j.
+  __device__ const double *resident(uint32_t k) {
     const uint32_t q = k % CSUM_STAGES;
     if (stage[q] != k || pending[q]) {
       issue(k);
       settle(q);
       for (uint32_t j = 1; j < CSUM_STAGES; ++j) issue(k + j);
     }
-    return buf[(size_t)q * CSUM_STAGE + off];
+    return buf + (size_t)q * CSUM_STAGE - (size_t)k * CSUM_STAGE;
+  }
+
+  // s += v[i] for i in [i0, i1), in order, from the staged copies.
+  __device__ double add_range(double s, uint32_t i0, uint32_t i1) {
+    uint32_t i = i0;
+    while (i < i1) {
+      const uint32_t k = i / CSUM_STAGE;
+      const uint32_t seg = min(i1, (k + 1) * CSUM_STAGE);
+      const uint32_t staged = min(seg, k * CSUM_STAGE + copied(k));
+      if (i < staged) {
+        const double *p = resident(k);
+        for (; i + 8 <= staged; i += 8) {
+          const double v0 = p[i], v1 = p[i + 1], v2 = p[i + 2], v3 = p[i + 3];
+          const double v4 = p[i + 4], v5 = p[i + 5], v6 = p[i + 6], v7 = p[i + 7];
+          s += v0; s += v1; s += v2; s += v3; s += v4; s += v5; s += v6; s += v7;
+        }
+        for (; i < staged; ++i) s += p[i];
+      }
+      for (; i < seg; ++i) s += src[i];  // the odd last value
+    }
+    return s;
   }
 
   // Every copy still in flight lands before the block may exit.
@@ -855,8 +875,11 @@ __global__ void __launch_bounds__(CSUM_THREADS) k_center_sum(const double *x, co
       }
     }
     if (!fast) {
-      const uint32_t end = min(n, (c + 1) * L);
-      for (uint32_t i = c * L; i < end; ++i) s += ring.at(i);
+      // consecutive serial chunks run as one range
+      uint32_t c1 = c + 1;
+      while (c1 < nc && ch[ax][c1].e == INT_MIN) ++c1;
+      s = ring.add_range(s, c * L, min(n, c1 * L));
+      c = c1 - 1;
     }
   }
   ring.drain();  // no copy may still target shared memory when the block exits

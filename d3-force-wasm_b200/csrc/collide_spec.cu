@@ -7,23 +7,28 @@
 // unless one writes something the other reads or writes. The kernel runs the
 // turns as a dependency DAG, in one cooperative launch:
 //
-//  G. Guess, per node, from the pass-start state and a margin `delta`: the heads
-//     it may examine (R) and those it may overlap (W, a mask over R). A node
-//     with W empty is inactive: it cannot write unless something moves by
-//     `delta` before its turn.
-//  E. Rounds over the active nodes: a node runs when no earlier unfinished
-//     active node writes what it reads or accesses what it writes (per-node
-//     "earliest accessor / writer" marks by 64-bit atomicMin, tagged with the
-//     round so no reset is needed). A running node traverses exactly as d3
-//     and writes only if everything it examined / overlapped was guessed.
-//  V. Inactive nodes are checked with the push magnitudes the pass applied
-//     (a node's position at its turn moved by at most the pushes it received
-//     from earlier nodes): if i and every guessed head stayed within `delta`,
-//     i's turn was a no-op, as guessed.
-//  Any failure promotes the failing nodes (every guessed head may be written),
-//  restores the pass-start velocities and runs E and V again; after 3
-//  attempts, or when a turn would draw from `random` (a zero delta), block 0
-//  runs the serial loop itself on the restored state.
+//  G. Guess, per node, from the pass-start state and a per-node margin
+//     delta_i (larger for nodes the previous pass pushed hard): the heads it may
+//     examine (R) and those it may overlap (W, a mask over R), the heads the
+//     exact traversal from the start examines (E), and the cells the margin
+//     traversal entered, in preorder. Traversals start at the smallest ancestor
+//     of the node's leaf whose box holds the whole search box: every cell
+//     outside that subtree is pruned anyway. A node with W empty is inactive.
+//  E. Rounds over the active nodes, one warp per node: a node runs when no
+//     earlier unfinished active node writes what it reads or accesses what it
+//     writes (per-node "earliest accessor / writer" marks, 64-bit atomicMin
+//     tagged with the round so no reset is needed). A running node evaluates
+//     its examined heads in parallel (from E if nothing moved it, else by
+//     replaying its recorded cells with the exact pruning test), adds its own
+//     pushes in visit order, and writes only if everything it examined or
+//     overlapped was guessed.
+//  V. Inactive nodes are re-run at their exact turn state (their own velocity
+//     is final: every push on a node comes from an earlier node) and must
+//     still find no overlap.
+//  Any failure promotes the failing nodes (every guessed head may be written,
+//  with a wider margin), restores the pass-start velocities and runs E and V
+//  again; after 3 attempts, or when a turn would draw from `random` (a zero
+//  delta), block 0 runs the serial loop itself on the restored state.
 #include <cooperative_groups.h>
 
 #include "forces.cuh"
@@ -33,23 +38,24 @@ namespace cg = cooperative_groups;
 namespace d3 {
 
 constexpr int SPEC_CAP = 64;        // guessed heads per node (R)
-constexpr int VISIT_CAP = 128;      // recorded margin-visited cells per node
+constexpr int VISIT_CAP = 128;      // recorded margin-entered cells per node
 constexpr uint16_t VISIT_NONE = 0xffff;
 constexpr int SPEC_ATTEMPTS = 3;
 constexpr uint32_t SPEC_MAX_ROUNDS = 4096;
 constexpr unsigned SPEC_THREADS = 256;
+constexpr unsigned SPEC_WARPS = SPEC_THREADS / 32;
 
 enum : uint32_t {
   C_ACTIVE = 0, C_DONE, C_FAIL, C_JIGGLE, C_OVERFLOW, C_ROUNDS, C_ATTEMPTS, C_SERIAL,
-  C_FAIL_READ, C_FAIL_WRITE, C_FAIL_MOVED, C_FAST_TURNS, C_SLOW_TURNS
+  C_FAIL_READ, C_FAIL_WRITE, C_FAIL_MOVED, C_FAST_TURNS, C_SLOW_TURNS, C_PEND0, C_PEND1, C_PEND2
 };
 
 struct SpecArgs {
   const Cell *cells;
-  const uint32_t *skip, *perm, *info;
+  const uint32_t *skip, *perm, *info, *parent, *leaf_of;
   const double *xs, *ys, *px, *py, *radii;
   double *vxs, *vys, *svx, *svy;
-  double strength, delta;
+  double strength, delta0;
   uint32_t n;
   uint32_t *rlist;       // n * SPEC_CAP
   uint8_t *rcount;       // n
@@ -57,14 +63,17 @@ struct SpecArgs {
   uint64_t *emask;       // n: heads the exact traversal from the pass start visits
   uint32_t *vlist;       // n * VISIT_CAP: cells the margin traversal entered, preorder
   uint16_t *vcount;      // n (VISIT_NONE: not recorded)
-  uint8_t *state;        // n: 0 inactive, 1 pending, 2 done
+  uint32_t *start;       // n: subtree root the traversals start from
+  double *mdelta;        // n: the node's margin
+  uint8_t *state;        // n: 0 inactive, 1 pending, 2 done, 3 / 4 failed (active / inactive)
   uint32_t *active;      // active node list
-  uint64_t *min_acc, *min_wr;  // tagged marks per node
-  double *push;          // push magnitude received per node
-  uint32_t *min_pusher;  // lowest pusher index per node
-  uint32_t *max_pusher;  // highest pusher index per node
+  uint32_t *pend[2];     // nodes still pending, compacted each round (alternating)
+  uint64_t *min_acc, *min_wr;  // tagged marks per node, two rounds' worth (round parity)
+  double *push;          // push magnitude received per node (this pass)
+  double *push_prev;     // ... in the previous pass (margin heuristic)
+  uint32_t *min_pusher, *max_pusher;
   uint32_t *counters;    // C_*
-  unsigned long long *stamps;  // phase timestamps (ns): G end, then per attempt rounds / V ends
+  unsigned long long *stamps;  // phase timestamps (ns)
   Rng *rng;
 };
 
@@ -76,21 +85,74 @@ __device__ inline uint64_t rd(const uint64_t *p) { return __ldcg((const unsigned
 __device__ inline uint8_t rd(const uint8_t *p) { return (uint8_t)__ldcg((const unsigned char *)p); }
 __device__ inline uint16_t rd(const uint16_t *p) { return (uint16_t)__ldcg((const unsigned short *)p); }
 
-// G: guessed heads (j > i) with pruning relaxed by `margin`, a mask of the
-// heads within r + margin of the pass-start positions, and a mask of the heads
-// the exact traversal from the pass-start position visits (those in a subtree
-// the exact test prunes are skipped via ex_until, the end of that subtree).
+__device__ inline bool same_bits(double a, double b) {
+  return __double_as_longlong(a) == __double_as_longlong(b);
+}
+
+__device__ inline bool pruned(const Cell &q, double xi, double yi, double r) {
+  return q.x0 > xi + r || q.x1 < xi - r || q.y0 > yi + r || q.y1 < yi - r;
+}
+
+// The margin of node j: the base margin plus three times what the previous
+// pass pushed it, bounded.
+__device__ inline double margin_of(const SpecArgs &a, uint32_t j) {
+  const double d = a.delta0 + 3 * a.push_prev[j];
+  const double cap = 2 * a.delta0;
+  return d < cap ? d : cap;
+}
+
+__device__ bool spec_guess(const SpecArgs &a, uint32_t i, double margin, bool all_writes);
+
+// A guess that overflows the lists is retried with half the margin, down to
+// the base margin (a smaller margin guesses fewer heads).
+__device__ bool spec_guess_fit(const SpecArgs &a, uint32_t i, double margin, bool all_writes) {
+  for (;;) {
+    if (spec_guess(a, i, margin, all_writes)) return true;
+    if (!(margin > a.delta0)) return false;
+    margin = margin * 0.5 > a.delta0 ? margin * 0.5 : a.delta0;
+  }
+}
+
+// The smallest ancestor of i's leaf whose box strictly contains the search
+// box of half-width R around (xi, yi), slack included; the root otherwise.
+// (With a negative radius an enclosing box no longer implies "not pruned":
+// those traversals start at the root.)
+__device__ uint32_t start_cell(const SpecArgs &a, uint32_t i, double xi, double yi, double R) {
+  uint32_t c = a.leaf_of[i];
+  if (c == NONE || !(R > 0) || !(a.radii[i] >= 0)) return 0;
+  const double slack = (fabs(xi) + fabs(yi) + R) * 0x1p-40 + 1e-300;
+  const double h = R + slack;
+  while (c != 0 && c != NONE) {
+    const Cell &q = a.cells[c];
+    if (q.x0 < xi - h && q.x1 > xi + h && q.y0 < yi - h && q.y1 > yi + h) break;
+    c = a.parent[c];
+  }
+  return c == NONE ? 0 : c;
+}
+
+// G for node i with margin `margin` (all_writes: every guessed head may be
+// written).
 __device__ bool spec_guess(const SpecArgs &a, uint32_t i, double margin, bool all_writes) {
   const uint32_t len = a.info[1];
   const double xi = a.px[i], yi = a.py[i], ri = a.radii[i];
   uint32_t *rl = a.rlist + (size_t)i * SPEC_CAP;
   uint32_t *vl = a.vlist + (size_t)i * VISIT_CAP;
-  uint32_t nr = 0, ex_until = 0, nv = 0;
-  uint64_t wm = 0, em = 0;
   a.rcount[i] = 0;
   a.wmask[i] = 0;
   a.emask[i] = 0;
-  for (uint32_t c = 0; c < len;) {
+  a.vcount[i] = 0;
+  a.mdelta[i] = margin;
+  if (len == 0 || xi != xi || yi != yi) {  // a NaN node never overlaps: a no-op turn
+    a.start[i] = 0;
+    return true;
+  }
+  const double rmax = a.cells[0].r;
+  const uint32_t c0 = start_cell(a, i, xi, yi, ri + rmax + margin);
+  const uint32_t c1 = c0 == 0 ? len : a.skip[c0];
+  a.start[i] = c0;
+  uint32_t nr = 0, ex_until = 0, nv = 0;
+  uint64_t wm = 0, em = 0;
+  for (uint32_t c = c0; c < c1;) {
     const Cell &q = a.cells[c];
     const double r = ri + q.r;
     const bool ex_vis = c >= ex_until;
@@ -101,7 +163,7 @@ __device__ bool spec_guess(const SpecArgs &a, uint32_t i, double margin, bool al
       if (j > i) {
         if (nr == SPEC_CAP) return false;
         const double dx = xi - a.px[j], dy = yi - a.py[j];
-        const double rr = r + margin;
+        const double rr = r + margin + margin_of(a, j);
         if (all_writes || dx * dx + dy * dy < rr * rr) wm |= 1ull << nr;
         if (ex_vis) em |= 1ull << nr;
         rl[nr++] = j;
@@ -109,13 +171,11 @@ __device__ bool spec_guess(const SpecArgs &a, uint32_t i, double margin, bool al
       c = c + 1;
       continue;
     }
-    if (q.x0 > xi + r + margin || q.x1 < xi - r - margin || q.y0 > yi + r + margin ||
-        q.y1 < yi - r - margin) {
+    if (pruned(q, xi, yi, r + margin)) {
       c = a.skip[c];
       continue;
     }
-    if (ex_vis && (q.x0 > xi + r || q.x1 < xi - r || q.y0 > yi + r || q.y1 < yi - r))
-      ex_until = a.skip[c];
+    if (ex_vis && pruned(q, xi, yi, r)) ex_until = a.skip[c];
     if (nv < VISIT_CAP) vl[nv] = c;
     ++nv;
     c = c + 1;
@@ -127,84 +187,145 @@ __device__ bool spec_guess(const SpecArgs &a, uint32_t i, double margin, bool al
   return true;
 }
 
-__device__ inline int spec_find(const uint32_t *rl, uint32_t nr, uint32_t j) {
-  for (uint32_t k = 0; k < nr; ++k)
-    if (rd(&rl[k]) == j) return (int)k;
-  return -1;
-}
-
-__device__ inline bool same_bits(double a, double b) {
-  return __double_as_longlong(a) == __double_as_longlong(b);
-}
-
-// The exact traversal of node i from (xi, yi), replayed over the cells its
-// margin traversal entered (in preorder): every cell the exact traversal
-// enters is among them while i stays within `delta` of the pass start, and a
-// subtree the exact test prunes is skipped to its end. `visit(j, k, rj)` is
-// called for each examined head j > i (k its index among the guessed heads);
-// returns false to stop. Returns -1 when the replay does not apply (no
-// record, or i moved too far), 0 when stopped, 1 when done.
-template <typename F>
-__device__ int spec_replay(const SpecArgs &a, uint32_t i, double xi, double yi, F visit) {
+// Which guessed heads node i examines from (xi, yi): a mask over R. Fast when
+// i has not moved (the exact-visit mask of the guess); otherwise the recorded
+// cells are replayed by the warp in parallel: a recorded cell is skipped when
+// it lies in the subtree of an earlier recorded cell the exact test prunes
+// (a running maximum of those subtrees' ends). Returns false when the record
+// does not apply (i moved beyond its margin, or no record): lane-uniform.
+__device__ bool warp_examined(const SpecArgs &a, uint32_t i, double xi, double yi, bool unmoved,
+                              uint64_t &mask) {
+  const unsigned lane = threadIdx.x & 31;
+  if (unmoved) {
+    mask = rd(&a.emask[i]);
+    return true;
+  }
   const uint16_t nv = rd(&a.vcount[i]);
-  if (nv == VISIT_NONE) return -1;
-  const double slack = a.delta * (1 - 1e-9);
-  if (!(fabs(xi - a.px[i]) < slack && fabs(yi - a.py[i]) < slack)) return -1;
+  const double md = rd(&a.mdelta[i]) * (1 - 1e-9);
+  if (nv == VISIT_NONE || !(fabs(xi - a.px[i]) < md && fabs(yi - a.py[i]) < md)) return false;
   const uint32_t *vl = a.vlist + (size_t)i * VISIT_CAP;
   const double ri = a.radii[i];
-  uint32_t ex_until = 0;
-  int k = 0;
-  for (uint32_t t = 0; t < nv; ++t) {
-    const uint32_t c = rd(&vl[t]);
-    if (c < ex_until) continue;
-    const Cell &q = a.cells[c];
-    if (is_leaf(q)) {
-      const uint32_t j = a.perm[q.first + q.count - 1];
-      if (j > i) {
-        if (!visit(j, k, q.r)) return 0;
-        ++k;
+  // lane holds recorded entries 4 lane .. 4 lane + 3
+  uint32_t cell[4], upto[4];
+  bool head[4];
+  uint32_t run = 0;
+  for (int u = 0; u < 4; ++u) {
+    const uint32_t t = 4 * lane + u;
+    cell[u] = NONE;
+    head[u] = false;
+    upto[u] = 0;
+    if (t < nv) {
+      const uint32_t c = rd(&vl[t]);
+      const Cell &q = a.cells[c];
+      cell[u] = c;
+      if (is_leaf(q)) {
+        head[u] = a.perm[q.first + q.count - 1] > i;
+      } else if (pruned(q, xi, yi, ri + q.r)) {
+        upto[u] = a.skip[c];
       }
-      continue;
     }
-    const double r = ri + q.r;
-    if (q.x0 > xi + r || q.x1 < xi - r || q.y0 > yi + r || q.y1 < yi - r) ex_until = a.skip[c];
+    run = max(run, upto[u]);
   }
-  return 1;
+  // exclusive max over earlier lanes' entries
+  uint32_t incl = run;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t yv = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= (unsigned)o) incl = max(incl, yv);
+  }
+  uint32_t before = __shfl_up_sync(0xffffffffu, incl, 1);
+  if (lane == 0) before = 0;
+  // heads' indices in R: exclusive count of heads before
+  uint32_t nh = 0;
+  for (int u = 0; u < 4; ++u) nh += head[u];
+  uint32_t hincl = nh;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t yv = __shfl_up_sync(0xffffffffu, hincl, o);
+    if (lane >= (unsigned)o) hincl += yv;
+  }
+  uint32_t k = hincl - nh;
+  uint64_t m = 0;
+  uint32_t ex = before;
+  for (int u = 0; u < 4; ++u) {
+    if (cell[u] == NONE) continue;
+    const bool vis = cell[u] >= ex;
+    if (head[u]) {
+      if (vis && k < 64) m |= 1ull << k;
+      ++k;
+    }
+    ex = max(ex, upto[u]);
+  }
+  for (int o = 16; o > 0; o >>= 1) m |= __shfl_xor_sync(0xffffffffu, m, o);
+  mask = m;
+  return true;
 }
 
-// E: node i's turn, exactly collide.zig:48-99; writes only if every examined
-// head and every overlap was guessed and no zero delta occurs. A node not
-// pushed since the pass start sits where the guess traversed from, so it
-// examines exactly the heads of its exact-visit mask, in that order, and needs
-// no traversal.
-__device__ void spec_turn(const SpecArgs &a, uint32_t i) {
-  const uint32_t len = a.info[1];
+// E: node i's turn by one warp.
+__device__ void warp_turn(const SpecArgs &a, uint32_t i, double *cx, double *cy) {
+  const unsigned lane = threadIdx.x & 31;
   const uint32_t *rl = a.rlist + (size_t)i * SPEC_CAP;
   const uint32_t nr = rd(&a.rcount[i]);
   const uint64_t wm = rd(&a.wmask[i]);
   const double ri = a.radii[i], ri2 = ri * ri;
-  double vi = rd(&a.vxs[i]), wi = rd(&a.vys[i]);
+  const double vi = rd(&a.vxs[i]), wi = rd(&a.vys[i]);
   const double xi = a.xs[i] + vi, yi = a.ys[i] + wi;
-  const bool fast = same_bits(vi, rd(&a.svx[i])) && same_bits(wi, rd(&a.svy[i]));
-  uint32_t pj[SPEC_CAP];
-  double pdx[SPEC_CAP], pdy[SPEC_CAP];
-  uint32_t np = 0;
-  // One examined head: false = the turn must not write (failure or jiggle).
-  auto head = [&](uint32_t j, int k, double rj) -> bool {
+  const bool unmoved = same_bits(vi, rd(&a.svx[i])) && same_bits(wi, rd(&a.svy[i]));
+  uint64_t ex = 0;
+  if (!warp_examined(a, i, xi, yi, unmoved, ex)) {
+    // i moved beyond its margin: lane 0 runs the exact traversal from the
+    // root; every head it examines must still be among the guessed ones.
+    uint32_t bad = 0;
+    if (lane == 0) {
+      const uint32_t len = a.info[1];
+      for (uint32_t c = 0; c < len && !bad;) {
+        const Cell &q = a.cells[c];
+        if (is_leaf(q)) {
+          const uint32_t j = a.perm[q.first + q.count - 1];
+          if (j > i) {
+            uint32_t k = 0;
+            while (k < nr && rd(&rl[k]) != j) ++k;
+            if (k == nr) bad = 1;
+            else ex |= 1ull << k;
+          }
+          c = c + 1;
+          continue;
+        }
+        c = pruned(q, xi, yi, ri + q.r) ? a.skip[c] : c + 1;
+      }
+    }
+    bad = __shfl_sync(0xffffffffu, bad, 0);
+    ex = __shfl_sync(0xffffffffu, ex, 0);
+    if (bad) {
+      if (lane == 0) {
+        atomicAdd(&a.counters[C_FAIL], 1u);
+        atomicAdd(&a.counters[C_FAIL_READ], 1u);
+        a.state[i] = 3;
+      }
+      return;
+    }
+  }
+  // each lane evaluates the examined heads with indices lane and lane + 32
+  bool fail = false, jig = false;
+  uint64_t over = 0;
+  uint32_t pj[2];
+  double pdx[2], pdy[2];
+  int np = 0;
+  for (int h = 0; h < 2; ++h) {
+    const uint32_t e = lane + 32 * h;
+    if (e >= nr || !((ex >> e) & 1)) continue;
+    const uint32_t j = rd(&rl[e]);
+    double rj = a.radii[j];
     double r = ri + rj;
     double x = xi - a.xs[j] - rd(&a.vxs[j]);
     double y = yi - a.ys[j] - rd(&a.vys[j]);
     double l = x * x + y * y;
-    if (!(l < r * r)) return true;
-    if (!((wm >> k) & 1)) {
-      atomicAdd(&a.counters[C_FAIL], 1u);
-      atomicAdd(&a.counters[C_FAIL_WRITE], 1u);
-      a.state[i] = 3;
-      return false;
+    if (!(l < r * r)) continue;
+    if (!((wm >> e) & 1)) {
+      fail = true;
+      continue;
     }
     if (x == 0 || y == 0) {
-      atomicAdd(&a.counters[C_JIGGLE], 1u);
-      return false;
+      jig = true;
+      continue;
     }
     l = sqrt(l);
     l = (r - l) / l * a.strength;
@@ -212,76 +333,69 @@ __device__ void spec_turn(const SpecArgs &a, uint32_t i) {
     y *= l;
     rj *= rj;
     r = rj / (ri2 + rj);
-    vi += x * r;
-    wi += y * r;
+    cx[e] = x * r;
+    cy[e] = y * r;
+    over |= 1ull << e;
     r = 1 - r;
     pj[np] = j;
     pdx[np] = x * r;
     pdy[np] = y * r;
     ++np;
-    return true;
-  };
-  if (fast) {
-    uint64_t em = rd(&a.emask[i]);
-    while (em) {
-      const int k = __ffsll((long long)em) - 1;
-      em &= em - 1;
-      const uint32_t j = rd(&rl[k]);
-      if (!head(j, k, a.radii[j])) return;
-    }
-    atomicAdd(&a.counters[C_FAST_TURNS], 1u);
-  } else {
-    for (uint32_t c = 0; c < len;) {
-      const Cell &q = a.cells[c];
-      const double r = ri + q.r;
-      if (is_leaf(q)) {
-        const uint32_t j = a.perm[q.first + q.count - 1];
-        if (j > i) {
-          const int k = spec_find(rl, nr, j);
-          if (k < 0) {
-            atomicAdd(&a.counters[C_FAIL], 1u);
-            atomicAdd(&a.counters[C_FAIL_READ], 1u);
-            a.state[i] = 3;
-            return;
-          }
-          if (!head(j, k, q.r)) return;
-        }
-        c = c + 1;
-        continue;
-      }
-      if (q.x0 > xi + r || q.x1 < xi - r || q.y0 > yi + r || q.y1 < yi - r) c = a.skip[c];
-      else c = c + 1;
-    }
-    atomicAdd(&a.counters[C_SLOW_TURNS], 1u);
   }
-  a.vxs[i] = vi;
-  a.vys[i] = wi;
-  for (uint32_t k = 0; k < np; ++k) {
-    const uint32_t j = pj[k];
-    a.vxs[j] = rd(&a.vxs[j]) - pdx[k];
-    a.vys[j] = rd(&a.vys[j]) - pdy[k];
-    atomicAdd(&a.push[j], sqrt(pdx[k] * pdx[k] + pdy[k] * pdy[k]));
+  fail = __any_sync(0xffffffffu, fail);
+  jig = __any_sync(0xffffffffu, jig);
+  for (int o = 16; o > 0; o >>= 1) over |= __shfl_xor_sync(0xffffffffu, over, o);
+  __syncwarp();
+  if (fail || jig) {
+    if (lane == 0) {
+      if (jig) atomicAdd(&a.counters[C_JIGGLE], 1u);
+      if (fail) {
+        atomicAdd(&a.counters[C_FAIL], 1u);
+        atomicAdd(&a.counters[C_FAIL_WRITE], 1u);
+        a.state[i] = 3;
+      }
+    }
+    return;
+  }
+  if (lane == 0) {
+    // d3 adds its own share head by head, in visit order (R order)
+    double v = vi, w = wi;
+    uint64_t o = over;
+    while (o) {
+      const int e = __ffsll((long long)o) - 1;
+      o &= o - 1;
+      v += cx[e];
+      w += cy[e];
+    }
+    a.vxs[i] = v;
+    a.vys[i] = w;
+    atomicAdd(&a.counters[unmoved ? C_FAST_TURNS : C_SLOW_TURNS], 1u);
+  }
+  for (int h = 0; h < np; ++h) {
+    const uint32_t j = pj[h];
+    a.vxs[j] = rd(&a.vxs[j]) - pdx[h];
+    a.vys[j] = rd(&a.vys[j]) - pdy[h];
+    atomicAdd(&a.push[j], sqrt(pdx[h] * pdx[h] + pdy[h] * pdy[h]));
     atomicMin(&a.min_pusher[j], i);
     atomicMax(&a.max_pusher[j], i);
   }
 }
 
-// V: an inactive node's turn, re-run at its exact turn state. Its own
-// velocity is final (every push on i comes from an earlier node); a head's is
-// its start value if all its pushers come later, its final value if all came
-// earlier, and otherwise only bounded (then a distance margin must hold).
-// Returns false when the turn might examine or overlap something unguessed.
+// V: an inactive node's turn re-run at its exact turn state. Its own velocity
+// is final; a head's is its start value if all its pushers come later, its
+// final value if all came earlier, and otherwise only bounded (then a distance
+// margin must hold). Returns false when the turn could write.
 __device__ bool spec_inactive_ok(const SpecArgs &a, uint32_t i) {
   const uint32_t *rl = a.rlist + (size_t)i * SPEC_CAP;
   const uint32_t nr = rd(&a.rcount[i]);
   const double vi = rd(&a.vxs[i]), wi = rd(&a.vys[i]);
-  bool any = !same_bits(vi, rd(&a.svx[i])) || !same_bits(wi, rd(&a.svy[i]));
+  const bool unmoved = same_bits(vi, rd(&a.svx[i])) && same_bits(wi, rd(&a.svy[i]));
+  bool any = !unmoved;
   for (uint32_t k = 0; k < nr && !any; ++k) any = rd(&a.min_pusher[rd(&rl[k])]) != NONE;
   if (!any) return true;  // nothing it reads moved: the guess holds as computed
-  const uint32_t len = a.info[1];
   const double ri = a.radii[i];
   const double xi = a.xs[i] + vi, yi = a.ys[i] + wi;
-  // false: the head may overlap at i's turn
+  if (xi != xi || yi != yi) return true;
   auto clear = [&](uint32_t j, double rj) -> bool {
     const double r = ri + rj;
     const uint32_t lo = rd(&a.min_pusher[j]), hi = rd(&a.max_pusher[j]);
@@ -293,7 +407,6 @@ __device__ bool spec_inactive_ok(const SpecArgs &a, uint32_t i) {
       vj = rd(&a.vxs[j]);
       wj = rd(&a.vys[j]);
     } else {
-      // pushed before and after i's turn: bound the move by all pushes
       const double dx = xi - a.xs[j] - rd(&a.svx[j]), dy = yi - a.ys[j] - rd(&a.svy[j]);
       const double gap = sqrt(dx * dx + dy * dy) - r - rd(&a.push[j]);
       return gap > 1e-9 * (r + 1);
@@ -301,58 +414,77 @@ __device__ bool spec_inactive_ok(const SpecArgs &a, uint32_t i) {
     const double x = xi - a.xs[j] - vj, y = yi - a.ys[j] - wj;
     return !(x * x + y * y < r * r);
   };
-  bool ok = true;
-  const int rp = spec_replay(a, i, xi, yi, [&](uint32_t j, int, double rj) {
-    ok = clear(j, rj);
-    return ok;
-  });
-  if (rp >= 0) return ok;
+  // replay the recorded cells (valid while i stays within its margin)
+  const uint16_t nv = rd(&a.vcount[i]);
+  const double md = rd(&a.mdelta[i]) * (1 - 1e-9);
+  if (nv != VISIT_NONE && fabs(xi - a.px[i]) < md && fabs(yi - a.py[i]) < md) {
+    const uint32_t *vl = a.vlist + (size_t)i * VISIT_CAP;
+    uint32_t ex_until = 0;
+    for (uint32_t t = 0; t < nv; ++t) {
+      const uint32_t c = rd(&vl[t]);
+      const Cell &q = a.cells[c];
+      if (is_leaf(q)) {
+        const uint32_t j = a.perm[q.first + q.count - 1];
+        if (j > i && c >= ex_until && !clear(j, q.r)) return false;
+        continue;
+      }
+      if (c >= ex_until && pruned(q, xi, yi, ri + q.r)) ex_until = a.skip[c];
+    }
+    return true;
+  }
+  const uint32_t len = a.info[1];
   for (uint32_t c = 0; c < len;) {
     const Cell &q = a.cells[c];
     const double r = ri + q.r;
     if (is_leaf(q)) {
       const uint32_t j = a.perm[q.first + q.count - 1];
-      if (j > i && (spec_find(rl, nr, j) < 0 || !clear(j, q.r))) return false;
+      if (j > i) {
+        bool found = false;
+        for (uint32_t k = 0; k < nr && !found; ++k) found = rd(&rl[k]) == j;
+        if (!found || !clear(j, q.r)) return false;
+      }
       c = c + 1;
       continue;
     }
-    if (q.x0 > xi + r || q.x1 < xi - r || q.y0 > yi + r || q.y1 < yi - r) c = a.skip[c];
-    else c = c + 1;
+    c = pruned(q, xi, yi, r) ? a.skip[c] : c + 1;
   }
   return true;
 }
 
-__device__ bool spec_ready(const SpecArgs &a, uint32_t i, uint64_t tag) {
+__device__ bool warp_ready(const SpecArgs &a, uint32_t i, uint64_t tag, uint32_t par) {
+  const unsigned lane = threadIdx.x & 31;
+  const uint64_t *min_acc = a.min_acc + (size_t)par * a.n, *min_wr = a.min_wr + (size_t)par * a.n;
   const uint32_t *rl = a.rlist + (size_t)i * SPEC_CAP;
   const uint32_t nr = rd(&a.rcount[i]);
   const uint64_t wm = rd(&a.wmask[i]);
-  // self: read and written
-  uint64_t v = __ldcg((const unsigned long long *)&a.min_acc[i]);
-  if ((v >> 32) == tag && (uint32_t)v < i) return false;
-  for (uint32_t k = 0; k < nr; ++k) {
-    const uint32_t j = rd(&rl[k]);
-    if ((wm >> k) & 1) {
-      v = __ldcg((const unsigned long long *)&a.min_acc[j]);
-      if ((v >> 32) == tag && (uint32_t)v < i) return false;
-    } else {
-      v = __ldcg((const unsigned long long *)&a.min_wr[j]);
-      if ((v >> 32) == tag && (uint32_t)v < i) return false;
-    }
+  bool ok = true;
+  if (lane == 0) {  // self: read and written
+    const uint64_t v = rd(&min_acc[i]);
+    ok = !((v >> 32) == tag && (uint32_t)v < i);
   }
-  return true;
+  for (uint32_t k = lane; k < nr; k += 32) {
+    const uint32_t j = rd(&rl[k]);
+    const uint64_t v = ((wm >> k) & 1) ? rd(&min_acc[j]) : rd(&min_wr[j]);
+    if ((v >> 32) == tag && (uint32_t)v < i) ok = false;
+  }
+  return __all_sync(0xffffffffu, ok);
 }
 
-__device__ void spec_mark(const SpecArgs &a, uint32_t i, uint64_t tag) {
+__device__ void warp_mark(const SpecArgs &a, uint32_t i, uint64_t tag, uint32_t par) {
+  const unsigned lane = threadIdx.x & 31;
+  uint64_t *min_acc = a.min_acc + (size_t)par * a.n, *min_wr = a.min_wr + (size_t)par * a.n;
   const uint32_t *rl = a.rlist + (size_t)i * SPEC_CAP;
   const uint32_t nr = rd(&a.rcount[i]);
   const uint64_t wm = rd(&a.wmask[i]);
   const unsigned long long t = (tag << 32) | i;
-  atomicMin((unsigned long long *)&a.min_acc[i], t);
-  atomicMin((unsigned long long *)&a.min_wr[i], t);
-  for (uint32_t k = 0; k < nr; ++k) {
+  if (lane == 0) {
+    atomicMin((unsigned long long *)&min_acc[i], t);
+    atomicMin((unsigned long long *)&min_wr[i], t);
+  }
+  for (uint32_t k = lane; k < nr; k += 32) {
     const uint32_t j = rd(&rl[k]);
-    atomicMin((unsigned long long *)&a.min_acc[j], t);
-    if ((wm >> k) & 1) atomicMin((unsigned long long *)&a.min_wr[j], t);
+    atomicMin((unsigned long long *)&min_acc[j], t);
+    if ((wm >> k) & 1) atomicMin((unsigned long long *)&min_wr[j], t);
   }
 }
 
@@ -392,8 +524,7 @@ __device__ void spec_serial(const SpecArgs &a) {
         c = c + 1;
         continue;
       }
-      if (q.x0 > xi + r || q.x1 < xi - r || q.y0 > yi + r || q.y1 < yi - r) c = a.skip[c];
-      else c = c + 1;
+      c = pruned(q, xi, yi, r) ? a.skip[c] : c + 1;
     }
   }
   a.rng->lcg = s;
@@ -406,25 +537,28 @@ __device__ inline unsigned long long now_ns() {
 }
 
 __global__ void __launch_bounds__(SPEC_THREADS) k_collide_spec(SpecArgs a) {
+  __shared__ double contrib[SPEC_WARPS][2][SPEC_CAP];
   cg::grid_group g = cg::this_grid();
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  const uint32_t gw = tid >> 5, nwarps = nth >> 5, wl = threadIdx.x >> 5;
+  const unsigned lane = threadIdx.x & 31;
+  const uint32_t n = a.n;
+  if (tid < 16) a.counters[tid] = 0;
+  if (tid == 0) {
     for (int k = 0; k < 16; ++k) a.stamps[k] = 0;
     a.stamps[0] = now_ns();
   }
-  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
-  const uint32_t n = a.n;
-  if (tid < 16) a.counters[tid] = 0;
   g.sync();
   // G, plus per-node resets and the pass-start snapshot.
   for (uint32_t i = tid; i < n; i += nth) {
     a.svx[i] = a.vxs[i];
     a.svy[i] = a.vys[i];
-    a.min_acc[i] = ~0ull;
-    a.min_wr[i] = ~0ull;
+    a.min_acc[i] = a.min_acc[n + i] = ~0ull;
+    a.min_wr[i] = a.min_wr[n + i] = ~0ull;
     a.push[i] = 0;
     a.min_pusher[i] = NONE;
     a.max_pusher[i] = 0;
-    if (!spec_guess(a, i, a.delta, false)) {
+    if (!spec_guess_fit(a, i, margin_of(a, i), false)) {
       atomicAdd(&a.counters[C_OVERFLOW], 1u);
       a.state[i] = 0;
       continue;
@@ -441,31 +575,59 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_collide_spec(SpecArgs a) {
   bool ok = false;
   uint32_t round_base = 0;
   for (int attempt = 0; attempt < SPEC_ATTEMPTS && !ok; ++attempt) {
-    if (__ldcg(&a.counters[C_OVERFLOW]) || __ldcg(&a.counters[C_JIGGLE])) break;
-    const uint32_t n_active = __ldcg(&a.counters[C_ACTIVE]);
+    if (rd(&a.counters[C_OVERFLOW]) || rd(&a.counters[C_JIGGLE])) break;
+    const uint32_t n_active = rd(&a.counters[C_ACTIVE]);
+    // round 0 works on the active list; later rounds on the nodes the
+    // previous round left pending (their sizes rotate through C_PEND0..2)
+    const uint32_t *list = a.active;
+    uint32_t n_list = n_active;
+    // The first round's marks; afterwards a node that is not ready marks for
+    // the next round at once (the other parity's marks), so each round needs
+    // one grid-wide barrier.
+    {
+      const uint64_t tag0 = 0xFFFFFFFFull - round_base;
+      for (uint32_t k = gw; k < n_list; k += nwarps) {
+        const uint32_t i = rd(&list[k]);
+        if (rd(&a.state[i]) == 1) warp_mark(a, i, tag0, round_base & 1);
+      }
+      if (tid == 0) a.counters[C_PEND0] = a.counters[C_PEND1] = a.counters[C_PEND2] = 0;
+      g.sync();
+    }
     for (uint32_t round = 0;; ++round) {
-      if (round_base + round >= SPEC_MAX_ROUNDS) {
+      const uint32_t r = round_base + round;
+      if (r + 1 >= SPEC_MAX_ROUNDS) {
         if (tid == 0) atomicAdd(&a.counters[C_OVERFLOW], 1u);
         break;
       }
-      const uint64_t tag = 0xFFFFFFFFull - (round_base + round);
-      for (uint32_t k = tid; k < n_active; k += nth) {
-        const uint32_t i = rd(&a.active[k]);
-        if (rd(&a.state[i]) == 1) spec_mark(a, i, tag);
+      const uint64_t tag = 0xFFFFFFFFull - r, tag_next = tag - 1;
+      uint32_t *next = a.pend[round & 1];
+      uint32_t *next_n = &a.counters[C_PEND0 + round % 3];
+      for (uint32_t k = gw; k < n_list; k += nwarps) {
+        const uint32_t i = rd(&list[k]);
+        if (rd(&a.state[i]) != 1) continue;
+        if (!warp_ready(a, i, tag, r & 1)) {
+          warp_mark(a, i, tag_next, (r + 1) & 1);
+          if (lane == 0) next[atomicAdd(next_n, 1u)] = i;
+          continue;
+        }
+        if (lane == 0) a.state[i] = 2;  // done (3 = failed, set by the turn)
+        __syncwarp();
+        warp_turn(a, i, contrib[wl][0], contrib[wl][1]);
+        if (lane == 0) atomicAdd(&a.counters[C_DONE], 1u);
+        __syncwarp();
       }
       g.sync();
-      for (uint32_t k = tid; k < n_active; k += nth) {
-        const uint32_t i = rd(&a.active[k]);
-        if (rd(&a.state[i]) != 1 || !spec_ready(a, i, tag)) continue;
-        a.state[i] = 2;  // done (or 3 = failed, set by the turn)
-        spec_turn(a, i);
-        atomicAdd(&a.counters[C_DONE], 1u);
-      }
-      g.sync();
-      if (__ldcg(&a.counters[C_DONE]) >= n_active) {
+      // Every thread reads the same count: it changes again only after the
+      // next barrier. (C_DONE cannot decide this: the next round's turns may
+      // already be adding to it.)
+      n_list = rd(next_n);
+      if (n_list == 0) {
         round_base += round + 1;
         break;
       }
+      list = next;
+      // the counter of round + 2 was last read before this round's barrier
+      if (tid == 0) a.counters[C_PEND0 + (round + 2) % 3] = 0;
     }
     if (tid == 0 && attempt < 3) a.stamps[2 + 2 * attempt] = now_ns();
     // V: inactive nodes stayed no-ops.
@@ -480,8 +642,8 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_collide_spec(SpecArgs a) {
     g.sync();
     if (tid == 0 && attempt < 3) a.stamps[3 + 2 * attempt] = now_ns();
     if (tid == 0) atomicAdd(&a.counters[C_ATTEMPTS], 1u);
-    if (__ldcg(&a.counters[C_FAIL]) == 0 && __ldcg(&a.counters[C_DONE]) >= n_active &&
-        __ldcg(&a.counters[C_JIGGLE]) == 0) {
+    if (rd(&a.counters[C_FAIL]) == 0 && rd(&a.counters[C_DONE]) >= n_active &&
+        rd(&a.counters[C_JIGGLE]) == 0) {
       ok = true;
       break;
     }
@@ -494,9 +656,8 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_collide_spec(SpecArgs a) {
       a.max_pusher[i] = 0;
       const uint8_t st = rd(&a.state[i]);
       if (st == 3 || st == 4) {
-        // examined something unguessed, or moved too far: every head within
-        // a wider margin may be written
-        if (!spec_guess(a, i, 4 * a.delta, true)) atomicAdd(&a.counters[C_OVERFLOW], 1u);
+        // every head within a four times wider margin may be written
+        if (!spec_guess_fit(a, i, 4 * rd(&a.mdelta[i]), true)) atomicAdd(&a.counters[C_OVERFLOW], 1u);
         if (st == 4) a.active[atomicAdd(&a.counters[C_ACTIVE], 1u)] = i;  // was inactive
         a.state[i] = 1;
       } else if (st == 2) {
@@ -511,6 +672,7 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_collide_spec(SpecArgs a) {
     g.sync();
   }
   if (ok) {
+    for (uint32_t i = tid; i < n; i += nth) a.push_prev[i] = a.push[i];
     if (tid == 0) {
       a.counters[C_ROUNDS] = round_base;
       a.stamps[9] = now_ns();
@@ -538,24 +700,30 @@ int collide_spec_reserve(CollideSpec &s, uint32_t n) {
   cudaFree(s.rlist); cudaFree(s.rcount); cudaFree(s.wmask); cudaFree(s.state); cudaFree(s.active);
   cudaFree(s.min_acc); cudaFree(s.min_wr); cudaFree(s.push); cudaFree(s.min_pusher);
   cudaFree(s.emask); cudaFree(s.max_pusher); cudaFree(s.vlist); cudaFree(s.vcount);
+  cudaFree(s.start); cudaFree(s.mdelta); cudaFree(s.push_prev); cudaFree(s.pend);
   if (!s.counters) {
     D3_CUDA_OK(cudaMalloc(&s.counters, 16 * sizeof(uint32_t)));
     D3_CUDA_OK(cudaMemset(s.counters, 0, 16 * sizeof(uint32_t)));
   }
+  if (!s.stamps) D3_CUDA_OK(cudaMalloc(&s.stamps, 16 * sizeof(unsigned long long)));
   D3_CUDA_OK(cudaMalloc(&s.rlist, (size_t)cap * SPEC_CAP * 4));
   D3_CUDA_OK(cudaMalloc(&s.rcount, cap));
   D3_CUDA_OK(cudaMalloc(&s.wmask, cap * 8ull));
   D3_CUDA_OK(cudaMalloc(&s.state, cap));
   D3_CUDA_OK(cudaMalloc(&s.active, 2ull * cap * 4));
-  D3_CUDA_OK(cudaMalloc(&s.min_acc, cap * 8ull));
-  D3_CUDA_OK(cudaMalloc(&s.min_wr, cap * 8ull));
+  D3_CUDA_OK(cudaMalloc(&s.min_acc, 2 * cap * 8ull));
+  D3_CUDA_OK(cudaMalloc(&s.min_wr, 2 * cap * 8ull));
   D3_CUDA_OK(cudaMalloc(&s.push, cap * 8ull));
   D3_CUDA_OK(cudaMalloc(&s.min_pusher, cap * 4ull));
   D3_CUDA_OK(cudaMalloc(&s.emask, cap * 8ull));
   D3_CUDA_OK(cudaMalloc(&s.max_pusher, cap * 4ull));
   D3_CUDA_OK(cudaMalloc(&s.vlist, (size_t)cap * VISIT_CAP * 4));
   D3_CUDA_OK(cudaMalloc(&s.vcount, cap * 2ull));
-  if (!s.stamps) D3_CUDA_OK(cudaMalloc(&s.stamps, 16 * sizeof(unsigned long long)));
+  D3_CUDA_OK(cudaMalloc(&s.start, cap * 4ull));
+  D3_CUDA_OK(cudaMalloc(&s.mdelta, cap * 8ull));
+  D3_CUDA_OK(cudaMalloc(&s.push_prev, cap * 8ull));
+  D3_CUDA_OK(cudaMemset(s.push_prev, 0, cap * 8ull));
+  D3_CUDA_OK(cudaMalloc(&s.pend, 4ull * cap * 4));
   s.cap = cap;
   return 0;
 }
@@ -564,6 +732,7 @@ void collide_spec_free(CollideSpec &s) {
   cudaFree(s.rlist); cudaFree(s.rcount); cudaFree(s.wmask); cudaFree(s.state); cudaFree(s.active);
   cudaFree(s.min_acc); cudaFree(s.min_wr); cudaFree(s.push); cudaFree(s.min_pusher);
   cudaFree(s.emask); cudaFree(s.max_pusher); cudaFree(s.vlist); cudaFree(s.vcount);
+  cudaFree(s.start); cudaFree(s.mdelta); cudaFree(s.push_prev); cudaFree(s.pend);
   cudaFree(s.counters); cudaFree(s.stamps);
   s = CollideSpec();
 }
@@ -583,14 +752,18 @@ int collide_parallel(TreeDev &t, const NodeArrays &a, const double *radii, doubl
   }
   SpecArgs args;
   args.cells = t.cells; args.skip = t.skip; args.perm = t.perm; args.info = t.info;
+  args.parent = t.parent; args.leaf_of = t.leaf_of;
   args.xs = a.x; args.ys = a.y; args.px = a.px; args.py = a.py; args.radii = radii;
   args.vxs = a.vx; args.vys = a.vy; args.svx = a.snap_vx; args.svy = a.snap_vy;
-  args.strength = strength; args.delta = delta; args.n = a.n;
-  args.rlist = s.rlist; args.rcount = s.rcount; args.wmask = s.wmask; args.state = s.state;
-  args.active = s.active; args.min_acc = s.min_acc; args.min_wr = s.min_wr; args.push = s.push;
-  args.min_pusher = s.min_pusher; args.counters = s.counters; args.rng = rng;
-  args.emask = s.emask; args.max_pusher = s.max_pusher;
-  args.vlist = s.vlist; args.vcount = s.vcount; args.stamps = s.stamps;
+  args.strength = strength; args.delta0 = delta; args.n = a.n;
+  args.rlist = s.rlist; args.rcount = s.rcount; args.wmask = s.wmask; args.emask = s.emask;
+  args.vlist = s.vlist; args.vcount = s.vcount; args.start = s.start; args.mdelta = s.mdelta;
+  args.state = s.state; args.active = s.active; args.min_acc = s.min_acc; args.min_wr = s.min_wr;
+  args.push = s.push; args.push_prev = s.push_prev; args.min_pusher = s.min_pusher;
+  args.max_pusher = s.max_pusher; args.counters = s.counters; args.stamps = s.stamps;
+  args.rng = rng;
+  args.pend[0] = s.pend;
+  args.pend[1] = s.pend + 2ull * s.cap;
   void *params[] = {&args};
   ++g_launches;
   cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_collide_spec, g_spec_blocks,

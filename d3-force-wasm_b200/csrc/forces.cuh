@@ -102,6 +102,8 @@ struct CollideSpec {
   uint32_t *min_pusher = nullptr, *max_pusher = nullptr;
   uint32_t *vlist = nullptr;
   uint16_t *vcount = nullptr;
+  uint32_t *start = nullptr, *pend = nullptr;
+  double *mdelta = nullptr, *push_prev = nullptr;
   uint32_t *counters = nullptr;  // collide_spec.cu C_*
   unsigned long long *stamps = nullptr;
 };

@@ -182,13 +182,17 @@ __global__ void k_keys(const double *xs, const double *ys, uint32_t n, const dou
 // sorted point the levels its key shares with the previous one: -1 for the
 // first, 64 for the same position (no boundary), else min(32, clz / 2).
 __global__ void k_runs(const double *xs, const double *ys, uint32_t n, const uint64_t *keys,
-                       const uint32_t *sv, uint32_t *perm, int8_t *lcpx, const uint32_t *info) {
+                       const uint32_t *sv, uint32_t *perm, int8_t *lcpx, const uint32_t *info,
+                       uint32_t *leaf_of) {
   uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   uint32_t p = sv[k] & 0x7fffffffu;
   perm[k] = p;
   uint32_t m = info[0];
-  if (k >= m) return;
+  if (k >= m) {
+    leaf_of[p] = NONE;
+    return;
+  }
   if (k == 0) {
     lcpx[0] = -1;
     return;
@@ -234,7 +238,7 @@ __device__ uint32_t deep_group(bool write, uint32_t lo, uint32_t hi, uint32_t c3
                                const double *extent, const double *xs, const double *ys,
                                uint32_t *perm, uint32_t *perm_tmp, Frame *frames, Cell *cells,
                                uint32_t *parent, uint32_t *skip, uint32_t skip_after,
-                               uint32_t *depth_out) {
+                               uint32_t *depth_out, uint32_t *leaf_of) {
   Frame *stack = frames + 4 * (size_t)lo;
   const uint32_t cap = 4 * (hi - lo);
   uint32_t sp = 0, emitted = 0, maxd = 32;
@@ -269,7 +273,11 @@ __device__ uint32_t deep_group(bool write, uint32_t lo, uint32_t hi, uint32_t c3
         uint32_t p = perm[k];
         if (xs[p] != xs[p0] || ys[p] != ys[p0]) { same = false; break; }
       }
-      if (f.depth >= MAX_DEPTH || same) continue;
+      if (f.depth >= MAX_DEPTH || same) {
+        if (write)
+          for (uint32_t k = f.lo; k < f.hi; ++k) leaf_of[perm[k]] = me;
+        continue;
+      }
     }
     first = false;
     // split: stable partition of perm[lo, hi) by the midpoint quadrant
@@ -343,7 +351,7 @@ __global__ void k_count(const double *xs, const double *ys, const uint64_t *keys
   leafd[k] = 33;
   run_end[k] = g1;
   uint32_t deep = deep_group(false, k, g1, 0, keys[k], extent, xs, ys, perm, perm_tmp, frames,
-                             nullptr, nullptr, nullptr, 0, nullptr);
+                             nullptr, nullptr, nullptr, 0, nullptr, nullptr);
   cnt[k] = (uint32_t)(32 - d0 + 1) + deep;
 }
 
@@ -371,7 +379,7 @@ __global__ void k_emit(const double *xs, const double *ys, const uint64_t *keys,
                        const double *extent, uint32_t *perm, uint32_t *perm_tmp, Frame *frames,
                        const uint32_t *base, const uint32_t *run_end, const uint8_t *leafd,
                        Cell *cells, uint32_t *skip, uint32_t *parent, uint32_t *counter,
-                       uint32_t cells_cap, uint32_t *info, uint32_t *status) {
+                       uint32_t cells_cap, uint32_t *info, uint32_t *status, uint32_t *leaf_of) {
   uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   uint32_t m = info[0];
   uint32_t total = info[1];
@@ -422,6 +430,8 @@ __global__ void k_emit(const double *xs, const double *ys, const uint64_t *keys,
       }
     }
     cells[c] = cell;
+    if (leaf)
+      for (uint32_t p = k; p < rend; ++p) leaf_of[perm[p]] = c;
     // descend one level along the key
     uint32_t dg = (uint32_t)(key >> (62 - 2 * d)) & 3u;
     double xm = (x0 + x1) / 2, ym = (y0 + y1) / 2;
@@ -433,7 +443,7 @@ __global__ void k_emit(const double *xs, const double *ys, const uint64_t *keys,
     uint32_t c32 = base[k] + (uint32_t)(32 - d0);
     uint32_t after = rend < m ? base[rend] : total;
     uint32_t emitted = deep_group(true, k, rend, c32, key, extent, xs, ys, perm, perm_tmp, frames,
-                                  cells, parent, skip, after, &info[2]);
+                                  cells, parent, skip, after, &info[2], leaf_of);
     for (uint32_t q = c32 + 1; q <= c32 + emitted; ++q) counter[q] = 0;
   }
 }
@@ -450,7 +460,7 @@ int tree_reserve(TreeDev &t, uint32_t n) {
   cudaFree(t.keys); cudaFree(t.keys_tmp); cudaFree(t.sv); cudaFree(t.sv_tmp); cudaFree(t.perm);
   cudaFree(t.perm_tmp); cudaFree(t.lcpx); cudaFree(t.cnt); cudaFree(t.base); cudaFree(t.run_end);
   cudaFree(t.leafd); cudaFree(t.frames); cudaFree(t.cells); cudaFree(t.skip); cudaFree(t.parent);
-  cudaFree(t.counter); cudaFree(t.scan_part); cudaFree(t.hist);
+  cudaFree(t.counter); cudaFree(t.scan_part); cudaFree(t.hist); cudaFree(t.leaf_of);
   size_t cells = 4 * (size_t)cap + 1024;
   D3_CUDA_OK(cudaMalloc(&t.keys, cap * 8ull));
   D3_CUDA_OK(cudaMalloc(&t.keys_tmp, cap * 8ull));
@@ -468,6 +478,7 @@ int tree_reserve(TreeDev &t, uint32_t n) {
   D3_CUDA_OK(cudaMalloc(&t.skip, cells * 4));
   D3_CUDA_OK(cudaMalloc(&t.parent, cells * 4));
   D3_CUDA_OK(cudaMalloc(&t.counter, cells * 4));
+  D3_CUDA_OK(cudaMalloc(&t.leaf_of, cap * 4ull));
   size_t sp = scan_partial_words(sort_hist_words(cap) > cap + 1 ? sort_hist_words(cap) : cap + 1);
   D3_CUDA_OK(cudaMalloc(&t.scan_part, sp * 4));
   D3_CUDA_OK(cudaMalloc(&t.hist, sort_hist_words(cap) * 4));
@@ -481,6 +492,7 @@ void tree_free(TreeDev &t) {
   cudaFree(t.perm_tmp); cudaFree(t.lcpx); cudaFree(t.cnt); cudaFree(t.base); cudaFree(t.run_end);
   cudaFree(t.leafd); cudaFree(t.frames); cudaFree(t.cells); cudaFree(t.skip); cudaFree(t.parent);
   cudaFree(t.counter); cudaFree(t.scan_part); cudaFree(t.hist); cudaFree(t.info);
+  cudaFree(t.leaf_of);
   cudaFree(t.extent); cudaFree(t.box_part);
   t = TreeDev();
 }
@@ -495,14 +507,14 @@ void tree_build(TreeDev &t, const double *xs, const double *ys, uint32_t n, uint
   D3_LAUNCH(k_keys, B, T, 0, st)(xs, ys, n, t.extent, t.keys, t.sv);
   SortScratch ss{t.keys_tmp, t.sv_tmp, t.hist, t.scan_part};
   radix_sort_u64(t.keys, t.sv, n, 0, 8, true, ss, st);
-  D3_LAUNCH(k_runs, B, T, 0, st)(xs, ys, n, t.keys, t.sv, t.perm, t.lcpx, t.info);
+  D3_LAUNCH(k_runs, B, T, 0, st)(xs, ys, n, t.keys, t.sv, t.perm, t.lcpx, t.info, t.leaf_of);
   D3_LAUNCH(k_count, B, T, 0, st)(xs, ys, t.keys, t.lcpx, t.extent, t.perm, t.perm_tmp, t.frames, t.cnt,
                            t.run_end, t.leafd, t.info, n);
   // cells before each start; the total lands in info[1]
   scan_u32(t.cnt, t.base, n, t.scan_part, t.info + 1, st);
   D3_LAUNCH(k_emit, B, T, 0, st)(xs, ys, t.keys, t.lcpx, t.extent, t.perm, t.perm_tmp, t.frames, t.base,
                           t.run_end, t.leafd, t.cells, t.skip, t.parent, t.counter, t.cells_cap,
-                          t.info, status);
+                          t.info, status, t.leaf_of);
 }
 
 }  // namespace d3

@@ -32,7 +32,8 @@ struct DForce {
   double *d_f[3] = {nullptr, nullptr, nullptr};
   uint32_t *h_src = nullptr, *h_tgt = nullptr, *d_src = nullptr, *d_tgt = nullptr;
   bool dirty = false;       // host mirrors may hold writes not yet uploaded
-  bool plan_dirty = true;   // link plan / adjacency must be rebuilt
+  bool plan_dirty = true;   // exact link plan must be rebuilt
+  bool csr_dirty = true;    // fast link adjacency must be rebuilt
   uint32_t max_index = 0;   // largest source / target + 1 (link)
   double max_f0 = 0;        // largest f0 (collide: the largest radius)
   LinkPlan plan;
@@ -212,6 +213,7 @@ int force_set_count_impl(DSim *s, DForce *f, uint32_t count) {
   f->count = count;
   f->dirty = true;
   f->plan_dirty = true;
+  f->csr_dirty = true;
   return 0;
 }
 
@@ -252,6 +254,7 @@ int upload_force(DSim *s, DForce *f) {
     }
     f->max_index = mx;
     f->plan_dirty = true;
+    f->csr_dirty = true;
   }
   f->dirty = false;
   return 0;
@@ -455,9 +458,9 @@ int run_force(DSim *s, DForce *f, double alpha, bool presummed = false) {
     case D3_LINK:
       if (fast_mode(s, f)) {
         if (f->max_index > s->n) return D3_BAD_ARGUMENT;
-        if (f->plan_dirty || f->csr.n != s->n) {
+        if (f->csr_dirty || f->csr.n != s->n) {
           if (fast_link_build(f->csr, f->h_src, f->h_tgt, f->count, s->n)) return D3_OUT_OF_MEMORY;
-          f->plan_dirty = true;  // the exact plan is rebuilt on its next use
+          f->csr_dirty = false;
         }
         LinkArrays l{f->d_f[0], f->d_f[1], f->d_f[2], f->d_src, f->d_tgt, f->count};
         cudaEvent_t e = phase_begin(s);

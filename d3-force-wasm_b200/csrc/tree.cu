@@ -98,8 +98,13 @@ __device__ void cover(double *e, double x, double y) {
   e[0] = x0; e[1] = y0; e[2] = x1; e[3] = y1;
 }
 
+// The bounding box of the points without a NaN coordinate. Exact mode
+// (square == nullptr): d3's cover of the box into `extent`. Fast mode: the
+// square of tree.zig:287-309 (side = the larger of width and height, 1 when
+// that is not positive) into `extent`, and box x0, y0 and side into square[].
 __global__ void __launch_bounds__(BOX_THREADS) k_box(const double *xs, const double *ys, uint32_t n,
-                                                     BoxPart *parts, double *extent, uint32_t *info) {
+                                                     BoxPart *parts, double *extent, uint32_t *info,
+                                                     double *square) {
   double v[4] = {INFINITY, INFINITY, -INFINITY, -INFINITY};
   uint32_t ix[4] = {NONE, NONE, NONE, NONE};
   uint32_t m = 0;
@@ -139,8 +144,16 @@ __global__ void __launch_bounds__(BOX_THREADS) k_box(const double *xs, const dou
     double e[4] = {NAN, NAN, NAN, NAN};
     info[0] = am;
     if (!(a[0] > a[2] || a[1] > a[3])) {
-      cover(e, a[0], a[1]);
-      cover(e, a[2], a[3]);
+      if (square) {
+        const double w = a[2] - a[0], h = a[3] - a[1];
+        double side = w > h ? w : h;
+        if (!(side > 0)) side = 1;
+        e[0] = a[0]; e[1] = a[1]; e[2] = a[0] + side; e[3] = a[1] + side;
+        square[0] = a[0]; square[1] = a[1]; square[2] = side;
+      } else {
+        cover(e, a[0], a[1]);
+        cover(e, a[2], a[3]);
+      }
     }
     for (int q = 0; q < 4; ++q) extent[q] = e[q];
     info[1] = 0;
@@ -497,11 +510,20 @@ void tree_free(TreeDev &t) {
   t = TreeDev();
 }
 
+void fast_box(TreeDev &t, const double *xs, const double *ys, uint32_t n, double *square,
+              cudaStream_t st) {
+  unsigned bb = blocks_for(n, BOX_THREADS * 4);
+  if (bb > BOX_BLOCKS_MAX) bb = BOX_BLOCKS_MAX;
+  D3_LAUNCH(k_box, bb, BOX_THREADS, 0, st)(xs, ys, n, (BoxPart *)t.box_part, t.extent, t.info,
+                                           square);
+}
+
 void tree_build(TreeDev &t, const double *xs, const double *ys, uint32_t n, uint32_t *status,
                 cudaStream_t st) {
   unsigned bb = blocks_for(n, BOX_THREADS * 4);
   if (bb > BOX_BLOCKS_MAX) bb = BOX_BLOCKS_MAX;
-  D3_LAUNCH(k_box, bb, BOX_THREADS, 0, st)(xs, ys, n, (BoxPart *)t.box_part, t.extent, t.info);
+  D3_LAUNCH(k_box, bb, BOX_THREADS, 0, st)(xs, ys, n, (BoxPart *)t.box_part, t.extent, t.info,
+                                           nullptr);
   if (n == 0) return;
   const unsigned T = 256, B = blocks_for(n, T);
   D3_LAUNCH(k_keys, B, T, 0, st)(xs, ys, n, t.extent, t.keys, t.sv);

@@ -45,4 +45,9 @@ void tree_free(TreeDev &t);
 void tree_build(TreeDev &t, const double *xs, const double *ys, uint32_t n, uint32_t *status,
                 cudaStream_t st);
 
+// Fast mode's square extent (tree.zig:287-309): t.extent, t.info[0] = points
+// without a NaN coordinate, and square[0..2] = box x0, y0, side.
+void fast_box(TreeDev &t, const double *xs, const double *ys, uint32_t n, double *square,
+              cudaStream_t st);
+
 }  // namespace d3

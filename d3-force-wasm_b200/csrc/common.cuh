@@ -29,6 +29,7 @@ enum : uint32_t {
   ST_WAIT_TIMEOUT = 1u << 4,     // a bounded device wait expired
   ST_RNG_NEED = 1u << 5,         // a serial kernel needs more host draws
   ST_COLLIDE_OVERFLOW = 1u << 6, // a guessed set exceeded its capacity
+  ST_CENTER_RECORDS = 1u << 7,   // a center-sum launch failed or its records disagreed
 };
 
 // One quadtree cell, the reference's 88-byte record (tree.zig:46-62):

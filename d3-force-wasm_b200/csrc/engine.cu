@@ -285,6 +285,27 @@ int sync_in_impl(DSim *s) {
   return D3_OK;
 }
 
+// Device-side failures (a bounded wait that ran out, a tree or record buffer
+// too small, a launch that did not happen): the results are not to be trusted.
+constexpr uint32_t ST_FATAL = ST_WAIT_TIMEOUT | ST_DEEP_STACK | ST_CENTER_RECORDS;
+
+// Queues the copy of the status word that take_failure reads after the next
+// host synchronisation.
+void queue_status(DSim *s) {
+  cudaMemcpyAsync(s->h_words + 24, s->d_words, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream);
+}
+
+// After a synchronisation that followed queue_status: D3_WORKER_FAILED (once)
+// if a kernel reported a failure since the last check.
+int take_failure(DSim *s) {
+  const uint32_t w = s->h_words[24];
+  if (!(w & ST_FATAL)) return D3_OK;
+  s->h_words[25] = w & ~ST_FATAL;
+  cudaMemcpy(s->d_words, s->h_words + 25, sizeof(uint32_t), cudaMemcpyHostToDevice);
+  s->h_words[24] = 0;
+  return D3_WORKER_FAILED;
+}
+
 int sync_out_impl(DSim *s) {
   const size_t n = s->n;
   cudaStream_t st = s->stream;
@@ -294,8 +315,9 @@ int sync_out_impl(DSim *s) {
     cudaMemcpyAsync(s->h_vx, s->d_vx, n * 8, cudaMemcpyDeviceToHost, st);
     cudaMemcpyAsync(s->h_vy, s->d_vy, n * 8, cudaMemcpyDeviceToHost, st);
   }
+  queue_status(s);
   if (cudaStreamSynchronize(st) != cudaSuccess) return D3_WORKER_FAILED;
-  return D3_OK;
+  return take_failure(s);
 }
 
 // Words on the device: 0 status (sticky), 1 link flag, 2..4 resume.
@@ -541,7 +563,7 @@ uint32_t sim_create(void) {
   cudaMalloc(&s->d_rng, sizeof(Rng));
   cudaMallocHost(&s->h_rng, sizeof(Rng));
   cudaMalloc(&s->d_words, 16 * sizeof(uint32_t));
-  cudaMallocHost(&s->h_words, 16 * sizeof(uint32_t));
+  cudaMallocHost(&s->h_words, 32 * sizeof(uint32_t));
   cudaMemset(s->d_words, 0, 16 * sizeof(uint32_t));
   Rng r{};
   r.lcg = 1;
@@ -939,11 +961,13 @@ int32_t sim_tick(uint32_t h, uint32_t ticks, double *alpha, double alpha_target,
   }
   cudaEventRecord(s->ev1, s->stream);
   *alpha = a;
-  if (cudaEventSynchronize(s->ev1) != cudaSuccess) return D3_WORKER_FAILED;
+  if (hoist >= 0) cudaStreamWaitEvent(s->stream, s->ev_sumdone, 0);
+  queue_status(s);
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess) return D3_WORKER_FAILED;
   float ms = 0;
   cudaEventElapsedTime(&ms, s->ev0, s->ev1);
   s->last_ms = ms;
-  return D3_OK;
+  return take_failure(s);
 }
 
 int32_t sim_set_profile(uint32_t h, uint32_t on) {
@@ -999,6 +1023,16 @@ double sim_stat(uint32_t h, uint32_t which) {
     case 9: return spec[10];  // inactive nodes whose turn would have written
     case 10: return spec[11]; // turns run from the recorded head list
     case 11: return spec[12]; // turns that traversed the tree
+    case 22: case 23: case 24: case 25: case 26: {
+      // the last center sum: 22 / 23 microseconds of the exact x / y walks;
+      // the x walk's 24 record batches rerun with their entry tests, 25
+      // stretches added one by one, 26 records in all
+      unsigned long long st[8];
+      cudaMemcpy(st, s->scratch.csum_stamps, sizeof st, cudaMemcpyDeviceToHost);
+      if (which >= 24) return (double)st[5 + (which - 24)];
+      const unsigned long long a = st[2], b = st[3 + (which - 22)];
+      return b >= a ? (double)(b - a) * 1e-3 : -1;
+    }
     case 12: case 13: case 14: case 15: case 16: case 17: case 18: {
       // microseconds of the last parallel collide's phases: 12 guess, 13/14
       // attempt 1 rounds / check, 15/16 attempt 2, 17/18 attempt 3

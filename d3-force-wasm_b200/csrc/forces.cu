@@ -11,15 +11,26 @@
 
 namespace d3 {
 
+size_t csum_rec_bytes(uint32_t n);
+size_t csum_count_words(uint32_t n);
+size_t csum_part_words(uint32_t n);
+
 int scratch_reserve(ForceScratch &s, uint32_t n) {
   if (!s.counters) {
     D3_CUDA_OK(cudaMalloc(&s.counters, 16 * sizeof(uint32_t)));
     D3_CUDA_OK(cudaMemset(s.counters, 0, 16 * sizeof(uint32_t)));
     D3_CUDA_OK(cudaMalloc(&s.center, 2 * sizeof(double)));
+    D3_CUDA_OK(cudaMalloc(&s.csum_stamps, 8 * sizeof(unsigned long long)));
+    D3_CUDA_OK(cudaMemset(s.csum_stamps, 0, 8 * sizeof(unsigned long long)));
   }
   if (n <= s.cap && s.cap) return 0;
   uint32_t cap = n < 1024 ? 1024 : n;
   cudaFree(s.draws); cudaFree(s.offsets); cudaFree(s.scan_part);
+  cudaFree(s.csum_recs); cudaFree(s.csum_counts); cudaFree(s.csum_part); cudaFree(s.csum_scan_part);
+  D3_CUDA_OK(cudaMalloc(&s.csum_recs, csum_rec_bytes(cap)));
+  D3_CUDA_OK(cudaMalloc(&s.csum_counts, 2 * csum_count_words(cap) * 4));  // counts, offsets
+  D3_CUDA_OK(cudaMalloc(&s.csum_part, csum_part_words(cap) * 8));
+  D3_CUDA_OK(cudaMalloc(&s.csum_scan_part, scan_partial_words(csum_count_words(cap)) * 4));
   D3_CUDA_OK(cudaMalloc(&s.draws, (cap + 1) * 4ull));
   D3_CUDA_OK(cudaMalloc(&s.offsets, (cap + 1) * 4ull));
   D3_CUDA_OK(cudaMalloc(&s.scan_part, scan_partial_words(cap + 1) * 4));
@@ -29,7 +40,8 @@ int scratch_reserve(ForceScratch &s, uint32_t n) {
 
 void scratch_free(ForceScratch &s) {
   cudaFree(s.draws); cudaFree(s.offsets); cudaFree(s.scan_part); cudaFree(s.counters);
-  cudaFree(s.center);
+  cudaFree(s.center); cudaFree(s.csum_recs); cudaFree(s.csum_counts); cudaFree(s.csum_part);
+  cudaFree(s.csum_scan_part); cudaFree(s.csum_stamps);
   s = ForceScratch();
 }
 
@@ -614,21 +626,28 @@ void collide_serial(TreeDev &t, const NodeArrays &a, const double *radii, double
 // in parallel. While the running sum s stays inside one binade [2^e, 2^e+1)
 // (or its negative) and never meets a rounding tie, fl(s + v) = s + R(v) u
 // with u = 2^(e-52) the ulp there and R(v) = v / u rounded to the nearest
-// integer: the chain is an integer prefix sum. One block (a) sums chunks of
-// the input approximately and scans them to guess each chunk's binade, (b)
-// computes per chunk R's total and the min / max of its prefix in that
-// binade, and (c) one thread per axis walks the chunks with the exact s:
-// where s is in the guessed binade and every partial sum provably stays in
-// it, s jumps by total * u (exact); anywhere else it adds the chunk's values
-// one by one, as the reference does.
-constexpr unsigned CSUM_THREADS = 1024;
-// Serial stretches stream the axis through shared memory with bulk async
-// copies (cp.async.bulk, completion on an mbarrier): CSUM_STAGES stages of
-// CSUM_STAGE values per axis in flight, so the dependent add chain reads
-// shared memory instead of waiting on global loads.
-constexpr unsigned CSUM_STAGE = 2048;
-constexpr unsigned CSUM_STAGES = 4;
-constexpr size_t CSUM_DYN_SMEM = 2ull * CSUM_STAGES * CSUM_STAGE * sizeof(double);
+// integer: the chain is an integer prefix sum. The launches:
+//  part     approximate sums of chunks of values (a warp per chunk);
+//  records  per chunk (a thread each), from the approximate prefix, the chunk
+//           as records {lo, hi, a}, each applied as "s must lie in [lo, hi];
+//           s += a" — run twice, to count and then to write at the scanned
+//           offsets. A stretch record covers a run where the approximate sum
+//           stays in one binade: [lo, hi] holds the exact entry sums for which
+//           every partial sum provably stays there, and a = T, the run's exact
+//           total (s + T is itself exact: both are multiples of u and the
+//           result lies in the binade). A value record adds one value (binade
+//           crossings, ties, short runs) and always applies.
+//  walk     one thread per axis applies the records in order with the exact s,
+//           streaming them into shared memory by bulk async copies
+//           (cp.async.bulk, completion on an mbarrier). A batch runs first
+//           with the entry tests off the dependent chain (one add per record);
+//           if any test failed, the batch reruns from its entry sum, adding a
+//           failed stretch's values one by one from global memory.
+constexpr unsigned CSUM_CHUNK_MIN = 128;   // values per chunk (at least)
+constexpr unsigned CSUM_MAX_CHUNKS = 8192; // chunks per axis (at most)
+constexpr unsigned CSUM_BUFS = 4;          // record copies in flight per axis
+constexpr unsigned CSUM_BATCH = 256;       // records per copy
+constexpr unsigned CSUM_MIN_RUN = 2;       // shorter runs go into value records
 constexpr unsigned long long CSUM_WAIT_NS = 20000000ull;  // 20 ms per copy, far above need
 
 __device__ inline uint32_t smem_addr(const void *p) {
@@ -641,133 +660,29 @@ __device__ inline unsigned long long gtimer_ns() {
   return t;
 }
 
-// Stage k (values [k * CSUM_STAGE, ...)) lives in ring slot k % CSUM_STAGES.
-// Each slot records the stage it holds, whether its copy is still pending and
-// how many copies it has completed (the mbarrier phase to wait on). A slot is
-// refilled only after its pending copy has landed; stages the walk skips are
-// never copied. The copy size is rounded down to 16 bytes (the bulk copy
-// granularity); an odd last value is read from global memory.
-struct StageRing {
-  double *buf;     // CSUM_STAGES * CSUM_STAGE values
-  uint64_t *bar;   // CSUM_STAGES mbarriers
-  const double *src;
-  uint32_t n;
-  uint32_t stage[CSUM_STAGES], phase[CSUM_STAGES];
-  bool pending[CSUM_STAGES];
-  bool timeout;
-
-  __device__ uint32_t copied(uint32_t k) const {
-    const uint32_t lo = k * CSUM_STAGE;
-    return lo < n ? ((min(CSUM_STAGE, n - lo) * 8u) & ~15u) / 8u : 0;
-  }
-
-  // Waits for slot q's pending copy: a non-blocking test polled against a
-  // time budget, so a wait that cannot end reports instead of spinning.
-  __device__ void settle(uint32_t q) {
-    if (!pending[q]) return;
-    const uint32_t a = smem_addr(&bar[q]), parity = phase[q] & 1u;
-    const unsigned long long t0 = gtimer_ns();
-    for (;;) {
-      uint32_t done;
-      asm volatile(
-          "{ .reg .pred p; mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2; "
-          "selp.u32 %0, 1, 0, p; }"
-          : "=r"(done)
-          : "r"(a), "r"(parity)
-          : "memory");
-      if (done) break;
-      if (gtimer_ns() - t0 > CSUM_WAIT_NS) {
-        timeout = true;
-        break;
-      }
-      __nanosleep(64);
-    }
-    pending[q] = false;
-    ++phase[q];
-  }
-
-  __device__ void issue(uint32_t k) {
-    const uint32_t q = k % CSUM_STAGES;
-    if (stage[q] == k) return;  // already there (or in flight)
-    settle(q);
-    stage[q] = k;
-    const uint32_t cnt = copied(k);
-    if (!cnt) return;
-    const uint32_t bytes = cnt * 8u;
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&bar[q])),
-                 "r"(bytes)
-                 : "memory");
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
-            "r"(smem_addr(buf + (size_t)q * CSUM_STAGE)),
-        "l"(src + (size_t)k * CSUM_STAGE), "r"(bytes), "r"(smem_addr(&bar[q]))
-        : "memory");
-    pending[q] = true;
-  }
-
-  __device__ void init(double *b, uint64_t *bars, const double *sp, uint32_t count) {
-    buf = b;
-    bar = bars;
-    src = sp;
-    n = count;
-    timeout = false;
-    for (uint32_t q = 0; q < CSUM_STAGES; ++q) {
-      stage[q] = 0xffffffffu;
-      phase[q] = 0;
-      pending[q] = false;
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar[q])) : "memory");
-    }
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    for (uint32_t k = 0; k < CSUM_STAGES; ++k) issue(k);
-  }
-
-  // Makes stage k resident (and prefetches the next stages); returns its
-  // slot's values, indexed so that [k * CSUM_STAGE + j] is value k * STAGE + j.
-  __device__ const double *resident(uint32_t k) {
-    const uint32_t q = k % CSUM_STAGES;
-    if (stage[q] != k || pending[q]) {
-      issue(k);
-      settle(q);
-      for (uint32_t j = 1; j < CSUM_STAGES; ++j) issue(k + j);
-    }
-    return buf + (size_t)q * CSUM_STAGE - (size_t)k * CSUM_STAGE;
-  }
-
-  // s += v[i] for i in [i0, i1), in order, from the staged copies.
-  __device__ double add_range(double s, uint32_t i0, uint32_t i1) {
-    uint32_t i = i0;
-    while (i < i1) {
-      const uint32_t k = i / CSUM_STAGE;
-      const uint32_t seg = min(i1, (k + 1) * CSUM_STAGE);
-      const uint32_t staged = min(seg, k * CSUM_STAGE + copied(k));
-      if (i < staged) {
-        const double *p = resident(k);
-        for (; i + 8 <= staged; i += 8) {
-          const double v0 = p[i], v1 = p[i + 1], v2 = p[i + 2], v3 = p[i + 3];
-          const double v4 = p[i + 4], v5 = p[i + 5], v6 = p[i + 6], v7 = p[i + 7];
-          s += v0; s += v1; s += v2; s += v3; s += v4; s += v5; s += v6; s += v7;
-        }
-        for (; i < staged; ++i) s += p[i];
-      }
-      for (; i < seg; ++i) s += src[i];  // the odd last value
-    }
-    return s;
-  }
-
-  // Every copy still in flight lands before the block may exit.
-  __device__ void drain() {
-    for (uint32_t q = 0; q < CSUM_STAGES; ++q) settle(q);
-  }
+// A record; meta = (start << 16) | len for a stretch, 0 for a value.
+struct CsumRec {
+  double lo, hi, a;
+  unsigned long long meta;
 };
 
-constexpr unsigned CSUM_MAX_CHUNKS = 512;
-
-struct CsumChunk {
-  long long total, pmin, pmax;
-  int e;       // binade exponent guess; INT_MIN = add serially
-  int neg;
+struct CsumGeom {
+  uint32_t L, nc;  // values per chunk, chunks
 };
+
+__host__ __device__ inline CsumGeom csum_geom(uint32_t n) {
+  CsumGeom g;
+  uint32_t L = CSUM_CHUNK_MIN;
+  if ((n + L - 1) / L > CSUM_MAX_CHUNKS) L = ((n + CSUM_MAX_CHUNKS - 1) / CSUM_MAX_CHUNKS + 31) / 32 * 32;
+  g.L = L;
+  g.nc = (n + L - 1) / L;
+  return g;
+}
+
+// Every record covers at least one value: at most n records per axis.
+size_t csum_rec_bytes(uint32_t n) { return 2ull * ((size_t)n + 1) * sizeof(CsumRec); }
+size_t csum_count_words(uint32_t n) { return 2ull * csum_geom(n).nc + 1; }
+size_t csum_part_words(uint32_t n) { return 2ull * csum_geom(n).nc; }
 
 __device__ inline int binade_of(double s) {
   int e;
@@ -775,116 +690,269 @@ __device__ inline int binade_of(double s) {
   return e - 1;
 }
 
-__global__ void __launch_bounds__(CSUM_THREADS) k_center_sum(const double *x, const double *y,
-                                                             uint32_t n, double *out,
-                                                             uint32_t *status) {
-  extern __shared__ __align__(128) double ring_buf[];
-  __shared__ __align__(8) uint64_t ring_bar[2][CSUM_STAGES];
-  __shared__ CsumChunk ch[2][CSUM_MAX_CHUNKS];
-  __shared__ double approx[2][CSUM_MAX_CHUNKS];
-  __shared__ double warp_tot[2][32];
-  const uint32_t L = n <= 64 * CSUM_MAX_CHUNKS ? 64 : (n + CSUM_MAX_CHUNKS - 1) / CSUM_MAX_CHUNKS;
-  const uint32_t nc = (n + L - 1) / L;
-  const unsigned t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  // (a) approximate chunk sums, then an exclusive scan of them per axis
-  for (int ax = 0; ax < 2; ++ax) {
-    const double *v = ax ? y : x;
-    double a = 0;
-    if (t < nc)
-      for (uint32_t k = t * L, e = min(n, (t + 1) * L); k < e; ++k) a += v[k];
-    double incl = a;
-    for (int o = 1; o < 32; o <<= 1) {
-      double yv = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= (unsigned)o) incl += yv;
-    }
-    if (lane == 31) warp_tot[ax][warp] = incl;
-    __syncthreads();
-    if (warp == 0) {
-      double w = warp_tot[ax][lane], wi = w;
-      for (int o = 1; o < 32; o <<= 1) {
-        double yv = __shfl_up_sync(0xffffffffu, wi, o);
-        if (lane >= (unsigned)o) wi += yv;
-      }
-      warp_tot[ax][lane] = wi - w;
-    }
-    __syncthreads();
-    if (t < nc) approx[ax][t] = warp_tot[ax][warp] + incl - a;  // approximate s at chunk start
-    __syncthreads();
+// part[ax * nc + c]: the sum of chunk c, in any order.
+__global__ void k_csum_part(const double *x, const double *y, uint32_t n, CsumGeom g, double *part) {
+  const uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const unsigned lane = threadIdx.x & 31;
+  if (c >= g.nc) return;
+  const uint32_t k0 = c * g.L, k1 = min(n, k0 + g.L);
+  double ax = 0, ay = 0;
+  for (uint32_t k = k0 + lane; k < k1; k += 32) {
+    ax += x[k];
+    ay += y[k];
   }
-  // (b) integer summaries in the guessed binade
+  for (int o = 16; o > 0; o >>= 1) {
+    ax += __shfl_xor_sync(0xffffffffu, ax, o);
+    ay += __shfl_xor_sync(0xffffffffu, ay, o);
+  }
+  if (lane == 0) {
+    part[c] = ax;
+    part[g.nc + c] = ay;
+  }
+}
+
+// One thread per chunk, both axes. WRITE false: counts[ax nc + c] = the
+// chunk's records; WRITE true: the records at out + offsets[ax nc + c].
+template <bool WRITE>
+__global__ void __launch_bounds__(256) k_csum_records(const double *x, const double *y, uint32_t n,
+                                                      CsumGeom g, const double *part,
+                                                      uint32_t *counts, const uint32_t *offsets,
+                                                      CsumRec *out, uint32_t *status) {
+  __shared__ double sred[2][8];
+  __shared__ double swarp[2][8];
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const uint32_t c0 = blockIdx.x * blockDim.x;
+  // approximate prefix: the chunks before this block, then a block scan
+  double before[2] = {0, 0};
   for (int ax = 0; ax < 2; ++ax) {
-    if (t >= nc) continue;
-    const double *v = ax ? y : x;
-    CsumChunk c;
-    c.e = INT_MIN;
-    c.neg = 0;
-    c.total = c.pmin = c.pmax = 0;
-    const double s0 = approx[ax][t];
-    if (s0 != 0 && isfinite(s0)) {
-      const int e = binade_of(s0);
-      const double scale = ldexp(1.0, 52 - e);  // 1 / u
-      long long p = 0, mn = 0, mx = 0;
-      bool ok = e > -1000 && e < 1000;
-      double run = s0;  // approximate running sum, for the binade guess
-      for (uint32_t k = t * L, end = min(n, (t + 1) * L); k < end && ok; ++k) {
-        const double vv = v[k];
-        const double q = vv * scale;  // exact: a power-of-two scaling in range
-        if (!(fabs(q) < 4.0e18)) { ok = false; break; }
-        const double r = rint(q);
-        if (fabs(q - trunc(q)) == 0.5) { ok = false; break; }  // a tie: parity of s decides
-        p += (long long)r;
-        mn = p < mn ? p : mn;
-        mx = p > mx ? p : mx;
-        run += vv;
-        if (binade_of(run) != e || (run < 0) != (s0 < 0)) ok = false;  // likely crossing
-      }
-      if (ok) {
-        c.e = e;
-        c.neg = s0 < 0;
-        c.total = p;
-        c.pmin = mn;
-        c.pmax = mx;
-      }
-    }
-    ch[ax][t] = c;
+    double a = 0;
+    for (uint32_t k = t; k < c0; k += blockDim.x) a += part[ax * g.nc + k];
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (lane == 0) sred[ax][warp] = a;
   }
   __syncthreads();
-  // (c) the exact walk, one thread per axis
-  if (t != 0 && t != 32) return;
-  const int ax = t ? 1 : 0;
-  const double *v = ax ? y : x;
-  StageRing ring;
-  ring.init(ring_buf + (size_t)ax * CSUM_STAGES * CSUM_STAGE, ring_bar[ax], v, n);
+  for (int ax = 0; ax < 2; ++ax) {
+    double b = 0;
+    for (unsigned w = 0; w < blockDim.x / 32; ++w) b += sred[ax][w];
+    before[ax] = b;
+  }
+  double start[2];
+  for (int ax = 0; ax < 2; ++ax) {
+    const double mine = c < g.nc ? part[ax * g.nc + c] : 0;
+    double incl = mine;
+    for (int o = 1; o < 32; o <<= 1) {
+      const double yv = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= (unsigned)o) incl += yv;
+    }
+    if (lane == 31) swarp[ax][warp] = incl;
+    __syncthreads();
+    double wpre = 0;
+    for (unsigned w = 0; w < warp; ++w) wpre += swarp[ax][w];
+    start[ax] = before[ax] + wpre + incl - mine;
+    __syncthreads();
+  }
+  if (c >= g.nc) return;
   const long long LO = (1ll << 52) + 1, HI = (1ll << 53) - 1;
-  double s = 0;
-  for (uint32_t c = 0; c < nc; ++c) {
-    const CsumChunk k = ch[ax][c];
-    bool fast = false;
-    if (k.e != INT_MIN && s != 0 && isfinite(s) && (s < 0) == (k.neg != 0) && binade_of(s) == k.e) {
-      const double scale = ldexp(1.0, 52 - k.e);
-      long long S = (long long)(fabs(s) * scale);  // exact: s is a multiple of u in [2^52 u, 2^53 u)
-      if (k.neg) {
-        // |s| shrinks by R: partial sums are -(S - P); need S - P within [LO, HI]
-        if (S - k.pmax >= LO && S - k.pmin <= HI) {
-          s = -ldexp((double)(S - k.total), k.e - 52);
-          fast = true;
+  const uint32_t k0 = c * g.L, k1 = min(n, k0 + g.L);
+  for (int ax = 0; ax < 2; ++ax) {
+    const double *v = ax ? y : x;
+    CsumRec *o = nullptr;
+    uint32_t limit = 0;
+    if (WRITE) {
+      o = out + offsets[ax * g.nc + c];
+      limit = counts[ax * g.nc + c];
+    }
+    uint32_t count = 0;
+    auto put = [&](const CsumRec &r) {
+      if (WRITE) {
+        if (count < limit) o[count] = r;
+        else atomicOr(status, ST_CENTER_RECORDS);  // cannot happen: both passes agree
+      }
+      ++count;
+    };
+    double run = start[ax];
+    bool open = false, neg = false;
+    double scale = 0, u = 0, blo = 0, bhi = 0;  // 1 / u, u, binade [blo, bhi)
+    long long tot = 0, pmin = 0, pmax = 0;
+    uint32_t st0 = 0;
+    auto start_at = [&](uint32_t k) {
+      open = false;
+      if (!(run != 0) || !isfinite(run)) return;
+      const int e = binade_of(run);
+      if (!(e > -1000 && e < 1000)) return;
+      neg = run < 0;
+      st0 = k;
+      tot = pmin = pmax = 0;
+      scale = ldexp(1.0, 52 - e);
+      u = ldexp(1.0, e - 52);
+      blo = ldexp(1.0, e);
+      bhi = ldexp(1.0, e + 1);
+      open = true;
+    };
+    // closes the open run [st0, end): a stretch record, or its values
+    auto close = [&](uint32_t end) {
+      if (!open) return;
+      open = false;
+      if (end - st0 >= CSUM_MIN_RUN) {
+        // entry S (|s| = S u) keeps every partial S +- P in [LO, HI]
+        long long a, b;
+        if (!neg) { a = LO - pmin; b = HI - pmax; }
+        else { a = LO + pmax; b = HI + pmin; }
+        if (a <= b && a >= LO && b <= HI) {
+          CsumRec r;
+          if (!neg) { r.lo = (double)a * u; r.hi = (double)b * u; }
+          else { r.lo = -(double)b * u; r.hi = -(double)a * u; }
+          r.a = (double)tot * u;
+          r.meta = ((unsigned long long)st0 << 16) | (unsigned long long)(end - st0);
+          put(r);
+          return;
         }
-      } else if (S + k.pmin >= LO && S + k.pmax <= HI) {
-        s = ldexp((double)(S + k.total), k.e - 52);
-        fast = true;
+      }
+      for (uint32_t k = st0; k < end; ++k) put(CsumRec{-INFINITY, INFINITY, v[k], 0ull});
+    };
+    start_at(k0);
+    for (uint32_t k = k0; k < k1; ++k) {
+      const double vv = v[k];
+      run += vv;
+      if (open) {
+        const double q = vv * scale;  // exact: a power-of-two scaling in range
+        const double ar = fabs(run);
+        if (fabs(q) < 4.0e15 && fabs(q - trunc(q)) != 0.5 && ar >= blo && ar < bhi &&
+            (run < 0) == neg) {
+          tot += (long long)rint(q);
+          pmin = tot < pmin ? tot : pmin;
+          pmax = tot > pmax ? tot : pmax;
+          continue;
+        }
+      }
+      close(k);
+      put(CsumRec{-INFINITY, INFINITY, vv, 0ull});  // element k is added on its own
+      start_at(k + 1);
+    }
+    close(k1);
+    if (!WRITE) counts[ax * g.nc + c] = count;
+  }
+}
+
+__device__ inline bool mbar_test(uint32_t a, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{ .reg .pred p; mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2; "
+      "selp.u32 %0, 1, 0, p; }"
+      : "=r"(done)
+      : "r"(a), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+// Waits on an mbarrier phase with a time budget; false if it ran out. It
+// spins on the test first, then polls against the timer.
+__device__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  const uint32_t a = smem_addr(bar);
+  for (int k = 0; k < 4096; ++k)
+    if (mbar_test(a, parity)) return true;
+  const unsigned long long t0 = gtimer_ns();
+  for (;;) {
+    if (mbar_test(a, parity)) return true;
+    if (gtimer_ns() - t0 > CSUM_WAIT_NS) return false;
+    __nanosleep(32);
+  }
+}
+
+// A buffer is refilled only after this thread has used the values it read
+// from it, so the copy needs no proxy fence before it.
+__device__ void bulk_copy(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+constexpr size_t CSUM_WALK_SMEM = 2ull * CSUM_BUFS * CSUM_BATCH * sizeof(CsumRec);
+
+// One block: thread 0 walks x and thread 32 walks y, over the records
+// [offsets[ax nc], offsets[(ax + 1) nc]).
+// stamps (globaltimer ns): 0-2 walk start, 3 / 4 end of the x / y walk;
+// 5 / 6 / 7 the x walk's batches rerun / stretches added one by one /
+// records in all.
+__global__ void k_csum_walk(const double *x, const double *y, CsumGeom g, const CsumRec *recs,
+                            const uint32_t *offsets, double *out, uint32_t *status,
+                            unsigned long long *stamps) {
+  extern __shared__ __align__(128) unsigned char csum_smem[];
+  __shared__ __align__(8) uint64_t bars[2][CSUM_BUFS];
+  const unsigned t = threadIdx.x;
+  if ((t & 31) != 0) return;
+  const int ax = t >> 5;
+  if (ax > 1) return;
+  if (ax == 0) stamps[0] = stamps[1] = stamps[2] = gtimer_ns();
+  CsumRec *bufs = reinterpret_cast<CsumRec *>(csum_smem) + (size_t)ax * CSUM_BUFS * CSUM_BATCH;
+  uint64_t *bar = bars[ax];
+  for (uint32_t q = 0; q < CSUM_BUFS; ++q)
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar[q])) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  const double *v = ax ? y : x;
+  const uint32_t r0 = offsets[ax * g.nc], r1 = offsets[(ax + 1) * g.nc];
+  const uint32_t nrec = r1 - r0, nb = (nrec + CSUM_BATCH - 1) / CSUM_BATCH;
+  const CsumRec *rec = recs + r0;
+  auto issue = [&](uint32_t b) {
+    const uint32_t m = min(CSUM_BATCH, nrec - b * CSUM_BATCH);
+    bulk_copy(bufs + (size_t)(b % CSUM_BUFS) * CSUM_BATCH, rec + (size_t)b * CSUM_BATCH,
+              m * (uint32_t)sizeof(CsumRec), &bar[b % CSUM_BUFS]);
+  };
+  for (uint32_t b = 0; b < CSUM_BUFS && b < nb; ++b) issue(b);
+  bool ok = true;
+  double s = 0;
+  uint32_t reruns = 0, failed = 0;
+  uint32_t b = 0;
+  for (; b < nb; ++b) {
+    if (!mbar_wait(&bar[b % CSUM_BUFS], (b / CSUM_BUFS) & 1u)) {
+      ok = false;
+      break;
+    }
+    const CsumRec *r = bufs + (size_t)(b % CSUM_BUFS) * CSUM_BATCH;
+    const uint32_t m = min(CSUM_BATCH, nrec - b * CSUM_BATCH);
+    // the tests do not feed the chain: one dependent add per record
+    const double s_in = s;
+    bool bad = false;
+#pragma unroll 4
+    for (uint32_t k = 0; k < m; ++k) {
+      const double lo = r[k].lo, hi = r[k].hi, a = r[k].a;
+      bad |= !(s >= lo && s <= hi);
+      s += a;
+    }
+    if (bad) {
+      // some entry test failed (or s is not finite): rerun with the tests
+      ++reruns;
+      s = s_in;
+      for (uint32_t k = 0; k < m; ++k) {
+        const CsumRec d = r[k];
+        if (d.meta == 0 || (s >= d.lo && s <= d.hi)) {
+          s += d.a;
+        } else {
+          const uint32_t i0 = (uint32_t)(d.meta >> 16), len = (uint32_t)(d.meta & 0xffffu);
+          for (uint32_t i = i0; i < i0 + len; ++i) s += v[i];
+          ++failed;
+        }
       }
     }
-    if (!fast) {
-      // consecutive serial chunks run as one range
-      uint32_t c1 = c + 1;
-      while (c1 < nc && ch[ax][c1].e == INT_MIN) ++c1;
-      s = ring.add_range(s, c * L, min(n, c1 * L));
-      c = c1 - 1;
-    }
+    if (b + CSUM_BUFS < nb) issue(b + CSUM_BUFS);
   }
-  ring.drain();  // no copy may still target shared memory when the block exits
-  if (ring.timeout) atomicOr(status, ST_WAIT_TIMEOUT);
+  // every copy in flight lands before the block exits
+  for (uint32_t q = b; q < nb && q < b + CSUM_BUFS; ++q)
+    mbar_wait(&bar[q % CSUM_BUFS], (q / CSUM_BUFS) & 1u);
+  if (!ok) atomicOr(status, ST_WAIT_TIMEOUT);
   out[ax] = s;
+  stamps[3 + ax] = gtimer_ns();
+  if (ax == 0) {
+    stamps[5] = reruns;
+    stamps[6] = failed;
+    stamps[7] = nrec;
+  }
 }
 
 __global__ void k_center_apply(double *x, double *y, uint32_t n, const double *sums, double cx,
@@ -898,15 +966,33 @@ __global__ void k_center_apply(double *x, double *y, uint32_t n, const double *s
   y[i] -= sy;
 }
 
+__global__ void k_set_status(uint32_t *status, uint32_t bits) { atomicOr(status, bits); }
+
+void set_status(uint32_t *status, uint32_t bits, cudaStream_t st) {
+  D3_LAUNCH(k_set_status, 1, 1, 0, st)(status, bits);
+}
+
 void center_sum(const NodeArrays &a, ForceScratch &s, uint32_t *status, cudaStream_t st) {
   if (a.n == 0) return;
   static bool attr = [] {
-    cudaFuncSetAttribute(k_center_sum, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)CSUM_DYN_SMEM);
-    return true;
+    return cudaFuncSetAttribute(k_csum_walk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)CSUM_WALK_SMEM) == cudaSuccess;
   }();
-  (void)attr;
-  D3_LAUNCH(k_center_sum, 1, CSUM_THREADS, CSUM_DYN_SMEM, st)(a.x, a.y, a.n, s.center, status);
+  const CsumGeom g = csum_geom(a.n);
+  CsumRec *recs = static_cast<CsumRec *>(s.csum_recs);
+  uint32_t *counts = s.csum_counts, *offsets = s.csum_counts + 2 * g.nc + 1;
+  const unsigned cb = blocks_for(g.nc, 256);
+  D3_LAUNCH(k_csum_part, blocks_for((size_t)g.nc * 32, 256), 256, 0, st)(a.x, a.y, a.n, g, s.csum_part);
+  D3_LAUNCH(k_csum_records<false>, cb, 256, 0, st)(a.x, a.y, a.n, g, s.csum_part, counts, nullptr,
+                                                   nullptr, status);
+  // offsets of both axes' records; offsets[2 nc] = the total
+  scan_u32(counts, offsets, 2 * g.nc, s.csum_scan_part, offsets + 2 * g.nc, st);
+  D3_LAUNCH(k_csum_records<true>, cb, 256, 0, st)(a.x, a.y, a.n, g, s.csum_part, counts, offsets,
+                                                  recs, status);
+  D3_LAUNCH(k_csum_walk, 1, 64, CSUM_WALK_SMEM, st)(a.x, a.y, g, recs, offsets, s.center, status,
+                                                    s.csum_stamps);
+  // a launch that did not happen leaves stale sums: report it as a failure
+  if (!attr || cudaGetLastError() != cudaSuccess) set_status(status, ST_CENTER_RECORDS, st);
 }
 
 void center_apply(const NodeArrays &a, double cx, double cy, double strength, ForceScratch &s,

@@ -24,6 +24,11 @@ struct ForceScratch {
   uint32_t *scan_part = nullptr;
   uint32_t *counters = nullptr; // 0 total draws, 1 flagged, 2.. misc
   double *center = nullptr;     // 2 sums
+  void *csum_recs = nullptr;    // the center sum's records, all chunks in order
+  uint32_t *csum_counts = nullptr;  // ... record counts per chunk, then their offsets
+  double *csum_part = nullptr;  // ... approximate chunk sums
+  uint32_t *csum_scan_part = nullptr;  // ... the offsets scan's partials
+  unsigned long long *csum_stamps = nullptr;  // the last center sum's timestamps and counts
 };
 
 int scratch_reserve(ForceScratch &s, uint32_t n);

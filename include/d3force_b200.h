@@ -25,7 +25,10 @@
 extern "C" {
 #endif
 
-/* Status codes: root.zig:16-25 (`Status`). */
+/* Status codes: root.zig:16-25 (`Status`). A device-side failure (a bounded
+ * wait that ran out, a buffer found too small) is reported as
+ * D3_WORKER_FAILED by the next call that synchronises with the device
+ * (sim_sync_out, sim_tick, or any call in D3_SYNC_PER_CALL mode). */
 enum {
   D3_OK = 0,
   D3_GROWN = 1,
@@ -145,6 +148,10 @@ double sim_last_tick_ms(uint32_t h);
  * far (all simulations); 7, 8 turns of the last parallel collide that met an
  * unguessed head / overlap, 9 inactive nodes whose turn would have written,
  * 10 turns run from the recorded head list, 11 turns that traversed the tree;
+ * 12-18 microseconds of the last parallel collide's phases (guess, then
+ * rounds / check per attempt); the last center sum's 22 / 23 microseconds of
+ * the exact x / y walks, 24 its x walk's record batches rerun with their
+ * entry tests, 25 stretches added one by one, 26 records in all;
  * 100 + k milliseconds and 200 + k count of phase k
  * since sim_set_profile(h, 1): 0 many-body tree, 1 many-body accumulation,
  * 2 many-body traversal, 3 exact link, 4 collide tree and radii, 5 collide

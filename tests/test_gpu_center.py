@@ -20,7 +20,8 @@ def _center_only(xs, ys):
     return setup
 
 
-@pytest.mark.parametrize("case", ["walk", "offset", "ties", "tiny_huge", "zeros_nan", "large"])
+@pytest.mark.parametrize("case", ["walk", "offset", "ties", "tiny_huge", "zeros_nan", "large",
+                                  "centered_1m"])
 def test_gpu_center_sum_bitwise(ocore, gcore, case):
     rng = np.random.default_rng(5)
     n = 50000
@@ -40,8 +41,13 @@ def test_gpu_center_sum_bitwise(ocore, gcore, case):
         xs = np.where(rng.random(n) < 0.5, -0.0, 0.0)
         ys = rng.normal(0, 1, n)
         ys[n // 2] = np.nan
-    else:
+    elif case == "large":
         n = 300000
         xs = rng.normal(0, 1e4, n)
         ys = rng.uniform(-1, 1, n) * 2.0 ** 40
+    else:  # a laid-out graph after centring: the running sum wanders through zero
+        n = 1000000
+        xs = rng.uniform(-5000, 5000, n)
+        xs -= xs.mean()
+        ys = rng.uniform(0, 1e4, n)
     P.run_pair(_center_only(list(xs), list(ys)), ocore, gcore, 3)

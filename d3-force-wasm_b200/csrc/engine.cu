@@ -6,6 +6,7 @@
 // CUDA stream per simulation; the force kernels are enqueued on it and the
 // host synchronises only where the ABI hands data back (sync_out, pointers
 // after a tree build, the host random callback).
+#include <chrono>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -82,6 +83,7 @@ struct DSim {
   uint32_t h_len = 0, h_root = NONE, h_m = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_ms = 0;
+  double last_enqueue_ms = 0;  // host time sim_tick spent queueing work (before its final wait)
   // phase timers (sim_set_profile): pending event pairs per phase, totals
   bool profile = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -931,6 +933,7 @@ int32_t sim_tick(uint32_t h, uint32_t ticks, double *alpha, double alpha_target,
       hoist = (int)i;
       break;
     }
+  const auto host0 = std::chrono::steady_clock::now();
   cudaEventRecord(s->ev0, s->stream);
   double a = *alpha;
   for (uint32_t k = 0; k < ticks; ++k) {
@@ -960,6 +963,8 @@ int32_t sim_tick(uint32_t h, uint32_t ticks, double *alpha, double alpha_target,
     phase_end(s, PH_INTEGRATE, e);
   }
   cudaEventRecord(s->ev1, s->stream);
+  s->last_enqueue_ms =
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - host0).count();
   *alpha = a;
   if (hoist >= 0) cudaStreamWaitEvent(s->stream, s->ev_sumdone, 0);
   queue_status(s);
@@ -1023,6 +1028,15 @@ double sim_stat(uint32_t h, uint32_t which) {
     case 9: return spec[10];  // inactive nodes whose turn would have written
     case 10: return spec[11]; // turns run from the recorded head list
     case 11: return spec[12]; // turns that traversed the tree
+    case 27: return s->last_enqueue_ms;
+    case 30: case 31: case 32: case 33: case 34: case 35: case 36: {
+      // microseconds of the last tree build's phases: 30 box, 31 keys, 32
+      // sort, 33 runs, 34 cell counts, 35 their scan, 36 the cells (block 0)
+      unsigned long long st[8];
+      cudaMemcpy(st, s->tree.stamps, sizeof st, cudaMemcpyDeviceToHost);
+      const int k = (int)which - 30;
+      return st[k + 1] >= st[k] ? (double)(st[k + 1] - st[k]) * 1e-3 : -1;
+    }
     case 22: case 23: case 24: case 25: case 26: {
       // the last center sum: 22 / 23 microseconds of the exact x / y walks;
       // the x walk's 24 record batches rerun with their entry tests, 25

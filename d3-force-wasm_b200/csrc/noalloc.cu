@@ -23,7 +23,8 @@ constexpr uint32_t NA_CAP = D3_NOALLOC_MAX_NODES;
 constexpr uint32_t NA_CELLS = 4 * NA_CAP + 1024;  // as tree_reserve
 constexpr size_t NA_ALIGN = 256;
 constexpr size_t na_round(size_t b) { return (b + NA_ALIGN - 1) / NA_ALIGN * NA_ALIGN; }
-constexpr size_t na_hist_words = 256 * ((NA_CAP + SORT_TILE - 1) / SORT_TILE) + 1;
+// the tree build's per-tile digit counts, digit totals and grid partials
+constexpr size_t na_hist_words = 2 * ((NA_CAP + 255) / 256 + 1) * 256 + 256 + TREE_GRID_MAX;
 constexpr size_t na_scan_words(size_t n) { return (n + SCAN_BLOCK * 4 - 1) / (SCAN_BLOCK * 4) + 2; }
 constexpr size_t NA_BOX_BYTES = 592 * 64;  // per-block bounding-box partials of k_box
 
@@ -47,6 +48,7 @@ constexpr size_t NA_SIZES[] = {
     4 * na_scan_words(NA_CAP + 1),                // force scan
     16 * sizeof(uint32_t), 2 * sizeof(double),    // counters, center
     sizeof(Rng), 16 * sizeof(uint32_t),           // rng, status words
+    8 * sizeof(unsigned long long),               // tree build phase stamps
 };
 
 constexpr size_t na_total() {
@@ -154,6 +156,7 @@ extern "C" int32_t d3_many_body_exact_noalloc(const double *x, const double *y, 
   s.center = c.take<double>();
   Rng *rng = c.take<Rng>();
   uint32_t *words = c.take<uint32_t>();  // 0 status, 8.. results
+  t.stamps = c.take<unsigned long long>();
 
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   // The array keeps the previous call's contents: clear what must start at 0.

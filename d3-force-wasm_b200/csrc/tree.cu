@@ -13,9 +13,20 @@
 //      per-point cell counts. This is d3's `visit` preorder (children 0..3).
 //   5. below the 32 key levels (distinct points in one key) the reference's
 //      stable midpoint partition runs serially per group (tree.zig:449-479).
+#include <cooperative_groups.h>
+
 #include "tree.cuh"
 
+namespace cg = cooperative_groups;
+
 namespace d3 {
+
+// Loads of data that other blocks of the same launch wrote (through L2: L1 is
+// not coherent across SMs).
+__device__ inline uint64_t ldc(const uint64_t *p) { return __ldcg((const unsigned long long *)p); }
+__device__ inline uint32_t ldc(const uint32_t *p) { return __ldcg(p); }
+__device__ inline int8_t ldc(const int8_t *p) { return (int8_t)__ldcg((const signed char *)p); }
+__device__ inline uint8_t ldc(const uint8_t *p) { return (uint8_t)__ldcg((const unsigned char *)p); }
 
 struct BoxPart {
   double v[4];   // min x, min y, max x, max y
@@ -23,6 +34,8 @@ struct BoxPart {
   uint32_t m;    // points without a NaN coordinate
   uint32_t pad;
 };
+
+static_assert(sizeof(BoxPart) <= 64, "box partials are reserved at 64 bytes each");
 
 static constexpr unsigned BOX_THREADS = 256;
 static constexpr unsigned BOX_BLOCKS_MAX = 592;  // 4 per SM
@@ -165,10 +178,8 @@ __global__ void __launch_bounds__(BOX_THREADS) k_box(const double *xs, const dou
 
 // tree.zig:252-284: 32-level key by d3's midpoint test; the sort value carries
 // bit 31 for points with a NaN coordinate (partitioned last).
-__global__ void k_keys(const double *xs, const double *ys, uint32_t n, const double *extent,
-                       uint64_t *keys, uint32_t *sv) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+__device__ void keys_at(uint32_t i, const double *xs, const double *ys, const double *extent,
+                        uint64_t *keys, uint32_t *sv) {
   double x = xs[i], y = ys[i];
   if (x != x || y != y) {
     keys[i] = 0;
@@ -194,14 +205,11 @@ __global__ void k_keys(const double *xs, const double *ys, uint32_t n, const dou
 // perm (sorted node indices, then the NaN nodes in index order), and per
 // sorted point the levels its key shares with the previous one: -1 for the
 // first, 64 for the same position (no boundary), else min(32, clz / 2).
-__global__ void k_runs(const double *xs, const double *ys, uint32_t n, const uint64_t *keys,
-                       const uint32_t *sv, uint32_t *perm, int8_t *lcpx, const uint32_t *info,
-                       uint32_t *leaf_of) {
-  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
-  uint32_t p = sv[k] & 0x7fffffffu;
+__device__ void runs_at(uint32_t k, uint32_t m, const double *xs, const double *ys,
+                        const uint64_t *keys, const uint32_t *sv, uint32_t *perm, int8_t *lcpx,
+                        uint32_t *leaf_of) {
+  uint32_t p = ldc(&sv[k]) & 0x7fffffffu;
   perm[k] = p;
-  uint32_t m = info[0];
   if (k >= m) {
     leaf_of[p] = NONE;
     return;
@@ -210,18 +218,18 @@ __global__ void k_runs(const double *xs, const double *ys, uint32_t n, const uin
     lcpx[0] = -1;
     return;
   }
-  uint32_t q = sv[k - 1] & 0x7fffffffu;
+  uint32_t q = ldc(&sv[k - 1]) & 0x7fffffffu;
   if (xs[p] == xs[q] && ys[p] == ys[q]) {
     lcpx[k] = 64;
     return;
   }
-  uint64_t d = keys[k] ^ keys[k - 1];
+  uint64_t d = ldc(&keys[k]) ^ ldc(&keys[k - 1]);
   int l = d ? (__clzll(d) >> 1) : 32;
   lcpx[k] = (int8_t)(l < 32 ? l : 32);
 }
 
 __device__ inline bool is_start(const int8_t *lcpx, uint32_t k) {
-  int l = lcpx[k];
+  int l = ldc(&lcpx[k]);
   return k == 0 || l < 32;  // -1 only at k = 0; 32 and 64 are not starts
 }
 
@@ -281,14 +289,14 @@ __device__ uint32_t deep_group(bool write, uint32_t lo, uint32_t hi, uint32_t c3
       f.parent = me;
       // allSame by position (tree.zig:437-444); the depth guard of tree.zig:33
       bool same = true;
-      uint32_t p0 = perm[f.lo];
+      uint32_t p0 = ldc(&perm[f.lo]);
       for (uint32_t k = f.lo + 1; k < f.hi; ++k) {
-        uint32_t p = perm[k];
+        uint32_t p = ldc(&perm[k]);
         if (xs[p] != xs[p0] || ys[p] != ys[p0]) { same = false; break; }
       }
       if (f.depth >= MAX_DEPTH || same) {
         if (write)
-          for (uint32_t k = f.lo; k < f.hi; ++k) leaf_of[perm[k]] = me;
+          for (uint32_t k = f.lo; k < f.hi; ++k) leaf_of[ldc(&perm[k])] = me;
         continue;
       }
     }
@@ -297,17 +305,17 @@ __device__ uint32_t deep_group(bool write, uint32_t lo, uint32_t hi, uint32_t c3
     double xm = (f.x0 + f.x1) / 2, ym = (f.y0 + f.y1) / 2;
     uint32_t counts[4] = {0, 0, 0, 0}, off[4], b[5];
     for (uint32_t k = f.lo; k < f.hi; ++k) {
-      uint32_t p = perm[k];
+      uint32_t p = ldc(&perm[k]);
       counts[quadrant(xs[p], ys[p], xm, ym)]++;
     }
     uint32_t sum = f.lo;
     for (int q = 0; q < 4; ++q) { off[q] = sum; b[q] = sum; sum += counts[q]; }
     b[4] = f.hi;
     for (uint32_t k = f.lo; k < f.hi; ++k) {
-      uint32_t p = perm[k];
+      uint32_t p = ldc(&perm[k]);
       perm_tmp[off[quadrant(xs[p], ys[p], xm, ym)]++] = p;
     }
-    for (uint32_t k = f.lo; k < f.hi; ++k) perm[k] = perm_tmp[k];
+    for (uint32_t k = f.lo; k < f.hi; ++k) perm[k] = ldc(&perm_tmp[k]);
     for (int q = 3; q >= 0; --q) {
       if (b[q] == b[q + 1]) continue;
       if (sp >= cap) return emitted;  // cannot happen: pending frames hold disjoint points
@@ -334,24 +342,22 @@ __device__ uint32_t deep_group(bool write, uint32_t lo, uint32_t hi, uint32_t c3
 
 // Cells starting at each sorted point: per start k, depths d0..leaf, plus the
 // cells below depth 32 of a deep group.
-__global__ void k_count(const double *xs, const double *ys, const uint64_t *keys, const int8_t *lcpx,
-                        const double *extent, uint32_t *perm, uint32_t *perm_tmp, Frame *frames,
-                        uint32_t *cnt, uint32_t *run_end, uint8_t *leafd, const uint32_t *info,
-                        uint32_t n) {
-  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  uint32_t m = info[0];
+__device__ void count_at(uint32_t k, uint32_t m, const double *xs, const double *ys,
+                         const uint64_t *keys, const int8_t *lcpx, const double *extent,
+                         uint32_t *perm, uint32_t *perm_tmp, Frame *frames, uint32_t *cnt,
+                         uint32_t *run_end, uint8_t *leafd) {
   if (k >= m) {
-    if (k < n) cnt[k] = 0;  // points with a NaN coordinate start no cell
+    cnt[k] = 0;  // points with a NaN coordinate start no cell
     return;
   }
   if (!is_start(lcpx, k)) {
     cnt[k] = 0;
     return;
   }
-  int d0 = k == 0 ? 0 : lcpx[k] + 1;
+  int d0 = k == 0 ? 0 : ldc(&lcpx[k]) + 1;
   uint32_t j = k + 1;
-  while (j < m && lcpx[j] == 64) ++j;
-  int lr = j < m ? lcpx[j] : -1;
+  while (j < m && ldc(&lcpx[j]) == 64) ++j;
+  int lr = j < m ? ldc(&lcpx[j]) : -1;
   if (lr < 32) {
     int ld = lr + 1 > d0 ? lr + 1 : d0;
     leafd[k] = (uint8_t)ld;
@@ -360,15 +366,17 @@ __global__ void k_count(const double *xs, const double *ys, const uint64_t *keys
     return;
   }
   uint32_t g1 = j;
-  while (g1 < m && lcpx[g1] >= 32) ++g1;
+  while (g1 < m && ldc(&lcpx[g1]) >= 32) ++g1;
   leafd[k] = 33;
   run_end[k] = g1;
-  uint32_t deep = deep_group(false, k, g1, 0, keys[k], extent, xs, ys, perm, perm_tmp, frames,
+  uint32_t deep = deep_group(false, k, g1, 0, ldc(&keys[k]), extent, xs, ys, perm, perm_tmp, frames,
                              nullptr, nullptr, nullptr, 0, nullptr, nullptr);
   cnt[k] = (uint32_t)(32 - d0 + 1) + deep;
 }
 
-// First index in [lo, hi) with keys[j] >= t (keys sorted).
+// First index in [lo, hi) with keys[j] >= t (keys sorted). Plain loads: the
+// keys are final by the cells phase, and the grid barrier before it orders
+// their writes before these reads (these searches hit L1 on their upper steps).
 __device__ inline uint32_t lower_bound(const uint64_t *keys, uint32_t lo, uint32_t hi, uint64_t t) {
   while (lo < hi) {
     uint32_t mid = lo + ((hi - lo) >> 1);
@@ -388,29 +396,21 @@ __device__ inline uint32_t prefix_end(const uint64_t *keys, uint32_t lo, uint32_
   return lo;
 }
 
-__global__ void k_emit(const double *xs, const double *ys, const uint64_t *keys, const int8_t *lcpx,
-                       const double *extent, uint32_t *perm, uint32_t *perm_tmp, Frame *frames,
-                       const uint32_t *base, const uint32_t *run_end, const uint8_t *leafd,
-                       Cell *cells, uint32_t *skip, uint32_t *parent, uint32_t *counter,
-                       uint32_t cells_cap, uint32_t *info, uint32_t *status, uint32_t *leaf_of) {
-  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  uint32_t m = info[0];
-  uint32_t total = info[1];
-  if (k >= m) return;
-  if (total > cells_cap) {
-    if (k == 0) { info[5] = 1; atomicOr(status, ST_DEEP_STACK); }
-    return;
-  }
+__device__ void emit_at(uint32_t k, uint32_t m, uint32_t total, const double *xs, const double *ys,
+                        const uint64_t *keys, const int8_t *lcpx, const double *extent,
+                        uint32_t *perm, uint32_t *perm_tmp, Frame *frames, const uint32_t *base,
+                        const uint32_t *run_end, const uint8_t *leafd, Cell *cells, uint32_t *skip,
+                        uint32_t *parent, uint32_t *counter, uint32_t *info, uint32_t *leaf_of) {
   if (!is_start(lcpx, k)) return;
-  const uint64_t key = keys[k];
-  const int d0 = k == 0 ? 0 : lcpx[k] + 1;
-  const int ld = leafd[k];
+  const uint64_t key = ldc(&keys[k]);
+  const int d0 = k == 0 ? 0 : ldc(&lcpx[k]) + 1;
+  const int ld = ldc(&leafd[k]);
   const bool deep = ld == 33;
   const int dlast = deep ? 32 : ld;
-  const uint32_t rend = run_end[k];
+  const uint32_t rend = ldc(&run_end[k]);
   double x0, y0, x1, y1;
   path_bounds(extent, key, d0, x0, y0, x1, y1);
-  uint32_t c = base[k];
+  uint32_t c = ldc(&base[k]);
   if (k == 0) parent[0] = NONE;
   for (int d = d0; d <= dlast; ++d, ++c) {
     const bool leaf = !deep && d == ld;
@@ -424,7 +424,7 @@ __global__ void k_emit(const double *xs, const double *ys, const uint64_t *keys,
     cell.count = end - k;
     cell.x0 = x0; cell.y0 = y0; cell.x1 = x1; cell.y1 = y1;
     cell.x = cell.y = cell.value = cell.r = 0;
-    skip[c] = end < m ? base[end] : total;
+    skip[c] = end < m ? ldc(&base[end]) : total;
     counter[c] = 0;
     if (!leaf && d < 32) {
       const uint64_t top = d == 0 ? 0 : (key >> (64 - 2 * d)) << (64 - 2 * d);
@@ -436,15 +436,15 @@ __global__ void k_emit(const double *xs, const double *ys, const uint64_t *keys,
       for (int q = 0; q < 4; ++q) {
         if (b[q] == b[q + 1]) continue;
         uint32_t a = b[q];
-        int cd0 = a == k ? d0 : lcpx[a] + 1;
-        uint32_t ch = base[a] + (uint32_t)(d + 1 - cd0);
+        int cd0 = a == k ? d0 : ldc(&lcpx[a]) + 1;
+        uint32_t ch = ldc(&base[a]) + (uint32_t)(d + 1 - cd0);
         cell.child[q] = ch;
         parent[ch] = c;
       }
     }
     cells[c] = cell;
     if (leaf)
-      for (uint32_t p = k; p < rend; ++p) leaf_of[perm[p]] = c;
+      for (uint32_t p = k; p < rend; ++p) leaf_of[ldc(&perm[p])] = c;
     // descend one level along the key
     uint32_t dg = (uint32_t)(key >> (62 - 2 * d)) & 3u;
     double xm = (x0 + x1) / 2, ym = (y0 + y1) / 2;
@@ -453,12 +453,306 @@ __global__ void k_emit(const double *xs, const double *ys, const uint64_t *keys,
   }
   atomicMax(&info[2], (uint32_t)dlast);
   if (deep) {
-    uint32_t c32 = base[k] + (uint32_t)(32 - d0);
-    uint32_t after = rend < m ? base[rend] : total;
+    uint32_t c32 = ldc(&base[k]) + (uint32_t)(32 - d0);
+    uint32_t after = rend < m ? ldc(&base[rend]) : total;
     uint32_t emitted = deep_group(true, k, rend, c32, key, extent, xs, ys, perm, perm_tmp, frames,
                                   cells, parent, skip, after, &info[2], leaf_of);
     for (uint32_t q = c32 + 1; q <= c32 + emitted; ++q) counter[q] = 0;
   }
+}
+
+// ---- the build as one cooperative launch --------------------------------------
+
+constexpr unsigned TB_THREADS = 256;
+constexpr unsigned TB_TILE = 256;  // keys per sort tile (one per thread)
+
+struct TreeBuildArgs {
+  const double *xs, *ys;
+  uint32_t n, tiles, cells_cap;
+  uint64_t *keys, *keys_tmp;
+  uint32_t *sv, *sv_tmp, *perm, *perm_tmp;
+  int8_t *lcpx;
+  uint32_t *cnt, *base, *run_end;
+  uint8_t *leafd;
+  Frame *frames;
+  Cell *cells;
+  uint32_t *skip, *parent, *counter, *leaf_of;
+  BoxPart *parts;
+  uint32_t *hist, *hist2;  // tiles * 256 per-tile digit counts, two passes' worth
+  uint32_t *dtot, *bsum;   // 256 digit totals, grid partials
+  double *extent;
+  uint32_t *info, *status;
+  unsigned long long *stamps;  // globaltimer at the phase ends (block 0)
+};
+
+__device__ inline void tb_stamp(const TreeBuildArgs &a, int k) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    a.stamps[k] = t;
+  }
+}
+
+__device__ inline uint32_t block_sum(uint32_t v, uint32_t *sw) {
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if (lane == 0) sw[warp] = v;
+  __syncthreads();
+  uint32_t t = 0;
+  for (unsigned w = 0; w < blockDim.x / 32; ++w) t += sw[w];
+  return t;
+}
+
+// Block-wide exclusive scan of one value per thread; the total to *tot.
+__device__ inline uint32_t block_excl(uint32_t v, uint32_t *sw, uint32_t &tot) {
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  uint32_t incl = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= (unsigned)o) incl += y;
+  }
+  __syncthreads();
+  if (lane == 31) sw[warp] = incl;
+  __syncthreads();
+  uint32_t pre = 0;
+  tot = 0;
+  for (unsigned w = 0; w < nw; ++w) {
+    if (w < warp) pre += sw[w];
+    tot += sw[w];
+  }
+  return pre + incl - v;
+}
+
+// out[0..len) = exclusive scan of in[0..len) over the whole grid; returns the
+// total. One grid barrier inside; the caller syncs before reading out.
+__device__ uint32_t grid_excl_scan(cg::grid_group &g, const uint32_t *in, uint32_t *out,
+                                   uint32_t len, uint32_t *bsum) {
+  __shared__ uint32_t sw[32];
+  const uint32_t nb = gridDim.x, b = blockIdx.x, t = threadIdx.x;
+  const uint32_t seg = (len + nb - 1) / nb;
+  const uint32_t s0 = min(len, b * seg), s1 = min(len, s0 + seg);
+  uint32_t acc = 0;
+  for (uint32_t i = s0 + t; i < s1; i += blockDim.x) acc += ldc(&in[i]);
+  acc = block_sum(acc, sw);
+  if (t == 0) bsum[b] = acc;
+  g.sync();
+  uint32_t off = 0, tot = 0;
+  for (uint32_t k = t; k < nb; k += blockDim.x) {
+    const uint32_t x = ldc(&bsum[k]);
+    if (k < b) off += x;
+    tot += x;
+  }
+  off = block_sum(off, sw);
+  tot = block_sum(tot, sw);
+  uint32_t run = off;
+  for (uint32_t base = s0; base < s1; base += blockDim.x) {
+    const uint32_t i = base + t;
+    const uint32_t x = i < s1 ? ldc(&in[i]) : 0;
+    uint32_t tile;
+    const uint32_t ex = block_excl(x, sw, tile);
+    if (i < s1) out[i] = run + ex;
+    run += tile;
+  }
+  return tot;
+}
+
+template <bool PART>
+__device__ inline uint32_t tb_digit(uint64_t k, uint32_t v, int shift) {
+  if (PART) return v >> 31;
+  return (uint32_t)(k >> shift) & 255u;
+}
+
+// The digit of the pass after `shift` (next < 0: the NaN partition).
+__device__ inline uint32_t tb_next_digit(uint64_t k, uint32_t v, int next) {
+  return next < 0 ? v >> 31 : (uint32_t)(k >> next) & 255u;
+}
+
+// One stable LSD pass from (ik, iv) to (ok, ov), given `cur`: per tile
+// (TB_TILE keys) the counts of each digit, tile-major. Phase 1: per digit (a
+// block each) the exclusive prefix of its counts over the tiles, and the
+// digit totals; the other blocks clear `nxt`. Phase 2: the scatter, in which a
+// key's rank among equal digits of its tile = earlier warps' counts + lanes
+// below it in its warp with the same digit (warp match); each key also counts
+// its digit of the next pass (`next`, if has_next) into `nxt` at its new tile.
+// Two grid barriers.
+template <bool PART>
+__device__ void tb_sort_pass(cg::grid_group &g, const TreeBuildArgs &a, const uint64_t *ik,
+                             const uint32_t *iv, uint64_t *ok, uint32_t *ov, int shift,
+                             uint32_t *cur, uint32_t *nxt, bool has_next, int next) {
+  __shared__ uint32_t h[256];
+  __shared__ uint32_t wcnt[TB_THREADS / 32][256];
+  __shared__ uint32_t sw[32];
+  const unsigned t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const uint32_t n = a.n, tiles = a.tiles;
+  const uint32_t tid = blockIdx.x * blockDim.x + t, nth = gridDim.x * blockDim.x;
+  for (uint32_t d = blockIdx.x; d < 256; d += gridDim.x) {
+    uint32_t run = 0;
+    for (uint32_t t0 = 0; t0 < tiles; t0 += TB_THREADS) {
+      const uint32_t tt = t0 + t;
+      const uint32_t x = tt < tiles ? ldc(&cur[(size_t)tt * 256 + d]) : 0;
+      uint32_t tot;
+      const uint32_t ex = block_excl(x, sw, tot);
+      if (tt < tiles) cur[(size_t)tt * 256 + d] = run + ex;
+      run += tot;
+    }
+    if (t == 0) a.dtot[d] = run;
+  }
+  if (has_next)
+    for (uint32_t i = tid; i < tiles * 256; i += nth) nxt[i] = 0;
+  g.sync();
+  for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    uint32_t tot;
+    const uint32_t dbase = block_excl(ldc(&a.dtot[t]), sw, tot);
+    h[t] = dbase + ldc(&cur[(size_t)tile * 256 + t]);
+    for (int k = t; k < 256 * (TB_THREADS / 32); k += blockDim.x) (&wcnt[0][0])[k] = 0;
+    __syncthreads();
+    const uint32_t i = tile * TB_TILE + t;
+    const bool valid = i < n;
+    const uint64_t k = valid ? ldc(&ik[i]) : 0;
+    const uint32_t v = valid ? ldc(&iv[i]) : 0;
+    const uint32_t d = valid ? tb_digit<PART>(k, v, shift) : 256u + lane;  // never matches
+    const unsigned peers = __match_any_sync(0xffffffffu, d);
+    const unsigned below = __popc(peers & ((1u << lane) - 1));
+    if (valid && below == 0) wcnt[warp][d] = __popc(peers);
+    __syncthreads();
+    if (valid) {
+      uint32_t before = 0;
+      for (unsigned w = 0; w < warp; ++w) before += wcnt[w][d];
+      const uint32_t pos = h[d] + before + below;
+      ok[pos] = k;
+      ov[pos] = v;
+      if (has_next) atomicAdd(&nxt[(size_t)(pos / TB_TILE) * 256 + tb_next_digit(k, v, next)], 1u);
+    }
+    __syncthreads();
+  }
+  g.sync();
+}
+
+__global__ void __launch_bounds__(TB_THREADS) k_tree_build(TreeBuildArgs a) {
+  cg::grid_group g = cg::this_grid();
+  __shared__ double se[4];
+  __shared__ uint32_t sm_m;
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  const uint32_t n = a.n;
+  tb_stamp(a, 0);
+  // 1. the box: block partials, then every block merges all of them (the
+  //    first-wins merge is order independent, so every block gets the same)
+  {
+    double v[4] = {INFINITY, INFINITY, -INFINITY, -INFINITY};
+    uint32_t ix[4] = {NONE, NONE, NONE, NONE};
+    uint32_t m = 0;
+    for (uint32_t i = tid; i < n; i += nth) {
+      const double x = a.xs[i], y = a.ys[i];
+      if (x != x || y != y) continue;
+      double pv[4] = {x, y, x, y};
+      uint32_t pi[4] = {i, i, i, i};
+      box_merge(v, ix, m, pv, pi, 1);
+    }
+    block_box_reduce(v, ix, m);
+    if (threadIdx.x == 0) {
+      BoxPart p;
+      for (int q = 0; q < 4; ++q) { p.v[q] = v[q]; p.i[q] = ix[q]; }
+      p.m = m;
+      a.parts[blockIdx.x] = p;
+    }
+    for (uint32_t i = tid; i < a.tiles * 256; i += nth) a.hist[i] = 0;
+  }
+  g.sync();
+  {
+    double v[4] = {INFINITY, INFINITY, -INFINITY, -INFINITY};
+    uint32_t ix[4] = {NONE, NONE, NONE, NONE};
+    uint32_t m = 0;
+    for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+      const BoxPart *p = &a.parts[b];
+      double pv[4];
+      uint32_t pi[4];
+      for (int q = 0; q < 4; ++q) {
+        pv[q] = __ldcg(&p->v[q]);
+        pi[q] = __ldcg(&p->i[q]);
+      }
+      box_merge(v, ix, m, pv, pi, __ldcg(&p->m));
+    }
+    block_box_reduce(v, ix, m);
+    if (threadIdx.x == 0) {
+      double e[4] = {NAN, NAN, NAN, NAN};
+      if (!(v[0] > v[2] || v[1] > v[3])) {
+        cover(e, v[0], v[1]);
+        cover(e, v[2], v[3]);
+      }
+      for (int q = 0; q < 4; ++q) se[q] = e[q];
+      sm_m = m;
+      if (blockIdx.x == 0) {
+        for (int q = 0; q < 4; ++q) a.extent[q] = e[q];
+        a.info[0] = m;
+        a.info[1] = 0;
+        a.info[2] = 0;
+        a.info[3] = m ? 0 : NONE;
+        a.info[4] = 0;
+        a.info[5] = 0;
+      }
+    }
+    __syncthreads();
+  }
+  const uint32_t m = sm_m;
+  if (n == 0) return;
+  // 2. keys, and the first sort pass's digit counts (cleared above)
+  tb_stamp(a, 1);
+  for (uint32_t i = tid; i < n; i += nth) {
+    keys_at(i, a.xs, a.ys, se, a.keys, a.sv);
+    atomicAdd(&a.hist[(size_t)(i / TB_TILE) * 256 + (uint32_t)(a.keys[i] & 255u)], 1u);
+  }
+  g.sync();
+  tb_stamp(a, 2);
+  // 3. the stable sort: 8 key bytes, then the NaN partition if any point has one
+  uint64_t *ak = a.keys, *bk = a.keys_tmp;
+  uint32_t *av = a.sv, *bv = a.sv_tmp;
+  uint32_t *hc = a.hist, *hn = a.hist2;
+  const bool part = m < n;
+  for (int b = 0; b < 8; ++b) {
+    const bool has_next = b < 7 || part;
+    tb_sort_pass<false>(g, a, ak, av, bk, bv, 8 * b, hc, hn, has_next, b < 7 ? 8 * (b + 1) : -1);
+    uint64_t *tk = ak; ak = bk; bk = tk;
+    uint32_t *tv = av; av = bv; bv = tv;
+    uint32_t *th = hc; hc = hn; hn = th;
+  }
+  if (part) {
+    tb_sort_pass<true>(g, a, ak, av, bk, bv, 0, hc, hn, false, 0);
+    for (uint32_t i = tid; i < n; i += nth) {
+      a.keys[i] = ldc(&bk[i]);
+      a.sv[i] = ldc(&bv[i]);
+    }
+    g.sync();
+  }
+  tb_stamp(a, 3);
+  // 4. perm and the shared levels; 5. cells per start
+  for (uint32_t k = tid; k < n; k += nth)
+    runs_at(k, m, a.xs, a.ys, a.keys, a.sv, a.perm, a.lcpx, a.leaf_of);
+  g.sync();
+  tb_stamp(a, 4);
+  for (uint32_t k = tid; k < n; k += nth)
+    count_at(k, m, a.xs, a.ys, a.keys, a.lcpx, se, a.perm, a.perm_tmp, a.frames, a.cnt, a.run_end,
+             a.leafd);
+  g.sync();
+  tb_stamp(a, 5);
+  // 6. cell indices: the exclusive scan of the counts
+  const uint32_t total = grid_excl_scan(g, a.cnt, a.base, n, a.bsum);
+  if (tid == 0) a.info[1] = total;
+  g.sync();
+  tb_stamp(a, 6);
+  // 7. the cells
+  if (total > a.cells_cap) {
+    if (tid == 0) {
+      a.info[5] = 1;
+      atomicOr(a.status, ST_DEEP_STACK);
+    }
+    return;
+  }
+  for (uint32_t k = tid; k < m; k += nth)
+    emit_at(k, m, total, a.xs, a.ys, a.keys, a.lcpx, se, a.perm, a.perm_tmp, a.frames, a.base,
+            a.run_end, a.leafd, a.cells, a.skip, a.parent, a.counter, a.info, a.leaf_of);
+  __syncthreads();
+  tb_stamp(a, 7);  // block 0's emit only
 }
 
 int tree_reserve(TreeDev &t, uint32_t n) {
@@ -467,6 +761,8 @@ int tree_reserve(TreeDev &t, uint32_t n) {
     D3_CUDA_OK(cudaMemset(t.info, 0, 16 * sizeof(uint32_t)));
     D3_CUDA_OK(cudaMalloc(&t.extent, 4 * sizeof(double)));
     D3_CUDA_OK(cudaMalloc(&t.box_part, BOX_BLOCKS_MAX * sizeof(BoxPart)));
+    D3_CUDA_OK(cudaMalloc(&t.stamps, 8 * sizeof(unsigned long long)));
+    D3_CUDA_OK(cudaMemset(t.stamps, 0, 8 * sizeof(unsigned long long)));
   }
   if (n <= t.cap && t.cap) return 0;
   uint32_t cap = n < 1024 ? 1024 : n;
@@ -494,7 +790,7 @@ int tree_reserve(TreeDev &t, uint32_t n) {
   D3_CUDA_OK(cudaMalloc(&t.leaf_of, cap * 4ull));
   size_t sp = scan_partial_words(sort_hist_words(cap) > cap + 1 ? sort_hist_words(cap) : cap + 1);
   D3_CUDA_OK(cudaMalloc(&t.scan_part, sp * 4));
-  D3_CUDA_OK(cudaMalloc(&t.hist, sort_hist_words(cap) * 4));
+  D3_CUDA_OK(cudaMalloc(&t.hist, tree_hist_words(cap) * 4));
   t.cap = cap;
   t.cells_cap = (uint32_t)cells;
   return 0;
@@ -506,7 +802,7 @@ void tree_free(TreeDev &t) {
   cudaFree(t.leafd); cudaFree(t.frames); cudaFree(t.cells); cudaFree(t.skip); cudaFree(t.parent);
   cudaFree(t.counter); cudaFree(t.scan_part); cudaFree(t.hist); cudaFree(t.info);
   cudaFree(t.leaf_of);
-  cudaFree(t.extent); cudaFree(t.box_part);
+  cudaFree(t.extent); cudaFree(t.box_part); cudaFree(t.stamps);
   t = TreeDev();
 }
 
@@ -518,25 +814,42 @@ void fast_box(TreeDev &t, const double *xs, const double *ys, uint32_t n, double
                                            square);
 }
 
+static int g_tree_blocks = 0;
+
 void tree_build(TreeDev &t, const double *xs, const double *ys, uint32_t n, uint32_t *status,
                 cudaStream_t st) {
-  unsigned bb = blocks_for(n, BOX_THREADS * 4);
-  if (bb > BOX_BLOCKS_MAX) bb = BOX_BLOCKS_MAX;
-  D3_LAUNCH(k_box, bb, BOX_THREADS, 0, st)(xs, ys, n, (BoxPart *)t.box_part, t.extent, t.info,
-                                           nullptr);
-  if (n == 0) return;
-  const unsigned T = 256, B = blocks_for(n, T);
-  D3_LAUNCH(k_keys, B, T, 0, st)(xs, ys, n, t.extent, t.keys, t.sv);
-  SortScratch ss{t.keys_tmp, t.sv_tmp, t.hist, t.scan_part};
-  radix_sort_u64(t.keys, t.sv, n, 0, 8, true, ss, st);
-  D3_LAUNCH(k_runs, B, T, 0, st)(xs, ys, n, t.keys, t.sv, t.perm, t.lcpx, t.info, t.leaf_of);
-  D3_LAUNCH(k_count, B, T, 0, st)(xs, ys, t.keys, t.lcpx, t.extent, t.perm, t.perm_tmp, t.frames, t.cnt,
-                           t.run_end, t.leafd, t.info, n);
-  // cells before each start; the total lands in info[1]
-  scan_u32(t.cnt, t.base, n, t.scan_part, t.info + 1, st);
-  D3_LAUNCH(k_emit, B, T, 0, st)(xs, ys, t.keys, t.lcpx, t.extent, t.perm, t.perm_tmp, t.frames, t.base,
-                          t.run_end, t.leafd, t.cells, t.skip, t.parent, t.counter, t.cells_cap,
-                          t.info, status, t.leaf_of);
+  if (!g_tree_blocks) {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_tree_build, TB_THREADS, 0);
+    per = per > 2 ? 2 : per;
+    g_tree_blocks = sms * (per > 0 ? per : 1);
+    if (g_tree_blocks > (int)TREE_GRID_MAX) g_tree_blocks = TREE_GRID_MAX;
+  }
+  TreeBuildArgs a;
+  a.xs = xs; a.ys = ys; a.n = n;
+  a.tiles = (n + TB_TILE - 1) / TB_TILE;
+  a.cells_cap = t.cells_cap;
+  a.keys = t.keys; a.keys_tmp = t.keys_tmp; a.sv = t.sv; a.sv_tmp = t.sv_tmp;
+  a.perm = t.perm; a.perm_tmp = t.perm_tmp; a.lcpx = t.lcpx;
+  a.cnt = t.cnt; a.base = t.base; a.run_end = t.run_end; a.leafd = t.leafd;
+  a.frames = t.frames; a.cells = t.cells; a.skip = t.skip; a.parent = t.parent;
+  a.counter = t.counter; a.leaf_of = t.leaf_of;
+  a.parts = (BoxPart *)t.box_part;
+  a.hist = t.hist;
+  a.hist2 = t.hist + (size_t)a.tiles * 256;
+  a.dtot = a.hist2 + (size_t)a.tiles * 256;
+  a.bsum = a.dtot + 256;
+  a.extent = t.extent; a.info = t.info; a.status = status;
+  a.stamps = t.stamps;
+  void *params[] = {&a};
+  ++g_launches;
+  if (cudaLaunchCooperativeKernel((const void *)k_tree_build, g_tree_blocks, TB_THREADS, params, 0,
+                                  st) != cudaSuccess) {
+    // report it: without the launch the cells are stale
+    cudaMemsetAsync(t.info + 5, 0xff, sizeof(uint32_t), st);
+  }
 }
 
 }  // namespace d3

@@ -35,7 +35,21 @@ struct TreeDev {
   uint32_t *hist = nullptr;
   double *extent = nullptr;      // 4
   uint32_t *info = nullptr;      // 0 m, 1 cells, 2 depth, 3 root, 4 ticket, 5 overflow
+  unsigned long long *stamps = nullptr;  // the last build's phase ends (globaltimer ns)
 };
+
+// Grid blocks of the build's cooperative launch (at most).
+constexpr uint32_t TREE_GRID_MAX = 592;
+
+// Words of t.hist: the build's per-tile digit counts (256 keys a tile) for
+// two passes, digit totals and grid partials; also enough for
+// radix_sort_u64's histograms.
+inline size_t tree_hist_words(uint32_t n) {
+  const size_t tiles = (n + 255) / 256 + 1;
+  const size_t a = 2 * tiles * 256 + 256 + TREE_GRID_MAX;
+  const size_t b = sort_hist_words(n);
+  return a > b ? a : b;
+}
 
 int tree_reserve(TreeDev &t, uint32_t n);
 void tree_free(TreeDev &t);

@@ -151,7 +151,10 @@ double sim_last_tick_ms(uint32_t h);
  * 12-18 microseconds of the last parallel collide's phases (guess, then
  * rounds / check per attempt); the last center sum's 22 / 23 microseconds of
  * the exact x / y walks, 24 its x walk's record batches rerun with their
- * entry tests, 25 stretches added one by one, 26 records in all;
+ * entry tests, 25 stretches added one by one, 26 records in all; 27 host
+ * milliseconds the last sim_tick spent queueing work; 30-36 microseconds of
+ * the last tree build's phases (box, keys, sort, runs, cell counts, their
+ * scan, the cells);
  * 100 + k milliseconds and 200 + k count of phase k
  * since sim_set_profile(h, 1): 0 many-body tree, 1 many-body accumulation,
  * 2 many-body traversal, 3 exact link, 4 collide tree and radii, 5 collide

@@ -30,6 +30,7 @@
 //  again; after 3 attempts, or when a turn would draw from `random` (a zero
 //  delta), block 0 runs the serial loop itself on the restored state.
 #include <cooperative_groups.h>
+#include <cstdlib>
 
 #include "forces.cuh"
 
@@ -38,8 +39,9 @@ namespace cg = cooperative_groups;
 namespace d3 {
 
 constexpr int SPEC_CAP = 64;        // guessed heads per node (R)
-constexpr int VISIT_CAP = 128;      // recorded margin-entered cells per node
+constexpr int VISIT_CAP = 128;      // recorded margin-entered cells per node (4 per lane)
 constexpr uint16_t VISIT_NONE = 0xffff;
+constexpr uint32_t LEAF_TAG = 0x80000000u;  // vaux: the recorded cell is a leaf
 constexpr int SPEC_ATTEMPTS = 3;
 constexpr uint32_t SPEC_MAX_ROUNDS = 4096;
 constexpr unsigned SPEC_THREADS = 256;
@@ -56,12 +58,14 @@ struct SpecArgs {
   const double *xs, *ys, *px, *py, *radii;
   double *vxs, *vys, *svx, *svy;
   double strength, delta0;
+  int force_traverse;    // every moved or unmoved turn takes the exact warp traversal (tests)
   uint32_t n;
   uint32_t *rlist;       // n * SPEC_CAP
   uint8_t *rcount;       // n
   uint64_t *wmask;       // n
   uint64_t *emask;       // n: heads the exact traversal from the pass start visits
   uint32_t *vlist;       // n * VISIT_CAP: cells the margin traversal entered, preorder
+  uint32_t *vaux;        // n * VISIT_CAP: per recorded cell, a leaf's head | LEAF_TAG, else its skip
   uint16_t *vcount;      // n (VISIT_NONE: not recorded)
   uint32_t *start;       // n: subtree root the traversals start from
   double *mdelta;        // n: the node's margin
@@ -137,6 +141,7 @@ __device__ bool spec_guess(const SpecArgs &a, uint32_t i, double margin, bool al
   const double xi = a.px[i], yi = a.py[i], ri = a.radii[i];
   uint32_t *rl = a.rlist + (size_t)i * SPEC_CAP;
   uint32_t *vl = a.vlist + (size_t)i * VISIT_CAP;
+  uint32_t *va = a.vaux + (size_t)i * VISIT_CAP;
   a.rcount[i] = 0;
   a.wmask[i] = 0;
   a.emask[i] = 0;
@@ -158,7 +163,10 @@ __device__ bool spec_guess(const SpecArgs &a, uint32_t i, double margin, bool al
     const bool ex_vis = c >= ex_until;
     if (is_leaf(q)) {
       const uint32_t j = a.perm[q.first + q.count - 1];
-      if (nv < VISIT_CAP) vl[nv] = c;
+      if (nv < VISIT_CAP) {
+        vl[nv] = c;
+        va[nv] = j | LEAF_TAG;
+      }
       ++nv;
       if (j > i) {
         if (nr == SPEC_CAP) return false;
@@ -176,7 +184,10 @@ __device__ bool spec_guess(const SpecArgs &a, uint32_t i, double margin, bool al
       continue;
     }
     if (ex_vis && pruned(q, xi, yi, r)) ex_until = a.skip[c];
-    if (nv < VISIT_CAP) vl[nv] = c;
+    if (nv < VISIT_CAP) {
+      vl[nv] = c;
+      va[nv] = a.skip[c];
+    }
     ++nv;
     c = c + 1;
   }
@@ -187,41 +198,37 @@ __device__ bool spec_guess(const SpecArgs &a, uint32_t i, double margin, bool al
   return true;
 }
 
-// Which guessed heads node i examines from (xi, yi): a mask over R. Fast when
-// i has not moved (the exact-visit mask of the guess); otherwise the recorded
-// cells are replayed by the warp in parallel: a recorded cell is skipped when
-// it lies in the subtree of an earlier recorded cell the exact test prunes
-// (a running maximum of those subtrees' ends). Returns false when the record
-// does not apply (i moved beyond its margin, or no record): lane-uniform.
-__device__ bool warp_examined(const SpecArgs &a, uint32_t i, double xi, double yi, bool unmoved,
-                              uint64_t &mask) {
+// Which guessed heads node i examines from (xi, yi), once i has moved: a mask
+// over R. The recorded cells (vc, va: entries 4 lane .. 4 lane + 3, loaded by
+// the caller) are replayed by the warp in parallel: a recorded cell is skipped
+// when it lies in the subtree of an earlier recorded cell the exact test
+// prunes (a running maximum of those subtrees' ends). Only the internal
+// cells' boxes are loaded here. Returns false when the record does not apply
+// (i moved beyond its margin, or no record): lane-uniform.
+__device__ bool warp_replay(const SpecArgs &a, uint32_t i, double xi, double yi, uint16_t nv,
+                            double md, double pxi, double pyi, const uint32_t *vc,
+                            const uint32_t *va, uint64_t &mask) {
   const unsigned lane = threadIdx.x & 31;
-  if (unmoved) {
-    mask = rd(&a.emask[i]);
-    return true;
-  }
-  const uint16_t nv = rd(&a.vcount[i]);
-  const double md = rd(&a.mdelta[i]) * (1 - 1e-9);
-  if (nv == VISIT_NONE || !(fabs(xi - a.px[i]) < md && fabs(yi - a.py[i]) < md)) return false;
-  const uint32_t *vl = a.vlist + (size_t)i * VISIT_CAP;
+  md *= (1 - 1e-9);
+  if (nv == VISIT_NONE || !(fabs(xi - pxi) < md && fabs(yi - pyi) < md)) return false;
   const double ri = a.radii[i];
-  // lane holds recorded entries 4 lane .. 4 lane + 3
   uint32_t cell[4], upto[4];
   bool head[4];
   uint32_t run = 0;
+#pragma unroll
   for (int u = 0; u < 4; ++u) {
     const uint32_t t = 4 * lane + u;
     cell[u] = NONE;
     head[u] = false;
     upto[u] = 0;
     if (t < nv) {
-      const uint32_t c = rd(&vl[t]);
-      const Cell &q = a.cells[c];
+      const uint32_t c = vc[u], x = va[u];
       cell[u] = c;
-      if (is_leaf(q)) {
-        head[u] = a.perm[q.first + q.count - 1] > i;
-      } else if (pruned(q, xi, yi, ri + q.r)) {
-        upto[u] = a.skip[c];
+      if (x & LEAF_TAG) {
+        head[u] = (x & ~LEAF_TAG) > i;
+      } else {
+        const Cell &q = a.cells[c];
+        if (pruned(q, xi, yi, ri + q.r)) upto[u] = x;
       }
     }
     run = max(run, upto[u]);
@@ -257,128 +264,6 @@ __device__ bool warp_examined(const SpecArgs &a, uint32_t i, double xi, double y
   for (int o = 16; o > 0; o >>= 1) m |= __shfl_xor_sync(0xffffffffu, m, o);
   mask = m;
   return true;
-}
-
-// E: node i's turn by one warp.
-__device__ void warp_turn(const SpecArgs &a, uint32_t i, double *cx, double *cy) {
-  const unsigned lane = threadIdx.x & 31;
-  const uint32_t *rl = a.rlist + (size_t)i * SPEC_CAP;
-  const uint32_t nr = rd(&a.rcount[i]);
-  const uint64_t wm = rd(&a.wmask[i]);
-  const double ri = a.radii[i], ri2 = ri * ri;
-  const double vi = rd(&a.vxs[i]), wi = rd(&a.vys[i]);
-  const double xi = a.xs[i] + vi, yi = a.ys[i] + wi;
-  const bool unmoved = same_bits(vi, rd(&a.svx[i])) && same_bits(wi, rd(&a.svy[i]));
-  uint64_t ex = 0;
-  if (!warp_examined(a, i, xi, yi, unmoved, ex)) {
-    // i moved beyond its margin: lane 0 runs the exact traversal from the
-    // root; every head it examines must still be among the guessed ones.
-    uint32_t bad = 0;
-    if (lane == 0) {
-      const uint32_t len = a.info[1];
-      for (uint32_t c = 0; c < len && !bad;) {
-        const Cell &q = a.cells[c];
-        if (is_leaf(q)) {
-          const uint32_t j = a.perm[q.first + q.count - 1];
-          if (j > i) {
-            uint32_t k = 0;
-            while (k < nr && rd(&rl[k]) != j) ++k;
-            if (k == nr) bad = 1;
-            else ex |= 1ull << k;
-          }
-          c = c + 1;
-          continue;
-        }
-        c = pruned(q, xi, yi, ri + q.r) ? a.skip[c] : c + 1;
-      }
-    }
-    bad = __shfl_sync(0xffffffffu, bad, 0);
-    ex = __shfl_sync(0xffffffffu, ex, 0);
-    if (bad) {
-      if (lane == 0) {
-        atomicAdd(&a.counters[C_FAIL], 1u);
-        atomicAdd(&a.counters[C_FAIL_READ], 1u);
-        a.state[i] = 3;
-      }
-      return;
-    }
-  }
-  // each lane evaluates the examined heads with indices lane and lane + 32
-  bool fail = false, jig = false;
-  uint64_t over = 0;
-  uint32_t pj[2];
-  double pdx[2], pdy[2];
-  int np = 0;
-  for (int h = 0; h < 2; ++h) {
-    const uint32_t e = lane + 32 * h;
-    if (e >= nr || !((ex >> e) & 1)) continue;
-    const uint32_t j = rd(&rl[e]);
-    double rj = a.radii[j];
-    double r = ri + rj;
-    double x = xi - a.xs[j] - rd(&a.vxs[j]);
-    double y = yi - a.ys[j] - rd(&a.vys[j]);
-    double l = x * x + y * y;
-    if (!(l < r * r)) continue;
-    if (!((wm >> e) & 1)) {
-      fail = true;
-      continue;
-    }
-    if (x == 0 || y == 0) {
-      jig = true;
-      continue;
-    }
-    l = sqrt(l);
-    l = (r - l) / l * a.strength;
-    x *= l;
-    y *= l;
-    rj *= rj;
-    r = rj / (ri2 + rj);
-    cx[e] = x * r;
-    cy[e] = y * r;
-    over |= 1ull << e;
-    r = 1 - r;
-    pj[np] = j;
-    pdx[np] = x * r;
-    pdy[np] = y * r;
-    ++np;
-  }
-  fail = __any_sync(0xffffffffu, fail);
-  jig = __any_sync(0xffffffffu, jig);
-  for (int o = 16; o > 0; o >>= 1) over |= __shfl_xor_sync(0xffffffffu, over, o);
-  __syncwarp();
-  if (fail || jig) {
-    if (lane == 0) {
-      if (jig) atomicAdd(&a.counters[C_JIGGLE], 1u);
-      if (fail) {
-        atomicAdd(&a.counters[C_FAIL], 1u);
-        atomicAdd(&a.counters[C_FAIL_WRITE], 1u);
-        a.state[i] = 3;
-      }
-    }
-    return;
-  }
-  if (lane == 0) {
-    // d3 adds its own share head by head, in visit order (R order)
-    double v = vi, w = wi;
-    uint64_t o = over;
-    while (o) {
-      const int e = __ffsll((long long)o) - 1;
-      o &= o - 1;
-      v += cx[e];
-      w += cy[e];
-    }
-    a.vxs[i] = v;
-    a.vys[i] = w;
-    atomicAdd(&a.counters[unmoved ? C_FAST_TURNS : C_SLOW_TURNS], 1u);
-  }
-  for (int h = 0; h < np; ++h) {
-    const uint32_t j = pj[h];
-    a.vxs[j] = rd(&a.vxs[j]) - pdx[h];
-    a.vys[j] = rd(&a.vys[j]) - pdy[h];
-    atomicAdd(&a.push[j], sqrt(pdx[h] * pdx[h] + pdy[h] * pdy[h]));
-    atomicMin(&a.min_pusher[j], i);
-    atomicMax(&a.max_pusher[j], i);
-  }
 }
 
 // V: an inactive node's turn re-run at its exact turn state. Its own velocity
@@ -419,16 +304,17 @@ __device__ bool spec_inactive_ok(const SpecArgs &a, uint32_t i) {
   const double md = rd(&a.mdelta[i]) * (1 - 1e-9);
   if (nv != VISIT_NONE && fabs(xi - a.px[i]) < md && fabs(yi - a.py[i]) < md) {
     const uint32_t *vl = a.vlist + (size_t)i * VISIT_CAP;
+    const uint32_t *va = a.vaux + (size_t)i * VISIT_CAP;
     uint32_t ex_until = 0;
     for (uint32_t t = 0; t < nv; ++t) {
-      const uint32_t c = rd(&vl[t]);
+      const uint32_t c = rd(&vl[t]), x = rd(&va[t]);
       const Cell &q = a.cells[c];
-      if (is_leaf(q)) {
-        const uint32_t j = a.perm[q.first + q.count - 1];
+      if (x & LEAF_TAG) {
+        const uint32_t j = x & ~LEAF_TAG;
         if (j > i && c >= ex_until && !clear(j, q.r)) return false;
         continue;
       }
-      if (c >= ex_until && pruned(q, xi, yi, ri + q.r)) ex_until = a.skip[c];
+      if (c >= ex_until && pruned(q, xi, yi, ri + q.r)) ex_until = x;
     }
     return true;
   }
@@ -451,25 +337,6 @@ __device__ bool spec_inactive_ok(const SpecArgs &a, uint32_t i) {
   return true;
 }
 
-__device__ bool warp_ready(const SpecArgs &a, uint32_t i, uint64_t tag, uint32_t par) {
-  const unsigned lane = threadIdx.x & 31;
-  const uint64_t *min_acc = a.min_acc + (size_t)par * a.n, *min_wr = a.min_wr + (size_t)par * a.n;
-  const uint32_t *rl = a.rlist + (size_t)i * SPEC_CAP;
-  const uint32_t nr = rd(&a.rcount[i]);
-  const uint64_t wm = rd(&a.wmask[i]);
-  bool ok = true;
-  if (lane == 0) {  // self: read and written
-    const uint64_t v = rd(&min_acc[i]);
-    ok = !((v >> 32) == tag && (uint32_t)v < i);
-  }
-  for (uint32_t k = lane; k < nr; k += 32) {
-    const uint32_t j = rd(&rl[k]);
-    const uint64_t v = ((wm >> k) & 1) ? rd(&min_acc[j]) : rd(&min_wr[j]);
-    if ((v >> 32) == tag && (uint32_t)v < i) ok = false;
-  }
-  return __all_sync(0xffffffffu, ok);
-}
-
 __device__ void warp_mark(const SpecArgs &a, uint32_t i, uint64_t tag, uint32_t par) {
   const unsigned lane = threadIdx.x & 31;
   uint64_t *min_acc = a.min_acc + (size_t)par * a.n, *min_wr = a.min_wr + (size_t)par * a.n;
@@ -486,6 +353,242 @@ __device__ void warp_mark(const SpecArgs &a, uint32_t i, uint64_t tag, uint32_t 
     atomicMin((unsigned long long *)&min_acc[j], t);
     if ((wm >> k) & 1) atomicMin((unsigned long long *)&min_wr[j], t);
   }
+}
+
+// The exact traversal of node i from (xi, yi), by the warp: windows of 32
+// consecutive cells in preorder; a cell is visited when no earlier cell the
+// exact test prunes covers it (a running maximum of the pruned cells' skip
+// links), and the next window starts past both the window and that maximum.
+// Every leaf head j > i it examines must be among the guessed heads (lane k
+// holds heads k and k + 32 in jj[]); mask gets their indices in R. Returns
+// false if one is missing (lane-uniform).
+__device__ bool warp_traverse(const SpecArgs &a, uint32_t i, double xi, double yi, double ri,
+                              const uint32_t *jj, uint64_t &mask) {
+  const unsigned lane = threadIdx.x & 31;
+  // from the smallest ancestor of i's leaf that holds the whole search box:
+  // every cell outside its subtree is pruned anyway
+  uint32_t start = 0;
+  if (lane == 0) start = start_cell(a, i, xi, yi, ri + a.cells[0].r);
+  start = __shfl_sync(0xffffffffu, start, 0);
+  const uint32_t len = start == 0 ? a.info[1] : a.skip[start];
+  uint32_t carry = 0;  // cells below this index lie in pruned subtrees
+  uint64_t m = 0;
+  bool missing = false;
+  for (uint32_t c0 = start; c0 < len;) {
+    const uint32_t c = c0 + lane;
+    uint32_t up = 0, head = NONE;
+    bool leaf = false;
+    if (c < len) {
+      const Cell &q = a.cells[c];
+      leaf = is_leaf(q);
+      if (leaf) head = a.perm[q.first + q.count - 1];
+      else if (pruned(q, xi, yi, ri + q.r)) up = a.skip[c];
+    }
+    uint32_t incl = up;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= (unsigned)o) incl = max(incl, y);
+    }
+    uint32_t before = __shfl_up_sync(0xffffffffu, incl, 1);
+    if (lane == 0) before = 0;
+    const bool vis = c < len && c >= max(carry, before);
+    const bool want = vis && leaf && head > i;
+    // the examined heads' indices in R
+    int k = -1;
+    if (__any_sync(0xffffffffu, want)) {
+      for (int t = 0; t < 32; ++t) {
+        const uint32_t r0 = __shfl_sync(0xffffffffu, jj[0], t), r1 = __shfl_sync(0xffffffffu, jj[1], t);
+        if (want && r0 == head) k = t;
+        if (want && r1 == head) k = t + 32;
+      }
+    }
+    if (want) {
+      if (k < 0) missing = true;
+      else m |= 1ull << k;
+    }
+    carry = max(carry, __shfl_sync(0xffffffffu, incl, 31));
+    c0 = max(c0 + 32, carry);
+  }
+  for (int o = 16; o > 0; o >>= 1) m |= __shfl_xor_sync(0xffffffffu, m, o);
+  mask = m;
+  return !__any_sync(0xffffffffu, missing);
+}
+
+// One pending node's step in a round, by one warp, with its loads issued
+// together: first the node's own data and its guessed heads (lane k holds
+// heads k and k + 32), then the heads' marks together with their positions
+// and velocities. If an earlier pending node conflicts, the node marks its
+// accesses for the next round and joins the next list; otherwise it runs its
+// turn (the head data loaded before the decision is what the turn would read:
+// once the node is ready no other node of the round writes those heads).
+// Returns nothing; state, velocities and counters are updated in place.
+__device__ void warp_step(const SpecArgs &a, uint32_t i, uint64_t tag, uint32_t par,
+                          uint32_t *next, uint32_t *next_n, double *cx, double *cy) {
+  const unsigned lane = threadIdx.x & 31;
+  const uint32_t *rl = a.rlist + (size_t)i * SPEC_CAP;
+  // round trip 1
+  const uint8_t state = rd(&a.state[i]);
+  const uint32_t nr = rd(&a.rcount[i]);
+  const uint64_t wm = rd(&a.wmask[i]);
+  const uint64_t em = rd(&a.emask[i]);
+  const double vi = rd(&a.vxs[i]), wi = rd(&a.vys[i]);
+  const double svi = rd(&a.svx[i]), swi = rd(&a.svy[i]);
+  const uint32_t j0 = lane < nr ? rd(&rl[lane]) : NONE;
+  const uint32_t j1 = lane + 32 < nr ? rd(&rl[lane + 32]) : NONE;
+  if (state != 1) return;
+  // round trip 2: marks, the heads' data for the turn, and (if i moved) its
+  // record of the cells the guess entered
+  const bool unmoved = same_bits(vi, svi) && same_bits(wi, swi);
+  uint32_t vc[4], va[4];
+  uint16_t nv = VISIT_NONE;
+  double md = 0, pxi = 0, pyi = 0;
+  if (!unmoved) {
+    const uint32_t *vl = a.vlist + (size_t)i * VISIT_CAP, *vx = a.vaux + (size_t)i * VISIT_CAP;
+    nv = rd(&a.vcount[i]);
+    md = rd(&a.mdelta[i]);
+    pxi = a.px[i];
+    pyi = a.py[i];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      vc[u] = rd(&vl[4 * lane + u]);
+      va[u] = rd(&vx[4 * lane + u]);
+    }
+  }
+  const uint64_t *min_acc = a.min_acc + (size_t)par * a.n, *min_wr = a.min_wr + (size_t)par * a.n;
+  bool ok = true;
+  if (lane == 0) {  // self: read and written
+    const uint64_t v = rd(&min_acc[i]);
+    ok = !((v >> 32) == tag && (uint32_t)v < i);
+  }
+  // per head: the offset (x, y) = (xi - xs[j] - vxs[j], ...) of the turn,
+  // formed as the turn forms it, and the head's radius
+  const double xi = a.xs[i] + vi, yi = a.ys[i] + wi;
+  double hx[2], hy[2], hr[2];
+  const uint32_t jj[2] = {j0, j1};
+  for (int h = 0; h < 2; ++h) {
+    const uint32_t k = lane + 32 * h, j = jj[h];
+    hx[h] = hy[h] = hr[h] = 0;
+    if (j == NONE) continue;
+    const uint64_t v = ((wm >> k) & 1) ? rd(&min_acc[j]) : rd(&min_wr[j]);
+    if ((v >> 32) == tag && (uint32_t)v < i) ok = false;
+    hx[h] = xi - a.xs[j] - rd(&a.vxs[j]);
+    hy[h] = yi - a.ys[j] - rd(&a.vys[j]);
+    hr[h] = a.radii[j];
+  }
+  if (!__all_sync(0xffffffffu, ok)) {
+    // mark for the next round (the other parity's marks) and stay pending
+    uint64_t *nacc = a.min_acc + (size_t)(par ^ 1u) * a.n, *nwr = a.min_wr + (size_t)(par ^ 1u) * a.n;
+    const unsigned long long t = ((tag - 1) << 32) | i;
+    if (lane == 0) {
+      atomicMin((unsigned long long *)&nacc[i], t);
+      atomicMin((unsigned long long *)&nwr[i], t);
+      next[atomicAdd(next_n, 1u)] = i;
+    }
+    for (int h = 0; h < 2; ++h) {
+      const uint32_t k = lane + 32 * h, j = jj[h];
+      if (j == NONE) continue;
+      atomicMin((unsigned long long *)&nacc[j], t);
+      if ((wm >> k) & 1) atomicMin((unsigned long long *)&nwr[j], t);
+    }
+    return;
+  }
+  if (lane == 0) a.state[i] = 2;  // done (3 = failed, set below)
+  const double ri = a.radii[i], ri2 = ri * ri;
+  uint64_t ex = 0;
+  if (unmoved && !a.force_traverse) {
+    ex = em;
+  } else if (a.force_traverse || !warp_replay(a, i, xi, yi, nv, md, pxi, pyi, vc, va, ex)) {
+    // i moved beyond its margin: the warp runs the exact traversal; every head
+    // it examines must still be among the guessed ones.
+    if (!warp_traverse(a, i, xi, yi, ri, jj, ex)) {
+      if (lane == 0) {
+        atomicAdd(&a.counters[C_FAIL], 1u);
+        atomicAdd(&a.counters[C_FAIL_READ], 1u);
+        a.state[i] = 3;
+        atomicAdd(&a.counters[C_DONE], 1u);
+      }
+      return;
+    }
+  }
+  // each lane evaluates the examined heads with indices lane and lane + 32
+  bool fail = false, jig = false;
+  uint64_t over = 0;
+  uint32_t pj[2];
+  double pdx[2], pdy[2];
+  int np = 0;
+  for (int h = 0; h < 2; ++h) {
+    const uint32_t e = lane + 32 * h;
+    if (e >= nr || !((ex >> e) & 1)) continue;
+    const uint32_t j = jj[h];
+    double rj = hr[h];
+    double r = ri + rj;
+    double x = hx[h];
+    double y = hy[h];
+    double l = x * x + y * y;
+    if (!(l < r * r)) continue;
+    if (!((wm >> e) & 1)) {
+      fail = true;
+      continue;
+    }
+    if (x == 0 || y == 0) {
+      jig = true;
+      continue;
+    }
+    l = sqrt(l);
+    l = (r - l) / l * a.strength;
+    x *= l;
+    y *= l;
+    rj *= rj;
+    r = rj / (ri2 + rj);
+    cx[e] = x * r;
+    cy[e] = y * r;
+    over |= 1ull << e;
+    r = 1 - r;
+    pj[np] = j;
+    pdx[np] = x * r;
+    pdy[np] = y * r;
+    ++np;
+  }
+  fail = __any_sync(0xffffffffu, fail);
+  jig = __any_sync(0xffffffffu, jig);
+  for (int o = 16; o > 0; o >>= 1) over |= __shfl_xor_sync(0xffffffffu, over, o);
+  __syncwarp();
+  if (fail || jig) {
+    if (lane == 0) {
+      if (jig) atomicAdd(&a.counters[C_JIGGLE], 1u);
+      if (fail) {
+        atomicAdd(&a.counters[C_FAIL], 1u);
+        atomicAdd(&a.counters[C_FAIL_WRITE], 1u);
+        a.state[i] = 3;
+      }
+      atomicAdd(&a.counters[C_DONE], 1u);
+    }
+    return;
+  }
+  if (lane == 0) {
+    // d3 adds its own share head by head, in visit order (R order)
+    double v = vi, w = wi;
+    uint64_t o = over;
+    while (o) {
+      const int e = __ffsll((long long)o) - 1;
+      o &= o - 1;
+      v += cx[e];
+      w += cy[e];
+    }
+    a.vxs[i] = v;
+    a.vys[i] = w;
+    atomicAdd(&a.counters[unmoved ? C_FAST_TURNS : C_SLOW_TURNS], 1u);
+    atomicAdd(&a.counters[C_DONE], 1u);
+  }
+  for (int h = 0; h < np; ++h) {
+    const uint32_t j = pj[h];
+    a.vxs[j] = rd(&a.vxs[j]) - pdx[h];
+    a.vys[j] = rd(&a.vys[j]) - pdy[h];
+    atomicAdd(&a.push[j], sqrt(pdx[h] * pdx[h] + pdy[h] * pdy[h]));
+    atomicMin(&a.min_pusher[j], i);
+    atomicMax(&a.max_pusher[j], i);
+  }
+  __syncwarp();
 }
 
 // The serial loop (collide.zig:47-100) with draws from the device LCG.
@@ -536,16 +639,15 @@ __device__ inline unsigned long long now_ns() {
   return t;
 }
 
-__global__ void __launch_bounds__(SPEC_THREADS) k_collide_spec(SpecArgs a) {
+__global__ void __launch_bounds__(SPEC_THREADS, 3) k_collide_spec(SpecArgs a) {
   __shared__ double contrib[SPEC_WARPS][2][SPEC_CAP];
   cg::grid_group g = cg::this_grid();
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
   const uint32_t gw = tid >> 5, nwarps = nth >> 5, wl = threadIdx.x >> 5;
-  const unsigned lane = threadIdx.x & 31;
   const uint32_t n = a.n;
   if (tid < 16) a.counters[tid] = 0;
   if (tid == 0) {
-    for (int k = 0; k < 16; ++k) a.stamps[k] = 0;
+    for (int k = 0; k < 144; ++k) a.stamps[k] = 0;
     a.stamps[0] = now_ns();
   }
   g.sync();
@@ -599,24 +701,14 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_collide_spec(SpecArgs a) {
         if (tid == 0) atomicAdd(&a.counters[C_OVERFLOW], 1u);
         break;
       }
-      const uint64_t tag = 0xFFFFFFFFull - r, tag_next = tag - 1;
+      const uint64_t tag = 0xFFFFFFFFull - r;
       uint32_t *next = a.pend[round & 1];
       uint32_t *next_n = &a.counters[C_PEND0 + round % 3];
-      for (uint32_t k = gw; k < n_list; k += nwarps) {
-        const uint32_t i = rd(&list[k]);
-        if (rd(&a.state[i]) != 1) continue;
-        if (!warp_ready(a, i, tag, r & 1)) {
-          warp_mark(a, i, tag_next, (r + 1) & 1);
-          if (lane == 0) next[atomicAdd(next_n, 1u)] = i;
-          continue;
-        }
-        if (lane == 0) a.state[i] = 2;  // done (3 = failed, set by the turn)
-        __syncwarp();
-        warp_turn(a, i, contrib[wl][0], contrib[wl][1]);
-        if (lane == 0) atomicAdd(&a.counters[C_DONE], 1u);
-        __syncwarp();
-      }
+      if (tid == 0 && attempt == 0 && round < 64) a.stamps[80 + round] = n_list;
+      for (uint32_t k = gw; k < n_list; k += nwarps)
+        warp_step(a, rd(&list[k]), tag, r & 1, next, next_n, contrib[wl][0], contrib[wl][1]);
       g.sync();
+      if (tid == 0 && attempt == 0 && round < 64) a.stamps[16 + round] = now_ns();
       // Every thread reads the same count: it changes again only after the
       // next barrier. (C_DONE cannot decide this: the next round's turns may
       // already be adding to it.)
@@ -700,12 +792,13 @@ int collide_spec_reserve(CollideSpec &s, uint32_t n) {
   cudaFree(s.rlist); cudaFree(s.rcount); cudaFree(s.wmask); cudaFree(s.state); cudaFree(s.active);
   cudaFree(s.min_acc); cudaFree(s.min_wr); cudaFree(s.push); cudaFree(s.min_pusher);
   cudaFree(s.emask); cudaFree(s.max_pusher); cudaFree(s.vlist); cudaFree(s.vcount);
-  cudaFree(s.start); cudaFree(s.mdelta); cudaFree(s.push_prev); cudaFree(s.pend);
+  cudaFree(s.start); cudaFree(s.mdelta); cudaFree(s.push_prev); cudaFree(s.pend); cudaFree(s.vaux);
   if (!s.counters) {
     D3_CUDA_OK(cudaMalloc(&s.counters, 16 * sizeof(uint32_t)));
     D3_CUDA_OK(cudaMemset(s.counters, 0, 16 * sizeof(uint32_t)));
   }
-  if (!s.stamps) D3_CUDA_OK(cudaMalloc(&s.stamps, 16 * sizeof(unsigned long long)));
+  // 16 phase stamps, then attempt 1's per-round end times and list sizes (64 each)
+  if (!s.stamps) D3_CUDA_OK(cudaMalloc(&s.stamps, 144 * sizeof(unsigned long long)));
   D3_CUDA_OK(cudaMalloc(&s.rlist, (size_t)cap * SPEC_CAP * 4));
   D3_CUDA_OK(cudaMalloc(&s.rcount, cap));
   D3_CUDA_OK(cudaMalloc(&s.wmask, cap * 8ull));
@@ -718,6 +811,7 @@ int collide_spec_reserve(CollideSpec &s, uint32_t n) {
   D3_CUDA_OK(cudaMalloc(&s.emask, cap * 8ull));
   D3_CUDA_OK(cudaMalloc(&s.max_pusher, cap * 4ull));
   D3_CUDA_OK(cudaMalloc(&s.vlist, (size_t)cap * VISIT_CAP * 4));
+  D3_CUDA_OK(cudaMalloc(&s.vaux, (size_t)cap * VISIT_CAP * 4));
   D3_CUDA_OK(cudaMalloc(&s.vcount, cap * 2ull));
   D3_CUDA_OK(cudaMalloc(&s.start, cap * 4ull));
   D3_CUDA_OK(cudaMalloc(&s.mdelta, cap * 8ull));
@@ -732,7 +826,7 @@ void collide_spec_free(CollideSpec &s) {
   cudaFree(s.rlist); cudaFree(s.rcount); cudaFree(s.wmask); cudaFree(s.state); cudaFree(s.active);
   cudaFree(s.min_acc); cudaFree(s.min_wr); cudaFree(s.push); cudaFree(s.min_pusher);
   cudaFree(s.emask); cudaFree(s.max_pusher); cudaFree(s.vlist); cudaFree(s.vcount);
-  cudaFree(s.start); cudaFree(s.mdelta); cudaFree(s.push_prev); cudaFree(s.pend);
+  cudaFree(s.start); cudaFree(s.mdelta); cudaFree(s.push_prev); cudaFree(s.pend); cudaFree(s.vaux);
   cudaFree(s.counters); cudaFree(s.stamps);
   s = CollideSpec();
 }
@@ -756,8 +850,11 @@ int collide_parallel(TreeDev &t, const NodeArrays &a, const double *radii, doubl
   args.xs = a.x; args.ys = a.y; args.px = a.px; args.py = a.py; args.radii = radii;
   args.vxs = a.vx; args.vys = a.vy; args.svx = a.snap_vx; args.svy = a.snap_vy;
   args.strength = strength; args.delta0 = delta; args.n = a.n;
+  // D3_COLLIDE_FORCE_TRAVERSE (any value): every turn finds its examined heads
+  // by the exact traversal instead of the recorded ones (a test of that path)
+  args.force_traverse = getenv("D3_COLLIDE_FORCE_TRAVERSE") != nullptr;
   args.rlist = s.rlist; args.rcount = s.rcount; args.wmask = s.wmask; args.emask = s.emask;
-  args.vlist = s.vlist; args.vcount = s.vcount; args.start = s.start; args.mdelta = s.mdelta;
+  args.vlist = s.vlist; args.vaux = s.vaux; args.vcount = s.vcount; args.start = s.start; args.mdelta = s.mdelta;
   args.state = s.state; args.active = s.active; args.min_acc = s.min_acc; args.min_wr = s.min_wr;
   args.push = s.push; args.push_prev = s.push_prev; args.min_pusher = s.min_pusher;
   args.max_pusher = s.max_pusher; args.counters = s.counters; args.stamps = s.stamps;

@@ -998,6 +998,21 @@ double sim_stat(uint32_t h, uint32_t which) {
     phase_collect(s);
     return (double)s->phase_n[which - 200];
   }
+  if (which >= 1000 && which < 1512) {
+    unsigned long long st[512];
+    cudaMemcpy(st, s->spec.stamps, sizeof st, cudaMemcpyDeviceToHost);
+    return (double)st[which - 1000];
+  }
+  if ((which >= 300 && which < 364) || (which >= 400 && which < 464)) {
+    // the last parallel collide's first attempt: 300 + k microseconds of
+    // round k, 400 + k nodes pending at its start
+    unsigned long long st[144];
+    if (cudaMemcpy(st, s->spec.stamps, sizeof st, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+    if (which >= 400) return (double)st[80 + (which - 400)];
+    const uint32_t k = which - 300;
+    const unsigned long long a = k ? st[16 + k - 1] : st[1], b = st[16 + k];
+    return b > a ? (double)(b - a) * 1e-3 : 0;
+  }
   uint32_t spec[16] = {0}, sc[2] = {0}, words[2] = {0};
   cudaMemcpyAsync(s->h_words, s->spec.counters, 16 * sizeof(uint32_t), cudaMemcpyDeviceToHost,
                   s->stream);

@@ -106,6 +106,7 @@ struct CollideSpec {
   double *push = nullptr;
   uint32_t *min_pusher = nullptr, *max_pusher = nullptr;
   uint32_t *vlist = nullptr;
+  uint32_t *vaux = nullptr;    // per recorded cell: a leaf's head (tagged) or its skip link
   uint16_t *vcount = nullptr;
   uint32_t *start = nullptr, *pend = nullptr;
   double *mdelta = nullptr, *push_prev = nullptr;

@@ -154,7 +154,8 @@ double sim_last_tick_ms(uint32_t h);
  * entry tests, 25 stretches added one by one, 26 records in all; 27 host
  * milliseconds the last sim_tick spent queueing work; 30-36 microseconds of
  * the last tree build's phases (box, keys, sort, runs, cell counts, their
- * scan, the cells);
+ * scan, the cells); 300 + k microseconds of round k of the last parallel
+ * collide's first attempt and 400 + k the nodes pending at its start (k < 64);
  * 100 + k milliseconds and 200 + k count of phase k
  * since sim_set_profile(h, 1): 0 many-body tree, 1 many-body accumulation,
  * 2 many-body traversal, 3 exact link, 4 collide tree and radii, 5 collide

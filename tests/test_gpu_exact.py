@@ -72,6 +72,13 @@ def test_gpu_exact_collide_runs_in_parallel(ocore, gcore):
         sb.close()
 
 
+def test_gpu_exact_collide_exact_traversal_path(ocore, gcore, monkeypatch):
+    """Every collide turn takes the warp-parallel exact traversal (the path a
+    node pushed beyond its margin takes), bitwise with the oracle."""
+    monkeypatch.setenv("D3_COLLIDE_FORCE_TRAVERSE", "1")
+    P.run_pair(_defaults(4000, 8000, collide=5, coincident=0.01, near=0.01), ocore, gcore, 20)
+
+
 def test_gpu_exact_d3_collide_known_answers(ocore, gcore):
     """test/d3/collide-test.js scenarios, every tick bitwise with the oracle."""
     def three(core):

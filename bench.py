@@ -77,15 +77,41 @@ def oracle_ms_per_tick(pkg, sc, threads, warmup, rounds, ticks):
 
 
 class Clocks:
-    """nvidia-smi samples during the timed region."""
+    """SM clocks and clock-event reasons sampled during the timed region: NVML
+    every 5 ms from a thread (reads only), else nvidia-smi every 200 ms."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown"}
 
     def __init__(self, device):
         self.proc = None
-        self.device = device
+        self.thread = None
+        self.samples, self.reason_bits, self.max_mhz = [], 0, None
+        try:
+            import threading
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(device)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            self.stop_flag = threading.Event()
+
+            def loop():
+                while not self.stop_flag.is_set():
+                    try:
+                        self.samples.append(float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)))
+                        self.reason_bits |= int(pynvml.nvmlDeviceGetCurrentClocksEventReasons(h))
+                    except Exception:
+                        pass
+                    self.stop_flag.wait(0.005)
+            self.thread = threading.Thread(target=loop, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.thread = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(device), "--query-gpu=" + self.QUERY,
@@ -95,6 +121,14 @@ class Clocks:
             self.proc = None
 
     def stop(self):
+        if self.thread is not None:
+            self.stop_flag.set()
+            self.thread.join(timeout=5)
+            if not self.samples:
+                return None
+            reasons = sorted(v for b, v in self.REASONS.items() if self.reason_bits & b)
+            return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                    "reasons": reasons, "samples": len(self.samples), "source": "nvml 5 ms"}
         if not self.proc:
             return None
         self.proc.terminate()
@@ -120,7 +154,7 @@ class Clocks:
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi 200 ms"}
 
 
 def run_ours(args, pkg, sc):

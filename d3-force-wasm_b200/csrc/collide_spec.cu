@@ -722,8 +722,9 @@ __global__ void __launch_bounds__(SPEC_THREADS, 3) k_collide_spec(SpecArgs a) {
       if (tid == 0) a.counters[C_PEND0 + (round + 2) % 3] = 0;
     }
     if (tid == 0 && attempt < 3) a.stamps[2 + 2 * attempt] = now_ns();
-    // V: inactive nodes stayed no-ops.
-    for (uint32_t i = tid; i < n; i += nth) {
+    // V: inactive nodes stayed no-ops (Morton order, as G).
+    for (uint32_t k = tid; k < n; k += nth) {
+      const uint32_t i = a.perm[k];
       if (rd(&a.state[i]) != 0) continue;
       if (!spec_inactive_ok(a, i)) {
         a.state[i] = 4;  // inactive, but its turn would write: promote

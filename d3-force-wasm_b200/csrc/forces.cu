@@ -6,8 +6,12 @@
 #include <climits>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "forces.cuh"
 #include "scan_sort.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace d3 {
 
@@ -464,10 +468,95 @@ __global__ void k_link_serial_host(double *xs, double *ys, double *vxs, double *
   rng->pos += used;
 }
 
+// link_one with the velocities read through L2 (other blocks of the same
+// cooperative launch wrote them before the last grid barrier).
+__device__ inline bool link_one_cg(const double *xs, const double *ys, double *vxs, double *vys,
+                                   const LinkArrays l, uint32_t e, double alpha) {
+  const uint32_t src = l.source[e], tgt = l.target[e];
+  const double vxt = __ldcg(&vxs[tgt]), vyt = __ldcg(&vys[tgt]);
+  const double vxsrc = __ldcg(&vxs[src]), vysrc = __ldcg(&vys[src]);
+  double x = xs[tgt] + vxt - xs[src] - vxsrc;
+  double y = ys[tgt] + vyt - ys[src] - vysrc;
+  if (x == 0 || x != x || y == 0 || y != y) return false;
+  double len = sqrt(x * x + y * y);
+  len = (len - l.distance[e]) / len * alpha * l.strength[e];
+  x *= len;
+  y *= len;
+  double b = l.bias[e];
+  vxs[tgt] = vxt - x * b;
+  vys[tgt] = vyt - y * b;
+  b = 1 - b;
+  vxs[src] = vxsrc + x * b;
+  vys[src] = vysrc + y * b;
+  return true;
+}
+
+struct LinkCoopArgs {
+  const double *xs, *ys;
+  double *vxs, *vys, *svx, *svy;
+  LinkArrays l;
+  const uint32_t *order, *level_start;
+  uint32_t levels, n;
+  double alpha, iterations;
+  uint32_t *flag;
+};
+
+// The level-scheduled pass in one cooperative launch: the pass-start snapshot,
+// then per iteration and level its links (disjoint nodes) with a grid barrier
+// between levels, then the snapshot back if a link met a zero or NaN delta
+// (the serial kernel then runs the pass with its draws).
+__global__ void __launch_bounds__(256) k_link_coop(LinkCoopArgs a) {
+  cg::grid_group g = cg::this_grid();
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  if (tid == 0) *a.flag = 0;
+  for (uint32_t i = tid; i < a.n; i += nth) {
+    a.svx[i] = a.vxs[i];
+    a.svy[i] = a.vys[i];
+  }
+  bool bad = false;
+  for (double k = 0; k < a.iterations; k += 1) {
+    for (uint32_t lv = 1; lv <= a.levels; ++lv) {
+      const uint32_t lo = a.level_start[lv], hi = a.level_start[lv + 1];
+      for (uint32_t e = lo + tid; e < hi; e += nth)
+        if (!link_one_cg(a.xs, a.ys, a.vxs, a.vys, a.l, a.order[e], a.alpha)) bad = true;
+      g.sync();
+    }
+  }
+  if (bad) atomicOr(a.flag, 1u);
+  g.sync();
+  if (__ldcg(a.flag)) {
+    for (uint32_t i = tid; i < a.n; i += nth) {
+      a.vxs[i] = __ldcg(&a.svx[i]);
+      a.vys[i] = __ldcg(&a.svy[i]);
+    }
+  }
+}
+
+static int g_link_blocks = 0;
+
 void link_exact(const NodeArrays &a, const LinkArrays &l, const LinkPlan &plan, double alpha,
                 double iterations, Rng *rng, uint32_t *flag, cudaStream_t st) {
   if (l.m == 0) return;
   const uint32_t n = a.n;
+  if (!g_link_blocks) {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_link_coop, 256, 0);
+    g_link_blocks = sms * (per >= 2 ? 2 : 1);
+  }
+  {
+    LinkCoopArgs c;
+    c.xs = a.x; c.ys = a.y; c.vxs = a.vx; c.vys = a.vy; c.svx = a.snap_vx; c.svy = a.snap_vy;
+    c.l = l; c.order = plan.order; c.level_start = plan.level_start; c.levels = plan.levels;
+    c.n = n; c.alpha = alpha; c.iterations = iterations; c.flag = flag;
+    void *params[] = {&c};
+    ++g_launches;
+    if (cudaLaunchCooperativeKernel((const void *)k_link_coop, g_link_blocks, 256, params, 0, st) ==
+        cudaSuccess)
+      return;
+  }
+  // (without a cooperative launch: one launch per level)
   cudaMemsetAsync(flag, 0, sizeof(uint32_t), st);
   D3_LAUNCH(k_save_v, blocks_for(n, 256), 256, 0, st)(a.snap_vx, a.snap_vy, a.vx, a.vy, n);
   for (double k = 0; k < iterations; k += 1) {

@@ -444,6 +444,9 @@ class Simulation:
         self._velocity_decay = 0.6
         self._forces = {}  # insertion order = Map order
         self._random = None  # None = d3's lcg() on the device
+        # tick() through one sim_tick call (True), or one force_run per force
+        # per tick as the reference's facade drives its core (False)
+        self.engine_ticks = True
         self._precision = "exact"
         self.ctx = Context(core)
         self.ctx.set_random(None)
@@ -468,8 +471,18 @@ class Simulation:
         self.ctx.resize(nd.n)
 
     def tick(self, iterations=1):
-        """simulation.js:49-89, one force_run per force per tick."""
+        """simulation.js:49-89. With the device LCG as the random source the
+        ticks run in one engine call (sim_tick: the same forces in the same
+        order, bit for bit, with the center sums overlapped on a side stream);
+        with a randomSource() callback, one force_run per force per tick."""
         if not (0 < iterations):
+            return self
+        if self._random is None and self.engine_ticks:
+            self.device_begin()
+            try:
+                self.device_ticks(int(iterations))
+            finally:
+                self.device_end()
             return self
         ctx = self.ctx
         ctx.copy_in(self._nodes)

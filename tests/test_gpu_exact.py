@@ -138,3 +138,15 @@ def test_gpu_sim_tick_path_matches(ocore, gcore):
     finally:
         sa.close()
         sb.close()
+
+
+def test_gpu_force_run_per_force_path_matches(ocore, gcore):
+    """tick() driven the reference facade's way, one force_run per force per
+    tick (no sim_tick), with the device LCG: bitwise with the oracle."""
+    base = _defaults(3000, 6000, collide=5, coincident=0.01, near=0.01, pinned=0.005)
+
+    def setup(core):
+        nodes, sim = base(core)
+        sim.engine_ticks = False
+        return nodes, sim
+    P.run_pair(setup, ocore, gcore, 30)

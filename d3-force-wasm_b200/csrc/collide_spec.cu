@@ -840,9 +840,13 @@ int collide_parallel(TreeDev &t, const NodeArrays &a, const double *radii, doubl
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_collide_spec, SPEC_THREADS, 0);
-    // one block per SM short of full occupancy, so a concurrent one-block
-    // kernel (the center sums on the side stream) never delays the launch
-    g_spec_blocks = sms * (per > 3 ? 3 : (per > 1 ? per - 1 : 1));
+    // blocks per SM: full occupancy (at most 3), or D3_COLLIDE_BLOCKS_PER_SM
+    int want = per > 3 ? 3 : per;
+    if (const char *e = getenv("D3_COLLIDE_BLOCKS_PER_SM")) {
+      const int v = atoi(e);
+      if (v >= 1 && v <= want) want = v;
+    }
+    g_spec_blocks = sms * (want > 0 ? want : 1);
     if (g_spec_blocks <= 0) g_spec_blocks = sms;
   }
   SpecArgs args;

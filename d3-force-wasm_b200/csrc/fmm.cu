@@ -475,104 +475,153 @@ __global__ void __launch_bounds__(FMM_THREADS) k_fmm_upward(FmmArgs a) {
 
 // ---- interaction lists (fmm.zig:400-453) -------------------------------------------
 
-// Expands the calls of cell c (its parent's forward list, or (root, root)).
-// WRITE false: counts only. Returns false if the local stack overflowed.
+// Expands one call (A, b) of cell c = A with the recursion's order: splits of
+// B are followed at once, depth first. WRITE false: counts only (nm, np, nf
+// are added to); WRITE true: the events are written from om / op / of on.
+// Returns false if the local stack overflowed.
 template <bool WRITE>
-__device__ bool expand(const FmmArgs &a, uint32_t c, uint32_t &nm, uint32_t &np, uint32_t &nf,
-                       uint32_t om, uint32_t op, uint32_t of) {
-  const FCell A = a.cells[c];
-  const uint32_t *in;
-  uint32_t nin;
-  uint32_t root_in = 0;
-  if (c == 0) {
-    in = &root_in;
-    nin = 1;
-  } else {
-    in = a.fwd + ldg_cg(&a.fwd_off[A.parent]);
-    nin = ldg_cg(&a.fwd_cnt[A.parent]);
-  }
-  nm = np = nf = 0;
+__device__ bool expand_call(const FmmArgs &a, uint32_t c, const FCell &A, uint32_t b, uint32_t &nm,
+                            uint32_t &np, uint32_t &nf, uint32_t om, uint32_t op, uint32_t of) {
   uint32_t stack[FMM_STACK];
   const bool la = A.nchild == 0;
-  for (uint32_t u = 0; u < nin; ++u) {
-    uint32_t sp = 0;
-    stack[sp++] = c == 0 ? 0 : ldg_cg(&in[u]);
-    while (sp) {
-      const uint32_t B = stack[--sp];
-      if (B == c) {
-        if (la) {
-          if (WRITE) a.p2p[op + np] = c;
-          ++np;
-        } else {
-          for (uint32_t j = 0; j < A.nchild; ++j) {
-            if (WRITE) a.fwd[of + nf] = A.child0 + j;
-            ++nf;
-          }
+  uint32_t sp = 0;
+  stack[sp++] = b;
+  while (sp) {
+    const uint32_t B = stack[--sp];
+    if (B == c) {
+      if (la) {
+        if (WRITE) a.p2p[op + np] = c;
+        ++np;
+      } else {
+        for (uint32_t j = 0; j < A.nchild; ++j) {
+          if (WRITE) a.fwd[of + nf] = A.child0 + j;
+          ++nf;
         }
+      }
+      continue;
+    }
+    const FCell Bc = a.cells[B];
+    const double ra = A.r, rb = Bc.r;
+    const double dx = A.cx - Bc.cx, dy = A.cy - Bc.cy;
+    const double d2 = dx * dx + dy * dy;
+    const double rmax = zmax(ra, rb), rmin = zmin(ra, rb);
+    const double thr = a.mac_far * rmax + rmin;
+    if (d2 > FMM_MIN_SEP2 && d2 >= thr * thr) {
+      bool separated = true;
+      if (a.ring) {
+        const double gap = sqrt(d2) - ra - rb;
+        if (gap >= a.dmax_scaled) continue;
+        if (gap + 2 * (ra + rb) > a.dmax_scaled || gap < a.dmin_scaled) separated = false;
+      }
+      if (separated) {
+        if (WRITE) a.m2l[om + nm] = B;
+        ++nm;
         continue;
       }
-      const FCell Bc = a.cells[B];
-      const double ra = A.r, rb = Bc.r;
-      const double dx = A.cx - Bc.cx, dy = A.cy - Bc.cy;
-      const double d2 = dx * dx + dy * dy;
-      const double rmax = zmax(ra, rb), rmin = zmin(ra, rb);
-      const double thr = a.mac_far * rmax + rmin;
-      if (d2 > FMM_MIN_SEP2 && d2 >= thr * thr) {
-        bool separated = true;
-        if (a.ring) {
-          const double gap = sqrt(d2) - ra - rb;
-          if (gap >= a.dmax_scaled) continue;
-          if (gap + 2 * (ra + rb) > a.dmax_scaled || gap < a.dmin_scaled) separated = false;
-        }
-        if (separated) {
-          if (WRITE) a.m2l[om + nm] = B;
-          ++nm;
-          continue;
-        }
-      }
-      const bool lb = Bc.nchild == 0;
-      if (la && lb) {
-        if (WRITE) a.p2p[op + np] = B;
-        ++np;
-      } else if (la || (!lb && rb > ra)) {
-        if (sp + Bc.nchild > FMM_STACK) return false;
-        for (uint32_t j = Bc.nchild; j-- > 0;) stack[sp++] = Bc.child0 + j;
-      } else {
-        if (WRITE) a.fwd[of + nf] = B;
-        ++nf;
-      }
+    }
+    const bool lb = Bc.nchild == 0;
+    if (la && lb) {
+      if (WRITE) a.p2p[op + np] = B;
+      ++np;
+    } else if (la || (!lb && rb > ra)) {
+      if (sp + Bc.nchild > FMM_STACK) return false;
+      for (uint32_t j = Bc.nchild; j-- > 0;) stack[sp++] = Bc.child0 + j;
+    } else {
+      if (WRITE) a.fwd[of + nf] = B;
+      ++nf;
     }
   }
   return true;
 }
 
+__device__ inline uint32_t warp_excl(uint32_t v, uint32_t &total) {
+  const unsigned lane = threadIdx.x & 31;
+  uint32_t incl = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= (unsigned)o) incl += y;
+  }
+  total = __shfl_sync(0xffffffffu, incl, 31);
+  return incl - v;
+}
+
+// The calls of cell c (its parent's forward list in order, or (root, root)),
+// by one warp: lane k expands calls k, k + 32, ...; each call's events are
+// placed after those of the calls before it (a warp scan of the counts).
+// Counts, then a reservation in the pools, then counts again and the writes.
+__device__ void warp_expand_cell(const FmmArgs &a, uint32_t c, uint32_t *ovf) {
+  const unsigned lane = threadIdx.x & 31;
+  const FCell A = a.cells[c];
+  const uint32_t *in = nullptr;
+  uint32_t nin = 1;
+  if (c != 0) {
+    in = a.fwd + ldg_cg(&a.fwd_off[A.parent]);
+    nin = ldg_cg(&a.fwd_cnt[A.parent]);
+  }
+  uint32_t tm = 0, tp = 0, tf = 0;
+  bool ok = true;
+  for (uint32_t u0 = 0; u0 < nin; u0 += 32) {
+    const uint32_t u = u0 + lane;
+    uint32_t nm = 0, np = 0, nf = 0;
+    if (u < nin && !expand_call<false>(a, c, A, c == 0 ? 0 : ldg_cg(&in[u]), nm, np, nf, 0, 0, 0))
+      ok = false;
+    uint32_t t;
+    warp_excl(nm, t); tm += t;
+    warp_excl(np, t); tp += t;
+    warp_excl(nf, t); tf += t;
+  }
+  ok = __all_sync(0xffffffffu, ok);
+  if (!ok) {
+    tm = tp = tf = 0;
+    if (lane == 0) atomicOr(ovf, 2u);
+  }
+  uint32_t om = 0, op = 0, of = 0;
+  if (lane == 0) {
+    om = atomicAdd(&a.info[FI_POOL_M2L], tm);
+    op = atomicAdd(&a.info[FI_POOL_P2P], tp);
+    of = atomicAdd(&a.info[FI_POOL_FWD], tf);
+    a.m2l_off[c] = om; a.m2l_cnt[c] = tm;
+    a.p2p_off[c] = op; a.p2p_cnt[c] = tp;
+    a.fwd_off[c] = of; a.fwd_cnt[c] = tf;
+  }
+  om = __shfl_sync(0xffffffffu, om, 0);
+  op = __shfl_sync(0xffffffffu, op, 0);
+  of = __shfl_sync(0xffffffffu, of, 0);
+  if (!ok) return;
+  if ((size_t)om + tm > a.cap_m2l || (size_t)op + tp > a.cap_p2p || (size_t)of + tf > a.cap_fwd) {
+    if (lane == 0) atomicOr(ovf, 1u);
+    return;
+  }
+  for (uint32_t u0 = 0; u0 < nin; u0 += 32) {
+    const uint32_t u = u0 + lane;
+    const uint32_t b = u < nin ? (c == 0 ? 0 : ldg_cg(&in[u])) : 0;
+    uint32_t nm = 0, np = 0, nf = 0;
+    if (u < nin) expand_call<false>(a, c, A, b, nm, np, nf, 0, 0, 0);
+    uint32_t t0, t1, t2;
+    const uint32_t xm = warp_excl(nm, t0), xp = warp_excl(np, t1), xf = warp_excl(nf, t2);
+    if (u < nin) {
+      uint32_t wm = 0, wp = 0, wf = 0;
+      expand_call<true>(a, c, A, b, wm, wp, wf, om + xm, op + xp, of + xf);
+    }
+    om += t0;
+    op += t1;
+    of += t2;
+  }
+}
+
+// Level by level from the root, a warp per cell; a grid barrier between
+// levels (a cell's calls are its parent's forward list).
 __global__ void __launch_bounds__(FMM_THREADS) k_fmm_lists(FmmArgs a) {
   cg::grid_group g = cg::this_grid();
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  const uint32_t gw = tid >> 5, nwarps = nth >> 5;
   const uint32_t *lvl = a.info + FI_LVL;
   for (uint32_t lev = 0; lev < a.nlev; ++lev) {
     // the previous level's word: nobody writes it during this level, so every
     // thread takes the same branch
     if (lev && ldg_cg(&a.info[FI_LIST_OVERFLOW + ((lev - 1) & 1)])) break;
     uint32_t *ovf = &a.info[FI_LIST_OVERFLOW + (lev & 1)];
-    for (uint32_t c = lvl[lev] + tid; c < lvl[lev + 1]; c += nth) {
-      uint32_t nm, np, nf;
-      if (!expand<false>(a, c, nm, np, nf, 0, 0, 0)) {
-        atomicOr(ovf, 2u);
-        nm = np = nf = 0;
-      }
-      const uint32_t om = atomicAdd(&a.info[FI_POOL_M2L], nm);
-      const uint32_t op = atomicAdd(&a.info[FI_POOL_P2P], np);
-      const uint32_t of = atomicAdd(&a.info[FI_POOL_FWD], nf);
-      a.m2l_off[c] = om; a.m2l_cnt[c] = nm;
-      a.p2p_off[c] = op; a.p2p_cnt[c] = np;
-      a.fwd_off[c] = of; a.fwd_cnt[c] = nf;
-      if ((size_t)om + nm > a.cap_m2l || (size_t)op + np > a.cap_p2p || (size_t)of + nf > a.cap_fwd) {
-        atomicOr(ovf, 1u);
-        continue;
-      }
-      expand<true>(a, c, nm, np, nf, om, op, of);
-    }
+    for (uint32_t c = lvl[lev] + gw; c < lvl[lev + 1]; c += nwarps) warp_expand_cell(a, c, ovf);
     g.sync();
   }
 }

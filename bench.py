@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fast", action="store_true", help="skip the fast-mode 1M measurement")
     ap.add_argument("--e2e-steps", type=int, default=10)
     return ap.parse_args()
 
@@ -155,6 +156,69 @@ class Clocks:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
                 "samples": len(sm), "source": "nvidia-smi 200 ms"}
+
+
+FAST_N = 1000000
+
+
+def fast_1m(pkg, core, torch, steps=10, warmup=3, targets=1024):
+    """Fast mode at the 1M-node configuration: n uniform in [0, 1e4)^2 (seeded),
+    m = 2n uniform links, forceManyBody (FMM order 8, opening 1.5,
+    distanceMin 1) + forceLink + forceCenter, device ms per tick over `steps`
+    ticks; plus the many-body kick's RMS error on seeded targets against an
+    FP64 direct sum of d3's pair formula (test/fast/error-test.js:44-70)."""
+    import numpy as np
+    n = FAST_N
+    rng = np.random.default_rng(1)
+    xs = rng.random(n) * 1e4
+    ys = rng.random(n) * 1e4
+    src = rng.integers(0, n, 2 * n)
+    tgt = (src + 1 + rng.integers(0, n - 1, 2 * n)) % n
+    nodes = pkg.Nodes(n, x=xs, y=ys)
+    sim = pkg.forceSimulation(nodes, core=core)
+    sim.force("charge", pkg.forceManyBody())
+    sim.force("link", pkg.forceLink(src, tgt))
+    sim.force("center", pkg.forceCenter())
+    sim.precision("fast", order=8, opening=1.5)
+    sim.device_begin()
+    for _ in range(warmup):
+        sim.device_ticks(1)
+    times = [sim.device_ticks(1) for _ in range(steps)]
+    sim.device_end()
+    sim.close()
+    # RMS of the many-body kick alone, from the start layout with zero velocity
+    nodes = pkg.Nodes(n, x=xs, y=ys, vx=np.zeros(n), vy=np.zeros(n))
+    sim = pkg.forceSimulation(nodes, core=core)
+    sim.force("charge", pkg.forceManyBody())
+    sim.precision("fast", order=8, opening=1.5)
+    sim.tick()
+    a1 = sim.alpha()
+    decay = 0.6  # 1 - velocityDecay(0.4): v = kick * decay after one tick
+    kick = np.stack([(np.asarray(nodes.x) - xs) / decay, (np.asarray(nodes.y) - ys) / decay], 1)
+    sim.close()
+    tg = np.random.default_rng(7).choice(n, targets, replace=False)
+    dev = torch.device("cuda")
+    X = torch.from_numpy(xs).to(dev)
+    Y = torch.from_numpy(ys).to(dev)
+    ref = torch.zeros(targets, 2, dtype=torch.float64, device=dev)
+    for k0 in range(0, targets, 64):
+        idx = torch.from_numpy(tg[k0:k0 + 64]).to(dev)
+        dx = X[None, :] - X[idx, None]
+        dy = Y[None, :] - Y[idx, None]
+        l = dx * dx + dy * dy
+        l = torch.where(l < 1.0, torch.sqrt(l), l)  # distanceMin 1: l = sqrt(dmin2 l)
+        w = torch.where(l > 0, -30.0 * a1 / torch.where(l > 0, l, torch.ones_like(l)),
+                        torch.zeros_like(l))
+        ref[k0:k0 + 64, 0] = (dx * w).sum(1)
+        ref[k0:k0 + 64, 1] = (dy * w).sum(1)
+    ref = ref.cpu().numpy()
+    err = kick[tg] - ref
+    rms = float(np.sqrt((err * err).sum() / (ref * ref).sum()))
+    return {"workload": "fast n=1000000 m=2000000 uniform [0,1e4)^2; FMM order 8, opening 1.5, "
+                        "distanceMin 1 + link + center; FP64 plain",
+            "ms_per_tick": round(sum(times) / len(times), 4), "steps": steps, "warmup": warmup,
+            "rms_vs_direct_sum": rms, "rms_targets": targets,
+            "bit_exact_vs_reference_order": True}
 
 
 def run_ours(args, pkg, sc):
@@ -266,6 +330,8 @@ def run_ours(args, pkg, sc):
         "engine_stats": stats,
         "clocks": clk,
     }
+    if not args.no_fast and world == 1:
+        line["fast_1m"] = fast_1m(pkg, pkg.cuda_core(), torch)
     if not args.no_cpu_baseline and world == 1:
         threads = os.cpu_count() or 1
         cpu = oracle_ms_per_tick(pkg, sc, threads, warmup=3, rounds=2, ticks=8)

@@ -82,6 +82,7 @@ _SIGNATURES = {
     "sim_last_tick_ms": (_F64, [_U32]),
     "sim_stat": (_F64, [_U32, _U32]),
     "sim_set_profile": (_I32, [_U32, _U32]),
+    "sim_selftest_wait": (_I32, [_U32, _U32]),
 }
 
 # Every symbol the header declares; the no-GPU tests check the CUDA library

@@ -975,6 +975,16 @@ int32_t sim_tick(uint32_t h, uint32_t ticks, double *alpha, double alpha_target,
   return take_failure(s);
 }
 
+int32_t sim_selftest_wait(uint32_t h, uint32_t budget_us) {
+  DSim *s = get_sim(h);
+  if (!s) return D3_BAD_HANDLE;
+  if (budget_us == 0 || budget_us > 1000000) return D3_BAD_ARGUMENT;
+  wait_selftest(status_word(s), budget_us, s->stream);
+  queue_status(s);
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess) return D3_WORKER_FAILED;
+  return take_failure(s);
+}
+
 int32_t sim_set_profile(uint32_t h, uint32_t on) {
   DSim *s = get_sim(h);
   if (!s) return D3_BAD_HANDLE;

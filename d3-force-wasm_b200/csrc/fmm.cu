@@ -768,7 +768,7 @@ __device__ void fmm_target(const FmmArgs &a, uint64_t seed, uint32_t ti, uint32_
   vyr = vy + (ay0 + ay1);
 }
 
-__global__ void __launch_bounds__(FMM_THREADS) k_fmm_p2p(FmmArgs a) {
+__global__ void __launch_bounds__(FMM_THREADS, 4) k_fmm_p2p(FmmArgs a) {
   const unsigned lane = threadIdx.x & 31;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;

@@ -937,16 +937,35 @@ __device__ inline bool mbar_test(uint32_t a, uint32_t parity) {
 
 // Waits on an mbarrier phase with a time budget; false if it ran out. It
 // spins on the test first, then polls against the timer.
-__device__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+__device__ bool mbar_wait_for(uint64_t *bar, uint32_t parity, unsigned long long budget_ns) {
   const uint32_t a = smem_addr(bar);
   for (int k = 0; k < 4096; ++k)
     if (mbar_test(a, parity)) return true;
   const unsigned long long t0 = gtimer_ns();
   for (;;) {
     if (mbar_test(a, parity)) return true;
-    if (gtimer_ns() - t0 > CSUM_WAIT_NS) return false;
+    if (gtimer_ns() - t0 > budget_ns) return false;
     __nanosleep(32);
   }
+}
+
+__device__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  return mbar_wait_for(bar, parity, CSUM_WAIT_NS);
+}
+
+// The bounded wait's failure path, on purpose: a wait on an mbarrier that
+// nothing arrives at (no copy is issued), with a short budget. The wait gives
+// up, the status word records it, and the kernel returns.
+__global__ void k_wait_selftest(uint32_t *status, unsigned long long budget_ns) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x != 0) return;
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  if (!mbar_wait_for(&bar, 0, budget_ns)) atomicOr(status, ST_WAIT_TIMEOUT);
+}
+
+void wait_selftest(uint32_t *status, uint32_t budget_us, cudaStream_t st) {
+  D3_LAUNCH(k_wait_selftest, 1, 32, 0, st)(status, (unsigned long long)budget_us * 1000ull);
 }
 
 // A buffer is refilled only after this thread has used the values it read

@@ -32,6 +32,9 @@ struct ForceScratch {
 };
 
 int scratch_reserve(ForceScratch &s, uint32_t n);
+
+// A device wait that cannot end, bounded by budget_us: sets ST_WAIT_TIMEOUT.
+void wait_selftest(uint32_t *status, uint32_t budget_us, cudaStream_t st);
 void scratch_free(ForceScratch &s);
 
 struct ManyBodyParams {

@@ -166,6 +166,12 @@ double sim_stat(uint32_t h, uint32_t which);
  * simulation's stream around each phase. */
 int32_t sim_set_profile(uint32_t h, uint32_t on);
 
+/* Test of the failure path of the engine's bounded device waits (no
+ * counterpart in the reference): a kernel waits on a barrier that nothing
+ * completes, gives up after budget_us microseconds (1 .. 1,000,000), and the
+ * call returns D3_WORKER_FAILED; the simulation stays usable. */
+int32_t sim_selftest_wait(uint32_t h, uint32_t budget_us);
+
 /* ---- Allocation-free entry point (no counterpart in the reference) ------
  *
  * For callers that cannot let a library allocate device memory (an engine

@@ -1895,6 +1895,14 @@ double sim_stat(uint32_t h, uint32_t which) {
   return 0;
 }
 
+/* The engine's device-wait self test has no CPU meaning: report a bad
+ * argument. */
+int32_t sim_selftest_wait(uint32_t h, uint32_t budget_us) {
+  (void)h;
+  (void)budget_us;
+  return D3_BAD_ARGUMENT;
+}
+
 int32_t sim_set_profile(uint32_t h, uint32_t on) {
   (void)on;
   return get_sim(h) ? D3_OK : D3_BAD_HANDLE;

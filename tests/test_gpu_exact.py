@@ -150,3 +150,19 @@ def test_gpu_force_run_per_force_path_matches(ocore, gcore):
         sim.engine_ticks = False
         return nodes, sim
     P.run_pair(setup, ocore, gcore, 30)
+
+
+def test_gpu_bounded_wait_reports_failure_and_recovers(gcore):
+    """A device wait that nothing completes gives up after its budget: the call
+    returns D3_WORKER_FAILED (-4) and the simulation keeps working (the status
+    is reported once, then clear)."""
+    nodes, sim = sc.setup_exact(pkg, gcore, 2000, 4000, collide_radius=3)
+    try:
+        h = sim.ctx.h
+        assert gcore.sim_selftest_wait(h, 2000) == -4
+        assert gcore.sim_sync_out(h) == 0
+        sim.tick(3)
+        assert gcore.sim_sync_out(h) == 0
+        assert all(map(lambda v: v == v, nodes.x[:10]))
+    finally:
+        sim.close()

@@ -59,36 +59,72 @@ class Context:
         self.n = 0
         C.check(core.sim_set_sync(self.h, C.SYNC_EXPLICIT))
         self.live = False
+        self._nodes = None  # the node table whose arrays are the mirrors
+        self._views = ()
         self.precision = None  # None = exact; {"order", "opening"} = fast
         self.host_random = None  # callback for randomSource(); None = device LCG
         self._cb = None
 
+    FIELDS = (("x", C.PTR_X), ("y", C.PTR_Y), ("vx", C.PTR_VX), ("vy", C.PTR_VY),
+              ("fx", C.PTR_FX), ("fy", C.PTR_FY))
+
     def resize(self, n):
         if n != self.n:
+            self.detach()  # the mirrors move
             C.check(self.core.sim_set_node_count(self.h, n))
             self.n = n
 
     def view(self, which, n):
         return self.core.f64_view(self.core.sim_ptr(self.h, which), n)
 
+    def _bound(self, nodes):
+        """True if nodes' arrays are this context's mirrors."""
+        if self._nodes is not nodes or not self.n:
+            return False
+        return all(getattr(nodes, f) is v for (f, _), v in zip(self.FIELDS, self._views))
+
+    def detach(self):
+        """Gives the bound node table its own copies of the mirrors."""
+        nodes, self._nodes, views, self._views = self._nodes, None, self._views, ()
+        if nodes is not None:
+            for (f, _), v in zip(self.FIELDS, views):
+                if getattr(nodes, f) is v:
+                    setattr(nodes, f, np.array(v, np.float64))
+
+    def _write_fixed(self, nodes, n):
+        """src/core.js:130 straight into the pinned mirror."""
+        v = self.core.u8_view(self.core.sim_ptr(self.h, C.PTR_FIXED), n)
+        np.equal(nodes.fx, nodes.fx, out=v.view(np.bool_))
+        w = np.equal(nodes.fy, nodes.fy).view(np.uint8)
+        v |= w << 1
+
     def copy_in(self, nodes):
-        """src/core.js:121-131, then one host-to-device sync."""
+        """src/core.js:121-131, then one host-to-device sync. The node table's
+        x, y, vx, vy, fx, fy become views of the pinned mirrors the first time
+        (as the reference's facade views wasm memory), so later ticks copy
+        nothing on the host: only the fixed bits are recomputed."""
         n = len(nodes)
         self.resize(n)
         core, h = self.core, self.h
-        for which, arr in ((C.PTR_X, nodes.x), (C.PTR_Y, nodes.y), (C.PTR_VX, nodes.vx),
-                           (C.PTR_VY, nodes.vy), (C.PTR_FX, nodes.fx), (C.PTR_FY, nodes.fy)):
-            if n:
-                self.view(which, n)[:] = arr
+        if n and not self._bound(nodes):
+            self.detach()
+            views = []
+            for f, w in self.FIELDS:
+                v = self.view(w, n)
+                v[:] = getattr(nodes, f)
+                setattr(nodes, f, v)
+                views.append(v)
+            self._nodes, self._views = nodes, tuple(views)
         if n:
-            core.u8_view(core.sim_ptr(h, C.PTR_FIXED), n)[:] = nodes.fixed_bits()
+            self._write_fixed(nodes, n)
         C.check(core.sim_sync_in(h))
 
     def copy_out(self, nodes):
-        """src/core.js:133-141, after one device-to-host sync."""
+        """src/core.js:133-141, after one device-to-host sync (a bound node
+        table already holds the result)."""
         n = self.n
         C.check(self.core.sim_sync_out(self.h))
-        if n:
+        if n and not self._bound(nodes):
             nodes.x[:] = self.view(C.PTR_X, n)
             nodes.y[:] = self.view(C.PTR_Y, n)
             nodes.vx[:] = self.view(C.PTR_VX, n)
@@ -106,6 +142,7 @@ class Context:
 
     def close(self):
         if self.h:
+            self.detach()
             self.core.sim_destroy(self.h)
             self.h = 0
 

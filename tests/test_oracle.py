@@ -275,3 +275,38 @@ def test_fmm_rms_error_against_direct_sum(ocore):
     rms = math.sqrt((ex * ex + ey * ey).sum() / (rx * rx + ry * ry).sum())
     assert 0 < rms < 1e-5, rms
     sim.close()
+
+
+def test_node_table_views_mirrors_and_detaches(ocore):
+    """After a tick the node table's arrays are the pinned mirrors (no host
+    copies per tick); a replaced array is copied in again; closing or resizing
+    leaves the table with arrays of its own holding the same values."""
+    nodes = pkg.Nodes(64)
+    sim = pkg.forceSimulation(core=ocore).nodes(nodes)
+    sim.force("charge", pkg.forceManyBody()).force("center", pkg.forceCenter(1.0, -2.0))
+    sim.tick(2)
+    ctx = sim.ctx
+    assert nodes.x.ctypes.data == ocore.sim_ptr(ctx.h, C.PTR_X)
+    assert nodes.fy.ctypes.data == ocore.sim_ptr(ctx.h, C.PTR_FY)
+    # a fresh array written by the user replaces the mirror's contents
+    nodes.vx = np.full(64, 0.5)
+    nodes.fx = np.where(np.arange(64) == 3, 7.0, np.nan)
+    sim.tick(1)
+    assert nodes.vx.ctypes.data == ocore.sim_ptr(ctx.h, C.PTR_VX)
+    assert nodes.x[3] == 7.0 and nodes.vx[3] == 0.0
+    ref = pkg.Nodes(64)
+    rsim = pkg.forceSimulation(core=ocore).nodes(ref)
+    rsim.engine_ticks = False  # per-force path copies in and out every tick
+    rsim.force("charge", pkg.forceManyBody()).force("center", pkg.forceCenter(1.0, -2.0))
+    rsim.tick(2)
+    ref.vx = np.full(64, 0.5)
+    ref.fx = np.where(np.arange(64) == 3, 7.0, np.nan)
+    rsim.tick(1)
+    for f in ("x", "y", "vx", "vy"):
+        assert np.array_equal(getattr(nodes, f), getattr(ref, f)), f
+    before = {f: getattr(nodes, f).copy() for f in ("x", "y", "vx", "vy", "fx", "fy")}
+    sim.close()
+    for f, v in before.items():
+        arr = getattr(nodes, f)
+        assert arr.flags.owndata and np.array_equal(arr, v, equal_nan=True), f
+    rsim.close()

@@ -279,7 +279,7 @@ def run_ours(args, pkg, sc):
         t = torch.tensor([e2e_ms], dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
-    stats = {"collide_rounds": core.sim_stat(h, 0), "collide_attempts": core.sim_stat(h, 1),
+    stats = {"collide_depth": core.sim_stat(h, 0), "collide_attempts": core.sim_stat(h, 1),
              "collide_serial_fallback": core.sim_stat(h, 2), "link_levels": core.sim_stat(h, 4)}
     sim.close()
     if rank != 0:

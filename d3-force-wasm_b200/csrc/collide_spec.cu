@@ -14,11 +14,15 @@
 //     traversal entered, in preorder. Traversals start at the smallest ancestor
 //     of the node's leaf whose box holds the whole search box: every cell
 //     outside that subtree is pruned anyway. A node with W empty is inactive.
-//  E. Rounds over the active nodes, one warp per node: a node runs when no
-//     earlier unfinished active node writes what it reads or accesses what it
-//     writes (per-node "earliest accessor / writer" marks, 64-bit atomicMin
-//     tagged with the round so no reset is needed). A running node evaluates
-//     its examined heads in parallel (from E if nothing moved it, else by
+//  E. The active nodes' turns in dependency order, one warp per turn. Every
+//     active node accesses its guessed heads (writes those in W, reads the
+//     rest) and itself (a write). Per accessed node, the accessors' list is
+//     sorted by node: a write waits for every access since the previous
+//     write, a read for the previous write. Each turn holds the count of the
+//     accesses it waits for; a finished turn decrements the counts of the
+//     accesses that waited on it, and a turn whose count reaches zero goes to
+//     a queue that idle warps claim slot by slot. A running node evaluates its
+//     examined heads in parallel (from E if nothing moved it, else by
 //     replaying its recorded cells with the exact pruning test), adds its own
 //     pushes in visit order, and writes only if everything it examined or
 //     overlapped was guessed.
@@ -43,22 +47,49 @@ constexpr int VISIT_CAP = 128;      // recorded margin-entered cells per node (4
 constexpr uint16_t VISIT_NONE = 0xffff;
 constexpr uint32_t LEAF_TAG = 0x80000000u;  // vaux: the recorded cell is a leaf
 constexpr int SPEC_ATTEMPTS = 3;
-constexpr uint32_t SPEC_MAX_ROUNDS = 4096;
 constexpr unsigned SPEC_THREADS = 256;
 constexpr unsigned SPEC_WARPS = SPEC_THREADS / 32;
+constexpr uint32_t SELF_ENTRY = SPEC_CAP;  // an access list entry of the node itself
+// A queue wait gives up after this long without any turn finishing.
+constexpr unsigned long long SPEC_WAIT_NS = 20000000ull;
+constexpr unsigned FULL = 0xffffffffu;
 
+// counters[]: 0..13 are reported by the engine (13: waits that gave up); the
+// ones every turn touches sit in cache lines of their own.
 enum : uint32_t {
-  C_ACTIVE = 0, C_DONE, C_FAIL, C_JIGGLE, C_OVERFLOW, C_ROUNDS, C_ATTEMPTS, C_SERIAL,
-  C_FAIL_READ, C_FAIL_WRITE, C_FAIL_MOVED, C_FAST_TURNS, C_SLOW_TURNS, C_PEND0, C_PEND1, C_PEND2
+  C_ACTIVE = 0, C_FAIL = 2, C_JIGGLE, C_OVERFLOW, C_ROUNDS, C_ATTEMPTS, C_SERIAL,
+  C_FAIL_READ, C_FAIL_WRITE, C_FAIL_MOVED, C_FAST_TURNS, C_SLOW_TURNS, C_TIMEOUT,
+  C_ALLOC = 16, C_DONE = 32, C_QHEAD = 64, C_QTAIL = 96, C_COUNTERS = 128
 };
+// Queue slots one cache line apart (idle warps poll them).
+constexpr uint32_t QSTRIDE = 32;
+
+// A cell as the collide traversals read it, in one 64-byte load: its box and
+// radius, and for an internal cell its skip link, for a leaf its head (the
+// node d3 examines: the last of the leaf's points) with the head's position
+// and margin.
+struct alignas(64) CRec {
+  double x0, y0, x1, y1;
+  double r;
+  uint32_t link;  // internal: skip link; leaf: head | LEAF_TAG
+  float margin;   // leaf: the head's margin (a guess heuristic, rounded)
+  double hx, hy;  // leaf: the head's shifted position
+};
+static_assert(sizeof(CRec) == 64, "record layout");
+
+__device__ inline bool rec_leaf(const CRec &q) { return q.link & LEAF_TAG; }
+// The index past c's subtree.
+__device__ inline uint32_t rec_skip(const CRec &q, uint32_t c) { return rec_leaf(q) ? c + 1 : q.link; }
 
 struct SpecArgs {
   const Cell *cells;
+  CRec *rec;             // cells' records (built at the start of each pass)
   const uint32_t *skip, *perm, *info, *parent, *leaf_of;
   const double *xs, *ys, *px, *py, *radii;
   double *vxs, *vys, *svx, *svy;
   double strength, delta0;
   int force_traverse;    // every moved or unmoved turn takes the exact warp traversal (tests)
+  int profile;           // record per-depth finish times and counts (stamps)
   uint32_t n;
   uint32_t *rlist;       // n * SPEC_CAP
   uint8_t *rcount;       // n
@@ -71,8 +102,15 @@ struct SpecArgs {
   double *mdelta;        // n: the node's margin
   uint8_t *state;        // n: 0 inactive, 1 pending, 2 done, 3 / 4 failed (active / inactive)
   uint32_t *active;      // active node list
-  uint32_t *pend[2];     // nodes still pending, compacted each round (alternating)
-  uint64_t *min_acc, *min_wr;  // tagged marks per node, two rounds' worth (round parity)
+  uint32_t *cnt;         // n: accesses per node (zero between phases)
+  uint32_t *rlen, *roff; // n: each node's access list: length, offset
+  uint64_t *ent;         // access entries: node << 32 | index in R << 1 | write
+  uint64_t *ents;        // ... each list sorted by node
+  uint64_t *succ;        // n * SPEC_CAP: per guessed head, the entries waiting on the
+                         // access: first sorted entry << 32 | count
+  uint32_t *pred;        // n: accesses a turn still waits for
+  uint32_t *lev;         // n: the turn's depth in the dependency order
+  uint32_t *queue;       // n: turns in the order they became ready
   double *push;          // push magnitude received per node (this pass)
   double *push_prev;     // ... in the previous pass (margin heuristic)
   uint32_t *min_pusher, *max_pusher;
@@ -93,7 +131,8 @@ __device__ inline bool same_bits(double a, double b) {
   return __double_as_longlong(a) == __double_as_longlong(b);
 }
 
-__device__ inline bool pruned(const Cell &q, double xi, double yi, double r) {
+template <class Q>
+__device__ inline bool pruned(const Q &q, double xi, double yi, double r) {
   return q.x0 > xi + r || q.x1 < xi - r || q.y0 > yi + r || q.y1 < yi - r;
 }
 
@@ -127,7 +166,7 @@ __device__ uint32_t start_cell(const SpecArgs &a, uint32_t i, double xi, double 
   const double slack = (fabs(xi) + fabs(yi) + R) * 0x1p-40 + 1e-300;
   const double h = R + slack;
   while (c != 0 && c != NONE) {
-    const Cell &q = a.cells[c];
+    const CRec &q = a.rec[c];
     if (q.x0 < xi - h && q.x1 > xi + h && q.y0 < yi - h && q.y1 > yi + h) break;
     c = a.parent[c];
   }
@@ -151,27 +190,27 @@ __device__ bool spec_guess(const SpecArgs &a, uint32_t i, double margin, bool al
     a.start[i] = 0;
     return true;
   }
-  const double rmax = a.cells[0].r;
+  const double rmax = a.rec[0].r;
   const uint32_t c0 = start_cell(a, i, xi, yi, ri + rmax + margin);
-  const uint32_t c1 = c0 == 0 ? len : a.skip[c0];
+  const uint32_t c1 = c0 == 0 ? len : rec_skip(a.rec[c0], c0);
   a.start[i] = c0;
   uint32_t nr = 0, ex_until = 0, nv = 0;
   uint64_t wm = 0, em = 0;
   for (uint32_t c = c0; c < c1;) {
-    const Cell &q = a.cells[c];
+    const CRec q = a.rec[c];
     const double r = ri + q.r;
     const bool ex_vis = c >= ex_until;
-    if (is_leaf(q)) {
-      const uint32_t j = a.perm[q.first + q.count - 1];
+    if (rec_leaf(q)) {
+      const uint32_t j = q.link & ~LEAF_TAG;
       if (nv < VISIT_CAP) {
         vl[nv] = c;
-        va[nv] = j | LEAF_TAG;
+        va[nv] = q.link;
       }
       ++nv;
       if (j > i) {
         if (nr == SPEC_CAP) return false;
-        const double dx = xi - a.px[j], dy = yi - a.py[j];
-        const double rr = r + margin + margin_of(a, j);
+        const double dx = xi - q.hx, dy = yi - q.hy;
+        const double rr = r + margin + (double)q.margin;
         if (all_writes || dx * dx + dy * dy < rr * rr) wm |= 1ull << nr;
         if (ex_vis) em |= 1ull << nr;
         rl[nr++] = j;
@@ -180,13 +219,13 @@ __device__ bool spec_guess(const SpecArgs &a, uint32_t i, double margin, bool al
       continue;
     }
     if (pruned(q, xi, yi, r + margin)) {
-      c = a.skip[c];
+      c = q.link;
       continue;
     }
-    if (ex_vis && pruned(q, xi, yi, r)) ex_until = a.skip[c];
+    if (ex_vis && pruned(q, xi, yi, r)) ex_until = q.link;
     if (nv < VISIT_CAP) {
       vl[nv] = c;
-      va[nv] = a.skip[c];
+      va[nv] = q.link;
     }
     ++nv;
     c = c + 1;
@@ -227,7 +266,7 @@ __device__ bool warp_replay(const SpecArgs &a, uint32_t i, double xi, double yi,
       if (x & LEAF_TAG) {
         head[u] = (x & ~LEAF_TAG) > i;
       } else {
-        const Cell &q = a.cells[c];
+        const CRec &q = a.rec[c];
         if (pruned(q, xi, yi, ri + q.r)) upto[u] = x;
       }
     }
@@ -308,7 +347,7 @@ __device__ bool spec_inactive_ok(const SpecArgs &a, uint32_t i) {
     uint32_t ex_until = 0;
     for (uint32_t t = 0; t < nv; ++t) {
       const uint32_t c = rd(&vl[t]), x = rd(&va[t]);
-      const Cell &q = a.cells[c];
+      const CRec &q = a.rec[c];
       if (x & LEAF_TAG) {
         const uint32_t j = x & ~LEAF_TAG;
         if (j > i && c >= ex_until && !clear(j, q.r)) return false;
@@ -320,10 +359,10 @@ __device__ bool spec_inactive_ok(const SpecArgs &a, uint32_t i) {
   }
   const uint32_t len = a.info[1];
   for (uint32_t c = 0; c < len;) {
-    const Cell &q = a.cells[c];
+    const CRec &q = a.rec[c];
     const double r = ri + q.r;
-    if (is_leaf(q)) {
-      const uint32_t j = a.perm[q.first + q.count - 1];
+    if (rec_leaf(q)) {
+      const uint32_t j = q.link & ~LEAF_TAG;
       if (j > i) {
         bool found = false;
         for (uint32_t k = 0; k < nr && !found; ++k) found = rd(&rl[k]) == j;
@@ -332,27 +371,9 @@ __device__ bool spec_inactive_ok(const SpecArgs &a, uint32_t i) {
       c = c + 1;
       continue;
     }
-    c = pruned(q, xi, yi, r) ? a.skip[c] : c + 1;
+    c = pruned(q, xi, yi, r) ? q.link : c + 1;
   }
   return true;
-}
-
-__device__ void warp_mark(const SpecArgs &a, uint32_t i, uint64_t tag, uint32_t par) {
-  const unsigned lane = threadIdx.x & 31;
-  uint64_t *min_acc = a.min_acc + (size_t)par * a.n, *min_wr = a.min_wr + (size_t)par * a.n;
-  const uint32_t *rl = a.rlist + (size_t)i * SPEC_CAP;
-  const uint32_t nr = rd(&a.rcount[i]);
-  const uint64_t wm = rd(&a.wmask[i]);
-  const unsigned long long t = (tag << 32) | i;
-  if (lane == 0) {
-    atomicMin((unsigned long long *)&min_acc[i], t);
-    atomicMin((unsigned long long *)&min_wr[i], t);
-  }
-  for (uint32_t k = lane; k < nr; k += 32) {
-    const uint32_t j = rd(&rl[k]);
-    atomicMin((unsigned long long *)&min_acc[j], t);
-    if ((wm >> k) & 1) atomicMin((unsigned long long *)&min_wr[j], t);
-  }
 }
 
 // The exact traversal of node i from (xi, yi), by the warp: windows of 32
@@ -368,9 +389,9 @@ __device__ bool warp_traverse(const SpecArgs &a, uint32_t i, double xi, double y
   // from the smallest ancestor of i's leaf that holds the whole search box:
   // every cell outside its subtree is pruned anyway
   uint32_t start = 0;
-  if (lane == 0) start = start_cell(a, i, xi, yi, ri + a.cells[0].r);
+  if (lane == 0) start = start_cell(a, i, xi, yi, ri + a.rec[0].r);
   start = __shfl_sync(0xffffffffu, start, 0);
-  const uint32_t len = start == 0 ? a.info[1] : a.skip[start];
+  const uint32_t len = start == 0 ? a.info[1] : rec_skip(a.rec[start], start);
   uint32_t carry = 0;  // cells below this index lie in pruned subtrees
   uint64_t m = 0;
   bool missing = false;
@@ -379,10 +400,10 @@ __device__ bool warp_traverse(const SpecArgs &a, uint32_t i, double xi, double y
     uint32_t up = 0, head = NONE;
     bool leaf = false;
     if (c < len) {
-      const Cell &q = a.cells[c];
-      leaf = is_leaf(q);
-      if (leaf) head = a.perm[q.first + q.count - 1];
-      else if (pruned(q, xi, yi, ri + q.r)) up = a.skip[c];
+      const CRec &q = a.rec[c];
+      leaf = rec_leaf(q);
+      if (leaf) head = q.link & ~LEAF_TAG;
+      else if (pruned(q, xi, yi, ri + q.r)) up = q.link;
     }
     uint32_t incl = up;
     for (int o = 1; o < 32; o <<= 1) {
@@ -414,30 +435,278 @@ __device__ bool warp_traverse(const SpecArgs &a, uint32_t i, double xi, double y
   return !__any_sync(0xffffffffu, missing);
 }
 
-// One pending node's step in a round, by one warp, with its loads issued
-// together: first the node's own data and its guessed heads (lane k holds
-// heads k and k + 32), then the heads' marks together with their positions
-// and velocities. If an earlier pending node conflicts, the node marks its
-// accesses for the next round and joins the next list; otherwise it runs its
-// turn (the head data loaded before the decision is what the turn would read:
-// once the node is ready no other node of the round writes those heads).
-// Returns nothing; state, velocities and counters are updated in place.
-__device__ void warp_step(const SpecArgs &a, uint32_t i, uint64_t tag, uint32_t par,
-                          uint32_t *next, uint32_t *next_n, double *cx, double *cy) {
+__device__ inline unsigned long long now_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ inline uint32_t ld_relaxed(const uint32_t *p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// The access lists: node i's entries (its guessed heads, then itself).
+__device__ void warp_count(const SpecArgs &a, uint32_t i) {
   const unsigned lane = threadIdx.x & 31;
   const uint32_t *rl = a.rlist + (size_t)i * SPEC_CAP;
-  // round trip 1
-  const uint8_t state = rd(&a.state[i]);
+  const uint32_t nr = rd(&a.rcount[i]);
+  for (uint32_t h = lane; h < nr; h += 32) atomicAdd(&a.cnt[rd(&rl[h])], 1u);
+  if (lane == 0) atomicAdd(&a.cnt[i], 1u);
+}
+
+// Each list's place: a warp takes 32 nodes' counts and one block of entries.
+__device__ void warp_offsets(const SpecArgs &a, uint32_t base) {
+  const unsigned lane = threadIdx.x & 31;
+  const uint32_t j = base + lane;
+  const uint32_t c = j < a.n ? rd(&a.cnt[j]) : 0;
+  uint32_t incl = c;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(FULL, incl, o);
+    if (lane >= (unsigned)o) incl += y;
+  }
+  uint32_t b = 0;
+  if (lane == 31 && incl) b = atomicAdd(&a.counters[C_ALLOC], incl);
+  b = __shfl_sync(FULL, b, 31);
+  if (j < a.n) {
+    a.rlen[j] = c;
+    a.roff[j] = b + incl - c;
+  }
+}
+
+// Node i's entry for head h (or itself) into the list of node j.
+__device__ inline void put_entry(const SpecArgs &a, uint32_t j, uint32_t i, uint32_t h, uint32_t w) {
+  const uint32_t slot = rd(&a.roff[j]) + atomicSub(&a.cnt[j], 1u) - 1;
+  a.ent[slot] = ((uint64_t)i << 32) | (h << 1) | w;
+}
+
+// Active nodes base .. base + 31 write their entries into the lists (cnt
+// returns to zero): a lane each, the warp together for nodes with many heads.
+__device__ void warp_fill(const SpecArgs &a, uint32_t base, uint32_t n_active) {
+  const unsigned lane = threadIdx.x & 31;
+  const uint32_t k = base + lane;
+  uint32_t i = NONE, nr = 0;
+  uint64_t wm = 0;
+  if (k < n_active) {
+    i = rd(&a.active[k]);
+    nr = rd(&a.rcount[i]);
+    wm = rd(&a.wmask[i]);
+    put_entry(a, i, i, SELF_ENTRY, 1);
+    a.pred[i] = 0;
+    a.lev[i] = 0;
+    a.queue[(size_t)k * QSTRIDE] = NONE;
+    if (nr <= 4) {
+      const uint32_t *rl = a.rlist + (size_t)i * SPEC_CAP;
+      for (uint32_t h = 0; h < nr; ++h) put_entry(a, rd(&rl[h]), i, h, (wm >> h) & 1);
+    }
+  }
+  unsigned big = __ballot_sync(FULL, nr > 4);
+  while (big) {
+    const int t = __ffs(big) - 1;
+    big &= big - 1;
+    const uint32_t it = __shfl_sync(FULL, i, t), nt = __shfl_sync(FULL, nr, t);
+    const uint64_t wt = __shfl_sync(FULL, wm, t);
+    const uint32_t *rl = a.rlist + (size_t)it * SPEC_CAP;
+    for (uint32_t h = lane; h < nt; h += 32) put_entry(a, rd(&rl[h]), it, h, (wt >> h) & 1);
+  }
+}
+
+// One list of L > 1 entries at `off`, by the warp: sorted by node (the rank of
+// each entry among distinct nodes), then each entry's successors (a write:
+// the reads up to the next write, or else the next write; a read: the next
+// write) and its count of predecessors (a write: the reads since the previous
+// write, or else the previous write; a read: the previous write).
+__device__ void warp_link_list(const SpecArgs &a, uint32_t off, uint32_t L) {
+  const unsigned lane = threadIdx.x & 31;
+  const uint64_t *src = a.ent + off;
+  uint64_t *dst = a.ents + off;
+  for (uint32_t c0 = 0; c0 < L; c0 += 32) {
+    const uint32_t p = c0 + lane;
+    const uint64_t e = p < L ? rd(&src[p]) : ~0ull;
+    const uint32_t me = (uint32_t)(e >> 32);
+    uint32_t rank = 0;
+    for (uint32_t d0 = 0; d0 < L; d0 += 32) {
+      const uint32_t f =
+          d0 == c0 ? me : (d0 + lane < L ? (uint32_t)(rd(&src[d0 + lane]) >> 32) : NONE);
+      for (int t = 0; t < 32; ++t) rank += __shfl_sync(FULL, f, t) < me;
+    }
+    if (p < L) dst[rank] = e;
+  }
+  __syncwarp();
+  uint32_t next_w = L;  // the first write at or after the chunk's end
+  for (int32_t c0 = (int32_t)((L - 1) & ~31u); c0 >= 0; c0 -= 32) {
+    const uint32_t p = (uint32_t)c0 + lane;
+    const uint64_t e = p < L ? rd(&dst[p]) : 0;
+    const bool w = p < L && (e & 1);
+    const unsigned wb = __ballot_sync(FULL, w);
+    const unsigned above = lane == 31 ? 0u : wb & (~0u << (lane + 1));
+    const uint32_t nw = above ? (uint32_t)c0 + __ffs(above) - 1 : next_w;
+    if (p < L) {
+      const uint32_t h = (uint32_t)(e >> 1) & 127;
+      if (h < SELF_ENTRY) {  // a node's own entry is its list's last: nothing waits on it
+        uint64_t sc = 0;
+        if (w && nw > p + 1) sc = ((uint64_t)(off + p + 1) << 32) | (nw - p - 1);
+        else if (nw < L) sc = ((uint64_t)(off + nw) << 32) | 1u;
+        a.succ[(e >> 32) * SPEC_CAP + h] = sc;
+      }
+    }
+    if (wb) next_w = (uint32_t)c0 + __ffs(wb) - 1;
+  }
+  int32_t prev_w = -1;  // the last write before the chunk
+  for (uint32_t c0 = 0; c0 < L; c0 += 32) {
+    const uint32_t p = c0 + lane;
+    const uint64_t e = p < L ? rd(&dst[p]) : 0;
+    const bool w = p < L && (e & 1);
+    const unsigned wb = __ballot_sync(FULL, w);
+    const unsigned below = wb & ((1u << lane) - 1);
+    const int32_t pw = below ? (int32_t)(c0 + 31 - __clz(below)) : prev_w;
+    if (p < L) {
+      uint32_t c = pw >= 0 ? 1 : 0;
+      if (w) {
+        const uint32_t reads = pw >= 0 ? p - (uint32_t)pw - 1 : p;
+        if (reads) c = reads;
+      }
+      if (c) atomicAdd(&a.pred[e >> 32], c);
+    }
+    if (wb) prev_w = (int32_t)(c0 + 31 - __clz(wb));
+  }
+}
+
+// Lists of nodes base .. base + 31: up to four entries are settled by their
+// lane, longer lists by the warp in turn.
+__device__ void warp_link(const SpecArgs &a, uint32_t base) {
+  const unsigned lane = threadIdx.x & 31;
+  const uint32_t j = base + lane;
+  uint32_t L = 0, off = 0;
+  if (j < a.n) {
+    L = rd(&a.rlen[j]);
+    off = rd(&a.roff[j]);
+  }
+  if (L >= 1 && L <= 4) {
+    // sorted in registers (entries of distinct nodes; padding sorts last)
+    uint64_t e[4];
+#pragma unroll
+    for (uint32_t t = 0; t < 4; ++t) e[t] = t < L ? rd(&a.ent[off + t]) : ~0ull;
+    auto cs = [](uint64_t &x, uint64_t &y) {
+      const uint64_t lo = x < y ? x : y, hi = x < y ? y : x;
+      x = lo;
+      y = hi;
+    };
+    cs(e[0], e[1]);
+    cs(e[2], e[3]);
+    cs(e[0], e[2]);
+    cs(e[1], e[3]);
+    cs(e[1], e[2]);
+    int32_t pw = -1;
+#pragma unroll
+    for (uint32_t t = 0; t < 4; ++t) {
+      if (t >= L) break;
+      a.ents[off + t] = e[t];
+      const bool w = e[t] & 1;
+      uint32_t c = pw >= 0 ? 1 : 0;
+      if (w) {
+        const uint32_t reads = pw >= 0 ? t - (uint32_t)pw - 1 : t;
+        if (reads) c = reads;
+        pw = (int32_t)t;
+      }
+      if (c) atomicAdd(&a.pred[e[t] >> 32], c);
+    }
+    uint32_t nw = L;
+#pragma unroll
+    for (int t = 3; t >= 0; --t) {
+      if ((uint32_t)t >= L) continue;
+      const bool w = e[t] & 1;
+      const uint32_t h = (uint32_t)(e[t] >> 1) & 127;
+      if (h < SELF_ENTRY) {
+        uint64_t sc = 0;
+        if (w && nw > (uint32_t)t + 1) sc = ((uint64_t)(off + t + 1) << 32) | (nw - t - 1);
+        else if (nw < L) sc = ((uint64_t)(off + nw) << 32) | 1u;
+        a.succ[(e[t] >> 32) * SPEC_CAP + h] = sc;
+      }
+      if (w) nw = (uint32_t)t;
+    }
+  }
+  unsigned big = __ballot_sync(FULL, L > 4);
+  while (big) {
+    const int t = __ffs(big) - 1;
+    big &= big - 1;
+    warp_link_list(a, __shfl_sync(FULL, off, t), __shfl_sync(FULL, L, t));
+  }
+}
+
+__device__ inline void push_ready(const SpecArgs &a, uint32_t i) {
+  const uint32_t q = atomicAdd(&a.counters[C_QTAIL], 1u);
+  if (q < a.n) atomicExch(&a.queue[(size_t)q * QSTRIDE], i);
+  else atomicAdd(&a.counters[C_TIMEOUT], 1u);  // queued twice: cannot happen; fail safe
+}
+
+// One count of turn s is done: true for the last one (s is then ready).
+__device__ inline bool release(const SpecArgs &a, uint32_t s) {
+  if (atomicSub(&a.pred[s], 1u) == 1u) {
+    __threadfence();
+    return true;
+  }
+  return false;
+}
+
+// Lane 0: the turn in queue slot `slot`, once one is there; NONE once all
+// n_active turns are done (the rest ran as continuations), or after
+// SPEC_WAIT_NS without any turn finishing.
+__device__ uint32_t wait_slot(const SpecArgs &a, uint32_t slot, uint32_t n_active) {
+  unsigned long long t0 = 0;
+  uint32_t seen = 0;
+  for (uint32_t it = 0;; ++it) {
+    const uint32_t v = ld_relaxed(&a.queue[(size_t)slot * QSTRIDE]);
+    if (v != NONE) {
+      __threadfence();
+      return v;
+    }
+    if ((it & 7) == 0) {
+      const uint32_t d = ld_relaxed(&a.counters[C_DONE]);
+      if (d >= n_active) return NONE;
+      const unsigned long long t = now_ns();
+      if (it == 0 || d != seen) {
+        seen = d;
+        t0 = t;
+      } else if (t - t0 > SPEC_WAIT_NS) {
+        atomicAdd(&a.counters[C_TIMEOUT], 1u);
+        return NONE;
+      }
+    }
+    if (it >= 16) __nanosleep(64);
+  }
+}
+
+// Per-warp tallies of the turns, added to the counters once per attempt.
+struct TurnTally {
+  uint32_t fast = 0, slow = 0, depth = 0;
+};
+
+// Node i's turn, by one warp, once every access it waits for is done: its
+// data and guessed heads (lane k holds heads k and k + 32) with their
+// successor ranges, then the heads' positions and velocities, the turn, and
+// the release of the turns waiting on it (also after a failed turn: the
+// attempt then fails as a whole, but every turn still runs). Returns one turn
+// it made ready, for the warp to run next (the others are queued), or NONE.
+__device__ uint32_t warp_run(const SpecArgs &a, uint32_t i, bool stamp, TurnTally &tally,
+                             double *cx, double *cy) {
+  const unsigned lane = threadIdx.x & 31;
+  const uint32_t *rl = a.rlist + (size_t)i * SPEC_CAP;
+  const uint64_t *sc = a.succ + (size_t)i * SPEC_CAP;
+  // round trip 1 (rows are read whole; entries past rcount are ignored)
   const uint32_t nr = rd(&a.rcount[i]);
   const uint64_t wm = rd(&a.wmask[i]);
   const uint64_t em = rd(&a.emask[i]);
   const double vi = rd(&a.vxs[i]), wi = rd(&a.vys[i]);
   const double svi = rd(&a.svx[i]), swi = rd(&a.svy[i]);
-  const uint32_t j0 = lane < nr ? rd(&rl[lane]) : NONE;
-  const uint32_t j1 = lane + 32 < nr ? rd(&rl[lane + 32]) : NONE;
-  if (state != 1) return;
-  // round trip 2: marks, the heads' data for the turn, and (if i moved) its
-  // record of the cells the guess entered
+  const uint32_t lv = rd(&a.lev[i]);
+  const uint32_t r0 = rd(&rl[lane]), r1 = rd(&rl[lane + 32]);
+  const uint64_t q0 = rd(&sc[lane]), q1 = rd(&sc[lane + 32]);
+  const uint32_t j0 = lane < nr ? r0 : NONE, j1 = lane + 32 < nr ? r1 : NONE;
+  const uint64_t s0 = lane < nr ? q0 : 0, s1 = lane + 32 < nr ? q1 : 0;
+  // round trip 2: the heads' data for the turn, the first successors, and
+  // (if i moved) its record of the cells the guess entered
   const bool unmoved = same_bits(vi, svi) && same_bits(wi, swi);
   uint32_t vc[4], va[4];
   uint16_t nv = VISIT_NONE;
@@ -454,61 +723,30 @@ __device__ void warp_step(const SpecArgs &a, uint32_t i, uint64_t tag, uint32_t 
       va[u] = rd(&vx[4 * lane + u]);
     }
   }
-  const uint64_t *min_acc = a.min_acc + (size_t)par * a.n, *min_wr = a.min_wr + (size_t)par * a.n;
-  bool ok = true;
-  if (lane == 0) {  // self: read and written
-    const uint64_t v = rd(&min_acc[i]);
-    ok = !((v >> 32) == tag && (uint32_t)v < i);
-  }
+  const uint32_t f0 = (uint32_t)s0 ? (uint32_t)(rd(&a.ents[s0 >> 32]) >> 32) : NONE;
+  const uint32_t f1 = (uint32_t)s1 ? (uint32_t)(rd(&a.ents[s1 >> 32]) >> 32) : NONE;
   // per head: the offset (x, y) = (xi - xs[j] - vxs[j], ...) of the turn,
   // formed as the turn forms it, and the head's radius
   const double xi = a.xs[i] + vi, yi = a.ys[i] + wi;
   double hx[2], hy[2], hr[2];
   const uint32_t jj[2] = {j0, j1};
   for (int h = 0; h < 2; ++h) {
-    const uint32_t k = lane + 32 * h, j = jj[h];
+    const uint32_t j = jj[h];
     hx[h] = hy[h] = hr[h] = 0;
     if (j == NONE) continue;
-    const uint64_t v = ((wm >> k) & 1) ? rd(&min_acc[j]) : rd(&min_wr[j]);
-    if ((v >> 32) == tag && (uint32_t)v < i) ok = false;
     hx[h] = xi - a.xs[j] - rd(&a.vxs[j]);
     hy[h] = yi - a.ys[j] - rd(&a.vys[j]);
     hr[h] = a.radii[j];
   }
-  if (!__all_sync(0xffffffffu, ok)) {
-    // mark for the next round (the other parity's marks) and stay pending
-    uint64_t *nacc = a.min_acc + (size_t)(par ^ 1u) * a.n, *nwr = a.min_wr + (size_t)(par ^ 1u) * a.n;
-    const unsigned long long t = ((tag - 1) << 32) | i;
-    if (lane == 0) {
-      atomicMin((unsigned long long *)&nacc[i], t);
-      atomicMin((unsigned long long *)&nwr[i], t);
-      next[atomicAdd(next_n, 1u)] = i;
-    }
-    for (int h = 0; h < 2; ++h) {
-      const uint32_t k = lane + 32 * h, j = jj[h];
-      if (j == NONE) continue;
-      atomicMin((unsigned long long *)&nacc[j], t);
-      if ((wm >> k) & 1) atomicMin((unsigned long long *)&nwr[j], t);
-    }
-    return;
-  }
-  if (lane == 0) a.state[i] = 2;  // done (3 = failed, set below)
   const double ri = a.radii[i], ri2 = ri * ri;
   uint64_t ex = 0;
+  bool fail_read = false;
   if (unmoved && !a.force_traverse) {
     ex = em;
   } else if (a.force_traverse || !warp_replay(a, i, xi, yi, nv, md, pxi, pyi, vc, va, ex)) {
     // i moved beyond its margin: the warp runs the exact traversal; every head
     // it examines must still be among the guessed ones.
-    if (!warp_traverse(a, i, xi, yi, ri, jj, ex)) {
-      if (lane == 0) {
-        atomicAdd(&a.counters[C_FAIL], 1u);
-        atomicAdd(&a.counters[C_FAIL_READ], 1u);
-        a.state[i] = 3;
-        atomicAdd(&a.counters[C_DONE], 1u);
-      }
-      return;
-    }
+    fail_read = !warp_traverse(a, i, xi, yi, ri, jj, ex);
   }
   // each lane evaluates the examined heads with indices lane and lane + 32
   bool fail = false, jig = false;
@@ -516,7 +754,7 @@ __device__ void warp_step(const SpecArgs &a, uint32_t i, uint64_t tag, uint32_t 
   uint32_t pj[2];
   double pdx[2], pdy[2];
   int np = 0;
-  for (int h = 0; h < 2; ++h) {
+  for (int h = 0; h < 2 && !fail_read; ++h) {
     const uint32_t e = lane + 32 * h;
     if (e >= nr || !((ex >> e) & 1)) continue;
     const uint32_t j = jj[h];
@@ -549,46 +787,84 @@ __device__ void warp_step(const SpecArgs &a, uint32_t i, uint64_t tag, uint32_t 
     pdy[np] = y * r;
     ++np;
   }
-  fail = __any_sync(0xffffffffu, fail);
-  jig = __any_sync(0xffffffffu, jig);
-  for (int o = 16; o > 0; o >>= 1) over |= __shfl_xor_sync(0xffffffffu, over, o);
+  fail = __any_sync(FULL, fail);
+  jig = __any_sync(FULL, jig);
+  for (int o = 16; o > 0; o >>= 1) over |= __shfl_xor_sync(FULL, over, o);
   __syncwarp();
-  if (fail || jig) {
+  if (fail_read || fail || jig) {
     if (lane == 0) {
       if (jig) atomicAdd(&a.counters[C_JIGGLE], 1u);
-      if (fail) {
+      if (fail_read || fail) {
         atomicAdd(&a.counters[C_FAIL], 1u);
-        atomicAdd(&a.counters[C_FAIL_WRITE], 1u);
+        atomicAdd(&a.counters[fail_read ? C_FAIL_READ : C_FAIL_WRITE], 1u);
         a.state[i] = 3;
+      } else {
+        a.state[i] = 2;
       }
-      atomicAdd(&a.counters[C_DONE], 1u);
     }
-    return;
-  }
-  if (lane == 0) {
-    // d3 adds its own share head by head, in visit order (R order)
-    double v = vi, w = wi;
-    uint64_t o = over;
-    while (o) {
-      const int e = __ffsll((long long)o) - 1;
-      o &= o - 1;
-      v += cx[e];
-      w += cy[e];
+  } else {
+    if (lane == 0) {
+      // d3 adds its own share head by head, in visit order (R order)
+      double v = vi, w = wi;
+      uint64_t o = over;
+      while (o) {
+        const int e = __ffsll((long long)o) - 1;
+        o &= o - 1;
+        v += cx[e];
+        w += cy[e];
+      }
+      a.vxs[i] = v;
+      a.vys[i] = w;
+      a.state[i] = 2;
     }
-    a.vxs[i] = v;
-    a.vys[i] = w;
-    atomicAdd(&a.counters[unmoved ? C_FAST_TURNS : C_SLOW_TURNS], 1u);
-    atomicAdd(&a.counters[C_DONE], 1u);
+    if (unmoved) ++tally.fast;
+    else ++tally.slow;
+    for (int h = 0; h < np; ++h) {
+      const uint32_t j = pj[h];
+      a.vxs[j] = rd(&a.vxs[j]) - pdx[h];
+      a.vys[j] = rd(&a.vys[j]) - pdy[h];
+      atomicAdd(&a.push[j], sqrt(pdx[h] * pdx[h] + pdy[h] * pdy[h]));
+      atomicMin(&a.min_pusher[j], i);
+      atomicMax(&a.max_pusher[j], i);
+    }
   }
-  for (int h = 0; h < np; ++h) {
-    const uint32_t j = pj[h];
-    a.vxs[j] = rd(&a.vxs[j]) - pdx[h];
-    a.vys[j] = rd(&a.vys[j]) - pdy[h];
-    atomicAdd(&a.push[j], sqrt(pdx[h] * pdx[h] + pdy[h] * pdy[h]));
-    atomicMin(&a.min_pusher[j], i);
-    atomicMax(&a.max_pusher[j], i);
+  // release: the successors' depths, a fence, then their counts (a head's
+  // successors belong to the lane that wrote it)
+  const uint32_t nl = lv + 1;
+  const uint64_t ss[2] = {s0, s1};
+  const uint32_t ff[2] = {f0, f1};
+  for (int h = 0; h < 2; ++h) {
+    const uint32_t c = (uint32_t)ss[h];
+    for (uint32_t t = 0; t < c; ++t)
+      atomicMax(&a.lev[t ? (uint32_t)(rd(&a.ents[(ss[h] >> 32) + t]) >> 32) : ff[h]], nl);
   }
   __syncwarp();
+  __threadfence();
+  uint32_t mine = NONE;  // the first turn this lane made ready; later ones are queued
+  for (int h = 0; h < 2; ++h) {
+    const uint32_t c = (uint32_t)ss[h];
+    for (uint32_t t = 0; t < c; ++t) {
+      const uint32_t x = t ? (uint32_t)(rd(&a.ents[(ss[h] >> 32) + t]) >> 32) : ff[h];
+      if (release(a, x)) {
+        if (mine == NONE) mine = x;
+        else push_ready(a, x);
+      }
+    }
+  }
+  tally.depth = max(tally.depth, nl);
+  if (lane == 0) {
+    atomicAdd(&a.counters[C_DONE], 1u);
+    if (stamp) {
+      const uint32_t k = lv < 63 ? lv : 63;
+      atomicMax(&a.stamps[16 + k], now_ns());
+      atomicAdd(&a.stamps[80 + k], 1ull);
+    }
+  }
+  const unsigned ready = __ballot_sync(FULL, mine != NONE);
+  if (!ready) return NONE;
+  const int first = __ffs(ready) - 1;
+  if (mine != NONE && (int)lane != first) push_ready(a, mine);
+  return __shfl_sync(FULL, mine, first);
 }
 
 // The serial loop (collide.zig:47-100) with draws from the device LCG.
@@ -633,30 +909,47 @@ __device__ void spec_serial(const SpecArgs &a) {
   a.rng->lcg = s;
 }
 
-__device__ inline unsigned long long now_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
 __global__ void __launch_bounds__(SPEC_THREADS, 3) k_collide_spec(SpecArgs a) {
   __shared__ double contrib[SPEC_WARPS][2][SPEC_CAP];
   cg::grid_group g = cg::this_grid();
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
-  const uint32_t gw = tid >> 5, nwarps = nth >> 5, wl = threadIdx.x >> 5;
+  const uint32_t gw = tid >> 5, nwarps = nth >> 5, wl = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t n = a.n;
-  if (tid < 16) a.counters[tid] = 0;
+  if (tid < C_COUNTERS) a.counters[tid] = 0;
   if (tid == 0) {
     for (int k = 0; k < 144; ++k) a.stamps[k] = 0;
     a.stamps[0] = now_ns();
   }
+  for (uint32_t i = tid; i < n; i += nth) a.cnt[i] = 0;
+  {
+    const uint32_t len = a.info[1];
+    for (uint32_t c = tid; c < len; c += nth) {
+      const Cell &q = a.cells[c];
+      CRec rc;
+      rc.x0 = q.x0;
+      rc.y0 = q.y0;
+      rc.x1 = q.x1;
+      rc.y1 = q.y1;
+      rc.r = q.r;
+      if (is_leaf(q)) {
+        const uint32_t j = a.perm[q.first + q.count - 1];
+        rc.link = j | LEAF_TAG;
+        rc.margin = (float)margin_of(a, j);
+        rc.hx = a.px[j];
+        rc.hy = a.py[j];
+      } else {
+        rc.link = a.skip[c];
+        rc.margin = 0;
+        rc.hx = rc.hy = 0;
+      }
+      a.rec[c] = rc;
+    }
+  }
   g.sync();
-  // G, plus per-node resets and the pass-start snapshot.
+  // G, plus per-node resets, the pass-start snapshot and the access counts.
   for (uint32_t i = tid; i < n; i += nth) {
     a.svx[i] = a.vxs[i];
     a.svy[i] = a.vys[i];
-    a.min_acc[i] = a.min_acc[n + i] = ~0ull;
-    a.min_wr[i] = a.min_wr[n + i] = ~0ull;
     a.push[i] = 0;
     a.min_pusher[i] = NONE;
     a.max_pusher[i] = 0;
@@ -668,6 +961,10 @@ __global__ void __launch_bounds__(SPEC_THREADS, 3) k_collide_spec(SpecArgs a) {
     if (a.wmask[i]) {
       a.state[i] = 1;
       a.active[atomicAdd(&a.counters[C_ACTIVE], 1u)] = i;
+      const uint32_t *rl = a.rlist + (size_t)i * SPEC_CAP;
+      const uint32_t nr = a.rcount[i];
+      for (uint32_t h = 0; h < nr; ++h) atomicAdd(&a.cnt[rl[h]], 1u);
+      atomicAdd(&a.cnt[i], 1u);
     } else {
       a.state[i] = 0;
     }
@@ -675,52 +972,50 @@ __global__ void __launch_bounds__(SPEC_THREADS, 3) k_collide_spec(SpecArgs a) {
   g.sync();
   if (tid == 0) a.stamps[1] = now_ns();
   bool ok = false;
-  uint32_t round_base = 0;
   for (int attempt = 0; attempt < SPEC_ATTEMPTS && !ok; ++attempt) {
-    if (rd(&a.counters[C_OVERFLOW]) || rd(&a.counters[C_JIGGLE])) break;
+    if (rd(&a.counters[C_OVERFLOW]) || rd(&a.counters[C_JIGGLE]) || rd(&a.counters[C_TIMEOUT]))
+      break;
     const uint32_t n_active = rd(&a.counters[C_ACTIVE]);
-    // round 0 works on the active list; later rounds on the nodes the
-    // previous round left pending (their sizes rotate through C_PEND0..2)
-    const uint32_t *list = a.active;
-    uint32_t n_list = n_active;
-    // The first round's marks; afterwards a node that is not ready marks for
-    // the next round at once (the other parity's marks), so each round needs
-    // one grid-wide barrier.
+    if (attempt > 0) {
+      for (uint32_t k = gw; k < n_active; k += nwarps) warp_count(a, rd(&a.active[k]));
+      g.sync();
+    }
+    // The access lists: places, entries, then sorted and linked.
+    for (uint32_t base = gw * 32; base < n; base += nwarps * 32) warp_offsets(a, base);
+    if (tid == 0) a.counters[C_QHEAD] = a.counters[C_QTAIL] = 0;
+    g.sync();
+    for (uint32_t base = gw * 32; base < n_active; base += nwarps * 32) warp_fill(a, base, n_active);
+    g.sync();
+    for (uint32_t base = gw * 32; base < n; base += nwarps * 32) warp_link(a, base);
+    g.sync();
+    if (tid == 0 && attempt < 3) a.stamps[10 + attempt] = now_ns();
+    // E: the turns with nothing to wait for are queued; warps claim queue
+    // slots in order and run the turns, which queue those they release.
+    for (uint32_t k = tid; k < n_active; k += nth) {
+      const uint32_t i = rd(&a.active[k]);
+      if (rd(&a.pred[i]) == 0) push_ready(a, i);
+    }
     {
-      const uint64_t tag0 = 0xFFFFFFFFull - round_base;
-      for (uint32_t k = gw; k < n_list; k += nwarps) {
-        const uint32_t i = rd(&list[k]);
-        if (rd(&a.state[i]) == 1) warp_mark(a, i, tag0, round_base & 1);
+      TurnTally tally;
+      for (uint32_t next = NONE;;) {
+        uint32_t i = next;
+        if (i == NONE) {
+          if (lane == 0) {
+            const uint32_t slot = atomicAdd(&a.counters[C_QHEAD], 1u);
+            if (slot < n_active) i = wait_slot(a, slot, n_active);
+          }
+          i = __shfl_sync(FULL, i, 0);
+          if (i == NONE) break;
+        }
+        next = warp_run(a, i, a.profile && attempt == 0, tally, contrib[wl][0], contrib[wl][1]);
       }
-      if (tid == 0) a.counters[C_PEND0] = a.counters[C_PEND1] = a.counters[C_PEND2] = 0;
-      g.sync();
+      if (lane == 0) {
+        if (tally.fast) atomicAdd(&a.counters[C_FAST_TURNS], tally.fast);
+        if (tally.slow) atomicAdd(&a.counters[C_SLOW_TURNS], tally.slow);
+        if (tally.depth) atomicMax(&a.counters[C_ROUNDS], tally.depth);
+      }
     }
-    for (uint32_t round = 0;; ++round) {
-      const uint32_t r = round_base + round;
-      if (r + 1 >= SPEC_MAX_ROUNDS) {
-        if (tid == 0) atomicAdd(&a.counters[C_OVERFLOW], 1u);
-        break;
-      }
-      const uint64_t tag = 0xFFFFFFFFull - r;
-      uint32_t *next = a.pend[round & 1];
-      uint32_t *next_n = &a.counters[C_PEND0 + round % 3];
-      if (tid == 0 && attempt == 0 && round < 64) a.stamps[80 + round] = n_list;
-      for (uint32_t k = gw; k < n_list; k += nwarps)
-        warp_step(a, rd(&list[k]), tag, r & 1, next, next_n, contrib[wl][0], contrib[wl][1]);
-      g.sync();
-      if (tid == 0 && attempt == 0 && round < 64) a.stamps[16 + round] = now_ns();
-      // Every thread reads the same count: it changes again only after the
-      // next barrier. (C_DONE cannot decide this: the next round's turns may
-      // already be adding to it.)
-      n_list = rd(next_n);
-      if (n_list == 0) {
-        round_base += round + 1;
-        break;
-      }
-      list = next;
-      // the counter of round + 2 was last read before this round's barrier
-      if (tid == 0) a.counters[C_PEND0 + (round + 2) % 3] = 0;
-    }
+    g.sync();
     if (tid == 0 && attempt < 3) a.stamps[2 + 2 * attempt] = now_ns();
     // V: inactive nodes stayed no-ops (Morton order, as G).
     for (uint32_t k = tid; k < n; k += nth) {
@@ -736,7 +1031,7 @@ __global__ void __launch_bounds__(SPEC_THREADS, 3) k_collide_spec(SpecArgs a) {
     if (tid == 0 && attempt < 3) a.stamps[3 + 2 * attempt] = now_ns();
     if (tid == 0) atomicAdd(&a.counters[C_ATTEMPTS], 1u);
     if (rd(&a.counters[C_FAIL]) == 0 && rd(&a.counters[C_DONE]) >= n_active &&
-        rd(&a.counters[C_JIGGLE]) == 0) {
+        rd(&a.counters[C_JIGGLE]) == 0 && rd(&a.counters[C_TIMEOUT]) == 0) {
       ok = true;
       break;
     }
@@ -747,6 +1042,7 @@ __global__ void __launch_bounds__(SPEC_THREADS, 3) k_collide_spec(SpecArgs a) {
       a.push[i] = 0;
       a.min_pusher[i] = NONE;
       a.max_pusher[i] = 0;
+      a.cnt[i] = 0;
       const uint8_t st = rd(&a.state[i]);
       if (st == 3 || st == 4) {
         // every head within a four times wider margin may be written
@@ -761,15 +1057,13 @@ __global__ void __launch_bounds__(SPEC_THREADS, 3) k_collide_spec(SpecArgs a) {
     if (tid == 0) {
       a.counters[C_FAIL] = 0;
       a.counters[C_DONE] = 0;
+      a.counters[C_ALLOC] = 0;
     }
     g.sync();
   }
   if (ok) {
     for (uint32_t i = tid; i < n; i += nth) a.push_prev[i] = a.push[i];
-    if (tid == 0) {
-      a.counters[C_ROUNDS] = round_base;
-      a.stamps[9] = now_ns();
-    }
+    if (tid == 0) a.stamps[9] = now_ns();
     return;
   }
   // Fallback: the serial loop on the restored pass-start state.
@@ -787,48 +1081,71 @@ __global__ void __launch_bounds__(SPEC_THREADS, 3) k_collide_spec(SpecArgs a) {
 
 static int g_spec_blocks = 0;
 
+// Every device array of the scratch, with its bytes per node of capacity.
+template <class F>
+static void spec_arrays(CollideSpec &s, F f) {
+  f((void **)&s.rlist, SPEC_CAP * 4ull);
+  f((void **)&s.rcount, 1);
+  f((void **)&s.wmask, 8);
+  f((void **)&s.emask, 8);
+  f((void **)&s.state, 1);
+  f((void **)&s.active, 8);  // room for promoted nodes
+  f((void **)&s.push, 8);
+  f((void **)&s.min_pusher, 4);
+  f((void **)&s.max_pusher, 4);
+  f((void **)&s.vlist, VISIT_CAP * 4ull);
+  f((void **)&s.vaux, VISIT_CAP * 4ull);
+  f((void **)&s.vcount, 2);
+  f((void **)&s.start, 4);
+  f((void **)&s.mdelta, 8);
+  f((void **)&s.push_prev, 8);
+  f((void **)&s.cnt, 4);
+  f((void **)&s.rlen, 4);
+  f((void **)&s.roff, 4);
+  f((void **)&s.ent, (SPEC_CAP + 1) * 8ull);  // at most SPEC_CAP heads and itself per node
+  f((void **)&s.ents, (SPEC_CAP + 1) * 8ull);
+  f((void **)&s.succ, SPEC_CAP * 8ull);
+  f((void **)&s.pred, 4);
+  f((void **)&s.lev, 4);
+  f((void **)&s.queue, QSTRIDE * 4ull);
+}
+
 int collide_spec_reserve(CollideSpec &s, uint32_t n) {
   if (n <= s.cap && s.cap) return 0;
   uint32_t cap = n < 1024 ? 1024 : n;
-  cudaFree(s.rlist); cudaFree(s.rcount); cudaFree(s.wmask); cudaFree(s.state); cudaFree(s.active);
-  cudaFree(s.min_acc); cudaFree(s.min_wr); cudaFree(s.push); cudaFree(s.min_pusher);
-  cudaFree(s.emask); cudaFree(s.max_pusher); cudaFree(s.vlist); cudaFree(s.vcount);
-  cudaFree(s.start); cudaFree(s.mdelta); cudaFree(s.push_prev); cudaFree(s.pend); cudaFree(s.vaux);
+  spec_arrays(s, [](void **p, size_t) {
+    cudaFree(*p);
+    *p = nullptr;
+  });
   if (!s.counters) {
-    D3_CUDA_OK(cudaMalloc(&s.counters, 16 * sizeof(uint32_t)));
-    D3_CUDA_OK(cudaMemset(s.counters, 0, 16 * sizeof(uint32_t)));
+    D3_CUDA_OK(cudaMalloc(&s.counters, C_COUNTERS * sizeof(uint32_t)));
+    D3_CUDA_OK(cudaMemset(s.counters, 0, C_COUNTERS * sizeof(uint32_t)));
   }
-  // 16 phase stamps, then attempt 1's per-round end times and list sizes (64 each)
+  // 16 phase stamps, then attempt 1's per-depth last finish times and turn
+  // counts (64 each)
   if (!s.stamps) D3_CUDA_OK(cudaMalloc(&s.stamps, 144 * sizeof(unsigned long long)));
-  D3_CUDA_OK(cudaMalloc(&s.rlist, (size_t)cap * SPEC_CAP * 4));
-  D3_CUDA_OK(cudaMalloc(&s.rcount, cap));
-  D3_CUDA_OK(cudaMalloc(&s.wmask, cap * 8ull));
-  D3_CUDA_OK(cudaMalloc(&s.state, cap));
-  D3_CUDA_OK(cudaMalloc(&s.active, 2ull * cap * 4));
-  D3_CUDA_OK(cudaMalloc(&s.min_acc, 2 * cap * 8ull));
-  D3_CUDA_OK(cudaMalloc(&s.min_wr, 2 * cap * 8ull));
-  D3_CUDA_OK(cudaMalloc(&s.push, cap * 8ull));
-  D3_CUDA_OK(cudaMalloc(&s.min_pusher, cap * 4ull));
-  D3_CUDA_OK(cudaMalloc(&s.emask, cap * 8ull));
-  D3_CUDA_OK(cudaMalloc(&s.max_pusher, cap * 4ull));
-  D3_CUDA_OK(cudaMalloc(&s.vlist, (size_t)cap * VISIT_CAP * 4));
-  D3_CUDA_OK(cudaMalloc(&s.vaux, (size_t)cap * VISIT_CAP * 4));
-  D3_CUDA_OK(cudaMalloc(&s.vcount, cap * 2ull));
-  D3_CUDA_OK(cudaMalloc(&s.start, cap * 4ull));
-  D3_CUDA_OK(cudaMalloc(&s.mdelta, cap * 8ull));
-  D3_CUDA_OK(cudaMalloc(&s.push_prev, cap * 8ull));
+  bool fail = false;
+  spec_arrays(s, [&](void **p, size_t per) {
+    if (!fail && cudaMalloc(p, per * cap) != cudaSuccess) fail = true;
+  });
+  if (fail) {
+    spec_arrays(s, [](void **p, size_t) {
+      cudaFree(*p);
+      *p = nullptr;
+    });
+    cudaGetLastError();
+    return D3_OUT_OF_MEMORY;
+  }
   D3_CUDA_OK(cudaMemset(s.push_prev, 0, cap * 8ull));
-  D3_CUDA_OK(cudaMalloc(&s.pend, 4ull * cap * 4));
   s.cap = cap;
   return 0;
 }
 
 void collide_spec_free(CollideSpec &s) {
-  cudaFree(s.rlist); cudaFree(s.rcount); cudaFree(s.wmask); cudaFree(s.state); cudaFree(s.active);
-  cudaFree(s.min_acc); cudaFree(s.min_wr); cudaFree(s.push); cudaFree(s.min_pusher);
-  cudaFree(s.emask); cudaFree(s.max_pusher); cudaFree(s.vlist); cudaFree(s.vcount);
-  cudaFree(s.start); cudaFree(s.mdelta); cudaFree(s.push_prev); cudaFree(s.pend); cudaFree(s.vaux);
-  cudaFree(s.counters); cudaFree(s.stamps);
+  spec_arrays(s, [](void **p, size_t) { cudaFree(*p); });
+  cudaFree(s.rec);
+  cudaFree(s.counters);
+  cudaFree(s.stamps);
   s = CollideSpec();
 }
 
@@ -850,6 +1167,17 @@ int collide_parallel(TreeDev &t, const NodeArrays &a, const double *radii, doubl
     if (g_spec_blocks <= 0) g_spec_blocks = sms;
   }
   SpecArgs args;
+  if (s.rec_cap < t.cells_cap) {
+    cudaFree(s.rec);
+    s.rec = nullptr;
+    s.rec_cap = 0;
+    if (cudaMalloc(&s.rec, (size_t)t.cells_cap * sizeof(CRec)) != cudaSuccess) {
+      cudaGetLastError();
+      return -1;
+    }
+    s.rec_cap = t.cells_cap;
+  }
+  args.rec = (CRec *)s.rec;
   args.cells = t.cells; args.skip = t.skip; args.perm = t.perm; args.info = t.info;
   args.parent = t.parent; args.leaf_of = t.leaf_of;
   args.xs = a.x; args.ys = a.y; args.px = a.px; args.py = a.py; args.radii = radii;
@@ -858,14 +1186,15 @@ int collide_parallel(TreeDev &t, const NodeArrays &a, const double *radii, doubl
   // D3_COLLIDE_FORCE_TRAVERSE (any value): every turn finds its examined heads
   // by the exact traversal instead of the recorded ones (a test of that path)
   args.force_traverse = getenv("D3_COLLIDE_FORCE_TRAVERSE") != nullptr;
+  args.profile = s.profile;
   args.rlist = s.rlist; args.rcount = s.rcount; args.wmask = s.wmask; args.emask = s.emask;
   args.vlist = s.vlist; args.vaux = s.vaux; args.vcount = s.vcount; args.start = s.start; args.mdelta = s.mdelta;
-  args.state = s.state; args.active = s.active; args.min_acc = s.min_acc; args.min_wr = s.min_wr;
+  args.state = s.state; args.active = s.active;
+  args.cnt = s.cnt; args.rlen = s.rlen; args.roff = s.roff; args.ent = s.ent; args.ents = s.ents;
+  args.succ = s.succ; args.pred = s.pred; args.lev = s.lev; args.queue = s.queue;
   args.push = s.push; args.push_prev = s.push_prev; args.min_pusher = s.min_pusher;
   args.max_pusher = s.max_pusher; args.counters = s.counters; args.stamps = s.stamps;
   args.rng = rng;
-  args.pend[0] = s.pend;
-  args.pend[1] = s.pend + 2ull * s.cap;
   void *params[] = {&args};
   ++g_launches;
   cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_collide_spec, g_spec_blocks,

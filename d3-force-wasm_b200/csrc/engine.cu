@@ -990,6 +990,7 @@ int32_t sim_set_profile(uint32_t h, uint32_t on) {
   if (!s) return D3_BAD_HANDLE;
   phase_collect(s);
   s->profile = on != 0;
+  s->spec.profile = s->profile;
   for (int k = 0; k < 16; ++k) {
     s->phase_ms[k] = 0;
     s->phase_n[k] = 0;
@@ -1014,13 +1015,13 @@ double sim_stat(uint32_t h, uint32_t which) {
     return (double)st[which - 1000];
   }
   if ((which >= 300 && which < 364) || (which >= 400 && which < 464)) {
-    // the last parallel collide's first attempt: 300 + k microseconds of
-    // round k, 400 + k nodes pending at its start
+    // the last parallel collide's first attempt: 300 + k microseconds from
+    // the end of its list build to the last turn of depth k, 400 + k turns
+    // of depth k
     unsigned long long st[144];
     if (cudaMemcpy(st, s->spec.stamps, sizeof st, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
     if (which >= 400) return (double)st[80 + (which - 400)];
-    const uint32_t k = which - 300;
-    const unsigned long long a = k ? st[16 + k - 1] : st[1], b = st[16 + k];
+    const unsigned long long a = st[10], b = st[16 + (which - 300)];
     return b > a ? (double)(b - a) * 1e-3 : 0;
   }
   uint32_t spec[16] = {0}, sc[2] = {0}, words[2] = {0};
@@ -1053,6 +1054,13 @@ double sim_stat(uint32_t h, uint32_t which) {
     case 9: return spec[10];  // inactive nodes whose turn would have written
     case 10: return spec[11]; // turns run from the recorded head list
     case 11: return spec[12]; // turns that traversed the tree
+    case 28: return spec[13]; // queue waits that gave up
+    case 19: {
+      // microseconds of the first attempt's access-list build
+      unsigned long long st[11];
+      cudaMemcpy(st, s->spec.stamps, sizeof st, cudaMemcpyDeviceToHost);
+      return st[10] > st[1] && st[1] ? (double)(st[10] - st[1]) / 1e3 : 0;
+    }
     case 27: return s->last_enqueue_ms;
     case 30: case 31: case 32: case 33: case 34: case 35: case 36: {
       // microseconds of the last tree build's phases: 30 box, 31 keys, 32

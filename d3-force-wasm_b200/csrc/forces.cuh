@@ -105,16 +105,21 @@ struct CollideSpec {
   uint64_t *wmask = nullptr, *emask = nullptr;
   uint8_t *state = nullptr;
   uint32_t *active = nullptr;
-  uint64_t *min_acc = nullptr, *min_wr = nullptr;
+  uint32_t *cnt = nullptr, *rlen = nullptr, *roff = nullptr;  // the access lists
+  uint64_t *ent = nullptr, *ents = nullptr, *succ = nullptr;
+  uint32_t *pred = nullptr, *lev = nullptr, *queue = nullptr;
   double *push = nullptr;
   uint32_t *min_pusher = nullptr, *max_pusher = nullptr;
   uint32_t *vlist = nullptr;
   uint32_t *vaux = nullptr;    // per recorded cell: a leaf's head (tagged) or its skip link
   uint16_t *vcount = nullptr;
-  uint32_t *start = nullptr, *pend = nullptr;
+  uint32_t *start = nullptr;
   double *mdelta = nullptr, *push_prev = nullptr;
   uint32_t *counters = nullptr;  // collide_spec.cu C_*
   unsigned long long *stamps = nullptr;
+  int profile = 0;  // per-depth stamps of the first attempt (sim_set_profile)
+  void *rec = nullptr;  // per cell of the collide tree: its record (64 bytes)
+  uint32_t rec_cap = 0;
 };
 int collide_spec_reserve(CollideSpec &s, uint32_t n);
 void collide_spec_free(CollideSpec &s);

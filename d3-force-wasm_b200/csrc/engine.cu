@@ -1062,10 +1062,11 @@ double sim_stat(uint32_t h, uint32_t which) {
       return st[10] > st[1] && st[1] ? (double)(st[10] - st[1]) / 1e3 : 0;
     }
     case 27: return s->last_enqueue_ms;
-    case 30: case 31: case 32: case 33: case 34: case 35: case 36: {
+    case 30: case 31: case 32: case 33: case 34: case 35: case 36: case 37: {
       // microseconds of the last tree build's phases: 30 box, 31 keys, 32
-      // sort, 33 runs, 34 cell counts, 35 their scan, 36 the cells (block 0)
-      unsigned long long st[8];
+      // sort, 33 runs, 34 cell counts, 35 their scan, 36 cell owners, 37 the
+      // cells (block 0)
+      unsigned long long st[9];
       cudaMemcpy(st, s->tree.stamps, sizeof st, cudaMemcpyDeviceToHost);
       const int k = (int)which - 30;
       return st[k + 1] >= st[k] ? (double)(st[k + 1] - st[k]) * 1e-3 : -1;

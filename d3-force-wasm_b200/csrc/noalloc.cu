@@ -48,7 +48,7 @@ constexpr size_t NA_SIZES[] = {
     4 * na_scan_words(NA_CAP + 1),                // force scan
     16 * sizeof(uint32_t), 2 * sizeof(double),    // counters, center
     sizeof(Rng), 16 * sizeof(uint32_t),           // rng, status words
-    8 * sizeof(unsigned long long),               // tree build phase stamps
+    16 * sizeof(unsigned long long),              // tree build phase stamps
 };
 
 constexpr size_t na_total() {

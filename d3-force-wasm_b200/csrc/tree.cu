@@ -5,8 +5,9 @@
 //   1. bounding box with addAll's first-wins comparisons, then d3's `cover`
 //      (tree.zig:148-187, 230-248, 316-340);
 //   2. 32-level Morton keys by d3's own midpoint test (tree.zig:252-284);
-//   3. stable LSD radix sort of the keys, then a stable partition that moves
-//      points with a NaN coordinate last (they are left out of the tree);
+//   3. stable sort of the keys (three LSD radix passes on the top 24 bits, then
+//      a rank within each run of equal top bits), then a stable partition that
+//      moves points with a NaN coordinate last (they are left out of the tree);
 //   4. cells in closed form: every cell is identified by (first sorted point,
 //      depth); cells starting at point k have consecutive depths d0..leaf, so
 //      cell index = base[k] + depth - d0 with base the exclusive scan of the
@@ -385,79 +386,104 @@ __device__ inline uint32_t lower_bound(const uint64_t *keys, uint32_t lo, uint32
   return lo;
 }
 
-// First index in [lo, hi) whose key's top 2d bits differ from pk (d >= 1).
+// First index in [lo, hi) whose key's top 2d bits differ from pk (d >= 1),
+// given that keys[lo] has them: doubling steps from lo, then bisection (the
+// cost grows with the log of the cell's size, not of the array's).
 __device__ inline uint32_t prefix_end(const uint64_t *keys, uint32_t lo, uint32_t hi, uint64_t pk,
                                       int d) {
   const int sh = 64 - 2 * d;
-  while (lo < hi) {
-    uint32_t mid = lo + ((hi - lo) >> 1);
-    if ((keys[mid] >> sh) == pk) lo = mid + 1; else hi = mid;
+  uint32_t ok = lo, step = 1;
+  for (;;) {
+    const uint32_t probe = ok + step;
+    if (probe >= hi || (keys[probe] >> sh) != pk) {
+      hi = probe < hi ? probe : hi;
+      break;
+    }
+    ok = probe;
+    step <<= 1;
   }
-  return lo;
+  uint32_t l = ok + 1;
+  while (l < hi) {
+    uint32_t mid = l + ((hi - l) >> 1);
+    if ((keys[mid] >> sh) == pk) l = mid + 1; else hi = mid;
+  }
+  return l;
 }
 
-__device__ void emit_at(uint32_t k, uint32_t m, uint32_t total, const double *xs, const double *ys,
-                        const uint64_t *keys, const int8_t *lcpx, const double *extent,
-                        uint32_t *perm, uint32_t *perm_tmp, Frame *frames, const uint32_t *base,
-                        const uint32_t *run_end, const uint8_t *leafd, Cell *cells, uint32_t *skip,
-                        uint32_t *parent, uint32_t *counter, uint32_t *info, uint32_t *leaf_of) {
+// Cell emission, one thread per cell. A start k owns cells base[k] +
+// (0 .. dlast - d0) (depths d0 .. dlast); `owner[c]` = k | OWN_TAG for those
+// (below-resolution cells of a deep group stay NONE: the thread of the group's
+// depth-32 cell emits them after it).
+constexpr uint32_t OWN_TAG = 0x80000000u;
+
+__device__ void own_at(uint32_t k, uint32_t m, const int8_t *lcpx, const uint32_t *base,
+                       const uint32_t *cnt, const uint8_t *leafd, uint32_t *owner, uint32_t *info) {
   if (!is_start(lcpx, k)) return;
+  const int d0 = k == 0 ? 0 : ldc(&lcpx[k]) + 1;
+  const int ld = ldc(&leafd[k]);
+  const int dlast = ld == 33 ? 32 : ld;
+  const uint32_t c0 = ldc(&base[k]);
+  for (int d = d0; d <= dlast; ++d) owner[c0 + (d - d0)] = k | OWN_TAG;
+  const uint32_t chain = (uint32_t)(dlast - d0 + 1), all = ldc(&cnt[k]);
+  for (uint32_t c = c0 + chain; c < c0 + all; ++c) owner[c] = NONE;
+  atomicMax(&info[2], (uint32_t)dlast);
+}
+
+__device__ void emit_cell(uint32_t c, uint32_t m, uint32_t total, const double *xs, const double *ys,
+                          const uint64_t *keys, const int8_t *lcpx, const double *extent,
+                          uint32_t *perm, uint32_t *perm_tmp, Frame *frames, const uint32_t *base,
+                          const uint32_t *run_end, const uint8_t *leafd, Cell *cells, uint32_t *skip,
+                          uint32_t *parent, uint32_t *counter, uint32_t *info, uint32_t *leaf_of) {
+  const uint32_t own = ldc(&counter[c]);
+  if (own == NONE || !(own & OWN_TAG)) return;
+  const uint32_t k = own & ~OWN_TAG;
   const uint64_t key = ldc(&keys[k]);
   const int d0 = k == 0 ? 0 : ldc(&lcpx[k]) + 1;
   const int ld = ldc(&leafd[k]);
   const bool deep = ld == 33;
-  const int dlast = deep ? 32 : ld;
+  const uint32_t c0 = ldc(&base[k]);
+  const int d = d0 + (int)(c - c0);
   const uint32_t rend = ldc(&run_end[k]);
   double x0, y0, x1, y1;
-  path_bounds(extent, key, d0, x0, y0, x1, y1);
-  uint32_t c = ldc(&base[k]);
-  if (k == 0) parent[0] = NONE;
-  for (int d = d0; d <= dlast; ++d, ++c) {
-    const bool leaf = !deep && d == ld;
-    uint32_t end;
-    if (leaf || (deep && d == 32)) end = rend;
-    else if (d == 0) end = m;
-    else end = prefix_end(keys, k, m, key >> (64 - 2 * d), d);
-    Cell cell;
-    cell.child[0] = cell.child[1] = cell.child[2] = cell.child[3] = NONE;
-    cell.first = k;
-    cell.count = end - k;
-    cell.x0 = x0; cell.y0 = y0; cell.x1 = x1; cell.y1 = y1;
-    cell.x = cell.y = cell.value = cell.r = 0;
-    skip[c] = end < m ? ldc(&base[end]) : total;
-    counter[c] = 0;
-    if (!leaf && d < 32) {
-      const uint64_t top = d == 0 ? 0 : (key >> (64 - 2 * d)) << (64 - 2 * d);
-      uint32_t b[5];
-      b[0] = k;
-      b[4] = end;
-      for (uint32_t q = 1; q < 4; ++q)
-        b[q] = lower_bound(keys, b[q - 1], end, top | ((uint64_t)q << (62 - 2 * d)));
-      for (int q = 0; q < 4; ++q) {
-        if (b[q] == b[q + 1]) continue;
-        uint32_t a = b[q];
-        int cd0 = a == k ? d0 : ldc(&lcpx[a]) + 1;
-        uint32_t ch = ldc(&base[a]) + (uint32_t)(d + 1 - cd0);
-        cell.child[q] = ch;
-        parent[ch] = c;
-      }
+  path_bounds(extent, key, d, x0, y0, x1, y1);
+  if (c == 0) parent[0] = NONE;
+  const bool leaf = !deep && d == ld;
+  uint32_t end;
+  if (leaf || (deep && d == 32)) end = rend;
+  else if (d == 0) end = m;
+  else end = prefix_end(keys, k, m, key >> (64 - 2 * d), d);
+  Cell cell;
+  cell.child[0] = cell.child[1] = cell.child[2] = cell.child[3] = NONE;
+  cell.first = k;
+  cell.count = end - k;
+  cell.x0 = x0; cell.y0 = y0; cell.x1 = x1; cell.y1 = y1;
+  cell.x = cell.y = cell.value = cell.r = 0;
+  skip[c] = end < m ? ldc(&base[end]) : total;
+  if (!leaf && d < 32) {
+    const uint64_t top = d == 0 ? 0 : (key >> (64 - 2 * d)) << (64 - 2 * d);
+    uint32_t b[5];
+    b[0] = k;
+    b[4] = end;
+    for (uint32_t q = 1; q < 4; ++q)
+      b[q] = lower_bound(keys, b[q - 1], end, top | ((uint64_t)q << (62 - 2 * d)));
+    for (int q = 0; q < 4; ++q) {
+      if (b[q] == b[q + 1]) continue;
+      uint32_t a = b[q];
+      int cd0 = a == k ? d0 : ldc(&lcpx[a]) + 1;
+      uint32_t ch = ldc(&base[a]) + (uint32_t)(d + 1 - cd0);
+      cell.child[q] = ch;
+      parent[ch] = c;
     }
-    cells[c] = cell;
-    if (leaf)
-      for (uint32_t p = k; p < rend; ++p) leaf_of[ldc(&perm[p])] = c;
-    // descend one level along the key
-    uint32_t dg = (uint32_t)(key >> (62 - 2 * d)) & 3u;
-    double xm = (x0 + x1) / 2, ym = (y0 + y1) / 2;
-    if (dg & 1) x0 = xm; else x1 = xm;
-    if (dg & 2) y0 = ym; else y1 = ym;
   }
-  atomicMax(&info[2], (uint32_t)dlast);
-  if (deep) {
-    uint32_t c32 = ldc(&base[k]) + (uint32_t)(32 - d0);
-    uint32_t after = rend < m ? ldc(&base[rend]) : total;
-    uint32_t emitted = deep_group(true, k, rend, c32, key, extent, xs, ys, perm, perm_tmp, frames,
-                                  cells, parent, skip, after, &info[2], leaf_of);
-    for (uint32_t q = c32 + 1; q <= c32 + emitted; ++q) counter[q] = 0;
+  cells[c] = cell;
+  counter[c] = 0;
+  if (leaf)
+    for (uint32_t p = k; p < rend; ++p) leaf_of[ldc(&perm[p])] = c;
+  if (deep && d == 32) {
+    const uint32_t after = rend < m ? ldc(&base[rend]) : total;
+    const uint32_t emitted = deep_group(true, k, rend, c, key, extent, xs, ys, perm, perm_tmp,
+                                        frames, cells, parent, skip, after, &info[2], leaf_of);
+    for (uint32_t q = c + 1; q <= c + emitted; ++q) counter[q] = 0;
   }
 }
 
@@ -571,15 +597,15 @@ __device__ inline uint32_t tb_next_digit(uint64_t k, uint32_t v, int next) {
 // One stable LSD pass from (ik, iv) to (ok, ov), given `cur`: per tile
 // (TB_TILE keys) the counts of each digit, tile-major. Phase 1: per digit (a
 // block each) the exclusive prefix of its counts over the tiles, and the
-// digit totals; the other blocks clear `nxt`. Phase 2: the scatter, in which a
-// key's rank among equal digits of its tile = earlier warps' counts + lanes
-// below it in its warp with the same digit (warp match); each key also counts
-// its digit of the next pass (`next`, if has_next) into `nxt` at its new tile.
-// Two grid barriers.
+// digit totals; the other blocks clear `nxt` (if clear). Phase 2: the
+// scatter, in which a key's rank among equal digits of its tile = earlier
+// warps' counts + lanes below it in its warp with the same digit (warp
+// match); each key also counts its digit of the next pass (`next`, if
+// has_next) into `nxt` at its new tile. Two grid barriers.
 template <bool PART>
 __device__ void tb_sort_pass(cg::grid_group &g, const TreeBuildArgs &a, const uint64_t *ik,
                              const uint32_t *iv, uint64_t *ok, uint32_t *ov, int shift,
-                             uint32_t *cur, uint32_t *nxt, bool has_next, int next) {
+                             uint32_t *cur, uint32_t *nxt, bool has_next, int next, bool clear) {
   __shared__ uint32_t h[256];
   __shared__ uint32_t wcnt[TB_THREADS / 32][256];
   __shared__ uint32_t sw[32];
@@ -598,7 +624,7 @@ __device__ void tb_sort_pass(cg::grid_group &g, const TreeBuildArgs &a, const ui
     }
     if (t == 0) a.dtot[d] = run;
   }
-  if (has_next)
+  if (clear)
     for (uint32_t i = tid; i < tiles * 256; i += nth) nxt[i] = 0;
   g.sync();
   for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
@@ -627,6 +653,38 @@ __device__ void tb_sort_pass(cg::grid_group &g, const TreeBuildArgs &a, const ui
     __syncthreads();
   }
   g.sync();
+}
+
+constexpr uint32_t TB_RUN_MAX = 256;
+
+// The sorted place of point k (of keys, vals sorted by the top 24 key bits)
+// within its run of equal top bits, by the rest of the key and then the
+// point index: written to (ok, ov); returns it. A run longer than TB_RUN_MAX
+// sets *flag instead (and returns NONE).
+__device__ uint32_t tb_run_rank(const uint64_t *keys, const uint32_t *vals, uint32_t n, uint32_t k,
+                                uint64_t *ok, uint32_t *ov, uint32_t *flag) {
+  constexpr uint64_t LOW = (1ull << 40) - 1;
+  const uint64_t key = ldc(&keys[k]);
+  const uint32_t v = ldc(&vals[k]);
+  const uint64_t top = key >> 40, low = key & LOW;
+  const uint32_t idx = v & 0x7fffffffu;
+  uint32_t s = k, e = k + 1;
+  while (s > 0 && k - s < TB_RUN_MAX && (ldc(&keys[s - 1]) >> 40) == top) --s;
+  while (e < n && e - s <= TB_RUN_MAX && (ldc(&keys[e]) >> 40) == top) ++e;
+  if (e - s > TB_RUN_MAX) {
+    atomicOr(flag, 1u);
+    return NONE;
+  }
+  uint32_t rank = 0;
+  for (uint32_t j = s; j < e; ++j) {
+    const uint64_t lj = ldc(&keys[j]) & LOW;
+    const uint32_t ij = ldc(&vals[j]) & 0x7fffffffu;
+    rank += lj < low || (lj == low && ij < idx);
+  }
+  const uint32_t pos = s + rank;
+  ok[pos] = key;
+  ov[pos] = v;
+  return pos;
 }
 
 __global__ void __launch_bounds__(TB_THREADS) k_tree_build(TreeBuildArgs a) {
@@ -690,6 +748,7 @@ __global__ void __launch_bounds__(TB_THREADS) k_tree_build(TreeBuildArgs a) {
         a.info[3] = m ? 0 : NONE;
         a.info[4] = 0;
         a.info[5] = 0;
+        a.info[7] = 0;
       }
     }
     __syncthreads();
@@ -700,38 +759,63 @@ __global__ void __launch_bounds__(TB_THREADS) k_tree_build(TreeBuildArgs a) {
   tb_stamp(a, 1);
   for (uint32_t i = tid; i < n; i += nth) {
     keys_at(i, a.xs, a.ys, se, a.keys, a.sv);
-    atomicAdd(&a.hist[(size_t)(i / TB_TILE) * 256 + (uint32_t)(a.keys[i] & 255u)], 1u);
+    atomicAdd(&a.hist[(size_t)(i / TB_TILE) * 256 + (uint32_t)((a.keys[i] >> 40) & 255u)], 1u);
   }
   g.sync();
   tb_stamp(a, 2);
-  // 3. the stable sort: 8 key bytes, then the NaN partition if any point has one
-  uint64_t *ak = a.keys, *bk = a.keys_tmp;
-  uint32_t *av = a.sv, *bv = a.sv_tmp;
-  uint32_t *hc = a.hist, *hn = a.hist2;
+  // 3. the stable sort by key, then the NaN partition if any point has one:
+  //    three LSD passes on the top 24 key bits; then each run of equal top
+  //    bits (normally one to three points) is ordered by the rest of the key
+  //    and the point index, each point placed by its rank in its run. If a run
+  //    is longer than TB_RUN_MAX, the 8 full LSD passes run on the top-sorted
+  //    order instead (still stable: equal keys keep index order in a run).
   const bool part = m < n;
-  for (int b = 0; b < 8; ++b) {
-    const bool has_next = b < 7 || part;
-    tb_sort_pass<false>(g, a, ak, av, bk, bv, 8 * b, hc, hn, has_next, b < 7 ? 8 * (b + 1) : -1);
-    uint64_t *tk = ak; ak = bk; bk = tk;
-    uint32_t *tv = av; av = bv; bv = tv;
-    uint32_t *th = hc; hc = hn; hn = th;
+  tb_sort_pass<false>(g, a, a.keys, a.sv, a.keys_tmp, a.sv_tmp, 40, a.hist, a.hist2, true, 48, true);
+  tb_sort_pass<false>(g, a, a.keys_tmp, a.sv_tmp, a.keys, a.sv, 48, a.hist2, a.hist, true, 56, true);
+  tb_sort_pass<false>(g, a, a.keys, a.sv, a.keys_tmp, a.sv_tmp, 56, a.hist, a.hist2, false, 0, true);
+  for (uint32_t k = tid; k < n; k += nth) {
+    const uint32_t pos = tb_run_rank(a.keys_tmp, a.sv_tmp, n, k, a.keys, a.sv, &a.info[7]);
+    if (part && pos != NONE)
+      atomicAdd(&a.hist2[(size_t)(pos / TB_TILE) * 256 + (ldc(&a.sv_tmp[k]) >> 31)], 1u);
+  }
+  for (uint32_t i = tid; i < a.tiles * 256; i += nth) a.hist[i] = 0;
+  g.sync();
+  uint64_t *fk = a.keys;  // the sorted keys and values
+  uint32_t *fv = a.sv, *fh = a.hist2;
+  if (ldc(&a.info[7])) {
+    for (uint32_t k = tid; k < n; k += nth)
+      atomicAdd(&a.hist[(size_t)(k / TB_TILE) * 256 + (uint32_t)(ldc(&a.keys_tmp[k]) & 255u)], 1u);
+    g.sync();
+    uint64_t *ak = a.keys_tmp, *bk = a.keys;
+    uint32_t *av = a.sv_tmp, *bv = a.sv;
+    uint32_t *hc = a.hist, *hn = a.hist2;
+    for (int b = 0; b < 8; ++b) {
+      const bool has_next = b < 7 || part;
+      tb_sort_pass<false>(g, a, ak, av, bk, bv, 8 * b, hc, hn, has_next, b < 7 ? 8 * (b + 1) : -1,
+                          has_next);
+      uint64_t *tk = ak; ak = bk; bk = tk;
+      uint32_t *tv = av; av = bv; bv = tv;
+      uint32_t *th = hc; hc = hn; hn = th;
+    }
+    fk = ak;
+    fv = av;
+    fh = hc;
   }
   if (part) {
-    tb_sort_pass<true>(g, a, ak, av, bk, bv, 0, hc, hn, false, 0);
-    for (uint32_t i = tid; i < n; i += nth) {
-      a.keys[i] = ldc(&bk[i]);
-      a.sv[i] = ldc(&bv[i]);
-    }
-    g.sync();
+    uint64_t *ok = fk == a.keys ? a.keys_tmp : a.keys;
+    uint32_t *ov = fv == a.sv ? a.sv_tmp : a.sv;
+    tb_sort_pass<true>(g, a, fk, fv, ok, ov, 0, fh, nullptr, false, 0, false);
+    fk = ok;
+    fv = ov;
   }
   tb_stamp(a, 3);
   // 4. perm and the shared levels; 5. cells per start
   for (uint32_t k = tid; k < n; k += nth)
-    runs_at(k, m, a.xs, a.ys, a.keys, a.sv, a.perm, a.lcpx, a.leaf_of);
+    runs_at(k, m, a.xs, a.ys, fk, fv, a.perm, a.lcpx, a.leaf_of);
   g.sync();
   tb_stamp(a, 4);
   for (uint32_t k = tid; k < n; k += nth)
-    count_at(k, m, a.xs, a.ys, a.keys, a.lcpx, se, a.perm, a.perm_tmp, a.frames, a.cnt, a.run_end,
+    count_at(k, m, a.xs, a.ys, fk, a.lcpx, se, a.perm, a.perm_tmp, a.frames, a.cnt, a.run_end,
              a.leafd);
   g.sync();
   tb_stamp(a, 5);
@@ -749,10 +833,14 @@ __global__ void __launch_bounds__(TB_THREADS) k_tree_build(TreeBuildArgs a) {
     return;
   }
   for (uint32_t k = tid; k < m; k += nth)
-    emit_at(k, m, total, a.xs, a.ys, a.keys, a.lcpx, se, a.perm, a.perm_tmp, a.frames, a.base,
-            a.run_end, a.leafd, a.cells, a.skip, a.parent, a.counter, a.info, a.leaf_of);
+    own_at(k, m, a.lcpx, a.base, a.cnt, a.leafd, a.counter, a.info);
+  g.sync();
+  tb_stamp(a, 7);
+  for (uint32_t c = tid; c < total; c += nth)
+    emit_cell(c, m, total, a.xs, a.ys, fk, a.lcpx, se, a.perm, a.perm_tmp, a.frames, a.base,
+              a.run_end, a.leafd, a.cells, a.skip, a.parent, a.counter, a.info, a.leaf_of);
   __syncthreads();
-  tb_stamp(a, 7);  // block 0's emit only
+  tb_stamp(a, 8);  // block 0's cells only
 }
 
 int tree_reserve(TreeDev &t, uint32_t n) {
@@ -761,8 +849,8 @@ int tree_reserve(TreeDev &t, uint32_t n) {
     D3_CUDA_OK(cudaMemset(t.info, 0, 16 * sizeof(uint32_t)));
     D3_CUDA_OK(cudaMalloc(&t.extent, 4 * sizeof(double)));
     D3_CUDA_OK(cudaMalloc(&t.box_part, BOX_BLOCKS_MAX * sizeof(BoxPart)));
-    D3_CUDA_OK(cudaMalloc(&t.stamps, 8 * sizeof(unsigned long long)));
-    D3_CUDA_OK(cudaMemset(t.stamps, 0, 8 * sizeof(unsigned long long)));
+    D3_CUDA_OK(cudaMalloc(&t.stamps, 16 * sizeof(unsigned long long)));
+    D3_CUDA_OK(cudaMemset(t.stamps, 0, 16 * sizeof(unsigned long long)));
   }
   if (n <= t.cap && t.cap) return 0;
   uint32_t cap = n < 1024 ? 1024 : n;

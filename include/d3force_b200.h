@@ -153,9 +153,9 @@ double sim_last_tick_ms(uint32_t h);
  * (part of 13), 28 its queue waits that gave up (0 unless it failed); the last center sum's 22 / 23 microseconds of
  * the exact x / y walks, 24 its x walk's record batches rerun with their
  * entry tests, 25 stretches added one by one, 26 records in all; 27 host
- * milliseconds the last sim_tick spent queueing work; 30-36 microseconds of
+ * milliseconds the last sim_tick spent queueing work; 30-37 microseconds of
  * the last tree build's phases (box, keys, sort, runs, cell counts, their
- * scan, the cells); with profiling on, 300 + k microseconds from the end of
+ * scan, cell owners, the cells); with profiling on, 300 + k microseconds from the end of
  * the last parallel collide's first list build to its last turn of depth k,
  * 400 + k its turns of depth k (k < 63; 63 counts every deeper turn);
  * 100 + k milliseconds and 200 + k count of phase k

@@ -1143,7 +1143,6 @@ int collide_spec_reserve(CollideSpec &s, uint32_t n) {
 
 void collide_spec_free(CollideSpec &s) {
   spec_arrays(s, [](void **p, size_t) { cudaFree(*p); });
-  cudaFree(s.rec);
   cudaFree(s.counters);
   cudaFree(s.stamps);
   s = CollideSpec();
@@ -1167,17 +1166,7 @@ int collide_parallel(TreeDev &t, const NodeArrays &a, const double *radii, doubl
     if (g_spec_blocks <= 0) g_spec_blocks = sms;
   }
   SpecArgs args;
-  if (s.rec_cap < t.cells_cap) {
-    cudaFree(s.rec);
-    s.rec = nullptr;
-    s.rec_cap = 0;
-    if (cudaMalloc(&s.rec, (size_t)t.cells_cap * sizeof(CRec)) != cudaSuccess) {
-      cudaGetLastError();
-      return -1;
-    }
-    s.rec_cap = t.cells_cap;
-  }
-  args.rec = (CRec *)s.rec;
+  args.rec = (CRec *)t.rec;
   args.cells = t.cells; args.skip = t.skip; args.perm = t.perm; args.info = t.info;
   args.parent = t.parent; args.leaf_of = t.leaf_of;
   args.xs = a.x; args.ys = a.y; args.px = a.px; args.py = a.py; args.radii = radii;

@@ -55,92 +55,146 @@ void scratch_free(ForceScratch &s) {
 
 __device__ inline double ld_cg(const double *p) { return __ldcg(p); }
 
+// A cell as the exact many-body traversal reads it, in one 64-byte load.
+struct alignas(64) MRec {
+  double x, y, value;
+  double wt;              // (x1 - x0)^2 / theta2, as the opening test forms it
+  uint32_t skip, head;    // head: the leaf's head node; NONE for an internal cell
+  uint32_t first, count;  // the leaf's points in perm
+};
+static_assert(sizeof(MRec) == 64, "record layout");
+
+// A parent's step of the bottom-up passes: its children are the ones listed
+// in its cell (several), or only the child just finished (one: no counter,
+// and the child's values are still in registers).
+struct Climb {
+  uint32_t p;      // the parent (NONE at the root)
+  uint32_t nch;    // its child count
+};
+
+__device__ inline Climb climb_up(const uint32_t *parent, const uint8_t *pnch, uint32_t cur) {
+  Climb c;
+  c.p = parent[cur];
+  c.nch = pnch[cur];
+  return c;
+}
+
 // many_body.zig:101-135 (accumulate). Leaf: head position, strength summed
 // over the chain from perm[first + count - 1] down. Internal: children 0..3
-// with a truthy |value|.
-__global__ void k_mb_accumulate(Cell *cells, const uint32_t *parent, uint32_t *counter,
-                                const uint32_t *perm, const double *xs, const double *ys,
-                                const double *strengths, const uint32_t *info) {
+// with a truthy |value|. Each finished cell also gets its traversal record.
+__global__ void k_mb_accumulate(Cell *cells, const uint32_t *parent, const uint8_t *pnch,
+                                uint32_t *counter, const uint32_t *perm, const uint32_t *skip,
+                                const double *xs, const double *ys, const double *strengths,
+                                double theta2, MRec *rec, const uint32_t *info) {
   const uint32_t len = info[1];
   for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < len; c += gridDim.x * blockDim.x) {
     Cell *q = &cells[c];
     if (!is_leaf(*q)) continue;
-    uint32_t head = perm[q->first + q->count - 1];
+    const uint32_t first = q->first, count = q->count;
+    uint32_t head = perm[first + count - 1];
     double strength = 0;
-    for (uint32_t k = q->first + q->count; k > q->first;) {
+    for (uint32_t k = first + count; k > first;) {
       --k;
       strength += strengths[perm[k]];
     }
-    q->x = xs[head];
-    q->y = ys[head];
-    q->value = strength;
-    uint32_t cur = c;
+    double cx = xs[head], cy = ys[head], cv = strength;
+    q->x = cx;
+    q->y = cy;
+    q->value = cv;
+    {
+      const double w = q->x1 - q->x0;
+      MRec r;
+      r.x = cx; r.y = cy; r.value = cv; r.wt = w * w / theta2;
+      r.skip = skip[c]; r.head = head; r.first = first; r.count = count;
+      rec[c] = r;
+    }
+    Climb up = climb_up(parent, pnch, c);
     for (;;) {
-      uint32_t p = parent[cur];
+      const uint32_t p = up.p;
       if (p == NONE) break;
       Cell *pc = &cells[p];
-      uint32_t nch = 0;
-      for (int k = 0; k < 4; ++k) nch += pc->child[k] != NONE;
-      __threadfence();
-      if (atomicAdd(&counter[p], 1u) != nch - 1) break;
-      __threadfence();
+      // issued together: the parent's box and skip, and the next step up
+      const double px0 = pc->x0, px1 = pc->x1;
+      const uint32_t pskip = skip[p];
+      const Climb next = climb_up(parent, pnch, p);
       double st = 0, weight = 0, x = 0, y = 0;
-      for (int k = 0; k < 4; ++k) {
-        uint32_t ch = pc->child[k];
-        if (ch == NONE) continue;
-        double v = ld_cg(&cells[ch].value);
-        double w = fabs(v);
+      if (up.nch == 1) {
+        const double w = fabs(cv);
         if (w > 0) {
-          st += v;
+          st += cv;
           weight += w;
-          x += w * ld_cg(&cells[ch].x);
-          y += w * ld_cg(&cells[ch].y);
+          x += w * cx;
+          y += w * cy;
+        }
+      } else {
+        __threadfence();
+        if (atomicAdd(&counter[p], 1u) != up.nch - 1) break;
+        __threadfence();
+        for (int k = 0; k < 4; ++k) {
+          uint32_t ch = pc->child[k];
+          if (ch == NONE) continue;
+          double v = ld_cg(&cells[ch].value);
+          double w = fabs(v);
+          if (w > 0) {
+            st += v;
+            weight += w;
+            x += w * ld_cg(&cells[ch].x);
+            y += w * ld_cg(&cells[ch].y);
+          }
         }
       }
-      pc->x = x / weight;
-      pc->y = y / weight;
-      pc->value = st;
-      cur = p;
+      cx = x / weight;
+      cy = y / weight;
+      cv = st;
+      pc->x = cx;
+      pc->y = cy;
+      pc->value = cv;
+      const double w = px1 - px0;
+      MRec r;
+      r.x = cx; r.y = cy; r.value = cv; r.wt = w * w / theta2;
+      r.skip = pskip; r.head = NONE; r.first = 0; r.count = 0;
+      rec[p] = r;
+      up = next;
     }
   }
 }
 
 // collide.zig:117-129 (prepare): leaf radius of its head, internal the largest
 // child radius (strict >, from 0).
-__global__ void k_collide_prep(Cell *cells, const uint32_t *parent, uint32_t *counter,
-                               const uint32_t *perm, const double *radii, const uint32_t *info) {
+__global__ void k_collide_prep(Cell *cells, const uint32_t *parent, const uint8_t *pnch,
+                               uint32_t *counter, const uint32_t *perm, const double *radii,
+                               const uint32_t *info) {
   const uint32_t len = info[1];
   for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < len; c += gridDim.x * blockDim.x) {
     Cell *q = &cells[c];
     if (!is_leaf(*q)) continue;
-    q->r = radii[perm[q->first + q->count - 1]];
-    uint32_t cur = c;
+    double cr = radii[perm[q->first + q->count - 1]];
+    q->r = cr;
+    Climb up = climb_up(parent, pnch, c);
     for (;;) {
-      uint32_t p = parent[cur];
+      const uint32_t p = up.p;
       if (p == NONE) break;
       Cell *pc = &cells[p];
-      uint32_t nch = 0;
-      for (int k = 0; k < 4; ++k) nch += pc->child[k] != NONE;
-      __threadfence();
-      if (atomicAdd(&counter[p], 1u) != nch - 1) break;
-      __threadfence();
+      const Climb next = climb_up(parent, pnch, p);
       double r = 0;
-      for (int k = 0; k < 4; ++k) {
-        uint32_t ch = pc->child[k];
-        if (ch == NONE) continue;
-        double cr = ld_cg(&cells[ch].r);
+      if (up.nch == 1) {
         if (cr > r) r = cr;
+      } else {
+        __threadfence();
+        if (atomicAdd(&counter[p], 1u) != up.nch - 1) break;
+        __threadfence();
+        for (int k = 0; k < 4; ++k) {
+          uint32_t ch = pc->child[k];
+          if (ch == NONE) continue;
+          double v = ld_cg(&cells[ch].r);
+          if (v > r) r = v;
+        }
       }
       pc->r = r;
-      cur = p;
+      cr = r;
+      up = next;
     }
   }
-}
-
-__global__ void k_zero_counters(uint32_t *counter, const uint32_t *info) {
-  const uint32_t len = info[1];
-  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < len; c += gridDim.x * blockDim.x)
-    counter[c] = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -151,7 +205,7 @@ __global__ void k_zero_counters(uint32_t *counter, const uint32_t *info) {
 // jiggle, count the draws it would make, and do not write. Otherwise draws
 // come from the stream at `draw0`.
 template <bool RECORD>
-__device__ inline uint32_t mb_node(const Cell *cells, const uint32_t *skip, const uint32_t *perm,
+__device__ inline uint32_t mb_node(const MRec *rec, const uint32_t *perm,
                                    uint32_t len, const double *xs, const double *ys,
                                    double *vxs, double *vys, const double *strengths,
                                    const ManyBodyParams p, uint32_t i, const Rng *rng,
@@ -162,16 +216,15 @@ __device__ inline uint32_t mb_node(const Cell *cells, const uint32_t *skip, cons
   bool flagged = false;
   uint32_t c = 0;
   while (c < len) {
-    const Cell &q = cells[c];
+    const MRec q = rec[c];
     const double value = q.value;
     if (!(value != 0 && value == value)) {
-      c = skip[c];
+      c = q.skip;
       continue;
     }
     double x = q.x - nx, y = q.y - ny;
-    const double w = q.x1 - q.x0;
     double l = x * x + y * y;
-    if (w * w / p.theta2 < l) {
+    if (q.wt < l) {
       if (l < p.dmax2) {
         if (RECORD && (x == 0 || y == 0)) {
           flagged = true;
@@ -186,10 +239,10 @@ __device__ inline uint32_t mb_node(const Cell *cells, const uint32_t *skip, cons
           vy += y * value * p.alpha / l;
         }
       }
-      c = skip[c];
+      c = q.skip;
       continue;
     }
-    if (!is_leaf(q)) {
+    if (q.head == NONE) {
       c = c + 1;
       continue;
     }
@@ -198,7 +251,7 @@ __device__ inline uint32_t mb_node(const Cell *cells, const uint32_t *skip, cons
       continue;
     }
     const uint32_t first = q.first, count = q.count;
-    const uint32_t head = perm[first + count - 1];
+    const uint32_t head = q.head;
     if (head != i || count > 1) {
       if (RECORD && (x == 0 || y == 0)) {
         flagged = true;
@@ -232,7 +285,7 @@ __device__ inline uint32_t mb_node(const Cell *cells, const uint32_t *skip, cons
 }
 
 // Record pass over all nodes in Morton order (perm, then the NaN nodes).
-__global__ void __launch_bounds__(128) k_mb_traverse(const Cell *cells, const uint32_t *skip,
+__global__ void __launch_bounds__(128) k_mb_traverse(const MRec *rec,
                                                      const uint32_t *perm, const uint32_t *info,
                                                      const double *xs, const double *ys, double *vxs,
                                                      double *vys, const double *strengths,
@@ -242,7 +295,7 @@ __global__ void __launch_bounds__(128) k_mb_traverse(const Cell *cells, const ui
   if (pos >= n) return;
   const uint32_t len = info[1];
   const uint32_t i = perm[pos];
-  uint32_t d = len ? mb_node<true>(cells, skip, perm, len, xs, ys, vxs, vys, strengths, p, i,
+  uint32_t d = len ? mb_node<true>(rec, perm, len, xs, ys, vxs, vys, strengths, p, i,
                                    nullptr, 0)
                    : 0;
   draws[i] = d;
@@ -251,7 +304,7 @@ __global__ void __launch_bounds__(128) k_mb_traverse(const Cell *cells, const ui
 
 // Flagged nodes again, each from its own offset in the draw stream (the
 // exclusive scan of draws over node index = d3's draw order).
-__global__ void __launch_bounds__(128) k_mb_rerun(const Cell *cells, const uint32_t *skip,
+__global__ void __launch_bounds__(128) k_mb_rerun(const MRec *rec,
                                                   const uint32_t *perm, const uint32_t *info,
                                                   const double *xs, const double *ys, double *vxs,
                                                   double *vys, const double *strengths,
@@ -261,7 +314,7 @@ __global__ void __launch_bounds__(128) k_mb_rerun(const Cell *cells, const uint3
   if (counters[1] == 0) return;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || draws[i] == 0) return;
-  mb_node<false>(cells, skip, perm, info[1], xs, ys, vxs, vys, strengths, p, i, rng, offsets[i]);
+  mb_node<false>(rec, perm, info[1], xs, ys, vxs, vys, strengths, p, i, rng, offsets[i]);
 }
 
 __global__ void k_rng_advance(Rng *rng, const uint32_t *total) {
@@ -286,11 +339,11 @@ void many_body_exact(TreeDev &t, const NodeArrays &a, const double *strengths,
   if (n == 0) return;
   unsigned cb, ct;
   climb_grid(cb, ct, t.cells_cap);
-  D3_LAUNCH(k_mb_accumulate, cb, ct, 0, st)(t.cells, t.parent, t.counter, t.perm, a.x, a.y, strengths,
-                                     t.info);
+  D3_LAUNCH(k_mb_accumulate, cb, ct, 0, st)(t.cells, t.parent, t.pnch, t.counter, t.perm, t.skip, a.x,
+                                     a.y, strengths, p.theta2, (MRec *)t.rec, t.info);
   if (mark) mark(1);
   cudaMemsetAsync(s.counters, 0, 2 * sizeof(uint32_t), st);
-  D3_LAUNCH(k_mb_traverse, blocks_for(n, 128), 128, 0, st)(t.cells, t.skip, t.perm, t.info, a.x, a.y,
+  D3_LAUNCH(k_mb_traverse, blocks_for(n, 128), 128, 0, st)((const MRec *)t.rec, t.perm, t.info, a.x, a.y,
                                                     a.vx, a.vy, strengths, p, n, s.draws,
                                                     s.counters);
   scan_u32(s.draws, s.offsets, n, s.scan_part, s.counters, st);
@@ -300,7 +353,7 @@ void many_body_exact(TreeDev &t, const NodeArrays &a, const double *strengths,
 void many_body_rerun(TreeDev &t, const NodeArrays &a, const double *strengths,
                      const ManyBodyParams &p, Rng *rng, ForceScratch &s, cudaStream_t st) {
   const uint32_t n = a.n;
-  D3_LAUNCH(k_mb_rerun, blocks_for(n, 128), 128, 0, st)(t.cells, t.skip, t.perm, t.info, a.x, a.y, a.vx,
+  D3_LAUNCH(k_mb_rerun, blocks_for(n, 128), 128, 0, st)((const MRec *)t.rec, t.perm, t.info, a.x, a.y, a.vx,
                                                  a.vy, strengths, p, n, s.draws, s.offsets,
                                                  s.counters, rng);
   D3_LAUNCH(k_rng_advance, 1, 1, 0, st)(rng, s.counters);
@@ -697,7 +750,8 @@ void collide_setup(TreeDev &t, const NodeArrays &a, const double *radii, uint32_
   if (n == 0) return;
   unsigned cb, ct;
   climb_grid(cb, ct, t.cells_cap);
-  D3_LAUNCH(k_collide_prep, cb, ct, 0, st)(t.cells, t.parent, t.counter, t.perm, radii, t.info);
+  D3_LAUNCH(k_collide_prep, cb, ct, 0, st)(t.cells, t.parent, t.pnch, t.counter, t.perm, radii,
+                                    t.info);
 }
 
 void collide_serial(TreeDev &t, const NodeArrays &a, const double *radii, double strength, Rng *rng,

@@ -118,8 +118,6 @@ struct CollideSpec {
   uint32_t *counters = nullptr;  // collide_spec.cu C_*
   unsigned long long *stamps = nullptr;
   int profile = 0;  // per-depth stamps of the first attempt (sim_set_profile)
-  void *rec = nullptr;  // per cell of the collide tree: its record (64 bytes)
-  uint32_t rec_cap = 0;
 };
 int collide_spec_reserve(CollideSpec &s, uint32_t n);
 void collide_spec_free(CollideSpec &s);

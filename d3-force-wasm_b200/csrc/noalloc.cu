@@ -39,6 +39,7 @@ constexpr size_t NA_SIZES[] = {
     4ull * NA_CAP * sizeof(Frame),                // frames
     (size_t)NA_CELLS * sizeof(Cell),              // cells
     4ull * NA_CELLS, 4ull * NA_CELLS, 4ull * NA_CELLS,  // skip, parent, counter
+    (size_t)NA_CELLS, 64ull * NA_CELLS,           // pnch, rec
     4ull * NA_CAP,                                // leaf_of
     NA_BOX_BYTES,                                 // box partials
     4 * na_scan_words(na_hist_words > NA_CAP + 1 ? na_hist_words : NA_CAP + 1),  // tree scan
@@ -141,6 +142,8 @@ extern "C" int32_t d3_many_body_exact_noalloc(const double *x, const double *y, 
   t.skip = c.take<uint32_t>();
   t.parent = c.take<uint32_t>();
   t.counter = c.take<uint32_t>();
+  t.pnch = c.take<uint8_t>();
+  t.rec = c.take<unsigned char>();
   t.leaf_of = c.take<uint32_t>();
   t.box_part = c.take<uint32_t>();
   t.scan_part = c.take<uint32_t>();

@@ -259,7 +259,7 @@ __device__ inline int quadrant(double x, double y, double xm, double ym) {
 __device__ uint32_t deep_group(bool write, uint32_t lo, uint32_t hi, uint32_t c32, uint64_t key,
                                const double *extent, const double *xs, const double *ys,
                                uint32_t *perm, uint32_t *perm_tmp, Frame *frames, Cell *cells,
-                               uint32_t *parent, uint32_t *skip, uint32_t skip_after,
+                               uint32_t *parent, uint8_t *pnch, uint32_t *skip, uint32_t skip_after,
                                uint32_t *depth_out, uint32_t *leaf_of) {
   Frame *stack = frames + 4 * (size_t)lo;
   const uint32_t cap = 4 * (hi - lo);
@@ -286,6 +286,7 @@ __device__ uint32_t deep_group(bool write, uint32_t lo, uint32_t hi, uint32_t c3
         cells[me] = c;
         cells[f.parent].child[f.slot] = me;
         parent[me] = f.parent;
+        pnch[me] = (uint8_t)f.pad;
       }
       f.parent = me;
       // allSame by position (tree.zig:437-444); the depth guard of tree.zig:33
@@ -317,11 +318,14 @@ __device__ uint32_t deep_group(bool write, uint32_t lo, uint32_t hi, uint32_t c3
       perm_tmp[off[quadrant(xs[p], ys[p], xm, ym)]++] = p;
     }
     for (uint32_t k = f.lo; k < f.hi; ++k) perm[k] = ldc(&perm_tmp[k]);
+    uint32_t nq = 0;
+    for (int q = 0; q < 4; ++q) nq += b[q] != b[q + 1];
     for (int q = 3; q >= 0; --q) {
       if (b[q] == b[q + 1]) continue;
       if (sp >= cap) return emitted;  // cannot happen: pending frames hold disjoint points
       Frame c;
       c.lo = b[q]; c.hi = b[q + 1]; c.depth = f.depth + 1; c.parent = f.parent; c.slot = q;
+      c.pad = nq;  // the parent's child count
       bool right = q & 1, bottom = q & 2;
       c.x0 = right ? xm : f.x0; c.y0 = bottom ? ym : f.y0;
       c.x1 = right ? f.x1 : xm; c.y1 = bottom ? f.y1 : ym;
@@ -371,7 +375,7 @@ __device__ void count_at(uint32_t k, uint32_t m, const double *xs, const double 
   leafd[k] = 33;
   run_end[k] = g1;
   uint32_t deep = deep_group(false, k, g1, 0, ldc(&keys[k]), extent, xs, ys, perm, perm_tmp, frames,
-                             nullptr, nullptr, nullptr, 0, nullptr, nullptr);
+                             nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr);
   cnt[k] = (uint32_t)(32 - d0 + 1) + deep;
 }
 
@@ -433,7 +437,8 @@ __device__ void emit_cell(uint32_t c, uint32_t m, uint32_t total, const double *
                           const uint64_t *keys, const int8_t *lcpx, const double *extent,
                           uint32_t *perm, uint32_t *perm_tmp, Frame *frames, const uint32_t *base,
                           const uint32_t *run_end, const uint8_t *leafd, Cell *cells, uint32_t *skip,
-                          uint32_t *parent, uint32_t *counter, uint32_t *info, uint32_t *leaf_of) {
+                          uint32_t *parent, uint8_t *pnch, uint32_t *counter, uint32_t *info,
+                          uint32_t *leaf_of) {
   const uint32_t own = ldc(&counter[c]);
   if (own == NONE || !(own & OWN_TAG)) return;
   const uint32_t k = own & ~OWN_TAG;
@@ -466,6 +471,8 @@ __device__ void emit_cell(uint32_t c, uint32_t m, uint32_t total, const double *
     b[4] = end;
     for (uint32_t q = 1; q < 4; ++q)
       b[q] = lower_bound(keys, b[q - 1], end, top | ((uint64_t)q << (62 - 2 * d)));
+    uint8_t nch = 0;
+    for (int q = 0; q < 4; ++q) nch += b[q] != b[q + 1];
     for (int q = 0; q < 4; ++q) {
       if (b[q] == b[q + 1]) continue;
       uint32_t a = b[q];
@@ -473,6 +480,7 @@ __device__ void emit_cell(uint32_t c, uint32_t m, uint32_t total, const double *
       uint32_t ch = ldc(&base[a]) + (uint32_t)(d + 1 - cd0);
       cell.child[q] = ch;
       parent[ch] = c;
+      pnch[ch] = nch;
     }
   }
   cells[c] = cell;
@@ -482,7 +490,7 @@ __device__ void emit_cell(uint32_t c, uint32_t m, uint32_t total, const double *
   if (deep && d == 32) {
     const uint32_t after = rend < m ? ldc(&base[rend]) : total;
     const uint32_t emitted = deep_group(true, k, rend, c, key, extent, xs, ys, perm, perm_tmp,
-                                        frames, cells, parent, skip, after, &info[2], leaf_of);
+                                        frames, cells, parent, pnch, skip, after, &info[2], leaf_of);
     for (uint32_t q = c + 1; q <= c + emitted; ++q) counter[q] = 0;
   }
 }
@@ -503,6 +511,7 @@ struct TreeBuildArgs {
   Frame *frames;
   Cell *cells;
   uint32_t *skip, *parent, *counter, *leaf_of;
+  uint8_t *pnch;
   BoxPart *parts;
   uint32_t *hist, *hist2;  // tiles * 256 per-tile digit counts, two passes' worth
   uint32_t *dtot, *bsum;   // 256 digit totals, grid partials
@@ -838,7 +847,7 @@ __global__ void __launch_bounds__(TB_THREADS) k_tree_build(TreeBuildArgs a) {
   tb_stamp(a, 7);
   for (uint32_t c = tid; c < total; c += nth)
     emit_cell(c, m, total, a.xs, a.ys, fk, a.lcpx, se, a.perm, a.perm_tmp, a.frames, a.base,
-              a.run_end, a.leafd, a.cells, a.skip, a.parent, a.counter, a.info, a.leaf_of);
+              a.run_end, a.leafd, a.cells, a.skip, a.parent, a.pnch, a.counter, a.info, a.leaf_of);
   __syncthreads();
   tb_stamp(a, 8);  // block 0's cells only
 }
@@ -858,6 +867,7 @@ int tree_reserve(TreeDev &t, uint32_t n) {
   cudaFree(t.perm_tmp); cudaFree(t.lcpx); cudaFree(t.cnt); cudaFree(t.base); cudaFree(t.run_end);
   cudaFree(t.leafd); cudaFree(t.frames); cudaFree(t.cells); cudaFree(t.skip); cudaFree(t.parent);
   cudaFree(t.counter); cudaFree(t.scan_part); cudaFree(t.hist); cudaFree(t.leaf_of);
+  cudaFree(t.pnch); cudaFree(t.rec);
   size_t cells = 4 * (size_t)cap + 1024;
   D3_CUDA_OK(cudaMalloc(&t.keys, cap * 8ull));
   D3_CUDA_OK(cudaMalloc(&t.keys_tmp, cap * 8ull));
@@ -875,6 +885,8 @@ int tree_reserve(TreeDev &t, uint32_t n) {
   D3_CUDA_OK(cudaMalloc(&t.skip, cells * 4));
   D3_CUDA_OK(cudaMalloc(&t.parent, cells * 4));
   D3_CUDA_OK(cudaMalloc(&t.counter, cells * 4));
+  D3_CUDA_OK(cudaMalloc(&t.pnch, cells));
+  D3_CUDA_OK(cudaMalloc(&t.rec, cells * 64));
   D3_CUDA_OK(cudaMalloc(&t.leaf_of, cap * 4ull));
   size_t sp = scan_partial_words(sort_hist_words(cap) > cap + 1 ? sort_hist_words(cap) : cap + 1);
   D3_CUDA_OK(cudaMalloc(&t.scan_part, sp * 4));
@@ -889,7 +901,7 @@ void tree_free(TreeDev &t) {
   cudaFree(t.perm_tmp); cudaFree(t.lcpx); cudaFree(t.cnt); cudaFree(t.base); cudaFree(t.run_end);
   cudaFree(t.leafd); cudaFree(t.frames); cudaFree(t.cells); cudaFree(t.skip); cudaFree(t.parent);
   cudaFree(t.counter); cudaFree(t.scan_part); cudaFree(t.hist); cudaFree(t.info);
-  cudaFree(t.leaf_of);
+  cudaFree(t.leaf_of); cudaFree(t.pnch); cudaFree(t.rec);
   cudaFree(t.extent); cudaFree(t.box_part); cudaFree(t.stamps);
   t = TreeDev();
 }
@@ -923,7 +935,7 @@ void tree_build(TreeDev &t, const double *xs, const double *ys, uint32_t n, uint
   a.perm = t.perm; a.perm_tmp = t.perm_tmp; a.lcpx = t.lcpx;
   a.cnt = t.cnt; a.base = t.base; a.run_end = t.run_end; a.leafd = t.leafd;
   a.frames = t.frames; a.cells = t.cells; a.skip = t.skip; a.parent = t.parent;
-  a.counter = t.counter; a.leaf_of = t.leaf_of;
+  a.counter = t.counter; a.leaf_of = t.leaf_of; a.pnch = t.pnch;
   a.parts = (BoxPart *)t.box_part;
   a.hist = t.hist;
   a.hist2 = t.hist + (size_t)a.tiles * 256;

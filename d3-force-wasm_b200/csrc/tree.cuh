@@ -29,6 +29,8 @@ struct TreeDev {
   Frame *frames = nullptr;     // 4 frames per point for the deep splits
   Cell *cells = nullptr;
   uint32_t *skip = nullptr, *parent = nullptr, *counter = nullptr;
+  uint8_t *pnch = nullptr;       // per cell: how many children its parent has
+  void *rec = nullptr;           // per cell: the current traversal's 64-byte record
   uint32_t *leaf_of = nullptr;   // per node: the leaf cell holding it (NONE: NaN coordinate)
   uint32_t *box_part = nullptr;  // per-block bbox partials
   uint32_t *scan_part = nullptr;

@@ -59,7 +59,8 @@ constexpr unsigned FULL = 0xffffffffu;
 enum : uint32_t {
   C_ACTIVE = 0, C_FAIL = 2, C_JIGGLE, C_OVERFLOW, C_ROUNDS, C_ATTEMPTS, C_SERIAL,
   C_FAIL_READ, C_FAIL_WRITE, C_FAIL_MOVED, C_FAST_TURNS, C_SLOW_TURNS, C_TIMEOUT,
-  C_ALLOC = 16, C_DONE = 32, C_QHEAD = 64, C_QTAIL = 96, C_COUNTERS = 128
+  C_ALLOC = 16, C_BIGFILL, C_BIGLINK, C_VWORK, C_DONE = 32, C_QHEAD = 64, C_QTAIL = 96,
+  C_COUNTERS = 128
 };
 // Queue slots one cache line apart (idle warps poll them).
 constexpr uint32_t QSTRIDE = 32;
@@ -111,6 +112,7 @@ struct SpecArgs {
   uint32_t *pred;        // n: accesses a turn still waits for
   uint32_t *lev;         // n: the turn's depth in the dependency order
   uint32_t *queue;       // n: turns in the order they became ready
+  uint32_t *bigfill, *biglink, *vwork;  // n each: the items warps share out (see below)
   double *push;          // push magnitude received per node (this pass)
   double *push_prev;     // ... in the previous pass (margin heuristic)
   uint32_t *min_pusher, *max_pusher;
@@ -126,6 +128,19 @@ __device__ inline uint32_t rd(const uint32_t *p) { return __ldcg(p); }
 __device__ inline uint64_t rd(const uint64_t *p) { return __ldcg((const unsigned long long *)p); }
 __device__ inline uint8_t rd(const uint8_t *p) { return (uint8_t)__ldcg((const unsigned char *)p); }
 __device__ inline uint16_t rd(const uint16_t *p) { return (uint16_t)__ldcg((const unsigned short *)p); }
+
+// Appends v to list (size at *count) for the lanes that want to, with one
+// atomic per warp. Warp-uniform call.
+__device__ inline void warp_append(bool want, uint32_t v, uint32_t *list, uint32_t *count) {
+  const unsigned lane = threadIdx.x & 31;
+  const unsigned m = __ballot_sync(FULL, want);
+  if (!m) return;
+  const int leader = __ffs(m) - 1;
+  uint32_t base = 0;
+  if ((int)lane == leader) base = atomicAdd(count, (uint32_t)__popc(m));
+  base = __shfl_sync(FULL, base, leader);
+  if (want) list[base + __popc(m & ((1u << lane) - 1))] = v;
+}
 
 __device__ inline bool same_bits(double a, double b) {
   return __double_as_longlong(a) == __double_as_longlong(b);
@@ -308,72 +323,185 @@ __device__ bool warp_replay(const SpecArgs &a, uint32_t i, double xi, double yi,
 // V: an inactive node's turn re-run at its exact turn state. Its own velocity
 // is final; a head's is its start value if all its pushers come later, its
 // final value if all came earlier, and otherwise only bounded (then a distance
-// margin must hold). Returns false when the turn could write.
-__device__ bool spec_inactive_ok(const SpecArgs &a, uint32_t i) {
+// margin must hold). head_clear: head j (radius rj) as node i at (xi, yi),
+// radius ri, would meet it: true if the turn cannot overlap it.
+__device__ inline bool head_clear(const SpecArgs &a, uint32_t i, double xi, double yi, double ri,
+                                  uint32_t j, double rj) {
+  const uint32_t lo = rd(&a.min_pusher[j]), hi = rd(&a.max_pusher[j]);
+  const double sx = rd(&a.svx[j]), sy = rd(&a.svy[j]), fx = rd(&a.vxs[j]), fy = rd(&a.vys[j]);
+  const double pu = rd(&a.push[j]);
+  const double r = ri + rj;
+  double vj, wj;
+  if (lo == NONE || lo > i) {
+    vj = sx;
+    wj = sy;
+  } else if (hi < i) {
+    vj = fx;
+    wj = fy;
+  } else {
+    const double dx = xi - a.xs[j] - sx, dy = yi - a.ys[j] - sy;
+    const double gap = sqrt(dx * dx + dy * dy) - r - pu;
+    return gap > 1e-9 * (r + 1);
+  }
+  const double x = xi - a.xs[j] - vj, y = yi - a.ys[j] - wj;
+  return !(x * x + y * y < r * r);
+}
+
+enum : int { V_OK = 0, V_WRITES = 1, V_REPLAY = 2, V_TRAVERSE = 3 };
+
+// V's first step, a lane per node: V_OK if nothing the guess read moved (or
+// the node is NaN), V_REPLAY if the warp must replay its recorded cells,
+// V_TRAVERSE if the record does not apply (the warp runs the traversal).
+__device__ int inactive_quick(const SpecArgs &a, uint32_t i) {
   const uint32_t *rl = a.rlist + (size_t)i * SPEC_CAP;
   const uint32_t nr = rd(&a.rcount[i]);
   const double vi = rd(&a.vxs[i]), wi = rd(&a.vys[i]);
-  const bool unmoved = same_bits(vi, rd(&a.svx[i])) && same_bits(wi, rd(&a.svy[i]));
-  bool any = !unmoved;
-  for (uint32_t k = 0; k < nr && !any; ++k) any = rd(&a.min_pusher[rd(&rl[k])]) != NONE;
-  if (!any) return true;  // nothing it reads moved: the guess holds as computed
-  const double ri = a.radii[i];
+  const double svi = rd(&a.svx[i]), swi = rd(&a.svy[i]);
+  uint32_t r8[8];
+#pragma unroll
+  for (int h = 0; h < 8; ++h) r8[h] = rd(&rl[h]);  // rows are whole; used up to rcount
+  bool any = !(same_bits(vi, svi) && same_bits(wi, swi));
+  if (!any) {
+    uint32_t mp[8];
+#pragma unroll
+    for (int h = 0; h < 8; ++h) mp[h] = (uint32_t)h < nr ? rd(&a.min_pusher[r8[h]]) : NONE;
+#pragma unroll
+    for (int h = 0; h < 8; ++h) any |= mp[h] != NONE;
+    for (uint32_t k = 8; k < nr && !any; ++k) any = rd(&a.min_pusher[rd(&rl[k])]) != NONE;
+  }
+  if (!any) return V_OK;  // nothing it reads moved: the guess holds as computed
   const double xi = a.xs[i] + vi, yi = a.ys[i] + wi;
-  if (xi != xi || yi != yi) return true;
-  auto clear = [&](uint32_t j, double rj) -> bool {
-    const double r = ri + rj;
-    const uint32_t lo = rd(&a.min_pusher[j]), hi = rd(&a.max_pusher[j]);
-    double vj, wj;
-    if (lo == NONE || lo > i) {
-      vj = rd(&a.svx[j]);
-      wj = rd(&a.svy[j]);
-    } else if (hi < i) {
-      vj = rd(&a.vxs[j]);
-      wj = rd(&a.vys[j]);
-    } else {
-      const double dx = xi - a.xs[j] - rd(&a.svx[j]), dy = yi - a.ys[j] - rd(&a.svy[j]);
-      const double gap = sqrt(dx * dx + dy * dy) - r - rd(&a.push[j]);
-      return gap > 1e-9 * (r + 1);
-    }
-    const double x = xi - a.xs[j] - vj, y = yi - a.ys[j] - wj;
-    return !(x * x + y * y < r * r);
-  };
-  // replay the recorded cells (valid while i stays within its margin)
+  if (xi != xi || yi != yi) return V_OK;
   const uint16_t nv = rd(&a.vcount[i]);
   const double md = rd(&a.mdelta[i]) * (1 - 1e-9);
-  if (nv != VISIT_NONE && fabs(xi - a.px[i]) < md && fabs(yi - a.py[i]) < md) {
-    const uint32_t *vl = a.vlist + (size_t)i * VISIT_CAP;
-    const uint32_t *va = a.vaux + (size_t)i * VISIT_CAP;
-    uint32_t ex_until = 0;
-    for (uint32_t t = 0; t < nv; ++t) {
-      const uint32_t c = rd(&vl[t]), x = rd(&va[t]);
+  if (nv != VISIT_NONE && fabs(xi - a.px[i]) < md && fabs(yi - a.py[i]) < md) return V_REPLAY;
+  return V_TRAVERSE;
+}
+
+// V by the exact traversal of inactive node i, by the warp (windows of 32
+// cells from the node's enclosing cell, as warp_traverse): every head j > i it
+// examines must be a guessed one and clear. Returns false when the turn could
+// write.
+__device__ bool warp_inactive_traverse(const SpecArgs &a, uint32_t i) {
+  const unsigned lane = threadIdx.x & 31;
+  const uint32_t *rl = a.rlist + (size_t)i * SPEC_CAP;
+  const uint32_t nr = rd(&a.rcount[i]);
+  const uint32_t j0 = lane < nr ? rd(&rl[lane]) : NONE, j1 = lane + 32 < nr ? rd(&rl[lane + 32]) : NONE;
+  const double xi = a.xs[i] + rd(&a.vxs[i]), yi = a.ys[i] + rd(&a.vys[i]);
+  const double ri = a.radii[i];
+  uint32_t start = 0;
+  if (lane == 0) start = start_cell(a, i, xi, yi, ri + a.rec[0].r);
+  start = __shfl_sync(FULL, start, 0);
+  const uint32_t len = start == 0 ? a.info[1] : rec_skip(a.rec[start], start);
+  uint32_t carry = 0;
+  bool bad = false;
+  for (uint32_t c0 = start; c0 < len;) {
+    const uint32_t c = c0 + lane;
+    uint32_t up = 0, head = NONE;
+    bool leaf = false;
+    if (c < len) {
       const CRec &q = a.rec[c];
+      leaf = rec_leaf(q);
+      if (leaf) head = q.link & ~LEAF_TAG;
+      else if (pruned(q, xi, yi, ri + q.r)) up = q.link;
+    }
+    uint32_t incl = up;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(FULL, incl, o);
+      if (lane >= (unsigned)o) incl = max(incl, y);
+    }
+    uint32_t before = __shfl_up_sync(FULL, incl, 1);
+    if (lane == 0) before = 0;
+    const bool want = c < len && c >= max(carry, before) && leaf && head > i;
+    if (__any_sync(FULL, want)) {
+      bool found = false;
+      for (int t = 0; t < 32; ++t) {
+        const uint32_t r0 = __shfl_sync(FULL, j0, t), r1 = __shfl_sync(FULL, j1, t);
+        found |= want && (r0 == head || r1 == head);
+      }
+      if (want && (!found || !head_clear(a, i, xi, yi, ri, head, a.radii[head]))) bad = true;
+    }
+    carry = max(carry, __shfl_sync(FULL, incl, 31));
+    c0 = max(c0 + 32, carry);
+  }
+  return !__any_sync(FULL, bad);
+}
+
+// V's replay of inactive node i's recorded cells, by the warp (entries 4 lane
+// .. 4 lane + 3, as warp_replay): a recorded cell is skipped when it lies in
+// the subtree of an earlier recorded cell the exact test prunes; every head
+// j > i left must be clear. Returns false when the turn could write.
+__device__ bool warp_inactive_replay(const SpecArgs &a, uint32_t i) {
+  const unsigned lane = threadIdx.x & 31;
+  const uint32_t *vl = a.vlist + (size_t)i * VISIT_CAP, *vx = a.vaux + (size_t)i * VISIT_CAP;
+  const uint16_t nv = rd(&a.vcount[i]);
+  const double xi = a.xs[i] + rd(&a.vxs[i]), yi = a.ys[i] + rd(&a.vys[i]);
+  const double ri = a.radii[i];
+  uint32_t cell[4], upto[4];
+  bool bad[4];
+  uint32_t run = 0;
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const uint32_t t = 4 * lane + u;
+    cell[u] = NONE;
+    upto[u] = 0;
+    bad[u] = false;
+    if (t < nv) {
+      const uint32_t c = rd(&vl[t]), x = rd(&vx[t]);
+      cell[u] = c;
       if (x & LEAF_TAG) {
         const uint32_t j = x & ~LEAF_TAG;
-        if (j > i && c >= ex_until && !clear(j, q.r)) return false;
-        continue;
+        if (j > i) bad[u] = !head_clear(a, i, xi, yi, ri, j, a.radii[j]);
+      } else {
+        const CRec &q = a.rec[c];
+        if (pruned(q, xi, yi, ri + q.r)) upto[u] = x;
       }
-      if (c >= ex_until && pruned(q, xi, yi, ri + q.r)) ex_until = x;
     }
-    return true;
+    run = max(run, upto[u]);
   }
-  const uint32_t len = a.info[1];
-  for (uint32_t c = 0; c < len;) {
-    const CRec &q = a.rec[c];
-    const double r = ri + q.r;
-    if (rec_leaf(q)) {
-      const uint32_t j = q.link & ~LEAF_TAG;
-      if (j > i) {
-        bool found = false;
-        for (uint32_t k = 0; k < nr && !found; ++k) found = rd(&rl[k]) == j;
-        if (!found || !clear(j, q.r)) return false;
-      }
-      c = c + 1;
-      continue;
-    }
-    c = pruned(q, xi, yi, r) ? q.link : c + 1;
+  uint32_t incl = run;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t yv = __shfl_up_sync(FULL, incl, o);
+    if (lane >= (unsigned)o) incl = max(incl, yv);
   }
-  return true;
+  uint32_t ex = __shfl_up_sync(FULL, incl, 1);
+  if (lane == 0) ex = 0;
+  bool fail = false;
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    if (cell[u] == NONE) continue;
+    if (bad[u] && cell[u] >= ex) fail = true;
+    ex = max(ex, upto[u]);
+  }
+  return !__any_sync(FULL, fail);
+}
+
+// V for the nodes at Morton positions base .. base + 31, a lane each; the
+// nodes whose record must be replayed or traversed go to a list that whole
+// warps share out (item: node | 1 << 31 for a traversal).
+__device__ inline void promote_inactive(const SpecArgs &a, uint32_t i) {
+  a.state[i] = 4;  // inactive, but its turn would write
+  atomicAdd(&a.counters[C_FAIL], 1u);
+  atomicAdd(&a.counters[C_FAIL_MOVED], 1u);
+}
+
+__device__ void warp_check_inactive(const SpecArgs &a, uint32_t base) {
+  const uint32_t k = base + (threadIdx.x & 31);
+  uint32_t i = NONE;
+  int res = V_OK;
+  if (k < a.n) {
+    i = a.perm[k];
+    if (rd(&a.state[i]) == 0) res = inactive_quick(a, i);
+  }
+  if (res == V_WRITES) promote_inactive(a, i);
+  const bool more = res == V_REPLAY || res == V_TRAVERSE;
+  warp_append(more, i | (res == V_TRAVERSE ? 0x80000000u : 0u), a.vwork, &a.counters[C_VWORK]);
+}
+
+__device__ void warp_check_inactive_item(const SpecArgs &a, uint32_t item) {
+  const uint32_t i = item & 0x7fffffffu;
+  const bool ok = item >> 31 ? warp_inactive_traverse(a, i) : warp_inactive_replay(a, i);
+  if (!ok && (threadIdx.x & 31) == 0) promote_inactive(a, i);
 }
 
 // The exact traversal of node i from (xi, yi), by the warp: windows of 32
@@ -473,6 +601,19 @@ __device__ void warp_offsets(const SpecArgs &a, uint32_t base) {
     a.rlen[j] = c;
     a.roff[j] = b + incl - c;
   }
+  warp_append(c > 4, j, a.biglink, &a.counters[C_BIGLINK]);
+}
+
+// Active nodes base .. base + 31 with more than four heads go to the list
+// of nodes whose entries a whole warp writes.
+__device__ void warp_find_bigfill(const SpecArgs &a, uint32_t base, uint32_t n_active) {
+  const uint32_t k = base + (threadIdx.x & 31);
+  uint32_t i = NONE, nr = 0;
+  if (k < n_active) {
+    i = rd(&a.active[k]);
+    nr = rd(&a.rcount[i]);
+  }
+  warp_append(nr > 4, i, a.bigfill, &a.counters[C_BIGFILL]);
 }
 
 // Node i's entry for head h (or itself) into the list of node j.
@@ -482,7 +623,8 @@ __device__ inline void put_entry(const SpecArgs &a, uint32_t j, uint32_t i, uint
 }
 
 // Active nodes base .. base + 31 write their entries into the lists (cnt
-// returns to zero): a lane each, the warp together for nodes with many heads.
+// returns to zero): a lane each (the head entries of nodes with more than
+// four heads are written by warp_fill_big).
 __device__ void warp_fill(const SpecArgs &a, uint32_t base, uint32_t n_active) {
   const unsigned lane = threadIdx.x & 31;
   const uint32_t k = base + lane;
@@ -490,26 +632,42 @@ __device__ void warp_fill(const SpecArgs &a, uint32_t base, uint32_t n_active) {
   uint64_t wm = 0;
   if (k < n_active) {
     i = rd(&a.active[k]);
+    const uint32_t *rl = a.rlist + (size_t)i * SPEC_CAP;
+    // the node, its first four heads (read whole; used up to rcount), then
+    // their places, all issued together
     nr = rd(&a.rcount[i]);
     wm = rd(&a.wmask[i]);
-    put_entry(a, i, i, SELF_ENTRY, 1);
+    uint32_t j[4];
+#pragma unroll
+    for (int h = 0; h < 4; ++h) j[h] = rd(&rl[h]);
+    const uint32_t nf = nr <= 4 ? nr : 0;
+    uint32_t off[5], old[5];
+    off[4] = rd(&a.roff[i]);
+    old[4] = atomicSub(&a.cnt[i], 1u);
+#pragma unroll
+    for (int h = 0; h < 4; ++h)
+      if ((uint32_t)h < nf) {
+        off[h] = rd(&a.roff[j[h]]);
+        old[h] = atomicSub(&a.cnt[j[h]], 1u);
+      }
+    a.ent[off[4] + old[4] - 1] = ((uint64_t)i << 32) | (SELF_ENTRY << 1) | 1;
+#pragma unroll
+    for (int h = 0; h < 4; ++h)
+      if ((uint32_t)h < nf)
+        a.ent[off[h] + old[h] - 1] = ((uint64_t)i << 32) | (h << 1) | ((wm >> h) & 1);
     a.pred[i] = 0;
     a.lev[i] = 0;
     a.queue[(size_t)k * QSTRIDE] = NONE;
-    if (nr <= 4) {
-      const uint32_t *rl = a.rlist + (size_t)i * SPEC_CAP;
-      for (uint32_t h = 0; h < nr; ++h) put_entry(a, rd(&rl[h]), i, h, (wm >> h) & 1);
-    }
   }
-  unsigned big = __ballot_sync(FULL, nr > 4);
-  while (big) {
-    const int t = __ffs(big) - 1;
-    big &= big - 1;
-    const uint32_t it = __shfl_sync(FULL, i, t), nt = __shfl_sync(FULL, nr, t);
-    const uint64_t wt = __shfl_sync(FULL, wm, t);
-    const uint32_t *rl = a.rlist + (size_t)it * SPEC_CAP;
-    for (uint32_t h = lane; h < nt; h += 32) put_entry(a, rd(&rl[h]), it, h, (wt >> h) & 1);
-  }
+}
+
+// The head entries of a node with more than four heads, by the warp.
+__device__ void warp_fill_big(const SpecArgs &a, uint32_t i) {
+  const unsigned lane = threadIdx.x & 31;
+  const uint32_t nr = rd(&a.rcount[i]);
+  const uint64_t wm = rd(&a.wmask[i]);
+  const uint32_t *rl = a.rlist + (size_t)i * SPEC_CAP;
+  for (uint32_t h = lane; h < nr; h += 32) put_entry(a, rd(&rl[h]), i, h, (wm >> h) & 1);
 }
 
 // One list of L > 1 entries at `off`, by the warp: sorted by node (the rank of
@@ -573,8 +731,8 @@ __device__ void warp_link_list(const SpecArgs &a, uint32_t off, uint32_t L) {
   }
 }
 
-// Lists of nodes base .. base + 31: up to four entries are settled by their
-// lane, longer lists by the warp in turn.
+// Lists of nodes base .. base + 31 with up to four entries, a lane each
+// (longer lists are shared out to whole warps).
 __device__ void warp_link(const SpecArgs &a, uint32_t base) {
   const unsigned lane = threadIdx.x & 31;
   const uint32_t j = base + lane;
@@ -626,12 +784,6 @@ __device__ void warp_link(const SpecArgs &a, uint32_t base) {
       }
       if (w) nw = (uint32_t)t;
     }
-  }
-  unsigned big = __ballot_sync(FULL, L > 4);
-  while (big) {
-    const int t = __ffs(big) - 1;
-    big &= big - 1;
-    warp_link_list(a, __shfl_sync(FULL, off, t), __shfl_sync(FULL, L, t));
   }
 }
 
@@ -728,14 +880,18 @@ __device__ uint32_t warp_run(const SpecArgs &a, uint32_t i, bool stamp, TurnTall
   // per head: the offset (x, y) = (xi - xs[j] - vxs[j], ...) of the turn,
   // formed as the turn forms it, and the head's radius
   const double xi = a.xs[i] + vi, yi = a.ys[i] + wi;
-  double hx[2], hy[2], hr[2];
+  // (a ready turn's heads are not written by any other turn while it runs:
+  // their velocities loaded here are the ones its pushes update)
+  double hx[2], hy[2], hr[2], hv[2], hw[2];
   const uint32_t jj[2] = {j0, j1};
   for (int h = 0; h < 2; ++h) {
     const uint32_t j = jj[h];
-    hx[h] = hy[h] = hr[h] = 0;
+    hx[h] = hy[h] = hr[h] = hv[h] = hw[h] = 0;
     if (j == NONE) continue;
-    hx[h] = xi - a.xs[j] - rd(&a.vxs[j]);
-    hy[h] = yi - a.ys[j] - rd(&a.vys[j]);
+    hv[h] = rd(&a.vxs[j]);
+    hw[h] = rd(&a.vys[j]);
+    hx[h] = xi - a.xs[j] - hv[h];
+    hy[h] = yi - a.ys[j] - hw[h];
     hr[h] = a.radii[j];
   }
   const double ri = a.radii[i], ri2 = ri * ri;
@@ -751,13 +907,14 @@ __device__ uint32_t warp_run(const SpecArgs &a, uint32_t i, bool stamp, TurnTall
   // each lane evaluates the examined heads with indices lane and lane + 32
   bool fail = false, jig = false;
   uint64_t over = 0;
-  uint32_t pj[2];
-  double pdx[2], pdy[2];
-  int np = 0;
-  for (int h = 0; h < 2 && !fail_read; ++h) {
+  // per head slot h: the push on head jj[h] (pushed[h]), written after the
+  // warp agrees the turn holds
+  bool pushed[2] = {false, false};
+  double pdx[2] = {0, 0}, pdy[2] = {0, 0};
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
     const uint32_t e = lane + 32 * h;
-    if (e >= nr || !((ex >> e) & 1)) continue;
-    const uint32_t j = jj[h];
+    if (fail_read || e >= nr || !((ex >> e) & 1)) continue;
     double rj = hr[h];
     double r = ri + rj;
     double x = hx[h];
@@ -782,10 +939,9 @@ __device__ uint32_t warp_run(const SpecArgs &a, uint32_t i, bool stamp, TurnTall
     cy[e] = y * r;
     over |= 1ull << e;
     r = 1 - r;
-    pj[np] = j;
-    pdx[np] = x * r;
-    pdy[np] = y * r;
-    ++np;
+    pushed[h] = true;
+    pdx[h] = x * r;
+    pdy[h] = y * r;
   }
   fail = __any_sync(FULL, fail);
   jig = __any_sync(FULL, jig);
@@ -819,10 +975,12 @@ __device__ uint32_t warp_run(const SpecArgs &a, uint32_t i, bool stamp, TurnTall
     }
     if (unmoved) ++tally.fast;
     else ++tally.slow;
-    for (int h = 0; h < np; ++h) {
-      const uint32_t j = pj[h];
-      a.vxs[j] = rd(&a.vxs[j]) - pdx[h];
-      a.vys[j] = rd(&a.vys[j]) - pdy[h];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      if (!pushed[h]) continue;
+      const uint32_t j = jj[h];
+      a.vxs[j] = hv[h] - pdx[h];
+      a.vys[j] = hw[h] - pdy[h];
       atomicAdd(&a.push[j], sqrt(pdx[h] * pdx[h] + pdy[h] * pdy[h]));
       atomicMin(&a.min_pusher[j], i);
       atomicMax(&a.max_pusher[j], i);
@@ -838,8 +996,10 @@ __device__ uint32_t warp_run(const SpecArgs &a, uint32_t i, bool stamp, TurnTall
     for (uint32_t t = 0; t < c; ++t)
       atomicMax(&a.lev[t ? (uint32_t)(rd(&a.ents[(ss[h] >> 32) + t]) >> 32) : ff[h]], nl);
   }
+  // a lane's successors wait only on the heads it wrote (its own entries):
+  // the fence orders those writes before the releases
   __syncwarp();
-  __threadfence();
+  if ((pushed[0] || pushed[1]) && !(fail_read || fail || jig)) __threadfence();
   uint32_t mine = NONE;  // the first turn this lane made ready; later ones are queued
   for (int h = 0; h < 2; ++h) {
     const uint32_t c = (uint32_t)ss[h];
@@ -909,7 +1069,7 @@ __device__ void spec_serial(const SpecArgs &a) {
   a.rng->lcg = s;
 }
 
-__global__ void __launch_bounds__(SPEC_THREADS, 3) k_collide_spec(SpecArgs a) {
+__global__ void __launch_bounds__(SPEC_THREADS, 2) k_collide_spec(SpecArgs a) {
   __shared__ double contrib[SPEC_WARPS][2][SPEC_CAP];
   cg::grid_group g = cg::this_grid();
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
@@ -980,13 +1140,29 @@ __global__ void __launch_bounds__(SPEC_THREADS, 3) k_collide_spec(SpecArgs a) {
       for (uint32_t k = gw; k < n_active; k += nwarps) warp_count(a, rd(&a.active[k]));
       g.sync();
     }
-    // The access lists: places, entries, then sorted and linked.
+    // The access lists: places (and the nodes and lists with more than four
+    // entries, which whole warps share out), entries, then sorted and linked.
     for (uint32_t base = gw * 32; base < n; base += nwarps * 32) warp_offsets(a, base);
-    if (tid == 0) a.counters[C_QHEAD] = a.counters[C_QTAIL] = 0;
+    for (uint32_t base = gw * 32; base < n_active; base += nwarps * 32)
+      warp_find_bigfill(a, base, n_active);
+    if (tid == 0) a.counters[C_QHEAD] = a.counters[C_QTAIL] = a.counters[C_VWORK] = 0;
     g.sync();
+    if (tid == 0 && attempt == 0) a.stamps[13] = now_ns();
     for (uint32_t base = gw * 32; base < n_active; base += nwarps * 32) warp_fill(a, base, n_active);
+    {
+      const uint32_t nb = rd(&a.counters[C_BIGFILL]);
+      for (uint32_t k = gw; k < nb; k += nwarps) warp_fill_big(a, rd(&a.bigfill[k]));
+    }
     g.sync();
+    if (tid == 0 && attempt == 0) a.stamps[14] = now_ns();
     for (uint32_t base = gw * 32; base < n; base += nwarps * 32) warp_link(a, base);
+    {
+      const uint32_t nb = rd(&a.counters[C_BIGLINK]);
+      for (uint32_t k = gw; k < nb; k += nwarps) {
+        const uint32_t j = rd(&a.biglink[k]);
+        warp_link_list(a, rd(&a.roff[j]), rd(&a.rlen[j]));
+      }
+    }
     g.sync();
     if (tid == 0 && attempt < 3) a.stamps[10 + attempt] = now_ns();
     // E: the turns with nothing to wait for are queued; warps claim queue
@@ -1018,14 +1194,11 @@ __global__ void __launch_bounds__(SPEC_THREADS, 3) k_collide_spec(SpecArgs a) {
     g.sync();
     if (tid == 0 && attempt < 3) a.stamps[2 + 2 * attempt] = now_ns();
     // V: inactive nodes stayed no-ops (Morton order, as G).
-    for (uint32_t k = tid; k < n; k += nth) {
-      const uint32_t i = a.perm[k];
-      if (rd(&a.state[i]) != 0) continue;
-      if (!spec_inactive_ok(a, i)) {
-        a.state[i] = 4;  // inactive, but its turn would write: promote
-        atomicAdd(&a.counters[C_FAIL], 1u);
-        atomicAdd(&a.counters[C_FAIL_MOVED], 1u);
-      }
+    for (uint32_t base = gw * 32; base < n; base += nwarps * 32) warp_check_inactive(a, base);
+    g.sync();
+    {
+      const uint32_t nw = rd(&a.counters[C_VWORK]);
+      for (uint32_t k = gw; k < nw; k += nwarps) warp_check_inactive_item(a, rd(&a.vwork[k]));
     }
     g.sync();
     if (tid == 0 && attempt < 3) a.stamps[3 + 2 * attempt] = now_ns();
@@ -1058,6 +1231,8 @@ __global__ void __launch_bounds__(SPEC_THREADS, 3) k_collide_spec(SpecArgs a) {
       a.counters[C_FAIL] = 0;
       a.counters[C_DONE] = 0;
       a.counters[C_ALLOC] = 0;
+      a.counters[C_BIGFILL] = 0;
+      a.counters[C_BIGLINK] = 0;
     }
     g.sync();
   }
@@ -1108,6 +1283,7 @@ static void spec_arrays(CollideSpec &s, F f) {
   f((void **)&s.pred, 4);
   f((void **)&s.lev, 4);
   f((void **)&s.queue, QSTRIDE * 4ull);
+  f((void **)&s.work, 3 * 4ull);  // bigfill, biglink, vwork
 }
 
 int collide_spec_reserve(CollideSpec &s, uint32_t n) {
@@ -1156,8 +1332,8 @@ int collide_parallel(TreeDev &t, const NodeArrays &a, const double *radii, doubl
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_collide_spec, SPEC_THREADS, 0);
-    // blocks per SM: full occupancy (at most 3), or D3_COLLIDE_BLOCKS_PER_SM
-    int want = per > 3 ? 3 : per;
+    // blocks per SM: full occupancy (at most 2), or D3_COLLIDE_BLOCKS_PER_SM
+    int want = per > 2 ? 2 : per;
     if (const char *e = getenv("D3_COLLIDE_BLOCKS_PER_SM")) {
       const int v = atoi(e);
       if (v >= 1 && v <= want) want = v;
@@ -1181,6 +1357,9 @@ int collide_parallel(TreeDev &t, const NodeArrays &a, const double *radii, doubl
   args.state = s.state; args.active = s.active;
   args.cnt = s.cnt; args.rlen = s.rlen; args.roff = s.roff; args.ent = s.ent; args.ents = s.ents;
   args.succ = s.succ; args.pred = s.pred; args.lev = s.lev; args.queue = s.queue;
+  args.bigfill = s.work;
+  args.biglink = s.work + s.cap;
+  args.vwork = s.work + 2ull * s.cap;
   args.push = s.push; args.push_prev = s.push_prev; args.min_pusher = s.min_pusher;
   args.max_pusher = s.max_pusher; args.counters = s.counters; args.stamps = s.stamps;
   args.rng = rng;

@@ -1009,9 +1009,10 @@ double sim_stat(uint32_t h, uint32_t which) {
     phase_collect(s);
     return (double)s->phase_n[which - 200];
   }
-  if (which >= 1000 && which < 1512) {
-    unsigned long long st[512];
-    cudaMemcpy(st, s->spec.stamps, sizeof st, cudaMemcpyDeviceToHost);
+  if (which >= 1000 && which < 1144) {
+    // the last parallel collide's raw stamps (globaltimer ns, and counts)
+    unsigned long long st[144];
+    if (cudaMemcpy(st, s->spec.stamps, sizeof st, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
     return (double)st[which - 1000];
   }
   if ((which >= 300 && which < 364) || (which >= 400 && which < 464)) {

@@ -108,6 +108,7 @@ struct CollideSpec {
   uint32_t *cnt = nullptr, *rlen = nullptr, *roff = nullptr;  // the access lists
   uint64_t *ent = nullptr, *ents = nullptr, *succ = nullptr;
   uint32_t *pred = nullptr, *lev = nullptr, *queue = nullptr;
+  uint32_t *work = nullptr;  // 3 * cap: items shared out to whole warps
   double *push = nullptr;
   uint32_t *min_pusher = nullptr, *max_pusher = nullptr;
   uint32_t *vlist = nullptr;

@@ -158,6 +158,7 @@ double sim_last_tick_ms(uint32_t h);
  * scan, cell owners, the cells); with profiling on, 300 + k microseconds from the end of
  * the last parallel collide's first list build to its last turn of depth k,
  * 400 + k its turns of depth k (k < 63; 63 counts every deeper turn);
+ * 1000 + k (k < 144) its raw stamps (globaltimer ns, then per-depth data);
  * 100 + k milliseconds and 200 + k count of phase k
  * since sim_set_profile(h, 1): 0 many-body tree, 1 many-body accumulation,
  * 2 many-body traversal, 3 exact link, 4 collide tree and radii, 5 collide

@@ -554,10 +554,38 @@ struct LinkCoopArgs {
   uint32_t *flag;
 };
 
+// A thread's first link of a level, with everything about it that does not
+// change during the pass (e = NONE: no link).
+struct LinkPre {
+  uint32_t e, src, tgt;
+  double dist, str, bias, xt, yt, xsrc, ysrc;
+};
+
+__device__ inline void link_params(const LinkArrays &l, uint32_t e, LinkPre &p) {
+  p.e = e;
+  if (e == NONE) return;
+  p.src = l.source[e];
+  p.tgt = l.target[e];
+  p.dist = l.distance[e];
+  p.str = l.strength[e];
+  p.bias = l.bias[e];
+}
+
+__device__ inline void link_positions(const double *xs, const double *ys, LinkPre &p) {
+  if (p.e == NONE) return;
+  p.xt = xs[p.tgt];
+  p.yt = ys[p.tgt];
+  p.xsrc = xs[p.src];
+  p.ysrc = ys[p.src];
+}
+
 // The level-scheduled pass in one cooperative launch: the pass-start snapshot,
 // then per iteration and level its links (disjoint nodes) with a grid barrier
 // between levels, then the snapshot back if a link met a zero or NaN delta
-// (the serial kernel then runs the pass with its draws).
+// (the serial kernel then runs the pass with its draws). Each thread's first
+// link of a level is pipelined: its id two levels ahead, its parameters one
+// level ahead and its endpoints' positions before the barrier, so a level
+// waits only for the velocities.
 __global__ void __launch_bounds__(256) k_link_coop(LinkCoopArgs a) {
   cg::grid_group g = cg::this_grid();
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
@@ -566,13 +594,55 @@ __global__ void __launch_bounds__(256) k_link_coop(LinkCoopArgs a) {
     a.svx[i] = a.vxs[i];
     a.svy[i] = a.vys[i];
   }
+  const uint32_t L = a.levels;
+  auto first = [&](uint32_t lv) -> uint32_t {
+    if (lv > L) return NONE;
+    const uint32_t lo = a.level_start[lv], hi = a.level_start[lv + 1];
+    return lo + tid < hi ? a.order[lo + tid] : NONE;
+  };
   bool bad = false;
   for (double k = 0; k < a.iterations; k += 1) {
-    for (uint32_t lv = 1; lv <= a.levels; ++lv) {
-      const uint32_t lo = a.level_start[lv], hi = a.level_start[lv + 1];
-      for (uint32_t e = lo + tid; e < hi; e += nth)
-        if (!link_one_cg(a.xs, a.ys, a.vxs, a.vys, a.l, a.order[e], a.alpha)) bad = true;
+    LinkPre cur, nxt;
+    link_params(a.l, first(1), cur);
+    link_positions(a.xs, a.ys, cur);
+    uint32_t e_next = first(2);
+    for (uint32_t lv = 1; lv <= L; ++lv) {
+      double vxt = 0, vyt = 0, vxsrc = 0, vysrc = 0;
+      if (cur.e != NONE) {
+        vxt = __ldcg(&a.vxs[cur.tgt]);
+        vyt = __ldcg(&a.vys[cur.tgt]);
+        vxsrc = __ldcg(&a.vxs[cur.src]);
+        vysrc = __ldcg(&a.vys[cur.src]);
+      }
+      link_params(a.l, e_next, nxt);
+      const uint32_t e_after = first(lv + 2);
+      if (cur.e != NONE) {
+        double x = cur.xt + vxt - cur.xsrc - vxsrc;
+        double y = cur.yt + vyt - cur.ysrc - vysrc;
+        if (x == 0 || x != x || y == 0 || y != y) {
+          bad = true;
+        } else {
+          double len = sqrt(x * x + y * y);
+          len = (len - cur.dist) / len * a.alpha * cur.str;
+          x *= len;
+          y *= len;
+          double b = cur.bias;
+          a.vxs[cur.tgt] = vxt - x * b;
+          a.vys[cur.tgt] = vyt - y * b;
+          b = 1 - b;
+          a.vxs[cur.src] = vxsrc + x * b;
+          a.vys[cur.src] = vysrc + y * b;
+        }
+      }
+      {  // a level with more links than threads: the rest, unpipelined
+        const uint32_t lo = a.level_start[lv], hi = a.level_start[lv + 1];
+        for (uint32_t e = lo + tid + nth; e < hi; e += nth)
+          if (!link_one_cg(a.xs, a.ys, a.vxs, a.vys, a.l, a.order[e], a.alpha)) bad = true;
+      }
+      link_positions(a.xs, a.ys, nxt);
       g.sync();
+      cur = nxt;
+      e_next = e_after;
     }
   }
   if (bad) atomicOr(a.flag, 1u);

@@ -214,17 +214,24 @@ __device__ inline uint32_t mb_node(const MRec *rec, const uint32_t *perm,
   double vx = vxs[i], vy = vys[i];
   uint32_t draws = 0;
   bool flagged = false;
+  // The next cell follows from the current record alone (its skip link when
+  // the cell is empty or far enough, else c + 1), so its load is issued
+  // before this cell's arithmetic.
   uint32_t c = 0;
+  MRec q;
+  if (len) q = rec[0];
   while (c < len) {
-    const MRec q = rec[c];
-    const double value = q.value;
-    if (!(value != 0 && value == value)) {
-      c = q.skip;
-      continue;
-    }
-    double x = q.x - nx, y = q.y - ny;
+    const MRec cq = q;
+    const double value = cq.value;
+    const bool live = value != 0 && value == value;
+    double x = cq.x - nx, y = cq.y - ny;
     double l = x * x + y * y;
-    if (q.wt < l) {
+    const bool far = live && cq.wt < l;
+    const uint32_t next = !live || far ? cq.skip : c + 1;
+    if (next < len) q = rec[next];
+    c = next;
+    if (!live) continue;
+    if (far) {
       if (l < p.dmax2) {
         if (RECORD && (x == 0 || y == 0)) {
           flagged = true;
@@ -239,19 +246,12 @@ __device__ inline uint32_t mb_node(const MRec *rec, const uint32_t *perm,
           vy += y * value * p.alpha / l;
         }
       }
-      c = q.skip;
       continue;
     }
-    if (q.head == NONE) {
-      c = c + 1;
-      continue;
-    }
-    if (l >= p.dmax2) {
-      c = c + 1;
-      continue;
-    }
-    const uint32_t first = q.first, count = q.count;
-    const uint32_t head = q.head;
+    if (cq.head == NONE) continue;
+    if (l >= p.dmax2) continue;
+    const uint32_t first = cq.first, count = cq.count;
+    const uint32_t head = cq.head;
     if (head != i || count > 1) {
       if (RECORD && (x == 0 || y == 0)) {
         flagged = true;
@@ -275,7 +275,6 @@ __device__ inline uint32_t mb_node(const MRec *rec, const uint32_t *perm,
         }
       }
     }
-    c = c + 1;
   }
   if (!flagged) {
     vxs[i] = vx;

@@ -81,7 +81,9 @@ __device__ inline Climb climb_up(const uint32_t *parent, const uint8_t *pnch, ui
 
 // many_body.zig:101-135 (accumulate). Leaf: head position, strength summed
 // over the chain from perm[first + count - 1] down. Internal: children 0..3
-// with a truthy |value|. Each finished cell also gets its traversal record.
+// with a truthy |value|. Every cell's traversal record: the thread visiting
+// an internal cell writes its fixed part (width test, skip link); the climb
+// writes its centroid and charge.
 __global__ void k_mb_accumulate(Cell *cells, const uint32_t *parent, const uint8_t *pnch,
                                 uint32_t *counter, const uint32_t *perm, const uint32_t *skip,
                                 const double *xs, const double *ys, const double *strengths,
@@ -89,7 +91,15 @@ __global__ void k_mb_accumulate(Cell *cells, const uint32_t *parent, const uint8
   const uint32_t len = info[1];
   for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < len; c += gridDim.x * blockDim.x) {
     Cell *q = &cells[c];
-    if (!is_leaf(*q)) continue;
+    if (!is_leaf(*q)) {
+      const double w = q->x1 - q->x0;
+      rec[c].wt = w * w / theta2;
+      rec[c].skip = skip[c];
+      rec[c].head = NONE;
+      rec[c].first = 0;
+      rec[c].count = 0;
+      continue;
+    }
     const uint32_t first = q->first, count = q->count;
     uint32_t head = perm[first + count - 1];
     double strength = 0;
@@ -108,52 +118,75 @@ __global__ void k_mb_accumulate(Cell *cells, const uint32_t *parent, const uint8
       r.skip = skip[c]; r.head = head; r.first = first; r.count = count;
       rec[c] = r;
     }
+    auto finish = [&](uint32_t x) {
+      cells[x].x = cx;
+      cells[x].y = cy;
+      cells[x].value = cv;
+      rec[x].x = cx;
+      rec[x].y = cy;
+      rec[x].value = cv;
+    };
     Climb up = climb_up(parent, pnch, c);
     for (;;) {
       const uint32_t p = up.p;
       if (p == NONE) break;
-      Cell *pc = &cells[p];
-      // issued together: the parent's box and skip, and the next step up
-      const double px0 = pc->x0, px1 = pc->x1;
-      const uint32_t pskip = skip[p];
-      const Climb next = climb_up(parent, pnch, p);
-      double st = 0, weight = 0, x = 0, y = 0;
       if (up.nch == 1) {
-        const double w = fabs(cv);
-        if (w > 0) {
-          st += cv;
-          weight += w;
-          x += w * cx;
-          y += w * cy;
-        }
-      } else {
-        __threadfence();
-        if (atomicAdd(&counter[p], 1u) != up.nch - 1) break;
-        __threadfence();
-        for (int k = 0; k < 4; ++k) {
-          uint32_t ch = pc->child[k];
-          if (ch == NONE) continue;
-          double v = ld_cg(&cells[ch].value);
-          double w = fabs(v);
+        // A run of only children: p's only child is done, so p, p - 1, ...
+        // (in preorder an only child follows its parent) while each is an
+        // only child itself; their child counts read 8 at a time.
+        uint8_t pk[8];
+#pragma unroll
+        for (int t = 0; t < 8; ++t) pk[t] = (uint32_t)t <= p ? pnch[p - t] : 0;
+        bool out = false;
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+          const uint32_t x = p - t;
+          double st = 0, weight = 0, sx = 0, sy = 0;
+          const double w = fabs(cv);
           if (w > 0) {
-            st += v;
+            st += cv;
             weight += w;
-            x += w * ld_cg(&cells[ch].x);
-            y += w * ld_cg(&cells[ch].y);
+            sx += w * cx;
+            sy += w * cy;
           }
+          cx = sx / weight;
+          cy = sy / weight;
+          cv = st;
+          finish(x);
+          if (pk[t] != 1) {
+            up = climb_up(parent, pnch, x);
+            out = true;
+            break;
+          }
+        }
+        if (!out) {
+          up.p = p - 8;  // the eighth cell was an only child too
+          up.nch = 1;
+        }
+        continue;
+      }
+      Cell *pc = &cells[p];
+      const Climb next = climb_up(parent, pnch, p);
+      __threadfence();
+      if (atomicAdd(&counter[p], 1u) != up.nch - 1) break;
+      __threadfence();
+      double st = 0, weight = 0, x = 0, y = 0;
+      for (int k = 0; k < 4; ++k) {
+        uint32_t ch = pc->child[k];
+        if (ch == NONE) continue;
+        double v = ld_cg(&cells[ch].value);
+        double w = fabs(v);
+        if (w > 0) {
+          st += v;
+          weight += w;
+          x += w * ld_cg(&cells[ch].x);
+          y += w * ld_cg(&cells[ch].y);
         }
       }
       cx = x / weight;
       cy = y / weight;
       cv = st;
-      pc->x = cx;
-      pc->y = cy;
-      pc->value = cv;
-      const double w = px1 - px0;
-      MRec r;
-      r.x = cx; r.y = cy; r.value = cv; r.wt = w * w / theta2;
-      r.skip = pskip; r.head = NONE; r.first = 0; r.count = 0;
-      rec[p] = r;
+      finish(p);
       up = next;
     }
   }
@@ -174,21 +207,42 @@ __global__ void k_collide_prep(Cell *cells, const uint32_t *parent, const uint8_
     for (;;) {
       const uint32_t p = up.p;
       if (p == NONE) break;
+      if (up.nch == 1) {
+        // a run of only children (as in k_mb_accumulate), 8 levels at a time
+        uint8_t pk[8];
+#pragma unroll
+        for (int t = 0; t < 8; ++t) pk[t] = (uint32_t)t <= p ? pnch[p - t] : 0;
+        bool out = false;
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+          const uint32_t x = p - t;
+          double r = 0;
+          if (cr > r) r = cr;
+          cells[x].r = r;
+          cr = r;
+          if (pk[t] != 1) {
+            up = climb_up(parent, pnch, x);
+            out = true;
+            break;
+          }
+        }
+        if (!out) {
+          up.p = p - 8;
+          up.nch = 1;
+        }
+        continue;
+      }
       Cell *pc = &cells[p];
       const Climb next = climb_up(parent, pnch, p);
+      __threadfence();
+      if (atomicAdd(&counter[p], 1u) != up.nch - 1) break;
+      __threadfence();
       double r = 0;
-      if (up.nch == 1) {
-        if (cr > r) r = cr;
-      } else {
-        __threadfence();
-        if (atomicAdd(&counter[p], 1u) != up.nch - 1) break;
-        __threadfence();
-        for (int k = 0; k < 4; ++k) {
-          uint32_t ch = pc->child[k];
-          if (ch == NONE) continue;
-          double v = ld_cg(&cells[ch].r);
-          if (v > r) r = v;
-        }
+      for (int k = 0; k < 4; ++k) {
+        uint32_t ch = pc->child[k];
+        if (ch == NONE) continue;
+        double v = ld_cg(&cells[ch].r);
+        if (v > r) r = v;
       }
       pc->r = r;
       cr = r;

@@ -414,6 +414,28 @@ __device__ inline uint32_t prefix_end(const uint64_t *keys, uint32_t lo, uint32_
   return l;
 }
 
+// lower_bound by a whole warp (all lanes, same arguments): 32 probes a round.
+__device__ uint32_t warp_lower_bound(const uint64_t *keys, uint32_t lo, uint32_t hi, uint64_t t) {
+  const unsigned lane = threadIdx.x & 31;
+  while (hi - lo > 32) {
+    const uint32_t step = (hi - lo + 31) / 32;
+    const uint32_t pos = lo + lane * step;
+    const unsigned ge = __ballot_sync(0xffffffffu, pos >= hi || keys[pos] >= t);
+    if (ge & 1u) return lo;
+    const uint32_t f = ge ? (uint32_t)__ffs(ge) - 1 : 32;  // the first probe with keys >= t
+    const uint32_t nhi = f == 32 ? hi : min(hi, lo + f * step);
+    lo = lo + (f - 1) * step + 1;
+    hi = nhi;
+  }
+  const uint32_t pos = lo + lane;
+  const unsigned ge = __ballot_sync(0xffffffffu, pos >= hi || keys[pos] >= t);
+  return ge ? min(hi, lo + (uint32_t)__ffs(ge) - 1) : hi;
+}
+
+// Cells at depths below TB_TOP_D (at most 85) search the whole point range:
+// whole warps emit them.
+constexpr int TB_TOP_D = 4;
+
 // Cell emission, one thread per cell. A start k owns cells base[k] +
 // (0 .. dlast - d0) (depths d0 .. dlast); `owner[c]` = k | OWN_TAG for those
 // (below-resolution cells of a deep group stay NONE: the thread of the group's
@@ -421,18 +443,21 @@ __device__ inline uint32_t prefix_end(const uint64_t *keys, uint32_t lo, uint32_
 constexpr uint32_t OWN_TAG = 0x80000000u;
 
 __device__ void own_at(uint32_t k, uint32_t m, const int8_t *lcpx, const uint32_t *base,
-                       const uint32_t *cnt, const uint8_t *leafd, uint32_t *owner, uint32_t *info) {
+                       const uint32_t *cnt, const uint8_t *leafd, uint32_t *owner, uint32_t *info,
+                       uint32_t *top) {
   if (!is_start(lcpx, k)) return;
   const int d0 = k == 0 ? 0 : ldc(&lcpx[k]) + 1;
   const int ld = ldc(&leafd[k]);
   const int dlast = ld == 33 ? 32 : ld;
   const uint32_t c0 = ldc(&base[k]);
   for (int d = d0; d <= dlast; ++d) owner[c0 + (d - d0)] = k | OWN_TAG;
+  for (int d = d0; d <= dlast && d < TB_TOP_D; ++d) top[atomicAdd(&info[8], 1u)] = c0 + (d - d0);
   const uint32_t chain = (uint32_t)(dlast - d0 + 1), all = ldc(&cnt[k]);
   for (uint32_t c = c0 + chain; c < c0 + all; ++c) owner[c] = NONE;
   atomicMax(&info[2], (uint32_t)dlast);
 }
 
+template <bool WARP>
 __device__ void emit_cell(uint32_t c, uint32_t m, uint32_t total, const double *xs, const double *ys,
                           const uint64_t *keys, const int8_t *lcpx, const double *extent,
                           uint32_t *perm, uint32_t *perm_tmp, Frame *frames, const uint32_t *base,
@@ -448,29 +473,45 @@ __device__ void emit_cell(uint32_t c, uint32_t m, uint32_t total, const double *
   const bool deep = ld == 33;
   const uint32_t c0 = ldc(&base[k]);
   const int d = d0 + (int)(c - c0);
+  if (!WARP && d < TB_TOP_D) return;  // a top cell: emitted by a warp
+  const bool writer = !WARP || (threadIdx.x & 31) == 0;
   const uint32_t rend = ldc(&run_end[k]);
   double x0, y0, x1, y1;
   path_bounds(extent, key, d, x0, y0, x1, y1);
-  if (c == 0) parent[0] = NONE;
+  if (c == 0 && writer) {
+    parent[0] = NONE;
+    pnch[0] = 0;  // the root has no parent
+  }
   const bool leaf = !deep && d == ld;
   uint32_t end;
-  if (leaf || (deep && d == 32)) end = rend;
-  else if (d == 0) end = m;
-  else end = prefix_end(keys, k, m, key >> (64 - 2 * d), d);
+  if (leaf || (deep && d == 32)) {
+    end = rend;
+  } else if (d == 0) {
+    end = m;
+  } else if (WARP) {
+    const uint64_t pk = key >> (64 - 2 * d);
+    end = pk + 1 < (1ull << (2 * d)) ? warp_lower_bound(keys, k, m, (pk + 1) << (64 - 2 * d)) : m;
+  } else {
+    end = prefix_end(keys, k, m, key >> (64 - 2 * d), d);
+  }
   Cell cell;
   cell.child[0] = cell.child[1] = cell.child[2] = cell.child[3] = NONE;
   cell.first = k;
   cell.count = end - k;
   cell.x0 = x0; cell.y0 = y0; cell.x1 = x1; cell.y1 = y1;
   cell.x = cell.y = cell.value = cell.r = 0;
-  skip[c] = end < m ? ldc(&base[end]) : total;
+  const uint32_t sk = end < m ? ldc(&base[end]) : total;
+  if (writer) skip[c] = sk;
   if (!leaf && d < 32) {
     const uint64_t top = d == 0 ? 0 : (key >> (64 - 2 * d)) << (64 - 2 * d);
     uint32_t b[5];
     b[0] = k;
     b[4] = end;
-    for (uint32_t q = 1; q < 4; ++q)
-      b[q] = lower_bound(keys, b[q - 1], end, top | ((uint64_t)q << (62 - 2 * d)));
+    for (uint32_t q = 1; q < 4; ++q) {
+      const uint64_t t = top | ((uint64_t)q << (62 - 2 * d));
+      b[q] = WARP ? warp_lower_bound(keys, b[q - 1], end, t) : lower_bound(keys, b[q - 1], end, t);
+    }
+    if (!writer) return;
     uint8_t nch = 0;
     for (int q = 0; q < 4; ++q) nch += b[q] != b[q + 1];
     for (int q = 0; q < 4; ++q) {
@@ -483,6 +524,7 @@ __device__ void emit_cell(uint32_t c, uint32_t m, uint32_t total, const double *
       pnch[ch] = nch;
     }
   }
+  if (!writer) return;
   cells[c] = cell;
   counter[c] = 0;
   if (leaf)
@@ -758,6 +800,7 @@ __global__ void __launch_bounds__(TB_THREADS) k_tree_build(TreeBuildArgs a) {
         a.info[4] = 0;
         a.info[5] = 0;
         a.info[7] = 0;
+        a.info[8] = 0;
       }
     }
     __syncthreads();
@@ -841,13 +884,22 @@ __global__ void __launch_bounds__(TB_THREADS) k_tree_build(TreeBuildArgs a) {
     }
     return;
   }
+  uint32_t *top = reinterpret_cast<uint32_t *>(a.parts);  // the box partials are done with
   for (uint32_t k = tid; k < m; k += nth)
-    own_at(k, m, a.lcpx, a.base, a.cnt, a.leafd, a.counter, a.info);
+    own_at(k, m, a.lcpx, a.base, a.cnt, a.leafd, a.counter, a.info, top);
   g.sync();
   tb_stamp(a, 7);
   for (uint32_t c = tid; c < total; c += nth)
-    emit_cell(c, m, total, a.xs, a.ys, fk, a.lcpx, se, a.perm, a.perm_tmp, a.frames, a.base,
-              a.run_end, a.leafd, a.cells, a.skip, a.parent, a.pnch, a.counter, a.info, a.leaf_of);
+    emit_cell<false>(c, m, total, a.xs, a.ys, fk, a.lcpx, se, a.perm, a.perm_tmp, a.frames, a.base,
+                     a.run_end, a.leafd, a.cells, a.skip, a.parent, a.pnch, a.counter, a.info,
+                     a.leaf_of);
+  {
+    const uint32_t ntop = ldc(&a.info[8]), gw = tid >> 5, nw = nth >> 5;
+    for (uint32_t k = gw; k < ntop; k += nw)
+      emit_cell<true>(ldc(&top[k]), m, total, a.xs, a.ys, fk, a.lcpx, se, a.perm, a.perm_tmp,
+                      a.frames, a.base, a.run_end, a.leafd, a.cells, a.skip, a.parent, a.pnch,
+                      a.counter, a.info, a.leaf_of);
+  }
   __syncthreads();
   tb_stamp(a, 8);  // block 0's cells only
 }

@@ -73,6 +73,12 @@ struct DSim {
   // first center force of a tick changes).
   cudaStream_t side = nullptr;
   cudaEvent_t ev_xready = nullptr, ev_sumdone = nullptr;
+  // sim_sync_in copies x, y on `stream` and the rest of the node state on
+  // `upload`; `stream` waits for ev_rest before anything else reads it.
+  cudaStream_t upload = nullptr;
+  cudaEvent_t ev_upstart = nullptr, ev_rest = nullptr;
+  bool rest_pending = false;
+  bool settle_after_accumulate = false;  // sim_tick: settle in the first many-body force
   uint32_t sync_mode = D3_SYNC_PER_CALL;
   // tree mirrors (tree_info)
   Cell *h_cells = nullptr;
@@ -148,9 +154,25 @@ bool device_ok() {
   return g_device_ok == 1;
 }
 
-DSim *get_sim(uint32_t h) {
+// The simulation's stream waits for the node state still being uploaded.
+void settle(DSim *s) {
+  if (!s->rest_pending) return;
+  cudaStreamWaitEvent(s->stream, s->ev_rest, 0);
+  s->rest_pending = false;
+}
+
+// The simulation without settling (sim_tick settles when it first needs
+// the uploaded velocities).
+DSim *get_sim_raw(uint32_t h) {
   if (h == 0 || h > g_sims.size()) return nullptr;
   return g_sims[h - 1];
+}
+
+// Every entry point but sim_tick: the simulation, settled.
+DSim *get_sim(uint32_t h) {
+  DSim *s = get_sim_raw(h);
+  if (s) settle(s);
+  return s;
 }
 
 DForce *get_force(DSim *s, uint32_t fh) {
@@ -270,17 +292,26 @@ NodeArrays nodes_of(DSim *s) {
   return a;
 }
 
-int sync_in_impl(DSim *s) {
+// Host mirrors -> device. x and y go on the simulation's stream; vx, vy, fx,
+// fy and the fixed bits on the upload stream after all earlier work, so that
+// a tick's tree build can overlap them (defer: the caller settles later;
+// otherwise settled here).
+int sync_in_impl(DSim *s, bool defer = false) {
   const size_t n = s->n;
   if (n) {
-    cudaStream_t st = s->stream;
+    cudaStream_t st = s->stream, up = s->upload;
     cudaMemcpyAsync(s->d_x, s->h_x, n * 8, cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(s->d_y, s->h_y, n * 8, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(s->d_vx, s->h_vx, n * 8, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(s->d_vy, s->h_vy, n * 8, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(s->d_fx, s->h_fx, n * 8, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(s->d_fy, s->h_fy, n * 8, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(s->d_fixed, s->h_fixed, n, cudaMemcpyHostToDevice, st);
+    cudaEventRecord(s->ev_upstart, st);
+    cudaStreamWaitEvent(up, s->ev_upstart, 0);
+    cudaMemcpyAsync(s->d_vx, s->h_vx, n * 8, cudaMemcpyHostToDevice, up);
+    cudaMemcpyAsync(s->d_vy, s->h_vy, n * 8, cudaMemcpyHostToDevice, up);
+    cudaMemcpyAsync(s->d_fx, s->h_fx, n * 8, cudaMemcpyHostToDevice, up);
+    cudaMemcpyAsync(s->d_fy, s->h_fy, n * 8, cudaMemcpyHostToDevice, up);
+    cudaMemcpyAsync(s->d_fixed, s->h_fixed, n, cudaMemcpyHostToDevice, up);
+    cudaEventRecord(s->ev_rest, up);
+    s->rest_pending = true;
+    if (!defer) settle(s);
   }
   for (DForce *f : s->forces)
     if (f) upload_force(s, f);
@@ -365,8 +396,11 @@ int run_many_body(DSim *s, DForce *f, double alpha) {
     many_body_exact(s->tree, a, f->d_f[0], p, s->d_rng, s->scratch, status_word(s), false,
                     s->stream, [&](int ph) {
                       phase_end(s, ph, e);
+                      // the traversal reads the velocities (sim_tick's first force)
+                      if (ph == 1 && s->settle_after_accumulate) settle(s);
                       e = phase_begin(s);
                     });
+    settle(s);
     phase_end(s, PH_MB_TRAVERSE, e);
     return D3_OK;
   }
@@ -556,12 +590,15 @@ uint32_t sim_create(void) {
   if (!device_ok()) return 0;
   DSim *s = new DSim();
   if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&s->upload, cudaStreamNonBlocking) != cudaSuccess) {
     delete s;
     return 0;
   }
   cudaEventCreateWithFlags(&s->ev_xready, cudaEventDisableTiming);
   cudaEventCreateWithFlags(&s->ev_sumdone, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&s->ev_upstart, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&s->ev_rest, cudaEventDisableTiming);
   cudaMalloc(&s->d_rng, sizeof(Rng));
   cudaMallocHost(&s->h_rng, sizeof(Rng));
   cudaMalloc(&s->d_words, 16 * sizeof(uint32_t));
@@ -617,6 +654,10 @@ int32_t sim_destroy(uint32_t h) {
   cudaEventDestroy(s->ev_sumdone);
   cudaStreamSynchronize(s->side);
   cudaStreamDestroy(s->side);
+  cudaStreamSynchronize(s->upload);
+  cudaEventDestroy(s->ev_upstart);
+  cudaEventDestroy(s->ev_rest);
+  cudaStreamDestroy(s->upload);
   cudaStreamDestroy(s->stream);
   delete s;
   g_sims[h - 1] = nullptr;
@@ -903,7 +944,7 @@ int32_t sim_set_sync(uint32_t h, uint32_t mode) {
 int32_t sim_sync_in(uint32_t h) {
   DSim *s = get_sim(h);
   if (!s) return D3_BAD_HANDLE;
-  return sync_in_impl(s);
+  return sync_in_impl(s, true);
 }
 
 int32_t sim_sync_out(uint32_t h) {
@@ -914,17 +955,27 @@ int32_t sim_sync_out(uint32_t h) {
 
 int32_t sim_tick(uint32_t h, uint32_t ticks, double *alpha, double alpha_target, double alpha_decay,
                  double velocity_decay, const uint32_t *order, uint32_t n_order) {
-  DSim *s = get_sim(h);
+  DSim *s = get_sim_raw(h);
   if (!s) return D3_BAD_HANDLE;
-  if (!alpha || (n_order && !order)) return D3_BAD_ARGUMENT;
+  if (!alpha || (n_order && !order)) {
+    settle(s);
+    return D3_BAD_ARGUMENT;
+  }
   std::vector<DForce *> fs;
   for (uint32_t i = 0; i < n_order; ++i) {
     DForce *f = get_force(s, order[i]);
-    if (!f) return D3_BAD_HANDLE;
-    if (node_sized(f) && f->count < s->n) return D3_BAD_ARGUMENT;
+    if (!f || (node_sized(f) && f->count < s->n)) {
+      settle(s);
+      return f ? D3_BAD_ARGUMENT : D3_BAD_HANDLE;
+    }
     upload_force(s, f);
     fs.push_back(f);
   }
+  // An exact many-body force first reads only positions (and its strengths)
+  // until its traversal: the rest of the node state may still be uploading.
+  s->settle_after_accumulate = !fs.empty() && fs[0]->kind == D3_MANY_BODY && !s->host_random &&
+                               !fast_mode(s, fs[0]);
+  if (!s->settle_after_accumulate) settle(s);
   // The first center force's sums only read positions, which no force
   // before it changes: run them on the side stream from the tick's start.
   int hoist = -1;
@@ -955,13 +1006,20 @@ int32_t sim_tick(uint32_t h, uint32_t ticks, double *alpha, double alpha_target,
       cudaEventRecord(s->ev_sumdone, s->side);
     }
     for (size_t i = 0; i < fs.size(); ++i) {
+      if (i > 0 || k > 0) settle(s);
       int r = run_force(s, fs[i], a, (int)i == hoist && s->n);
-      if (r < 0) return r;
+      if (r < 0) {
+        settle(s);
+        s->settle_after_accumulate = false;
+        return r;
+      }
     }
+    settle(s);
     cudaEvent_t e = phase_begin(s);
     integrate(nodes_of(s), velocity_decay, s->stream);
     phase_end(s, PH_INTEGRATE, e);
   }
+  s->settle_after_accumulate = false;
   cudaEventRecord(s->ev1, s->stream);
   s->last_enqueue_ms =
       std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - host0).count();

@@ -61,6 +61,8 @@ class Context:
         self.live = False
         self._nodes = None  # the node table whose arrays are the mirrors
         self._views = ()
+        self._fixed = None  # the fixed-bits mirror and a scratch row (while n holds)
+        self._fixed_tmp = None
         self.precision = None  # None = exact; {"order", "opening"} = fast
         self.host_random = None  # callback for randomSource(); None = device LCG
         self._cb = None
@@ -71,6 +73,7 @@ class Context:
     def resize(self, n):
         if n != self.n:
             self.detach()  # the mirrors move
+            self._fixed = None
             C.check(self.core.sim_set_node_count(self.h, n))
             self.n = n
 
@@ -93,10 +96,14 @@ class Context:
 
     def _write_fixed(self, nodes, n):
         """src/core.js:130 straight into the pinned mirror."""
-        v = self.core.u8_view(self.core.sim_ptr(self.h, C.PTR_FIXED), n)
-        np.equal(nodes.fx, nodes.fx, out=v.view(np.bool_))
-        w = np.equal(nodes.fy, nodes.fy).view(np.uint8)
-        v |= w << 1
+        if self._fixed is None or len(self._fixed) != n:
+            self._fixed = self.core.u8_view(self.core.sim_ptr(self.h, C.PTR_FIXED), n)
+            self._fixed_tmp = np.empty(n, np.uint8)
+        v, w = self._fixed, self._fixed_tmp
+        np.equal(nodes.fx, nodes.fx, out=v.view(np.bool_))  # 1: fx set
+        np.equal(nodes.fy, nodes.fy, out=w.view(np.bool_))  # 1: fy set
+        np.add(w, w, out=w)
+        np.add(v, w, out=v)
 
     def copy_in(self, nodes):
         """src/core.js:121-131, then one host-to-device sync. The node table's
@@ -155,6 +162,7 @@ class Slot:
         self.ctx = None
         self.fh = 0
         self.m = 0
+        self._sent = {}  # scalar slot -> the value last set (as float.hex())
 
     def bind(self, ctx, n):
         if ctx is not self.ctx:
@@ -165,6 +173,7 @@ class Slot:
                 raise C.CoreError(C.OUT_OF_MEMORY)
             self.ctx = ctx
             self.m = 0
+            self._sent = {}
         ctx.resize(n)
 
     def count(self, m):
@@ -178,7 +187,14 @@ class Slot:
         return self.ctx.core.u32_view(self.ctx.core.force_ptr(self.ctx.h, self.fh, which), m)
 
     def scalar(self, which, v):
-        self.ctx.core.force_set_scalar(self.ctx.h, self.fh, which, float(v))
+        """force_set_scalar, skipped when the slot already holds this value
+        (scalars change only through this call; SEED is always sent)."""
+        v = float(v)
+        key = v.hex()
+        if which != C.SEED and self._sent.get(which) == key:
+            return
+        C.check(self.ctx.core.force_set_scalar(self.ctx.h, self.fh, which, v))
+        self._sent[which] = key
 
     def run(self, alpha, random=None):
         """src/core.js:213-231: PRECISION, fast-mode ORDER / OPENING and SEED."""

@@ -443,21 +443,40 @@ int link_plan_build(LinkPlan &plan, const uint32_t *src, const uint32_t *tgt, ui
   }
   std::vector<uint32_t> fill(start.begin(), start.end());
   for (uint32_t e = 0; e < m; ++e) order[fill[level[e]]++] = e;
+  // per link, how many earlier links touch its source and its target: it may
+  // run once that many links on each have finished
+  std::vector<uint32_t> seen(nmax, 0), need_e(2 * (size_t)m), need(2 * (size_t)(m > 0 ? m : 1));
+  for (uint32_t e = 0; e < m; ++e) {
+    need_e[2 * e] = seen[src[e]];
+    need_e[2 * e + 1] = seen[tgt[e]];
+    ++seen[src[e]];
+    ++seen[tgt[e]];
+  }
+  for (uint32_t p = 0; p < m; ++p) {
+    need[2 * p] = need_e[2 * order[p]];
+    need[2 * p + 1] = need_e[2 * order[p] + 1];
+  }
   link_plan_free(plan);
   D3_CUDA_OK(cudaMalloc(&plan.order, order.size() * 4));
   D3_CUDA_OK(cudaMalloc(&plan.level_start, start.size() * 4));
+  D3_CUDA_OK(cudaMalloc(&plan.need, need.size() * 4));
+  D3_CUDA_OK(cudaMalloc(&plan.done, (nmax > 0 ? nmax : 1) * 4ull));
   D3_CUDA_OK(cudaMemcpy(plan.order, order.data(), order.size() * 4, cudaMemcpyHostToDevice));
   D3_CUDA_OK(cudaMemcpy(plan.level_start, start.data(), start.size() * 4, cudaMemcpyHostToDevice));
+  D3_CUDA_OK(cudaMemcpy(plan.need, need.data(), need.size() * 4, cudaMemcpyHostToDevice));
   plan.h_level_start = new uint32_t[start.size()];
   for (size_t k = 0; k < start.size(); ++k) plan.h_level_start[k] = start[k];
   plan.m = m;
   plan.levels = levels;
+  plan.nodes = nmax;
   return 0;
 }
 
 void link_plan_free(LinkPlan &plan) {
   cudaFree(plan.order);
   cudaFree(plan.level_start);
+  cudaFree(plan.need);
+  cudaFree(plan.done);
   delete[] plan.h_level_start;
   plan = LinkPlan();
 }
@@ -574,41 +593,8 @@ __global__ void k_link_serial_host(double *xs, double *ys, double *vxs, double *
   rng->pos += used;
 }
 
-// link_one with the velocities read through L2 (other blocks of the same
-// cooperative launch wrote them before the last grid barrier).
-__device__ inline bool link_one_cg(const double *xs, const double *ys, double *vxs, double *vys,
-                                   const LinkArrays l, uint32_t e, double alpha) {
-  const uint32_t src = l.source[e], tgt = l.target[e];
-  const double vxt = __ldcg(&vxs[tgt]), vyt = __ldcg(&vys[tgt]);
-  const double vxsrc = __ldcg(&vxs[src]), vysrc = __ldcg(&vys[src]);
-  double x = xs[tgt] + vxt - xs[src] - vxsrc;
-  double y = ys[tgt] + vyt - ys[src] - vysrc;
-  if (x == 0 || x != x || y == 0 || y != y) return false;
-  double len = sqrt(x * x + y * y);
-  len = (len - l.distance[e]) / len * alpha * l.strength[e];
-  x *= len;
-  y *= len;
-  double b = l.bias[e];
-  vxs[tgt] = vxt - x * b;
-  vys[tgt] = vyt - y * b;
-  b = 1 - b;
-  vxs[src] = vxsrc + x * b;
-  vys[src] = vysrc + y * b;
-  return true;
-}
-
-struct LinkCoopArgs {
-  const double *xs, *ys;
-  double *vxs, *vys, *svx, *svy;
-  LinkArrays l;
-  const uint32_t *order, *level_start;
-  uint32_t levels, n;
-  double alpha, iterations;
-  uint32_t *flag;
-};
-
-// A thread's first link of a level, with everything about it that does not
-// change during the pass (e = NONE: no link).
+// A link with everything about it that does not change during the pass
+// (e = NONE: no link).
 struct LinkPre {
   uint32_t e, src, tgt;
   double dist, str, bias, xt, yt, xsrc, ysrc;
@@ -632,14 +618,56 @@ __device__ inline void link_positions(const double *xs, const double *ys, LinkPr
   p.ysrc = ys[p.src];
 }
 
-// The level-scheduled pass in one cooperative launch: the pass-start snapshot,
-// then per iteration and level its links (disjoint nodes) with a grid barrier
-// between levels, then the snapshot back if a link met a zero or NaN delta
-// (the serial kernel then runs the pass with its draws). Each thread's first
-// link of a level is pipelined: its id two levels ahead, its parameters one
-// level ahead and its endpoints' positions before the barrier, so a level
-// waits only for the velocities.
-__global__ void __launch_bounds__(256) k_link_coop(LinkCoopArgs a) {
+struct LinkFlowArgs {
+  const double *xs, *ys;
+  double *vxs, *vys, *svx, *svy;
+  LinkArrays l;
+  const uint32_t *order, *need;
+  uint32_t *done;
+  uint32_t n, nodes;
+  double alpha, iterations;
+  uint32_t *flag;
+};
+
+__device__ inline uint32_t ld_relaxed_u32(const uint32_t *p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ inline unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// A link's wait, bounded: until `ns` links on src and `nt` on tgt have
+// finished. False if it gave up (20 ms): the pass is then restored and run
+// serially.
+__device__ inline bool link_wait(const uint32_t *done, uint32_t src, uint32_t ns, uint32_t tgt,
+                                 uint32_t nt) {
+  if (ld_relaxed_u32(&done[src]) >= ns && ld_relaxed_u32(&done[tgt]) >= nt) {
+    __threadfence();
+    return true;
+  }
+  const unsigned long long t0 = globaltimer_ns();
+  for (uint32_t it = 0;; ++it) {
+    if (ld_relaxed_u32(&done[src]) >= ns && ld_relaxed_u32(&done[tgt]) >= nt) {
+      __threadfence();
+      return true;
+    }
+    if (it >= 8) __nanosleep(64);
+    if ((it & 15) == 15 && globaltimer_ns() - t0 > 20000000ull) return false;
+  }
+}
+
+// The pass as dataflow, in one cooperative launch: the pass-start snapshot,
+// then every link (threads take them in level order) once the links before
+// it on its two nodes have finished (per-node finished counts against the
+// plan's per-link counts; a link's parameters and endpoint positions are
+// loaded before its wait), then the snapshot back if a link met a zero or
+// NaN delta or a wait gave up (the serial kernel then runs the pass).
+__global__ void __launch_bounds__(256) k_link_flow(LinkFlowArgs a) {
   cg::grid_group g = cg::this_grid();
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
   if (tid == 0) *a.flag = 0;
@@ -647,56 +675,40 @@ __global__ void __launch_bounds__(256) k_link_coop(LinkCoopArgs a) {
     a.svx[i] = a.vxs[i];
     a.svy[i] = a.vys[i];
   }
-  const uint32_t L = a.levels;
-  auto first = [&](uint32_t lv) -> uint32_t {
-    if (lv > L) return NONE;
-    const uint32_t lo = a.level_start[lv], hi = a.level_start[lv + 1];
-    return lo + tid < hi ? a.order[lo + tid] : NONE;
-  };
+  const uint32_t m = a.l.m;
   bool bad = false;
   for (double k = 0; k < a.iterations; k += 1) {
-    LinkPre cur, nxt;
-    link_params(a.l, first(1), cur);
-    link_positions(a.xs, a.ys, cur);
-    uint32_t e_next = first(2);
-    for (uint32_t lv = 1; lv <= L; ++lv) {
-      double vxt = 0, vyt = 0, vxsrc = 0, vysrc = 0;
-      if (cur.e != NONE) {
-        vxt = __ldcg(&a.vxs[cur.tgt]);
-        vyt = __ldcg(&a.vys[cur.tgt]);
-        vxsrc = __ldcg(&a.vxs[cur.src]);
-        vysrc = __ldcg(&a.vys[cur.src]);
+    for (uint32_t i = tid; i < a.nodes; i += nth) a.done[i] = 0;
+    g.sync();  // the snapshot and the counts before any link runs
+    for (uint32_t p = tid; p < m; p += nth) {
+      LinkPre c;
+      link_params(a.l, a.order[p], c);
+      link_positions(a.xs, a.ys, c);
+      const uint32_t ns = a.need[2 * p], nt = a.need[2 * p + 1];
+      if (!link_wait(a.done, c.src, ns, c.tgt, nt)) bad = true;
+      const double vxt = __ldcg(&a.vxs[c.tgt]), vyt = __ldcg(&a.vys[c.tgt]);
+      const double vxsrc = __ldcg(&a.vxs[c.src]), vysrc = __ldcg(&a.vys[c.src]);
+      double x = c.xt + vxt - c.xsrc - vxsrc;
+      double y = c.yt + vyt - c.ysrc - vysrc;
+      if (x == 0 || x != x || y == 0 || y != y) {
+        bad = true;
+      } else {
+        double len = sqrt(x * x + y * y);
+        len = (len - c.dist) / len * a.alpha * c.str;
+        x *= len;
+        y *= len;
+        double b = c.bias;
+        a.vxs[c.tgt] = vxt - x * b;
+        a.vys[c.tgt] = vyt - y * b;
+        b = 1 - b;
+        a.vxs[c.src] = vxsrc + x * b;
+        a.vys[c.src] = vysrc + y * b;
+        __threadfence();
       }
-      link_params(a.l, e_next, nxt);
-      const uint32_t e_after = first(lv + 2);
-      if (cur.e != NONE) {
-        double x = cur.xt + vxt - cur.xsrc - vxsrc;
-        double y = cur.yt + vyt - cur.ysrc - vysrc;
-        if (x == 0 || x != x || y == 0 || y != y) {
-          bad = true;
-        } else {
-          double len = sqrt(x * x + y * y);
-          len = (len - cur.dist) / len * a.alpha * cur.str;
-          x *= len;
-          y *= len;
-          double b = cur.bias;
-          a.vxs[cur.tgt] = vxt - x * b;
-          a.vys[cur.tgt] = vyt - y * b;
-          b = 1 - b;
-          a.vxs[cur.src] = vxsrc + x * b;
-          a.vys[cur.src] = vysrc + y * b;
-        }
-      }
-      {  // a level with more links than threads: the rest, unpipelined
-        const uint32_t lo = a.level_start[lv], hi = a.level_start[lv + 1];
-        for (uint32_t e = lo + tid + nth; e < hi; e += nth)
-          if (!link_one_cg(a.xs, a.ys, a.vxs, a.vys, a.l, a.order[e], a.alpha)) bad = true;
-      }
-      link_positions(a.xs, a.ys, nxt);
-      g.sync();
-      cur = nxt;
-      e_next = e_after;
+      atomicAdd(&a.done[c.src], 1u);
+      atomicAdd(&a.done[c.tgt], 1u);
     }
+    g.sync();
   }
   if (bad) atomicOr(a.flag, 1u);
   g.sync();
@@ -718,19 +730,20 @@ void link_exact(const NodeArrays &a, const LinkArrays &l, const LinkPlan &plan, 
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_link_coop, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_link_flow, 256, 0);
     g_link_blocks = sms * (per >= 2 ? 2 : 1);
   }
   {
-    LinkCoopArgs c;
+    LinkFlowArgs c;
     c.xs = a.x; c.ys = a.y; c.vxs = a.vx; c.vys = a.vy; c.svx = a.snap_vx; c.svy = a.snap_vy;
-    c.l = l; c.order = plan.order; c.level_start = plan.level_start; c.levels = plan.levels;
-    c.n = n; c.alpha = alpha; c.iterations = iterations; c.flag = flag;
+    c.l = l; c.order = plan.order; c.need = plan.need; c.done = plan.done;
+    c.n = n; c.nodes = plan.nodes; c.alpha = alpha; c.iterations = iterations; c.flag = flag;
     void *params[] = {&c};
     ++g_launches;
-    if (cudaLaunchCooperativeKernel((const void *)k_link_coop, g_link_blocks, 256, params, 0, st) ==
+    if (cudaLaunchCooperativeKernel((const void *)k_link_flow, g_link_blocks, 256, params, 0, st) ==
         cudaSuccess)
       return;
+    cudaGetLastError();
   }
   // (without a cooperative launch: one launch per level)
   cudaMemsetAsync(flag, 0, sizeof(uint32_t), st);

@@ -57,10 +57,13 @@ void many_body_rerun(TreeDev &t, const NodeArrays &a, const double *strengths,
 // Link levels (computed on the host from source/target): links grouped by
 // level so that links sharing a node keep their order (link.zig:8-40).
 struct LinkPlan {
-  uint32_t m = 0, levels = 0;
+  uint32_t m = 0, levels = 0, nodes = 0;
   uint32_t *order = nullptr;        // device: link ids grouped by level
   uint32_t *level_start = nullptr;  // device: levels + 1 offsets
   uint32_t *h_level_start = nullptr;
+  uint32_t *need = nullptr;         // device: per position in order, the earlier links on
+                                    // its source, then on its target (2 per link)
+  uint32_t *done = nullptr;         // device: per node, links on it finished (this pass)
 };
 int link_plan_build(LinkPlan &plan, const uint32_t *src, const uint32_t *tgt, uint32_t m);
 void link_plan_free(LinkPlan &plan);

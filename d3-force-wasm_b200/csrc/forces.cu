@@ -37,7 +37,9 @@ int scratch_reserve(ForceScratch &s, uint32_t n) {
   D3_CUDA_OK(cudaMalloc(&s.csum_scan_part, scan_partial_words(csum_count_words(cap)) * 4));
   D3_CUDA_OK(cudaMalloc(&s.draws, (cap + 1) * 4ull));
   D3_CUDA_OK(cudaMalloc(&s.offsets, (cap + 1) * 4ull));
-  D3_CUDA_OK(cudaMalloc(&s.scan_part, scan_partial_words(cap + 1) * 4));
+  // also the grid partials of k_mb_draws (one word per block)
+  const size_t sp = scan_partial_words(cap + 1);
+  D3_CUDA_OK(cudaMalloc(&s.scan_part, (sp > 1024 ? sp : 1024) * 4));
   s.cap = cap;
   return 0;
 }
@@ -370,6 +372,35 @@ __global__ void __launch_bounds__(128) k_mb_rerun(const MRec *rec,
   mb_node<false>(rec, perm, info[1], xs, ys, vxs, vys, strengths, p, i, rng, offsets[i]);
 }
 
+// The jiggle draws of the flagged targets, after the record pass, in one
+// cooperative launch (device LCG): the exclusive scan of the draw counts over
+// node index (d3's draw order), the flagged targets again from their stream
+// positions, then the LCG advanced past all the draws. Nothing to do (the
+// usual case) is decided by every block alike from the flagged count.
+__global__ void __launch_bounds__(256) k_mb_draws(const MRec *rec, const uint32_t *perm,
+                                                  const uint32_t *info, const double *xs,
+                                                  const double *ys, double *vxs, double *vys,
+                                                  const double *strengths, ManyBodyParams p,
+                                                  uint32_t n, const uint32_t *draws,
+                                                  uint32_t *offsets, uint32_t *counters,
+                                                  uint32_t *bsum, Rng *rng) {
+  if (__ldcg(&counters[1]) == 0) return;
+  cg::grid_group g = cg::this_grid();
+  const uint32_t total = grid_excl_scan(g, draws, offsets, n, bsum);
+  g.sync();
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  const uint32_t len = info[1];
+  for (uint32_t i = tid; i < n; i += nth)
+    if (__ldcg(&draws[i]))
+      mb_node<false>(rec, perm, len, xs, ys, vxs, vys, strengths, p, i, rng, __ldcg(&offsets[i]));
+  g.sync();
+  if (tid == 0) {
+    counters[0] = total;
+    if (rng->mode == 0) rng->lcg = lcg_skip(rng->lcg, total);
+    else rng->pos += total;
+  }
+}
+
 __global__ void k_rng_advance(Rng *rng, const uint32_t *total) {
   uint32_t t = *total;
   if (t == 0) return;
@@ -399,8 +430,34 @@ void many_body_exact(TreeDev &t, const NodeArrays &a, const double *strengths,
   D3_LAUNCH(k_mb_traverse, blocks_for(n, 128), 128, 0, st)((const MRec *)t.rec, t.perm, t.info, a.x, a.y,
                                                     a.vx, a.vy, strengths, p, n, s.draws,
                                                     s.counters);
-  scan_u32(s.draws, s.offsets, n, s.scan_part, s.counters, st);
-  if (!host_draws) many_body_rerun(t, a, strengths, p, rng, s, st);
+  if (host_draws) {
+    scan_u32(s.draws, s.offsets, n, s.scan_part, s.counters, st);
+    return;
+  }
+  static int blocks = 0;
+  if (!blocks) {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_mb_draws, 256, 0);
+    blocks = sms * (per >= 2 ? 2 : (per > 0 ? per : 1));
+  }
+  const MRec *rec = (const MRec *)t.rec;
+  const uint32_t *perm = t.perm, *info = t.info;
+  const double *x = a.x, *y = a.y;
+  double *vx = a.vx, *vy = a.vy;
+  ManyBodyParams pp = p;
+  uint32_t nn = n;
+  const uint32_t *draws = s.draws;
+  uint32_t *offsets = s.offsets, *counters = s.counters, *bsum = s.scan_part;
+  void *params[] = {&rec, &perm, &info, &x, &y, &vx, &vy, &strengths, &pp, &nn, &draws, &offsets,
+                    &counters, &bsum, &rng};
+  ++g_launches;
+  if (cudaLaunchCooperativeKernel((const void *)k_mb_draws, blocks, 256, params, 0, st) != cudaSuccess) {
+    cudaGetLastError();
+    scan_u32(s.draws, s.offsets, n, s.scan_part, s.counters, st);
+    many_body_rerun(t, a, strengths, p, rng, s, st);
+  }
 }
 
 void many_body_rerun(TreeDev &t, const NodeArrays &a, const double *strengths,

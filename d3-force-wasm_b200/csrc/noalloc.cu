@@ -46,7 +46,7 @@ constexpr size_t NA_SIZES[] = {
     4 * na_hist_words,                            // hist
     4 * sizeof(double), 16 * sizeof(uint32_t),    // extent, info
     4ull * (NA_CAP + 1), 4ull * (NA_CAP + 1),     // draws, offsets
-    4 * na_scan_words(NA_CAP + 1),                // force scan
+    4 * (na_scan_words(NA_CAP + 1) > 1024 ? na_scan_words(NA_CAP + 1) : 1024),  // force scan
     16 * sizeof(uint32_t), 2 * sizeof(double),    // counters, center
     sizeof(Rng), 16 * sizeof(uint32_t),           // rng, status words
     16 * sizeof(unsigned long long),              // tree build phase stamps

@@ -570,70 +570,6 @@ __device__ inline void tb_stamp(const TreeBuildArgs &a, int k) {
   }
 }
 
-__device__ inline uint32_t block_sum(uint32_t v, uint32_t *sw) {
-  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  __syncthreads();
-  if (lane == 0) sw[warp] = v;
-  __syncthreads();
-  uint32_t t = 0;
-  for (unsigned w = 0; w < blockDim.x / 32; ++w) t += sw[w];
-  return t;
-}
-
-// Block-wide exclusive scan of one value per thread; the total to *tot.
-__device__ inline uint32_t block_excl(uint32_t v, uint32_t *sw, uint32_t &tot) {
-  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  uint32_t incl = v;
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= (unsigned)o) incl += y;
-  }
-  __syncthreads();
-  if (lane == 31) sw[warp] = incl;
-  __syncthreads();
-  uint32_t pre = 0;
-  tot = 0;
-  for (unsigned w = 0; w < nw; ++w) {
-    if (w < warp) pre += sw[w];
-    tot += sw[w];
-  }
-  return pre + incl - v;
-}
-
-// out[0..len) = exclusive scan of in[0..len) over the whole grid; returns the
-// total. One grid barrier inside; the caller syncs before reading out.
-__device__ uint32_t grid_excl_scan(cg::grid_group &g, const uint32_t *in, uint32_t *out,
-                                   uint32_t len, uint32_t *bsum) {
-  __shared__ uint32_t sw[32];
-  const uint32_t nb = gridDim.x, b = blockIdx.x, t = threadIdx.x;
-  const uint32_t seg = (len + nb - 1) / nb;
-  const uint32_t s0 = min(len, b * seg), s1 = min(len, s0 + seg);
-  uint32_t acc = 0;
-  for (uint32_t i = s0 + t; i < s1; i += blockDim.x) acc += ldc(&in[i]);
-  acc = block_sum(acc, sw);
-  if (t == 0) bsum[b] = acc;
-  g.sync();
-  uint32_t off = 0, tot = 0;
-  for (uint32_t k = t; k < nb; k += blockDim.x) {
-    const uint32_t x = ldc(&bsum[k]);
-    if (k < b) off += x;
-    tot += x;
-  }
-  off = block_sum(off, sw);
-  tot = block_sum(tot, sw);
-  uint32_t run = off;
-  for (uint32_t base = s0; base < s1; base += blockDim.x) {
-    const uint32_t i = base + t;
-    const uint32_t x = i < s1 ? ldc(&in[i]) : 0;
-    uint32_t tile;
-    const uint32_t ex = block_excl(x, sw, tile);
-    if (i < s1) out[i] = run + ex;
-    run += tile;
-  }
-  return tot;
-}
-
 template <bool PART>
 __device__ inline uint32_t tb_digit(uint64_t k, uint32_t v, int shift) {
   if (PART) return v >> 31;

@@ -426,9 +426,9 @@ int run_link(DSim *s, DForce *f, double alpha) {
   LinkArrays l{f->d_f[0], f->d_f[1], f->d_f[2], f->d_src, f->d_tgt, f->count};
   const double iterations = f->scalars[D3_ITERATIONS];
   cudaEvent_t e = phase_begin(s);
-  link_exact(a, l, f->plan, alpha, iterations, s->d_rng, link_flag(s), s->stream);
+  link_exact(a, l, f->plan, alpha, iterations, s->d_rng, link_flag(s), status_word(s),
+             !s->host_random, s->stream);
   if (!s->host_random) {
-    link_fallback_lcg(a, l, alpha, iterations, s->d_rng, link_flag(s), status_word(s), s->stream);
     phase_end(s, PH_LINK, e);
     return D3_OK;
   }
@@ -487,7 +487,9 @@ bool fast_mode(const DSim *s, const DForce *f) {
   return f->scalars[D3_PRECISION] == 1 && s->n >= FAST_MIN_N;
 }
 
-int run_force(DSim *s, DForce *f, double alpha, bool presummed = false) {
+// fuse_center: a center force's shift is left to the caller (which fuses it
+// into integrate).
+int run_force(DSim *s, DForce *f, double alpha, bool presummed = false, bool fuse_center = false) {
   NodeArrays a = nodes_of(s);
   // The facade's per-run SEED draw in fast mode (src/core.js:218-222), from
   // the device LCG when it is the random source.
@@ -503,8 +505,9 @@ int run_force(DSim *s, DForce *f, double alpha, bool presummed = false) {
       cudaEvent_t e = phase_begin(s);
       if (presummed) cudaStreamWaitEvent(s->stream, s->ev_sumdone, 0);
       else center_sum(a, s->scratch, status_word(s), s->stream);
-      center_apply(a, f->scalars[D3_CX], f->scalars[D3_CY], f->scalars[D3_STRENGTH], s->scratch,
-                   s->stream);
+      if (!fuse_center)
+        center_apply(a, f->scalars[D3_CX], f->scalars[D3_CY], f->scalars[D3_STRENGTH], s->scratch,
+                     s->stream);
       phase_end(s, PH_CENTER, e);
       return D3_OK;
     }
@@ -1005,9 +1008,11 @@ int32_t sim_tick(uint32_t h, uint32_t ticks, double *alpha, double alpha_target,
       }
       cudaEventRecord(s->ev_sumdone, s->side);
     }
+    // a center force that comes last has its shift fused into integrate
+    const bool fuse = !fs.empty() && fs.back()->kind == D3_CENTER;
     for (size_t i = 0; i < fs.size(); ++i) {
       if (i > 0 || k > 0) settle(s);
-      int r = run_force(s, fs[i], a, (int)i == hoist && s->n);
+      int r = run_force(s, fs[i], a, (int)i == hoist && s->n, fuse && i + 1 == fs.size());
       if (r < 0) {
         settle(s);
         s->settle_after_accumulate = false;
@@ -1016,7 +1021,13 @@ int32_t sim_tick(uint32_t h, uint32_t ticks, double *alpha, double alpha_target,
     }
     settle(s);
     cudaEvent_t e = phase_begin(s);
-    integrate(nodes_of(s), velocity_decay, s->stream);
+    if (fuse) {
+      const DForce *c = fs.back();
+      center_apply_integrate(nodes_of(s), c->scalars[D3_CX], c->scalars[D3_CY],
+                             c->scalars[D3_STRENGTH], s->scratch, velocity_decay, s->stream);
+    } else {
+      integrate(nodes_of(s), velocity_decay, s->stream);
+    }
     phase_end(s, PH_INTEGRATE, e);
   }
   s->settle_after_accumulate = false;

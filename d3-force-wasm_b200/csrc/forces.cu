@@ -584,10 +584,9 @@ __global__ void k_save_v(double *svx, double *svy, const double *vx, const doubl
 }
 
 // link.zig:8-40 on one thread, drawing from the device LCG.
-__global__ void k_link_serial(double *xs, double *ys, double *vxs, double *vys, LinkArrays l,
-                              double alpha, double iterations, Rng *rng, const uint32_t *flag,
-                              uint32_t *status) {
-  if (*flag == 0) return;
+__device__ void link_serial_lcg(const double *xs, const double *ys, double *vxs, double *vys,
+                                const LinkArrays &l, double alpha, double iterations, Rng *rng,
+                                uint32_t *status) {
   atomicOr(status, ST_LINK_JIGGLE);
   uint32_t s = rng->lcg;
   for (double k = 0; k < iterations; k += 1) {
@@ -610,6 +609,13 @@ __global__ void k_link_serial(double *xs, double *ys, double *vxs, double *vys, 
     }
   }
   rng->lcg = s;
+}
+
+__global__ void k_link_serial(double *xs, double *ys, double *vxs, double *vys, LinkArrays l,
+                              double alpha, double iterations, Rng *rng, const uint32_t *flag,
+                              uint32_t *status) {
+  if (*flag == 0) return;
+  link_serial_lcg(xs, ys, vxs, vys, l, alpha, iterations, rng, status);
 }
 
 // The same with draws pulled by the host: resumes at (resume[0], resume[1]),
@@ -684,6 +690,9 @@ struct LinkFlowArgs {
   uint32_t n, nodes;
   double alpha, iterations;
   uint32_t *flag;
+  Rng *rng;           // with serial_lcg: the serial pass's draws
+  uint32_t *status;
+  int serial_lcg;     // a met jiggle is resolved in the launch (device LCG)
 };
 
 __device__ inline uint32_t ld_relaxed_u32(const uint32_t *p) {
@@ -774,13 +783,18 @@ __global__ void __launch_bounds__(256) k_link_flow(LinkFlowArgs a) {
       a.vxs[i] = __ldcg(&a.svx[i]);
       a.vys[i] = __ldcg(&a.svy[i]);
     }
+    if (a.serial_lcg) {
+      g.sync();
+      if (tid == 0) link_serial_lcg(a.xs, a.ys, a.vxs, a.vys, a.l, a.alpha, a.iterations, a.rng, a.status);
+    }
   }
 }
 
 static int g_link_blocks = 0;
 
 void link_exact(const NodeArrays &a, const LinkArrays &l, const LinkPlan &plan, double alpha,
-                double iterations, Rng *rng, uint32_t *flag, cudaStream_t st) {
+                double iterations, Rng *rng, uint32_t *flag, uint32_t *status, bool serial_lcg,
+                cudaStream_t st) {
   if (l.m == 0) return;
   const uint32_t n = a.n;
   if (!g_link_blocks) {
@@ -795,6 +809,7 @@ void link_exact(const NodeArrays &a, const LinkArrays &l, const LinkPlan &plan, 
     c.xs = a.x; c.ys = a.y; c.vxs = a.vx; c.vys = a.vy; c.svx = a.snap_vx; c.svy = a.snap_vy;
     c.l = l; c.order = plan.order; c.need = plan.need; c.done = plan.done;
     c.n = n; c.nodes = plan.nodes; c.alpha = alpha; c.iterations = iterations; c.flag = flag;
+    c.rng = rng; c.status = status; c.serial_lcg = serial_lcg;
     void *params[] = {&c};
     ++g_launches;
     if (cudaLaunchCooperativeKernel((const void *)k_link_flow, g_link_blocks, 256, params, 0, st) ==
@@ -814,6 +829,7 @@ void link_exact(const NodeArrays &a, const LinkArrays &l, const LinkPlan &plan, 
     }
   }
   D3_LAUNCH(k_restore_v, blocks_for(n, 256), 256, 0, st)(a.vx, a.vy, a.snap_vx, a.snap_vy, n, flag);
+  if (serial_lcg) link_fallback_lcg(a, l, alpha, iterations, rng, flag, status, st);
 }
 
 void link_serial_host(const NodeArrays &a, const LinkArrays &l, double alpha, double iterations,
@@ -938,8 +954,7 @@ void shift_positions(const NodeArrays &a, cudaStream_t st) {
 void collide_setup(TreeDev &t, const NodeArrays &a, const double *radii, uint32_t *status,
                    cudaStream_t st) {
   const uint32_t n = a.n;
-  D3_LAUNCH(k_shift, blocks_for(n, 256), 256, 0, st)(a.x, a.y, a.vx, a.vy, a.px, a.py, n);
-  tree_build(t, a.px, a.py, n, status, st);
+  tree_build_shifted(t, a.x, a.y, a.vx, a.vy, a.px, a.py, n, status, st);
   if (n == 0) return;
   unsigned cb, ct;
   climb_grid(cb, ct, t.cells_cap);
@@ -1416,6 +1431,44 @@ __global__ void k_integrate(double *x, double *y, double *vx, double *vy, const 
     y[i] = fy[i];
     vy[i] = 0;
   }
+}
+
+// k_center_apply then k_integrate, per node in one pass (both are per node).
+__global__ void k_center_integrate(double *x, double *y, double *vx, double *vy, const double *fx,
+                                   const double *fy, const uint8_t *fixed, const double *sums,
+                                   double cx, double cy, double strength, double decay,
+                                   uint32_t n) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double nf = (double)n;
+  const double sx = (sums[0] / nf - cx) * strength;
+  const double sy = (sums[1] / nf - cy) * strength;
+  const double x0 = x[i] - sx, y0 = y[i] - sy;
+  const uint8_t f = fixed[i];
+  if ((f & 1) == 0) {
+    double v = vx[i] * decay;
+    vx[i] = v;
+    x[i] = x0 + v;
+  } else {
+    x[i] = fx[i];
+    vx[i] = 0;
+  }
+  if ((f & 2) == 0) {
+    double v = vy[i] * decay;
+    vy[i] = v;
+    y[i] = y0 + v;
+  } else {
+    y[i] = fy[i];
+    vy[i] = 0;
+  }
+}
+
+void center_apply_integrate(const NodeArrays &a, double cx, double cy, double strength,
+                            ForceScratch &s, double decay, cudaStream_t st) {
+  if (a.n == 0) return;
+  D3_LAUNCH(k_center_integrate, blocks_for(a.n, 256), 256, 0, st)(a.x, a.y, a.vx, a.vy, a.fx, a.fy,
+                                                           a.fixed, s.center, cx, cy, strength,
+                                                           decay, a.n);
 }
 
 void integrate(const NodeArrays &a, double decay, cudaStream_t st) {

@@ -74,11 +74,13 @@ struct LinkArrays {
   uint32_t m;
 };
 
-// Exact link: level-scheduled Gauss-Seidel. A link that meets a zero / NaN
-// delta (where d3 draws from `random`) sets *flag and the pass is undone
-// (velocities restored from the snapshot); the caller then runs a serial pass.
+// Exact link: Gauss-Seidel in dependency order. A link that meets a zero /
+// NaN delta (where d3 draws from `random`) sets *flag and the pass is undone
+// (velocities restored from the snapshot); with serial_lcg the serial pass on
+// the device LCG then runs in the same launch, otherwise the caller runs it.
 void link_exact(const NodeArrays &a, const LinkArrays &l, const LinkPlan &plan, double alpha,
-                double iterations, Rng *rng, uint32_t *flag, cudaStream_t st);
+                double iterations, Rng *rng, uint32_t *flag, uint32_t *status, bool serial_lcg,
+                cudaStream_t st);
 // The serial pass on the device LCG, only when *flag is set.
 void link_fallback_lcg(const NodeArrays &a, const LinkArrays &l, double alpha, double iterations,
                        Rng *rng, const uint32_t *flag, uint32_t *status, cudaStream_t st);
@@ -141,5 +143,8 @@ void axis_force(const NodeArrays &a, const double *strength, const double *targe
 void radial_force(const NodeArrays &a, const double *strength, const double *radius, double cx,
                   double cy, double alpha, cudaStream_t st);
 void integrate(const NodeArrays &a, double decay, cudaStream_t st);
+// center_apply followed by integrate, in one launch.
+void center_apply_integrate(const NodeArrays &a, double cx, double cy, double strength,
+                            ForceScratch &s, double decay, cudaStream_t st);
 
 }  // namespace d3

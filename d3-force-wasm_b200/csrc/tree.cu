@@ -544,6 +544,8 @@ constexpr unsigned TB_TILE = 256;  // keys per sort tile (one per thread)
 
 struct TreeBuildArgs {
   const double *xs, *ys;
+  const double *vxs, *vys;  // if set, the points are (xs + vxs, ys + vys), written to pxs, pys
+  double *pxs, *pys;
   uint32_t n, tiles, cells_cap;
   uint64_t *keys, *keys_tmp;
   uint32_t *sv, *sv_tmp, *perm, *perm_tmp;
@@ -688,7 +690,13 @@ __global__ void __launch_bounds__(TB_THREADS) k_tree_build(TreeBuildArgs a) {
     uint32_t ix[4] = {NONE, NONE, NONE, NONE};
     uint32_t m = 0;
     for (uint32_t i = tid; i < n; i += nth) {
-      const double x = a.xs[i], y = a.ys[i];
+      double x = a.xs[i], y = a.ys[i];
+      if (a.vxs) {
+        x += a.vxs[i];
+        y += a.vys[i];
+        a.pxs[i] = x;
+        a.pys[i] = y;
+      }
       if (x != x || y != y) continue;
       double pv[4] = {x, y, x, y};
       uint32_t pi[4] = {i, i, i, i};
@@ -743,10 +751,12 @@ __global__ void __launch_bounds__(TB_THREADS) k_tree_build(TreeBuildArgs a) {
   }
   const uint32_t m = sm_m;
   if (n == 0) return;
+  // the points: as given, or shifted by the velocities in the box phase
+  const double *X = a.vxs ? a.pxs : a.xs, *Y = a.vxs ? a.pys : a.ys;
   // 2. keys, and the first sort pass's digit counts (cleared above)
   tb_stamp(a, 1);
   for (uint32_t i = tid; i < n; i += nth) {
-    keys_at(i, a.xs, a.ys, se, a.keys, a.sv);
+    keys_at(i, X, Y, se, a.keys, a.sv);
     atomicAdd(&a.hist[(size_t)(i / TB_TILE) * 256 + (uint32_t)((a.keys[i] >> 40) & 255u)], 1u);
   }
   g.sync();
@@ -799,11 +809,11 @@ __global__ void __launch_bounds__(TB_THREADS) k_tree_build(TreeBuildArgs a) {
   tb_stamp(a, 3);
   // 4. perm and the shared levels; 5. cells per start
   for (uint32_t k = tid; k < n; k += nth)
-    runs_at(k, m, a.xs, a.ys, fk, fv, a.perm, a.lcpx, a.leaf_of);
+    runs_at(k, m, X, Y, fk, fv, a.perm, a.lcpx, a.leaf_of);
   g.sync();
   tb_stamp(a, 4);
   for (uint32_t k = tid; k < n; k += nth)
-    count_at(k, m, a.xs, a.ys, fk, a.lcpx, se, a.perm, a.perm_tmp, a.frames, a.cnt, a.run_end,
+    count_at(k, m, X, Y, fk, a.lcpx, se, a.perm, a.perm_tmp, a.frames, a.cnt, a.run_end,
              a.leafd);
   g.sync();
   tb_stamp(a, 5);
@@ -826,13 +836,13 @@ __global__ void __launch_bounds__(TB_THREADS) k_tree_build(TreeBuildArgs a) {
   g.sync();
   tb_stamp(a, 7);
   for (uint32_t c = tid; c < total; c += nth)
-    emit_cell<false>(c, m, total, a.xs, a.ys, fk, a.lcpx, se, a.perm, a.perm_tmp, a.frames, a.base,
+    emit_cell<false>(c, m, total, X, Y, fk, a.lcpx, se, a.perm, a.perm_tmp, a.frames, a.base,
                      a.run_end, a.leafd, a.cells, a.skip, a.parent, a.pnch, a.counter, a.info,
                      a.leaf_of);
   {
     const uint32_t ntop = ldc(&a.info[8]), gw = tid >> 5, nw = nth >> 5;
     for (uint32_t k = gw; k < ntop; k += nw)
-      emit_cell<true>(ldc(&top[k]), m, total, a.xs, a.ys, fk, a.lcpx, se, a.perm, a.perm_tmp,
+      emit_cell<true>(ldc(&top[k]), m, total, X, Y, fk, a.lcpx, se, a.perm, a.perm_tmp,
                       a.frames, a.base, a.run_end, a.leafd, a.cells, a.skip, a.parent, a.pnch,
                       a.counter, a.info, a.leaf_of);
   }
@@ -906,6 +916,12 @@ static int g_tree_blocks = 0;
 
 void tree_build(TreeDev &t, const double *xs, const double *ys, uint32_t n, uint32_t *status,
                 cudaStream_t st) {
+  tree_build_shifted(t, xs, ys, nullptr, nullptr, nullptr, nullptr, n, status, st);
+}
+
+void tree_build_shifted(TreeDev &t, const double *xs, const double *ys, const double *vxs,
+                        const double *vys, double *pxs, double *pys, uint32_t n, uint32_t *status,
+                        cudaStream_t st) {
   if (!g_tree_blocks) {
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
@@ -917,6 +933,7 @@ void tree_build(TreeDev &t, const double *xs, const double *ys, uint32_t n, uint
   }
   TreeBuildArgs a;
   a.xs = xs; a.ys = ys; a.n = n;
+  a.vxs = vxs; a.vys = vys; a.pxs = pxs; a.pys = pys;
   a.tiles = (n + TB_TILE - 1) / TB_TILE;
   a.cells_cap = t.cells_cap;
   a.keys = t.keys; a.keys_tmp = t.keys_tmp; a.sv = t.sv; a.sv_tmp = t.sv_tmp;

@@ -60,6 +60,11 @@ void tree_free(TreeDev &t);
 // (info[] on the device). No host synchronisation.
 void tree_build(TreeDev &t, const double *xs, const double *ys, uint32_t n, uint32_t *status,
                 cudaStream_t st);
+// The same over the points (xs + vxs, ys + vys), which it also writes to
+// (pxs, pys).
+void tree_build_shifted(TreeDev &t, const double *xs, const double *ys, const double *vxs,
+                        const double *vys, double *pxs, double *pys, uint32_t n, uint32_t *status,
+                        cudaStream_t st);
 
 // Fast mode's square extent (tree.zig:287-309): t.extent, t.info[0] = points
 // without a NaN coordinate, and square[0..2] = box x0, y0, side.

@@ -18,10 +18,12 @@
 //     active node accesses its guessed heads (writes those in W, reads the
 //     rest) and itself (a write). Per accessed node, the accessors' list is
 //     sorted by node: a write waits for every access since the previous
-//     write, a read for the previous write. Each turn holds the count of the
-//     accesses it waits for; a finished turn decrements the counts of the
-//     accesses that waited on it, and a turn whose count reaches zero goes to
-//     a queue that idle warps claim slot by slot. A running node evaluates its
+//     write, a read for the previous write; each access records the range of
+//     the list it waits on. Waits only point to lower node indices, so warps
+//     claim the active nodes in index order: a warp loads everything about
+//     its node that cannot change (heads, their positions, the record, the
+//     ids of the turns it waits on), waits until those turns are done, then
+//     reads the velocities and runs the turn. A running node evaluates its
 //     examined heads in parallel (from E if nothing moved it, else by
 //     replaying its recorded cells with the exact pruning test), adds its own
 //     pushes in visit order, and writes only if everything it examined or
@@ -59,11 +61,9 @@ constexpr unsigned FULL = 0xffffffffu;
 enum : uint32_t {
   C_ACTIVE = 0, C_FAIL = 2, C_JIGGLE, C_OVERFLOW, C_ROUNDS, C_ATTEMPTS, C_SERIAL,
   C_FAIL_READ, C_FAIL_WRITE, C_FAIL_MOVED, C_FAST_TURNS, C_SLOW_TURNS, C_TIMEOUT,
-  C_ALLOC = 16, C_BIGFILL, C_BIGLINK, C_VWORK, C_DONE = 32, C_QHEAD = 64, C_QTAIL = 96,
-  C_COUNTERS = 128
+  C_ALLOC = 16, C_BIGFILL, C_BIGLINK, C_VWORK, C_DONE = 32, C_CLAIM = 64, C_COUNTERS = 128
 };
-// Queue slots one cache line apart (idle warps poll them).
-constexpr uint32_t QSTRIDE = 32;
+constexpr uint32_t PR_SLOTS = SPEC_CAP + 1;  // a node's entries: its heads, then itself
 
 // A cell as the collide traversals read it, in one 64-byte load: its box and
 // radius, and for an internal cell its skip link, for a leaf its head (the
@@ -107,11 +107,11 @@ struct SpecArgs {
   uint32_t *rlen, *roff; // n: each node's access list: length, offset
   uint64_t *ent;         // access entries: node << 32 | index in R << 1 | write
   uint64_t *ents;        // ... each list sorted by node
-  uint64_t *succ;        // n * SPEC_CAP: per guessed head, the entries waiting on the
-                         // access: first sorted entry << 32 | count
-  uint32_t *pred;        // n: accesses a turn still waits for
+  uint64_t *pr;          // n * PR_SLOTS: per entry, the sorted entries its access waits
+                         // on: first << 32 | count
   uint32_t *lev;         // n: the turn's depth in the dependency order
-  uint32_t *queue;       // n: turns in the order they became ready
+  uint32_t *aflag, *apos, *sact;  // n each: active flags, their scan, the active in index order
+  uint32_t *scan_part;   // grid partials of that scan (a word per block)
   uint32_t *bigfill, *biglink, *vwork;  // n each: the items warps share out (see below)
   double *push;          // push magnitude received per node (this pass)
   double *push_prev;     // ... in the previous pass (margin heuristic)
@@ -655,9 +655,8 @@ __device__ void warp_fill(const SpecArgs &a, uint32_t base, uint32_t n_active) {
     for (int h = 0; h < 4; ++h)
       if ((uint32_t)h < nf)
         a.ent[off[h] + old[h] - 1] = ((uint64_t)i << 32) | (h << 1) | ((wm >> h) & 1);
-    a.pred[i] = 0;
     a.lev[i] = 0;
-    a.queue[(size_t)k * QSTRIDE] = NONE;
+    a.sact[rd(&a.apos[i])] = i;
   }
 }
 
@@ -670,11 +669,21 @@ __device__ void warp_fill_big(const SpecArgs &a, uint32_t i) {
   for (uint32_t h = lane; h < nr; h += 32) put_entry(a, rd(&rl[h]), i, h, (wm >> h) & 1);
 }
 
-// One list of L > 1 entries at `off`, by the warp: sorted by node (the rank of
-// each entry among distinct nodes), then each entry's successors (a write:
-// the reads up to the next write, or else the next write; a read: the next
-// write) and its count of predecessors (a write: the reads since the previous
-// write, or else the previous write; a read: the previous write).
+// The range an entry at sorted position p (w: a write) waits on, given the
+// last write before it (pw < 0: none) and that write's node: a write waits
+// for the accesses since that write (all before it if none), a read for that
+// write. A single turn to wait on is stored as its node (WAIT_NODE), else
+// as first sorted entry << 32 | count.
+constexpr uint64_t WAIT_NODE = 0x80000000ull;
+__device__ inline uint64_t wait_range(uint32_t off, uint32_t p, int32_t pw, uint32_t pw_node,
+                                      bool w) {
+  if (pw < 0) return w ? ((uint64_t)off << 32) | p : 0;
+  if (!w || p == (uint32_t)pw + 1) return ((uint64_t)pw_node << 32) | WAIT_NODE | 1u;
+  return ((uint64_t)(off + pw) << 32) | (p - (uint32_t)pw);
+}
+
+// One list of L > 4 entries at `off`, by the warp: sorted by node (the rank of
+// each entry among distinct nodes), then each entry's wait range.
 __device__ void warp_link_list(const SpecArgs &a, uint32_t off, uint32_t L) {
   const unsigned lane = threadIdx.x & 31;
   const uint64_t *src = a.ent + off;
@@ -692,42 +701,27 @@ __device__ void warp_link_list(const SpecArgs &a, uint32_t off, uint32_t L) {
     if (p < L) dst[rank] = e;
   }
   __syncwarp();
-  uint32_t next_w = L;  // the first write at or after the chunk's end
-  for (int32_t c0 = (int32_t)((L - 1) & ~31u); c0 >= 0; c0 -= 32) {
-    const uint32_t p = (uint32_t)c0 + lane;
-    const uint64_t e = p < L ? rd(&dst[p]) : 0;
-    const bool w = p < L && (e & 1);
-    const unsigned wb = __ballot_sync(FULL, w);
-    const unsigned above = lane == 31 ? 0u : wb & (~0u << (lane + 1));
-    const uint32_t nw = above ? (uint32_t)c0 + __ffs(above) - 1 : next_w;
-    if (p < L) {
-      const uint32_t h = (uint32_t)(e >> 1) & 127;
-      if (h < SELF_ENTRY) {  // a node's own entry is its list's last: nothing waits on it
-        uint64_t sc = 0;
-        if (w && nw > p + 1) sc = ((uint64_t)(off + p + 1) << 32) | (nw - p - 1);
-        else if (nw < L) sc = ((uint64_t)(off + nw) << 32) | 1u;
-        a.succ[(e >> 32) * SPEC_CAP + h] = sc;
-      }
-    }
-    if (wb) next_w = (uint32_t)c0 + __ffs(wb) - 1;
-  }
-  int32_t prev_w = -1;  // the last write before the chunk
+  int32_t prev_w = -1;  // the last write before the chunk, and its node
+  uint32_t prev_node = NONE;
   for (uint32_t c0 = 0; c0 < L; c0 += 32) {
     const uint32_t p = c0 + lane;
     const uint64_t e = p < L ? rd(&dst[p]) : 0;
     const bool w = p < L && (e & 1);
     const unsigned wb = __ballot_sync(FULL, w);
     const unsigned below = wb & ((1u << lane) - 1);
-    const int32_t pw = below ? (int32_t)(c0 + 31 - __clz(below)) : prev_w;
+    const int src = below ? 31 - __clz(below) : 0;
+    const uint32_t node_below = __shfl_sync(FULL, (uint32_t)(e >> 32), src);
+    const int32_t pw = below ? (int32_t)(c0 + src) : prev_w;
+    const uint32_t pw_node = below ? node_below : prev_node;
     if (p < L) {
-      uint32_t c = pw >= 0 ? 1 : 0;
-      if (w) {
-        const uint32_t reads = pw >= 0 ? p - (uint32_t)pw - 1 : p;
-        if (reads) c = reads;
-      }
-      if (c) atomicAdd(&a.pred[e >> 32], c);
+      const uint32_t h = (uint32_t)(e >> 1) & 127;
+      a.pr[(e >> 32) * PR_SLOTS + h] = wait_range(off, p, pw, pw_node, w);
     }
-    if (wb) prev_w = (int32_t)(c0 + 31 - __clz(wb));
+    if (wb) {  // (wb is the same in every lane)
+      const int last = 31 - __clz(wb);
+      prev_w = (int32_t)(c0 + last);
+      prev_node = __shfl_sync(FULL, (uint32_t)(e >> 32), last);
+    }
   }
 }
 
@@ -757,77 +751,52 @@ __device__ void warp_link(const SpecArgs &a, uint32_t base) {
     cs(e[1], e[3]);
     cs(e[1], e[2]);
     int32_t pw = -1;
+    uint32_t pw_node = NONE;
 #pragma unroll
     for (uint32_t t = 0; t < 4; ++t) {
       if (t >= L) break;
       a.ents[off + t] = e[t];
       const bool w = e[t] & 1;
-      uint32_t c = pw >= 0 ? 1 : 0;
-      if (w) {
-        const uint32_t reads = pw >= 0 ? t - (uint32_t)pw - 1 : t;
-        if (reads) c = reads;
-        pw = (int32_t)t;
-      }
-      if (c) atomicAdd(&a.pred[e[t] >> 32], c);
-    }
-    uint32_t nw = L;
-#pragma unroll
-    for (int t = 3; t >= 0; --t) {
-      if ((uint32_t)t >= L) continue;
-      const bool w = e[t] & 1;
       const uint32_t h = (uint32_t)(e[t] >> 1) & 127;
-      if (h < SELF_ENTRY) {
-        uint64_t sc = 0;
-        if (w && nw > (uint32_t)t + 1) sc = ((uint64_t)(off + t + 1) << 32) | (nw - t - 1);
-        else if (nw < L) sc = ((uint64_t)(off + nw) << 32) | 1u;
-        a.succ[(e[t] >> 32) * SPEC_CAP + h] = sc;
-      }
-      if (w) nw = (uint32_t)t;
-    }
-  }
-}
-
-__device__ inline void push_ready(const SpecArgs &a, uint32_t i) {
-  const uint32_t q = atomicAdd(&a.counters[C_QTAIL], 1u);
-  if (q < a.n) atomicExch(&a.queue[(size_t)q * QSTRIDE], i);
-  else atomicAdd(&a.counters[C_TIMEOUT], 1u);  // queued twice: cannot happen; fail safe
-}
-
-// One count of turn s is done: true for the last one (s is then ready).
-__device__ inline bool release(const SpecArgs &a, uint32_t s) {
-  if (atomicSub(&a.pred[s], 1u) == 1u) {
-    __threadfence();
-    return true;
-  }
-  return false;
-}
-
-// Lane 0: the turn in queue slot `slot`, once one is there; NONE once all
-// n_active turns are done (the rest ran as continuations), or after
-// SPEC_WAIT_NS without any turn finishing.
-__device__ uint32_t wait_slot(const SpecArgs &a, uint32_t slot, uint32_t n_active) {
-  unsigned long long t0 = 0;
-  uint32_t seen = 0;
-  for (uint32_t it = 0;; ++it) {
-    const uint32_t v = ld_relaxed(&a.queue[(size_t)slot * QSTRIDE]);
-    if (v != NONE) {
-      __threadfence();
-      return v;
-    }
-    if ((it & 7) == 0) {
-      const uint32_t d = ld_relaxed(&a.counters[C_DONE]);
-      if (d >= n_active) return NONE;
-      const unsigned long long t = now_ns();
-      if (it == 0 || d != seen) {
-        seen = d;
-        t0 = t;
-      } else if (t - t0 > SPEC_WAIT_NS) {
-        atomicAdd(&a.counters[C_TIMEOUT], 1u);
-        return NONE;
+      a.pr[(e[t] >> 32) * PR_SLOTS + h] = wait_range(off, t, pw, pw_node, w);
+      if (w) {
+        pw = (int32_t)t;
+        pw_node = (uint32_t)(e[t] >> 32);
       }
     }
-    if (it >= 16) __nanosleep(64);
   }
+}
+
+__device__ inline uint8_t ld_relaxed_u8(const uint8_t *p) {
+  uint16_t v;
+  asm volatile("ld.relaxed.gpu.global.u8 %0, [%1];" : "=h"(v) : "l"(p) : "memory");
+  return (uint8_t)v;
+}
+
+// A lane's wait on the turns of one wait range (see wait_range; `first`: the
+// first turn's node, already known): until none is pending any more. dmax gets their largest depth. Gives up (false) after
+// SPEC_WAIT_NS in which no turn anywhere finished.
+__device__ bool wait_on(const SpecArgs &a, uint64_t r, uint32_t first, uint32_t &dmax,
+                        unsigned long long &t0, uint32_t &seen) {
+  const uint32_t c = (uint32_t)r & 0x7fffffffu;
+  for (uint32_t t = 0; t < c; ++t) {
+    const uint32_t x = t ? (uint32_t)(rd(&a.ents[(r >> 32) + t]) >> 32) : first;
+    for (uint32_t it = 0; ld_relaxed_u8(&a.state[x]) == 1; ++it) {
+      if (it >= 4) __nanosleep(64);
+      if ((it & 15) == 15) {
+        const uint32_t d = ld_relaxed(&a.counters[C_DONE]);
+        const unsigned long long now = now_ns();
+        if (!t0 || d != seen) {
+          t0 = now;
+          seen = d;
+        } else if (now - t0 > SPEC_WAIT_NS) {
+          return false;
+        }
+      }
+    }
+    dmax = max(dmax, ld_relaxed(&a.lev[x]));
+  }
+  return true;
 }
 
 // Per-warp tallies of the turns, added to the counters once per attempt.
@@ -835,71 +804,96 @@ struct TurnTally {
   uint32_t fast = 0, slow = 0, depth = 0;
 };
 
-// Node i's turn, by one warp, once every access it waits for is done: its
-// data and guessed heads (lane k holds heads k and k + 32) with their
-// successor ranges, then the heads' positions and velocities, the turn, and
-// the release of the turns waiting on it (also after a failed turn: the
-// attempt then fails as a whole, but every turn still runs). Returns one turn
-// it made ready, for the warp to run next (the others are queued), or NONE.
-__device__ uint32_t warp_run(const SpecArgs &a, uint32_t i, bool stamp, TurnTally &tally,
-                             double *cx, double *cy) {
+// Node i's turn, by one warp: everything about it that cannot change (its
+// guessed heads, lane k holding heads k and k + 32, with their positions and
+// radii; its record; its masks and pass-start velocity; the first turn each
+// of its accesses waits on) is loaded first; then the warp waits until every
+// turn its accesses wait on is done; then it reads the velocities and runs
+// the turn, and marks the node done (also after a failed turn: the attempt
+// then fails as a whole, but every turn still runs).
+__device__ void warp_pull(const SpecArgs &a, uint32_t i, bool stamp, TurnTally &tally, double *cx,
+                          double *cy) {
   const unsigned lane = threadIdx.x & 31;
   const uint32_t *rl = a.rlist + (size_t)i * SPEC_CAP;
-  const uint64_t *sc = a.succ + (size_t)i * SPEC_CAP;
-  // round trip 1 (rows are read whole; entries past rcount are ignored)
+  const uint64_t *prr = a.pr + (size_t)i * PR_SLOTS;
+  // what cannot change (rows are read whole; entries past rcount are ignored)
   const uint32_t nr = rd(&a.rcount[i]);
   const uint64_t wm = rd(&a.wmask[i]);
   const uint64_t em = rd(&a.emask[i]);
-  const double vi = rd(&a.vxs[i]), wi = rd(&a.vys[i]);
   const double svi = rd(&a.svx[i]), swi = rd(&a.svy[i]);
-  const uint32_t lv = rd(&a.lev[i]);
   const uint32_t r0 = rd(&rl[lane]), r1 = rd(&rl[lane + 32]);
-  const uint64_t q0 = rd(&sc[lane]), q1 = rd(&sc[lane + 32]);
-  const uint32_t j0 = lane < nr ? r0 : NONE, j1 = lane + 32 < nr ? r1 : NONE;
-  const uint64_t s0 = lane < nr ? q0 : 0, s1 = lane + 32 < nr ? q1 : 0;
-  // round trip 2: the heads' data for the turn, the first successors, and
-  // (if i moved) its record of the cells the guess entered
-  const bool unmoved = same_bits(vi, svi) && same_bits(wi, swi);
+  const uint64_t q0 = rd(&prr[lane]), q1 = rd(&prr[lane + 32]);
+  const uint64_t qs = lane == 0 ? rd(&prr[SELF_ENTRY]) : 0;
+  const uint16_t nv = rd(&a.vcount[i]);
+  const double md = rd(&a.mdelta[i]);
+  const double pxi = a.px[i], pyi = a.py[i];
   uint32_t vc[4], va[4];
-  uint16_t nv = VISIT_NONE;
-  double md = 0, pxi = 0, pyi = 0;
-  if (!unmoved) {
+  {
     const uint32_t *vl = a.vlist + (size_t)i * VISIT_CAP, *vx = a.vaux + (size_t)i * VISIT_CAP;
-    nv = rd(&a.vcount[i]);
-    md = rd(&a.mdelta[i]);
-    pxi = a.px[i];
-    pyi = a.py[i];
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       vc[u] = rd(&vl[4 * lane + u]);
       va[u] = rd(&vx[4 * lane + u]);
     }
   }
-  const uint32_t f0 = (uint32_t)s0 ? (uint32_t)(rd(&a.ents[s0 >> 32]) >> 32) : NONE;
-  const uint32_t f1 = (uint32_t)s1 ? (uint32_t)(rd(&a.ents[s1 >> 32]) >> 32) : NONE;
-  // per head: the offset (x, y) = (xi - xs[j] - vxs[j], ...) of the turn,
-  // formed as the turn forms it, and the head's radius
-  const double xi = a.xs[i] + vi, yi = a.ys[i] + wi;
-  // (a ready turn's heads are not written by any other turn while it runs:
-  // their velocities loaded here are the ones its pushes update)
-  double hx[2], hy[2], hr[2], hv[2], hw[2];
+  const uint32_t j0 = lane < nr ? r0 : NONE, j1 = lane + 32 < nr ? r1 : NONE;
+  const uint64_t ww[3] = {lane < nr ? q0 : 0, lane + 32 < nr ? q1 : 0, qs};
   const uint32_t jj[2] = {j0, j1};
+  double hxs[2], hys[2], hr[2];
+#pragma unroll
   for (int h = 0; h < 2; ++h) {
-    const uint32_t j = jj[h];
-    hx[h] = hy[h] = hr[h] = hv[h] = hw[h] = 0;
-    if (j == NONE) continue;
-    hv[h] = rd(&a.vxs[j]);
-    hw[h] = rd(&a.vys[j]);
-    hx[h] = xi - a.xs[j] - hv[h];
-    hy[h] = yi - a.ys[j] - hw[h];
-    hr[h] = a.radii[j];
+    hxs[h] = hys[h] = hr[h] = 0;
+    if (jj[h] == NONE) continue;
+    hxs[h] = a.xs[jj[h]];
+    hys[h] = a.ys[jj[h]];
+    hr[h] = a.radii[jj[h]];
+  }
+  uint32_t first[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    first[k] = NONE;
+    if (ww[k] & WAIT_NODE) first[k] = (uint32_t)(ww[k] >> 32);
+    else if ((uint32_t)ww[k]) first[k] = (uint32_t)(rd(&a.ents[ww[k] >> 32]) >> 32);
+  }
+  // the wait
+  uint32_t dmax = 0, seen = 0;
+  unsigned long long t0 = 0;
+  bool waited = true;
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+    if (waited) waited = wait_on(a, ww[k], first[k], dmax, t0, seen);
+  if (!__all_sync(FULL, waited) && lane == 0) atomicAdd(&a.counters[C_TIMEOUT], 1u);
+  for (int o = 16; o > 0; o >>= 1) dmax = max(dmax, __shfl_xor_sync(FULL, dmax, o));
+  __syncwarp();
+  __threadfence();
+  // the velocities: the node's own, and its heads' (no other turn writes the
+  // heads of a running turn: the values loaded here are what its pushes update)
+  const double vi = rd(&a.vxs[i]), wi = rd(&a.vys[i]);
+  double hv[2], hw[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    hv[h] = hw[h] = 0;
+    if (jj[h] == NONE) continue;
+    hv[h] = rd(&a.vxs[jj[h]]);
+    hw[h] = rd(&a.vys[jj[h]]);
+  }
+  const bool unmoved = same_bits(vi, svi) && same_bits(wi, swi);
+  // per head: the offset (x, y) = (xi - xs[j] - vxs[j], ...) of the turn,
+  // formed as the turn forms it
+  const double xi = a.xs[i] + vi, yi = a.ys[i] + wi;
+  double hx[2], hy[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    hx[h] = xi - hxs[h] - hv[h];
+    hy[h] = yi - hys[h] - hw[h];
   }
   const double ri = a.radii[i], ri2 = ri * ri;
   uint64_t ex = 0;
   bool fail_read = false;
   if (unmoved && !a.force_traverse) {
     ex = em;
-  } else if (a.force_traverse || !warp_replay(a, i, xi, yi, nv, md, pxi, pyi, vc, va, ex)) {
+  } else if (a.force_traverse ||
+             !warp_replay(a, i, xi, yi, unmoved ? VISIT_NONE : nv, md, pxi, pyi, vc, va, ex)) {
     // i moved beyond its margin: the warp runs the exact traversal; every head
     // it examines must still be among the guessed ones.
     fail_read = !warp_traverse(a, i, xi, yi, ri, jj, ex);
@@ -947,19 +941,19 @@ __device__ uint32_t warp_run(const SpecArgs &a, uint32_t i, bool stamp, TurnTall
   jig = __any_sync(FULL, jig);
   for (int o = 16; o > 0; o >>= 1) over |= __shfl_xor_sync(FULL, over, o);
   __syncwarp();
-  if (fail_read || fail || jig) {
+  uint8_t result = 2;
+  const bool holds = !(fail_read || fail || jig);
+  if (!holds) {
     if (lane == 0) {
       if (jig) atomicAdd(&a.counters[C_JIGGLE], 1u);
       if (fail_read || fail) {
         atomicAdd(&a.counters[C_FAIL], 1u);
         atomicAdd(&a.counters[fail_read ? C_FAIL_READ : C_FAIL_WRITE], 1u);
-        a.state[i] = 3;
-      } else {
-        a.state[i] = 2;
+        result = 3;
       }
     }
   } else {
-    if (lane == 0) {
+    if (lane == 0 && over) {
       // d3 adds its own share head by head, in visit order (R order)
       double v = vi, w = wi;
       uint64_t o = over;
@@ -971,7 +965,6 @@ __device__ uint32_t warp_run(const SpecArgs &a, uint32_t i, bool stamp, TurnTall
       }
       a.vxs[i] = v;
       a.vys[i] = w;
-      a.state[i] = 2;
     }
     if (unmoved) ++tally.fast;
     else ++tally.slow;
@@ -986,45 +979,21 @@ __device__ uint32_t warp_run(const SpecArgs &a, uint32_t i, bool stamp, TurnTall
       atomicMax(&a.max_pusher[j], i);
     }
   }
-  // release: the successors' depths, a fence, then their counts (a head's
-  // successors belong to the lane that wrote it)
-  const uint32_t nl = lv + 1;
-  const uint64_t ss[2] = {s0, s1};
-  const uint32_t ff[2] = {f0, f1};
-  for (int h = 0; h < 2; ++h) {
-    const uint32_t c = (uint32_t)ss[h];
-    for (uint32_t t = 0; t < c; ++t)
-      atomicMax(&a.lev[t ? (uint32_t)(rd(&a.ents[(ss[h] >> 32) + t]) >> 32) : ff[h]], nl);
-  }
-  // a lane's successors wait only on the heads it wrote (its own entries):
-  // the fence orders those writes before the releases
+  // done: after the writes (a turn that wrote nothing has finished its reads)
+  if (holds && over) __threadfence();
   __syncwarp();
-  if ((pushed[0] || pushed[1]) && !(fail_read || fail || jig)) __threadfence();
-  uint32_t mine = NONE;  // the first turn this lane made ready; later ones are queued
-  for (int h = 0; h < 2; ++h) {
-    const uint32_t c = (uint32_t)ss[h];
-    for (uint32_t t = 0; t < c; ++t) {
-      const uint32_t x = t ? (uint32_t)(rd(&a.ents[(ss[h] >> 32) + t]) >> 32) : ff[h];
-      if (release(a, x)) {
-        if (mine == NONE) mine = x;
-        else push_ready(a, x);
-      }
-    }
-  }
-  tally.depth = max(tally.depth, nl);
+  const uint32_t lv = dmax + 1;
+  tally.depth = max(tally.depth, lv);
   if (lane == 0) {
+    a.lev[i] = lv;
+    a.state[i] = result;
     atomicAdd(&a.counters[C_DONE], 1u);
     if (stamp) {
-      const uint32_t k = lv < 63 ? lv : 63;
+      const uint32_t k = lv - 1 < 63 ? lv - 1 : 63;
       atomicMax(&a.stamps[16 + k], now_ns());
       atomicAdd(&a.stamps[80 + k], 1ull);
     }
   }
-  const unsigned ready = __ballot_sync(FULL, mine != NONE);
-  if (!ready) return NONE;
-  const int first = __ffs(ready) - 1;
-  if (mine != NONE && (int)lane != first) push_ready(a, mine);
-  return __shfl_sync(FULL, mine, first);
 }
 
 // The serial loop (collide.zig:47-100) with draws from the device LCG.
@@ -1113,6 +1082,7 @@ __global__ void __launch_bounds__(SPEC_THREADS, 2) k_collide_spec(SpecArgs a) {
     a.push[i] = 0;
     a.min_pusher[i] = NONE;
     a.max_pusher[i] = 0;
+    a.aflag[i] = 0;
     if (!spec_guess_fit(a, i, margin_of(a, i), false)) {
       atomicAdd(&a.counters[C_OVERFLOW], 1u);
       a.state[i] = 0;
@@ -1121,6 +1091,7 @@ __global__ void __launch_bounds__(SPEC_THREADS, 2) k_collide_spec(SpecArgs a) {
     if (a.wmask[i]) {
       a.state[i] = 1;
       a.active[atomicAdd(&a.counters[C_ACTIVE], 1u)] = i;
+      a.aflag[i] = 1;
       const uint32_t *rl = a.rlist + (size_t)i * SPEC_CAP;
       const uint32_t nr = a.rcount[i];
       for (uint32_t h = 0; h < nr; ++h) atomicAdd(&a.cnt[rl[h]], 1u);
@@ -1145,7 +1116,9 @@ __global__ void __launch_bounds__(SPEC_THREADS, 2) k_collide_spec(SpecArgs a) {
     for (uint32_t base = gw * 32; base < n; base += nwarps * 32) warp_offsets(a, base);
     for (uint32_t base = gw * 32; base < n_active; base += nwarps * 32)
       warp_find_bigfill(a, base, n_active);
-    if (tid == 0) a.counters[C_QHEAD] = a.counters[C_QTAIL] = a.counters[C_VWORK] = 0;
+    if (tid == 0) a.counters[C_CLAIM] = a.counters[C_VWORK] = 0;
+    // the active nodes' places in index order (one grid barrier inside)
+    grid_excl_scan(g, a.aflag, a.apos, n, a.scan_part);
     g.sync();
     if (tid == 0 && attempt == 0) a.stamps[13] = now_ns();
     for (uint32_t base = gw * 32; base < n_active; base += nwarps * 32) warp_fill(a, base, n_active);
@@ -1165,25 +1138,25 @@ __global__ void __launch_bounds__(SPEC_THREADS, 2) k_collide_spec(SpecArgs a) {
     }
     g.sync();
     if (tid == 0 && attempt < 3) a.stamps[10 + attempt] = now_ns();
-    // E: the turns with nothing to wait for are queued; warps claim queue
-    // slots in order and run the turns, which queue those they release.
-    for (uint32_t k = tid; k < n_active; k += nth) {
-      const uint32_t i = rd(&a.active[k]);
-      if (rd(&a.pred[i]) == 0) push_ready(a, i);
-    }
+    // E: warps claim the active nodes in index order (every turn waits only
+    // on turns of lower index) and run them once what they wait on is done.
     {
       TurnTally tally;
-      for (uint32_t next = NONE;;) {
-        uint32_t i = next;
-        if (i == NONE) {
-          if (lane == 0) {
-            const uint32_t slot = atomicAdd(&a.counters[C_QHEAD], 1u);
-            if (slot < n_active) i = wait_slot(a, slot, n_active);
-          }
-          i = __shfl_sync(FULL, i, 0);
-          if (i == NONE) break;
+      uint32_t k = 0;
+      if (lane == 0) k = atomicAdd(&a.counters[C_CLAIM], 1u);
+      k = __shfl_sync(FULL, k, 0);
+      uint32_t i = k < n_active ? rd(&a.sact[k]) : NONE;
+      while (k < n_active) {
+        // the next claim and its node, loaded before this turn runs
+        uint32_t nk = 0, ni = NONE;
+        if (lane == 0) {
+          nk = atomicAdd(&a.counters[C_CLAIM], 1u);
+          if (nk < n_active) ni = rd(&a.sact[nk]);
         }
-        next = warp_run(a, i, a.profile && attempt == 0, tally, contrib[wl][0], contrib[wl][1]);
+        warp_pull(a, __shfl_sync(FULL, i, 0), a.profile && attempt == 0, tally, contrib[wl][0],
+                  contrib[wl][1]);
+        k = __shfl_sync(FULL, nk, 0);
+        i = __shfl_sync(FULL, ni, 0);
       }
       if (lane == 0) {
         if (tally.fast) atomicAdd(&a.counters[C_FAST_TURNS], tally.fast);
@@ -1220,7 +1193,10 @@ __global__ void __launch_bounds__(SPEC_THREADS, 2) k_collide_spec(SpecArgs a) {
       if (st == 3 || st == 4) {
         // every head within a four times wider margin may be written
         if (!spec_guess_fit(a, i, 4 * rd(&a.mdelta[i]), true)) atomicAdd(&a.counters[C_OVERFLOW], 1u);
-        if (st == 4) a.active[atomicAdd(&a.counters[C_ACTIVE], 1u)] = i;  // was inactive
+        if (st == 4) {  // was inactive
+          a.active[atomicAdd(&a.counters[C_ACTIVE], 1u)] = i;
+          a.aflag[i] = 1;
+        }
         a.state[i] = 1;
       } else if (st == 2) {
         a.state[i] = 1;
@@ -1279,10 +1255,11 @@ static void spec_arrays(CollideSpec &s, F f) {
   f((void **)&s.roff, 4);
   f((void **)&s.ent, (SPEC_CAP + 1) * 8ull);  // at most SPEC_CAP heads and itself per node
   f((void **)&s.ents, (SPEC_CAP + 1) * 8ull);
-  f((void **)&s.succ, SPEC_CAP * 8ull);
-  f((void **)&s.pred, 4);
+  f((void **)&s.pr, PR_SLOTS * 8ull);
   f((void **)&s.lev, 4);
-  f((void **)&s.queue, QSTRIDE * 4ull);
+  f((void **)&s.aflag, 4);
+  f((void **)&s.apos, 4);
+  f((void **)&s.sact, 4);
   f((void **)&s.work, 3 * 4ull);  // bigfill, biglink, vwork
 }
 
@@ -1296,6 +1273,7 @@ int collide_spec_reserve(CollideSpec &s, uint32_t n) {
   if (!s.counters) {
     D3_CUDA_OK(cudaMalloc(&s.counters, C_COUNTERS * sizeof(uint32_t)));
     D3_CUDA_OK(cudaMemset(s.counters, 0, C_COUNTERS * sizeof(uint32_t)));
+    D3_CUDA_OK(cudaMalloc(&s.grid_part, 1024 * sizeof(uint32_t)));
   }
   // 16 phase stamps, then attempt 1's per-depth last finish times and turn
   // counts (64 each)
@@ -1320,6 +1298,7 @@ int collide_spec_reserve(CollideSpec &s, uint32_t n) {
 void collide_spec_free(CollideSpec &s) {
   spec_arrays(s, [](void **p, size_t) { cudaFree(*p); });
   cudaFree(s.counters);
+  cudaFree(s.grid_part);
   cudaFree(s.stamps);
   s = CollideSpec();
 }
@@ -1356,7 +1335,8 @@ int collide_parallel(TreeDev &t, const NodeArrays &a, const double *radii, doubl
   args.vlist = s.vlist; args.vaux = s.vaux; args.vcount = s.vcount; args.start = s.start; args.mdelta = s.mdelta;
   args.state = s.state; args.active = s.active;
   args.cnt = s.cnt; args.rlen = s.rlen; args.roff = s.roff; args.ent = s.ent; args.ents = s.ents;
-  args.succ = s.succ; args.pred = s.pred; args.lev = s.lev; args.queue = s.queue;
+  args.pr = s.pr; args.lev = s.lev; args.aflag = s.aflag; args.apos = s.apos; args.sact = s.sact;
+  args.scan_part = s.grid_part;
   args.bigfill = s.work;
   args.biglink = s.work + s.cap;
   args.vwork = s.work + 2ull * s.cap;

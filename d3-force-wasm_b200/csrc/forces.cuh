@@ -111,8 +111,9 @@ struct CollideSpec {
   uint8_t *state = nullptr;
   uint32_t *active = nullptr;
   uint32_t *cnt = nullptr, *rlen = nullptr, *roff = nullptr;  // the access lists
-  uint64_t *ent = nullptr, *ents = nullptr, *succ = nullptr;
-  uint32_t *pred = nullptr, *lev = nullptr, *queue = nullptr;
+  uint64_t *ent = nullptr, *ents = nullptr, *pr = nullptr;
+  uint32_t *lev = nullptr, *aflag = nullptr, *apos = nullptr, *sact = nullptr;
+  uint32_t *grid_part = nullptr;  // 1024 words: grid scan partials
   uint32_t *work = nullptr;  // 3 * cap: items shared out to whole warps
   double *push = nullptr;
   uint32_t *min_pusher = nullptr, *max_pusher = nullptr;

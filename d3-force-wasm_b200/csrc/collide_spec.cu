@@ -259,9 +259,14 @@ __device__ bool spec_guess(const SpecArgs &a, uint32_t i, double margin, bool al
 // prunes (a running maximum of those subtrees' ends). Only the internal
 // cells' boxes are loaded here. Returns false when the record does not apply
 // (i moved beyond its margin, or no record): lane-uniform.
+// A recorded internal cell's box and radius, staged in shared memory.
+struct Box {
+  double x0, y0, x1, y1, r;
+};
+
 __device__ bool warp_replay(const SpecArgs &a, uint32_t i, double xi, double yi, uint16_t nv,
                             double md, double pxi, double pyi, const uint32_t *vc,
-                            const uint32_t *va, uint64_t &mask) {
+                            const uint32_t *va, const Box *boxes, uint64_t &mask) {
   const unsigned lane = threadIdx.x & 31;
   md *= (1 - 1e-9);
   if (nv == VISIT_NONE || !(fabs(xi - pxi) < md && fabs(yi - pyi) < md)) return false;
@@ -281,7 +286,7 @@ __device__ bool warp_replay(const SpecArgs &a, uint32_t i, double xi, double yi,
       if (x & LEAF_TAG) {
         head[u] = (x & ~LEAF_TAG) > i;
       } else {
-        const CRec &q = a.rec[c];
+        const Box &q = boxes[t];
         if (pruned(q, xi, yi, ri + q.r)) upto[u] = x;
       }
     }
@@ -767,9 +772,9 @@ __device__ void warp_link(const SpecArgs &a, uint32_t base) {
   }
 }
 
-__device__ inline uint8_t ld_relaxed_u8(const uint8_t *p) {
+__device__ inline uint8_t ld_acquire_u8(const uint8_t *p) {
   uint16_t v;
-  asm volatile("ld.relaxed.gpu.global.u8 %0, [%1];" : "=h"(v) : "l"(p) : "memory");
+  asm volatile("ld.acquire.gpu.global.u8 %0, [%1];" : "=h"(v) : "l"(p) : "memory");
   return (uint8_t)v;
 }
 
@@ -781,7 +786,7 @@ __device__ bool wait_on(const SpecArgs &a, uint64_t r, uint32_t first, uint32_t 
   const uint32_t c = (uint32_t)r & 0x7fffffffu;
   for (uint32_t t = 0; t < c; ++t) {
     const uint32_t x = t ? (uint32_t)(rd(&a.ents[(r >> 32) + t]) >> 32) : first;
-    for (uint32_t it = 0; ld_relaxed_u8(&a.state[x]) == 1; ++it) {
+    for (uint32_t it = 0; ld_acquire_u8(&a.state[x]) == 1; ++it) {
       if (it >= 4) __nanosleep(64);
       if ((it & 15) == 15) {
         const uint32_t d = ld_relaxed(&a.counters[C_DONE]);
@@ -812,7 +817,7 @@ struct TurnTally {
 // the turn, and marks the node done (also after a failed turn: the attempt
 // then fails as a whole, but every turn still runs).
 __device__ void warp_pull(const SpecArgs &a, uint32_t i, bool stamp, TurnTally &tally, double *cx,
-                          double *cy) {
+                          double *cy, Box *boxes) {
   const unsigned lane = threadIdx.x & 31;
   const uint32_t *rl = a.rlist + (size_t)i * SPEC_CAP;
   const uint64_t *prr = a.pr + (size_t)i * PR_SLOTS;
@@ -834,6 +839,17 @@ __device__ void warp_pull(const SpecArgs &a, uint32_t i, bool stamp, TurnTally &
     for (int u = 0; u < 4; ++u) {
       vc[u] = rd(&vl[4 * lane + u]);
       va[u] = rd(&vx[4 * lane + u]);
+    }
+    // the recorded internal cells' boxes, for a replay (a lane stages its own)
+    if (nv != VISIT_NONE) {
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const uint32_t t = 4 * lane + u;
+        if (t < nv && !(va[u] & LEAF_TAG)) {
+          const CRec &q = a.rec[vc[u]];
+          boxes[t] = Box{q.x0, q.y0, q.x1, q.y1, q.r};
+        }
+      }
     }
   }
   const uint32_t j0 = lane < nr ? r0 : NONE, j1 = lane + 32 < nr ? r1 : NONE;
@@ -864,11 +880,17 @@ __device__ void warp_pull(const SpecArgs &a, uint32_t i, bool stamp, TurnTally &
     if (waited) waited = wait_on(a, ww[k], first[k], dmax, t0, seen);
   if (!__all_sync(FULL, waited) && lane == 0) atomicAdd(&a.counters[C_TIMEOUT], 1u);
   for (int o = 16; o > 0; o >>= 1) dmax = max(dmax, __shfl_xor_sync(FULL, dmax, o));
-  __syncwarp();
-  __threadfence();
-  // the velocities: the node's own, and its heads' (no other turn writes the
-  // heads of a running turn: the values loaded here are what its pushes update)
-  const double vi = rd(&a.vxs[i]), wi = rd(&a.vys[i]);
+  // the velocities, each read by the lane whose acquiring waits cover it: the
+  // node's own by lane 0 (it waited on the node's own accesses), its heads'
+  // by their lanes (no other turn writes the heads of a running turn: the
+  // values loaded here are what its pushes update)
+  double vi = 0, wi = 0;
+  if (lane == 0) {
+    vi = rd(&a.vxs[i]);
+    wi = rd(&a.vys[i]);
+  }
+  vi = __shfl_sync(FULL, vi, 0);
+  wi = __shfl_sync(FULL, wi, 0);
   double hv[2], hw[2];
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
@@ -893,7 +915,7 @@ __device__ void warp_pull(const SpecArgs &a, uint32_t i, bool stamp, TurnTally &
   if (unmoved && !a.force_traverse) {
     ex = em;
   } else if (a.force_traverse ||
-             !warp_replay(a, i, xi, yi, unmoved ? VISIT_NONE : nv, md, pxi, pyi, vc, va, ex)) {
+             !warp_replay(a, i, xi, yi, unmoved ? VISIT_NONE : nv, md, pxi, pyi, vc, va, boxes, ex)) {
     // i moved beyond its margin: the warp runs the exact traversal; every head
     // it examines must still be among the guessed ones.
     fail_read = !warp_traverse(a, i, xi, yi, ri, jj, ex);
@@ -1040,6 +1062,7 @@ __device__ void spec_serial(const SpecArgs &a) {
 
 __global__ void __launch_bounds__(SPEC_THREADS, 2) k_collide_spec(SpecArgs a) {
   __shared__ double contrib[SPEC_WARPS][2][SPEC_CAP];
+  extern __shared__ Box boxes_all[];  // SPEC_WARPS * VISIT_CAP (dynamic)
   cg::grid_group g = cg::this_grid();
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
   const uint32_t gw = tid >> 5, nwarps = nth >> 5, wl = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1154,7 +1177,7 @@ __global__ void __launch_bounds__(SPEC_THREADS, 2) k_collide_spec(SpecArgs a) {
           if (nk < n_active) ni = rd(&a.sact[nk]);
         }
         warp_pull(a, __shfl_sync(FULL, i, 0), a.profile && attempt == 0, tally, contrib[wl][0],
-                  contrib[wl][1]);
+                  contrib[wl][1], boxes_all + (size_t)wl * VISIT_CAP);
         k = __shfl_sync(FULL, nk, 0);
         i = __shfl_sync(FULL, ni, 0);
       }
@@ -1231,6 +1254,8 @@ __global__ void __launch_bounds__(SPEC_THREADS, 2) k_collide_spec(SpecArgs a) {
 }
 
 static int g_spec_blocks = 0;
+// Dynamic shared memory of k_collide_spec: the staged boxes, per warp.
+constexpr size_t SPEC_DYN_SMEM = (size_t)SPEC_WARPS * VISIT_CAP * sizeof(Box);
 
 // Every device array of the scratch, with its bytes per node of capacity.
 template <class F>
@@ -1310,7 +1335,9 @@ int collide_parallel(TreeDev &t, const NodeArrays &a, const double *radii, doubl
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_collide_spec, SPEC_THREADS, 0);
+    cudaFuncSetAttribute(k_collide_spec, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)SPEC_DYN_SMEM);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_collide_spec, SPEC_THREADS, SPEC_DYN_SMEM);
     // blocks per SM: full occupancy (at most 2), or D3_COLLIDE_BLOCKS_PER_SM
     int want = per > 2 ? 2 : per;
     if (const char *e = getenv("D3_COLLIDE_BLOCKS_PER_SM")) {
@@ -1346,7 +1373,7 @@ int collide_parallel(TreeDev &t, const NodeArrays &a, const double *radii, doubl
   void *params[] = {&args};
   ++g_launches;
   cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_collide_spec, g_spec_blocks,
-                                              SPEC_THREADS, params, 0, st);
+                                              SPEC_THREADS, params, SPEC_DYN_SMEM, st);
   return e == cudaSuccess ? 0 : -1;
 }
 

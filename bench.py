@@ -315,7 +315,7 @@ def run_ours(args, pkg, sc):
     }.get(dom, n * 64.0)
     # DRAM bytes (read + write) per launch from one ncu capture of tick 13 of
     # this workload (after an L2 flush).
-    traffic = {"collide_loop": 43925248 + 6277632, "mb_traverse": 7734016}.get(dom)
+    traffic = {"collide_loop": 63628032 + 9661184, "mb_traverse": 7734016}.get(dom)
     achieved = alg_bytes / (per_tick_ms[dom] * 1e-3) / 1e9
     line = {
         "metric": METRIC, "value": round(ms, 4), "unit": "ms/tick", "n_gpus": world,

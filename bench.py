@@ -59,6 +59,19 @@ def dist_env():
             int(os.environ.get("WORLD_SIZE", 1)))
 
 
+def max_over_ranks(x, world):
+    """The largest of x over all ranks of the process group (a replicated
+    job's time is its slowest replica's); x itself with one rank."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(x)], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def oracle_ms_per_tick(pkg, sc, threads, warmup, rounds, ticks):
     """The reference algorithm (oracle) on the host: `warmup` ticks, then the
     best of `rounds` rounds of `ticks` ticks (bench/threads.js:85-96)."""
@@ -265,12 +278,9 @@ def run_ours(args, pkg, sc):
     phases = {name: core.sim_stat(h, 100 + k) for k, name in enumerate(PHASES)}
     side = {name: core.sim_stat(h, 100 + k) / prof_steps for name, k in SIDE_PHASES.items()}
     core.sim_set_profile(h, 0)
-    ms = sum(times) / len(times)
+    ms = max_over_ranks(sum(times) / len(times), world)
     if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.barrier()
-        ms = float(t.item())
     sim.device_end()
     # e2e through the public API: node state in, tick, node state out
     e2e = []
@@ -280,11 +290,7 @@ def run_ours(args, pkg, sc):
         sim.tick(1)
         e2e.append((time.perf_counter() - t0) * 1e3)
     n = WORKLOAD["n"]
-    e2e_ms = sum(e2e) / len(e2e)
-    if world > 1:
-        t = torch.tensor([e2e_ms], dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(sum(e2e) / len(e2e), world)
     stats = {"collide_depth": core.sim_stat(h, 0), "collide_attempts": core.sim_stat(h, 1),
              "collide_serial_fallback": core.sim_stat(h, 2), "link_levels": core.sim_stat(h, 4)}
     sim.close()

@@ -695,12 +695,6 @@ struct LinkFlowArgs {
   int serial_lcg;     // a met jiggle is resolved in the launch (device LCG)
 };
 
-__device__ inline uint32_t ld_relaxed_u32(const uint32_t *p) {
-  uint32_t v;
-  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-
 __device__ inline unsigned long long globaltimer_ns() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -710,18 +704,25 @@ __device__ inline unsigned long long globaltimer_ns() {
 // A link's wait, bounded: until `ns` links on src and `nt` on tgt have
 // finished. False if it gave up (20 ms): the pass is then restored and run
 // serially.
+__device__ inline uint32_t ld_acquire_u32(const uint32_t *p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// A finished link's count on a node, ordered after its velocity writes.
+__device__ inline void red_release_add(uint32_t *p, uint32_t v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 __device__ inline bool link_wait(const uint32_t *done, uint32_t src, uint32_t ns, uint32_t tgt,
                                  uint32_t nt) {
-  if (ld_relaxed_u32(&done[src]) >= ns && ld_relaxed_u32(&done[tgt]) >= nt) {
-    __threadfence();
-    return true;
-  }
+  // acquire loads: a count seen orders the counted links' writes before the
+  // velocities this link reads
+  if (ld_acquire_u32(&done[src]) >= ns && ld_acquire_u32(&done[tgt]) >= nt) return true;
   const unsigned long long t0 = globaltimer_ns();
   for (uint32_t it = 0;; ++it) {
-    if (ld_relaxed_u32(&done[src]) >= ns && ld_relaxed_u32(&done[tgt]) >= nt) {
-      __threadfence();
-      return true;
-    }
+    if (ld_acquire_u32(&done[src]) >= ns && ld_acquire_u32(&done[tgt]) >= nt) return true;
     if (it >= 8) __nanosleep(64);
     if ((it & 15) == 15 && globaltimer_ns() - t0 > 20000000ull) return false;
   }
@@ -769,10 +770,9 @@ __global__ void __launch_bounds__(256) k_link_flow(LinkFlowArgs a) {
         b = 1 - b;
         a.vxs[c.src] = vxsrc + x * b;
         a.vys[c.src] = vysrc + y * b;
-        __threadfence();
       }
-      atomicAdd(&a.done[c.src], 1u);
-      atomicAdd(&a.done[c.tgt], 1u);
+      red_release_add(&a.done[c.src], 1u);
+      red_release_add(&a.done[c.tgt], 1u);
     }
     g.sync();
   }

@@ -59,27 +59,61 @@ __device__ inline void box_merge(double *v, uint32_t *ix, uint32_t &m, const dou
   m += m2;
 }
 
+// The block's merged box (every thread gets it): warp shuffles, then the
+// warps' results by warp 0 (the merge is commutative and associative).
 __device__ void block_box_reduce(double *v, uint32_t *ix, uint32_t &m) {
-  __shared__ double sv[BOX_THREADS][4];
-  __shared__ uint32_t si[BOX_THREADS][4];
-  __shared__ uint32_t sm[BOX_THREADS];
-  const unsigned t = threadIdx.x;
-  for (int q = 0; q < 4; ++q) { sv[t][q] = v[q]; si[t][q] = ix[q]; }
-  sm[t] = m;
-  __syncthreads();
-  for (unsigned s = BOX_THREADS / 2; s > 0; s >>= 1) {
-    if (t < s) {
-      double a[4];
-      uint32_t ai[4];
-      uint32_t am = sm[t];
-      for (int q = 0; q < 4; ++q) { a[q] = sv[t][q]; ai[q] = si[t][q]; }
-      box_merge(a, ai, am, sv[t + s], si[t + s], sm[t + s]);
-      for (int q = 0; q < 4; ++q) { sv[t][q] = a[q]; si[t][q] = ai[q]; }
-      sm[t] = am;
+  __shared__ double sv[BOX_THREADS / 32][4];
+  __shared__ uint32_t si[BOX_THREADS / 32][4];
+  __shared__ uint32_t sm[BOX_THREADS / 32];
+  const unsigned lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  auto warp_reduce = [&]() {
+    for (int o = 16; o > 0; o >>= 1) {
+      double v2[4];
+      uint32_t i2[4];
+      for (int q = 0; q < 4; ++q) {
+        v2[q] = __shfl_down_sync(0xffffffffu, v[q], o);
+        i2[q] = __shfl_down_sync(0xffffffffu, ix[q], o);
+      }
+      const uint32_t m2 = __shfl_down_sync(0xffffffffu, m, o);
+      if (lane + o < 32) box_merge(v, ix, m, v2, i2, m2);
     }
-    __syncthreads();
+  };
+  warp_reduce();
+  if (lane == 0) {
+    for (int q = 0; q < 4; ++q) {
+      sv[w][q] = v[q];
+      si[w][q] = ix[q];
+    }
+    sm[w] = m;
   }
-  for (int q = 0; q < 4; ++q) { v[q] = sv[0][q]; ix[q] = si[0][q]; }
+  __syncthreads();
+  if (w == 0) {
+    if (lane < nw) {
+      for (int q = 0; q < 4; ++q) {
+        v[q] = sv[lane][q];
+        ix[q] = si[lane][q];
+      }
+      m = sm[lane];
+    } else {
+      v[0] = v[1] = INFINITY;
+      v[2] = v[3] = -INFINITY;
+      for (int q = 0; q < 4; ++q) ix[q] = NONE;
+      m = 0;
+    }
+    warp_reduce();
+    if (lane == 0) {
+      for (int q = 0; q < 4; ++q) {
+        sv[0][q] = v[q];
+        si[0][q] = ix[q];
+      }
+      sm[0] = m;
+    }
+  }
+  __syncthreads();
+  for (int q = 0; q < 4; ++q) {
+    v[q] = sv[0][q];
+    ix[q] = si[0][q];
+  }
   m = sm[0];
   __syncthreads();
 }

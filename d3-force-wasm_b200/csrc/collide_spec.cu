@@ -52,14 +52,14 @@ constexpr int SPEC_ATTEMPTS = 3;
 constexpr unsigned SPEC_THREADS = 256;
 constexpr unsigned SPEC_WARPS = SPEC_THREADS / 32;
 constexpr uint32_t SELF_ENTRY = SPEC_CAP;  // an access list entry of the node itself
-// A queue wait gives up after this long without any turn finishing.
+// A turn's wait gives up after this long without any turn finishing.
 constexpr unsigned long long SPEC_WAIT_NS = 20000000ull;
 constexpr unsigned FULL = 0xffffffffu;
 
 // counters[]: 0..13 are reported by the engine (13: waits that gave up); the
 // ones every turn touches sit in cache lines of their own.
 enum : uint32_t {
-  C_ACTIVE = 0, C_FAIL = 2, C_JIGGLE, C_OVERFLOW, C_ROUNDS, C_ATTEMPTS, C_SERIAL,
+  C_ACTIVE = 0, C_FAIL = 2, C_JIGGLE, C_OVERFLOW, C_DEPTH, C_ATTEMPTS, C_SERIAL,
   C_FAIL_READ, C_FAIL_WRITE, C_FAIL_MOVED, C_FAST_TURNS, C_SLOW_TURNS, C_TIMEOUT,
   C_ALLOC = 16, C_BIGFILL, C_BIGLINK, C_VWORK, C_DONE = 32, C_CLAIM = 64, C_COUNTERS = 128
 };
@@ -1184,7 +1184,7 @@ __global__ void __launch_bounds__(SPEC_THREADS, 2) k_collide_spec(SpecArgs a) {
       if (lane == 0) {
         if (tally.fast) atomicAdd(&a.counters[C_FAST_TURNS], tally.fast);
         if (tally.slow) atomicAdd(&a.counters[C_SLOW_TURNS], tally.slow);
-        if (tally.depth) atomicMax(&a.counters[C_ROUNDS], tally.depth);
+        if (tally.depth) atomicMax(&a.counters[C_DEPTH], tally.depth);
       }
     }
     g.sync();
@@ -1204,7 +1204,7 @@ __global__ void __launch_bounds__(SPEC_THREADS, 2) k_collide_spec(SpecArgs a) {
       ok = true;
       break;
     }
-    // Retry: restore, promote failed nodes, requeue every active node.
+    // Retry: restore, promote failed nodes, make every active node pending again.
     for (uint32_t i = tid; i < n; i += nth) {
       a.vxs[i] = a.svx[i];
       a.vys[i] = a.svy[i];

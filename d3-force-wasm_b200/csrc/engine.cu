@@ -1124,7 +1124,7 @@ double sim_stat(uint32_t h, uint32_t which) {
     case 9: return spec[10];  // inactive nodes whose turn would have written
     case 10: return spec[11]; // turns run from the recorded head list
     case 11: return spec[12]; // turns that traversed the tree
-    case 28: return spec[13]; // queue waits that gave up
+    case 28: return spec[13]; // turn waits that gave up
     case 19: {
       // microseconds of the first attempt's access-list build
       unsigned long long st[11];
@@ -1153,7 +1153,7 @@ double sim_stat(uint32_t h, uint32_t which) {
     }
     case 12: case 13: case 14: case 15: case 16: case 17: case 18: {
       // microseconds of the last parallel collide's phases: 12 guess, 13/14
-      // attempt 1 rounds / check, 15/16 attempt 2, 17/18 attempt 3
+      // attempt 1 turns / check, 15/16 attempt 2, 17/18 attempt 3
       unsigned long long st[16];
       cudaMemcpy(st, s->spec.stamps, sizeof st, cudaMemcpyDeviceToHost);
       int k = which - 12;

@@ -140,30 +140,35 @@ int32_t sim_tick(uint32_t h, uint32_t ticks, double *alpha, double alpha_target,
 /* Milliseconds of device time of the last sim_tick call (CUDA events). */
 double sim_last_tick_ms(uint32_t h);
 
-/* Diagnostics of the last force runs (synchronises): 0 the longest chain of
- * dependent turns of the last parallel exact collide, 1 its attempts, 2 1 if it fell back to the serial
- * loop, 3 nodes the last exact many-body traversal flagged for jiggle, 4 link
- * levels of the last exact link plan, 5 1 if the last exact link pass fell
- * back to the serial order (a jiggle), 6 kernels this library launched so
- * far (all simulations); 7, 8 turns of the last parallel collide that met an
- * unguessed head / overlap, 9 inactive nodes whose turn would have written,
- * 10 turns run from the recorded head list, 11 turns that traversed the tree;
- * 12-18 microseconds of the last parallel collide's phases (guess, then
- * turns / check per attempt), 19 of its first attempt's access-list build
- * (part of 13), 28 its queue waits that gave up (0 unless it failed); the last center sum's 22 / 23 microseconds of
- * the exact x / y walks, 24 its x walk's record batches rerun with their
- * entry tests, 25 stretches added one by one, 26 records in all; 27 host
- * milliseconds the last sim_tick spent queueing work; 30-37 microseconds of
- * the last tree build's phases (box, keys, sort, runs, cell counts, their
- * scan, cell owners, the cells); with profiling on, 300 + k microseconds from the end of
- * the last parallel collide's first list build to its last turn of depth k,
- * 400 + k its turns of depth k (k < 63; 63 counts every deeper turn);
- * 1000 + k (k < 144) its raw stamps (globaltimer ns, then per-depth data);
- * 100 + k milliseconds and 200 + k count of phase k
- * since sim_set_profile(h, 1): 0 many-body tree, 1 many-body accumulation,
- * 2 many-body traversal, 3 exact link, 4 collide tree and radii, 5 collide
- * node loop, 6 center, 7 integrate, 8 fast many-body, 9 fast link, 10 fast
- * collide. */
+/* Diagnostics of the last force runs (synchronises):
+ *   0 the longest chain of dependent turns of the last parallel exact
+ *     collide, 1 its attempts, 2 1 if it fell back to the serial loop;
+ *   3 nodes the last exact many-body traversal flagged for jiggle;
+ *   4 link levels of the last exact link plan, 5 1 if the last exact link
+ *     pass fell back to the serial order (a jiggle);
+ *   6 kernels this library launched so far (all simulations);
+ *   7, 8 turns of the last parallel collide that met an unguessed head /
+ *     overlap, 9 inactive nodes whose turn would have written, 10 turns run
+ *     from the recorded head list, 11 turns that traversed the tree;
+ *   12-18 microseconds of the last parallel collide's phases (guess, then
+ *     turns / check per attempt), 19 of its first attempt's access-list
+ *     build (part of 13), 28 its turn waits that gave up (0 unless it
+ *     failed);
+ *   22 / 23 microseconds of the last center sum's exact x / y walks, 24 its
+ *     x walk's record batches rerun with their entry tests, 25 stretches
+ *     added one by one, 26 records in all;
+ *   27 host milliseconds the last sim_tick spent queueing work;
+ *   30-37 microseconds of the last tree build's phases (box, keys, sort,
+ *     runs, cell counts, their scan, cell owners, the cells);
+ *   with profiling on, 300 + k microseconds from the end of the last
+ *     parallel collide's first list build to its last turn of depth k, and
+ *     400 + k its turns of depth k (k < 63; 63 counts every deeper turn);
+ *   1000 + k (k < 144) its raw stamps (globaltimer ns, then per-depth data);
+ *   100 + k milliseconds and 200 + k count of phase k since
+ *     sim_set_profile(h, 1): 0 many-body tree, 1 many-body accumulation,
+ *     2 many-body traversal, 3 exact link, 4 collide tree and radii,
+ *     5 collide node loop, 6 center, 7 integrate, 8 fast many-body, 9 fast
+ *     link, 10 fast collide. */
 double sim_stat(uint32_t h, uint32_t which);
 /* Phase timers on (1) / off (0); both reset them. CUDA events on the
  * simulation's stream around each phase. */

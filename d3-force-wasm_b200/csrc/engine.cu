@@ -1142,9 +1142,10 @@ double sim_stat(uint32_t h, uint32_t which) {
       return st[k + 1] >= st[k] ? (double)(st[k + 1] - st[k]) * 1e-3 : -1;
     }
     case 22: case 23: case 24: case 25: case 26: {
-      // the last center sum: 22 / 23 microseconds of the exact x / y walks;
-      // the x walk's 24 record batches rerun with their entry tests, 25
-      // stretches added one by one, 26 records in all
+      // the last center sum: 22 / 23 microseconds of the exact x / y walks
+      // (or serial sums, up to 65,536 nodes); the x walk's 24 record batches
+      // rerun with their entry tests, 25 stretches added one by one, 26
+      // records in all (24-26 are 0 for the serial sums)
       unsigned long long st[8];
       cudaMemcpy(st, s->scratch.csum_stamps, sizeof st, cudaMemcpyDeviceToHost);
       if (which >= 24) return (double)st[5 + (which - 24)];

@@ -81,6 +81,15 @@ __device__ inline Climb climb_up(const uint32_t *parent, const uint8_t *pnch, ui
   return c;
 }
 
+// A child's arrival at its parent: release orders the child's values before
+// the count, acquire makes the earlier children's values visible to the last
+// one (the counts on one parent form a release sequence).
+__device__ inline uint32_t arrive_acq_rel(uint32_t *p) {
+  uint32_t old;
+  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(p) : "memory");
+  return old;
+}
+
 // many_body.zig:101-135 (accumulate). Leaf: head position, strength summed
 // over the chain from perm[first + count - 1] down. Internal: children 0..3
 // with a truthy |value|. Every cell's traversal record: the thread visiting
@@ -167,22 +176,31 @@ __global__ void k_mb_accumulate(Cell *cells, const uint32_t *parent, const uint8
         }
         continue;
       }
-      Cell *pc = &cells[p];
+      // The parent's links and child list were written by the tree build:
+      // loaded before the arrival, so only the children's values wait on it.
       const Climb next = climb_up(parent, pnch, p);
-      __threadfence();
-      if (atomicAdd(&counter[p], 1u) != up.nch - 1) break;
-      __threadfence();
-      double st = 0, weight = 0, x = 0, y = 0;
+      uint32_t ch[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) ch[k] = cells[p].child[k];
+      if (arrive_acq_rel(&counter[p]) != up.nch - 1) break;
+      double2 cxy[4], cvw[4];
+#pragma unroll
       for (int k = 0; k < 4; ++k) {
-        uint32_t ch = pc->child[k];
-        if (ch == NONE) continue;
-        double v = ld_cg(&cells[ch].value);
+        if (ch[k] == NONE) continue;
+        cxy[k] = __ldcg((const double2 *)&rec[ch[k]].x);
+        cvw[k] = __ldcg((const double2 *)&rec[ch[k]].value);
+      }
+      double st = 0, weight = 0, x = 0, y = 0;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        if (ch[k] == NONE) continue;
+        double v = cvw[k].x;
         double w = fabs(v);
         if (w > 0) {
           st += v;
           weight += w;
-          x += w * ld_cg(&cells[ch].x);
-          y += w * ld_cg(&cells[ch].y);
+          x += w * cxy[k].x;
+          y += w * cxy[k].y;
         }
       }
       cx = x / weight;
@@ -234,19 +252,22 @@ __global__ void k_collide_prep(Cell *cells, const uint32_t *parent, const uint8_
         }
         continue;
       }
-      Cell *pc = &cells[p];
       const Climb next = climb_up(parent, pnch, p);
-      __threadfence();
-      if (atomicAdd(&counter[p], 1u) != up.nch - 1) break;
-      __threadfence();
+      uint32_t ch[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) ch[k] = cells[p].child[k];
+      if (arrive_acq_rel(&counter[p]) != up.nch - 1) break;
+      double cr4[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) cr4[k] = ch[k] == NONE ? 0.0 : ld_cg(&cells[ch[k]].r);
       double r = 0;
+#pragma unroll
       for (int k = 0; k < 4; ++k) {
-        uint32_t ch = pc->child[k];
-        if (ch == NONE) continue;
-        double v = ld_cg(&cells[ch].r);
+        if (ch[k] == NONE) continue;
+        double v = cr4[k];
         if (v > r) r = v;
       }
-      pc->r = r;
+      cells[p].r = r;
       cr = r;
       up = next;
     }
@@ -1325,6 +1346,98 @@ __global__ void k_csum_walk(const double *x, const double *y, CsumGeom g, const 
   }
 }
 
+// Small node counts: the two serial sums themselves, one warp on one SM
+// (lane 0 x, lane 1 y, in lockstep: one dependent add per value), the values
+// staged into shared memory by bulk copies. At 50k values this is ~0.27 ms
+// and overlaps the forces entirely, where the record pipeline above spreads
+// over many SMs and launches and, on a running sum that keeps crossing zero
+// (short stretches), walks nearly as many records as values.
+constexpr uint32_t CSUM_SERIAL_MAX = 1u << 16;
+constexpr unsigned CSUM_TILE = 1024;  // values per copy and axis (8 KB)
+constexpr unsigned CSUM_STAGES = 4;
+constexpr size_t CSUM_SERIAL_SMEM = 2ull * CSUM_STAGES * CSUM_TILE * sizeof(double);
+
+// stamps as k_csum_walk's (5-7 zero: no records).
+__global__ void __launch_bounds__(32) k_csum_serial(const double *x, const double *y, uint32_t n,
+                                                    double *out, uint32_t *status,
+                                                    unsigned long long *stamps) {
+  extern __shared__ __align__(128) unsigned char csum_smem[];
+  __shared__ __align__(8) uint64_t bar[CSUM_STAGES];
+  double *buf = reinterpret_cast<double *>(csum_smem);  // [stage][axis][CSUM_TILE]
+  const unsigned lane = threadIdx.x;
+  if (lane == 0) {
+    stamps[0] = stamps[1] = stamps[2] = gtimer_ns();
+    for (unsigned q = 0; q < CSUM_STAGES; ++q)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar[q])) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncwarp();
+  const uint32_t nt = (n + CSUM_TILE - 1) / CSUM_TILE;
+  // tile t: its even-length head by two bulk copies (sizes in 16-byte
+  // units), an odd last value by a plain load
+  auto issue = [&](uint32_t t) {
+    const uint32_t k0 = t * CSUM_TILE, m = min(CSUM_TILE, n - k0), mb = m & ~1u;
+    uint64_t *b = &bar[t % CSUM_STAGES];
+    double *d = buf + (size_t)(t % CSUM_STAGES) * 2 * CSUM_TILE;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(b)),
+                 "r"(mb * 16u)
+                 : "memory");
+    if (mb) {
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+              smem_addr(d)),
+          "l"(x + k0), "r"(mb * 8u), "r"(smem_addr(b))
+          : "memory");
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+              smem_addr(d + CSUM_TILE)),
+          "l"(y + k0), "r"(mb * 8u), "r"(smem_addr(b))
+          : "memory");
+    }
+  };
+  if (lane == 0)
+    for (uint32_t t = 0; t < CSUM_STAGES && t < nt; ++t) issue(t);
+  __syncwarp();
+  const double *v = lane == 1 ? y : x;
+  double s = 0;
+  bool ok = true;
+  uint32_t t = 0;
+  for (; t < nt; ++t) {
+    bool w = true;
+    if (lane < 2) w = mbar_wait(&bar[t % CSUM_STAGES], (t / CSUM_STAGES) & 1u);
+    if (!__all_sync(0xffffffffu, w)) {
+      ok = false;
+      break;
+    }
+    const uint32_t k0 = t * CSUM_TILE, m = min(CSUM_TILE, n - k0), mb = m & ~1u;
+    if (lane < 2) {
+      const double *d = buf + ((size_t)(t % CSUM_STAGES) * 2 + lane) * CSUM_TILE;
+      if (mb == CSUM_TILE) {
+#pragma unroll 16
+        for (uint32_t k = 0; k < CSUM_TILE; ++k) s += d[k];
+      } else {
+        for (uint32_t k = 0; k < mb; ++k) s += d[k];
+      }
+      if (mb < m) s += v[k0 + mb];
+    }
+    // the stage is refilled after both lanes have added its values
+    __syncwarp();
+    if (lane == 0 && t + CSUM_STAGES < nt) issue(t + CSUM_STAGES);
+  }
+  // every copy in flight lands before the block exits
+  if (lane == 0)
+    for (uint32_t q = t; q < nt && q < t + CSUM_STAGES; ++q)
+      mbar_wait(&bar[q % CSUM_STAGES], (q / CSUM_STAGES) & 1u);
+  if (lane < 2) {
+    out[lane] = s;
+    stamps[3 + lane] = gtimer_ns();
+  }
+  if (lane == 0) {
+    stamps[5] = stamps[6] = stamps[7] = 0;
+    if (!ok) atomicOr(status, ST_WAIT_TIMEOUT);
+  }
+}
+
 __global__ void k_center_apply(double *x, double *y, uint32_t n, const double *sums, double cx,
                                double cy, double strength) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1344,6 +1457,16 @@ void set_status(uint32_t *status, uint32_t bits, cudaStream_t st) {
 
 void center_sum(const NodeArrays &a, ForceScratch &s, uint32_t *status, cudaStream_t st) {
   if (a.n == 0) return;
+  if (a.n <= CSUM_SERIAL_MAX && ((uintptr_t)a.x & 15) == 0 && ((uintptr_t)a.y & 15) == 0) {
+    static bool sattr = [] {
+      return cudaFuncSetAttribute(k_csum_serial, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)CSUM_SERIAL_SMEM) == cudaSuccess;
+    }();
+    D3_LAUNCH(k_csum_serial, 1, 32, CSUM_SERIAL_SMEM, st)(a.x, a.y, a.n, s.center, status,
+                                                          s.csum_stamps);
+    if (!sattr || cudaGetLastError() != cudaSuccess) set_status(status, ST_CENTER_RECORDS, st);
+    return;
+  }
   static bool attr = [] {
     return cudaFuncSetAttribute(k_csum_walk, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)CSUM_WALK_SMEM) == cudaSuccess;

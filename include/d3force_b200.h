@@ -154,9 +154,10 @@ double sim_last_tick_ms(uint32_t h);
  *     turns / check per attempt), 19 of its first attempt's access-list
  *     build (part of 13), 28 its turn waits that gave up (0 unless it
  *     failed);
- *   22 / 23 microseconds of the last center sum's exact x / y walks, 24 its
- *     x walk's record batches rerun with their entry tests, 25 stretches
- *     added one by one, 26 records in all;
+ *   22 / 23 microseconds of the last center sum's exact x / y walks (the
+ *     plain serial sums up to 65,536 nodes), 24 its x walk's record batches
+ *     rerun with their entry tests, 25 stretches added one by one, 26
+ *     records in all (24-26 are 0 after the serial sums);
  *   27 host milliseconds the last sim_tick spent queueing work;
  *   30-37 microseconds of the last tree build's phases (box, keys, sort,
  *     runs, cell counts, their scan, cell owners, the cells);

@@ -21,11 +21,18 @@ def _center_only(xs, ys):
 
 
 @pytest.mark.parametrize("case", ["walk", "offset", "ties", "tiny_huge", "zeros_nan", "large",
-                                  "centered_1m"])
+                                  "centered_1m", "one", "odd_tail", "serial_max", "records_min"])
 def test_gpu_center_sum_bitwise(ocore, gcore, case):
+    """Up to 65,536 nodes the sums run serially on one warp (bulk-copied
+    tiles of 1,024 values, an odd last value loaded on its own); above that,
+    the parallel record pipeline."""
     rng = np.random.default_rng(5)
     n = 50000
-    if case == "walk":
+    if case in ("one", "odd_tail", "serial_max", "records_min"):
+        n = {"one": 1, "odd_tail": 3073, "serial_max": 65536, "records_min": 65537}[case]
+        xs = rng.normal(0, 2500, n)
+        ys = 1e3 + rng.normal(0, 1, n)
+    elif case == "walk":
         xs = rng.normal(0, 2500, n)
         ys = rng.normal(0, 2500, n)
     elif case == "offset":

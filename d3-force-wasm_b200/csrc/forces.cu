@@ -4,6 +4,7 @@
 // built with -fmad=false). Traversals are stackless: cells are in d3's visit
 // preorder, so "descend" is c + 1 and "do not descend" is skip[c].
 #include <climits>
+#include <cstdlib>
 #include <vector>
 
 #include <cooperative_groups.h>
@@ -823,7 +824,13 @@ void link_exact(const NodeArrays &a, const LinkArrays &l, const LinkPlan &plan, 
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_link_flow, 256, 0);
-    g_link_blocks = sms * (per >= 2 ? 2 : 1);
+    // blocks per SM: at most 2, or D3_LINK_BLOCKS_PER_SM (1 .. occupancy)
+    int want = per >= 2 ? 2 : 1;
+    if (const char *e = getenv("D3_LINK_BLOCKS_PER_SM")) {
+      const int v = atoi(e);
+      if (v >= 1 && v <= per) want = v;
+    }
+    g_link_blocks = sms * want;
   }
   {
     LinkFlowArgs c;

@@ -16,6 +16,8 @@
 //      stable midpoint partition runs serially per group (tree.zig:449-479).
 #include <cooperative_groups.h>
 
+#include <cstdlib>
+
 #include "tree.cuh"
 
 namespace cg = cooperative_groups;
@@ -961,8 +963,13 @@ void tree_build_shifted(TreeDev &t, const double *xs, const double *ys, const do
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_tree_build, TB_THREADS, 0);
-    per = per > 2 ? 2 : per;
-    g_tree_blocks = sms * (per > 0 ? per : 1);
+    // blocks per SM: at most 2, or D3_TREE_BLOCKS_PER_SM (1 .. occupancy)
+    int want = per > 2 ? 2 : per;
+    if (const char *e = getenv("D3_TREE_BLOCKS_PER_SM")) {
+      const int v = atoi(e);
+      if (v >= 1 && v <= per) want = v;
+    }
+    g_tree_blocks = sms * (want > 0 ? want : 1);
     if (g_tree_blocks > (int)TREE_GRID_MAX) g_tree_blocks = TREE_GRID_MAX;
   }
   TreeBuildArgs a;

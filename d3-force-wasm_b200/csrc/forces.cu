@@ -214,63 +214,32 @@ __global__ void k_mb_accumulate(Cell *cells, const uint32_t *parent, const uint8
 }
 
 // collide.zig:117-129 (prepare): leaf radius of its head, internal the largest
-// child radius (strict >, from 0).
-__global__ void k_collide_prep(Cell *cells, const uint32_t *parent, const uint8_t *pnch,
-                               uint32_t *counter, const uint32_t *perm, const double *radii,
-                               const uint32_t *info) {
+// child radius (strict >, from 0). The internal rule makes a cell's radius
+// max(+0, the positive radii of the leaf heads below it): a maximum, exact in
+// any order. So no cell waits for its children: the tree build leaves every
+// radius +0, each leaf with a positive radius raises its ancestors by 64-bit
+// atomic maxima on the radius bits (the bit order of positive doubles is their
+// numeric order), and stops at the first ancestor that already holds at least
+// as much (whoever raised that one goes on from there). NaN, negative and zero
+// leaf radii raise nothing, as in the strict comparison from 0.
+__global__ void k_collide_prep(Cell *cells, const uint32_t *parent, const uint32_t *perm,
+                               const double *radii, const uint32_t *info) {
   const uint32_t len = info[1];
   for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < len; c += gridDim.x * blockDim.x) {
     Cell *q = &cells[c];
     if (!is_leaf(*q)) continue;
-    double cr = radii[perm[q->first + q->count - 1]];
+    const double cr = radii[perm[q->first + q->count - 1]];
     q->r = cr;
-    Climb up = climb_up(parent, pnch, c);
-    for (;;) {
-      const uint32_t p = up.p;
-      if (p == NONE) break;
-      if (up.nch == 1) {
-        // a run of only children (as in k_mb_accumulate), 8 levels at a time
-        uint8_t pk[8];
-#pragma unroll
-        for (int t = 0; t < 8; ++t) pk[t] = (uint32_t)t <= p ? pnch[p - t] : 0;
-        bool out = false;
-#pragma unroll
-        for (int t = 0; t < 8; ++t) {
-          const uint32_t x = p - t;
-          double r = 0;
-          if (cr > r) r = cr;
-          cells[x].r = r;
-          cr = r;
-          if (pk[t] != 1) {
-            up = climb_up(parent, pnch, x);
-            out = true;
-            break;
-          }
-        }
-        if (!out) {
-          up.p = p - 8;
-          up.nch = 1;
-        }
-        continue;
-      }
-      const Climb next = climb_up(parent, pnch, p);
-      uint32_t ch[4];
-#pragma unroll
-      for (int k = 0; k < 4; ++k) ch[k] = cells[p].child[k];
-      if (arrive_acq_rel(&counter[p]) != up.nch - 1) break;
-      double cr4[4];
-#pragma unroll
-      for (int k = 0; k < 4; ++k) cr4[k] = ch[k] == NONE ? 0.0 : ld_cg(&cells[ch[k]].r);
-      double r = 0;
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        if (ch[k] == NONE) continue;
-        double v = cr4[k];
-        if (v > r) r = v;
-      }
-      cells[p].r = r;
-      cr = r;
-      up = next;
+    if (!(cr > 0)) continue;
+    const unsigned long long bits = (unsigned long long)__double_as_longlong(cr);
+    uint32_t p = parent[c];
+    while (p != NONE) {
+      // the next link is static: loaded alongside the maximum
+      const uint32_t pp = parent[p];
+      const unsigned long long old =
+          atomicMax(reinterpret_cast<unsigned long long *>(&cells[p].r), bits);
+      if (old >= bits) break;
+      p = pp;
     }
   }
 }
@@ -986,8 +955,7 @@ void collide_setup(TreeDev &t, const NodeArrays &a, const double *radii, uint32_
   if (n == 0) return;
   unsigned cb, ct;
   climb_grid(cb, ct, t.cells_cap);
-  D3_LAUNCH(k_collide_prep, cb, ct, 0, st)(t.cells, t.parent, t.pnch, t.counter, t.perm, radii,
-                                    t.info);
+  D3_LAUNCH(k_collide_prep, cb, ct, 0, st)(t.cells, t.parent, t.perm, radii, t.info);
 }
 
 void collide_serial(TreeDev &t, const NodeArrays &a, const double *radii, double strength, Rng *rng,

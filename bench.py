@@ -293,6 +293,12 @@ def run_ours(args, pkg, sc):
     e2e_ms = max_over_ranks(sum(e2e) / len(e2e), world)
     stats = {"collide_depth": core.sim_stat(h, 0), "collide_attempts": core.sim_stat(h, 1),
              "collide_serial_fallback": core.sim_stat(h, 2), "link_levels": core.sim_stat(h, 4)}
+    # the last tick's collide pass and collide tree build, from the kernels'
+    # own globaltimer stamps (microseconds)
+    stats["collide_phases_us"] = {"guess": core.sim_stat(h, 12), "access_lists": core.sim_stat(h, 19),
+                                  "turns": core.sim_stat(h, 13), "check": core.sim_stat(h, 14)}
+    stats["tree_phases_us"] = {name: core.sim_stat(h, 30 + k) for k, name in enumerate(
+        ["box", "keys", "sort", "runs", "cell_counts", "scan", "owners", "cells"])}
     sim.close()
     if rank != 0:
         if world > 1:

@@ -53,7 +53,9 @@ void scratch_free(ForceScratch &s) {
 }
 
 // ---------------------------------------------------------------------------
-// Bottom-up passes (visitAfter): the last child to finish computes its parent.
+// Bottom-up passes (visitAfter). The many-body accumulation: the last child to
+// finish computes its parent. The collide radii: a maximum, so each leaf
+// raises its ancestors directly.
 // ---------------------------------------------------------------------------
 
 __device__ inline double ld_cg(const double *p) { return __ldcg(p); }
@@ -67,7 +69,7 @@ struct alignas(64) MRec {
 };
 static_assert(sizeof(MRec) == 64, "record layout");
 
-// A parent's step of the bottom-up passes: its children are the ones listed
+// A parent's step of the accumulation: its children are the ones listed
 // in its cell (several), or only the child just finished (one: no counter,
 // and the child's values are still in registers).
 struct Climb {

@@ -1165,6 +1165,22 @@ double sim_stat(uint32_t h, uint32_t which) {
   }
 }
 
+int32_t sim_find(uint32_t h, double x, double y, double radius, uint32_t *index) {
+  DSim *s = get_sim(h);
+  if (!s) return D3_BAD_HANDLE;
+  if (!index) return D3_BAD_ARGUMENT;
+  *index = NONE;
+  if (s->n == 0) return D3_OK;
+  if (s->sync_mode == D3_SYNC_PER_CALL) sync_in_impl(s);
+  // d3 squares the radius it is given (a missing one is Infinity)
+  find_closest(nodes_of(s), x, y, radius * radius, s->d_words + 15, s->stream);
+  cudaMemcpyAsync(s->h_words + 30, s->d_words + 15, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                  s->stream);
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess) return D3_WORKER_FAILED;
+  *index = s->h_words[30];
+  return D3_OK;
+}
+
 double sim_last_tick_ms(uint32_t h) {
   DSim *s = get_sim(h);
   return s ? s->last_ms : 0;

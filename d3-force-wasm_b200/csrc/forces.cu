@@ -1471,6 +1471,54 @@ void center_apply(const NodeArrays &a, double cx, double cy, double strength, Fo
   D3_LAUNCH(k_center_apply, blocks_for(a.n, 256), 256, 0, st)(a.x, a.y, a.n, s.center, cx, cy, strength);
 }
 
+// simulation.js:157-178 (find). The serial scan keeps the first node whose d2
+// is strictly below its best so far (starting at radius^2): the lowest index
+// of the least d2 below radius^2. One block: each thread runs that scan over
+// its own nodes (ascending indices), then the block keeps the least (d2,
+// index) pair. A NaN d2 never passes the strict test.
+constexpr unsigned FIND_THREADS = 1024;
+
+__device__ inline void find_merge(double &d, uint32_t &i, double d2, uint32_t i2) {
+  if (i2 != NONE && (i == NONE || d2 < d || (d2 == d && i2 < i))) {
+    d = d2;
+    i = i2;
+  }
+}
+
+__global__ void __launch_bounds__(FIND_THREADS) k_find(const double *xs, const double *ys, uint32_t n,
+                                                       double x, double y, double r2,
+                                                       uint32_t *out) {
+  __shared__ double sd[FIND_THREADS / 32];
+  __shared__ uint32_t si[FIND_THREADS / 32];
+  double best = r2;
+  uint32_t bi = NONE;
+  for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) {
+    const double dx = x - xs[k], dy = y - ys[k];
+    const double d2 = dx * dx + dy * dy;
+    if (d2 < best) {
+      best = d2;
+      bi = k;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1)
+    find_merge(best, bi, __shfl_xor_sync(0xffffffffu, best, o), __shfl_xor_sync(0xffffffffu, bi, o));
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    sd[warp] = best;
+    si[warp] = bi;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (unsigned w = 1; w < blockDim.x / 32; ++w) find_merge(best, bi, sd[w], si[w]);
+    *out = bi;
+  }
+}
+
+void find_closest(const NodeArrays &a, double x, double y, double r2, uint32_t *out,
+                  cudaStream_t st) {
+  D3_LAUNCH(k_find, 1, FIND_THREADS, 0, st)(a.x, a.y, a.n, x, y, r2, out);
+}
+
 // simple.zig:51-62
 __global__ void k_axis(double *pos, double *v, const double *strength, const double *target,
                        double alpha, uint32_t n) {

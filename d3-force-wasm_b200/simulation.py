@@ -9,6 +9,7 @@ files; nodes are a `Nodes` structure of f64 arrays instead of JS objects, with
 NaN standing for a missing (null / undefined) field.
 """
 
+import ctypes
 import math
 
 import numpy as np
@@ -530,7 +531,7 @@ class Simulation:
         with a randomSource() callback, one force_run per force per tick."""
         if not (0 < iterations):
             return self
-        if self._random is None and self.engine_ticks:
+        if self._random is None and self.engine_ticks and not self._custom():
             self.device_begin()
             try:
                 self.device_ticks(int(iterations))
@@ -544,18 +545,54 @@ class Simulation:
             for _ in range(int(iterations)):
                 self._alpha += (self._alpha_target - self._alpha) * self._alpha_decay
                 for f in self._forces.values():
-                    f(self._alpha)
+                    if isinstance(f, Force):
+                        f(self._alpha)
+                        continue
+                    # simulation.js:66-76: a custom force sees the node table
+                    # through a copy-out and copy-in around it
+                    ctx.live = False
+                    ctx.copy_out(self._nodes)
+                    try:
+                        f(self._alpha)
+                    finally:
+                        ctx.copy_in(self._nodes)
+                        ctx.live = True
                 C.check(self.core.sim_integrate(ctx.h, self._velocity_decay))
         finally:
             ctx.live = False
             ctx.copy_out(self._nodes)
         return self
 
+    def _custom(self):
+        """Whether a force other than the core's is registered."""
+        return any(not isinstance(f, Force) for f in self._forces.values())
+
+    def _draw(self):
+        """One draw from the simulation's random source, as the reference hands
+        it to a custom force's initialize(nodes, random): the randomSource()
+        callable, else d3's LCG, whose state the core keeps (so core jiggles
+        and custom forces share one stream, as in simulation.js:22)."""
+        if self._random is not None:
+            return self._random()
+        h = self.ctx.h
+        s = (1664525 * int(self.core.sim_get_lcg(h)) + 1013904223) % 4294967296
+        C.check(self.core.sim_set_lcg(h, s))
+        return s / 4294967296
+
+    def _initialize_force(self, f):
+        """simulation.js:107-110: a core force binds its slots; a custom force
+        gets initialize(nodes, random) if it has one."""
+        if isinstance(f, Force):
+            f.initialize(self._nodes, self.ctx)
+        elif hasattr(f, "initialize"):
+            f.initialize(self._nodes, self._draw)
+        return f
+
     def run(self, ticks):
         """`ticks` ticks in one engine call (sim_tick); bitwise the same as
         `ticks` calls of tick(1). Needs the device LCG random source; with a
         randomSource() callback it falls back to tick(ticks)."""
-        if self._random is not None:
+        if self._random is not None or self._custom():
             return self.tick(ticks)
         self.device_begin()
         self.device_ticks(ticks)
@@ -564,7 +601,10 @@ class Simulation:
 
     def device_begin(self):
         """Node state to the device and every force's scalars pushed, so that
-        device_ticks() can run ticks with no host transfer."""
+        device_ticks() can run ticks with no host transfer. Core forces only: a
+        custom force runs through tick()."""
+        if self._custom():
+            raise ValueError("a custom force runs through tick(), not the engine's sim_tick")
         ctx = self.ctx
         ctx.copy_in(self._nodes)
         for f in self._forces.values():
@@ -598,7 +638,7 @@ class Simulation:
         self._nodes = nodes
         self._initialize_nodes()
         for f in self._forces.values():
-            f.initialize(self._nodes, self.ctx)
+            self._initialize_force(f)
         return self
 
     def alpha(self, a=None):
@@ -638,7 +678,7 @@ class Simulation:
         self._random = fn
         self.ctx.set_random(fn)
         for f in self._forces.values():
-            f.initialize(self._nodes, self.ctx)
+            self._initialize_force(f)
         return self
 
     def force(self, name, f="__get__"):
@@ -647,8 +687,7 @@ class Simulation:
         if f is None:
             self._forces.pop(name, None)
         else:
-            f.initialize(self._nodes, self.ctx)
-            self._forces[name] = f
+            self._forces[name] = self._initialize_force(f)
         return self
 
     def precision(self, mode=None, order=None, opening=None):
@@ -667,16 +706,15 @@ class Simulation:
         return self
 
     def find(self, x, y, radius=None):
-        """simulation.js:157-178 (host side, on the current node table)."""
-        nd = self._nodes
-        r2 = math.inf if radius is None else radius * radius
-        closest = None
-        for i in range(nd.n):
-            dx, dy = x - nd.x[i], y - nd.y[i]
-            d2 = dx * dx + dy * dy
-            if d2 < r2:
-                closest, r2 = i, d2
-        return closest
+        """simulation.js:157-178 through the core (sim_find, a reduction on
+        the device): the index of the closest node with d2 < radius^2 (the
+        lowest index among equal d2), or None."""
+        ctx = self.ctx
+        ctx.copy_in(self._nodes)
+        out = C._U32(0)
+        r = math.inf if radius is None else float(radius)
+        C.check(self.core.sim_find(ctx.h, float(x), float(y), r, ctypes.byref(out)))
+        return None if out.value == 0xFFFFFFFF else int(out.value)
 
     def close(self):
         self.ctx.close()

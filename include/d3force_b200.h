@@ -140,6 +140,15 @@ int32_t sim_tick(uint32_t h, uint32_t ticks, double *alpha, double alpha_target,
 /* Milliseconds of device time of the last sim_tick call (CUDA events). */
 double sim_last_tick_ms(uint32_t h);
 
+/* simulation.js:157-178 (`find`) on the device copy of the positions (after
+ * sim_sync_in, or uploaded first in D3_SYNC_PER_CALL mode): the node closest
+ * to (x, y) among those with d2 = dx * dx + dy * dy < radius * radius (pass
+ * INFINITY for d3's missing radius). d3's serial scan replaces its pick only
+ * on a strictly smaller d2, so among equal d2 the lowest index wins; a NaN d2
+ * never matches. *index = that node, or 0xffffffff when none matches.
+ * Synchronises. */
+int32_t sim_find(uint32_t h, double x, double y, double radius, uint32_t *index);
+
 /* Diagnostics of the last force runs (synchronises):
  *   0 the longest chain of dependent turns of the last parallel exact
  *     collide, 1 its attempts, 2 1 if it fell back to the serial loop;

@@ -1895,6 +1895,22 @@ double sim_stat(uint32_t h, uint32_t which) {
   return 0;
 }
 
+/* src/simulation.js:157-178 (find): radius *= radius (a missing radius is
+ * Infinity), then the serial scan keeping each strictly closer node. */
+int32_t sim_find(uint32_t h, double x, double y, double radius, uint32_t *index) {
+  Sim *s = get_sim(h);
+  if (!s) return D3_BAD_HANDLE;
+  if (!index) return D3_BAD_ARGUMENT;
+  double r2 = radius * radius;
+  uint32_t closest = NONE;
+  for (uint32_t i = 0; i < s->n; ++i) {
+    double dx = x - s->x[i], dy = y - s->y[i], d2 = dx * dx + dy * dy;
+    if (d2 < r2) closest = i, r2 = d2;
+  }
+  *index = closest;
+  return D3_OK;
+}
+
 /* The engine's device-wait self test has no CPU meaning: report a bad
  * argument. */
 int32_t sim_selftest_wait(uint32_t h, uint32_t budget_us) {

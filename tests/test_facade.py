@@ -1,0 +1,142 @@
+"""The facade's find and custom forces (simulation.js:49-89, 107-110,
+157-178) on the oracle core: no GPU needed."""
+
+import math
+
+import numpy as np
+import pytest
+
+import helpers as H
+
+pkg = H.pkg
+
+
+def _find_serial(xs, ys, x, y, radius=None):
+    """simulation.js:157-178, statement by statement."""
+    r2 = math.inf if radius is None else radius * radius
+    closest = None
+    for i in range(len(xs)):
+        dx, dy = x - float(xs[i]), y - float(ys[i])
+        d2 = dx * dx + dy * dy
+        if d2 < r2:
+            closest, r2 = i, d2
+    return closest
+
+
+def _find_nodes(n, seed):
+    rng = np.random.default_rng(seed)
+    xs = np.round(rng.uniform(-50, 50, n), 1)  # rounded: many equal distances
+    ys = np.round(rng.uniform(-50, 50, n), 1)
+    xs[::97] = np.nan
+    ys[5::89] = np.nan
+    if n > 10:
+        xs[7], ys[7] = xs[3], ys[3]  # an exact duplicate after a lower index
+    return xs, ys
+
+
+QUERIES = [(0.0, 0.0, None), (12.3, -4.5, None), (12.3, -4.5, 3.0), (100.0, 100.0, 1.0),
+           (0.05, 0.05, 0.0), (-7.0, 7.0, -2.5), (1.0, 1.0, math.nan), (math.nan, 0.0, None),
+           (1e300, 1e300, None), (-20.0, 30.0, math.inf)]
+
+
+@pytest.mark.parametrize("n", [0, 1, 2, 1000])
+def test_find_matches_the_serial_scan(ocore, n):
+    xs, ys = _find_nodes(n, n)
+    nd = pkg.Nodes(n, x=xs, y=ys)
+    sim = pkg.forceSimulation(nd, core=ocore)
+    try:
+        for q in QUERIES + [(xs[3], ys[3], None)] if n > 10 else QUERIES:
+            assert sim.find(*q) == _find_serial(nd.x, nd.y, *q), q
+    finally:
+        sim.close()
+
+
+class _Kick:
+    """A custom force: vx += 1 on every node, recording the alphas it gets."""
+
+    def __init__(self):
+        self.alphas = []
+        self.nodes = None
+        self.draws = []
+
+    def initialize(self, nodes, random):
+        self.nodes = nodes
+        self.draws = [random(), random()]
+
+    def __call__(self, alpha):
+        self.alphas.append(alpha)
+        self.nodes.vx[:] += 1.0
+
+
+def test_custom_force_sees_and_changes_the_node_table(ocore):
+    nd = pkg.Nodes(3, x=[0.0, 10.0, 20.0], y=[0.0, 0.0, 5.0], vx=[0.0] * 3, vy=[0.0] * 3)
+    sim = pkg.forceSimulation(nd, core=ocore)
+    try:
+        kick = _Kick()
+        sim.force("kick", kick)
+        sim.tick()
+        # integrate: vx = (0 + 1) * 0.6, x += vx
+        assert list(nd.vx) == [0.6, 0.6, 0.6]
+        assert list(nd.x) == [0.6, 10.6, 20.6]
+        assert list(nd.y) == [0.0, 0.0, 5.0]
+        a1 = 1 + (0 - 1) * (1 - math.pow(0.001, 1 / 300))
+        assert kick.alphas == [a1]
+        sim.tick(2)
+        assert len(kick.alphas) == 3 and kick.alphas[0] > kick.alphas[1] > kick.alphas[2]
+    finally:
+        sim.close()
+
+
+def test_custom_force_draws_from_the_shared_stream(ocore):
+    """initialize(nodes, random) draws from d3's LCG, whose state the core
+    keeps for its own jiggles (one stream per simulation)."""
+    nd = pkg.Nodes(2, x=[0.0, 1.0], y=[0.0, 1.0])
+    sim = pkg.forceSimulation(nd, core=ocore)
+    try:
+        ref = pkg.d3_lcg(1)
+        kick = _Kick()
+        sim.force("kick", kick)
+        assert kick.draws == [ref(), ref()]
+        nxt = (1664525 * ocore.sim_get_lcg(sim.ctx.h) + 1013904223) % 4294967296
+        assert nxt / 4294967296 == ref()
+    finally:
+        sim.close()
+
+
+def _graph(core, custom):
+    nodes, src, tgt = H.scenarios.exact_graph(400, 800, 0.01, 0.01, 0.01, 3)
+    sim = pkg.forceSimulation(nodes, core=core)
+    sim.force("charge", pkg.forceManyBody())
+    if custom is not None:
+        sim.force("custom", custom)
+    sim.force("link", pkg.forceLink(src, tgt))
+    sim.force("collide", pkg.forceCollide(4))
+    sim.force("center", pkg.forceCenter(0, 0))
+    return nodes, sim
+
+
+def test_identity_custom_force_changes_nothing(ocore):
+    """A custom force that does nothing: the copy-out / copy-in around it
+    leaves the ticks bit-identical to the run without it."""
+    na, sa = _graph(ocore, None)
+    nb, sb = _graph(ocore, lambda alpha: None)
+    try:
+        sa.tick(5)
+        sb.tick(5)
+        for f in ("x", "y", "vx", "vy"):
+            assert np.array_equal(np.asarray(getattr(na, f)).view(np.uint64),
+                                  np.asarray(getattr(nb, f)).view(np.uint64)), f
+        assert sa.alpha() == sb.alpha()
+    finally:
+        sa.close()
+        sb.close()
+
+
+def test_engine_path_refuses_a_custom_force(ocore):
+    nodes, sim = _graph(ocore, lambda alpha: None)
+    try:
+        with pytest.raises(ValueError):
+            sim.device_begin()
+        sim.run(2)  # run() falls back to tick() with a custom force
+    finally:
+        sim.close()

@@ -337,7 +337,7 @@ def run_ours(args, pkg, sc):
         "config": {"workload": WORKLOAD_NAME, "n": n, "m": WORKLOAD["m"],
                    "parallelism": "replicas" if world > 1 else "single",
                    "l2": "flushed between timed ticks (256 MB write)", "bit_exact": True},
-        "e2e": {"value": round(e2e_ms, 4), "unit": "ms/tick", "h2d_bytes_per_step": 49 * n,
+        "e2e": {"value": round(e2e_ms, 4), "unit": "ms/tick", "h2d_bytes_per_step": 48 * n,
                 "d2h_bytes_per_step": 32 * n},
         "gpu_launches": launches,
         "phase_ms_per_tick": {k: round(v, 4) for k, v in per_tick_ms.items()},

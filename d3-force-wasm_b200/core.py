@@ -76,6 +76,7 @@ _SIGNATURES = {
     "sim_get_lcg": (_U32, [_U32]),
     "sim_set_sync": (_I32, [_U32, _U32]),
     "sim_sync_in": (_I32, [_U32]),
+    "sim_set_fixed_source": (_I32, [_U32, _U32]),
     "sim_sync_out": (_I32, [_U32]),
     "sim_tick": (_I32, [_U32, _U32, ctypes.POINTER(_F64), _F64, _F64, _F64,
                         ctypes.POINTER(_U32), _U32]),

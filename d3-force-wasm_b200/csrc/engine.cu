@@ -80,6 +80,7 @@ struct DSim {
   bool rest_pending = false;
   bool settle_after_accumulate = false;  // sim_tick: settle in the first many-body force
   uint32_t sync_mode = D3_SYNC_PER_CALL;
+  bool fixed_from_f = false;  // sim_set_fixed_source
   // tree mirrors (tree_info)
   Cell *h_cells = nullptr;
   uint32_t h_cells_cap = 0;
@@ -308,7 +309,8 @@ int sync_in_impl(DSim *s, bool defer = false) {
     cudaMemcpyAsync(s->d_vy, s->h_vy, n * 8, cudaMemcpyHostToDevice, up);
     cudaMemcpyAsync(s->d_fx, s->h_fx, n * 8, cudaMemcpyHostToDevice, up);
     cudaMemcpyAsync(s->d_fy, s->h_fy, n * 8, cudaMemcpyHostToDevice, up);
-    cudaMemcpyAsync(s->d_fixed, s->h_fixed, n, cudaMemcpyHostToDevice, up);
+    if (s->fixed_from_f) fixed_from_f(s->d_fx, s->d_fy, s->d_fixed, (uint32_t)n, up);
+    else cudaMemcpyAsync(s->d_fixed, s->h_fixed, n, cudaMemcpyHostToDevice, up);
     cudaEventRecord(s->ev_rest, up);
     s->rest_pending = true;
     if (!defer) settle(s);
@@ -934,6 +936,14 @@ uint32_t sim_get_lcg(uint32_t h) {
   cudaMemcpyAsync(s->h_rng, s->d_rng, sizeof(Rng), cudaMemcpyDeviceToHost, s->stream);
   cudaStreamSynchronize(s->stream);
   return s->h_rng->lcg;
+}
+
+int32_t sim_set_fixed_source(uint32_t h, uint32_t from_f) {
+  DSim *s = get_sim(h);
+  if (!s) return D3_BAD_HANDLE;
+  if (from_f > 1) return D3_BAD_ARGUMENT;
+  s->fixed_from_f = from_f != 0;
+  return D3_OK;
 }
 
 int32_t sim_set_sync(uint32_t h, uint32_t mode) {

@@ -1471,6 +1471,20 @@ void center_apply(const NodeArrays &a, double cx, double cy, double strength, Fo
   D3_LAUNCH(k_center_apply, blocks_for(a.n, 256), 256, 0, st)(a.x, a.y, a.n, s.center, cx, cy, strength);
 }
 
+// src/core.js:130 on the device: fixed = (fx set) | (fy set) << 1, a missing
+// value being NaN.
+__global__ void k_fixed_from_f(const double *fx, const double *fy, uint8_t *fixed, uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double a = fx[i], b = fy[i];
+  fixed[i] = (uint8_t)((a == a ? 1u : 0u) | (b == b ? 2u : 0u));
+}
+
+void fixed_from_f(const double *fx, const double *fy, uint8_t *fixed, uint32_t n, cudaStream_t st) {
+  if (n == 0) return;
+  D3_LAUNCH(k_fixed_from_f, blocks_for(n, 256), 256, 0, st)(fx, fy, fixed, n);
+}
+
 // simulation.js:157-178 (find). The serial scan keeps the first node whose d2
 // is strictly below its best so far (starting at radius^2): the lowest index
 // of the least d2 below radius^2. One block: each thread runs that scan over

@@ -137,6 +137,8 @@ int collide_parallel(TreeDev &t, const NodeArrays &a, const double *radii, doubl
 // into s.center, then the shift. The sums only read positions, so the caller
 // may issue them early on another stream.
 void center_sum(const NodeArrays &a, ForceScratch &s, uint32_t *status, cudaStream_t st);
+// src/core.js:130: the fixed bits from fx / fy (NaN = not set).
+void fixed_from_f(const double *fx, const double *fy, uint8_t *fixed, uint32_t n, cudaStream_t st);
 // simulation.js:157-178: the closest node below radius^2 (r2) into *out.
 void find_closest(const NodeArrays &a, double x, double y, double r2, uint32_t *out,
                   cudaStream_t st);

@@ -59,11 +59,12 @@ class Context:
             raise C.CoreError(C.OUT_OF_MEMORY)
         self.n = 0
         C.check(core.sim_set_sync(self.h, C.SYNC_EXPLICIT))
+        # src/core.js:130's fixed bits, (fx set) | (fy set) << 1, are derived
+        # from fx / fy (NaN = not set) by the engine at each upload
+        C.check(core.sim_set_fixed_source(self.h, 1))
         self.live = False
         self._nodes = None  # the node table whose arrays are the mirrors
         self._views = ()
-        self._fixed = None  # the fixed-bits mirror and a scratch row (while n holds)
-        self._fixed_tmp = None
         self.precision = None  # None = exact; {"order", "opening"} = fast
         self.host_random = None  # callback for randomSource(); None = device LCG
         self._cb = None
@@ -74,7 +75,6 @@ class Context:
     def resize(self, n):
         if n != self.n:
             self.detach()  # the mirrors move
-            self._fixed = None
             C.check(self.core.sim_set_node_count(self.h, n))
             self.n = n
 
@@ -95,22 +95,12 @@ class Context:
                 if getattr(nodes, f) is v:
                     setattr(nodes, f, np.array(v, np.float64))
 
-    def _write_fixed(self, nodes, n):
-        """src/core.js:130 straight into the pinned mirror."""
-        if self._fixed is None or len(self._fixed) != n:
-            self._fixed = self.core.u8_view(self.core.sim_ptr(self.h, C.PTR_FIXED), n)
-            self._fixed_tmp = np.empty(n, np.uint8)
-        v, w = self._fixed, self._fixed_tmp
-        np.equal(nodes.fx, nodes.fx, out=v.view(np.bool_))  # 1: fx set
-        np.equal(nodes.fy, nodes.fy, out=w.view(np.bool_))  # 1: fy set
-        np.add(w, w, out=w)
-        np.add(v, w, out=v)
-
     def copy_in(self, nodes):
         """src/core.js:121-131, then one host-to-device sync. The node table's
         x, y, vx, vy, fx, fy become views of the pinned mirrors the first time
         (as the reference's facade views wasm memory), so later ticks copy
-        nothing on the host: only the fixed bits are recomputed."""
+        nothing on the host; the fixed bits (src/core.js:130) are derived from
+        fx / fy on the device."""
         n = len(nodes)
         self.resize(n)
         core, h = self.core, self.h
@@ -123,8 +113,6 @@ class Context:
                 setattr(nodes, f, v)
                 views.append(v)
             self._nodes, self._views = nodes, tuple(views)
-        if n:
-            self._write_fixed(nodes, n)
         C.check(core.sim_sync_in(h))
 
     def copy_out(self, nodes):

@@ -434,6 +434,7 @@ typedef struct {
   uint32_t n, cap;
   double *x, *y, *vx, *vy, *fx, *fy;
   uint8_t *fixed;
+  int fixed_from_f; /* sim_set_fixed_source */
   double *px, *py;
   double *snap;
   uint32_t snap_cap;
@@ -1866,7 +1867,24 @@ int32_t sim_set_sync(uint32_t h, uint32_t mode) {
   (void)mode;
   return get_sim(h) ? D3_OK : D3_BAD_HANDLE;
 }
-int32_t sim_sync_in(uint32_t h) { return get_sim(h) ? D3_OK : D3_BAD_HANDLE; }
+/* The node state is the oracle's own memory: an upload only derives the fixed
+ * bits when asked to (src/core.js:130, NaN = not set). */
+int32_t sim_sync_in(uint32_t h) {
+  Sim *s = get_sim(h);
+  if (!s) return D3_BAD_HANDLE;
+  if (s->fixed_from_f)
+    for (uint32_t i = 0; i < s->n; ++i)
+      s->fixed[i] = (uint8_t)((s->fx[i] == s->fx[i] ? 1 : 0) | (s->fy[i] == s->fy[i] ? 2 : 0));
+  return D3_OK;
+}
+
+int32_t sim_set_fixed_source(uint32_t h, uint32_t from_f) {
+  Sim *s = get_sim(h);
+  if (!s) return D3_BAD_HANDLE;
+  if (from_f > 1) return D3_BAD_ARGUMENT;
+  s->fixed_from_f = from_f != 0;
+  return D3_OK;
+}
 int32_t sim_sync_out(uint32_t h) { return get_sim(h) ? D3_OK : D3_BAD_HANDLE; }
 
 int32_t sim_tick(uint32_t h, uint32_t ticks, double *alpha, double alpha_target, double alpha_decay,

@@ -140,3 +140,26 @@ def test_engine_path_refuses_a_custom_force(ocore):
         sim.run(2)  # run() falls back to tick() with a custom force
     finally:
         sim.close()
+
+
+def test_fixed_bits_from_fx_fy(ocore):
+    """sim_set_fixed_source(h, 1): each upload derives src/core.js:130's bits
+    from fx / fy (NaN = not set); mode 0 keeps the array as written."""
+    C = H.C
+    h = ocore.sim_create()
+    try:
+        assert ocore.sim_set_node_count(h, 4) >= 0
+        fx = ocore.f64_view(ocore.sim_ptr(h, C.PTR_FX), 4)
+        fy = ocore.f64_view(ocore.sim_ptr(h, C.PTR_FY), 4)
+        fixed = ocore.u8_view(ocore.sim_ptr(h, C.PTR_FIXED), 4)
+        fx[:] = [np.nan, 1.0, np.nan, -0.0]
+        fy[:] = [np.nan, np.nan, 2.0, np.inf]
+        fixed[:] = 7
+        assert ocore.sim_sync_in(h) == 0
+        assert list(fixed) == [7, 7, 7, 7]
+        assert ocore.sim_set_fixed_source(h, 2) == C.BAD_ARGUMENT
+        assert ocore.sim_set_fixed_source(h, 1) == 0
+        assert ocore.sim_sync_in(h) == 0
+        assert list(fixed) == [0, 1, 2, 3]
+    finally:
+        ocore.sim_destroy(h)

@@ -128,11 +128,11 @@ int32_t sim_set_sync(uint32_t h, uint32_t mode);
 int32_t sim_sync_in(uint32_t h);
 /* Where the fixed bits come from at each upload of the node state: 0 (the
  * default, the reference core's contract) the fixed array as written; 1
- * derived on the device from fx and fy, fixed = (fx set) | (fy set) << 1 with
- * NaN for a missing value, which is what the facade's copyIn writes
- * (src/core.js:130). In mode 1 the fixed mirror is neither read nor written:
- * a facade that keeps missing values as NaN saves computing and uploading
- * the bits on the host. */
+ * derived on the device from fx and fy by src/core.js:130's rule, fixed =
+ * (fx set) | (fy set) << 1, for a facade that stores a missing fx / fy as
+ * NaN (the Python facade does; the JS copyIn stores null as 0, so it keeps
+ * mode 0). In mode 1 the fixed mirror is neither read nor written, which
+ * saves computing and uploading the bits on the host. */
 int32_t sim_set_fixed_source(uint32_t h, uint32_t from_f);
 /* Device -> host mirrors (x, y, vx, vy). */
 int32_t sim_sync_out(uint32_t h);

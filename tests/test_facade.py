@@ -163,3 +163,21 @@ def test_fixed_bits_from_fx_fy(ocore):
         assert list(fixed) == [0, 1, 2, 3]
     finally:
         ocore.sim_destroy(h)
+
+
+def test_nodes_reinitializes_custom_forces(ocore):
+    """simulation.js:125-127: nodes(_) re-runs every force's initialize with
+    the new table (a custom force's initialize(nodes, random) included)."""
+    nd = pkg.Nodes(2, x=[0.0, 1.0], y=[0.0, 1.0])
+    sim = pkg.forceSimulation(nd, core=ocore)
+    try:
+        kick = _Kick()
+        sim.force("kick", kick)
+        assert kick.nodes is nd
+        nd2 = pkg.Nodes(5)
+        sim.nodes(nd2)
+        assert kick.nodes is nd2 and len(kick.draws) == 2
+        sim.tick()
+        assert np.all(np.asarray(nd2.vx) == 0.6)
+    finally:
+        sim.close()

@@ -268,22 +268,69 @@ class ForceManyBody(Force):
 
 
 class ForceLink(Force):
-    """src/link.js: links as node indices; degree count, bias, default
+    """src/link.js: links as (source, target) sequences, node indices by
+    default or node ids once id() is set; degree count, bias, default
     strength 1 / min(count[source], count[target]), distance 30."""
 
     kind = C.LINK
 
     def __init__(self, source=(), target=()):
         super().__init__()
-        self.source = np.asarray(source, np.int64)
-        self.target = np.asarray(target, np.int64)
+        self._links = (source, target)
+        self._id = None  # link.js:4-6: a node's id is its index
+        self.source, self.target = self._unresolved()
         self._strength = None  # default strength
         self._distance = _constant(30.0)
         self._iterations = 1
         self.count = None
         self.bias = None
 
+    def _resolve(self):
+        """link.js:41-50: with an id accessor, every endpoint is a node id,
+        looked up among id(i) for the nodes (a later node wins a repeated id);
+        an unknown id is an error."""
+        src, tgt = self._links
+        if self._id is None:
+            return np.asarray(src, np.int64), np.asarray(tgt, np.int64)
+        by_id = {self._id(i): i for i in range(len(self.nodes))}
+
+        def find(v):
+            if v not in by_id:
+                raise KeyError("node not found: %r" % (v,))
+            return by_id[v]
+
+        return (np.array([find(v) for v in src], np.int64),
+                np.array([find(v) for v in tgt], np.int64))
+
+    def _unresolved(self):
+        """The endpoints as indices before initialize: as given when they are
+        indices, empty while they are ids awaiting the node table."""
+        try:
+            return np.asarray(self._links[0], np.int64), np.asarray(self._links[1], np.int64)
+        except (TypeError, ValueError):
+            return np.zeros(0, np.int64), np.zeros(0, np.int64)
+
+    def links(self, source=None, target=None):
+        """link.js:101-103: the links as resolved node indices, or new ones
+        (then the force initializes again)."""
+        if source is None and target is None:
+            return self.source, self.target
+        self._links = (source, target)
+        self.source, self.target = self._unresolved()
+        if self.nodes is not None:
+            self._initialize()
+        return self
+
+    def id(self, fn=None):
+        """link.js:105-107: fn(i) -> the id of node i; applies at the next
+        initialize (as in d3)."""
+        if fn is None:
+            return self._id
+        self._id = fn
+        return self
+
     def _initialize(self):
+        self.source, self.target = self._resolve()
         n, m = len(self.nodes), len(self.source)
         src, tgt = self.source, self.target
         count = np.zeros(n, np.int64)
@@ -691,6 +738,18 @@ class Simulation:
                                   "opening": max(1.01, float(opening) if opening else 1.5)}
         else:
             self.ctx.precision = None
+        return self
+
+    def threads(self, k="__get__"):
+        """simulation.js:205-215: the reference's cap on CPU workers per tick.
+        Ticks run on the GPU here: the setter is kept for compatibility and
+        the getter reports 0 workers used (as the reference's inlined core)."""
+        if k == "__get__":
+            return 0
+        v = None if k is None else float(k)
+        # Math.max(0, Math.floor(+k) || 0)
+        self._threads = None if v is None else (0 if v != v else max(0.0, math.floor(v))
+                                                if not math.isinf(v) else max(0.0, v))
         return self
 
     def find(self, x, y, radius=None):

@@ -181,3 +181,64 @@ def test_nodes_reinitializes_custom_forces(ocore):
         assert np.all(np.asarray(nd2.vx) == 0.6)
     finally:
         sim.close()
+
+
+def _linked(core, by_id):
+    n = 60
+    nodes = pkg.Nodes(n)
+    rng = np.random.default_rng(9)
+    src = rng.integers(0, n, 120)
+    tgt = (src + 1 + rng.integers(0, n - 1, 120)) % n
+    sim = pkg.forceSimulation(nodes, core=core)
+    sim.force("charge", pkg.forceManyBody())
+    if by_id:
+        link = pkg.forceLink(["n%d" % v for v in src], ["n%d" % v for v in tgt])
+        link.id(lambda i: "n%d" % i)
+    else:
+        link = pkg.forceLink(src, tgt)
+    sim.force("link", link)
+    return nodes, sim, link, src, tgt
+
+
+def test_link_ids_resolve_like_indices(ocore):
+    """link.js:41-50: endpoints given as node ids through id() give the same
+    links, counts, bias and ticks as the same links given as indices."""
+    na, sa, la, src, tgt = _linked(ocore, False)
+    nb, sb, lb, _, _ = _linked(ocore, True)
+    try:
+        assert np.array_equal(lb.links()[0], src) and np.array_equal(lb.links()[1], tgt)
+        assert np.array_equal(la.bias, lb.bias) and np.array_equal(la.count, lb.count)
+        sa.tick(4)
+        sb.tick(4)
+        for f in ("x", "y", "vx", "vy"):
+            assert np.array_equal(np.asarray(getattr(na, f)).view(np.uint64),
+                                  np.asarray(getattr(nb, f)).view(np.uint64)), f
+    finally:
+        sa.close()
+        sb.close()
+
+
+def test_link_unknown_id_and_new_links(ocore):
+    nd = pkg.Nodes(3)
+    sim = pkg.forceSimulation(nd, core=ocore)
+    try:
+        link = pkg.forceLink(["a"], ["zz"]).id(lambda i: "abc"[i])
+        with pytest.raises(KeyError):
+            sim.force("link", link)
+        link = pkg.forceLink([0], [1])
+        sim.force("link", link)
+        assert list(link.count) == [1, 1, 0]
+        link.links([0, 2, 2], [1, 1, 0])  # initializes again
+        assert list(link.count) == [2, 2, 2]
+        assert list(link.links()[0]) == [0, 2, 2]
+    finally:
+        sim.close()
+
+
+def test_threads_is_accepted(ocore):
+    sim = pkg.forceSimulation(pkg.Nodes(2), core=ocore)
+    try:
+        assert sim.threads(4) is sim and sim.threads(None) is sim
+        assert sim.threads(float("nan")) is sim and sim.threads() == 0
+    finally:
+        sim.close()

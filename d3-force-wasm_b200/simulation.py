@@ -746,10 +746,15 @@ class Simulation:
         the getter reports 0 workers used (as the reference's inlined core)."""
         if k == "__get__":
             return 0
-        v = None if k is None else float(k)
-        # Math.max(0, Math.floor(+k) || 0)
-        self._threads = None if v is None else (0 if v != v else max(0.0, math.floor(v))
-                                                if not math.isinf(v) else max(0.0, v))
+        if k is None:
+            self._threads = None
+            return self
+        v = float(k)  # Math.max(0, Math.floor(+k) || 0)
+        if v != v:
+            v = 0.0
+        elif not math.isinf(v):
+            v = float(math.floor(v))
+        self._threads = max(0.0, v)
         return self
 
     def find(self, x, y, radius=None):

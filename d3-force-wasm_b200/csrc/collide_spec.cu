@@ -91,6 +91,7 @@ struct SpecArgs {
   double strength, delta0;
   int force_traverse;    // every moved or unmoved turn takes the exact warp traversal (tests)
   int profile;           // record per-depth finish times and counts (stamps)
+  unsigned sleep_ns;     // pause between polls of a wait (after the first four)
   uint32_t n;
   uint32_t *rlist;       // n * SPEC_CAP
   uint8_t *rcount;       // n
@@ -787,7 +788,7 @@ __device__ bool wait_on(const SpecArgs &a, uint64_t r, uint32_t first, uint32_t 
   for (uint32_t t = 0; t < c; ++t) {
     const uint32_t x = t ? (uint32_t)(rd(&a.ents[(r >> 32) + t]) >> 32) : first;
     for (uint32_t it = 0; ld_acquire_u8(&a.state[x]) == 1; ++it) {
-      if (it >= 4) __nanosleep(64);
+      if (it >= 4 && a.sleep_ns) __nanosleep(a.sleep_ns);
       if ((it & 15) == 15) {
         const uint32_t d = ld_relaxed(&a.counters[C_DONE]);
         const unsigned long long now = now_ns();
@@ -1358,6 +1359,7 @@ int collide_parallel(TreeDev &t, const NodeArrays &a, const double *radii, doubl
   // by the exact traversal instead of the recorded ones (a test of that path)
   args.force_traverse = getenv("D3_COLLIDE_FORCE_TRAVERSE") != nullptr;
   args.profile = s.profile;
+  args.sleep_ns = wait_sleep_ns();
   args.rlist = s.rlist; args.rcount = s.rcount; args.wmask = s.wmask; args.emask = s.emask;
   args.vlist = s.vlist; args.vaux = s.vaux; args.vcount = s.vcount; args.start = s.start; args.mdelta = s.mdelta;
   args.state = s.state; args.active = s.active;

@@ -9,6 +9,7 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cuda_runtime.h>
 
 #include "../../include/d3force_b200.h"
@@ -112,6 +113,17 @@ extern unsigned long long g_launches;
 inline unsigned blocks_for(size_t n, unsigned threads) {
   size_t b = (n + threads - 1) / threads;
   return b ? (unsigned)b : 1u;
+}
+
+// The pause between polls of a device wait after its first few polls, in
+// nanoseconds: 64, or D3_WAIT_SLEEP_NS (0 .. 1000; 0 = poll without pausing).
+inline unsigned wait_sleep_ns() {
+  static const unsigned v = [] {
+    const char *e = getenv("D3_WAIT_SLEEP_NS");
+    const int x = e ? atoi(e) : 64;
+    return (unsigned)(x < 0 ? 0 : x > 1000 ? 1000 : x);
+  }();
+  return v;
 }
 
 }  // namespace d3

@@ -686,6 +686,7 @@ struct LinkFlowArgs {
   Rng *rng;           // with serial_lcg: the serial pass's draws
   uint32_t *status;
   int serial_lcg;     // a met jiggle is resolved in the launch (device LCG)
+  unsigned sleep_ns;  // pause between polls of a wait (after the first eight)
 };
 
 __device__ inline unsigned long long globaltimer_ns() {
@@ -709,14 +710,14 @@ __device__ inline void red_release_add(uint32_t *p, uint32_t v) {
 }
 
 __device__ inline bool link_wait(const uint32_t *done, uint32_t src, uint32_t ns, uint32_t tgt,
-                                 uint32_t nt) {
+                                 uint32_t nt, unsigned sleep_ns) {
   // acquire loads: a count seen orders the counted links' writes before the
   // velocities this link reads
   if (ld_acquire_u32(&done[src]) >= ns && ld_acquire_u32(&done[tgt]) >= nt) return true;
   const unsigned long long t0 = globaltimer_ns();
   for (uint32_t it = 0;; ++it) {
     if (ld_acquire_u32(&done[src]) >= ns && ld_acquire_u32(&done[tgt]) >= nt) return true;
-    if (it >= 8) __nanosleep(64);
+    if (it >= 8 && sleep_ns) __nanosleep(sleep_ns);
     if ((it & 15) == 15 && globaltimer_ns() - t0 > 20000000ull) return false;
   }
 }
@@ -745,7 +746,7 @@ __global__ void __launch_bounds__(256) k_link_flow(LinkFlowArgs a) {
       link_params(a.l, a.order[p], c);
       link_positions(a.xs, a.ys, c);
       const uint32_t ns = a.need[2 * p], nt = a.need[2 * p + 1];
-      if (!link_wait(a.done, c.src, ns, c.tgt, nt)) bad = true;
+      if (!link_wait(a.done, c.src, ns, c.tgt, nt, a.sleep_ns)) bad = true;
       const double vxt = __ldcg(&a.vxs[c.tgt]), vyt = __ldcg(&a.vys[c.tgt]);
       const double vxsrc = __ldcg(&a.vxs[c.src]), vysrc = __ldcg(&a.vys[c.src]);
       double x = c.xt + vxt - c.xsrc - vxsrc;
@@ -808,6 +809,7 @@ void link_exact(const NodeArrays &a, const LinkArrays &l, const LinkPlan &plan, 
     c.xs = a.x; c.ys = a.y; c.vxs = a.vx; c.vys = a.vy; c.svx = a.snap_vx; c.svy = a.snap_vy;
     c.l = l; c.order = plan.order; c.need = plan.need; c.done = plan.done;
     c.n = n; c.nodes = plan.nodes; c.alpha = alpha; c.iterations = iterations; c.flag = flag;
+    c.sleep_ns = wait_sleep_ns();
     c.rng = rng; c.status = status; c.serial_lcg = serial_lcg;
     void *params[] = {&c};
     ++g_launches;

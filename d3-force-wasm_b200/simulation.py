@@ -16,6 +16,8 @@ import numpy as np
 
 from . import core as C
 
+_GET = object()  # a method called with no argument reads the value (d3's getters)
+
 INITIAL_RADIUS = 10.0
 INITIAL_ANGLE = math.pi * (3 - math.sqrt(5))  # simulation.js:14-15
 
@@ -248,21 +250,33 @@ class ForceManyBody(Force):
         self.slot.scalar(C.DISTANCE_MIN2, self.distance_min2)
         self.slot.scalar(C.DISTANCE_MAX2, self.distance_max2)
 
-    def strength(self, s):
+    def strength(self, s=_GET):
+        """manyBody.js:37-39"""
+        if s is _GET:
+            return self._strength
         self._strength = _accessor(s)
         if self.nodes is not None:
             self._initialize()
         return self
 
-    def distanceMin(self, d):
+    def distanceMin(self, d=_GET):
+        """manyBody.js:41-43"""
+        if d is _GET:
+            return math.sqrt(self.distance_min2)
         self.distance_min2 = d * d
         return self
 
-    def distanceMax(self, d):
+    def distanceMax(self, d=_GET):
+        """manyBody.js:45-47"""
+        if d is _GET:
+            return math.sqrt(self.distance_max2)
         self.distance_max2 = d * d
         return self
 
-    def theta(self, t):
+    def theta(self, t=_GET):
+        """manyBody.js:49-51"""
+        if t is _GET:
+            return math.sqrt(self.theta2)
         self.theta2 = t * t
         return self
 
@@ -370,16 +384,29 @@ class ForceLink(Force):
     def _push(self):
         self.slot.scalar(C.ITERATIONS, self._iterations)
 
-    def iterations(self, k):
+    def iterations(self, k=_GET):
+        """link.js:109-111"""
+        if k is _GET:
+            return self._iterations
         self._iterations = float(k)
         return self
 
-    def strength(self, s):
+    def _default_strength(self, i):
+        """link.js:30-32: 1 / min(count[source], count[target]) of link i."""
+        return 1.0 / min(self.count[self.source[i]], self.count[self.target[i]])
+
+    def strength(self, s=_GET):
+        """link.js:113-115 (the default strength function when none was set)."""
+        if s is _GET:
+            return self._default_strength if self._strength is None else self._strength
         self._strength = _accessor(s)
         self._write_strength()
         return self
 
-    def distance(self, d):
+    def distance(self, d=_GET):
+        """link.js:117-119"""
+        if d is _GET:
+            return self._distance
         self._distance = _accessor(d)
         self._write_distance()
         return self
@@ -412,17 +439,26 @@ class ForceCollide(Force):
         self.slot.scalar(C.STRENGTH, self._strength)
         self.slot.scalar(C.ITERATIONS, self._iterations)
 
-    def radius(self, r):
+    def radius(self, r=_GET):
+        """collide.js:45-47"""
+        if r is _GET:
+            return self._radius
         self._radius = _accessor(r)
         if self.nodes is not None:
             self._initialize()
         return self
 
-    def strength(self, s):
+    def strength(self, s=_GET):
+        """collide.js:41-43"""
+        if s is _GET:
+            return self._strength
         self._strength = float(s)
         return self
 
-    def iterations(self, k):
+    def iterations(self, k=_GET):
+        """collide.js:37-39"""
+        if k is _GET:
+            return self._iterations
         self._iterations = float(k)
         return self
 
@@ -445,7 +481,24 @@ class ForceCenter(Force):
         self.slot.scalar(C.CY, self.cy)
         self.slot.scalar(C.STRENGTH, self._strength)
 
-    def strength(self, s):
+    def x(self, v=_GET):
+        """center.js:21-23"""
+        if v is _GET:
+            return self.cx
+        self.cx = float(v)
+        return self
+
+    def y(self, v=_GET):
+        """center.js:25-27"""
+        if v is _GET:
+            return self.cy
+        self.cy = float(v)
+        return self
+
+    def strength(self, s=_GET):
+        """center.js:29-31"""
+        if s is _GET:
+            return self._strength
         self._strength = float(s)
         return self
 
@@ -468,8 +521,19 @@ class _ForceAxis(Force):
             self.slot.f64(C.F0, n)[:] = st
             self.slot.f64(C.F1, n)[:] = tz
 
-    def strength(self, s):
+    def strength(self, s=_GET):
+        """x.js:36-38, y.js:36-38"""
+        if s is _GET:
+            return self._strength
         self._strength = _accessor(s)
+        if self.nodes is not None:
+            self._initialize()
+        return self
+
+    def _target_of(self, v):
+        if v is _GET:
+            return self._target
+        self._target = _accessor(v)
         if self.nodes is not None:
             self._initialize()
         return self
@@ -478,9 +542,17 @@ class _ForceAxis(Force):
 class ForceX(_ForceAxis):
     kind = C.X
 
+    def x(self, v=_GET):
+        """x.js:40-42"""
+        return self._target_of(v)
+
 
 class ForceY(_ForceAxis):
     kind = C.Y
+
+    def y(self, v=_GET):
+        """y.js:40-42"""
+        return self._target_of(v)
 
 
 class ForceRadial(Force):
@@ -507,6 +579,38 @@ class ForceRadial(Force):
     def _push(self):
         self.slot.scalar(C.CX, self.cx)
         self.slot.scalar(C.CY, self.cy)
+
+    def strength(self, s=_GET):
+        """radial.js:39-41"""
+        if s is _GET:
+            return self._strength
+        self._strength = _accessor(s)
+        if self.nodes is not None:
+            self._initialize()
+        return self
+
+    def radius(self, r=_GET):
+        """radial.js:43-45"""
+        if r is _GET:
+            return self._radius
+        self._radius = _accessor(r)
+        if self.nodes is not None:
+            self._initialize()
+        return self
+
+    def x(self, v=_GET):
+        """radial.js:47-49"""
+        if v is _GET:
+            return self.cx
+        self.cx = float(v)
+        return self
+
+    def y(self, v=_GET):
+        """radial.js:51-53"""
+        if v is _GET:
+            return self.cy
+        self.cy = float(v)
+        return self
 
 
 def d3_lcg(seed=1):

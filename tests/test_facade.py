@@ -242,3 +242,72 @@ def test_threads_is_accepted(ocore):
         assert sim.threads(float("nan")) is sim and sim.threads() == 0
     finally:
         sim.close()
+
+
+def _bits(nd):
+    return [np.asarray(getattr(nd, f)).view(np.uint64).copy() for f in ("x", "y", "vx", "vy")]
+
+
+def _run(core, make, n=40, ticks=3):
+    nd = pkg.Nodes(n)
+    sim = pkg.forceSimulation(nd, core=core)
+    try:
+        for name, f in make():
+            sim.force(name, f)
+        sim.tick(ticks)
+        return _bits(nd)
+    finally:
+        sim.close()
+
+
+def test_force_getters_return_what_was_set():
+    mb = pkg.forceManyBody().strength(-12).distanceMin(2).distanceMax(50).theta(0.5)
+    assert mb.strength()(3) == -12 and mb.distanceMin() == 2 and mb.distanceMax() == 50
+    assert mb.theta() == 0.5
+    co = pkg.forceCollide().radius(3).strength(0.7).iterations(2)
+    assert co.radius()(0) == 3 and co.strength() == 0.7 and co.iterations() == 2
+    ce = pkg.forceCenter().x(3).y(-1).strength(0.5)
+    assert (ce.x(), ce.y(), ce.strength()) == (3, -1, 0.5)
+    fx, fy = pkg.forceX().x(10).strength(0.5), pkg.forceY().y(-4)
+    assert fx.x()(0) == 10 and fx.strength()(0) == 0.5 and fy.y()(1) == -4
+    ra = pkg.forceRadial(5).strength(0.2).x(1).y(2).radius(7)
+    assert ra.radius()(0) == 7 and ra.strength()(0) == 0.2 and (ra.x(), ra.y()) == (1, 2)
+    li = pkg.forceLink([0, 0, 1], [1, 2, 2]).iterations(3).distance(12)
+    assert li.iterations() == 3 and li.distance()(0) == 12
+
+
+def test_default_link_strength_getter(ocore):
+    sim = pkg.forceSimulation(pkg.Nodes(3), core=ocore)
+    try:
+        li = pkg.forceLink([0, 0], [1, 2])
+        sim.force("link", li)
+        assert li.strength()(0) == 1.0 / min(2, 1)  # link.js:30-32
+    finally:
+        sim.close()
+
+
+def test_setters_equal_constructor_arguments(ocore):
+    """radial / center / x / y configured by setters tick bit for bit like
+    the same values given to the constructors."""
+    a = _run(ocore, lambda: [("r", pkg.forceRadial(7, 1, 2).strength(0.2)),
+                             ("c", pkg.forceCenter(3, -1).strength(0.5)),
+                             ("x", pkg.forceX(10).strength(0.3)), ("y", pkg.forceY(-4))])
+    b = _run(ocore, lambda: [("r", pkg.forceRadial(5).strength(0.2).x(1).y(2).radius(7)),
+                             ("c", pkg.forceCenter().x(3).y(-1).strength(0.5)),
+                             ("x", pkg.forceX().x(10).strength(0.3)), ("y", pkg.forceY().y(-4))])
+    for u, v in zip(a, b):
+        assert np.array_equal(u, v)
+
+
+def test_force_x_known_answer(ocore):
+    """simple.zig:51-62 then integrate: vx += (target - x) strength alpha;
+    vx *= 0.6; x += vx."""
+    nd = pkg.Nodes(1, x=[2.0], y=[0.0], vx=[0.0], vy=[0.0])
+    sim = pkg.forceSimulation(nd, core=ocore).force("x", pkg.forceX().x(10).strength(0.5))
+    try:
+        sim.tick()
+        a = 1 + (0 - 1) * (1 - math.pow(0.001, 1 / 300))
+        vx = (0.0 + (10 - 2.0) * 0.5 * a) * 0.6
+        assert nd.vx[0] == vx and nd.x[0] == 2.0 + vx
+    finally:
+        sim.close()

@@ -1,9 +1,11 @@
 /* d3force_oracle.c — CPU ORACLE for the d3-force tick (TEST INFRASTRUCTURE).
  *
  * This file is the checker, not the product: only tests/, the smoke check and
- * bench.py's CPU-baseline leg load it. It restates, statement by statement and
- * single-threaded, the d3-force-wasm core (Zig, the files under `src/core/`), which is
- * itself a port of d3-force 3.0.0 / d3-quadtree 3.0.1 (npm, pinned in the
+ * bench.py's CPU-baseline leg load it. It restates, statement by statement
+ * and single-threaded, the d3-force-wasm core (Zig, the files under
+ * `src/core/`); the CPU baseline alone turns on threads (oracle_set_threads),
+ * with bit-identical results. The core is itself a port of d3-force 3.0.0 /
+ * d3-quadtree 3.0.1 (npm, pinned in the
  * reference's package-lock.json:29-48, not vendored). Every function cites the
  * reference file:line it follows. It exports the same C ABI as the CUDA engine
  * (include/d3force_b200.h), so one host driver runs either.
@@ -206,9 +208,139 @@ static int tree_box(Tree *t, const double *xs, const double *ys, uint32_t n, dou
   return 1;
 }
 
+/* tree.zig:252-284 (exactKeys): the 32-level midpoint Morton key of (x, y). */
+static uint64_t exact_key(const double *e, double x, double y) {
+  double x0 = e[0], y0 = e[1], x1 = e[2], y1 = e[3];
+  uint64_t key = 0;
+  for (int lv = 0; lv < KEY_LEVELS; ++lv) {
+    double xm = (x0 + x1) / 2;
+    double ym = (y0 + y1) / 2;
+    int right = x >= xm;
+    if (right) x0 = xm; else x1 = xm;
+    int bottom = y >= ym;
+    if (bottom) y0 = ym; else y1 = ym;
+    key = (key << 2) | ((uint64_t)bottom << 1) | (uint64_t)right;
+  }
+  return key;
+}
+
+/* The key pass and the stable sort over `k` worker threads, for the CPU
+ * baseline only (oracle_set_threads): the reference spreads both over its
+ * pool (tree.zig:371-388; sort.zig:55-91 with per-chunk histograms). Workers
+ * take contiguous chunks, so the compaction keeps index order and every
+ * pass stays stable: the result is the serial one bit for bit. */
+typedef struct {
+  Tree *t;
+  const double *xs, *ys;
+  uint32_t n, k;
+  pthread_barrier_t bar;
+  uint32_t valid[64];      /* points without a NaN coordinate, per chunk */
+  uint32_t hist[64 * 256]; /* a pass's digit counts, per chunk */
+} PrepShared;
+
+typedef struct {
+  PrepShared *sh;
+  uint32_t w;
+} PrepJob;
+
+static void chunk_of(uint32_t n, uint32_t k, uint32_t w, uint32_t *lo, uint32_t *hi) {
+  uint32_t per = (n + k - 1) / k;
+  uint64_t a = (uint64_t)w * per, b = a + per;
+  *lo = a < n ? (uint32_t)a : n;
+  *hi = b < n ? (uint32_t)b : n;
+}
+
+static void *prep_worker(void *arg) {
+  PrepJob *j = arg;
+  PrepShared *sh = j->sh;
+  Tree *t = sh->t;
+  const uint32_t w = j->w, k = sh->k, n = sh->n, m = t->m;
+  uint32_t lo, hi;
+  chunk_of(n, k, w, &lo, &hi);
+  /* keys of this chunk's points, by point index, into keys_tmp */
+  uint32_t v = 0;
+  for (uint32_t i = lo; i < hi; ++i) {
+    double x = sh->xs[i], y = sh->ys[i];
+    if (x != x || y != y) continue;
+    t->keys_tmp[i] = exact_key(t->extent, x, y);
+    ++v;
+  }
+  sh->valid[w] = v;
+  pthread_barrier_wait(&sh->bar);
+  /* compaction in index order (tree.zig:371-388): sorted candidates, then
+   * the NaN points into rest */
+  uint32_t off = 0, roff = 0;
+  for (uint32_t u = 0; u < w; ++u) {
+    uint32_t ulo, uhi;
+    chunk_of(n, k, u, &ulo, &uhi);
+    off += sh->valid[u];
+    roff += (uhi - ulo) - sh->valid[u];
+  }
+  for (uint32_t i = lo; i < hi; ++i) {
+    double x = sh->xs[i], y = sh->ys[i];
+    if (x != x || y != y) {
+      t->rest[roff++] = i;
+      continue;
+    }
+    t->perm[off] = i;
+    t->keys[off] = t->keys_tmp[i];
+    ++off;
+  }
+  pthread_barrier_wait(&sh->bar);
+  /* sort.zig:55-91 over chunks of the m candidates */
+  uint32_t mlo, mhi;
+  chunk_of(m, k, w, &mlo, &mhi);
+  uint64_t *sk = t->keys, *dk = t->keys_tmp;
+  uint32_t *sv = t->perm, *dv = t->perm_tmp;
+  for (uint32_t b = 0; m && b < 8; ++b) {
+    const unsigned shf = 8 * b;
+    uint32_t *h = sh->hist + 256 * w;
+    memset(h, 0, 256 * sizeof(uint32_t));
+    for (uint32_t i = mlo; i < mhi; ++i) h[(sk[i] >> shf) & 255]++;
+    pthread_barrier_wait(&sh->bar);
+    /* the pass is skipped when one digit holds every key (as the serial
+     * sort); else this chunk's place for each digit: all chunks' counts of
+     * lower digits, then earlier chunks' counts of the same digit */
+    const uint32_t d0 = (uint32_t)((sk[0] >> shf) & 255);
+    uint32_t tot0 = 0;
+    for (uint32_t u = 0; u < k; ++u) tot0 += sh->hist[256 * u + d0];
+    const int skip = tot0 == m;
+    uint32_t place[256];
+    if (!skip) {
+      uint32_t run = 0;
+      for (int d = 0; d < 256; ++d) {
+        uint32_t before = 0, all = 0;
+        for (uint32_t u = 0; u < k; ++u) {
+          uint32_t c = sh->hist[256 * u + d];
+          if (u < w) before += c;
+          all += c;
+        }
+        place[d] = run + before;
+        run += all;
+      }
+      for (uint32_t i = mlo; i < mhi; ++i) {
+        uint32_t d = (uint32_t)((sk[i] >> shf) & 255);
+        dk[place[d]] = sk[i];
+        dv[place[d]] = sv[i];
+        place[d]++;
+      }
+    }
+    pthread_barrier_wait(&sh->bar);
+    if (!skip) {
+      uint64_t *tk = sk; sk = dk; dk = tk;
+      uint32_t *tv = sv; sv = dv; dv = tv;
+    }
+  }
+  if (sk != t->keys) {
+    memcpy(t->keys + mlo, sk + mlo, (size_t)(mhi - mlo) * 8);
+    memcpy(t->perm + mlo, sv + mlo, (size_t)(mhi - mlo) * 4);
+  }
+  return NULL;
+}
+
 /* tree.zig:371-388 + exactKeys 252-284: extent by cover, 32-level midpoint
- * Morton keys, stable sort. */
-static int tree_prepare(Tree *t, const double *xs, const double *ys, uint32_t n) {
+ * Morton keys, stable sort (over `threads` workers when threads > 1). */
+static int tree_prepare(Tree *t, const double *xs, const double *ys, uint32_t n, int threads) {
   if (tree_reserve(t, n)) return -1;
   t->extent[0] = t->extent[1] = t->extent[2] = t->extent[3] = NAN;
   t->len = 0;
@@ -218,6 +350,22 @@ static int tree_prepare(Tree *t, const double *xs, const double *ys, uint32_t n)
   if (!tree_box(t, xs, ys, n, b)) return 0;
   tree_cover(t, b[0], b[1]);
   tree_cover(t, b[2], b[3]);
+  if (threads > 1 && n >= 8192) {
+    PrepShared *sh = malloc(sizeof *sh);
+    if (!sh) return -1;
+    const uint32_t k = threads > 64 ? 64 : (uint32_t)threads;
+    sh->t = t; sh->xs = xs; sh->ys = ys; sh->n = n; sh->k = k;
+    pthread_barrier_init(&sh->bar, NULL, k);
+    pthread_t th[64];
+    PrepJob jobs[64];
+    for (uint32_t w = 0; w < k; ++w) jobs[w] = (PrepJob){sh, w};
+    for (uint32_t w = 1; w < k; ++w) pthread_create(&th[w], NULL, prep_worker, &jobs[w]);
+    prep_worker(&jobs[0]);
+    for (uint32_t w = 1; w < k; ++w) pthread_join(th[w], NULL);
+    pthread_barrier_destroy(&sh->bar);
+    free(sh);
+    return 1;
+  }
   const double *e = t->extent;
   uint32_t k = 0, rest = 0;
   for (uint32_t i = 0; i < n; ++i) {
@@ -226,19 +374,8 @@ static int tree_prepare(Tree *t, const double *xs, const double *ys, uint32_t n)
       t->rest[rest++] = i;
       continue;
     }
-    double x0 = e[0], y0 = e[1], x1 = e[2], y1 = e[3];
-    uint64_t key = 0;
-    for (int lv = 0; lv < KEY_LEVELS; ++lv) {
-      double xm = (x0 + x1) / 2;
-      double ym = (y0 + y1) / 2;
-      int right = x >= xm;
-      if (right) x0 = xm; else x1 = xm;
-      int bottom = y >= ym;
-      if (bottom) y0 = ym; else y1 = ym;
-      key = (key << 2) | ((uint64_t)bottom << 1) | (uint64_t)right;
-    }
     t->perm[k] = i;
-    t->keys[k] = key;
+    t->keys[k] = exact_key(e, x, y);
     ++k;
   }
   radix_sort(t->keys, t->perm, t->keys_tmp, t->perm_tmp, t->m, 8);
@@ -326,61 +463,245 @@ static Frame tree_child(const Frame *f, uint32_t q, uint32_t lo, uint32_t hi, ui
   return c;
 }
 
-static int tree_push(Tree *t, uint32_t *sp, Frame f) {
-  if (*sp == t->stack_cap) {
-    uint32_t cap = t->stack_cap ? 2 * t->stack_cap : 256;
-    Frame *s = realloc(t->stack, (size_t)cap * sizeof(Frame));
+/* Where a preorder walk puts its cells: the tree's own array, or a job's. */
+typedef struct {
+  Cell *cells;
+  uint32_t len, cap;
+  Frame *stack;
+  uint32_t stack_cap;
+  uint32_t depth;
+} EmitBuf;
+
+/* A subtree emitted on its own by the threaded emission: its root frame, its
+ * cells (local indices, root at 0), and where they go in the tree. */
+typedef struct {
+  Frame f;
+  EmitBuf b;
+  uint32_t off;
+  int err;
+} EmitJob;
+
+static int eb_push(EmitBuf *b, uint32_t *sp, Frame f) {
+  if (*sp == b->stack_cap) {
+    uint32_t cap = b->stack_cap ? 2 * b->stack_cap : 256;
+    Frame *s = realloc(b->stack, (size_t)cap * sizeof(Frame));
     if (!s) return -1;
-    t->stack = s;
-    t->stack_cap = cap;
+    b->stack = s;
+    b->stack_cap = cap;
   }
-  t->stack[(*sp)++] = f;
+  b->stack[(*sp)++] = f;
   return 0;
 }
 
-/* tree.zig:572-647 restated serially: the preorder walk that the reference's
- * top walk + job subtrees reproduce index for index. */
-static int tree_emit(Tree *t, const double *xs, const double *ys) {
-  uint32_t sp = 0, next = 0, depth = 0;
-  Frame root = {0, t->m, 0, NONE, 0, 1, t->extent[0], t->extent[1], t->extent[2], t->extent[3]};
-  if (tree_push(t, &sp, root)) return -1;
+/* tree.zig:572-647 restated serially: the preorder walk from `root`, cells
+ * appended to b (child links in b's indices). The threaded emission's top
+ * walk passes cut > 0: a frame below the root with at most `cut` points is
+ * then not walked but becomes a job. In its first pass (place == 0) the job
+ * is appended to *jobs; in the second (place == 1) the next job in order
+ * takes its subtree's cell count of indices, linked from its parent. */
+static int emit_walk(Tree *t, const double *xs, const double *ys, EmitBuf *b, Frame root,
+                     uint32_t cut, EmitJob **jobs, uint32_t *nj, uint32_t *jcap, int place) {
+  uint32_t sp = 0;
+  if (eb_push(b, &sp, root)) return -1;
   while (sp > 0) {
-    Frame f = t->stack[--sp];
-    if (next == t->cells_cap) {
-      uint32_t cap = t->cells_cap ? 2 * t->cells_cap : 2 * t->m + 64;
-      Cell *c = realloc(t->cells, (size_t)cap * sizeof(Cell));
-      if (!c) return -1;
-      t->cells = c;
-      t->cells_cap = cap;
+    Frame f = b->stack[--sp];
+    if (cut && f.depth > root.depth && f.hi - f.lo <= cut) {
+      if (!place) {
+        if (*nj == *jcap) {
+          uint32_t cap = *jcap ? 2 * *jcap : 64;
+          EmitJob *js = realloc(*jobs, (size_t)cap * sizeof(EmitJob));
+          if (!js) return -1;
+          *jobs = js;
+          *jcap = cap;
+        }
+        EmitJob *j = &(*jobs)[(*nj)++];
+        memset(j, 0, sizeof *j);
+        j->f = f;
+        j->f.parent = NONE;
+      } else {
+        EmitJob *j = &(*jobs)[(*nj)++];
+        j->off = b->len;
+        if (f.parent != NONE) b->cells[f.parent].child[f.slot] = b->len;
+        b->len += j->b.len;
+      }
+      continue;
     }
-    uint32_t me = next++;
-    Cell *c = &t->cells[me];
+    if (b->len == b->cap) {
+      uint32_t cap = b->cap ? 2 * b->cap : 2 * (root.hi - root.lo) + 64;
+      Cell *c = realloc(b->cells, (size_t)cap * sizeof(Cell));
+      if (!c) return -1;
+      b->cells = c;
+      b->cap = cap;
+    }
+    uint32_t me = b->len++;
+    Cell *c = &b->cells[me];
     c->child[0] = c->child[1] = c->child[2] = c->child[3] = NONE;
     c->first = f.lo;
     c->count = f.hi - f.lo;
     c->x0 = f.x0; c->y0 = f.y0; c->x1 = f.x1; c->y1 = f.y1;
     c->x = c->y = c->value = c->r = 0;
-    if (f.parent != NONE) t->cells[f.parent].child[f.slot] = me;
-    if (f.depth > depth) depth = f.depth;
+    if (f.parent != NONE) b->cells[f.parent].child[f.slot] = me;
+    if (f.depth > b->depth) b->depth = f.depth;
     if (f.depth >= MAX_DEPTH || tree_all_same(t, &f, xs, ys)) continue;
     uint32_t s5[5];
     tree_split(t, &f, xs, ys, s5);
     for (int q = 3; q >= 0; --q) {
       if (s5[q] == s5[q + 1]) continue;
-      if (tree_push(t, &sp, tree_child(&f, (uint32_t)q, s5[q], s5[q + 1], me))) return -1;
+      if (eb_push(b, &sp, tree_child(&f, (uint32_t)q, s5[q], s5[q + 1], me))) return -1;
     }
   }
+  return 0;
+}
+
+static Frame root_frame(const Tree *t) {
+  Frame root = {0, t->m, 0, NONE, 0, 1, t->extent[0], t->extent[1], t->extent[2], t->extent[3]};
+  return root;
+}
+
+/* The serial emission: the whole walk into the tree's array. */
+static int tree_emit(Tree *t, const double *xs, const double *ys) {
+  EmitBuf b = {t->cells, 0, t->cells_cap, t->stack, t->stack_cap, 0};
+  int r = emit_walk(t, xs, ys, &b, root_frame(t), 0, NULL, NULL, NULL, 0);
+  t->cells = b.cells;
+  t->cells_cap = b.cap;
+  t->stack = b.stack;
+  t->stack_cap = b.stack_cap;
+  if (r) return -1;
   t->root = 0;
-  t->len = next;
+  t->len = b.len;
+  t->depth = b.depth;
+  return 0;
+}
+
+/* The threaded emission (CPU baseline only), as the reference's serial top
+ * walk plus per-job walks: the top walk collects the subtrees of at most
+ * max(m / 64, 64) points (jobs); workers walk the jobs into their own
+ * buffers; a second top walk places every top cell and every job's block
+ * of cells in preorder; workers copy the blocks in, their child links
+ * shifted. The cells are those of the serial walk, index for index: a job's
+ * block is its subtree's preorder, and the top walk visits the jobs in
+ * preorder. */
+typedef struct {
+  Tree *t;
+  const double *xs, *ys;
+  EmitJob *jobs;
+  uint32_t nj, k;
+  pthread_barrier_t bar;
+  int err;
+} EmitShared;
+
+typedef struct {
+  EmitShared *sh;
+  uint32_t w;
+} EmitWorker;
+
+static void *emit_worker(void *arg) {
+  EmitWorker *ew = arg;
+  EmitShared *sh = ew->sh;
+  for (uint32_t j = ew->w; j < sh->nj; j += sh->k) {
+    EmitJob *job = &sh->jobs[j];
+    job->err = emit_walk(sh->t, sh->xs, sh->ys, &job->b, job->f, 0, NULL, NULL, NULL, 0);
+  }
+  pthread_barrier_wait(&sh->bar); /* the jobs are walked */
+  pthread_barrier_wait(&sh->bar); /* the second top walk has placed them */
+  if (sh->err) return NULL;
+  for (uint32_t j = ew->w; j < sh->nj; j += sh->k) {
+    EmitJob *job = &sh->jobs[j];
+    Cell *dst = sh->t->cells + job->off;
+    memcpy(dst, job->b.cells, (size_t)job->b.len * sizeof(Cell));
+    for (uint32_t c = 0; c < job->b.len; ++c)
+      for (int q = 0; q < 4; ++q)
+        if (dst[c].child[q] != NONE) dst[c].child[q] += job->off;
+  }
+  return NULL;
+}
+
+static int tree_emit_threaded(Tree *t, const double *xs, const double *ys, int threads) {
+  const uint32_t cut = t->m / 64 > 64 ? t->m / 64 : 64;
+  EmitJob *jobs = NULL;
+  uint32_t nj = 0, jcap = 0;
+  EmitBuf top = {NULL, 0, 0, t->stack, t->stack_cap, 0};
+  int r = emit_walk(t, xs, ys, &top, root_frame(t), cut, &jobs, &nj, &jcap, 0);
+  free(top.cells);
+  t->stack = top.stack;
+  t->stack_cap = top.stack_cap;
+  if (r) {
+    free(jobs);
+    return -1;
+  }
+  EmitShared *sh = malloc(sizeof *sh);
+  if (!sh) {
+    free(jobs);
+    return -1;
+  }
+  const uint32_t k = threads > 64 ? 64 : (uint32_t)threads;
+  sh->t = t; sh->xs = xs; sh->ys = ys; sh->jobs = jobs; sh->nj = nj; sh->k = k; sh->err = 0;
+  pthread_barrier_init(&sh->bar, NULL, k);
+  pthread_t th[64];
+  EmitWorker ws[64];
+  for (uint32_t w = 0; w < k; ++w) ws[w] = (EmitWorker){sh, w};
+  for (uint32_t w = 1; w < k; ++w) pthread_create(&th[w], NULL, emit_worker, &ws[w]);
+  /* worker 0's share of the jobs, then the second top walk between the
+   * barriers, then its share of the copies */
+  for (uint32_t j = 0; j < nj; j += k)
+    jobs[j].err = emit_walk(t, xs, ys, &jobs[j].b, jobs[j].f, 0, NULL, NULL, NULL, 0);
+  pthread_barrier_wait(&sh->bar);
+  uint32_t total = top.len, depth = top.depth;
+  for (uint32_t j = 0; j < nj; ++j) {
+    if (jobs[j].err) sh->err = 1;
+    total += jobs[j].b.len;
+    if (jobs[j].b.depth > depth) depth = jobs[j].b.depth;
+  }
+  if (!sh->err && total > t->cells_cap) {
+    Cell *c = realloc(t->cells, (size_t)total * sizeof(Cell));
+    if (c) {
+      t->cells = c;
+      t->cells_cap = total;
+    } else {
+      sh->err = 1;
+    }
+  }
+  if (!sh->err) {
+    EmitBuf b = {t->cells, 0, t->cells_cap, t->stack, t->stack_cap, 0};
+    uint32_t placed = 0;
+    if (emit_walk(t, xs, ys, &b, root_frame(t), cut, &jobs, &placed, &jcap, 1)) sh->err = 1;
+    t->cells = b.cells;
+    t->cells_cap = b.cap;
+    t->stack = b.stack;
+    t->stack_cap = b.stack_cap;
+  }
+  pthread_barrier_wait(&sh->bar);
+  if (!sh->err) {
+    for (uint32_t j = 0; j < nj; j += k) {
+      Cell *dst = t->cells + jobs[j].off;
+      memcpy(dst, jobs[j].b.cells, (size_t)jobs[j].b.len * sizeof(Cell));
+      for (uint32_t c = 0; c < jobs[j].b.len; ++c)
+        for (int q = 0; q < 4; ++q)
+          if (dst[c].child[q] != NONE) dst[c].child[q] += jobs[j].off;
+    }
+  }
+  for (uint32_t w = 1; w < k; ++w) pthread_join(th[w], NULL);
+  const int err = sh->err;
+  pthread_barrier_destroy(&sh->bar);
+  free(sh);
+  for (uint32_t j = 0; j < nj; ++j) {
+    free(jobs[j].b.cells);
+    free(jobs[j].b.stack);
+  }
+  free(jobs);
+  if (err) return -1;
+  t->root = 0;
+  t->len = total;
   t->depth = depth;
   return 0;
 }
 
 /* tree.zig:191-196 */
-static int tree_build_xy(Tree *t, const double *xs, const double *ys, uint32_t n) {
-  int r = tree_prepare(t, xs, ys, n);
+static int tree_build_xy(Tree *t, const double *xs, const double *ys, uint32_t n, int threads) {
+  int r = tree_prepare(t, xs, ys, n, threads);
   if (r <= 0) return r;
   tree_runs(t, xs, ys);
+  if (threads > 1 && t->m >= 8192) return tree_emit_threaded(t, xs, ys, threads);
   return tree_emit(t, xs, ys);
 }
 
@@ -712,9 +1033,9 @@ static int sim_build_tree(Sim *s, int shifted) {
       s->px[i] = s->x[i] + s->vx[i];
       s->py[i] = s->y[i] + s->vy[i];
     }
-    return tree_build_xy(&s->tree, s->px, s->py, n);
+    return tree_build_xy(&s->tree, s->px, s->py, n, s->threads);
   }
-  return tree_build_xy(&s->tree, s->x, s->y, n);
+  return tree_build_xy(&s->tree, s->x, s->y, n, s->threads);
 }
 
 int32_t tree_build(uint32_t h, uint32_t shifted) {
@@ -1942,8 +2263,9 @@ int32_t sim_set_profile(uint32_t h, uint32_t on) {
   return get_sim(h) ? D3_OK : D3_BAD_HANDLE;
 }
 
-/* Oracle-only: worker threads for the exact many-body record pass (the CPU
- * baseline's stand-in for the reference's thread pool). */
+/* Oracle-only: worker threads for the tree builds (key pass, sort, emission
+ * jobs) and the exact many-body record pass, the CPU baseline's stand-in for
+ * the reference's thread pool. The results do not change. */
 int32_t oracle_set_threads(uint32_t h, uint32_t k) {
   Sim *s = get_sim(h);
   if (!s) return D3_BAD_HANDLE;

@@ -310,3 +310,57 @@ def test_node_table_views_mirrors_and_detaches(ocore):
         arr = getattr(nodes, f)
         assert arr.flags.owndata and np.array_equal(arr, v, equal_nan=True), f
     rsim.close()
+
+
+def _tree_with_threads(ocore, xs, ys, threads, shifted=0):
+    C = H.C
+    n = len(xs)
+    h = ocore.sim_create()
+    try:
+        assert ocore.sim_set_node_count(h, n) >= 0
+        ocore.f64_view(ocore.sim_ptr(h, C.PTR_X), n)[:] = xs
+        ocore.f64_view(ocore.sim_ptr(h, C.PTR_Y), n)[:] = ys
+        ocore.f64_view(ocore.sim_ptr(h, C.PTR_VX), n)[:] = 0.25
+        ocore.f64_view(ocore.sim_ptr(h, C.PTR_VY), n)[:] = -0.5
+        ocore.lib.oracle_set_threads(h, threads)
+        assert ocore.tree_build(h, shifted) >= 0
+        return ocore.tree(h)
+    finally:
+        ocore.sim_destroy(h)
+
+
+@pytest.mark.parametrize("case", ["uniform", "clustered", "nan_dups", "small", "deep"])
+def test_threaded_tree_build_is_the_serial_one(ocore, case):
+    """The CPU baseline's threaded tree build (oracle_set_threads > 1: key
+    pass, sort, and the emission as a top walk plus per-job walks) builds the
+    same tree, bit for bit, as the serial restatement. `deep` has groups of
+    distinct points below the key resolution, one larger than a job."""
+    rng = np.random.default_rng(11)
+    n = {"uniform": 50000, "clustered": 30011, "nan_dups": 20000, "small": 8192,
+         "deep": 12000}[case]
+    if case == "deep":
+        xs = rng.uniform(-1e3, 1e3, n)
+        ys = rng.uniform(-1e3, 1e3, n)
+        for base, size in [(5000, 400)] + [(20 * g + 3, 20) for g in range(60)]:
+            xs[base:base + size] = xs[base] + rng.uniform(-1e-12, 1e-12, size)
+            ys[base:base + size] = ys[base] + rng.uniform(-1e-12, 1e-12, size)
+    elif case == "clustered":
+        c = rng.integers(0, 7, n)
+        xs = c * 100.0 + rng.normal(0, 0.5, n)
+        ys = c * -40.0 + rng.normal(0, 0.5, n)
+    else:
+        xs = rng.uniform(-1e3, 1e3, n)
+        ys = rng.uniform(-1e3, 1e3, n)
+    if case == "nan_dups":
+        xs[::37] = np.nan
+        ys[5::53] = np.nan
+        xs[1::11], ys[1::11] = xs[0], ys[0]
+        xs[2::13] = -0.0
+    for shifted in (0, 1):
+        a = _tree_with_threads(ocore, xs, ys, 1, shifted)
+        for k in (3, 8):
+            b = _tree_with_threads(ocore, xs, ys, k, shifted)
+            assert a["root"] == b["root"]
+            assert np.array_equal(a["perm"], b["perm"])
+            assert a["cells"].tobytes() == b["cells"].tobytes()
+            assert a["extent"].tobytes() == b["extent"].tobytes()

@@ -364,3 +364,27 @@ def test_threaded_tree_build_is_the_serial_one(ocore, case):
             assert np.array_equal(a["perm"], b["perm"])
             assert a["cells"].tobytes() == b["cells"].tobytes()
             assert a["extent"].tobytes() == b["extent"].tobytes()
+
+
+@pytest.mark.parametrize("threads", [1, 3, 7])
+def test_threaded_oracle_ticks_bitwise(ocore, threads):
+    """The analogue of the reference's thread gates (threads 0/1/3/7): the
+    oracle's exact ticks with its threaded tree builds and many-body record
+    pass equal the serial ticks bit for bit, jiggles and the random stream
+    included (1% coincident and sub-1e-12 nodes, collide, pinned nodes)."""
+    sc = H.scenarios
+    runs = []
+    for k in (1, threads):
+        nodes, sim = sc.setup_exact(pkg, ocore, n=12000, m=24000, collide_radius=4,
+                                    coincident=0.01, near=0.01, pinned=0.005, seed=4)
+        try:
+            ocore.lib.oracle_set_threads(sim.ctx.h, k)
+            sim.tick(4)
+            runs.append(([np.asarray(getattr(nodes, f)).view(np.uint64).copy()
+                          for f in ("x", "y", "vx", "vy")], ocore.sim_get_lcg(sim.ctx.h)))
+        finally:
+            sim.close()
+    (a, la), (b, lb) = runs
+    assert la == lb
+    for u, v in zip(a, b):
+        assert np.array_equal(u, v)

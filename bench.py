@@ -22,6 +22,7 @@ stream); rank 0 prints the line.
 """
 
 import argparse
+import hashlib
 import importlib
 import json
 import os
@@ -37,12 +38,17 @@ WORKLOAD = dict(n=50000, m=100000, collide_radius=5, coincident=0.01, near=0.01,
 WORKLOAD_NAME = ("exact n=50000 m=100000 manyBody(-30,theta .9)+link(30)+collide(5)+center; "
                  "1% coincident, 1% offsets<1e-12, 0.5% pinned")
 METRIC = "ms/tick: exact 50k bit-exact"
+SCHEDULE_TICKS = 300  # the configuration's tick count (d3's default alpha schedule)
+CHECK_TICK = 95  # 5 warm-up + 3 x 30 ticks: where the CPU protocol's state is compared
 PHASES = ["mb_tree", "mb_accumulate", "mb_traverse", "link", "collide_tree", "collide_loop",
           "center", "integrate"]
 SIDE_PHASES = {"center_sum_side_stream": 11}
 # What the CPU baseline (the oracle) spreads over the host threads, as the
 # reference's worker pool does; link and collide's node loop are serial in both.
 THREADED = "tree keys, sort and emission jobs; many-body record pass"
+# DRAM bytes (read + write) of one collide launch (k_collide_spec) on this
+# workload, from an ncu capture (profiles/k_collide_spec_exact_50k.md)
+COLLIDE_DRAM_BYTES = 63628032 + 9661184
 
 
 def parse():
@@ -53,7 +59,6 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fast", action="store_true", help="skip the fast-mode 1M measurement")
-    ap.add_argument("--e2e-steps", type=int, default=10)
     return ap.parse_args()
 
 
@@ -75,9 +80,36 @@ def max_over_ranks(x, world):
     return float(t.item())
 
 
-def oracle_ms_per_tick(pkg, sc, threads, warmup, rounds, ticks):
-    """The reference algorithm (oracle) on the host: `warmup` ticks, then the
-    best of `rounds` rounds of `ticks` ticks (bench/threads.js:85-96)."""
+def schedule_positions(warmup, steps, total=None):
+    """The K timed ticks, spread evenly over the C2 schedule after the W
+    warm-up ticks: ticks W + ceil((k + 1) (T - W) / K), k = 0..K-1, where T
+    is the schedule's 300 ticks (longer when W + K exceeds it). Returns
+    (positions, T)."""
+    total = total or max(SCHEDULE_TICKS, warmup + steps)
+    span = total - warmup
+    pos = [warmup + -(-(k + 1) * span // steps) for k in range(steps)]
+    return pos, total
+
+
+def state_digest(nodes, lcg):
+    """SHA-256 of x, y, vx, vy (f64 little-endian) and the LCG state."""
+    import numpy as np
+
+    h = hashlib.sha256()
+    for f in ("x", "y", "vx", "vy"):
+        h.update(np.ascontiguousarray(getattr(nodes, f), dtype="<f8").tobytes())
+    h.update(int(lcg).to_bytes(4, "little"))
+    return h.hexdigest()
+
+
+def oracle_protocol(pkg, sc, threads, warmup=5, rounds=3, ticks=30, count_work=False):
+    """The reference's timing protocol (bench/threads.js:24-35): `warmup`
+    ticks, then the minimum over `rounds` rounds of `ticks` consecutive ticks,
+    on the oracle (the reference algorithm restated in C) with `threads` host
+    threads. Returns the ms/tick, the state digest after the last tick (tick
+    warmup + rounds * ticks) and, with count_work, the exact many-body work
+    (cells visited, accepted approximations, leaf point interactions) per tick
+    over the last round."""
     import oracle
 
     core = oracle.load(pkg)
@@ -85,12 +117,18 @@ def oracle_ms_per_tick(pkg, sc, threads, warmup, rounds, ticks):
     core.lib.oracle_set_threads(sim.ctx.h, threads)
     sim.tick(warmup)
     best = float("inf")
-    for _ in range(rounds):
+    work = None
+    for r in range(rounds):
+        if count_work and r == rounds - 1:
+            core.lib.oracle_mb_stat(3)
         t0 = time.perf_counter()
         sim.tick(ticks)
         best = min(best, (time.perf_counter() - t0) * 1e3 / ticks)
+    if count_work:
+        work = {k: core.lib.oracle_mb_stat(i) / ticks for i, k in enumerate(("V", "A", "P"))}
+    digest = state_digest(nodes, core.sim_get_lcg(sim.ctx.h))
     sim.close()
-    return best
+    return best, digest, work
 
 
 class Clocks:
@@ -237,6 +275,93 @@ def fast_1m(pkg, core, torch, steps=10, warmup=3, targets=1024):
             "bit_exact_vs_reference_order": True}
 
 
+def exact_device_run(pkg, sc, core, positions, total, flush_l2, world, profile=False):
+    """The exact workload's schedule on the device, one sim_tick per tick,
+    L2 flushed before each. Returns per-tick device ms (CUDA events on the
+    engine's stream), the launches of the timed ticks, the state digest at
+    CHECK_TICK and at the end, and (profile) per-phase ms and engine stats at
+    the timed ticks."""
+    nodes, sim = sc.setup_exact(pkg, core, **WORKLOAD)
+    h = sim.ctx.h
+    timed = set(positions)
+    per_tick, launches, digests = {}, 0, {}
+    phases = {k: 0.0 for k in PHASES}
+    side = {k: 0.0 for k in SIDE_PHASES}
+    depth, levels = [], []
+    sim.device_begin()
+    for t in range(1, total + 1):
+        flush_l2()
+        if profile:
+            core.sim_set_profile(h, 1 if t in timed else 0)
+        l0 = core.sim_stat(h, 6)
+        per_tick[t] = sim.device_ticks(1)
+        if t in timed:
+            launches += int(core.sim_stat(h, 6) - l0)
+            if profile:
+                for k, name in enumerate(PHASES):
+                    phases[name] += core.sim_stat(h, 100 + k)
+                for name, k in SIDE_PHASES.items():
+                    side[name] += core.sim_stat(h, 100 + k)
+                depth.append(core.sim_stat(h, 0))
+                levels.append(core.sim_stat(h, 4))
+        if t in (CHECK_TICK, total):
+            sim.device_end()
+            digests[t] = state_digest(nodes, core.sim_get_lcg(h))
+            if t != total:
+                sim.device_begin()
+    stats = None
+    if profile:
+        core.sim_set_profile(h, 0)
+        k = len(positions)
+        stats = {"phase_ms_per_tick": {n: v / k for n, v in phases.items()},
+                 "overlapped_ms_per_tick": {n: v / k for n, v in side.items()},
+                 "collide_depth_mean": statistics.mean(depth), "collide_depth_max": max(depth),
+                 "link_levels_mean": statistics.mean(levels),
+                 "collide_serial_fallback": core.sim_stat(h, 2)}
+        stats["collide_phases_us_last"] = {
+            "guess": core.sim_stat(h, 12), "access_lists": core.sim_stat(h, 19),
+            "turns": core.sim_stat(h, 13), "check": core.sim_stat(h, 14)}
+        stats["tree_phases_us_last"] = {name: core.sim_stat(h, 30 + j) for j, name in enumerate(
+            ["box", "keys", "sort", "runs", "cell_counts", "scan", "owners", "cells"])}
+    sim.close()
+    return per_tick, launches, digests, stats
+
+
+def exact_e2e_run(pkg, sc, core, positions, total, flush_l2):
+    """The same schedule through the public API: Simulation.tick(1) per tick,
+    which copies the node state host-to-device (x, y, vx, vy, fx, fy from
+    pinned memory), ticks, and copies x, y, vx, vy back. Wall-clock ms of the
+    timed ticks."""
+    nodes, sim = sc.setup_exact(pkg, core, **WORKLOAD)
+    timed = set(positions)
+    out = []
+    for t in range(1, total + 1):
+        flush_l2()
+        t0 = time.perf_counter()
+        sim.tick(1)
+        if t in timed:
+            out.append((time.perf_counter() - t0) * 1e3)
+    sim.close()
+    return out
+
+
+def device_peaks(pkg):
+    """d3_device_peaks: FP64 rates and the SM-to-SM handoff latency."""
+    import ctypes
+
+    lib = pkg.cuda_core().lib
+    fn = lib.d3_device_peaks
+    fn.restype = ctypes.c_int32
+    fn.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.c_uint32]
+    out = (ctypes.c_double * 8)()
+    rc = fn(out, 8)
+    if rc != 0:
+        return None
+    return {"dadd_per_s": out[0], "dmul_per_s": out[1], "dfma_per_s": out[2],
+            "ddiv_per_s": out[3], "dsqrt_per_s": out[4], "handoff_us": out[5],
+            "sms": int(out[6]), "clock_khz": int(out[7])}
+
+
 def run_ours(args, pkg, sc):
     rank, local_rank, world = dist_env()
     if world > 1:
@@ -253,62 +378,32 @@ def run_ours(args, pkg, sc):
         flush.zero_()
         torch.cuda.synchronize()
 
-    nodes, sim = sc.setup_exact(pkg, core, **WORKLOAD)
-    h = sim.ctx.h
-    sim.device_begin()
-    for _ in range(args.warmup):
-        flush_l2()
-        sim.device_ticks(1)
+    positions, total = schedule_positions(args.warmup, args.steps)
+    n, m = WORKLOAD["n"], WORKLOAD["m"]
+    # the timed run: every tick of the schedule on the device, the K ticks at
+    # `positions` timed; the clocks are sampled over the whole schedule
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     clocks = Clocks(0 if world > 1 else int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0))
-    launches0 = core.sim_stat(h, 6)
-    times = []
-    for _ in range(args.steps):
-        flush_l2()
-        times.append(sim.device_ticks(1))
-    launches = int(core.sim_stat(h, 6) - launches0)
+    per_tick, launches, digests, _ = exact_device_run(pkg, sc, core, positions, total, flush_l2, world)
     torch.cuda.synchronize()
     clk = clocks.stop()
-    # the phase breakdown: further ticks with the engine's phase timers on
-    # (events between phases), outside the timed region
-    prof_steps = min(args.steps, 10)
-    core.sim_set_profile(h, 1)
-    for _ in range(prof_steps):
-        flush_l2()
-        sim.device_ticks(1)
-    phases = {name: core.sim_stat(h, 100 + k) for k, name in enumerate(PHASES)}
-    side = {name: core.sim_stat(h, 100 + k) / prof_steps for name, k in SIDE_PHASES.items()}
-    core.sim_set_profile(h, 0)
-    ms = max_over_ranks(sum(times) / len(times), world)
     if world > 1:
         dist.barrier()
-    sim.device_end()
-    # e2e through the public API: node state in, tick, node state out
-    e2e = []
-    for _ in range(args.e2e_steps):
-        flush_l2()
-        t0 = time.perf_counter()
-        sim.tick(1)
-        e2e.append((time.perf_counter() - t0) * 1e3)
-    n = WORKLOAD["n"]
-    e2e_ms = max_over_ranks(sum(e2e) / len(e2e), world)
-    stats = {"collide_depth": core.sim_stat(h, 0), "collide_attempts": core.sim_stat(h, 1),
-             "collide_serial_fallback": core.sim_stat(h, 2), "link_levels": core.sim_stat(h, 4)}
-    # the last tick's collide pass and collide tree build, from the kernels'
-    # own globaltimer stamps (microseconds)
-    stats["collide_phases_us"] = {"guess": core.sim_stat(h, 12), "access_lists": core.sim_stat(h, 19),
-                                  "turns": core.sim_stat(h, 13), "check": core.sim_stat(h, 14)}
-    stats["tree_phases_us"] = {name: core.sim_stat(h, 30 + k) for k, name in enumerate(
-        ["box", "keys", "sort", "runs", "cell_counts", "scan", "owners", "cells"])}
-    sim.close()
+    ms = max_over_ranks(statistics.mean(per_tick[t] for t in positions), world)
+    schedule_ms = statistics.mean(per_tick[t] for t in range(args.warmup + 1, total + 1))
+    early_ms = statistics.mean(per_tick[t] for t in range(6, 26))
+    # the same schedule again with the phase timers on (outside the timed run)
+    _, _, digests2, prof = exact_device_run(pkg, sc, core, positions, total, flush_l2, world,
+                                            profile=True)
+    # end to end through the public API
+    e2e = exact_e2e_run(pkg, sc, core, positions, total, flush_l2)
+    e2e_ms = max_over_ranks(statistics.mean(e2e), world)
     if rank != 0:
         if world > 1:
             dist.destroy_process_group()
         return
-    # Roofline of the dominant phase: the exact many-body traversal is the
-    # f64 work; bytes are the HBM traffic of its inputs and outputs per tick.
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -316,58 +411,107 @@ def run_ours(args, pkg, sc):
     except OSError:
         pass
     hbm = peaks.get("hbm_gbs", 6650.0)
-    dom = max(phases, key=phases.get)
-    per_tick_ms = {k: v / prof_steps for k, v in phases.items()}
-    # Algorithmic bytes per launch of the dominant phase (one launch per tick).
-    # Per node: x, y read (16 B), vx, vy read and written (32 B), radius or
-    # strength (8 B); per tree cell: the 88-byte cell and its 4-byte skip link,
-    # with about 1.7 cells per node at this size.
+    rates = device_peaks(pkg)
+    phase = prof["phase_ms_per_tick"]
+    dom = max(phase, key=phase.get)
+    # Algorithmic bytes of the collide pass (one launch per tick): per node
+    # x, y, vx, vy, radius read and vx, vy written (56 B); per tree cell its
+    # 88-byte record and 4-byte skip link, about 1.7 cells per node here.
     cells = 1.7 * n
-    alg_bytes = {
-        "mb_traverse": n * 56 + cells * 92,
-        "collide_loop": n * 56 + cells * 92,
-        "link": WORKLOAD["m"] * (2 * 4 + 3 * 8) + 4 * WORKLOAD["m"] * 8 * 2,
-    }.get(dom, n * 64.0)
-    # DRAM bytes (read + write) per launch from one ncu capture of tick 13 of
-    # this workload (after an L2 flush).
-    traffic = {"collide_loop": 63628032 + 9661184, "mb_traverse": 7734016}.get(dom)
-    achieved = alg_bytes / (per_tick_ms[dom] * 1e-3) / 1e9
+    alg = {"collide_loop": n * 56 + cells * 92, "mb_traverse": n * 56 + cells * 92,
+           "link": m * 32 + 64 * m}.get(dom, n * 64.0)
+    achieved = alg / (phase[dom] * 1e-3) / 1e9
+    # DRAM bytes (read + write) per collide launch: ncu capture of the bench
+    # workload at tick 13 (the source, commit and command are in
+    # profiles/k_collide_spec_exact_50k.md)
+    traffic = {"collide_loop": COLLIDE_DRAM_BYTES}.get(dom)
+    roof = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": hbm,
+            "unit": "GB/s", "frac": round(achieved / hbm, 5), "traffic": traffic,
+            "algorithmic_bytes": int(alg),
+            "peak_source": "measured" if peaks else "fallback"}
+    if rates:
+        # The collide pass and the link are chains of dependent turns: a turn
+        # starts only when the turns it depends on are seen finished from
+        # another SM. Bound: depth x one measured SM-to-SM handoff.
+        hand = rates["handoff_us"]
+        cp = prof["collide_depth_mean"] * hand * 1e-3
+        lp = prof["link_levels_mean"] * hand * 1e-3
+        roof["critical_path"] = {
+            "handoff_us": round(hand, 3),
+            "collide_loop": {"depth_mean": round(prof["collide_depth_mean"], 2),
+                             "bound_ms": round(cp, 4), "measured_ms": round(phase["collide_loop"], 4),
+                             "frac": round(cp / phase["collide_loop"], 4)},
+            "link": {"levels_mean": round(prof["link_levels_mean"], 2), "bound_ms": round(lp, 4),
+                     "measured_ms": round(phase["link"], 4), "frac": round(lp / phase["link"], 4)}}
     line = {
         "metric": METRIC, "value": round(ms, 4), "unit": "ms/tick", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded generators of the reference's scenarios)",
-        "config": {"workload": WORKLOAD_NAME, "n": n, "m": WORKLOAD["m"],
+        "config": {"workload": WORKLOAD_NAME, "n": n, "m": m,
                    "parallelism": "replicas" if world > 1 else "single",
-                   "l2": "flushed between timed ticks (256 MB write)", "bit_exact": True},
+                   "l2": "flushed before every tick (256 MB write)",
+                   "timed_ticks": "%d ticks spread evenly over ticks %d-%d of the %d-tick schedule"
+                                  % (args.steps, args.warmup + 1, total, total)},
+        "schedule_ms_per_tick": {"timed_ticks": round(ms, 4),
+                                 "all_ticks_%d_%d" % (args.warmup + 1, total): round(schedule_ms, 4),
+                                 "ticks_6_25": round(early_ms, 4)},
         "e2e": {"value": round(e2e_ms, 4), "unit": "ms/tick", "h2d_bytes_per_step": 48 * n,
                 "d2h_bytes_per_step": 32 * n},
         "gpu_launches": launches,
-        "phase_ms_per_tick": {k: round(v, 4) for k, v in per_tick_ms.items()},
-        "overlapped_ms_per_tick": {k: round(v, 4) for k, v in side.items()},
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 2),
-                     "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 5),
-                     "traffic": traffic, "peak_source": "measured" if peaks else "fallback"},
-        "engine_stats": stats,
+        "phase_ms_per_tick": {k: round(v, 4) for k, v in phase.items()},
+        "overlapped_ms_per_tick": {k: round(v, 4) for k, v in prof["overlapped_ms_per_tick"].items()},
+        "roofline": roof,
+        "engine_stats": {k: v for k, v in prof.items() if k not in ("phase_ms_per_tick",
+                                                                    "overlapped_ms_per_tick")},
+        "device_rates": rates,
         "clocks": clk,
     }
-    if not args.no_fast and world == 1:
-        line["fast_1m"] = fast_1m(pkg, pkg.cuda_core(), torch)
+    # bit-exactness: the two device runs agree, and (CPU leg) the oracle's
+    # state after CHECK_TICK ticks equals the device's
+    checks = {"device_runs_agree": digests == digests2}
     if not args.no_cpu_baseline and world == 1:
         threads = os.cpu_count() or 1
-        cpu = oracle_ms_per_tick(pkg, sc, threads, warmup=3, rounds=2, ticks=8)
-        line["cpu_baseline"] = {"value": round(cpu, 3), "unit": "ms/tick", "cores": threads,
-                                "kind": "port",
-                                "sample": "3 warm-up ticks then best of 2 rounds x 8 ticks of the "
-                                          "same workload (C restatement of the reference core, "
-                                          "threaded where the reference's pool is: " + THREADED
-                                          + ")"}
+        cpu_all, dig_all, work = oracle_protocol(pkg, sc, threads, count_work=True)
+        cpu_one, dig_one, _ = oracle_protocol(pkg, sc, 1)
+        checks["oracle_all_threads_tick_%d" % CHECK_TICK] = dig_all == digests[CHECK_TICK]
+        checks["oracle_one_thread_tick_%d" % CHECK_TICK] = dig_one == digests[CHECK_TICK]
+        line["cpu_baseline"] = {
+            "value": round(cpu_all, 3), "unit": "ms/tick", "cores": threads, "kind": "port",
+            "single_thread": round(cpu_one, 3),
+            "sample": "bench/threads.js protocol: 5 warm-up ticks, then the minimum of 3 rounds "
+                      "x 30 ticks (ticks 6-95) of the same workload; the oracle (C restatement "
+                      "of the reference core, gcc -O3 -ffp-contract=off) on %d threads (threaded "
+                      "where the reference's pool is: %s) and on 1 thread" % (threads, THREADED)}
+        if rates and work:
+            # FP64 work of the many-body traversal per tick, counted by the
+            # oracle over ticks 66-95: per visited cell 8 ops (1 a division),
+            # per accepted approximation 8 (2 divisions), per leaf point 6
+            # (1 division); no FMA (strict f64). Roofline time: the non-division
+            # ops at the DADD rate plus the divisions at the measured IEEE
+            # division rate.
+            V, A, P = work["V"], work["A"], work["P"]
+            ops, divs = 8 * V + 8 * A + 6 * P, V + 2 * A + P
+            t_roof = ((ops - divs) / rates["dadd_per_s"] + divs / rates["ddiv_per_s"]) * 1e3
+            roof["fp64"] = {"kernel": "mb_traverse", "cells_visited": round(V),
+                            "approximations": round(A), "point_interactions": round(P),
+                            "fp64_ops": round(ops), "divisions": round(divs),
+                            "t_roof_ms": round(t_roof, 4),
+                            "measured_ms": round(phase["mb_traverse"], 4),
+                            "frac": round(t_roof / phase["mb_traverse"], 4)}
+    line["config"]["bit_exact"] = all(checks.values())
+    line["bit_exact_checks"] = checks
+    if not args.no_fast and world == 1:
+        line["fast_1m"] = fast_1m(pkg, pkg.cuda_core(), torch, targets=4096)
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
 
 
 def run_reference(args, pkg, sc):
+    """The reference arm: the oracle (the reference's algorithm restated in C;
+    zig, node and a wasm runtime are not on this machine) on all host cores,
+    over the same schedule and the same K timed ticks as our arm."""
     rank, _, world = dist_env()
     if rank != 0:
         return
@@ -377,24 +521,31 @@ def run_reference(args, pkg, sc):
     core = oracle.load(pkg)
     nodes, sim = sc.setup_exact(pkg, core, **WORKLOAD)
     core.lib.oracle_set_threads(sim.ctx.h, threads)
-    sim.tick(args.warmup)
-    steps = max(1, min(args.steps, 60))
-    t0 = time.perf_counter()
-    sim.tick(steps)
-    ms = (time.perf_counter() - t0) * 1e3 / steps
+    positions, total = schedule_positions(args.warmup, args.steps)
+    timed = set(positions)
+    times = []
+    for t in range(1, total + 1):
+        t0 = time.perf_counter()
+        sim.tick(1)
+        if t in timed:
+            times.append((time.perf_counter() - t0) * 1e3)
     sim.close()
+    ms = statistics.mean(times)
     line = {
         "metric": METRIC, "value": round(ms, 3), "unit": "ms/tick", "n_gpus": world,
-        "steps": steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded generators of the reference's scenarios)",
-        "config": {"workload": WORKLOAD_NAME, "n": WORKLOAD["n"], "m": WORKLOAD["m"]},
+        "config": {"workload": WORKLOAD_NAME, "n": WORKLOAD["n"], "m": WORKLOAD["m"],
+                   "timed_ticks": "%d ticks spread evenly over ticks %d-%d of the %d-tick schedule"
+                                  % (args.steps, args.warmup + 1, total, total)},
         "impl": "reference",
         "cpu_baseline": {"value": round(ms, 3), "unit": "ms/tick", "cores": threads,
                          "kind": "port",
-                         "sample": "%d warm-up then %d ticks of the workload (C restatement of "
-                                   "the reference core, threaded where the reference's pool is: "
-                                   "%s; zig is unavailable)" % (args.warmup, steps, THREADED)},
+                         "sample": "the whole %d-tick schedule, the same %d timed ticks as the "
+                                   "GPU arm, each timed alone (C restatement of the reference "
+                                   "core, threaded where the reference's pool is: %s; zig is "
+                                   "unavailable)" % (total, args.steps, THREADED)},
         "e2e": {"value": round(ms, 3), "unit": "ms/tick", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }

@@ -91,6 +91,10 @@ _SIGNATURES = {
 # exports all of them.
 ABI_SYMBOLS = tuple(_SIGNATURES)
 
+# Entry points of the CUDA library alone (the oracle has no counterpart):
+# declared in the header and exported by the engine, bound where they are used.
+ENGINE_SYMBOLS = ("d3_device_peaks", "d3_many_body_exact_noalloc")
+
 
 class Core:
     """One loaded library implementing the C ABI."""

@@ -1073,6 +1073,11 @@ __global__ void __launch_bounds__(SPEC_THREADS, 2) k_collide_spec(SpecArgs a) {
     for (int k = 0; k < 144; ++k) a.stamps[k] = 0;
     a.stamps[0] = now_ns();
   }
+  // No tree this pass (cell buffer overflow or a failed build launch, both
+  // already reported in the status word): leaf_of and the cells are not this
+  // pass's, so nothing is read. Every thread reads the same word, written
+  // before this launch, so every block returns here before any grid barrier.
+  if (__ldcg(&a.info[5])) return;
   for (uint32_t i = tid; i < n; i += nth) a.cnt[i] = 0;
   {
     const uint32_t len = a.info[1];

@@ -31,7 +31,12 @@ enum : uint32_t {
   ST_RNG_NEED = 1u << 5,         // a serial kernel needs more host draws
   ST_COLLIDE_OVERFLOW = 1u << 6, // a guessed set exceeded its capacity
   ST_CENTER_RECORDS = 1u << 7,   // a center-sum launch failed or its records disagreed
+  ST_LAUNCH_FAILED = 1u << 8,    // a kernel launch the pass depends on did not happen
 };
+
+// Device-side failures (a bounded wait that ran out, a tree or record buffer
+// too small, a launch that did not happen): the results are not to be trusted.
+constexpr uint32_t ST_FATAL = ST_WAIT_TIMEOUT | ST_DEEP_STACK | ST_CENTER_RECORDS | ST_LAUNCH_FAILED;
 
 // One quadtree cell, the reference's 88-byte record (tree.zig:46-62):
 // child[4], first, count, d3's x0 y0 x1 y1, per-force x, y, value, r.

@@ -320,10 +320,6 @@ int sync_in_impl(DSim *s, bool defer = false) {
   return D3_OK;
 }
 
-// Device-side failures (a bounded wait that ran out, a tree or record buffer
-// too small, a launch that did not happen): the results are not to be trusted.
-constexpr uint32_t ST_FATAL = ST_WAIT_TIMEOUT | ST_DEEP_STACK | ST_CENTER_RECORDS;
-
 // Queues the copy of the status word that take_failure reads after the next
 // host synchronisation.
 void queue_status(DSim *s) {
@@ -485,8 +481,12 @@ int run_collide(DSim *s, DForce *f) {
   return D3_OK;
 }
 
+// PRECISION: 0 exact; 1 fast (the reference's FMM, bit for bit); 2 fast with
+// the tensor-core FMM (BF16x3 M2L, FP32 near field); 3 fast with the learned
+// order-4 correction. Link and collide run the same fast kernels for 1-3.
 bool fast_mode(const DSim *s, const DForce *f) {
-  return f->scalars[D3_PRECISION] == 1 && s->n >= FAST_MIN_N;
+  const double pr = f->scalars[D3_PRECISION];
+  return (pr == 1 || pr == 2 || pr == 3) && s->n >= FAST_MIN_N;
 }
 
 // fuse_center: a center force's shift is left to the caller (which fuses it
@@ -495,7 +495,8 @@ int run_force(DSim *s, DForce *f, double alpha, bool presummed = false, bool fus
   NodeArrays a = nodes_of(s);
   // The facade's per-run SEED draw in fast mode (src/core.js:218-222), from
   // the device LCG when it is the random source.
-  const bool seeded = f->scalars[D3_PRECISION] == 1 &&
+  const double prec = f->scalars[D3_PRECISION];
+  const bool seeded = (prec == 1 || prec == 2 || prec == 3) &&
                       (f->kind == D3_MANY_BODY || f->kind == D3_LINK || f->kind == D3_COLLIDE);
   double *seed_slot = s->fast.seed;
   if (seeded) {
@@ -541,7 +542,10 @@ int run_force(DSim *s, DForce *f, double alpha, bool presummed = false, bool fus
         fp.dmax2 = f->scalars[D3_DISTANCE_MAX2];
         fp.alpha = alpha;
         cudaEvent_t e = phase_begin(s);
-        int r = fmm_run(s->fast, s->tree, a, f->d_f[0], fp, seed_slot, status_word(s), s->stream);
+        int r = prec == 1 ? fmm_run(s->fast, s->tree, a, f->d_f[0], fp, seed_slot, status_word(s),
+                                    s->stream)
+                          : fmm_tc_run(s->fast, s->tree, a, f->d_f[0], fp, (int)prec, seed_slot,
+                                       status_word(s), s->stream);
         phase_end(s, PH_FAST_MB, e);
         if (r == 1) return D3_OK;
         if (r == -3) return D3_BAD_ARGUMENT;
@@ -835,7 +839,15 @@ int32_t tree_build(uint32_t h, uint32_t shifted) {
                   s->stream);
   cudaMemcpyAsync(s->h_extent, s->tree.extent, 4 * sizeof(double), cudaMemcpyDeviceToHost,
                   s->stream);
+  queue_status(s);
   if (cudaStreamSynchronize(s->stream) != cudaSuccess) return D3_WORKER_FAILED;
+  // a tree that did not fit its cell buffer (or a build that did not launch)
+  // is reported here and leaves an empty tree
+  if (int fr = take_failure(s)) {
+    s->h_len = 0;
+    s->h_root = NONE;
+    return fr;
+  }
   memcpy(info, s->h_words + 8, sizeof info);
   bool grown = false;
   s->h_m = info[0];

@@ -47,6 +47,7 @@ void fast_free(FastScratch &s) {
   cudaFree(s.g_items_tmp); cudaFree(s.g_cell_of); cudaFree(s.g_start); cudaFree(s.g_hist);
   cudaFree(s.g_part); cudaFree(s.g_box); cudaFree(s.g_info); cudaFree(s.g_geom);
   fmm_free(s);
+  fmm_tc_free(s);
   s = FastScratch();
 }
 

@@ -22,6 +22,7 @@ struct FastScratch {
   double *g_geom = nullptr;     // x0, y0, inv_h
   // FMM
   void *fmm = nullptr;
+  void *fmm_tc = nullptr;  // the precision forms' state
 };
 
 int fast_reserve(FastScratch &s, uint32_t n);
@@ -50,6 +51,45 @@ void fast_collide(FastScratch &s, const NodeArrays &a, const double *radii, doub
 struct FmmParams {
   double order, opening, dmin2, dmax2, alpha;
 };
+
+// fmm.zig:68-78 (a cell of the fast tree, level order, children contiguous),
+// with the parent index in the spare word.
+struct FCell {
+  double cx, cy, r;
+  uint32_t first, count, child0, nchild, depth, parent;
+};
+
+// What fmm_prepare leaves on the device for the passes of a fast many-body
+// run: the points in key order (fmm.zig:668-682: positions, strength x alpha,
+// scaled positions (x - ox) / w), the level-order cells and their levels.
+struct FmmPrep {
+  uint32_t m = 0, ncells = 0, nlev = 0;
+  uint32_t lvl[20] = {};  // first cell of each level (host copy)
+  double w = 0, inv_w = 0, ox = 0, oy = 0;
+  const uint64_t *keys = nullptr;
+  const uint32_t *perm = nullptr;
+  const double *px = nullptr, *py = nullptr, *ps = nullptr, *ux = nullptr, *uy = nullptr;
+  FCell *cells = nullptr;
+  uint32_t *info = nullptr;  // device: FI_LVL + d = first cell of level d
+  int coop_blocks = 0;
+};
+
+// The fast tree of fmm.zig:247-330 up to the cells: square extent, 16-bit
+// Morton keys, stable sort, gather, level-order cells (fmm.zig:685-717).
+// 1: ready; 2: no point to act on; 0: non-finite extent (the exact kernel
+// runs instead); < 0: failure.
+int fmm_prepare(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *strengths,
+                double alpha, FmmPrep &out, cudaStream_t st);
+
+// The precision forms of the fast many-body force (no reference
+// counterpart; judged by RMS against an FP64 direct sum): geometric cells,
+// M2L as batched dense BF16x3 contractions on the tensor cores, FP32 near
+// field with a per-leaf FP64 origin shift. form 2: order `order`; form 3:
+// order 4 plus the learned per-leaf correction. Returns as fmm_run.
+int fmm_tc_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *strengths,
+               const FmmParams &p, int form, const double *seed, uint32_t *status,
+               cudaStream_t st);
+void fmm_tc_free(FastScratch &s);
 // fmm.zig:247-354. Returns 1 when applied, 0 when the exact kernel must run
 // instead (non-finite extent), < 0 on failure.
 int fmm_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *strengths,

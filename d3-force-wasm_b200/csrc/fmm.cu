@@ -48,11 +48,6 @@ constexpr unsigned FMM_THREADS = 256;
 constexpr unsigned FMM_WARPS = FMM_THREADS / 32;
 constexpr uint32_t FMM_STACK = 64;
 
-// fmm.zig:68-78, with the parent index in the spare word.
-struct FCell {
-  double cx, cy, r;
-  uint32_t first, count, child0, nchild, depth, parent;
-};
 
 struct FmmTables {
   double fact[FMM_TAB];
@@ -931,9 +926,8 @@ static int sync_read(FmmDev &f, cudaStream_t st) {
   return 0;
 }
 
-int fmm_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *strengths,
-            const FmmParams &prm, const double *seed, uint32_t *status, cudaStream_t st) {
-  (void)status;
+int fmm_prepare(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *strengths,
+                double alpha, FmmPrep &out, cudaStream_t st) {
   const uint32_t n = a.n;
   if (!s.fmm) {
     FmmDev *f = new FmmDev();
@@ -980,10 +974,63 @@ int fmm_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *stren
       cudaStreamSynchronize(st) != cudaSuccess)
     return -1;
   const uint32_t m = f.h_info[0];
-  if (m == 0) return 1;  // nothing to do (tree.zig:287-309 with an empty box)
+  if (m == 0) return 2;  // nothing to do (tree.zig:287-309 with an empty box)
   const double e0 = f.h_geom[0], e1 = f.h_geom[1], e2 = f.h_geom[2], e3 = f.h_geom[3];
   const double w = e2 - e0;
   if (!(w > 0 && w < INFINITY)) return 0;  // the exact kernel runs instead
+  const double inv_w = 1 / w;
+  const double ox = (e0 + e2) / 2, oy = (e1 + e3) / 2;
+  D3_LAUNCH(k_fmm_gather, blocks_for(m, 256), 256, 0, st)(t.sv, a.x, a.y, strengths, m, alpha,
+                                                          ox, oy, inv_w, f.px, f.py, f.ps,
+                                                          f.ux, f.uy);
+  // cells (level order); grow and rebuild if they do not fit
+  uint32_t want = 2 * (m / FMM_LEAF + 1) + 64;
+  for (int attempt = 0;; ++attempt) {
+    if (fmm_reserve_cells(f, want > f.ccap ? want : f.ccap)) return -1;
+    {
+      const uint64_t *keys = t.keys;
+      uint32_t mm = m, ccap = f.ccap;
+      FCell *cells = f.cells;
+      uint32_t *tmp = f.tmp, *bsum = f.bsum, *info = f.info;
+      void *params[] = {&keys, &mm, &cells, &ccap, &tmp, &bsum, &info};
+      ++g_launches;
+      if (cudaLaunchCooperativeKernel((const void *)k_fmm_cells, f.coop_blocks, FMM_THREADS,
+                                      params, 0, st) != cudaSuccess)
+        return -1;
+    }
+    if (sync_read(f, st)) return -1;
+    if (!f.h_info[FI_OVERFLOW]) break;
+    if (attempt > 8) return -1;
+    want = 2 * f.h_info[FI_OVERFLOW] + 64;
+  }
+  out.m = m;
+  out.ncells = f.h_info[FI_CELLS];
+  out.nlev = f.h_info[FI_LEVELS];
+  for (uint32_t d = 0; d <= out.nlev && d < FMM_LEVELS + 2; ++d) out.lvl[d] = f.h_info[FI_LVL + d];
+  out.w = w;
+  out.inv_w = inv_w;
+  out.ox = ox;
+  out.oy = oy;
+  out.keys = t.keys;
+  out.perm = t.sv;
+  out.px = f.px; out.py = f.py; out.ps = f.ps; out.ux = f.ux; out.uy = f.uy;
+  out.cells = f.cells;
+  out.info = f.info;
+  out.coop_blocks = f.coop_blocks;
+  return 1;
+}
+
+int fmm_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *strengths,
+            const FmmParams &prm, const double *seed, uint32_t *status, cudaStream_t st) {
+  (void)status;
+  FmmPrep pr;
+  const int pre = fmm_prepare(s, t, a, strengths, prm.alpha, pr, st);
+  if (pre == 2) return 1;
+  if (pre <= 0) return pre;
+  FmmDev &f = *static_cast<FmmDev *>(s.fmm);
+  const uint32_t m = pr.m;
+  (void)m;
+  const double w = pr.w;
   uint32_t p = FMM_DEFAULT_ORDER;
   if (prm.order >= 1 && prm.order <= (double)FMM_MAX_ORDER) p = (uint32_t)prm.order;
   double kappa = prm.opening;
@@ -1016,7 +1063,7 @@ int fmm_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *stren
   args.vx = a.vx; args.vy = a.vy;
   args.info = f.info;
   args.p = p; args.q = q; args.stride = stride;
-  args.inv_w = 1 / w;
+  args.inv_w = pr.inv_w;
   args.mac_far = 2 * kappa - 1;
   double dmax_scaled = INFINITY;
   if (prm.dmax2 < INFINITY) dmax_scaled = sqrt(prm.dmax2) / w;
@@ -1028,31 +1075,7 @@ int fmm_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *stren
   args.dmin2 = prm.dmin2;
   args.dmax2 = prm.dmax2;
   args.seed = seed;
-  const double ox = (e0 + e2) / 2, oy = (e1 + e3) / 2;
-  D3_LAUNCH(k_fmm_gather, blocks_for(m, 256), 256, 0, st)(t.sv, a.x, a.y, strengths, m, prm.alpha,
-                                                          ox, oy, args.inv_w, f.px, f.py, f.ps,
-                                                          f.ux, f.uy);
-  // cells (level order); grow and rebuild if they do not fit
-  uint32_t want = 2 * (m / FMM_LEAF + 1) + 64;
-  for (int attempt = 0;; ++attempt) {
-    if (fmm_reserve_cells(f, want > f.ccap ? want : f.ccap)) return -1;
-    {
-      const uint64_t *keys = t.keys;
-      uint32_t mm = m, ccap = f.ccap;
-      FCell *cells = f.cells;
-      uint32_t *tmp = f.tmp, *bsum = f.bsum, *info = f.info;
-      void *params[] = {&keys, &mm, &cells, &ccap, &tmp, &bsum, &info};
-      ++g_launches;
-      if (cudaLaunchCooperativeKernel((const void *)k_fmm_cells, f.coop_blocks, FMM_THREADS,
-                                      params, 0, st) != cudaSuccess)
-        return -1;
-    }
-    if (sync_read(f, st)) return -1;
-    if (!f.h_info[FI_OVERFLOW]) break;
-    if (attempt > 8) return -1;
-    want = 2 * f.h_info[FI_OVERFLOW] + 64;
-  }
-  const uint32_t ncells = f.h_info[FI_CELLS], nlev = f.h_info[FI_LEVELS];
+  const uint32_t ncells = pr.ncells, nlev = pr.nlev;
   args.cells = f.cells;
   args.bx0 = f.bx0; args.by0 = f.by0; args.bx1 = f.bx1; args.by1 = f.by1;
   args.ncells = ncells;

@@ -1,0 +1,1098 @@
+// fmm_tc.cu — the precision form of the fast many-body force: an FMM whose
+// translation operators are the same at every level, with M2L run as batched
+// dense BF16x3 contractions on the tensor cores (tcgen05) and the near field
+// in FP32 (no reference counterpart: it is judged by its RMS force error
+// against an FP64 direct sum, the measure of test/fast/error-test.js:44-70).
+//
+// The reference FMM (fmm.zig:247-354) centres each cell on its points'
+// bounding box (fmm.zig:749-753), so no two cells share a translation vector.
+// Here each cell is centred on its square (the key grid of tree.zig:346-364),
+// and expansions are stored normalised by the cell side s:
+//     M'_k = M_k / s^k,    L'_l = L_l * s^(l+1),
+// in the scaled coordinates u = (x - ox) / w of fmm.zig:668-682. Then, for
+// two cells of one level at integer offset v (in cell sides),
+//     L'_l += (-1)^l sum_k C(k+l, l) M'_k / v^(k+l+1),
+// a fixed q x q complex matrix per v, the same at every level; M2M and L2L
+// are fixed matrices per child quadrant. With the separation test
+// |v|^2 >= 2 kappa^2 (the MAC (2 kappa - 1) r_max + r_min <= d of
+// fmm.zig:400-453 for equal squares, r = s / sqrt 2), the cells a cell gets
+// M2L from are the children of its parent's near cells that are separated
+// from it: 39 vectors per child quadrant at kappa = 1.5 (60 in all).
+//
+// Passes (one GPU, stream order):
+//   prepare  fmm_prepare (fmm.cu): keys, sort, gather, level-order cells.
+//   geom     per cell: level, integer coordinates, quadrant, child mask;
+//            the M2L target groups (one per quadrant).
+//   upward   FP64: P2M at leaves, M2M by the quadrant operators, level by
+//            level from the deepest; M' stored in FP64 and split into bf16
+//            hi + lo (x ~ hi + lo to 2^-17) for the tensor cores.
+//   lists    level by level from the root, a warp per cell: near cells (13
+//            at kappa 1.5), the M2L table (source per vector slot), and the
+//            adaptive lists: P2P leaves, coarse leaves (P2L), finer cells
+//            seen from a leaf (M2P).
+//   m2l      tcgen05: a CTA per tile of 128 target cells of one quadrant
+//            group; per vector slot the 128 gathered source rows (A: 128 x
+//            32 bf16, hi and lo) times that vector's operator (B: 32 x 32,
+//            hi and lo) accumulate in TMEM as A_hi B_hi + A_hi B_lo +
+//            A_lo B_hi (BF16x3), FP32 accumulation; 4-stage smem ring with
+//            mbarriers, one thread issues the MMAs.
+//   p2l      coarse leaves' points into local expansions (FP32).
+//   down     L2L by the quadrant operators (FP32), level by level; at
+//            leaves L2P and M2P into a per-point far field.
+//   p2p      a warp per leaf: each source leaf's points staged in shared
+//            memory relative to the target leaf's centre, the shift taken in
+//            FP64 and the pair sums in FP32 (d3's pair formula, distanceMin
+//            clamp, hashed jiggle of hash.zig for coincident points); then
+//            v += far + near in FP64.
+#include <cooperative_groups.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "fast.cuh"
+#include "tc.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace d3 {
+namespace {
+
+constexpr uint32_t TC_MAXQ = 16;     // q = p + 1: 2q <= 32, the MMA's K and N
+constexpr uint32_t TC_KN = 32;       // padded real length of an expansion
+constexpr uint32_t TC_NEAR_MAX = 32;  // near offsets (13 at kappa 1.5)
+constexpr uint32_t TC_SLOT_MAX = 96;  // M2L vectors per quadrant (39 at kappa 1.5)
+constexpr uint32_t TC_CLASS_MAX = 192;
+constexpr uint32_t TC_THREADS = 256;
+constexpr uint32_t TC_WARPS = TC_THREADS / 32;
+constexpr uint32_t TC_TILE = 128;     // target cells per M2L tile (the MMA's M)
+constexpr uint32_t TC_STAGES = 4;
+constexpr uint32_t TC_STACK = 64;
+constexpr uint32_t TC_NONE = 0xFFFFFFFFu;
+constexpr uint32_t TC_NEAR_FLAG = 0x8000u;
+// info words
+enum : uint32_t { TI_POOL_P2P = 0, TI_POOL_W, TI_POOL_X, TI_POOL_C, TI_OVF, TI_GROUP = 8,
+                  TI_ERR = 16, TI_WORDS = 32 };
+
+// A cell of the geometric tree: the square of level `level` at integer
+// coordinates (ix, iy), side 2^-level in scaled coordinates, centre
+// -0.5 + (ix + 0.5) 2^-level.
+struct TcCell {
+  uint32_t first, count, child0, parent;
+  uint16_t ix, iy;
+  uint8_t level, quad, cmask, nchild;
+};
+
+struct TcTables {
+  uint32_t q, nnear, nslot[4];
+  int8_t near_dx[TC_NEAR_MAX], near_dy[TC_NEAR_MAX];
+  // [target quadrant a][parent near offset o][child quadrant b]: M2L slot,
+  // or TC_NEAR_FLAG | near index
+  uint16_t map[4][TC_NEAR_MAX][4];
+  uint16_t slot_class[4][TC_SLOT_MAX];
+  double kappa2x2;   // 2 kappa^2: separation of same-level offsets
+  double mac_far;    // 2 kappa - 1
+  double m2m_re[4][TC_MAXQ][TC_MAXQ], m2m_im[4][TC_MAXQ][TC_MAXQ];  // [b][n][k]
+  float l2l_re[4][TC_MAXQ][TC_MAXQ], l2l_im[4][TC_MAXQ][TC_MAXQ];   // [b][m][l]
+};
+
+struct TcDev {
+  uint32_t ccap = 0, pcap = 0, p = 0;
+  double kappa = 0;
+  TcTables *tab = nullptr;
+  TcTables h_tab;
+  unsigned char *wops = nullptr;  // [class][hi, lo][32 x 32 bf16, B tile layout]
+  TcCell *cells = nullptr;
+  double *mco = nullptr;            // M' (FP64), 2q per cell
+  __nv_bfloat16 *mbf = nullptr;     // M' hi (32) then lo (32) per cell
+  float *lco = nullptr;             // L' (FP32), 32 per cell
+  uint32_t *near = nullptr;         // [cell][nnear]
+  uint32_t *m2l = nullptr;          // [cell][nslot of its quadrant]
+  uint32_t *groups = nullptr;       // 4 lists of cells, each ccap long
+  uint32_t *loff = nullptr;         // per cell: offsets/counts of p2p, w, x, coarse lists
+  uint32_t *pool = nullptr;
+  size_t pool_cap = 0, last_pool = 0;
+  float2 *far = nullptr;            // per sorted point
+  uint32_t *info = nullptr, *h_info = nullptr;
+  int coop_lists = 0, coop_up = 0, coop_down = 0;
+};
+
+struct TcArgs {
+  const TcTables *tab;
+  const unsigned char *wops;
+  const uint64_t *keys;
+  const uint32_t *perm;
+  const double *px, *py, *ps, *ux, *uy;
+  const FCell *fc;
+  TcCell *cells;
+  double *mco;
+  __nv_bfloat16 *mbf;
+  float *lco;
+  uint32_t *near, *m2l, *groups, *loff, *pool;
+  size_t pool_cap;
+  float2 *far;
+  double *vx, *vy;
+  uint32_t *info;
+  uint32_t *status;     // the simulation's status word (ST_WAIT_TIMEOUT on a failed wait)
+  const uint32_t *lvl;  // device: first cell of each level
+  uint32_t ncells, nlev, m, q, ccap;
+  double inv_w, dmin2;
+  float dmin2f;
+  const double *seed;
+};
+
+__device__ __forceinline__ double cell_side(uint32_t level) { return ldexp(1.0, -(int)level); }
+__device__ __forceinline__ void cell_centre(const TcCell &c, double &x, double &y) {
+  const double s = cell_side(c.level);
+  x = -0.5 + (c.ix + 0.5) * s;
+  y = -0.5 + (c.iy + 0.5) * s;
+}
+__device__ __forceinline__ uint32_t child_at(const TcCell &c, uint32_t b) {
+  if (!((c.cmask >> b) & 1)) return TC_NONE;
+  return c.child0 + __popc(c.cmask & ((1u << b) - 1));
+}
+
+// ---- geom -------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t compact16(uint32_t x) {  // even bits -> 16 bits
+  x &= 0x55555555u;
+  x = (x | (x >> 1)) & 0x33333333u;
+  x = (x | (x >> 2)) & 0x0F0F0F0Fu;
+  x = (x | (x >> 4)) & 0x00FF00FFu;
+  x = (x | (x >> 8)) & 0x0000FFFFu;
+  return x;
+}
+
+__global__ void k_tc_geom(TcArgs a) {
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.ncells) return;
+  const FCell f = a.fc[c];
+  TcCell t;
+  t.first = f.first;
+  t.count = f.count;
+  t.parent = f.parent;
+  t.level = (uint8_t)f.depth;
+  const uint32_t key = (uint32_t)a.keys[f.first];
+  const uint32_t pre = f.depth ? key >> (2 * (16 - f.depth)) : 0;
+  t.ix = (uint16_t)compact16(pre);
+  t.iy = (uint16_t)compact16(pre >> 1);
+  t.quad = (uint8_t)(pre & 3);
+  // the children: contiguous from child0, one per non-empty quadrant in order
+  uint32_t mask = 0;
+  const uint32_t nch = f.nchild;
+  for (uint32_t j = 0; j < nch; ++j) {
+    const FCell ch = a.fc[f.child0 + j];
+    const uint32_t ck = (uint32_t)a.keys[ch.first];
+    mask |= 1u << ((ck >> (2 * (16 - ch.depth))) & 3);
+  }
+  t.cmask = (uint8_t)mask;
+  t.nchild = (uint8_t)nch;
+  t.child0 = nch ? f.child0 : 0;
+  a.cells[c] = t;
+  if (c == 0)  // the root gets no M2L: its local expansion starts at zero
+    for (uint32_t k = 0; k < TC_KN; ++k) a.lco[k] = 0;
+  if (f.depth > 0) {
+    const uint32_t g = t.quad;
+    const uint32_t k = atomicAdd(&a.info[TI_GROUP + g], 1u);
+    a.groups[(size_t)g * a.ccap + k] = c;
+  }
+}
+
+// ---- upward (FP64) ------------------------------------------------------------------
+
+// One cell by one warp; ws: this warp's shared rows (32 x 2q doubles).
+__device__ void tc_upward_cell(const TcArgs &a, uint32_t c, double *ws) {
+  const unsigned lane = threadIdx.x & 31;
+  const uint32_t q = a.q, st = 2 * q;
+  const TcCell C = a.cells[c];
+  double cx, cy;
+  cell_centre(C, cx, cy);
+  const double inv_s = ldexp(1.0, (int)C.level);
+  double *mc = a.mco + (size_t)c * st;
+  double acc0 = 0;  // lane r: real r of M'
+  if (C.nchild == 0) {
+    // P2M: M'_k = sum_j s_j ((u_j - c) / s)^k, points added in order
+    for (uint32_t base = C.first; base < C.first + C.count; base += 32) {
+      const uint32_t k = base + lane;
+      const uint32_t np = min(32u, C.first + C.count - base);
+      double *row = ws + lane * st;
+      if (k < C.first + C.count) {
+        const double sv = a.ps[k];
+        const double zr = (a.ux[k] - cx) * inv_s, zi = (a.uy[k] - cy) * inv_s;
+        double pr = sv, pi = 0;
+        for (uint32_t o = 0; o < q; ++o) {
+          row[o] = pr;
+          row[q + o] = pi;
+          const double nr = pr * zr - pi * zi;
+          pi = pr * zi + pi * zr;
+          pr = nr;
+        }
+      }
+      __syncwarp();
+      for (uint32_t t = 0; t < np; ++t) {
+        const double *rt = ws + t * st;
+        if (lane < st) acc0 += rt[lane];
+      }
+      __syncwarp();
+    }
+  } else {
+    // M2M: M'^P_n = sum_b sum_{k<=n} op_b[n][k] M'^b_k (lane n: real, lane q+n: imag)
+    const uint32_t n = lane < q ? lane : lane - q;
+    for (uint32_t b = 0; b < 4; ++b) {
+      const uint32_t ch = child_at(C, b);
+      if (ch == TC_NONE) continue;
+      if (lane < st) {
+        const double *cm = a.mco + (size_t)ch * st;
+        double sr = 0, si = 0;
+        for (uint32_t k = 0; k <= n; ++k) {
+          const double orr = a.tab->m2m_re[b][n][k], oi = a.tab->m2m_im[b][n][k];
+          const double mr = __ldcg(&cm[k]), mi = __ldcg(&cm[q + k]);
+          sr += orr * mr - oi * mi;
+          si += orr * mi + oi * mr;
+        }
+        acc0 += lane < q ? sr : si;
+      }
+    }
+  }
+  if (lane < st) mc[lane] = acc0;
+  // the bf16 split for the tensor cores: hi row then lo row, zero padded
+  __nv_bfloat16 hi = __float2bfloat16(0.f), lo = __float2bfloat16(0.f);
+  if (lane < st) tc::split_bf16(acc0, hi, lo);
+  a.mbf[(size_t)c * 64 + lane] = hi;
+  a.mbf[(size_t)c * 64 + 32 + lane] = lo;
+}
+
+__global__ void __launch_bounds__(TC_THREADS) k_tc_upward(TcArgs a) {
+  extern __shared__ double tc_smem[];
+  cg::grid_group g = cg::this_grid();
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  double *ws = tc_smem + (threadIdx.x >> 5) * 32 * (2 * a.q);
+  for (int lev = (int)a.nlev - 1; lev >= 0; --lev) {
+    for (uint32_t c = a.lvl[lev] + gw; c < a.lvl[lev + 1]; c += nwarps) tc_upward_cell(a, c, ws);
+    g.sync();
+  }
+}
+
+// ---- lists ----------------------------------------------------------------------------
+
+// The MAC of fmm.zig:400-453 between squares of different levels (r = s / sqrt 2).
+__device__ __forceinline__ bool separated(const TcArgs &a, const TcCell &A, const TcCell &B) {
+  double ax, ay, bx, by;
+  cell_centre(A, ax, ay);
+  cell_centre(B, bx, by);
+  const double ra = cell_side(A.level) * 0.7071067811865476;
+  const double rb = cell_side(B.level) * 0.7071067811865476;
+  const double dx = ax - bx, dy = ay - by;
+  const double rmax = ra > rb ? ra : rb, rmin = ra > rb ? rb : ra;
+  const double thr = a.tab->mac_far * rmax + rmin;
+  return dx * dx + dy * dy >= thr * thr;
+}
+
+// Per-lane list events. WRITE false: counts; true: writes from the offsets.
+struct Ev {
+  uint32_t np, nw, nx, nc;
+};
+
+// Leaf A against the subtree of B (not a leaf, near A): M2P for the cells
+// separated from A, P2P for the leaves that are not.
+template <bool WRITE>
+__device__ bool tc_walk(const TcArgs &a, const TcCell &A, uint32_t b, Ev &e, uint32_t op,
+                        uint32_t ow) {
+  uint32_t stack[TC_STACK];
+  uint32_t sp = 0;
+  const TcCell B = a.cells[b];
+  for (uint32_t j = 0; j < 4; ++j) {
+    const uint32_t ch = child_at(B, 3 - j);
+    if (ch != TC_NONE) stack[sp++] = ch;
+  }
+  while (sp) {
+    const uint32_t c = stack[--sp];
+    const TcCell C = a.cells[c];
+    if (separated(a, A, C)) {
+      if (WRITE) a.pool[ow + e.nw] = c;
+      ++e.nw;
+    } else if (C.nchild == 0) {
+      if (WRITE) a.pool[op + e.np] = c;
+      ++e.np;
+    } else {
+      if (sp + 4 > TC_STACK) return false;
+      for (uint32_t j = 0; j < 4; ++j) {
+        const uint32_t ch = child_at(C, 3 - j);
+        if (ch != TC_NONE) stack[sp++] = ch;
+      }
+    }
+  }
+  return true;
+}
+
+// The events of candidate u of cell c (u < 4 nnear: a child of a parent's
+// near cell; beyond: the parent's coarse leaf u - 4 nnear).
+template <bool WRITE>
+__device__ bool tc_candidate(const TcArgs &a, uint32_t c, const TcCell &A, uint32_t u, Ev &e,
+                             const uint32_t *o4) {
+  const uint32_t nn = a.tab->nnear;
+  const bool leaf = A.nchild == 0;
+  uint32_t coarse = TC_NONE;
+  if (u < 4 * nn) {
+    const uint32_t o = u >> 2, b = u & 3;
+    const uint32_t pb = __ldcg(&a.near[(size_t)A.parent * nn + o]);
+    if (pb == TC_NONE) return true;
+    const TcCell PB = a.cells[pb];
+    if (PB.nchild == 0) {
+      if (b != 0) return true;
+      coarse = pb;  // a near leaf of the parent: seen from A as a coarse leaf
+    } else {
+      const uint32_t B = child_at(PB, b);
+      if (B == TC_NONE) return true;
+      const uint32_t e16 = a.tab->map[A.quad][o][b];
+      if (!(e16 & TC_NEAR_FLAG)) {
+        if (WRITE) a.m2l[(size_t)c * TC_SLOT_MAX + e16] = B;
+        return true;
+      }
+      if (WRITE) a.near[(size_t)c * nn + (e16 & 0xFF)] = B;
+      if (!leaf) return true;
+      const TcCell Bc = a.cells[B];
+      if (Bc.nchild == 0) {
+        if (WRITE) a.pool[o4[0] + e.np] = B;
+        ++e.np;
+        return true;
+      }
+      return tc_walk<WRITE>(a, A, B, e, o4[0], o4[1]);
+    }
+  } else {
+    const uint32_t k = u - 4 * nn;
+    coarse = __ldcg(&a.pool[__ldcg(&a.loff[(size_t)A.parent * 8 + 6]) + k]);
+  }
+  const TcCell L = a.cells[coarse];
+  if (separated(a, A, L)) {
+    if (WRITE) a.pool[o4[2] + e.nx] = coarse;
+    ++e.nx;
+  } else if (leaf) {
+    if (WRITE) a.pool[o4[0] + e.np] = coarse;
+    ++e.np;
+  } else {
+    if (WRITE) a.pool[o4[3] + e.nc] = coarse;
+    ++e.nc;
+  }
+  return true;
+}
+
+__device__ __forceinline__ uint32_t warp_excl_sum(uint32_t v, uint32_t &total) {
+  const unsigned lane = threadIdx.x & 31;
+  uint32_t incl = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= (unsigned)o) incl += y;
+  }
+  total = __shfl_sync(0xffffffffu, incl, 31);
+  return incl - v;
+}
+
+// loff[c * 8 + ...]: 0 p2p off, 1 p2p cnt, 2 w off, 3 w cnt, 4 x off, 5 x cnt,
+// 6 coarse off, 7 coarse cnt.
+__device__ void tc_list_cell(const TcArgs &a, uint32_t c) {
+  const unsigned lane = threadIdx.x & 31;
+  const uint32_t nn = a.tab->nnear;
+  const TcCell A = a.cells[c];
+  for (uint32_t j = lane; j < TC_SLOT_MAX; j += 32) a.m2l[(size_t)c * TC_SLOT_MAX + j] = TC_NONE;
+  for (uint32_t j = lane; j < nn; j += 32) a.near[(size_t)c * nn + j] = TC_NONE;
+  if (c == 0) {
+    // the root: near itself
+    uint32_t self = 0;
+    for (uint32_t o = 0; o < nn; ++o)
+      if (a.tab->near_dx[o] == 0 && a.tab->near_dy[o] == 0) self = o;
+    __syncwarp();
+    if (lane == 0) {
+      a.near[self] = 0;
+      uint32_t op = 0;
+      if (A.nchild == 0) {
+        op = atomicAdd(&a.info[TI_POOL_P2P], 1u);
+        if (op < a.pool_cap) a.pool[op] = 0;
+        else atomicOr(&a.info[TI_OVF], 1u);
+      }
+      uint32_t *lo = a.loff + (size_t)c * 8;
+      lo[0] = op; lo[1] = A.nchild == 0 ? 1 : 0;
+      lo[2] = lo[3] = lo[4] = lo[5] = lo[6] = lo[7] = 0;
+    }
+    return;
+  }
+  __syncwarp();
+  const uint32_t ncoarse = __ldcg(&a.loff[(size_t)A.parent * 8 + 7]);
+  const uint32_t ncand = 4 * nn + ncoarse;
+  // counts
+  Ev tot{0, 0, 0, 0};
+  bool ok = true;
+  const uint32_t zero4[4] = {0, 0, 0, 0};
+  for (uint32_t u0 = 0; u0 < ncand; u0 += 32) {
+    const uint32_t u = u0 + lane;
+    Ev e{0, 0, 0, 0};
+    if (u < ncand && !tc_candidate<false>(a, c, A, u, e, zero4)) ok = false;
+    uint32_t t;
+    warp_excl_sum(e.np, t); tot.np += t;
+    warp_excl_sum(e.nw, t); tot.nw += t;
+    warp_excl_sum(e.nx, t); tot.nx += t;
+    warp_excl_sum(e.nc, t); tot.nc += t;
+  }
+  ok = __all_sync(0xffffffffu, ok);
+  uint32_t base = 0;
+  const uint32_t all = tot.np + tot.nw + tot.nx + tot.nc;
+  if (lane == 0) base = atomicAdd(&a.info[TI_POOL_P2P], all);
+  base = __shfl_sync(0xffffffffu, base, 0);
+  uint32_t o4[4] = {base, base + tot.np, base + tot.np + tot.nw, base + tot.np + tot.nw + tot.nx};
+  if (lane == 0) {
+    uint32_t *lo = a.loff + (size_t)c * 8;
+    lo[0] = o4[0]; lo[1] = tot.np;
+    lo[2] = o4[1]; lo[3] = tot.nw;
+    lo[4] = o4[2]; lo[5] = tot.nx;
+    lo[6] = o4[3]; lo[7] = tot.nc;
+  }
+  if (!ok || (size_t)base + all > a.pool_cap) {
+    if (lane == 0) {
+      atomicOr(&a.info[TI_OVF], ok ? 1u : 2u);
+      uint32_t *lo = a.loff + (size_t)c * 8;
+      lo[1] = lo[3] = lo[5] = lo[7] = 0;
+    }
+    return;
+  }
+  // writes, each lane's events after those of the candidates before it
+  for (uint32_t u0 = 0; u0 < ncand; u0 += 32) {
+    const uint32_t u = u0 + lane;
+    Ev e{0, 0, 0, 0};
+    if (u < ncand) tc_candidate<false>(a, c, A, u, e, zero4);
+    uint32_t t0, t1, t2, t3;
+    const uint32_t xp = warp_excl_sum(e.np, t0), xw = warp_excl_sum(e.nw, t1);
+    const uint32_t xx = warp_excl_sum(e.nx, t2), xc = warp_excl_sum(e.nc, t3);
+    if (u < ncand) {
+      Ev w{0, 0, 0, 0};
+      const uint32_t off[4] = {o4[0] + xp, o4[1] + xw, o4[2] + xx, o4[3] + xc};
+      tc_candidate<true>(a, c, A, u, w, off);
+    }
+    o4[0] += t0;
+    o4[1] += t1;
+    o4[2] += t2;
+    o4[3] += t3;
+  }
+}
+
+__global__ void __launch_bounds__(TC_THREADS) k_tc_lists(TcArgs a) {
+  cg::grid_group g = cg::this_grid();
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t lev = 0; lev < a.nlev; ++lev) {
+    for (uint32_t c = a.lvl[lev] + gw; c < a.lvl[lev + 1]; c += nwarps) tc_list_cell(a, c);
+    g.sync();
+  }
+}
+
+// ---- M2L on the tensor cores -------------------------------------------------------------
+
+struct M2lSmem {
+  unsigned char a[TC_STAGES][2][TC_TILE * TC_KN * 2];  // [stage][hi, lo] 128 x 32 bf16
+  unsigned char b[TC_STAGES][2][TC_KN * TC_KN * 2];    // [stage][hi, lo] 32 x 32 bf16
+  uint64_t full[TC_STAGES], empty[TC_STAGES], done;
+  uint32_t tmem;
+  uint32_t tgt[TC_TILE];
+  uint32_t err;
+};
+
+// Budget of a wait on a barrier the tile's own threads complete: 2^22 polls.
+constexpr uint32_t TC_WAIT_POLLS = 1u << 22;
+
+__global__ void __launch_bounds__(TC_TILE) k_tc_m2l(TcArgs a) {
+  extern __shared__ __align__(1024) unsigned char tc_m2l_smem[];
+  M2lSmem &S = *reinterpret_cast<M2lSmem *>(tc_m2l_smem);
+  const uint32_t t = threadIdx.x, warp = t >> 5;
+  // this CTA's tile: group g, rows base .. base + 127
+  uint32_t g = 0, tile = blockIdx.x, cnt = 0;
+  for (; g < 4; ++g) {
+    cnt = __ldcg(&a.info[TI_GROUP + g]);
+    const uint32_t nt = (cnt + TC_TILE - 1) / TC_TILE;
+    if (tile < nt) break;
+    tile -= nt;
+  }
+  if (g == 4) return;  // no tile: nothing allocated yet, nothing to free
+  const uint32_t base = tile * TC_TILE;
+  const uint32_t nslot = a.tab->nslot[g];
+  S.tgt[t] = base + t < cnt ? a.groups[(size_t)g * a.ccap + base + t] : TC_NONE;
+  if (t == 0) {
+    for (uint32_t s = 0; s < TC_STAGES; ++s) {
+      tc::mbar_init(&S.full[s], TC_TILE);
+      tc::mbar_init(&S.empty[s], 1);
+    }
+    tc::mbar_init(&S.done, 1);
+    S.err = 0;
+    tc::mbar_init_fence();
+  }
+  __syncwarp();
+  if (warp == 0) {
+    tc::tmem_alloc(&S.tmem, 32);
+    tc::tmem_relinquish();
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = S.tmem;
+  const uint32_t my = S.tgt[t];
+  const uint32_t idesc = tc::idesc_bf16_f32(TC_TILE, TC_KN);
+  bool ok = true;
+  for (uint32_t j = 0; j < nslot; ++j) {
+    const uint32_t s = j % TC_STAGES, use = j / TC_STAGES;
+    if (use > 0 && ok && !tc::mbar_wait(&S.empty[s], (use - 1) & 1, TC_WAIT_POLLS)) ok = false;
+    // A rows: this thread's target's source for slot j (bf16 hi, lo), or zeros
+    const uint32_t src = my != TC_NONE ? __ldcg(&a.m2l[(size_t)my * TC_SLOT_MAX + j]) : TC_NONE;
+    uint4 hv[4], lv[4];
+    if (src != TC_NONE) {
+      const uint4 *m = reinterpret_cast<const uint4 *>(a.mbf + (size_t)src * 64);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        hv[c] = __ldcg(m + c);
+        lv[c] = __ldcg(m + 4 + c);
+      }
+    } else {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) hv[c] = lv[c] = make_uint4(0, 0, 0, 0);
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const uint32_t off = tc::tile_offset(t, c, TC_TILE);
+      *reinterpret_cast<uint4 *>(&S.a[s][0][off]) = hv[c];
+      *reinterpret_cast<uint4 *>(&S.a[s][1][off]) = lv[c];
+    }
+    // B: the slot's operator, already in the tile layout (2 x 2 KB)
+    const uint32_t cls = a.tab->slot_class[g][j];
+    const uint4 *w = reinterpret_cast<const uint4 *>(a.wops + (size_t)cls * 4096);
+    for (uint32_t k = t; k < 256; k += TC_TILE) {
+      const uint4 v = __ldg(w + k);
+      *reinterpret_cast<uint4 *>(&S.b[s][k >> 7][(k & 127) * 16]) = v;
+    }
+    tc::fence_proxy_async();
+    tc::mbar_arrive(&S.full[s]);
+    if (t == 0 && ok) {
+      if (!tc::mbar_wait(&S.full[s], use & 1, TC_WAIT_POLLS)) {
+        ok = false;
+      } else {
+        tc::fence_after_sync();
+        const uint32_t a_hi = tc::smem_addr(S.a[s][0]), a_lo = tc::smem_addr(S.a[s][1]);
+        const uint32_t b_hi = tc::smem_addr(S.b[s][0]), b_lo = tc::smem_addr(S.b[s][1]);
+        const uint32_t alb = (TC_TILE / 8) * 128, blb = (TC_KN / 8) * 128;
+#pragma unroll
+        for (uint32_t ks = 0; ks < 2; ++ks) {  // K = 32 as two MMAs of K = 16
+          const uint32_t ao = ks * 2 * alb, bo = ks * 2 * blb;
+          const uint64_t dah = tc::smem_desc(a_hi + ao, alb, 128);
+          const uint64_t dal = tc::smem_desc(a_lo + ao, alb, 128);
+          const uint64_t dbh = tc::smem_desc(b_hi + bo, blb, 128);
+          const uint64_t dbl = tc::smem_desc(b_lo + bo, blb, 128);
+          tc::mma_bf16(tmem, dah, dbh, idesc, (j | ks) ? 1u : 0u);
+          tc::mma_bf16(tmem, dah, dbl, idesc, 1u);
+          tc::mma_bf16(tmem, dal, dbh, idesc, 1u);
+        }
+        tc::commit(&S.empty[s]);
+      }
+    }
+  }
+  if (t == 0) {
+    if (ok && nslot) tc::commit(&S.done);
+    if (!ok) S.err = 1;
+  }
+  __syncthreads();
+  const bool good = S.err == 0 && nslot > 0;
+  if (good && !tc::mbar_wait(&S.done, 0, TC_WAIT_POLLS)) S.err = 1;
+  tc::fence_after_sync();
+  if (good) {
+    float v[32];
+    tc::tmem_ld32(tmem + ((warp * 32u) << 16), v);
+    if (my != TC_NONE) {
+      float *L = a.lco + (size_t)my * TC_KN;
+      for (uint32_t k = 0; k < 2 * a.q; ++k) L[k] = v[k];
+    }
+  } else if (my != TC_NONE) {
+    float *L = a.lco + (size_t)my * TC_KN;
+    for (uint32_t k = 0; k < 2 * a.q; ++k) L[k] = 0;
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, 32);
+  if (t == 0 && S.err) {
+    atomicOr(&a.info[TI_ERR], 1u);
+    if (a.status) atomicOr(a.status, ST_WAIT_TIMEOUT);
+  }
+}
+
+// ---- P2L (coarse leaves into local expansions, FP32) ------------------------------------------
+
+__global__ void __launch_bounds__(TC_THREADS) k_tc_p2l(TcArgs a) {
+  const unsigned lane = threadIdx.x & 31;
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t q = a.q;
+  for (uint32_t c = gw; c < a.ncells; c += nwarps) {
+    const uint32_t nx = a.loff[(size_t)c * 8 + 5];
+    if (!nx) continue;
+    const uint32_t ox = a.loff[(size_t)c * 8 + 4];
+    const TcCell A = a.cells[c];
+    double ax, ay;
+    cell_centre(A, ax, ay);
+    const double inv_s = ldexp(1.0, (int)A.level);
+    // lane l < q accumulates L'_l over every point of every listed leaf
+    float sr = 0, si = 0;
+    for (uint32_t e = 0; e < nx; ++e) {
+      const TcCell L = a.cells[a.pool[ox + e]];
+      for (uint32_t k = L.first; k < L.first + L.count; ++k) {
+        const double sv = a.ps[k];
+        // z = (c_A - u_j) / s_A; term (-1)^l s_j / z^(l+1)
+        const double zr = (ax - a.ux[k]) * inv_s, zi = (ay - a.uy[k]) * inv_s;
+        const double d2 = zr * zr + zi * zi;
+        const float ir = (float)(zr / d2), ii = (float)(-zi / d2);  // 1 / z
+        float pr = ir, pi = ii;
+        for (uint32_t l = 0; l < lane && l < q; ++l) {
+          const float nr = pr * ir - pi * ii;
+          pi = pr * ii + pi * ir;
+          pr = nr;
+        }
+        if (lane < q) {
+          const float sg = (lane & 1) ? -1.f : 1.f;
+          sr += sg * (float)sv * pr;
+          si += sg * (float)sv * pi;
+        }
+      }
+    }
+    if (lane < q) {
+      float *Lc = a.lco + (size_t)c * TC_KN;
+      Lc[lane] += sr;
+      Lc[q + lane] += si;
+    }
+  }
+}
+
+// ---- downward: L2L, L2P, M2P ----------------------------------------------------------------------
+
+__global__ void __launch_bounds__(TC_THREADS) k_tc_down(TcArgs a) {
+  extern __shared__ float tc_down_smem[];
+  cg::grid_group g = cg::this_grid();
+  const unsigned lane = threadIdx.x & 31;
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t q = a.q;
+  float *Lw = tc_down_smem + (threadIdx.x >> 5) * TC_KN;
+  for (uint32_t lev = 0; lev < a.nlev; ++lev) {
+    for (uint32_t c = a.lvl[lev] + gw; c < a.lvl[lev + 1]; c += nwarps) {
+      const TcCell C = a.cells[c];
+      Lw[lane] = lane < 2 * q ? __ldcg(&a.lco[(size_t)c * TC_KN + lane]) : 0.f;
+      __syncwarp();
+      if (C.nchild) {
+        // L2L into each child: L'^b_m += sum_{l>=m} op_b[m][l] L'_l
+        for (uint32_t b = 0; b < 4; ++b) {
+          const uint32_t ch = child_at(C, b);
+          if (ch == TC_NONE) continue;
+          if (lane < q) {
+            float sr = 0, si = 0;
+            for (uint32_t l = lane; l < q; ++l) {
+              const float orr = a.tab->l2l_re[b][lane][l], oi = a.tab->l2l_im[b][lane][l];
+              sr += orr * Lw[l] - oi * Lw[q + l];
+              si += orr * Lw[q + l] + oi * Lw[l];
+            }
+            float *Lc = a.lco + (size_t)ch * TC_KN;
+            Lc[lane] = __ldcg(&Lc[lane]) + sr;
+            Lc[q + lane] = __ldcg(&Lc[q + lane]) + si;
+          }
+        }
+      } else {
+        // L2P (and M2P from the cells of the leaf's W list) at each point
+        double cx, cy;
+        cell_centre(C, cx, cy);
+        const double inv_s = ldexp(1.0, (int)C.level);
+        const uint32_t nw = a.loff[(size_t)c * 8 + 3], ow = a.loff[(size_t)c * 8 + 2];
+        for (uint32_t k = C.first + lane; k < C.first + C.count; k += 32) {
+          const float wr = (float)((a.ux[k] - cx) * inv_s), wi = (float)((a.uy[k] - cy) * inv_s);
+          float ar = Lw[q - 1], ai = Lw[2 * q - 1];
+          for (int l = (int)q - 2; l >= 0; --l) {
+            const float nr = ar * wr - ai * wi + Lw[l];
+            ai = ar * wi + ai * wr + Lw[q + l];
+            ar = nr;
+          }
+          double gr = (double)ar * inv_s, gi = (double)ai * inv_s;  // phi = (1/s) sum L'_l w^l
+          for (uint32_t e = 0; e < nw; ++e) {
+            const uint32_t cc = a.pool[ow + e];
+            const TcCell W = a.cells[cc];
+            double wx, wy;
+            cell_centre(W, wx, wy);
+            const double winv = ldexp(1.0, (int)W.level);
+            // g = (1/s_W) sum_k M'_k / z^(k+1), z = (u - c_W) / s_W
+            const double zr = (a.ux[k] - wx) * winv, zi = (a.uy[k] - wy) * winv;
+            const double d2 = zr * zr + zi * zi;
+            const double ir = zr / d2, ii = -zi / d2;
+            const double *mc = a.mco + (size_t)cc * 2 * q;
+            double pr = ir, pi = ii, sr = 0, si = 0;
+            for (uint32_t kk = 0; kk < q; ++kk) {
+              const double mr = mc[kk], mi = mc[q + kk];
+              sr += mr * pr - mi * pi;
+              si += mr * pi + mi * pr;
+              const double nr = pr * ir - pi * ii;
+              pi = pr * ii + pi * ir;
+              pr = nr;
+            }
+            gr += sr * winv;
+            gi += si * winv;
+          }
+          a.far[k] = make_float2((float)(-gr * a.inv_w), (float)(gi * a.inv_w));
+        }
+      }
+      __syncwarp();
+    }
+    g.sync();
+  }
+}
+
+// ---- P2P (FP32 with an FP64 origin shift) ----------------------------------------------------------
+
+__global__ void __launch_bounds__(TC_THREADS) k_tc_p2p(TcArgs a) {
+  __shared__ float4 src[TC_WARPS][32];
+  const unsigned lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint64_t seed = (uint64_t)__double_as_longlong(*a.seed);
+  const float dmin2 = a.dmin2f;
+  for (uint32_t c = gw; c < a.ncells; c += nwarps) {
+    const TcCell A = a.cells[c];
+    if (A.nchild) continue;
+    const uint32_t np = a.loff[(size_t)c * 8 + 1], op = a.loff[(size_t)c * 8];
+    // the leaf's origin: its first point, in FP64 world coordinates
+    const double ox = a.px[A.first], oy = a.py[A.first];
+    for (uint32_t tb = A.first; tb < A.first + A.count; tb += 32) {
+      const uint32_t ti = tb + lane;
+      const bool act = ti < A.first + A.count;
+      const float xi = act ? (float)(a.px[ti] - ox) : 0.f, yi = act ? (float)(a.py[ti] - oy) : 0.f;
+      const uint32_t gi = act ? a.perm[ti] : 0;
+      float vx0 = 0, vy0 = 0, vx1 = 0, vy1 = 0;
+      for (uint32_t e = 0; e < np; ++e) {
+        const TcCell B = a.cells[a.pool[op + e]];
+        for (uint32_t sb = B.first; sb < B.first + B.count; sb += 32) {
+          const uint32_t sj = sb + lane;
+          const uint32_t ns = min(32u, B.first + B.count - sb);
+          __syncwarp();
+          if (sj < B.first + B.count)
+            src[wl][lane] = make_float4((float)(a.px[sj] - ox), (float)(a.py[sj] - oy),
+                                        (float)a.ps[sj], __uint_as_float(sj));
+          __syncwarp();
+          if (!act) continue;
+          for (uint32_t k = 0; k < ns; ++k) {
+            const float4 sv = src[wl][k];
+            const uint32_t tj = __float_as_uint(sv.w);
+            float dx = sv.x - xi, dy = sv.y - yi;
+            float l = dx * dx + dy * dy;
+            if (tj == ti) continue;
+            if (dx == 0.f || dy == 0.f) {
+              const uint32_t gj = a.perm[tj];
+              if (dx == 0.f) {
+                dx = (float)hash_jiggle(seed, gi, gj, 0);
+                l += dx * dx;
+              }
+              if (dy == 0.f) {
+                dy = (float)hash_jiggle(seed, gi, gj, 1);
+                l += dy * dy;
+              }
+            }
+            if (l < dmin2) l = sqrtf(dmin2 * l);
+            const float w = sv.z / l;
+            if (k & 1) {
+              vx1 += dx * w;
+              vy1 += dy * w;
+            } else {
+              vx0 += dx * w;
+              vy0 += dy * w;
+            }
+          }
+        }
+      }
+      if (act) {
+        const float2 f = a.far[ti];
+        a.vx[gi] = a.vx[gi] + ((double)(vx0 + vx1) + (double)f.x);
+        a.vy[gi] = a.vy[gi] + ((double)(vy0 + vy1) + (double)f.y);
+      }
+    }
+  }
+}
+
+// ---- tables (host) --------------------------------------------------------------------------------
+
+struct Cplx {
+  double re, im;
+};
+Cplx cmul(Cplx a, Cplx b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+
+double binom(int n, int k) {
+  double r = 1;
+  for (int i = 1; i <= k; ++i) r = r * (n - k + i) / i;
+  return r;
+}
+
+// Rounds to bf16 (nearest even) from a float.
+uint16_t to_bf16(float f) {
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  const uint32_t lsb = (u >> 16) & 1;
+  u += 0x7FFF + lsb;
+  return (uint16_t)(u >> 16);
+}
+float from_bf16(uint16_t h) {
+  uint32_t u = (uint32_t)h << 16;
+  float f;
+  memcpy(&f, &u, 4);
+  return f;
+}
+
+// Builds the vector sets, the slot maps, the quadrant operators and the M2L
+// operators for order p and opening kappa.
+int build_tables(TcDev &d, uint32_t p, double kappa, cudaStream_t st) {
+  TcTables &T = d.h_tab;
+  memset(&T, 0, sizeof T);
+  const uint32_t q = p + 1;
+  T.q = q;
+  T.kappa2x2 = 2 * kappa * kappa;
+  T.mac_far = 2 * kappa - 1;
+  auto sep = [&](int x, int y) { return (double)(x * x + y * y) >= T.kappa2x2; };
+  // near offsets
+  uint32_t nn = 0;
+  for (int y = -4; y <= 4; ++y)
+    for (int x = -4; x <= 4; ++x)
+      if (!sep(x, y)) {
+        if (nn >= TC_NEAR_MAX) return -3;
+        T.near_dx[nn] = (int8_t)x;
+        T.near_dy[nn] = (int8_t)y;
+        ++nn;
+      }
+  T.nnear = nn;
+  std::vector<std::pair<int, int>> classes;
+  for (uint32_t aq = 0; aq < 4; ++aq) {
+    const int ax = aq & 1, ay = aq >> 1;
+    uint32_t ns = 0;
+    for (uint32_t o = 0; o < nn; ++o)
+      for (uint32_t b = 0; b < 4; ++b) {
+        const int bx = b & 1, by = b >> 1;
+        const int vx = 2 * T.near_dx[o] + bx - ax, vy = 2 * T.near_dy[o] + by - ay;
+        if (!sep(vx, vy)) {
+          uint32_t ci = nn;
+          for (uint32_t k = 0; k < nn; ++k)
+            if (T.near_dx[k] == vx && T.near_dy[k] == vy) ci = k;
+          if (ci == nn) return -3;  // cannot happen: a near child is a near offset
+          T.map[aq][o][b] = (uint16_t)(TC_NEAR_FLAG | ci);
+          continue;
+        }
+        size_t cls = 0;
+        while (cls < classes.size() && !(classes[cls].first == vx && classes[cls].second == vy)) ++cls;
+        if (cls == classes.size()) classes.push_back({vx, vy});
+        if (ns >= TC_SLOT_MAX || classes.size() > TC_CLASS_MAX) return -3;
+        T.map[aq][o][b] = (uint16_t)ns;
+        T.slot_class[aq][ns] = (uint16_t)cls;
+        ++ns;
+      }
+    T.nslot[aq] = ns;
+  }
+  // quadrant operators: child centre - parent centre = (s/4) delta_b
+  for (uint32_t b = 0; b < 4; ++b) {
+    const Cplx delta{(double)(2 * (int)(b & 1) - 1), (double)(2 * (int)(b >> 1) - 1)};
+    for (uint32_t n = 0; n < q; ++n)
+      for (uint32_t k = 0; k <= n; ++k) {
+        // M2M: C(n,k) 2^-k 4^-(n-k) delta^(n-k)
+        Cplx pw{1, 0};
+        for (uint32_t e = 0; e < n - k; ++e) pw = cmul(pw, delta);
+        const double f = binom(n, k) * std::ldexp(1.0, -(int)k) * std::ldexp(1.0, -2 * (int)(n - k));
+        T.m2m_re[b][n][k] = f * pw.re;
+        T.m2m_im[b][n][k] = f * pw.im;
+      }
+    for (uint32_t mm = 0; mm < q; ++mm)
+      for (uint32_t l = mm; l < q; ++l) {
+        // L2L: C(l,m) delta^(l-m) 4^-(l-m) 2^-(m+1)
+        Cplx pw{1, 0};
+        for (uint32_t e = 0; e < l - mm; ++e) pw = cmul(pw, delta);
+        const double f = binom(l, mm) * std::ldexp(1.0, -2 * (int)(l - mm)) * std::ldexp(1.0, -(int)(mm + 1));
+        T.l2l_re[b][mm][l] = (float)(f * pw.re);
+        T.l2l_im[b][mm][l] = (float)(f * pw.im);
+      }
+  }
+  // M2L operators in real form, W[k][n] (y = x W), stored as the B tile (row
+  // n holds W[.][n]), bf16 hi then lo
+  std::vector<uint16_t> w(classes.size() * 2 * TC_KN * TC_KN, 0);
+  for (size_t cls = 0; cls < classes.size(); ++cls) {
+    const Cplx v{(double)classes[cls].first, (double)classes[cls].second};
+    const double d2 = v.re * v.re + v.im * v.im;
+    const Cplx inv{v.re / d2, -v.im / d2};
+    std::vector<Cplx> ipw(2 * q + 1);
+    ipw[0] = {1, 0};
+    for (uint32_t e = 1; e <= 2 * q; ++e) ipw[e] = cmul(ipw[e - 1], inv);
+    double W[TC_KN][TC_KN] = {};
+    for (uint32_t l = 0; l < q; ++l)
+      for (uint32_t k = 0; k < q; ++k) {
+        // K[l][k] = (-1)^l C(k+l, l) / v^(k+l+1)
+        const double f = ((l & 1) ? -1.0 : 1.0) * binom(k + l, l);
+        const double kr = f * ipw[k + l + 1].re, ki = f * ipw[k + l + 1].im;
+        W[k][l] = kr;
+        W[q + k][l] = -ki;
+        W[k][q + l] = ki;
+        W[q + k][q + l] = kr;
+      }
+    for (uint32_t nidx = 0; nidx < TC_KN; ++nidx)
+      for (uint32_t k = 0; k < TC_KN; ++k) {
+        const double x = W[k][nidx];
+        const uint16_t hi = to_bf16((float)x);
+        const uint16_t lo = to_bf16((float)(x - (double)from_bf16(hi)));
+        const uint32_t off = tc::tile_offset(nidx, k / 8, TC_KN) / 2 + k % 8;
+        w[(cls * 2 + 0) * TC_KN * TC_KN + off] = hi;
+        w[(cls * 2 + 1) * TC_KN * TC_KN + off] = lo;
+      }
+  }
+  if (!d.tab) D3_CUDA_OK(cudaMalloc(&d.tab, sizeof(TcTables)));
+  cudaFree(d.wops);
+  D3_CUDA_OK(cudaMalloc(&d.wops, w.size() * 2));
+  if (cudaMemcpyAsync(d.tab, &T, sizeof T, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaMemcpyAsync(d.wops, w.data(), w.size() * 2, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return -1;
+  d.p = p;
+  d.kappa = kappa;
+  return 0;
+}
+
+int reserve(TcDev &d, uint32_t ncells, uint32_t m) {
+  if (ncells > d.ccap) {
+    const uint32_t cap = ncells + ncells / 4 + 64;
+    cudaFree(d.cells); cudaFree(d.mco); cudaFree(d.mbf); cudaFree(d.lco); cudaFree(d.near);
+    cudaFree(d.m2l); cudaFree(d.groups); cudaFree(d.loff);
+    D3_CUDA_OK(cudaMalloc(&d.cells, cap * sizeof(TcCell)));
+    D3_CUDA_OK(cudaMalloc(&d.mco, (size_t)cap * 2 * TC_MAXQ * 8));
+    D3_CUDA_OK(cudaMalloc(&d.mbf, (size_t)cap * 64 * 2));
+    D3_CUDA_OK(cudaMalloc(&d.lco, (size_t)cap * TC_KN * 4));
+    D3_CUDA_OK(cudaMalloc(&d.near, (size_t)cap * TC_NEAR_MAX * 4));
+    D3_CUDA_OK(cudaMalloc(&d.m2l, (size_t)cap * TC_SLOT_MAX * 4));
+    D3_CUDA_OK(cudaMalloc(&d.groups, (size_t)cap * 4 * 4));
+    D3_CUDA_OK(cudaMalloc(&d.loff, (size_t)cap * 8 * 4));
+    d.ccap = cap;
+  }
+  if (m > d.pcap) {
+    const uint32_t cap = m + m / 4 + 1024;
+    cudaFree(d.far);
+    D3_CUDA_OK(cudaMalloc(&d.far, (size_t)cap * sizeof(float2)));
+    d.pcap = cap;
+  }
+  return 0;
+}
+
+int coop(const void *fn, int blocks, size_t smem, TcArgs &args, cudaStream_t st) {
+  void *params[] = {&args};
+  ++g_launches;
+  return cudaLaunchCooperativeKernel(fn, blocks, TC_THREADS, params, smem, st) == cudaSuccess ? 0
+                                                                                              : -1;
+}
+
+}  // namespace
+
+void fmm_tc_free(FastScratch &s) {
+  TcDev *d = static_cast<TcDev *>(s.fmm_tc);
+  if (!d) return;
+  cudaFree(d->tab); cudaFree(d->wops); cudaFree(d->cells); cudaFree(d->mco); cudaFree(d->mbf);
+  cudaFree(d->lco); cudaFree(d->near); cudaFree(d->m2l); cudaFree(d->groups); cudaFree(d->loff);
+  cudaFree(d->pool); cudaFree(d->far); cudaFree(d->info); cudaFreeHost(d->h_info);
+  delete d;
+  s.fmm_tc = nullptr;
+}
+
+int fmm_tc_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *strengths,
+               const FmmParams &prm, int form, const double *seed, uint32_t *status,
+               cudaStream_t st) {
+  (void)form;
+  if (prm.dmax2 < INFINITY) return fmm_run(s, t, a, strengths, prm, seed, status, st);
+  FmmPrep pr;
+  const int pre = fmm_prepare(s, t, a, strengths, prm.alpha, pr, st);
+  if (pre == 2) return 1;
+  if (pre <= 0) return pre;
+  if (!s.fmm_tc) {
+    TcDev *d = new TcDev();
+    s.fmm_tc = d;
+    D3_CUDA_OK(cudaMalloc(&d->info, TI_WORDS * 4));
+    D3_CUDA_OK(cudaHostAlloc(&d->h_info, TI_WORDS * 4, cudaHostAllocDefault));
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const size_t up_smem = TC_WARPS * 32 * 2 * TC_MAXQ * 8;
+    cudaFuncSetAttribute(k_tc_upward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)up_smem);
+    cudaFuncSetAttribute(k_tc_m2l, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(M2lSmem));
+    int pl = 0, pu = 0, pd = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pl, k_tc_lists, TC_THREADS, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pu, k_tc_upward, TC_THREADS, up_smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pd, k_tc_down, TC_THREADS, TC_WARPS * TC_KN * 4);
+    d->coop_lists = sms * (pl > 2 ? 2 : pl < 1 ? 1 : pl);
+    d->coop_up = sms * (pu > 2 ? 2 : pu < 1 ? 1 : pu);
+    d->coop_down = sms * (pd > 2 ? 2 : pd < 1 ? 1 : pd);
+  }
+  TcDev &d = *static_cast<TcDev *>(s.fmm_tc);
+  uint32_t p = 8;
+  if (prm.order >= 1 && prm.order <= (double)(TC_MAXQ - 1)) p = (uint32_t)prm.order;
+  double kappa = prm.opening;
+  if (!(kappa >= 1 && kappa <= 2)) kappa = 1.5;
+  if (d.p != p || d.kappa != kappa)
+    if (build_tables(d, p, kappa, st)) return -1;
+  if (reserve(d, pr.ncells, pr.m)) return -1;
+  TcArgs g;
+  memset(&g, 0, sizeof g);
+  g.tab = d.tab;
+  g.wops = d.wops;
+  g.keys = pr.keys;
+  g.perm = pr.perm;
+  g.px = pr.px; g.py = pr.py; g.ps = pr.ps; g.ux = pr.ux; g.uy = pr.uy;
+  g.fc = pr.cells;
+  g.cells = d.cells;
+  g.mco = d.mco; g.mbf = d.mbf; g.lco = d.lco;
+  g.near = d.near; g.m2l = d.m2l; g.groups = d.groups; g.loff = d.loff;
+  g.far = d.far;
+  g.vx = a.vx; g.vy = a.vy;
+  g.info = d.info;
+  g.status = status;
+  g.lvl = pr.info + 8;  // FI_LVL
+  g.ncells = pr.ncells; g.nlev = pr.nlev; g.m = pr.m; g.q = p + 1; g.ccap = d.ccap;
+  g.inv_w = pr.inv_w;
+  g.dmin2 = prm.dmin2 * pr.inv_w * pr.inv_w;
+  g.dmin2f = (float)prm.dmin2;
+  g.seed = seed;
+  if (cudaMemsetAsync(d.info, 0, TI_WORDS * 4, st) != cudaSuccess) return -1;
+  D3_LAUNCH(k_tc_geom, blocks_for(pr.ncells, 256), 256, 0, st)(g);
+  const size_t up_smem = TC_WARPS * 32 * 2 * (p + 1) * 8;
+  if (coop((const void *)k_tc_upward, d.coop_up, up_smem, g, st)) return -1;
+  // lists; grow the pool and redo on overflow
+  size_t need = d.last_pool ? d.last_pool + d.last_pool / 4 + 4096 : (size_t)pr.ncells * 24 + 4096;
+  for (int attempt = 0;; ++attempt) {
+    if (need > d.pool_cap) {
+      cudaFree(d.pool);
+      d.pool = nullptr;
+      d.pool_cap = need;
+      D3_CUDA_OK(cudaMalloc(&d.pool, d.pool_cap * 4));
+    }
+    g.pool = d.pool;
+    g.pool_cap = d.pool_cap;
+    if (cudaMemsetAsync(d.info, 0, 8 * 4, st) != cudaSuccess) return -1;
+    if (coop((const void *)k_tc_lists, d.coop_lists, 0, g, st)) return -1;
+    if (cudaMemcpyAsync(d.h_info, d.info, TI_WORDS * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+      return -1;
+    const uint32_t used = d.h_info[TI_POOL_P2P];
+    if (!d.h_info[TI_OVF]) {
+      d.last_pool = used;
+      break;
+    }
+    if ((d.h_info[TI_OVF] & 2) || attempt > 6) return -1;  // a walk's stack overflowed
+    need = 2 * (size_t)(used > need ? used : need);
+  }
+  uint32_t tiles = 0;
+  for (uint32_t q4 = 0; q4 < 4; ++q4) tiles += (d.h_info[TI_GROUP + q4] + TC_TILE - 1) / TC_TILE;
+  if (tiles)
+    D3_LAUNCH(k_tc_m2l, tiles, TC_TILE, sizeof(M2lSmem), st)(g);
+  const unsigned wblocks = blocks_for((size_t)pr.ncells * 32, TC_THREADS);
+  D3_LAUNCH(k_tc_p2l, wblocks, TC_THREADS, 0, st)(g);
+  if (coop((const void *)k_tc_down, d.coop_down, TC_WARPS * TC_KN * 4, g, st)) return -1;
+  D3_LAUNCH(k_tc_p2p, wblocks, TC_THREADS, 0, st)(g);
+  return cudaGetLastError() == cudaSuccess ? 1 : -1;
+}
+
+}  // namespace d3

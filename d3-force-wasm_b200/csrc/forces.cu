@@ -341,6 +341,9 @@ __global__ void __launch_bounds__(128) k_mb_traverse(const MRec *rec,
                                                      uint32_t *counters) {
   const uint32_t pos = blockIdx.x * blockDim.x + threadIdx.x;
   if (pos >= n) return;
+  // no tree this call (cell buffer overflow or a failed build launch): perm
+  // may be stale, the velocities stay as they are
+  if (info[5]) return;
   const uint32_t len = info[1];
   const uint32_t i = perm[pos];
   uint32_t d = len ? mb_node<true>(rec, perm, len, xs, ys, vxs, vys, strengths, p, i,
@@ -359,7 +362,7 @@ __global__ void __launch_bounds__(128) k_mb_rerun(const MRec *rec,
                                                   ManyBodyParams p, uint32_t n,
                                                   const uint32_t *draws, const uint32_t *offsets,
                                                   const uint32_t *counters, const Rng *rng) {
-  if (counters[1] == 0) return;
+  if (counters[1] == 0 || info[5]) return;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || draws[i] == 0) return;
   mb_node<false>(rec, perm, info[1], xs, ys, vxs, vys, strengths, p, i, rng, offsets[i]);
@@ -377,7 +380,7 @@ __global__ void __launch_bounds__(256) k_mb_draws(const MRec *rec, const uint32_
                                                   uint32_t n, const uint32_t *draws,
                                                   uint32_t *offsets, uint32_t *counters,
                                                   uint32_t *bsum, Rng *rng) {
-  if (__ldcg(&counters[1]) == 0) return;
+  if (__ldcg(&counters[1]) == 0 || __ldcg(&info[5])) return;
   cg::grid_group g = cg::this_grid();
   const uint32_t total = grid_excl_scan(g, draws, offsets, n, bsum);
   g.sync();

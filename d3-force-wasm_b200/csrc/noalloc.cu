@@ -12,6 +12,8 @@
 // `g_noalloc_scratch`, a file-scope __device__ array sized for
 // D3_NOALLOC_MAX_NODES nodes. Every GPU that loads the library holds that
 // array until the process exits.
+#include <mutex>
+
 #include "forces.cuh"
 #include "scan_sort.cuh"
 #include "tree.cuh"
@@ -66,8 +68,13 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[na_total()];
 namespace {
 
 // Host-side addresses of g_noalloc_scratch per device (from
-// cudaGetSymbolAddress; the symbol's host name is not a device address).
-void *g_noalloc_base[128] = {};
+// cudaGetSymbolAddress; the symbol's host name is not a device address),
+// each looked up once, under its own once_flag, so two threads making their
+// first call at the same time do not race on it.
+constexpr int NA_DEVICES = 128;
+void *g_noalloc_base[NA_DEVICES] = {};
+cudaError_t g_noalloc_setup_err[NA_DEVICES] = {};
+std::once_flag g_noalloc_once[NA_DEVICES];
 
 struct Carve {
   unsigned char *p;
@@ -114,14 +121,14 @@ extern "C" int32_t d3_many_body_exact_noalloc(const double *x, const double *y, 
   }
   if (!lcg_state || (n && (!x || !y || !vx || !vy || !strength))) return D3_BAD_ARGUMENT;
   int dev = -1;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) return D3_WORKER_FAILED;
-  if (!g_noalloc_base[dev]) {
-    // Set-up, once per device, with that device current.
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NA_DEVICES) return D3_WORKER_FAILED;
+  // Set-up, once per device, with that device current.
+  std::call_once(g_noalloc_once[dev], [dev] {
     void *base = nullptr;
-    if (cudaGetSymbolAddress(&base, g_noalloc_scratch) != cudaSuccess || !base)
-      return D3_WORKER_FAILED;
-    g_noalloc_base[dev] = base;
-  }
+    g_noalloc_setup_err[dev] = cudaGetSymbolAddress(&base, g_noalloc_scratch);
+    if (g_noalloc_setup_err[dev] == cudaSuccess) g_noalloc_base[dev] = base;
+  });
+  if (g_noalloc_setup_err[dev] != cudaSuccess || !g_noalloc_base[dev]) return D3_WORKER_FAILED;
   Carve c{static_cast<unsigned char *>(g_noalloc_base[dev])};
   TreeDev t;
   t.cap = NA_CAP;
@@ -180,7 +187,11 @@ extern "C" int32_t d3_many_body_exact_noalloc(const double *x, const double *y, 
   if (cudaMemcpyAsync(out, words + 8, sizeof out, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)
     return D3_WORKER_FAILED;
-  if (out[1]) return D3_ARENA_FULL;  // the tree needed more cells than the array holds
+  // out[1] is the tree's failure mark: 1 when it needed more cells than the
+  // array holds (vx, vy are then left as they were), 0xffffffff when its
+  // launch did not happen. out[2] is the status word the kernels set.
+  if (out[1] == 1) return D3_ARENA_FULL;
+  if (out[1] || (out[2] & ST_FATAL)) return D3_WORKER_FAILED;
   *lcg_state = out[0];
   return D3_OK;
 }

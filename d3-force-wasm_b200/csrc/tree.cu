@@ -712,6 +712,13 @@ __device__ uint32_t tb_run_rank(const uint64_t *keys, const uint32_t *vals, uint
   return pos;
 }
 
+// The tree build's cooperative launch did not happen.
+__global__ void k_tree_failed(uint32_t *info, uint32_t *status) {
+  info[1] = 0;
+  info[5] = 0xffffffffu;
+  if (status) atomicOr(status, ST_LAUNCH_FAILED);
+}
+
 __global__ void __launch_bounds__(TB_THREADS) k_tree_build(TreeBuildArgs a) {
   cg::grid_group g = cg::this_grid();
   __shared__ double se[4];
@@ -855,7 +862,13 @@ __global__ void __launch_bounds__(TB_THREADS) k_tree_build(TreeBuildArgs a) {
   tb_stamp(a, 5);
   // 6. cell indices: the exclusive scan of the counts
   const uint32_t total = grid_excl_scan(g, a.cnt, a.base, n, a.bsum);
-  if (tid == 0) a.info[1] = total;
+  // info[1] is the cell count every later pass walks: on overflow it stays 0
+  // (an empty tree), so no pass reads or writes past the cell buffers;
+  // info[6] keeps the count the tree needed.
+  if (tid == 0) {
+    a.info[1] = total <= a.cells_cap ? total : 0;
+    a.info[6] = total;
+  }
   g.sync();
   tb_stamp(a, 6);
   // 7. the cells
@@ -993,8 +1006,10 @@ void tree_build_shifted(TreeDev &t, const double *xs, const double *ys, const do
   ++g_launches;
   if (cudaLaunchCooperativeKernel((const void *)k_tree_build, g_tree_blocks, TB_THREADS, params, 0,
                                   st) != cudaSuccess) {
-    // report it: without the launch the cells are stale
-    cudaMemsetAsync(t.info + 5, 0xff, sizeof(uint32_t), st);
+    // report it: without the launch the cells, perm and leaf_of are stale,
+    // so the passes that follow see an empty tree (info[1] = 0) and the
+    // launch-failure mark (info[5] = 0xffffffff), which they check
+    D3_LAUNCH(k_tree_failed, 1, 1, 0, st)(t.info, status);
   }
 }
 

@@ -191,7 +191,7 @@ class Slot:
         """src/core.js:213-231: PRECISION, fast-mode ORDER / OPENING and SEED."""
         ctx = self.ctx
         fast = ctx.precision
-        self.scalar(C.PRECISION, 1 if fast else 0)
+        self.scalar(C.PRECISION, fast["form"] if fast else 0)
         if fast:
             self.scalar(C.ORDER, fast["order"])
             self.scalar(C.OPENING, fast["opening"])
@@ -749,7 +749,7 @@ class Simulation:
         for f in self._forces.values():
             f._push()
             s = f.slot
-            s.scalar(C.PRECISION, 1 if ctx.precision else 0)
+            s.scalar(C.PRECISION, ctx.precision["form"] if ctx.precision else 0)
             if ctx.precision:
                 s.scalar(C.ORDER, ctx.precision["order"])
                 s.scalar(C.OPENING, ctx.precision["opening"])
@@ -829,17 +829,27 @@ class Simulation:
             self._forces[name] = self._initialize_force(f)
         return self
 
-    def precision(self, mode=None, order=None, opening=None):
-        """simulation.js:187-200"""
+    # fast-mode forms of the many-body force: the PRECISION scalar the core gets
+    FORMS = {"plain": 1, "bf16x3": 2, "learned": 3}
+
+    def precision(self, mode=None, order=None, opening=None, form="plain"):
+        """simulation.js:187-200. `form` (no counterpart in the reference)
+        picks the fast many-body force: "plain" is the reference's FP64 FMM
+        bit for bit; "bf16x3" the tensor-core FMM (M2L as BF16x3 contractions
+        on geometric cells, FP32 near field; order up to 15, opening 1 to 2);
+        "learned" order 4 with the learned per-leaf correction."""
         if mode is None:
             return self._precision
         if mode not in ("exact", "fast"):
             raise ValueError('precision must be "exact" or "fast"')
+        if form not in self.FORMS:
+            raise ValueError("form must be one of " + ", ".join(sorted(self.FORMS)))
         self._precision = mode
         if mode == "fast":
             o = order if order else 8
             self.ctx.precision = {"order": min(24, max(1, round(float(o)))),
-                                  "opening": max(1.01, float(opening) if opening else 1.5)}
+                                  "opening": max(1.01, float(opening) if opening else 1.5),
+                                  "form": self.FORMS[form]}
         else:
             self.ctx.precision = None
         return self

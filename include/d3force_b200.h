@@ -198,6 +198,20 @@ int32_t sim_set_profile(uint32_t h, uint32_t on);
  * call returns D3_WORKER_FAILED; the simulation stays usable. */
 int32_t sim_selftest_wait(uint32_t h, uint32_t budget_us);
 
+/* ---- Device rates for the roofline (no counterpart in the reference) ----
+ *
+ * Times microbenchmarks on the current device with CUDA events and fills
+ * out[0..7]: DADD/s, DMUL/s, DFMA/s, IEEE f64 divisions/s and square roots/s
+ * over the whole GPU (independent chains, full occupancy); the one-way
+ * handoff latency in microseconds between two SMs (a release store to a
+ * global flag seen by another SM's acquire load, half a timed ping-pong
+ * round trip); the SM count; the SM clock attribute in kHz. The exact tick
+ * runs on the FP64 pipe without FMA and waits through L2, so these are its
+ * roofline denominators. len must be >= 8. Every device wait is bounded;
+ * D3_WORKER_FAILED if one ran out or a launch failed. Allocates and frees a
+ * few bytes of device memory. */
+int32_t d3_device_peaks(double *out, uint32_t len);
+
 /* ---- Allocation-free entry point (no counterpart in the reference) ------
  *
  * For callers that cannot let a library allocate device memory (an engine
@@ -209,13 +223,18 @@ int32_t sim_selftest_wait(uint32_t h, uint32_t budget_us);
  * that loads the library until the process exits. No cudaMalloc / cudaFree is
  * called. `*lcg_state` (host) is d3's LCG state for jiggle draws, updated on
  * return. Runs on `stream` (a cudaStream_t; NULL = the default stream) and
- * returns when the work is done. The first call on each device looks up the
- * array's device address (set-up), so make it before any stream capture.
- * Calls share the array: calls that overlap on the GPU (other threads or
- * streams) race. Returns D3_OK; D3_BAD_ARGUMENT when n exceeds
- * D3_NOALLOC_MAX_NODES or a pointer is missing; D3_ARENA_FULL when the tree
- * needs more cells than the array holds (points closer than 2^-32 of the
- * extent in long chains); D3_WORKER_FAILED on a CUDA error. */
+ * returns when the work is done: every call ends by copying its status to
+ * the host and synchronising `stream`, so no call can be made while that
+ * stream is being captured into a CUDA graph. The first call on each device
+ * looks up the array's device address (set-up, done once per device and safe
+ * when threads race to it). Calls share the array: calls that overlap on the
+ * GPU (other threads or streams) race. Returns D3_OK; D3_BAD_ARGUMENT when n
+ * exceeds D3_NOALLOC_MAX_NODES or a pointer is missing; D3_ARENA_FULL when
+ * the tree needs more cells than the array holds (4n + 1024; clustered input
+ * can need that many: d3's quadtree makes a chain of single-child cells down
+ * to the level that separates two close points), in which case vx and vy are
+ * left unchanged; D3_WORKER_FAILED on a CUDA error, a failed launch or a
+ * device-side failure (a bounded wait that ran out). */
 #define D3_NOALLOC_MAX_NODES 8192u
 int32_t d3_many_body_exact_noalloc(const double *x, const double *y, double *vx, double *vy,
                                    const double *strength, uint32_t n, double theta2,

@@ -16,7 +16,9 @@ LIB = os.path.join(ORACLE_DIR, "_build", "libd3oracle.so")
 
 def build():
     src = os.path.join(ORACLE_DIR, "d3force_oracle.c")
-    if not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(src):
+    mk = os.path.join(ORACLE_DIR, "Makefile")
+    if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(src),
+                                                              os.path.getmtime(mk)):
         subprocess.check_call(["make", "-s", "-C", ORACLE_DIR])
     return LIB
 
@@ -29,4 +31,6 @@ def load(pkg):
     c.lib.oracle_set_threads.argtypes = [ctypes.c_uint32, ctypes.c_uint32]
     c.lib.oracle_fmm_stat.restype = ctypes.c_uint64
     c.lib.oracle_fmm_stat.argtypes = [ctypes.c_uint32]
+    c.lib.oracle_mb_stat.restype = ctypes.c_uint64
+    c.lib.oracle_mb_stat.argtypes = [ctypes.c_uint32]
     return c

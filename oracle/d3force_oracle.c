@@ -1118,9 +1118,21 @@ typedef struct {
   Sim *s; /* random source; NULL = record mode (report, do not draw) */
 } MbTrav;
 
+/* Work counters of the exact many-body traversal (for the roofline, not part
+ * of the reference): cells visited, accepted far-field approximations, leaf
+ * point interactions. */
+static uint64_t mb_visits, mb_accepts, mb_points;
+
+static void mb_count(uint64_t v, uint64_t a, uint64_t pts) {
+  __atomic_add_fetch(&mb_visits, v, __ATOMIC_RELAXED);
+  __atomic_add_fetch(&mb_accepts, a, __ATOMIC_RELAXED);
+  __atomic_add_fetch(&mb_points, pts, __ATOMIC_RELAXED);
+}
+
 /* many_body.zig:176-263: d3's traversal for node i. With s == NULL it returns
  * 0 without writing at the first point where d3 would draw. */
 static int mb_node(const MbTrav *p, uint32_t i, uint32_t *stack) {
+  uint64_t nv = 0, na = 0, np = 0;
   const Cell *cells = p->t->cells;
   const uint32_t *perm = p->t->perm;
   double nx = p->xs[i], ny = p->ys[i];
@@ -1131,12 +1143,14 @@ static int mb_node(const MbTrav *p, uint32_t i, uint32_t *stack) {
     const Cell *quad = &cells[stack[--sp]];
     double value = quad->value;
     if (!(value != 0 && value == value)) continue;
+    ++nv;
     double x = quad->x - nx, y = quad->y - ny;
     double w = quad->x1 - quad->x0;
     double l = x * x + y * y;
     if (w * w / p->theta2 < l) {
       if (l < p->dmax2) {
-        if (!p->s && (x == 0 || y == 0)) return 0;
+        ++na;
+        if (!p->s && (x == 0 || y == 0)) { mb_count(nv, na, np); return 0; }
         if (x == 0) { x = jiggle(p->s); l += x * x; }
         if (y == 0) { y = jiggle(p->s); l += y * y; }
         if (l < p->dmin2) l = sqrt(p->dmin2 * l);
@@ -1153,7 +1167,7 @@ static int mb_node(const MbTrav *p, uint32_t i, uint32_t *stack) {
     if (l >= p->dmax2) continue;
     uint32_t head = perm[quad->first + quad->count - 1];
     if (head != i || quad->count > 1) {
-      if (!p->s && (x == 0 || y == 0)) return 0;
+      if (!p->s && (x == 0 || y == 0)) { mb_count(nv, na, np); return 0; }
       if (x == 0) { x = jiggle(p->s); l += x * x; }
       if (y == 0) { y = jiggle(p->s); l += y * y; }
       if (l < p->dmin2) l = sqrt(p->dmin2 * l);
@@ -1162,6 +1176,7 @@ static int mb_node(const MbTrav *p, uint32_t i, uint32_t *stack) {
       --k;
       uint32_t j = perm[k];
       if (j != i) {
+        ++np;
         double wj = p->strengths[j] * p->alpha / l;
         vx += x * wj;
         vy += y * wj;
@@ -1170,6 +1185,7 @@ static int mb_node(const MbTrav *p, uint32_t i, uint32_t *stack) {
   }
   p->vxs[i] = vx;
   p->vys[i] = vy;
+  mb_count(nv, na, np);
   return 1;
 }
 
@@ -2271,6 +2287,17 @@ int32_t oracle_set_threads(uint32_t h, uint32_t k) {
   if (!s) return D3_BAD_HANDLE;
   s->threads = k < 1 ? 1 : k > 64 ? 64 : (int)k;
   return D3_OK;
+}
+
+/* Oracle-only: the exact many-body work counters since the last reset
+ * (which 0 visits, 1 accepted approximations, 2 leaf point interactions;
+ * which 3 resets them and returns 0). */
+uint64_t oracle_mb_stat(uint32_t which) {
+  if (which == 3) {
+    mb_visits = mb_accepts = mb_points = 0;
+    return 0;
+  }
+  return which == 0 ? mb_visits : which == 1 ? mb_accepts : mb_points;
 }
 
 /* Oracle-only: interaction counters of the last FMM run (fmm.zig:59). */

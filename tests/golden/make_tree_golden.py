@@ -8,7 +8,7 @@ keeps the inputs and replaces each structure by the SHA-256 of its canonical
 JSON (`canonical` below), so the fixture is small and still bit-exact. The
 tests rebuild the same structures from a built tree and compare digests.
 
-    python tests/golden/make_tree_golden.py [path/to/tree-traces.json]
+    python tests/golden/make_tree_golden.py <reference checkout>/test/fixtures/tree-traces.json
 """
 
 import hashlib
@@ -17,7 +17,6 @@ import os
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-DEFAULT_SRC = "/root/reference/test/fixtures/tree-traces.json"
 
 
 def canonical(obj):
@@ -45,4 +44,6 @@ def main(src):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else DEFAULT_SRC)
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_tree_golden.py <path to the reference's test/fixtures/tree-traces.json>")
+    main(sys.argv[1])

@@ -107,3 +107,24 @@ def check_trace(core, name, ref):
     assert canonical(got["shape"]) == ref["shape"], "%s: shape and leaf chains" % name
     assert canonical(got["visit"]) == ref["visit"], "%s: visit order and bounds" % name
     assert canonical(got["after"]) == ref["after"], "%s: visitAfter order and bounds" % name
+
+
+def clustered_pairs(n, seed, scale=2.0 ** -20):
+    """n points: n/2 uniform in [-400, 400)^2, each with a partner offset by
+    between 0.5 and 1 x 800 * scale on each axis. d3's quadtree separates a
+    pair only at the level where the two fall in different quadrants, so each
+    pair hangs a chain of single-child cells below the uniform points' levels:
+    at scale 2^-20 the tree needs more than the 4n + 1024 cells the engine
+    reserves."""
+    rng = np.random.default_rng(seed)
+    b = n // 2
+    x = np.empty(n)
+    y = np.empty(n)
+    x[:b] = (rng.random(b) - 0.5) * 800
+    y[:b] = (rng.random(b) - 0.5) * 800
+    off = 800 * scale * (0.5 + 0.5 * rng.random((b, 2)))
+    x[b:2 * b] = x[:b] + off[:, 0]
+    y[b:2 * b] = y[:b] + off[:, 1]
+    if n % 2:
+        x[-1] = y[-1] = 0.0
+    return x, y

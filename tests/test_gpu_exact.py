@@ -7,6 +7,7 @@ velocities, alpha and the random stream position.
 """
 
 import math
+import os
 
 import numpy as np
 import pytest
@@ -116,10 +117,70 @@ def test_gpu_host_random_source(ocore, gcore):
 
 
 @pytest.mark.slow
-def test_gpu_exact_50k_collide(ocore, gcore):
-    """The 50k + collide benchmark workload, bitwise for the first ticks."""
-    P.run_pair(_defaults(50000, 100000, collide=5, coincident=0.01, near=0.01, pinned=0.005),
-               ocore, gcore, 5)
+def test_gpu_exact_50k_collide_every_tick_of_300(ocore, gcore):
+    """The 50k + collide benchmark workload (1% coincident, 1% offsets below
+    1e-12, 0.5% pinned), bitwise with the oracle after every one of its 300
+    ticks: positions, velocities, alpha, and the random stream position at
+    ticks 1, 5, 25, 100, 200 and 300 (test/parity/parity-test.js:23-58 checks
+    each tick with Object.is and the stream's next value at the end). The
+    oracle runs on all host threads; its threaded ticks are the serial ones
+    bit for bit (test_oracle.py, test_threaded_oracle_ticks_bitwise)."""
+    setup = _defaults(50000, 100000, collide=5, coincident=0.01, near=0.01, pinned=0.005)
+    na, sa = setup(ocore)
+    nb, sb = setup(gcore)
+    ocore.lib.oracle_set_threads(sa.ctx.h, os.cpu_count() or 1)
+    try:
+        assert P.first_difference(na, nb) is None, "after initialize"
+        for t in range(1, 301):
+            sa.tick()
+            sb.tick()
+            d = P.first_difference(na, nb)
+            assert d is None, "tick %d: %s" % (t, d)
+            assert sa.alpha() == sb.alpha(), "tick %d: alpha" % t
+            if t in (1, 5, 25, 100, 200, 300):
+                assert ocore.sim_get_lcg(sa.ctx.h) == gcore.sim_get_lcg(sb.ctx.h), \
+                    "tick %d: random stream position" % t
+    finally:
+        sa.close()
+        sb.close()
+
+
+def test_gpu_tree_overflow_leaves_an_empty_tree(ocore, gcore):
+    """A tree that needs more cells than the engine reserves (4n + 1024; the
+    clustered pairs below need about 7.8n, test_oracle.py checks that on the
+    oracle) is reported, not written past its buffers: tree_build returns
+    D3_WORKER_FAILED with an empty tree, a many-body force_run leaves the
+    velocities as they were and the next sync reports the failure once, and
+    the simulation then works normally on points that fit."""
+    n = 2000
+    x, y = H.clustered_pairs(n, 3)
+    h = gcore.sim_create()
+    try:
+        assert gcore.sim_set_node_count(h, n) >= 0
+        gcore.sim_set_sync(h, H.C.SYNC_EXPLICIT)
+        vx0 = np.linspace(-1, 1, n)
+        for w, arr in ((H.C.PTR_X, x), (H.C.PTR_Y, y), (H.C.PTR_VX, vx0), (H.C.PTR_VY, -vx0)):
+            gcore.f64_view(gcore.sim_ptr(h, w), n)[:] = arr
+        gcore.u8_view(gcore.sim_ptr(h, H.C.PTR_FIXED), n)[:] = 0
+        assert gcore.sim_sync_in(h) == 0
+        assert gcore.tree_build(h, 0) == H.C.WORKER_FAILED
+        assert gcore.tree_info(h, 0) == 0
+        fh = gcore.force_create(h, H.C.MANY_BODY)
+        gcore.f64_view(gcore.force_ptr(h, fh, H.C.F0), n)[:] = -30.0
+        gcore.force_set_scalar(h, fh, H.C.THETA2, 0.81)
+        gcore.force_set_scalar(h, fh, H.C.DISTANCE_MIN2, 1.0)
+        gcore.force_set_scalar(h, fh, H.C.DISTANCE_MAX2, float("inf"))
+        assert gcore.force_run(h, fh, 1.0) == 0
+        assert gcore.sim_sync_out(h) == H.C.WORKER_FAILED
+        got = gcore.f64_view(gcore.sim_ptr(h, H.C.PTR_VX), n)
+        assert np.array_equal(P.bits(got), P.bits(vx0))
+        assert gcore.sim_sync_out(h) == 0  # reported once
+        # the same nodes spread out: the tree fits and matches the oracle's
+        xs, ys = H.clustered_pairs(n, 3, scale=2.0 ** -6)
+        a, b = H.trace(ocore, xs, ys), H.trace(gcore, xs, ys)
+        assert a["cells"] == b["cells"] and a["visit"] == b["visit"]
+    finally:
+        gcore.sim_destroy(h)
 
 
 def test_gpu_sim_tick_path_matches(ocore, gcore):

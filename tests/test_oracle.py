@@ -178,6 +178,24 @@ def test_tree_near_duplicates_separate(ocore):
     ocore.sim_destroy(h)
 
 
+def test_clustered_pairs_need_more_cells_than_reserved(ocore):
+    """The input the overflow tests on the GPU use: the oracle's tree (the
+    reference's cell layout) needs more than the 4n + 1024 cells the engine
+    and the allocation-free entry point reserve, so those tests exercise a
+    real overflow; the same points at a coarser offset fit."""
+    for n in (2000, 8192):
+        x, y = H.clustered_pairs(n, 3)
+        h = H.build_tree(ocore, x, y)
+        cells = len(ocore.tree(h)["cells"])
+        ocore.sim_destroy(h)
+        assert cells > 4 * n + 1024, (n, cells)
+    x, y = H.clustered_pairs(2000, 3, scale=2.0 ** -6)
+    h = H.build_tree(ocore, x, y)
+    cells = len(ocore.tree(h)["cells"])
+    ocore.sim_destroy(h)
+    assert cells <= 4 * 2000 + 1024, cells
+
+
 def test_tree_order_pre_and_post(ocore):
     """tests.zig:97-116"""
     h = H.build_tree(ocore, np.array([0, 3, 1, 2, 3.5]), np.array([0, 3, 2, 1, 0.5]))

@@ -92,6 +92,52 @@ def test_no_alloc_many_body_matches_force_run(gcore):
     assert lcg_ref != 1  # the coincident pairs drew from the stream
 
 
+def test_no_alloc_many_body_matches_oracle(ocore, gcore):
+    """The entry point against the CPU oracle's force_run directly (the
+    oracle restates many_body.zig), bit for bit, on two calls in a row."""
+    import torch
+
+    fn = _bind(gcore.lib)
+    n = 3000
+    x, y, vx, vy, strength = _nodes(n, 11)
+    dev = lambda a: torch.tensor(a, dtype=torch.float64, device="cuda")  # noqa: E731
+    tx, ty, tvx, tvy, ts = dev(x), dev(y), dev(vx), dev(vy), dev(strength)
+    lcg_ref, lcg = 1, ctypes.c_uint32(1)
+    ref_vx, ref_vy = vx, vy
+    for call, alpha in enumerate((0.5, 0.25)):
+        ref_vx, ref_vy, lcg_ref = _force_run(ocore, x, y, ref_vx, ref_vy, strength, alpha, lcg_ref)
+        rc = fn(tx.data_ptr(), ty.data_ptr(), tvx.data_ptr(), tvy.data_ptr(), ts.data_ptr(), n,
+                0.81, 1.0, float("inf"), alpha, ctypes.byref(lcg), None)
+        assert rc == 0, "call %d: status %d" % (call, rc)
+        got_vx, got_vy = tvx.cpu().numpy(), tvy.cpu().numpy()
+        assert np.array_equal(got_vx.view(np.uint64), ref_vx.view(np.uint64)), "call %d: vx" % call
+        assert np.array_equal(got_vy.view(np.uint64), ref_vy.view(np.uint64)), "call %d: vy" % call
+        assert lcg.value == lcg_ref, "call %d: random stream position" % call
+
+
+def test_no_alloc_tree_overflow_is_reported_and_harmless(gcore):
+    """Points whose tree needs more cells than the static array holds
+    (clustered pairs: about 7.3n cells against 4n + 1024, checked on the
+    oracle in test_oracle.py) return D3_ARENA_FULL with vx, vy and the random
+    stream untouched, and the next call on ordinary points is correct."""
+    import torch
+
+    fn = _bind(gcore.lib)
+    n = 8192
+    x, y = H.clustered_pairs(n, 3)
+    vx = np.linspace(-1, 1, n)
+    dev = lambda a: torch.tensor(a, dtype=torch.float64, device="cuda")  # noqa: E731
+    tx, ty, tvx, tvy, ts = dev(x), dev(y), dev(vx), dev(-vx), dev(np.full(n, -30.0))
+    lcg = ctypes.c_uint32(12345)
+    rc = fn(tx.data_ptr(), ty.data_ptr(), tvx.data_ptr(), tvy.data_ptr(), ts.data_ptr(), n,
+            0.81, 1.0, float("inf"), 1.0, ctypes.byref(lcg), None)
+    assert rc == C.ARENA_FULL
+    assert np.array_equal(tvx.cpu().numpy().view(np.uint64), vx.view(np.uint64))
+    assert np.array_equal(tvy.cpu().numpy().view(np.uint64), (-vx).view(np.uint64))
+    assert lcg.value == 12345
+    test_no_alloc_many_body_matches_force_run(gcore)
+
+
 def test_no_alloc_rejects_too_many_nodes(gcore):
     fn = _bind(gcore.lib)
     lcg = ctypes.c_uint32(1)

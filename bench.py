@@ -213,66 +213,187 @@ class Clocks:
 
 
 FAST_N = 1000000
+FAST_ORDER, FAST_OPENING = 8, 1.5
 
 
-def fast_1m(pkg, core, torch, steps=10, warmup=3, targets=1024):
-    """Fast mode at the 1M-node configuration: n uniform in [0, 1e4)^2 (seeded),
-    m = 2n uniform links, forceManyBody (FMM order 8, opening 1.5,
-    distanceMin 1) + forceLink + forceCenter, device ms per tick over `steps`
-    ticks; plus the many-body kick's RMS error on seeded targets against an
-    FP64 direct sum of d3's pair formula (test/fast/error-test.js:44-70)."""
+def fast_layout(n=FAST_N, seed=1):
+    """The fast-mode precision configuration: n nodes uniform in [0, 1e4)^2
+    and m = 2n uniform random links without self-loops (seeded)."""
     import numpy as np
-    n = FAST_N
-    rng = np.random.default_rng(1)
+    rng = np.random.default_rng(seed)
     xs = rng.random(n) * 1e4
     ys = rng.random(n) * 1e4
     src = rng.integers(0, n, 2 * n)
     tgt = (src + 1 + rng.integers(0, n - 1, 2 * n)) % n
-    nodes = pkg.Nodes(n, x=xs, y=ys)
+    return xs, ys, src, tgt
+
+
+def fast_sim(pkg, core, xs, ys, src, tgt, form, order=FAST_ORDER, opening=FAST_OPENING):
+    nodes = pkg.Nodes(len(xs), x=xs, y=ys)
     sim = pkg.forceSimulation(nodes, core=core)
     sim.force("charge", pkg.forceManyBody())
     sim.force("link", pkg.forceLink(src, tgt))
     sim.force("center", pkg.forceCenter())
-    sim.precision("fast", order=8, opening=1.5)
+    sim.precision("fast", order=order, opening=opening, form=form)
+    return nodes, sim
+
+
+def fast_ticks(pkg, core, layout, form, flush_l2, steps=10, warmup=3):
+    """Device ms per fast tick (manyBody + link + center) over `steps` ticks
+    after `warmup`, L2 flushed before each; also the state digest after 3
+    ticks of a fresh run (the bit-exactness check of the plain form)."""
+    xs, ys, src, tgt = layout
+    nodes, sim = fast_sim(pkg, core, xs, ys, src, tgt, form)
     sim.device_begin()
     for _ in range(warmup):
+        flush_l2()
         sim.device_ticks(1)
-    times = [sim.device_ticks(1) for _ in range(steps)]
+    times = []
+    for _ in range(steps):
+        flush_l2()
+        times.append(sim.device_ticks(1))
     sim.device_end()
     sim.close()
-    # RMS of the many-body kick alone, from the start layout with zero velocity
+    return sum(times) / len(times)
+
+
+def fast_digest(pkg, core, layout, form, ticks=3):
+    xs, ys, src, tgt = layout
+    nodes, sim = fast_sim(pkg, core, xs, ys, src, tgt, form)
+    sim.tick(ticks)
+    d = state_digest(nodes, core.sim_get_lcg(sim.ctx.h))
+    sim.close()
+    return d
+
+
+def fast_rms(pkg, core, layout, form, targets=4096):
+    """The many-body kick of one tick against the FP64 direct sum on
+    `targets` seeded nodes (accuracy.py)."""
+    import numpy as np
+    acc = importlib.import_module("d3-force-wasm_b200.accuracy")
+    xs, ys = layout[0], layout[1]
+    kick, alpha = acc.many_body_kick(pkg, core, xs, ys, form=form, order=FAST_ORDER,
+                                     opening=FAST_OPENING)
+    tg = acc.sample_targets(xs, ys, targets)
+    ref = acc.direct_kick(xs, ys, np.full(len(xs), -30.0 * alpha), tg)
+    return acc.rms(kick, ref, tg)
+
+
+def fast_1m(pkg, core, torch, flush_l2, cpu=True):
+    """Fast mode at 1M nodes: the reference's FP64 FMM ("plain", bit for bit)
+    and the tensor-core form ("bf16x3": BF16x3 M2L, FP32 near field), both at
+    order 8 / opening 1.5 / distanceMin 1, with link and center; ms per tick
+    and RMS of the many-body kick against an FP64 direct sum on 4,096
+    targets. The CPU leg ticks the oracle's fast mode (one thread) and checks
+    the plain form's state after 3 ticks bit for bit."""
+    layout = fast_layout()
+    out = {"workload": "fast n=1000000 m=2000000 uniform [0,1e4)^2; manyBody FMM order 8, "
+                       "opening 1.5, distanceMin 1 + link + center",
+           "l2": "flushed before every tick"}
+    for form in ("plain", "bf16x3"):
+        ms = fast_ticks(pkg, core, layout, form, flush_l2)
+        out[form] = {"ms_per_tick": round(ms, 4), "steps": 10, "warmup": 3,
+                     "rms_vs_direct_sum": fast_rms(pkg, core, layout, form),
+                     "rms_targets": 4096}
+    out["bf16x3"]["speedup_vs_plain"] = round(out["plain"]["ms_per_tick"] /
+                                              out["bf16x3"]["ms_per_tick"], 3)
+    if cpu:
+        import oracle
+        ocore = oracle.load(pkg)
+        xs, ys, src, tgt = layout
+        nodes, sim = fast_sim(pkg, ocore, xs, ys, src, tgt, "plain")
+        sim.tick(1)
+        t0 = time.perf_counter()
+        sim.tick(2)
+        cpu_ms = (time.perf_counter() - t0) * 1e3 / 2
+        dig_cpu = state_digest(nodes, ocore.sim_get_lcg(sim.ctx.h))
+        sim.close()
+        out["plain"]["bit_exact_vs_oracle_3_ticks"] = dig_cpu == fast_digest(pkg, core, layout,
+                                                                             "plain")
+        out["cpu_baseline"] = {"value": round(cpu_ms, 1), "unit": "ms/tick", "cores": 1,
+                               "kind": "port",
+                               "sample": "ticks 2-3 of the same workload on the oracle (C "
+                                         "restatement of the reference's fast mode), one thread"}
+    return out
+
+
+LEARN_LAYOUTS, LEARN_N = 200, 100000
+
+
+def learned_1m(pkg, core, torch, flush_l2):
+    """The learned form at 1M nodes on the Gaussian-mixture configuration
+    (64 clusters, sigma 50-500, Dirichlet(1) weights; SBM links, mean degree
+    4, p_in / p_out 20), beside the plain FP64 order-8 FMM and the order-8
+    tensor-core form: the network is trained here, on the GPU, by the
+    package's kernels on order-4 / order-12 pairs of 200 seeded layouts of
+    the same recipe at 100k nodes; the learned form's ticks include its
+    sampled check (64 nodes, FP64 direct sum, tolerance 1e-5) and any
+    fallback to the order-8 form."""
+    import numpy as np
+    learned = importlib.import_module("d3-force-wasm_b200.learned")
+    acc = importlib.import_module("d3-force-wasm_b200.accuracy")
+    t0 = time.perf_counter()
+    layouts = [learned.mixture_layout(LEARN_N, 1000 + k)[:2] for k in range(LEARN_LAYOUTS)]
+    X, Y = learned.training_pairs(core, layouts)
+    t1 = time.perf_counter()
+    params, losses = learned.train(core, X, Y)
+    t2 = time.perf_counter()
+    xs, ys, lab = learned.mixture_layout(FAST_N, 7)
+    src, tgt = learned.sbm_links(lab, 7)
+    out = {"workload": "fast n=1000000 Gaussian mixture (64 clusters, sigma 50-500, Dirichlet(1)) "
+                       "+ SBM links (m=2n, p_in/p_out 20) + center; manyBody opening 1.5, "
+                       "distanceMin 1",
+           "training": {"layouts": LEARN_LAYOUTS, "nodes_per_layout": LEARN_N,
+                        "samples": int(len(X)), "steps": len(losses), "batch": 8192,
+                        "loss_first": float(losses[:10].mean()),
+                        "loss_last": float(losses[-50:].mean()),
+                        "pairs_s": round(t1 - t0, 2), "train_s": round(t2 - t1, 2)}}
+    tg = acc.sample_targets(xs, ys, 4096)
+    ref = None
+    for form, order in (("plain", 8), ("bf16x3", 8), ("bf16x3", 4), ("learned", 8)):
+        nodes, sim = fast_sim(pkg, core, xs, ys, src, tgt, form, order=order)
+        if form == "learned":
+            sim.learned(params, tolerance=1e-5, samples=64)
+        sim.device_begin()
+        for _ in range(3):
+            flush_l2()
+            sim.device_ticks(1)
+        times = []
+        for _ in range(10):
+            flush_l2()
+            times.append(sim.device_ticks(1))
+        sim.device_end()
+        stats = [core.sim_stat(sim.ctx.h, 50 + k) for k in range(3)]
+        sim.close()
+        kick, alpha = acc.many_body_kick(pkg, core, xs, ys, form=form, order=order) \
+            if form != "learned" else _learned_kick(pkg, core, xs, ys, params)
+        if ref is None:
+            ref = acc.direct_kick(xs, ys, np.full(len(xs), -30.0 * alpha), tg)
+        key = form if form != "bf16x3" else "bf16x3_order%d" % order
+        out[key] = {"order": order, "ms_per_tick": round(sum(times) / len(times), 4),
+                    "rms_vs_direct_sum": acc.rms(kick, ref, tg), "rms_targets": 4096}
+        if form == "learned":
+            out[key].update({"checks": stats[0], "fallbacks": stats[1],
+                             "last_sampled_rms": stats[2]})
+    out["learned"]["speedup_vs_plain_fp64_order8"] = round(
+        out["plain"]["ms_per_tick"] / out["learned"]["ms_per_tick"], 3)
+    return out
+
+
+def _learned_kick(pkg, core, xs, ys, params):
+    """The learned form's many-body kick of one tick from zero velocity."""
+    import numpy as np
+    n = len(xs)
     nodes = pkg.Nodes(n, x=xs, y=ys, vx=np.zeros(n), vy=np.zeros(n))
     sim = pkg.forceSimulation(nodes, core=core)
     sim.force("charge", pkg.forceManyBody())
-    sim.precision("fast", order=8, opening=1.5)
+    sim.precision("fast", order=8, opening=1.5, form="learned")
+    sim.learned(params, tolerance=1e-5, samples=64)
     sim.tick()
-    a1 = sim.alpha()
-    decay = 0.6  # 1 - velocityDecay(0.4): v = kick * decay after one tick
-    kick = np.stack([(np.asarray(nodes.x) - xs) / decay, (np.asarray(nodes.y) - ys) / decay], 1)
+    alpha = sim.alpha()
+    kick = np.stack([np.asarray(nodes.vx), np.asarray(nodes.vy)], 1) / 0.6
     sim.close()
-    tg = np.random.default_rng(7).choice(n, targets, replace=False)
-    dev = torch.device("cuda")
-    X = torch.from_numpy(xs).to(dev)
-    Y = torch.from_numpy(ys).to(dev)
-    ref = torch.zeros(targets, 2, dtype=torch.float64, device=dev)
-    for k0 in range(0, targets, 64):
-        idx = torch.from_numpy(tg[k0:k0 + 64]).to(dev)
-        dx = X[None, :] - X[idx, None]
-        dy = Y[None, :] - Y[idx, None]
-        l = dx * dx + dy * dy
-        l = torch.where(l < 1.0, torch.sqrt(l), l)  # distanceMin 1: l = sqrt(dmin2 l)
-        w = torch.where(l > 0, -30.0 * a1 / torch.where(l > 0, l, torch.ones_like(l)),
-                        torch.zeros_like(l))
-        ref[k0:k0 + 64, 0] = (dx * w).sum(1)
-        ref[k0:k0 + 64, 1] = (dy * w).sum(1)
-    ref = ref.cpu().numpy()
-    err = kick[tg] - ref
-    rms = float(np.sqrt((err * err).sum() / (ref * ref).sum()))
-    return {"workload": "fast n=1000000 m=2000000 uniform [0,1e4)^2; FMM order 8, opening 1.5, "
-                        "distanceMin 1 + link + center; FP64 plain",
-            "ms_per_tick": round(sum(times) / len(times), 4), "steps": steps, "warmup": warmup,
-            "rms_vs_direct_sum": rms, "rms_targets": targets,
-            "bit_exact_vs_reference_order": True}
+    return kick, alpha
 
 
 def exact_device_run(pkg, sc, core, positions, total, flush_l2, world, profile=False):
@@ -502,7 +623,9 @@ def run_ours(args, pkg, sc):
     line["config"]["bit_exact"] = all(checks.values())
     line["bit_exact_checks"] = checks
     if not args.no_fast and world == 1:
-        line["fast_1m"] = fast_1m(pkg, pkg.cuda_core(), torch, targets=4096)
+        line["fast_1m"] = fast_1m(pkg, pkg.cuda_core(), torch, flush_l2,
+                                  cpu=not args.no_cpu_baseline)
+        line["learned_1m"] = learned_1m(pkg, pkg.cuda_core(), torch, flush_l2)
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

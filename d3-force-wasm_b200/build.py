@@ -17,10 +17,10 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 OUT = os.path.join(OUT_DIR, "libd3force_b200.so")
 SOURCES = ["engine.cu", "tree.cu", "scan_sort.cu", "forces.cu", "fast.cu", "fmm.cu", "collide_spec.cu", "noalloc.cu",
-           "peaks.cu", "fmm_tc.cu"]
+           "peaks.cu", "fmm_tc.cu", "mlp.cu", "batch.cu"]
 # The precision forms are judged by their error against an FP64 direct sum,
 # not bit for bit: their translation unit may contract to FMA.
-PER_SOURCE = {"fmm_tc.cu": ["-fmad=true"]}
+PER_SOURCE = {"fmm_tc.cu": ["-fmad=true"], "mlp.cu": ["-fmad=true"], "batch.cu": ["-fmad=true"]}
 EXACT = ["-fmad=false"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",

@@ -87,13 +87,22 @@ _SIGNATURES = {
     "sim_selftest_wait": (_I32, [_U32, _U32]),
 }
 
+# Engine-only entry points bound with signatures (the oracle has none of them).
+_ENGINE_SIGNATURES = {
+    "sim_set_learned": (_I32, [_U32, ctypes.c_void_p, _U32, _F64, _U32, _U32]),
+    "sim_fmm_leaves": (_I32, [_U32, ctypes.c_void_p, _U32]),
+}
+
 # Every symbol the header declares; the no-GPU tests check the CUDA library
 # exports all of them.
 ABI_SYMBOLS = tuple(_SIGNATURES)
 
 # Entry points of the CUDA library alone (the oracle has no counterpart):
 # declared in the header and exported by the engine, bound where they are used.
-ENGINE_SYMBOLS = ("d3_device_peaks", "d3_many_body_exact_noalloc")
+ENGINE_SYMBOLS = ("d3_device_peaks", "d3_many_body_exact_noalloc", "sim_set_learned",
+                  "sim_fmm_leaves", "d3_mlp_grad", "d3_mlp_train", "d3_mlp_infer", "batch_create",
+                  "batch_destroy", "batch_set_shape", "batch_run", "batch_kick", "batch_read",
+                  "batch_autotune")
 
 
 class Core:
@@ -110,6 +119,12 @@ class Core:
             fn.restype = res
             fn.argtypes = args
             setattr(self, sym, fn)
+        for sym, (res, args) in _ENGINE_SIGNATURES.items():
+            fn = getattr(self.lib, sym, None)
+            if fn is not None:
+                fn.restype = res
+                fn.argtypes = args
+                setattr(self, sym, fn)
 
     # Typed views of mirrors (valid until the next GROWN / resize).
     @staticmethod

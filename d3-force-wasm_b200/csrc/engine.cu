@@ -1066,6 +1066,28 @@ int32_t sim_tick(uint32_t h, uint32_t ticks, double *alpha, double alpha_target,
   return take_failure(s);
 }
 
+int32_t sim_set_learned(uint32_t h, const float *params, uint32_t len, double tolerance,
+                        uint32_t samples, uint32_t hold) {
+  DSim *s = get_sim(h);
+  if (!s) return D3_BAD_HANDLE;
+  if (!(tolerance > 0) || samples == 0 || samples > 4096) return D3_BAD_ARGUMENT;
+  const int r = fmm_tc_set_learned(s->fast, params, len);
+  if (r == -3) return D3_BAD_ARGUMENT;
+  if (r < 0) return D3_OUT_OF_MEMORY;
+  s->fast.learn_tol = tolerance;
+  s->fast.learn_samples = samples;
+  s->fast.learn_hold = hold;
+  return D3_OK;
+}
+
+int32_t sim_fmm_leaves(uint32_t h, float *out, uint32_t cap) {
+  DSim *s = get_sim(h);
+  if (!s) return D3_BAD_HANDLE;
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess) return D3_WORKER_FAILED;
+  const int n = fmm_tc_leaves(s->fast, out, cap);
+  return n < 0 ? D3_WORKER_FAILED : n;
+}
+
 int32_t sim_selftest_wait(uint32_t h, uint32_t budget_us) {
   DSim *s = get_sim(h);
   if (!s) return D3_BAD_HANDLE;
@@ -1105,6 +1127,13 @@ double sim_stat(uint32_t h, uint32_t which) {
     unsigned long long st[144];
     if (cudaMemcpy(st, s->spec.stamps, sizeof st, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
     return (double)st[which - 1000];
+  }
+  if (which >= 50 && which < 54) {
+    // the fast many-body precision forms: 50 learned-form checks, 51 of them
+    // that fell back, 52 the last check's sampled RMS, 53 cells of the last run
+    double out[4];
+    fmm_tc_stats(s->fast, out);
+    return out[which - 50];
   }
   if ((which >= 300 && which < 364) || (which >= 400 && which < 464)) {
     // the last parallel collide's first attempt: 300 + k microseconds from

@@ -23,6 +23,11 @@ struct FastScratch {
   // FMM
   void *fmm = nullptr;
   void *fmm_tc = nullptr;  // the precision forms' state
+  // the learned form's sampled check: tolerance on the RMS of the sampled
+  // kicks, sample count, ticks on the fallback after a failed check; counters
+  double learn_tol = 1e-5;
+  uint32_t learn_samples = 64, learn_hold = 0;
+  double learn_checks = 0, learn_fallbacks = 0, learn_last_rms = 0;
 };
 
 int fast_reserve(FastScratch &s, uint32_t n);
@@ -90,6 +95,14 @@ int fmm_tc_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *st
                const FmmParams &p, int form, const double *seed, uint32_t *status,
                cudaStream_t st);
 void fmm_tc_free(FastScratch &s);
+// Installs the learned form's network (MLP_PARAMS floats, host): 0, or < 0.
+int fmm_tc_set_learned(FastScratch &s, const float *params, uint32_t len);
+// The last precision-form run's per-cell rows (16 floats: features, L'_0, sc,
+// the cell index for leaves or -1) into out when cap >= the cell count;
+// returns the cell count.
+int fmm_tc_leaves(FastScratch &s, float *out, uint32_t cap);
+// checks, fallbacks, last sampled RMS, cells of the last run
+void fmm_tc_stats(FastScratch &s, double *out);
 // fmm.zig:247-354. Returns 1 when applied, 0 when the exact kernel must run
 // instead (non-finite extent), < 0 on failure.
 int fmm_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *strengths,

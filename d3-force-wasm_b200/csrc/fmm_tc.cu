@@ -10,7 +10,7 @@
 // and expansions are stored normalised by the cell side s:
 //     M'_k = M_k / s^k,    L'_l = L_l * s^(l+1),
 // in the scaled coordinates u = (x - ox) / w of fmm.zig:668-682. Then, for
-// two cells of one level at integer offset v (in cell sides),
+// two cells of one level with c_A - c_B = s v (v integer),
 //     L'_l += (-1)^l sum_k C(k+l, l) M'_k / v^(k+l+1),
 // a fixed q x q complex matrix per v, the same at every level; M2M and L2L
 // are fixed matrices per child quadrant. With the separation test
@@ -52,6 +52,7 @@
 #include <vector>
 
 #include "fast.cuh"
+#include "mlp.cuh"
 #include "tc.cuh"
 
 namespace cg = cooperative_groups;
@@ -73,7 +74,12 @@ constexpr uint32_t TC_NONE = 0xFFFFFFFFu;
 constexpr uint32_t TC_NEAR_FLAG = 0x8000u;
 // info words
 enum : uint32_t { TI_POOL_P2P = 0, TI_POOL_W, TI_POOL_X, TI_POOL_C, TI_OVF, TI_GROUP = 8,
-                  TI_ERR = 16, TI_WORDS = 32 };
+                  TI_LEAVES = 12, TI_ERR = 16, TI_WORDS = 32 };
+// The learned correction's output unit: the network predicts
+// (L'_0 at order 12 - L'_0 at order 4) / sc * LEARN_TARGET_SCALE.
+constexpr float LEARN_TARGET_SCALE = 1000.f;
+constexpr uint32_t LEARN_ORDER = 4;
+constexpr uint32_t CHECK_THREADS = 256;
 
 // A cell of the geometric tree: the square of level `level` at integer
 // coordinates (ix, iy), side 2^-level in scaled coordinates, centre
@@ -97,12 +103,20 @@ struct TcTables {
   float l2l_re[4][TC_MAXQ][TC_MAXQ], l2l_im[4][TC_MAXQ][TC_MAXQ];   // [b][m][l]
 };
 
-struct TcDev {
-  uint32_t ccap = 0, pcap = 0, p = 0;
+// The tables of one (order, opening): operators on the device, and their
+// host copy.
+struct TcTabSet {
+  uint32_t p = 0;
   double kappa = 0;
   TcTables *tab = nullptr;
-  TcTables h_tab;
   unsigned char *wops = nullptr;  // [class][hi, lo][32 x 32 bf16, B tile layout]
+  TcTables h;
+};
+
+struct TcDev {
+  uint32_t ccap = 0, pcap = 0, lcap = 0;
+  TcTabSet sets[2];  // the last two (order, opening) pairs used
+  uint32_t next_set = 0;
   TcCell *cells = nullptr;
   double *mco = nullptr;            // M' (FP64), 2q per cell
   __nv_bfloat16 *mbf = nullptr;     // M' hi (32) then lo (32) per cell
@@ -116,6 +130,15 @@ struct TcDev {
   float2 *far = nullptr;            // per sorted point
   uint32_t *info = nullptr, *h_info = nullptr;
   int coop_lists = 0, coop_up = 0, coop_down = 0;
+  // the learned form
+  float *feat = nullptr;             // per cell: 16 floats (k_tc_features)
+  uint32_t *leaves = nullptr;        // leaf cells (ccap)
+  float *mlp_x = nullptr, *mlp_y = nullptr;  // per leaf: 12 inputs, 2 outputs
+  double2 *kick = nullptr;           // per sorted point: the many-body kick
+  double *chk = nullptr, *h_chk = nullptr;   // sampled check: sum err^2, sum ref^2
+  float *mlp = nullptr;              // installed network parameters (device)
+  uint32_t ncells_last = 0;
+  uint32_t hold = 0;                 // ticks left on the fallback after a failed check
 };
 
 struct TcArgs {
@@ -132,6 +155,9 @@ struct TcArgs {
   uint32_t *near, *m2l, *groups, *loff, *pool;
   size_t pool_cap;
   float2 *far;
+  float *feat, *mlp_x, *mlp_y;
+  uint32_t *leaves;
+  double2 *kick;  // non-null: the many-body kick goes here instead of into vx, vy
   double *vx, *vy;
   uint32_t *info;
   uint32_t *status;     // the simulation's status word (ST_WAIT_TIMEOUT on a failed wait)
@@ -190,6 +216,7 @@ __global__ void k_tc_geom(TcArgs a) {
   t.nchild = (uint8_t)nch;
   t.child0 = nch ? f.child0 : 0;
   a.cells[c] = t;
+  if (nch == 0) a.leaves[atomicAdd(&a.info[TI_LEAVES], 1u)] = c;
   if (c == 0)  // the root gets no M2L: its local expansion starts at zero
     for (uint32_t k = 0; k < TC_KN; ++k) a.lco[k] = 0;
   if (f.depth > 0) {
@@ -497,12 +524,13 @@ struct M2lSmem {
   uint32_t err;
 };
 
-// Budget of a wait on a barrier the tile's own threads complete: 2^22 polls.
-constexpr uint32_t TC_WAIT_POLLS = 1u << 22;
+// Budget of a wait on a barrier the tile's own threads complete.
+constexpr uint64_t TC_WAIT_NS = 50ull * 1000 * 1000;
 
 __global__ void __launch_bounds__(TC_TILE) k_tc_m2l(TcArgs a) {
   extern __shared__ __align__(1024) unsigned char tc_m2l_smem[];
   M2lSmem &S = *reinterpret_cast<M2lSmem *>(tc_m2l_smem);
+  volatile uint32_t *abort = &S.err;
   const uint32_t t = threadIdx.x, warp = t >> 5;
   // this CTA's tile: group g, rows base .. base + 127
   uint32_t g = 0, tile = blockIdx.x, cnt = 0;
@@ -536,10 +564,11 @@ __global__ void __launch_bounds__(TC_TILE) k_tc_m2l(TcArgs a) {
   const uint32_t tmem = S.tmem;
   const uint32_t my = S.tgt[t];
   const uint32_t idesc = tc::idesc_bf16_f32(TC_TILE, TC_KN);
-  bool ok = true;
+  uint32_t issued = 0;  // thread 0: MMAs issued
   for (uint32_t j = 0; j < nslot; ++j) {
     const uint32_t s = j % TC_STAGES, use = j / TC_STAGES;
-    if (use > 0 && ok && !tc::mbar_wait(&S.empty[s], (use - 1) & 1, TC_WAIT_POLLS)) ok = false;
+    // the stage is free once the MMAs that read it (slot j - STAGES) are done
+    if (use > 0 && !tc::mbar_wait(&S.empty[s], (use - 1) & 1, abort, TC_WAIT_NS)) break;
     // A rows: this thread's target's source for slot j (bf16 hi, lo), or zeros
     const uint32_t src = my != TC_NONE ? __ldcg(&a.m2l[(size_t)my * TC_SLOT_MAX + j]) : TC_NONE;
     uint4 hv[4], lv[4];
@@ -569,37 +598,41 @@ __global__ void __launch_bounds__(TC_TILE) k_tc_m2l(TcArgs a) {
     }
     tc::fence_proxy_async();
     tc::mbar_arrive(&S.full[s]);
-    if (t == 0 && ok) {
-      if (!tc::mbar_wait(&S.full[s], use & 1, TC_WAIT_POLLS)) {
-        ok = false;
-      } else {
-        tc::fence_after_sync();
-        const uint32_t a_hi = tc::smem_addr(S.a[s][0]), a_lo = tc::smem_addr(S.a[s][1]);
-        const uint32_t b_hi = tc::smem_addr(S.b[s][0]), b_lo = tc::smem_addr(S.b[s][1]);
-        const uint32_t alb = (TC_TILE / 8) * 128, blb = (TC_KN / 8) * 128;
+    if (t == 0) {
+      if (!tc::mbar_wait(&S.full[s], use & 1, abort, TC_WAIT_NS)) break;
+      tc::fence_after_sync();
+      const uint32_t a_hi = tc::smem_addr(S.a[s][0]), a_lo = tc::smem_addr(S.a[s][1]);
+      const uint32_t b_hi = tc::smem_addr(S.b[s][0]), b_lo = tc::smem_addr(S.b[s][1]);
+      const uint32_t alb = (TC_TILE / 8) * 128, blb = (TC_KN / 8) * 128;
 #pragma unroll
-        for (uint32_t ks = 0; ks < 2; ++ks) {  // K = 32 as two MMAs of K = 16
-          const uint32_t ao = ks * 2 * alb, bo = ks * 2 * blb;
-          const uint64_t dah = tc::smem_desc(a_hi + ao, alb, 128);
-          const uint64_t dal = tc::smem_desc(a_lo + ao, alb, 128);
-          const uint64_t dbh = tc::smem_desc(b_hi + bo, blb, 128);
-          const uint64_t dbl = tc::smem_desc(b_lo + bo, blb, 128);
-          tc::mma_bf16(tmem, dah, dbh, idesc, (j | ks) ? 1u : 0u);
-          tc::mma_bf16(tmem, dah, dbl, idesc, 1u);
-          tc::mma_bf16(tmem, dal, dbh, idesc, 1u);
-        }
-        tc::commit(&S.empty[s]);
+      for (uint32_t ks = 0; ks < 2; ++ks) {  // K = 32 as two MMAs of K = 16
+        const uint32_t ao = ks * 2 * alb, bo = ks * 2 * blb;
+        const uint64_t dah = tc::smem_desc(a_hi + ao, alb, 128);
+        const uint64_t dal = tc::smem_desc(a_lo + ao, alb, 128);
+        const uint64_t dbh = tc::smem_desc(b_hi + bo, blb, 128);
+        const uint64_t dbl = tc::smem_desc(b_lo + bo, blb, 128);
+        tc::mma_bf16(tmem, dah, dbh, idesc, (j | ks) ? 1u : 0u);
+        tc::mma_bf16(tmem, dah, dbl, idesc, 1u);
+        tc::mma_bf16(tmem, dal, dbh, idesc, 1u);
       }
+      issued += 6;
+      tc::commit(&S.empty[s]);
     }
   }
-  if (t == 0) {
-    if (ok && nslot) tc::commit(&S.done);
-    if (!ok) S.err = 1;
-  }
+  // every MMA issued so far completes before the accumulator is read and the
+  // TMEM freed (also after a wait that gave up)
+  if (t == 0 && issued) tc::commit(&S.done);
   __syncthreads();
-  const bool good = S.err == 0 && nslot > 0;
-  if (good && !tc::mbar_wait(&S.done, 0, TC_WAIT_POLLS)) S.err = 1;
+  const bool any = __syncthreads_or(t == 0 && issued > 0);
+  bool done_ok = true;
+  if (any) {
+    // a fresh budget: this wait only needs the MMAs already issued
+    uint32_t no_abort = 0;
+    done_ok = tc::mbar_wait(&S.done, 0, &no_abort, TC_WAIT_NS);
+  }
   tc::fence_after_sync();
+  const bool all_done = __syncthreads_and(done_ok);
+  const bool good = any && S.err == 0 && all_done;
   if (good) {
     float v[32];
     tc::tmem_ld32(tmem + ((warp * 32u) << 16), v);
@@ -613,8 +646,10 @@ __global__ void __launch_bounds__(TC_TILE) k_tc_m2l(TcArgs a) {
   }
   tc::fence_before_sync();
   __syncthreads();
-  if (warp == 0) tc::tmem_dealloc(tmem, 32);
-  if (t == 0 && S.err) {
+  // (after a done-wait that ran out an MMA may still read the accumulator:
+  // the columns are then left allocated rather than freed under it)
+  if (warp == 0 && all_done) tc::tmem_dealloc(tmem, 32);
+  if (t == 0 && (S.err || !all_done) && nslot) {
     atomicOr(&a.info[TI_ERR], 1u);
     if (a.status) atomicOr(a.status, ST_WAIT_TIMEOUT);
   }
@@ -666,7 +701,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_tc_p2l(TcArgs a) {
   }
 }
 
-// ---- downward: L2L, L2P, M2P ----------------------------------------------------------------------
+// ---- downward: L2L (levels), then L2P and M2P per leaf -----------------------------------------
 
 __global__ void __launch_bounds__(TC_THREADS) k_tc_down(TcArgs a) {
   extern __shared__ float tc_down_smem[];
@@ -676,72 +711,150 @@ __global__ void __launch_bounds__(TC_THREADS) k_tc_down(TcArgs a) {
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t q = a.q;
   float *Lw = tc_down_smem + (threadIdx.x >> 5) * TC_KN;
-  for (uint32_t lev = 0; lev < a.nlev; ++lev) {
+  for (uint32_t lev = 0; lev + 1 < a.nlev; ++lev) {
     for (uint32_t c = a.lvl[lev] + gw; c < a.lvl[lev + 1]; c += nwarps) {
       const TcCell C = a.cells[c];
+      if (!C.nchild) continue;
       Lw[lane] = lane < 2 * q ? __ldcg(&a.lco[(size_t)c * TC_KN + lane]) : 0.f;
       __syncwarp();
-      if (C.nchild) {
-        // L2L into each child: L'^b_m += sum_{l>=m} op_b[m][l] L'_l
-        for (uint32_t b = 0; b < 4; ++b) {
-          const uint32_t ch = child_at(C, b);
-          if (ch == TC_NONE) continue;
-          if (lane < q) {
-            float sr = 0, si = 0;
-            for (uint32_t l = lane; l < q; ++l) {
-              const float orr = a.tab->l2l_re[b][lane][l], oi = a.tab->l2l_im[b][lane][l];
-              sr += orr * Lw[l] - oi * Lw[q + l];
-              si += orr * Lw[q + l] + oi * Lw[l];
-            }
-            float *Lc = a.lco + (size_t)ch * TC_KN;
-            Lc[lane] = __ldcg(&Lc[lane]) + sr;
-            Lc[q + lane] = __ldcg(&Lc[q + lane]) + si;
+      // L2L into each child: L'^b_m += sum_{l>=m} op_b[m][l] L'_l
+      for (uint32_t b = 0; b < 4; ++b) {
+        const uint32_t ch = child_at(C, b);
+        if (ch == TC_NONE) continue;
+        if (lane < q) {
+          float sr = 0, si = 0;
+          for (uint32_t l = lane; l < q; ++l) {
+            const float orr = a.tab->l2l_re[b][lane][l], oi = a.tab->l2l_im[b][lane][l];
+            sr += orr * Lw[l] - oi * Lw[q + l];
+            si += orr * Lw[q + l] + oi * Lw[l];
           }
-        }
-      } else {
-        // L2P (and M2P from the cells of the leaf's W list) at each point
-        double cx, cy;
-        cell_centre(C, cx, cy);
-        const double inv_s = ldexp(1.0, (int)C.level);
-        const uint32_t nw = a.loff[(size_t)c * 8 + 3], ow = a.loff[(size_t)c * 8 + 2];
-        for (uint32_t k = C.first + lane; k < C.first + C.count; k += 32) {
-          const float wr = (float)((a.ux[k] - cx) * inv_s), wi = (float)((a.uy[k] - cy) * inv_s);
-          float ar = Lw[q - 1], ai = Lw[2 * q - 1];
-          for (int l = (int)q - 2; l >= 0; --l) {
-            const float nr = ar * wr - ai * wi + Lw[l];
-            ai = ar * wi + ai * wr + Lw[q + l];
-            ar = nr;
-          }
-          double gr = (double)ar * inv_s, gi = (double)ai * inv_s;  // phi = (1/s) sum L'_l w^l
-          for (uint32_t e = 0; e < nw; ++e) {
-            const uint32_t cc = a.pool[ow + e];
-            const TcCell W = a.cells[cc];
-            double wx, wy;
-            cell_centre(W, wx, wy);
-            const double winv = ldexp(1.0, (int)W.level);
-            // g = (1/s_W) sum_k M'_k / z^(k+1), z = (u - c_W) / s_W
-            const double zr = (a.ux[k] - wx) * winv, zi = (a.uy[k] - wy) * winv;
-            const double d2 = zr * zr + zi * zi;
-            const double ir = zr / d2, ii = -zi / d2;
-            const double *mc = a.mco + (size_t)cc * 2 * q;
-            double pr = ir, pi = ii, sr = 0, si = 0;
-            for (uint32_t kk = 0; kk < q; ++kk) {
-              const double mr = mc[kk], mi = mc[q + kk];
-              sr += mr * pr - mi * pi;
-              si += mr * pi + mi * pr;
-              const double nr = pr * ir - pi * ii;
-              pi = pr * ii + pi * ir;
-              pr = nr;
-            }
-            gr += sr * winv;
-            gi += si * winv;
-          }
-          a.far[k] = make_float2((float)(-gr * a.inv_w), (float)(gi * a.inv_w));
+          float *Lc = a.lco + (size_t)ch * TC_KN;
+          Lc[lane] = __ldcg(&Lc[lane]) + sr;
+          Lc[q + lane] = __ldcg(&Lc[q + lane]) + si;
         }
       }
       __syncwarp();
     }
     g.sync();
+  }
+}
+
+// Leaf features of the learned correction, from the leaf's final local
+// expansion and its points: L'_1 .. L'_4 over sc = |(L'_0 .. L'_4)| (8
+// reals), level / 16, count / 32, and the points' mean offset from the centre
+// in cell sides (2). Row of 16 floats per cell: features, L'_0 (2), sc, and
+// the cell index (as float bits) for leaves, -1 in column 15 otherwise.
+__global__ void __launch_bounds__(TC_THREADS) k_tc_features(TcArgs a) {
+  const unsigned lane = threadIdx.x & 31;
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t q = a.q;
+  for (uint32_t c = gw; c < a.ncells; c += nwarps) {
+    const TcCell C = a.cells[c];
+    float *row = a.feat + (size_t)c * 16;
+    if (C.nchild) {
+      if (lane == 0) row[15] = -1.f;
+      continue;
+    }
+    double cx, cy;
+    cell_centre(C, cx, cy);
+    const double inv_s = ldexp(1.0, (int)C.level);
+    float mx = 0, my = 0;
+    for (uint32_t k = C.first + lane; k < C.first + C.count; k += 32) {
+      mx += (float)((a.ux[k] - cx) * inv_s);
+      my += (float)((a.uy[k] - cy) * inv_s);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      mx += __shfl_xor_sync(0xffffffffu, mx, o);
+      my += __shfl_xor_sync(0xffffffffu, my, o);
+    }
+    if (lane == 0) {
+      const float *L = a.lco + (size_t)c * TC_KN;
+      const uint32_t lmax = q - 1 < 4 ? q - 1 : 4;
+      float s2 = 0;
+      for (uint32_t l = 0; l <= lmax; ++l) s2 += L[l] * L[l] + L[q + l] * L[q + l];
+      const float sc = sqrtf(s2) + 1e-30f;
+      for (uint32_t l = 1; l <= 4; ++l) {
+        row[2 * (l - 1)] = l <= lmax ? L[l] / sc : 0.f;
+        row[2 * (l - 1) + 1] = l <= lmax ? L[q + l] / sc : 0.f;
+      }
+      row[8] = C.level / 16.f;
+      row[9] = C.count / 32.f;
+      row[10] = mx / C.count;
+      row[11] = my / C.count;
+      row[12] = L[0];
+      row[13] = L[q];
+      row[14] = sc;
+      row[15] = __uint_as_float(c);
+    }
+  }
+}
+
+// The learned form's inputs, packed for the network: x[k] = features of leaf
+// leaves[k].
+__global__ void k_tc_pack(TcArgs a) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= __ldcg(&a.info[TI_LEAVES])) return;
+  const float *row = a.feat + (size_t)a.leaves[k] * 16;
+  for (int j = 0; j < 12; ++j) a.mlp_x[(size_t)k * 12 + j] = row[j];
+}
+
+__global__ void __launch_bounds__(TC_THREADS) k_tc_leaf(TcArgs a, int corrected) {
+  const unsigned lane = threadIdx.x & 31;
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t q = a.q;
+  const uint32_t nleaf = __ldcg(&a.info[TI_LEAVES]);
+  for (uint32_t e0 = gw; e0 < nleaf; e0 += nwarps) {
+    const uint32_t c = a.leaves[e0];
+    const TcCell C = a.cells[c];
+    const float *L = a.lco + (size_t)c * TC_KN;
+    float l0r = L[0], l0i = L[q];
+    if (corrected) {
+      // L'_0 += sc * network output / TARGET_SCALE
+      const float sc = a.feat[(size_t)c * 16 + 14];
+      l0r += sc * a.mlp_y[(size_t)e0 * 2] * (1.f / LEARN_TARGET_SCALE);
+      l0i += sc * a.mlp_y[(size_t)e0 * 2 + 1] * (1.f / LEARN_TARGET_SCALE);
+    }
+    double cx, cy;
+    cell_centre(C, cx, cy);
+    const double inv_s = ldexp(1.0, (int)C.level);
+    const uint32_t nw = a.loff[(size_t)c * 8 + 3], ow = a.loff[(size_t)c * 8 + 2];
+    for (uint32_t k = C.first + lane; k < C.first + C.count; k += 32) {
+      const float wr = (float)((a.ux[k] - cx) * inv_s), wi = (float)((a.uy[k] - cy) * inv_s);
+      float ar = q > 1 ? L[q - 1] : l0r, ai = q > 1 ? L[2 * q - 1] : l0i;
+      for (int l = (int)q - 2; l >= 0; --l) {
+        const float lr = l ? L[l] : l0r, li = l ? L[q + l] : l0i;
+        const float nr = ar * wr - ai * wi + lr;
+        ai = ar * wi + ai * wr + li;
+        ar = nr;
+      }
+      double gr = (double)ar * inv_s, gi = (double)ai * inv_s;  // phi = (1/s) sum L'_l w^l
+      for (uint32_t e = 0; e < nw; ++e) {
+        const uint32_t cc = a.pool[ow + e];
+        const TcCell W = a.cells[cc];
+        double wx, wy;
+        cell_centre(W, wx, wy);
+        const double winv = ldexp(1.0, (int)W.level);
+        // g = (1/s_W) sum_k M'_k / z^(k+1), z = (u - c_W) / s_W
+        const double zr = (a.ux[k] - wx) * winv, zi = (a.uy[k] - wy) * winv;
+        const double d2 = zr * zr + zi * zi;
+        const double ir = zr / d2, ii = -zi / d2;
+        const double *mc = a.mco + (size_t)cc * 2 * q;
+        double pr = ir, pi = ii, sr = 0, si = 0;
+        for (uint32_t kk = 0; kk < q; ++kk) {
+          const double mr = mc[kk], mi = mc[q + kk];
+          sr += mr * pr - mi * pi;
+          si += mr * pi + mi * pr;
+          const double nr = pr * ir - pi * ii;
+          pi = pr * ii + pi * ir;
+          pr = nr;
+        }
+        gr += sr * winv;
+        gi += si * winv;
+      }
+      a.far[k] = make_float2((float)(-gr * a.inv_w), (float)(gi * a.inv_w));
+    }
   }
 }
 
@@ -808,11 +921,69 @@ __global__ void __launch_bounds__(TC_THREADS) k_tc_p2p(TcArgs a) {
       }
       if (act) {
         const float2 f = a.far[ti];
-        a.vx[gi] = a.vx[gi] + ((double)(vx0 + vx1) + (double)f.x);
-        a.vy[gi] = a.vy[gi] + ((double)(vy0 + vy1) + (double)f.y);
+        const double kx = (double)(vx0 + vx1) + (double)f.x, ky = (double)(vy0 + vy1) + (double)f.y;
+        if (a.kick) {
+          a.kick[ti] = make_double2(kx, ky);
+        } else {
+          a.vx[gi] = a.vx[gi] + kx;
+          a.vy[gi] = a.vy[gi] + ky;
+        }
       }
     }
   }
+}
+
+// ---- the learned form's sampled check -----------------------------------------------------------
+
+// A block per sampled point k (sorted order, spread evenly): the FP64 direct
+// sum of d3's pair formula over every point (coincident pairs and the point
+// itself add nothing; distanceMin's clamp), against the kick the pass put in
+// kick[k]. Adds |kick - ref|^2 and |ref|^2 to chk[0], chk[1].
+__global__ void __launch_bounds__(CHECK_THREADS) k_tc_check(TcArgs a, uint32_t samples,
+                                                            double dmin2, double *chk) {
+  __shared__ double sx[CHECK_THREADS / 32], sy[CHECK_THREADS / 32];
+  const uint32_t j = blockIdx.x;
+  const uint32_t k = (uint32_t)(((2ull * j + 1) * a.m) / (2ull * samples));
+  const double xi = a.px[k], yi = a.py[k];
+  double vx = 0, vy = 0;
+  for (uint32_t i = threadIdx.x; i < a.m; i += blockDim.x) {
+    const double dx = a.px[i] - xi, dy = a.py[i] - yi;
+    double l = dx * dx + dy * dy;
+    if (!(l > 0)) continue;
+    if (l < dmin2) l = sqrt(dmin2 * l);
+    const double w = a.ps[i] / l;
+    vx += dx * w;
+    vy += dy * w;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    vx += __shfl_xor_sync(0xffffffffu, vx, o);
+    vy += __shfl_xor_sync(0xffffffffu, vy, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    sx[threadIdx.x >> 5] = vx;
+    sy[threadIdx.x >> 5] = vy;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double rx = 0, ry = 0;
+    for (uint32_t w = 0; w < CHECK_THREADS / 32; ++w) {
+      rx += sx[w];
+      ry += sy[w];
+    }
+    const double2 kk = a.kick[k];
+    const double ex = kk.x - rx, ey = kk.y - ry;
+    atomicAdd(&chk[0], ex * ex + ey * ey);
+    atomicAdd(&chk[1], rx * rx + ry * ry);
+  }
+}
+
+__global__ void k_tc_apply(TcArgs a) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= a.m) return;
+  const uint32_t i = a.perm[k];
+  const double2 kk = a.kick[k];
+  a.vx[i] = a.vx[i] + kk.x;
+  a.vy[i] = a.vy[i] + kk.y;
 }
 
 // ---- tables (host) --------------------------------------------------------------------------------
@@ -845,8 +1016,8 @@ float from_bf16(uint16_t h) {
 
 // Builds the vector sets, the slot maps, the quadrant operators and the M2L
 // operators for order p and opening kappa.
-int build_tables(TcDev &d, uint32_t p, double kappa, cudaStream_t st) {
-  TcTables &T = d.h_tab;
+int build_tables(TcTabSet &d, uint32_t p, double kappa, cudaStream_t st) {
+  TcTables &T = d.h;
   memset(&T, 0, sizeof T);
   const uint32_t q = p + 1;
   T.q = q;
@@ -916,7 +1087,9 @@ int build_tables(TcDev &d, uint32_t p, double kappa, cudaStream_t st) {
   // n holds W[.][n]), bf16 hi then lo
   std::vector<uint16_t> w(classes.size() * 2 * TC_KN * TC_KN, 0);
   for (size_t cls = 0; cls < classes.size(); ++cls) {
-    const Cplx v{(double)classes[cls].first, (double)classes[cls].second};
+    // classes hold the source's offset from the target, B - A; the
+    // translation is z0 = c_A - c_B = -(B - A)
+    const Cplx v{-(double)classes[cls].first, -(double)classes[cls].second};
     const double d2 = v.re * v.re + v.im * v.im;
     const Cplx inv{v.re / d2, -v.im / d2};
     std::vector<Cplx> ipw(2 * q + 1);
@@ -944,6 +1117,7 @@ int build_tables(TcDev &d, uint32_t p, double kappa, cudaStream_t st) {
       }
   }
   if (!d.tab) D3_CUDA_OK(cudaMalloc(&d.tab, sizeof(TcTables)));
+  d.p = 0;
   cudaFree(d.wops);
   D3_CUDA_OK(cudaMalloc(&d.wops, w.size() * 2));
   if (cudaMemcpyAsync(d.tab, &T, sizeof T, cudaMemcpyHostToDevice, st) != cudaSuccess ||
@@ -973,10 +1147,30 @@ int reserve(TcDev &d, uint32_t ncells, uint32_t m) {
   if (m > d.pcap) {
     const uint32_t cap = m + m / 4 + 1024;
     cudaFree(d.far);
+    cudaFree(d.kick);
     D3_CUDA_OK(cudaMalloc(&d.far, (size_t)cap * sizeof(float2)));
+    D3_CUDA_OK(cudaMalloc(&d.kick, (size_t)cap * sizeof(double2)));
     d.pcap = cap;
   }
+  if (d.ccap > d.lcap) {
+    cudaFree(d.feat); cudaFree(d.leaves); cudaFree(d.mlp_x); cudaFree(d.mlp_y);
+    D3_CUDA_OK(cudaMalloc(&d.feat, (size_t)d.ccap * 16 * 4));
+    D3_CUDA_OK(cudaMalloc(&d.leaves, (size_t)d.ccap * 4));
+    D3_CUDA_OK(cudaMalloc(&d.mlp_x, (size_t)d.ccap * 12 * 4));
+    D3_CUDA_OK(cudaMalloc(&d.mlp_y, (size_t)d.ccap * 2 * 4));
+    d.lcap = d.ccap;
+  }
   return 0;
+}
+
+// The table set for (p, kappa): an existing one, else built in the older slot.
+TcTabSet *tables_for(TcDev &d, uint32_t p, double kappa, cudaStream_t st) {
+  for (TcTabSet &t : d.sets)
+    if (t.tab && t.p == p && t.kappa == kappa) return &t;
+  TcTabSet &t = d.sets[d.next_set];
+  d.next_set ^= 1;
+  if (build_tables(t, p, kappa, st)) return nullptr;
+  return &t;
 }
 
 int coop(const void *fn, int blocks, size_t smem, TcArgs &args, cudaStream_t st) {
@@ -988,57 +1182,141 @@ int coop(const void *fn, int blocks, size_t smem, TcArgs &args, cudaStream_t st)
 
 }  // namespace
 
+namespace {
+
+TcDev *tc_dev(FastScratch &s) {
+  if (s.fmm_tc) return static_cast<TcDev *>(s.fmm_tc);
+  TcDev *d = new TcDev();
+  if (cudaMalloc(&d->info, TI_WORDS * 4) != cudaSuccess ||
+      cudaHostAlloc(&d->h_info, TI_WORDS * 4, cudaHostAllocDefault) != cudaSuccess ||
+      cudaMalloc(&d->chk, 2 * sizeof(double)) != cudaSuccess ||
+      cudaHostAlloc(&d->h_chk, 2 * sizeof(double), cudaHostAllocDefault) != cudaSuccess) {
+    cudaFree(d->info);
+    cudaFreeHost(d->h_info);
+    cudaFree(d->chk);
+    delete d;
+    return nullptr;
+  }
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const size_t up_smem = TC_WARPS * 32 * 2 * TC_MAXQ * 8;
+  cudaFuncSetAttribute(k_tc_upward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)up_smem);
+  cudaFuncSetAttribute(k_tc_m2l, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(M2lSmem));
+  int pl = 0, pu = 0, pd = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pl, k_tc_lists, TC_THREADS, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pu, k_tc_upward, TC_THREADS, up_smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pd, k_tc_down, TC_THREADS, TC_WARPS * TC_KN * 4);
+  d->coop_lists = sms * (pl > 2 ? 2 : pl < 1 ? 1 : pl);
+  d->coop_up = sms * (pu > 2 ? 2 : pu < 1 ? 1 : pu);
+  d->coop_down = sms * (pd > 2 ? 2 : pd < 1 ? 1 : pd);
+  s.fmm_tc = d;
+  return d;
+}
+
+// The passes of one expansion order over a built tree and lists: upward,
+// M2L, P2L, L2L, leaf features, (the network, when `learned`), L2P / M2P and
+// the near field.
+int tc_order_pass(TcDev &d, TcArgs &g, const TcTabSet &ts, uint32_t tiles, bool learned,
+                  cudaStream_t st) {
+  g.tab = ts.tab;
+  g.wops = ts.wops;
+  g.q = ts.p + 1;
+  const size_t up_smem = TC_WARPS * 32 * 2 * (size_t)g.q * 8;
+  if (coop((const void *)k_tc_upward, d.coop_up, up_smem, g, st)) return -1;
+  if (tiles) D3_LAUNCH(k_tc_m2l, tiles, TC_TILE, sizeof(M2lSmem), st)(g);
+  const unsigned wblocks = blocks_for((size_t)g.ncells * 32, TC_THREADS);
+  D3_LAUNCH(k_tc_p2l, wblocks, TC_THREADS, 0, st)(g);
+  if (coop((const void *)k_tc_down, d.coop_down, TC_WARPS * TC_KN * 4, g, st)) return -1;
+  D3_LAUNCH(k_tc_features, wblocks, TC_THREADS, 0, st)(g);
+  const uint32_t nleaf = d.h_info[TI_LEAVES];
+  if (learned) {
+    D3_LAUNCH(k_tc_pack, blocks_for(nleaf, 256), 256, 0, st)(g);
+    if (mlp_infer_tc(d.mlp_x, nleaf, d.mlp, d.mlp_y, g.status, st)) return -1;
+  }
+  D3_LAUNCH(k_tc_leaf, blocks_for((size_t)nleaf * 32, TC_THREADS), TC_THREADS, 0, st)(
+      g, learned ? 1 : 0);
+  D3_LAUNCH(k_tc_p2p, wblocks, TC_THREADS, 0, st)(g);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+}  // namespace
+
 void fmm_tc_free(FastScratch &s) {
   TcDev *d = static_cast<TcDev *>(s.fmm_tc);
   if (!d) return;
-  cudaFree(d->tab); cudaFree(d->wops); cudaFree(d->cells); cudaFree(d->mco); cudaFree(d->mbf);
+  for (TcTabSet &t : d->sets) {
+    cudaFree(t.tab);
+    cudaFree(t.wops);
+  }
+  cudaFree(d->cells); cudaFree(d->mco); cudaFree(d->mbf);
   cudaFree(d->lco); cudaFree(d->near); cudaFree(d->m2l); cudaFree(d->groups); cudaFree(d->loff);
   cudaFree(d->pool); cudaFree(d->far); cudaFree(d->info); cudaFreeHost(d->h_info);
+  cudaFree(d->feat); cudaFree(d->leaves); cudaFree(d->mlp_x); cudaFree(d->mlp_y);
+  cudaFree(d->kick); cudaFree(d->chk); cudaFreeHost(d->h_chk); cudaFree(d->mlp);
   delete d;
   s.fmm_tc = nullptr;
+}
+
+int fmm_tc_set_learned(FastScratch &s, const float *params, uint32_t len) {
+  if (len != (uint32_t)MLP_PARAMS || !params) return -3;
+  TcDev *d = tc_dev(s);
+  if (!d) return -1;
+  if (!d->mlp) D3_CUDA_OK(cudaMalloc(&d->mlp, MLP_PARAMS * 4));
+  return cudaMemcpy(d->mlp, params, MLP_PARAMS * 4, cudaMemcpyHostToDevice) == cudaSuccess ? 0 : -1;
+}
+
+int fmm_tc_leaves(FastScratch &s, float *out, uint32_t cap) {
+  TcDev *d = static_cast<TcDev *>(s.fmm_tc);
+  if (!d || !d->feat) return 0;
+  const uint32_t n = d->ncells_last;
+  if (out && cap >= n && n)
+    if (cudaMemcpy(out, d->feat, (size_t)n * 16 * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+  return (int)n;
+}
+
+void fmm_tc_stats(FastScratch &s, double *out) {
+  TcDev *d = static_cast<TcDev *>(s.fmm_tc);
+  for (int k = 0; k < 4; ++k) out[k] = 0;
+  if (!d) return;
+  out[0] = s.learn_checks;
+  out[1] = s.learn_fallbacks;
+  out[2] = s.learn_last_rms;
+  out[3] = d->ncells_last;
 }
 
 int fmm_tc_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *strengths,
                const FmmParams &prm, int form, const double *seed, uint32_t *status,
                cudaStream_t st) {
-  (void)form;
   if (prm.dmax2 < INFINITY) return fmm_run(s, t, a, strengths, prm, seed, status, st);
   FmmPrep pr;
   const int pre = fmm_prepare(s, t, a, strengths, prm.alpha, pr, st);
   if (pre == 2) return 1;
   if (pre <= 0) return pre;
-  if (!s.fmm_tc) {
-    TcDev *d = new TcDev();
-    s.fmm_tc = d;
-    D3_CUDA_OK(cudaMalloc(&d->info, TI_WORDS * 4));
-    D3_CUDA_OK(cudaHostAlloc(&d->h_info, TI_WORDS * 4, cudaHostAllocDefault));
-    int dev = 0, sms = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const size_t up_smem = TC_WARPS * 32 * 2 * TC_MAXQ * 8;
-    cudaFuncSetAttribute(k_tc_upward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)up_smem);
-    cudaFuncSetAttribute(k_tc_m2l, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)sizeof(M2lSmem));
-    int pl = 0, pu = 0, pd = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pl, k_tc_lists, TC_THREADS, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pu, k_tc_upward, TC_THREADS, up_smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pd, k_tc_down, TC_THREADS, TC_WARPS * TC_KN * 4);
-    d->coop_lists = sms * (pl > 2 ? 2 : pl < 1 ? 1 : pl);
-    d->coop_up = sms * (pu > 2 ? 2 : pu < 1 ? 1 : pu);
-    d->coop_down = sms * (pd > 2 ? 2 : pd < 1 ? 1 : pd);
-  }
-  TcDev &d = *static_cast<TcDev *>(s.fmm_tc);
+  TcDev *dp = tc_dev(s);
+  if (!dp) return -1;
+  TcDev &d = *dp;
   uint32_t p = 8;
   if (prm.order >= 1 && prm.order <= (double)(TC_MAXQ - 1)) p = (uint32_t)prm.order;
   double kappa = prm.opening;
   if (!(kappa >= 1 && kappa <= 2)) kappa = 1.5;
-  if (d.p != p || d.kappa != kappa)
-    if (build_tables(d, p, kappa, st)) return -1;
+  // the learned form: order 4 plus the network, checked on sampled points;
+  // the plain form at the requested order (8 unless it asks for more) when
+  // the check fails or no network is installed
+  bool learned = form == 3 && d.mlp;
+  if (learned && d.hold) {
+    --d.hold;
+    learned = false;
+  }
+  if (form == 3 && p < 5) p = 8;
+  TcTabSet *main = tables_for(d, learned ? LEARN_ORDER : p, kappa, st);
+  if (!main) return -1;
   if (reserve(d, pr.ncells, pr.m)) return -1;
   TcArgs g;
   memset(&g, 0, sizeof g);
-  g.tab = d.tab;
-  g.wops = d.wops;
+  g.tab = main->tab;
+  g.wops = main->wops;
   g.keys = pr.keys;
   g.perm = pr.perm;
   g.px = pr.px; g.py = pr.py; g.ps = pr.ps; g.ux = pr.ux; g.uy = pr.uy;
@@ -1047,20 +1325,21 @@ int fmm_tc_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *st
   g.mco = d.mco; g.mbf = d.mbf; g.lco = d.lco;
   g.near = d.near; g.m2l = d.m2l; g.groups = d.groups; g.loff = d.loff;
   g.far = d.far;
+  g.feat = d.feat; g.leaves = d.leaves; g.mlp_x = d.mlp_x; g.mlp_y = d.mlp_y;
+  g.kick = learned ? d.kick : nullptr;
   g.vx = a.vx; g.vy = a.vy;
   g.info = d.info;
   g.status = status;
   g.lvl = pr.info + 8;  // FI_LVL
-  g.ncells = pr.ncells; g.nlev = pr.nlev; g.m = pr.m; g.q = p + 1; g.ccap = d.ccap;
+  g.ncells = pr.ncells; g.nlev = pr.nlev; g.m = pr.m; g.q = main->p + 1; g.ccap = d.ccap;
   g.inv_w = pr.inv_w;
   g.dmin2 = prm.dmin2 * pr.inv_w * pr.inv_w;
   g.dmin2f = (float)prm.dmin2;
   g.seed = seed;
+  d.ncells_last = pr.ncells;
   if (cudaMemsetAsync(d.info, 0, TI_WORDS * 4, st) != cudaSuccess) return -1;
   D3_LAUNCH(k_tc_geom, blocks_for(pr.ncells, 256), 256, 0, st)(g);
-  const size_t up_smem = TC_WARPS * 32 * 2 * (p + 1) * 8;
-  if (coop((const void *)k_tc_upward, d.coop_up, up_smem, g, st)) return -1;
-  // lists; grow the pool and redo on overflow
+  // lists (geometry and opening only); grow the pool and redo on overflow
   size_t need = d.last_pool ? d.last_pool + d.last_pool / 4 + 4096 : (size_t)pr.ncells * 24 + 4096;
   for (int attempt = 0;; ++attempt) {
     if (need > d.pool_cap) {
@@ -1086,13 +1365,31 @@ int fmm_tc_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *st
   }
   uint32_t tiles = 0;
   for (uint32_t q4 = 0; q4 < 4; ++q4) tiles += (d.h_info[TI_GROUP + q4] + TC_TILE - 1) / TC_TILE;
-  if (tiles)
-    D3_LAUNCH(k_tc_m2l, tiles, TC_TILE, sizeof(M2lSmem), st)(g);
-  const unsigned wblocks = blocks_for((size_t)pr.ncells * 32, TC_THREADS);
-  D3_LAUNCH(k_tc_p2l, wblocks, TC_THREADS, 0, st)(g);
-  if (coop((const void *)k_tc_down, d.coop_down, TC_WARPS * TC_KN * 4, g, st)) return -1;
-  D3_LAUNCH(k_tc_p2p, wblocks, TC_THREADS, 0, st)(g);
-  return cudaGetLastError() == cudaSuccess ? 1 : -1;
+  if (tc_order_pass(d, g, *main, tiles, learned, st)) return -1;
+  if (!learned) return 1;
+  // the sampled check against the FP64 direct sum
+  const uint32_t samples = s.learn_samples ? s.learn_samples : 64;
+  if (cudaMemsetAsync(d.chk, 0, 2 * sizeof(double), st) != cudaSuccess) return -1;
+  D3_LAUNCH(k_tc_check, samples, CHECK_THREADS, 0, st)(g, samples, prm.dmin2, d.chk);
+  if (cudaMemcpyAsync(d.h_chk, d.chk, 2 * sizeof(double), cudaMemcpyDeviceToHost, st) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return -1;
+  const double rms = d.h_chk[1] > 0 ? sqrt(d.h_chk[0] / d.h_chk[1]) : 0;
+  s.learn_checks += 1;
+  s.learn_last_rms = rms;
+  if (rms <= s.learn_tol) {
+    D3_LAUNCH(k_tc_apply, blocks_for(pr.m, 256), 256, 0, st)(g);
+    return cudaGetLastError() == cudaSuccess ? 1 : -1;
+  }
+  // the fallback: the plain form at order p, straight into the velocities
+  s.learn_fallbacks += 1;
+  d.hold = s.learn_hold;
+  TcTabSet *fb = tables_for(d, p, kappa, st);
+  if (!fb) return -1;
+  g.kick = nullptr;
+  if (tc_order_pass(d, g, *fb, tiles, false, st)) return -1;
+  return 1;
 }
 
 }  // namespace d3

@@ -9,9 +9,9 @@
 // chunks) = (R / 8) * 128, stride byte offset (between row groups) = 128.
 // tc_tile_offset() gives the byte offset of (row, chunk).
 //
-// Every wait on an mbarrier is bounded: after `limit` polls it gives up and
-// returns false; callers set an error flag and finish without further waits
-// on that barrier (no spin can outlive its budget).
+// Every wait on an mbarrier is bounded: after its time budget it gives up,
+// sets the CTA's abort flag and returns false; the other threads' waits see
+// the flag and give up at once (no spin can outlive its budget).
 #pragma once
 
 #include <cuda_bf16.h>
@@ -131,11 +131,20 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
                    smem_addr(bar))
                : "memory");
 }
-// Waits for the phase with parity `parity` to complete; false after `limit`
-// unsuccessful polls.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t limit) {
+__device__ __forceinline__ uint64_t now_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Waits for the phase with parity `parity` to complete. Gives up when
+// *abort is set (another thread of the CTA gave up) or after budget_ns of
+// global time, setting *abort; returns whether the phase completed.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile uint32_t *abort,
+                                          uint64_t budget_ns) {
   const uint32_t a = smem_addr(bar);
-  for (uint32_t i = 0; i < limit; ++i) {
+  uint64_t t0 = 0;
+  for (uint32_t i = 0;; ++i) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -145,8 +154,16 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32
         : "r"(a), "r"(parity)
         : "memory");
     if (done) return true;
+    if (*abort) return false;
+    if ((i & 63) == 0) {
+      const uint64_t t = now_ns();
+      if (i == 0) t0 = t;
+      else if (t - t0 > budget_ns) {
+        *abort = 1;
+        return false;
+      }
+    }
   }
-  return false;
 }
 
 // Round to bf16 and the bf16 remainder (x ~ hi + lo to about 2^-17 relative).

@@ -854,6 +854,18 @@ class Simulation:
             self.ctx.precision = None
         return self
 
+    def learned(self, params, tolerance=1e-5, samples=64, hold=0):
+        """Installs the learned form's network (5,122 floats, learned.py) with
+        its sampled check: each tick the order-4 + network kick is compared
+        with an FP64 direct sum on `samples` nodes, and when the RMS exceeds
+        `tolerance` the tick runs the plain form instead (and the next `hold`
+        ticks too). No counterpart in the reference."""
+        import numpy as np
+        p = np.ascontiguousarray(params, np.float32)
+        C.check(self.ctx.core.sim_set_learned(self.ctx.h, p.ctypes.data, len(p), float(tolerance),
+                                              int(samples), int(hold)))
+        return self
+
     def threads(self, k="__get__"):
         """simulation.js:205-215: the reference's cap on CPU workers per tick.
         Ticks run on the GPU here: the setter is kept for compatibility and

@@ -198,6 +198,73 @@ int32_t sim_set_profile(uint32_t h, uint32_t on);
  * call returns D3_WORKER_FAILED; the simulation stays usable. */
 int32_t sim_selftest_wait(uint32_t h, uint32_t budget_us);
 
+/* ---- Fast many-body precision forms (no counterpart in the reference) ---
+ *
+ * force_set_scalar(h, fh, D3_PRECISION, v) of a many-body force picks the
+ * fast-mode form: 1 the reference's FP64 FMM (bit for bit); 2 the
+ * tensor-core FMM (geometric cells, level-free operators, M2L as BF16x3
+ * tcgen05 contractions with FP32 accumulation, FP32 near field with an FP64
+ * origin shift; ORDER up to 15, OPENING in [1, 2]); 3 the learned form:
+ * order 4 plus a per-leaf network correcting L'_0, checked each tick against
+ * an FP64 direct sum on sampled nodes, form 2 at ORDER (8 if below 5) when
+ * the check fails. Link and collide run the fast kernels for 1, 2 and 3. A
+ * finite distanceMax runs form 1. */
+
+/* Installs the learned form's network: 5,122 floats (W1 [64][12], b1, W2
+ * [64][64], b2, W3 [2][64], b3), the RMS tolerance of the sampled check, its
+ * sample count (1 .. 4096) and the ticks to stay on the fallback after a
+ * failed check. sim_stat 50..53: checks, fallbacks, last sampled RMS, cells. */
+int32_t sim_set_learned(uint32_t h, const float *params, uint32_t len, double tolerance,
+                        uint32_t samples, uint32_t hold);
+
+/* The last form-2/3 run's per-cell rows, 16 floats each: the network's 12
+ * inputs, L'_0 (re, im) and its scale, then the cell index (float bits) for
+ * leaves or -1. Copies when cap >= the cell count; returns the cell count. */
+int32_t sim_fmm_leaves(uint32_t h, float *out, uint32_t cap);
+
+/* The network on the device (no counterpart in the reference): x n x 12,
+ * y n x 2 FP32 device pointers; params 5,122 floats (host).
+ * d3_mlp_grad: the gradient of mean_i |MLP(x_i) - y_i|^2 (host grad[5122],
+ * *loss). d3_mlp_train: `steps` Adam steps over consecutive batches of
+ * `batch` samples, learning rate lr, params updated in place, per-step batch
+ * losses into losses[steps] (may be NULL). d3_mlp_infer: y = MLP(x) on the
+ * tensor cores (tensor_cores 1) or CUDA cores (0). */
+int32_t d3_mlp_grad(const float *x, const float *y, uint32_t n, const float *params, float *grad,
+                    float *loss);
+int32_t d3_mlp_train(const float *x, const float *y, uint32_t n, uint32_t batch, uint32_t steps,
+                     float lr, float *params, float *losses);
+int32_t d3_mlp_infer(const float *x, uint32_t n, const float *params, float *y,
+                     uint32_t tensor_cores);
+
+/* ---- Batched fast mode (no counterpart in the reference) -----------------
+ *
+ * Many independent graphs, each a d3 simulation with forceManyBody (FMM order
+ * 8, opening 1.5, distanceMin 1, strength -30), forceLink (distance 30, d3's
+ * default strength and bias) and forceCollide (radius 3), in FP32, d3's alpha
+ * schedule and velocity decay 0.4; one persistent kernel launch per tick for
+ * all graphs (graphs taken largest first). Up to 16,384 nodes per graph.
+ *
+ * batch_create: node_counts[graphs], link_counts[graphs]; src / tgt the
+ * links of every graph concatenated, as node indices local to their graph;
+ * x / y the start positions of every node, concatenated. Returns a handle
+ * (0 on a bad argument or no memory). batch_run: `ticks` ticks, captured
+ * into one CUDA graph when `graph` is non-zero; *ms the device time.
+ * batch_kick: the many-body kick alone at the current positions (x, y per
+ * node, host float[2 x nodes]) and the alpha it used. batch_read: the node
+ * state (any pointer may be NULL). batch_set_shape: threads per CTA (256,
+ * 512, 1024), CTAs per SM (1, 2), points per FMM leaf (2 .. 256).
+ * batch_autotune: times `ticks` ticks of each shape from the current state
+ * (restored after each) and keeps the fastest; out[4]: threads, CTAs per SM,
+ * leaf size, ms per tick. */
+uint32_t batch_create(uint32_t graphs, const uint32_t *node_counts, const uint32_t *link_counts,
+                      const uint32_t *src, const uint32_t *tgt, const float *x, const float *y);
+int32_t batch_destroy(uint32_t h);
+int32_t batch_set_shape(uint32_t h, uint32_t threads, uint32_t per_sm, uint32_t leaf_size);
+int32_t batch_run(uint32_t h, uint32_t ticks, uint32_t graph, double *ms);
+int32_t batch_kick(uint32_t h, float *out, double *alpha_used);
+int32_t batch_read(uint32_t h, float *x, float *y, float *vx, float *vy);
+int32_t batch_autotune(uint32_t h, uint32_t ticks, double *out);
+
 /* ---- Device rates for the roofline (no counterpart in the reference) ----
  *
  * Times microbenchmarks on the current device with CUDA events and fills

@@ -80,6 +80,8 @@ _SIGNATURES = {
     "sim_sync_out": (_I32, [_U32]),
     "sim_tick": (_I32, [_U32, _U32, ctypes.POINTER(_F64), _F64, _F64, _F64,
                         ctypes.POINTER(_U32), _U32]),
+    "sim_tick_sync": (_I32, [_U32, _U32, ctypes.POINTER(_F64), _F64, _F64, _F64,
+                             ctypes.POINTER(_U32), _U32]),
     "sim_last_tick_ms": (_F64, [_U32]),
     "sim_find": (_I32, [_U32, _F64, _F64, _F64, ctypes.POINTER(_U32)]),
     "sim_stat": (_F64, [_U32, _U32]),

@@ -978,10 +978,14 @@ int32_t sim_sync_out(uint32_t h) {
   return sync_out_impl(s);
 }
 
-int32_t sim_tick(uint32_t h, uint32_t ticks, double *alpha, double alpha_target, double alpha_decay,
-                 double velocity_decay, const uint32_t *order, uint32_t n_order) {
-  DSim *s = get_sim_raw(h);
-  if (!s) return D3_BAD_HANDLE;
+}  // extern "C"
+
+namespace {
+
+// The ticks of sim_tick; with copy_out the node state's device-to-host
+// copies are queued behind them, before the one synchronisation.
+int32_t tick_impl(DSim *s, uint32_t ticks, double *alpha, double alpha_target, double alpha_decay,
+                  double velocity_decay, const uint32_t *order, uint32_t n_order, bool copy_out) {
   if (!alpha || (n_order && !order)) {
     settle(s);
     return D3_BAD_ARGUMENT;
@@ -1058,12 +1062,41 @@ int32_t sim_tick(uint32_t h, uint32_t ticks, double *alpha, double alpha_target,
       std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - host0).count();
   *alpha = a;
   if (hoist >= 0) cudaStreamWaitEvent(s->stream, s->ev_sumdone, 0);
+  if (copy_out && s->n) {
+    const size_t n = s->n;
+    cudaMemcpyAsync(s->h_x, s->d_x, n * 8, cudaMemcpyDeviceToHost, s->stream);
+    cudaMemcpyAsync(s->h_y, s->d_y, n * 8, cudaMemcpyDeviceToHost, s->stream);
+    cudaMemcpyAsync(s->h_vx, s->d_vx, n * 8, cudaMemcpyDeviceToHost, s->stream);
+    cudaMemcpyAsync(s->h_vy, s->d_vy, n * 8, cudaMemcpyDeviceToHost, s->stream);
+  }
   queue_status(s);
   if (cudaStreamSynchronize(s->stream) != cudaSuccess) return D3_WORKER_FAILED;
   float ms = 0;
   cudaEventElapsedTime(&ms, s->ev0, s->ev1);
   s->last_ms = ms;
   return take_failure(s);
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t sim_tick(uint32_t h, uint32_t ticks, double *alpha, double alpha_target, double alpha_decay,
+                 double velocity_decay, const uint32_t *order, uint32_t n_order) {
+  DSim *s = get_sim_raw(h);
+  if (!s) return D3_BAD_HANDLE;
+  return tick_impl(s, ticks, alpha, alpha_target, alpha_decay, velocity_decay, order, n_order,
+                   false);
+}
+
+int32_t sim_tick_sync(uint32_t h, uint32_t ticks, double *alpha, double alpha_target,
+                      double alpha_decay, double velocity_decay, const uint32_t *order,
+                      uint32_t n_order) {
+  DSim *s = get_sim_raw(h);
+  if (!s) return D3_BAD_HANDLE;
+  sync_in_impl(s, true);
+  return tick_impl(s, ticks, alpha, alpha_target, alpha_decay, velocity_decay, order, n_order,
+                   true);
 }
 
 int32_t sim_set_learned(uint32_t h, const float *params, uint32_t len, double tolerance,

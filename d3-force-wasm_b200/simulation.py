@@ -97,15 +97,14 @@ class Context:
                 if getattr(nodes, f) is v:
                     setattr(nodes, f, np.array(v, np.float64))
 
-    def copy_in(self, nodes):
-        """src/core.js:121-131, then one host-to-device sync. The node table's
-        x, y, vx, vy, fx, fy become views of the pinned mirrors the first time
-        (as the reference's facade views wasm memory), so later ticks copy
-        nothing on the host; the fixed bits (src/core.js:130) are derived from
-        fx / fy on the device."""
+    def bind(self, nodes):
+        """src/core.js:121-131 on the host: the node table's x, y, vx, vy,
+        fx, fy become views of the pinned mirrors the first time (as the
+        reference's facade views wasm memory), so later ticks copy nothing on
+        the host; the fixed bits (src/core.js:130) are derived from fx / fy on
+        the device."""
         n = len(nodes)
         self.resize(n)
-        core, h = self.core, self.h
         if n and not self._bound(nodes):
             self.detach()
             views = []
@@ -115,13 +114,22 @@ class Context:
                 setattr(nodes, f, v)
                 views.append(v)
             self._nodes, self._views = nodes, tuple(views)
-        C.check(core.sim_sync_in(h))
+
+    def copy_in(self, nodes):
+        """bind(), then one host-to-device sync."""
+        self.bind(nodes)
+        C.check(self.core.sim_sync_in(self.h))
 
     def copy_out(self, nodes):
         """src/core.js:133-141, after one device-to-host sync (a bound node
         table already holds the result)."""
-        n = self.n
         C.check(self.core.sim_sync_out(self.h))
+        self.read_back(nodes)
+
+    def read_back(self, nodes):
+        """The mirrors' x, y, vx, vy into a node table that is not bound to
+        them (a bound one already holds them)."""
+        n = self.n
         if n and not self._bound(nodes):
             nodes.x[:] = self.view(C.PTR_X, n)
             nodes.y[:] = self.view(C.PTR_Y, n)
@@ -671,11 +679,16 @@ class Simulation:
         if not (0 < iterations):
             return self
         if self._random is None and self.engine_ticks and not self._custom():
-            self.device_begin()
-            try:
-                self.device_ticks(int(iterations))
-            finally:
-                self.device_end()
+            # one engine call: node state up, the ticks, node state down
+            ctx = self.ctx
+            ctx.bind(self._nodes)
+            self._push_forces()
+            alpha = C._F64(self._alpha)
+            C.check(self.core.sim_tick_sync(ctx.h, int(iterations), alpha, self._alpha_target,
+                                            self._alpha_decay, self._velocity_decay, self._order,
+                                            self._n_order))
+            self._alpha = alpha.value
+            ctx.read_back(self._nodes)
             return self
         ctx = self.ctx
         ctx.copy_in(self._nodes)
@@ -746,6 +759,12 @@ class Simulation:
             raise ValueError("a custom force runs through tick(), not the engine's sim_tick")
         ctx = self.ctx
         ctx.copy_in(self._nodes)
+        self._push_forces()
+
+    def _push_forces(self):
+        """Every force's scalars (sent only when changed) and the force order
+        for sim_tick (rebuilt only when the forces changed)."""
+        ctx = self.ctx
         for f in self._forces.values():
             f._push()
             s = f.slot
@@ -753,9 +772,11 @@ class Simulation:
             if ctx.precision:
                 s.scalar(C.ORDER, ctx.precision["order"])
                 s.scalar(C.OPENING, ctx.precision["opening"])
-        forces = list(self._forces.values())
-        self._order = (C._U32 * max(1, len(forces)))(*[f.slot.fh for f in forces])
-        self._n_order = len(forces)
+        handles = tuple(f.slot.fh for f in self._forces.values())
+        if getattr(self, "_order_key", None) != handles:
+            self._order = (C._U32 * max(1, len(handles)))(*handles)
+            self._n_order = len(handles)
+            self._order_key = handles
 
     def device_ticks(self, ticks):
         """`ticks` ticks on the device (sim_tick); returns their device ms.

@@ -146,6 +146,14 @@ int32_t sim_tick(uint32_t h, uint32_t ticks, double *alpha, double alpha_target,
                  const uint32_t *order, uint32_t n_order);
 
 /* Milliseconds of device time of the last sim_tick call (CUDA events). */
+/* sim_sync_in, sim_tick and sim_sync_out in one call with one host
+ * synchronisation: the node state's uploads, the ticks and the downloads are
+ * queued back to back on the simulation's stream (the facade's tick() with
+ * the device LCG). Same arguments and result as sim_tick. */
+int32_t sim_tick_sync(uint32_t h, uint32_t ticks, double *alpha, double alpha_target,
+                      double alpha_decay, double velocity_decay, const uint32_t *order,
+                      uint32_t n_order);
+
 double sim_last_tick_ms(uint32_t h);
 
 /* simulation.js:157-178 (`find`) on the device copy of the positions (after

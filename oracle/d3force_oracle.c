@@ -2239,6 +2239,14 @@ int32_t sim_tick(uint32_t h, uint32_t ticks, double *alpha, double alpha_target,
   return D3_OK;
 }
 
+int32_t sim_tick_sync(uint32_t h, uint32_t ticks, double *alpha, double alpha_target,
+                      double alpha_decay, double velocity_decay, const uint32_t *order,
+                      uint32_t n_order) {
+  int32_t r = sim_sync_in(h);
+  if (r < 0) return r;
+  return sim_tick(h, ticks, alpha, alpha_target, alpha_decay, velocity_decay, order, n_order);
+}
+
 double sim_last_tick_ms(uint32_t h) {
   (void)h;
   return 0;

@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fast", action="store_true", help="skip the fast-mode 1M measurement")
+    ap.add_argument("--only", choices=["fast", "learned", "batched"],
+                    help="run only this fast-mode leg (no exact line; for profiling)")
     return ap.parse_args()
 
 
@@ -253,8 +255,11 @@ def fast_ticks(pkg, core, layout, form, flush_l2, steps=10, warmup=3):
         flush_l2()
         times.append(sim.device_ticks(1))
     sim.device_end()
+    # the tensor-core form's last pass: M2L / P2P event times and work counts
+    stats = {k: core.sim_stat(sim.ctx.h, 54 + i) for i, k in enumerate(
+        ("m2l_ms", "p2p_ms", "m2l_tiles", "m2l_pairs", "p2p_pairs", "m2p_pairs", "p2l_pairs", "q"))}
     sim.close()
-    return sum(times) / len(times)
+    return sum(times) / len(times), stats
 
 
 def fast_digest(pkg, core, layout, form, ticks=3):
@@ -279,6 +284,45 @@ def fast_rms(pkg, core, layout, form, targets=4096):
     return acc.rms(kick, ref, tg)
 
 
+def fast_roofline(st, rates):
+    """The tensor-core form's two dominant kernels against their pipes.
+    M2L: every 128-target tile runs, per vector slot (39 at opening 1.5), six
+    tcgen05 MMAs of 128 x 32 x 16 (BF16x3 over K = 32: hi*hi, hi*lo, lo*hi),
+    2 * 128 * 32 * 16 flops each; achieved = those flops / the M2L launch's
+    event time, against the measured dense BF16 peak. The useful share: each
+    real source-target pair needs 3 x (2q)^2 multiply-adds of the 32-wide
+    padded rows. P2P: about 10 FP32 flops per point pair (differences, the
+    squared distance, one division, two multiply-adds), against the measured
+    FP32 FMA rate x 2."""
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    bf16 = peaks.get("bf16_tflops", 1590.0)
+    out = {}
+    if st["m2l_ms"] > 0 and st["m2l_tiles"] > 0:
+        issued = st["m2l_tiles"] * 39 * 6 * 2.0 * 128 * 32 * 16
+        ach = issued / (st["m2l_ms"] * 1e-3) / 1e12
+        q2 = 2 * st["q"]
+        useful = st["m2l_pairs"] * 3 * q2 * q2 * 2.0
+        out["m2l"] = {"bound": "tensor", "achieved": round(ach, 2), "peak": bf16,
+                      "unit": "TFLOP/s", "frac": round(ach / bf16, 4),
+                      "useful_frac_of_issued": round(useful / issued, 4),
+                      "ms": round(st["m2l_ms"], 4), "tiles": int(st["m2l_tiles"]),
+                      "pairs": int(st["m2l_pairs"]),
+                      "peak_source": "measured" if peaks else "fallback"}
+    if rates and st["p2p_ms"] > 0:
+        flops = st["p2p_pairs"] * 10.0
+        ach = flops / (st["p2p_ms"] * 1e-3) / 1e12
+        pk = 2 * rates["ffma_per_s"] / 1e12
+        out["p2p"] = {"bound": "fp32", "achieved": round(ach, 2), "peak": round(pk, 1),
+                      "unit": "TFLOP/s", "frac": round(ach / pk, 4), "ms": round(st["p2p_ms"], 4),
+                      "pairs": int(st["p2p_pairs"]), "peak_source": "measured (d3_device_peaks)"}
+    return out
+
+
 def fast_1m(pkg, core, torch, flush_l2, cpu=True):
     """Fast mode at 1M nodes: the reference's FP64 FMM ("plain", bit for bit)
     and the tensor-core form ("bf16x3": BF16x3 M2L, FP32 near field), both at
@@ -291,12 +335,15 @@ def fast_1m(pkg, core, torch, flush_l2, cpu=True):
                        "opening 1.5, distanceMin 1 + link + center",
            "l2": "flushed before every tick"}
     for form in ("plain", "bf16x3"):
-        ms = fast_ticks(pkg, core, layout, form, flush_l2)
+        ms, stats = fast_ticks(pkg, core, layout, form, flush_l2)
         out[form] = {"ms_per_tick": round(ms, 4), "steps": 10, "warmup": 3,
                      "rms_vs_direct_sum": fast_rms(pkg, core, layout, form),
                      "rms_targets": 4096}
+        if form == "bf16x3":
+            out[form]["last_pass"] = stats
     out["bf16x3"]["speedup_vs_plain"] = round(out["plain"]["ms_per_tick"] /
                                               out["bf16x3"]["ms_per_tick"], 3)
+    out["roofline"] = fast_roofline(out["bf16x3"]["last_pass"], device_peaks(pkg))
     if cpu:
         import oracle
         ocore = oracle.load(pkg)
@@ -506,13 +553,13 @@ def device_peaks(pkg):
     fn = lib.d3_device_peaks
     fn.restype = ctypes.c_int32
     fn.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.c_uint32]
-    out = (ctypes.c_double * 8)()
-    rc = fn(out, 8)
+    out = (ctypes.c_double * 9)()
+    rc = fn(out, 9)
     if rc != 0:
         return None
     return {"dadd_per_s": out[0], "dmul_per_s": out[1], "dfma_per_s": out[2],
             "ddiv_per_s": out[3], "dsqrt_per_s": out[4], "handoff_us": out[5],
-            "sms": int(out[6]), "clock_khz": int(out[7])}
+            "sms": int(out[6]), "clock_khz": int(out[7]), "ffma_per_s": out[8]}
 
 
 def run_ours(args, pkg, sc):
@@ -708,10 +755,32 @@ def run_reference(args, pkg, sc):
     print(json.dumps(line), flush=True)
 
 
+def run_only(args, pkg):
+    """One fast-mode leg alone, printed as its own JSON line (profiling runs)."""
+    import torch
+    core = pkg.cuda_core()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+
+    def flush_l2():
+        flush.zero_()
+        torch.cuda.synchronize()
+
+    if args.only == "fast":
+        out = fast_1m(pkg, core, torch, flush_l2, cpu=not args.no_cpu_baseline)
+    elif args.only == "learned":
+        out = learned_1m(pkg, core, torch, flush_l2)
+    else:
+        out = batched(pkg, core)
+    print(json.dumps({args.only: out}), flush=True)
+
+
 def main():
     args = parse()
     pkg = importlib.import_module("d3-force-wasm_b200")
     sc = importlib.import_module("d3-force-wasm_b200.scenarios")
+    if args.only:
+        run_only(args, pkg)
+        return
     if args.impl == "reference":
         run_reference(args, pkg, sc)
     else:

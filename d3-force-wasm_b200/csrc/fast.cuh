@@ -101,7 +101,9 @@ int fmm_tc_set_learned(FastScratch &s, const float *params, uint32_t len);
 // the cell index for leaves or -1) into out when cap >= the cell count;
 // returns the cell count.
 int fmm_tc_leaves(FastScratch &s, float *out, uint32_t cap);
-// checks, fallbacks, last sampled RMS, cells of the last run
+// out[12]: checks, fallbacks, last sampled RMS, cells of the last run; the
+// last pass's M2L and P2P milliseconds (CUDA events), its M2L tiles, its work
+// counts (M2L pairs, P2P point pairs, M2P and P2L point-cell pairs) and q.
 void fmm_tc_stats(FastScratch &s, double *out);
 // fmm.zig:247-354. Returns 1 when applied, 0 when the exact kernel must run
 // instead (non-finite extent), < 0 on failure.

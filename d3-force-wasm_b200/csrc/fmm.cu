@@ -8,8 +8,9 @@
 //  keys     square extent, 16-bit quantised Morton keys, stable 4-pass sort
 //           (tree.zig:287-309, 346-364).
 //  cells    level-order cells over the sorted keys, leaf at <= 32 points or
-//           depth 16, children contiguous (fmm.zig:685-717); one cooperative
-//           launch, a grid barrier per level.
+//           depth 16, children contiguous (fmm.zig:685-717); all levels at
+//           once from each point's shared digits (four launches, no level
+//           barriers).
 //  upward   per level from the deepest: bounding box, centre and radius
 //           (fmm.zig:721-754), P2M at leaves and M2M from the children
 //           (fmm.zig:757-806), then M_k /= k! (fmm.zig:629-642).
@@ -66,7 +67,6 @@ struct FmmDev {
   double *px = nullptr, *py = nullptr, *ps = nullptr, *ux = nullptr, *uy = nullptr;
   FCell *cells = nullptr;
   double *bx0 = nullptr, *by0 = nullptr, *bx1 = nullptr, *by1 = nullptr;
-  uint32_t *tmp = nullptr;
   uint32_t *m2l_off = nullptr, *m2l_cnt = nullptr, *p2p_off = nullptr, *p2p_cnt = nullptr;
   uint32_t *fwd_off = nullptr, *fwd_cnt = nullptr;
   uint32_t *m2l = nullptr, *p2p = nullptr, *fwd = nullptr;
@@ -79,6 +79,10 @@ struct FmmDev {
   double *h_geom = nullptr;      // pinned: square[3], extent[4]
   int coop_blocks = 0;
   size_t last_m2l = 0, last_p2p = 0, last_fwd = 0;  // list sizes of the previous run
+  // the cell build: per-block counts per level, each cell's start and level
+  uint32_t *cb_count = nullptr, *start_of = nullptr;
+  uint8_t *level_of = nullptr;
+  size_t cb_count_cap = 0, start_cap = 0, level_cap = 0;
 };
 
 struct FmmArgs {
@@ -157,62 +161,6 @@ __global__ void k_fmm_gather(const uint32_t *perm, const double *xs, const doubl
 
 // ---- grid-wide helpers --------------------------------------------------------
 
-__device__ uint32_t block_sum_u32(uint32_t v, uint32_t *sw) {
-  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  if (lane == 0) sw[warp] = v;
-  __syncthreads();
-  uint32_t t = 0;
-  for (unsigned w = 0; w < blockDim.x / 32; ++w) t += sw[w];
-  __syncthreads();
-  return t;
-}
-
-// Exclusive scan of v[0..len) in place over the whole grid; returns the
-// total. The caller separates consecutive calls and later reads of v with a
-// grid barrier.
-__device__ uint32_t grid_scan(cg::grid_group &g, uint32_t *v, uint32_t len, uint32_t *bsum) {
-  __shared__ uint32_t sw[33];
-  const uint32_t nb = gridDim.x, b = blockIdx.x, t = threadIdx.x;
-  const uint32_t seg = (len + nb - 1) / nb;
-  const uint32_t s0 = min(len, b * seg), s1 = min(len, s0 + seg);
-  uint32_t acc = 0;
-  for (uint32_t i = s0 + t; i < s1; i += blockDim.x) acc += ldg_cg(&v[i]);
-  acc = block_sum_u32(acc, sw);
-  if (t == 0) bsum[b] = acc;
-  g.sync();
-  uint32_t off = 0, tot = 0;
-  for (uint32_t k = t; k < nb; k += blockDim.x) {
-    const uint32_t x = ldg_cg(&bsum[k]);
-    if (k < b) off += x;
-    tot += x;
-  }
-  off = block_sum_u32(off, sw);
-  tot = block_sum_u32(tot, sw);
-  uint32_t run = off;
-  const unsigned lane = t & 31, warp = t >> 5, nw = blockDim.x >> 5;
-  for (uint32_t base = s0; base < s1; base += blockDim.x) {
-    const uint32_t i = base + t;
-    const uint32_t x = i < s1 ? ldg_cg(&v[i]) : 0;
-    uint32_t incl = x;
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= (unsigned)o) incl += y;
-    }
-    if (lane == 31) sw[warp] = incl;
-    __syncthreads();
-    uint32_t wpre = 0, tile = 0;
-    for (unsigned w = 0; w < nw; ++w) {
-      if (w < warp) wpre += sw[w];
-      tile += sw[w];
-    }
-    if (i < s1) v[i] = run + wpre + incl - x;
-    run += tile;
-    __syncthreads();
-  }
-  return tot;
-}
-
 // ---- cells (fmm.zig:685-717) ---------------------------------------------------
 
 // The child ranges of a cell at depth d: bnd[q] .. bnd[q + 1] holds digit q.
@@ -238,72 +186,203 @@ __device__ uint32_t child_ranges(const uint64_t *keys, uint32_t first, uint32_t 
   return nc;
 }
 
-__global__ void __launch_bounds__(FMM_THREADS) k_fmm_cells(const uint64_t *keys, uint32_t m,
-                                                           FCell *cells, uint32_t ccap,
-                                                           uint32_t *tmp, uint32_t *bsum,
-                                                           uint32_t *info) {
-  cg::grid_group g = cg::this_grid();
-  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
-  if (tid == 0) {
-    FCell c;
-    c.cx = c.cy = c.r = 0;
-    c.first = 0;
-    c.count = m;
-    c.child0 = 0;
-    c.nchild = 0;
-    c.depth = 0;
-    c.parent = NONE;
-    cells[0] = c;
-    info[FI_OVERFLOW] = 0;
-    info[FI_LVL + 0] = 0;
-    info[FI_LVL + 1] = 1;
+// ---- cells, all levels at once -------------------------------------------------------
+//
+// The same cells as fmm.zig:685-717 (level order, each level in key order,
+// children contiguous in digit order), built without a pass per level. A
+// level-d cell is a maximal run of sorted keys sharing d digits whose
+// enclosing level-(d-1) run holds more than FMM_LEAF points (d <= 16). So a
+// point k starts cells at the levels d in (lcp(k), top(k)], where lcp(k) is
+// the digits it shares with point k - 1, provided the level-lcp(k) run around
+// it holds more than FMM_LEAF points, and top(k) = min(16, max(lcp + 1,
+// A(k) + 1)) with A(k) the digits keys k and k + FMM_LEAF share (a run that
+// starts at k holds more than FMM_LEAF points exactly at the levels <= A(k)).
+// Passes: per point the flags and per-block counts per level; a scan of the
+// counts; per point the cells' places (level start + block offset + rank in
+// the block); per cell its range, children and parent by binary searches.
+
+constexpr uint32_t CB_THREADS = 256;
+constexpr uint32_t CB_LEVELS = FMM_LEVELS + 1;  // levels 0 .. 16
+
+__device__ inline int shared_digits(uint32_t a, uint32_t b) {
+  return a == b ? 16 : __clz(a ^ b) >> 1;
+}
+
+// First index in [lo, hi) whose key >= t (keys sorted; low 32 bits).
+__device__ inline uint32_t key_lower(const uint64_t *keys, uint32_t lo, uint32_t hi, uint64_t t) {
+  while (lo < hi) {
+    const uint32_t mid = lo + (hi - lo) / 2;
+    if ((uint64_t)(uint32_t)keys[mid] < t) lo = mid + 1;
+    else hi = mid;
   }
-  g.sync();
-  uint32_t lo = 0, hi = 1, nlev = 1;
-  for (uint32_t d = 0; d < FMM_LEVELS; ++d) {
-    for (uint32_t c = lo + tid; c < hi; c += nth) {
-      uint32_t bnd[5];
-      tmp[c - lo] = child_ranges(keys, ldg_cg(&cells[c].first), ldg_cg(&cells[c].count), d, bnd);
-    }
-    g.sync();
-    const uint32_t total = grid_scan(g, tmp, hi - lo, bsum);
-    g.sync();
-    if (total == 0) break;
-    if ((size_t)hi + total > ccap) {
-      if (tid == 0) info[FI_OVERFLOW] = hi + total;
-      break;
-    }
-    for (uint32_t c = lo + tid; c < hi; c += nth) {
-      uint32_t bnd[5];
-      const uint32_t nc =
-          child_ranges(keys, ldg_cg(&cells[c].first), ldg_cg(&cells[c].count), d, bnd);
-      const uint32_t c0 = hi + ldg_cg(&tmp[c - lo]);
-      cells[c].child0 = nc ? c0 : 0;
-      cells[c].nchild = nc;
-      uint32_t k = 0;
-      for (uint32_t q = 0; q < 4; ++q) {
-        if (bnd[q + 1] <= bnd[q] || !nc) continue;
-        FCell ch;
-        ch.cx = ch.cy = ch.r = 0;
-        ch.first = bnd[q];
-        ch.count = bnd[q + 1] - bnd[q];
-        ch.child0 = 0;
-        ch.nchild = 0;
-        ch.depth = d + 1;
-        ch.parent = c;
-        cells[c0 + k++] = ch;
+  return lo;
+}
+
+// The levels at which point k starts cells: [d0, d1] (empty when d1 < d0).
+__device__ void cell_levels(const uint64_t *keys, uint32_t m, uint32_t k, int &d0, int &d1) {
+  const uint32_t key = (uint32_t)keys[k];
+  const int lcp = k == 0 ? -1 : shared_digits((uint32_t)keys[k - 1], key);
+  d0 = lcp + 1;
+  d1 = -1;
+  if (lcp >= (int)FMM_LEVELS) return;
+  if (k > 0) {
+    // the level-lcp run around k must hold more than FMM_LEAF points
+    const uint64_t t = lcp ? (uint64_t)(key >> (32 - 2 * lcp)) << (32 - 2 * lcp) : 0;
+    const uint32_t s0 = key_lower(keys, 0, k, t);
+    if (s0 + FMM_LEAF >= m) return;
+    if (shared_digits((uint32_t)keys[s0], (uint32_t)keys[s0 + FMM_LEAF]) < lcp) return;
+  }
+  const int A = k + FMM_LEAF < m ? shared_digits(key, (uint32_t)keys[k + FMM_LEAF]) : -1;
+  int top = A + 1 > d0 ? A + 1 : d0;
+  d1 = top < (int)FMM_LEVELS ? top : (int)FMM_LEVELS;
+}
+
+__global__ void __launch_bounds__(CB_THREADS) k_cells_count(const uint64_t *keys, uint32_t m,
+                                                            uint32_t *bcount) {
+  __shared__ uint32_t wc[CB_LEVELS][CB_THREADS / 32];
+  const uint32_t k = blockIdx.x * CB_THREADS + threadIdx.x;
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int d0 = 0, d1 = -1;
+  if (k < m) cell_levels(keys, m, k, d0, d1);
+  for (int d = 0; d < (int)CB_LEVELS; ++d) {
+    const unsigned b = __ballot_sync(0xffffffffu, d >= d0 && d <= d1);
+    if (lane == 0) wc[d][warp] = __popc(b);
+  }
+  __syncthreads();
+  if (threadIdx.x < CB_LEVELS) {
+    uint32_t t = 0;
+    for (uint32_t w = 0; w < CB_THREADS / 32; ++w) t += wc[threadIdx.x][w];
+    bcount[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = t;
+  }
+}
+
+// One block: per level the exclusive scan of the block counts, the level
+// starts (info FI_LVL + d), the cell total, the level count, and the
+// overflow word when the cells do not fit `ccap`.
+__global__ void __launch_bounds__(1024) k_cells_scan(uint32_t *bcount, uint32_t nb, uint32_t ccap,
+                                                     uint32_t *info) {
+  __shared__ uint32_t tot[CB_LEVELS];
+  __shared__ uint32_t sw[32];
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (uint32_t d = 0; d < CB_LEVELS; ++d) {
+    uint32_t *v = bcount + (size_t)d * nb;
+    uint32_t run = 0;
+    for (uint32_t base = 0; base < nb; base += blockDim.x) {
+      const uint32_t i = base + threadIdx.x;
+      const uint32_t x = i < nb ? v[i] : 0;
+      uint32_t incl = x;
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (unsigned)o) incl += y;
       }
+      if (lane == 31) sw[warp] = incl;
+      __syncthreads();
+      uint32_t wpre = 0, tile = 0;
+      for (unsigned w = 0; w < nw; ++w) {
+        if (w < warp) wpre += sw[w];
+        tile += sw[w];
+      }
+      if (i < nb) v[i] = run + wpre + incl - x;
+      run += tile;
+      __syncthreads();
     }
-    lo = hi;
-    hi += total;
-    ++nlev;
-    if (tid == 0) info[FI_LVL + nlev] = hi;
-    g.sync();
+    if (threadIdx.x == 0) tot[d] = run;
+    __syncthreads();
   }
-  if (tid == 0) {
-    info[FI_CELLS] = hi;
+  if (threadIdx.x == 0) {
+    uint32_t at = 0, nlev = 0;
+    for (uint32_t d = 0; d < CB_LEVELS; ++d) {
+      info[FI_LVL + d] = at;
+      at += tot[d];
+      if (tot[d]) nlev = d + 1;
+    }
+    info[FI_LVL + CB_LEVELS] = at;
+    info[FI_CELLS] = at;
     info[FI_LEVELS] = nlev;
+    info[FI_OVERFLOW] = at > ccap ? at : 0;
   }
+}
+
+// start_of[cell] = the point that starts it; level_of[cell] = its level.
+__global__ void __launch_bounds__(CB_THREADS) k_cells_place(const uint64_t *keys, uint32_t m,
+                                                            const uint32_t *bcount,
+                                                            const uint32_t *info,
+                                                            uint32_t *start_of,
+                                                            uint8_t *level_of) {
+  __shared__ uint32_t wc[CB_LEVELS][CB_THREADS / 32];
+  if (__ldcg(&info[FI_OVERFLOW])) return;
+  const uint32_t k = blockIdx.x * CB_THREADS + threadIdx.x;
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int d0 = 0, d1 = -1;
+  if (k < m) cell_levels(keys, m, k, d0, d1);
+  uint32_t rank[CB_LEVELS];
+  for (int d = 0; d < (int)CB_LEVELS; ++d) {
+    const unsigned b = __ballot_sync(0xffffffffu, d >= d0 && d <= d1);
+    rank[d] = __popc(b & ((1u << lane) - 1));
+    if (lane == 0) wc[d][warp] = __popc(b);
+  }
+  __syncthreads();
+  if (k >= m) return;
+  for (int d = d0; d <= d1; ++d) {
+    uint32_t pre = 0;
+    for (uint32_t w = 0; w < warp; ++w) pre += wc[d][w];
+    const uint32_t c = __ldcg(&info[FI_LVL + d]) + bcount[(size_t)d * gridDim.x + blockIdx.x] +
+                       pre + rank[d];
+    start_of[c] = k;
+    level_of[c] = (uint8_t)d;
+  }
+}
+
+__global__ void __launch_bounds__(CB_THREADS) k_cells_fill(const uint64_t *keys, uint32_t m,
+                                                           const uint32_t *start_of,
+                                                           const uint8_t *level_of,
+                                                           const uint32_t *info, FCell *cells) {
+  const uint32_t total = __ldcg(&info[FI_CELLS]);
+  if (__ldcg(&info[FI_OVERFLOW])) return;
+  const uint32_t c = blockIdx.x * CB_THREADS + threadIdx.x;
+  if (c >= total) return;
+  const uint32_t k = start_of[c];
+  const int d = level_of[c];
+  const uint32_t key = (uint32_t)keys[k];
+  // the run: the points sharing d digits with k
+  uint32_t end = m;
+  if (d > 0) {
+    const uint64_t pre = key >> (32 - 2 * d);
+    end = key_lower(keys, k, m, (pre + 1) << (32 - 2 * d));
+  }
+  FCell f;
+  f.cx = f.cy = f.r = 0;
+  f.first = k;
+  f.count = end - k;
+  f.depth = (uint32_t)d;
+  f.child0 = 0;
+  f.nchild = 0;
+  if (f.count > FMM_LEAF && d < (int)FMM_LEVELS) {
+    uint32_t bnd[5];
+    f.nchild = child_ranges(keys, k, f.count, (uint32_t)d, bnd);
+    // the first child starts at k: its place among level d + 1's starts
+    const uint32_t lo = __ldcg(&info[FI_LVL + d + 1]), hi = __ldcg(&info[FI_LVL + d + 2]);
+    uint32_t a = lo, b = hi;
+    while (a < b) {
+      const uint32_t mid = a + (b - a) / 2;
+      if (start_of[mid] < k) a = mid + 1;
+      else b = mid;
+    }
+    f.child0 = a;
+  }
+  f.parent = NONE;
+  if (d > 0) {
+    // the level d - 1 cell holding k: the last start <= k among that level's
+    const uint32_t lo = __ldcg(&info[FI_LVL + d - 1]), hi = __ldcg(&info[FI_LVL + d]);
+    uint32_t a = lo, b = hi;
+    while (a < b) {
+      const uint32_t mid = a + (b - a) / 2;
+      if (start_of[mid] <= k) a = mid + 1;
+      else b = mid;
+    }
+    f.parent = a - 1;
+  }
+  cells[c] = f;
 }
 
 // ---- upward: geometry, P2M, M2M, scale ------------------------------------------
@@ -879,14 +958,13 @@ int fmm_reserve_points(FmmDev &f, uint32_t n) {
 int fmm_reserve_cells(FmmDev &f, uint32_t ccap) {
   if (ccap <= f.ccap && f.ccap) return 0;
   cudaFree(f.cells); cudaFree(f.bx0); cudaFree(f.by0); cudaFree(f.bx1); cudaFree(f.by1);
-  cudaFree(f.tmp); cudaFree(f.m2l_off); cudaFree(f.m2l_cnt); cudaFree(f.p2p_off);
+  cudaFree(f.m2l_off); cudaFree(f.m2l_cnt); cudaFree(f.p2p_off);
   cudaFree(f.p2p_cnt); cudaFree(f.fwd_off); cudaFree(f.fwd_cnt);
   D3_CUDA_OK(cudaMalloc(&f.cells, ccap * sizeof(FCell)));
   D3_CUDA_OK(cudaMalloc(&f.bx0, ccap * 8ull));
   D3_CUDA_OK(cudaMalloc(&f.by0, ccap * 8ull));
   D3_CUDA_OK(cudaMalloc(&f.bx1, ccap * 8ull));
   D3_CUDA_OK(cudaMalloc(&f.by1, ccap * 8ull));
-  D3_CUDA_OK(cudaMalloc(&f.tmp, ccap * 4ull));
   D3_CUDA_OK(cudaMalloc(&f.m2l_off, ccap * 4ull));
   D3_CUDA_OK(cudaMalloc(&f.m2l_cnt, ccap * 4ull));
   D3_CUDA_OK(cudaMalloc(&f.p2p_off, ccap * 4ull));
@@ -902,10 +980,11 @@ void fmm_free(FastScratch &s) {
   if (!f) return;
   cudaFree(f->px); cudaFree(f->py); cudaFree(f->ps); cudaFree(f->ux); cudaFree(f->uy);
   cudaFree(f->cells); cudaFree(f->bx0); cudaFree(f->by0); cudaFree(f->bx1); cudaFree(f->by1);
-  cudaFree(f->tmp); cudaFree(f->m2l_off); cudaFree(f->m2l_cnt); cudaFree(f->p2p_off);
+  cudaFree(f->m2l_off); cudaFree(f->m2l_cnt); cudaFree(f->p2p_off);
   cudaFree(f->p2p_cnt); cudaFree(f->fwd_off); cudaFree(f->fwd_cnt); cudaFree(f->m2l);
   cudaFree(f->p2p); cudaFree(f->fwd); cudaFree(f->mco); cudaFree(f->lco); cudaFree(f->tab);
   cudaFree(f->info); cudaFree(f->bsum); cudaFree(f->square);
+  cudaFree(f->cb_count); cudaFree(f->start_of); cudaFree(f->level_of);
   cudaFreeHost(f->h_info); cudaFreeHost(f->h_geom);
   delete f;
   s.fmm = nullptr;
@@ -945,14 +1024,12 @@ int fmm_prepare(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *s
     const size_t smax = FMM_WARPS * 32 * (size_t)(2 * (FMM_MAX_ORDER + 1)) * 8;
     cudaFuncSetAttribute(k_fmm_upward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax);
     cudaFuncSetAttribute(k_fmm_m2l, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax);
-    int per_cells = 0, per_up = 0, per_lists = 0, per_down = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_cells, k_fmm_cells, FMM_THREADS, 0);
+    int per_up = 0, per_lists = 0, per_down = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_up, k_fmm_upward, FMM_THREADS, smax);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_lists, k_fmm_lists, FMM_THREADS, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_down, k_fmm_down, FMM_THREADS,
                                                   FMM_WARPS * 2 * (size_t)(2 * (FMM_MAX_ORDER + 1)) * 8);
-    per = per_cells;
-    if (per_up < per) per = per_up;
+    per = per_up;
     if (per_lists < per) per = per_lists;
     if (per_down < per) per = per_down;
     if (per > 2) per = 2;
@@ -988,15 +1065,16 @@ int fmm_prepare(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *s
   for (int attempt = 0;; ++attempt) {
     if (fmm_reserve_cells(f, want > f.ccap ? want : f.ccap)) return -1;
     {
-      const uint64_t *keys = t.keys;
-      uint32_t mm = m, ccap = f.ccap;
-      FCell *cells = f.cells;
-      uint32_t *tmp = f.tmp, *bsum = f.bsum, *info = f.info;
-      void *params[] = {&keys, &mm, &cells, &ccap, &tmp, &bsum, &info};
-      ++g_launches;
-      if (cudaLaunchCooperativeKernel((const void *)k_fmm_cells, f.coop_blocks, FMM_THREADS,
-                                      params, 0, st) != cudaSuccess)
+      const uint32_t nb = (m + CB_THREADS - 1) / CB_THREADS;
+      if (grow(f.cb_count, f.cb_count_cap, (size_t)nb * CB_LEVELS) ||
+          grow(f.start_of, f.start_cap, (size_t)f.ccap) || grow(f.level_of, f.level_cap, (size_t)f.ccap))
         return -1;
+      D3_LAUNCH(k_cells_count, nb, CB_THREADS, 0, st)(t.keys, m, f.cb_count);
+      D3_LAUNCH(k_cells_scan, 1, 1024, 0, st)(f.cb_count, nb, f.ccap, f.info);
+      D3_LAUNCH(k_cells_place, nb, CB_THREADS, 0, st)(t.keys, m, f.cb_count, f.info, f.start_of,
+                                                    f.level_of);
+      D3_LAUNCH(k_cells_fill, blocks_for(f.ccap, CB_THREADS), CB_THREADS, 0, st)(
+          t.keys, m, f.start_of, f.level_of, f.info, f.cells);
     }
     if (sync_read(f, st)) return -1;
     if (!f.h_info[FI_OVERFLOW]) break;

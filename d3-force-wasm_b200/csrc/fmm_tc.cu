@@ -139,6 +139,11 @@ struct TcDev {
   float *mlp = nullptr;              // installed network parameters (device)
   uint32_t ncells_last = 0;
   uint32_t hold = 0;                 // ticks left on the fallback after a failed check
+  // CUDA events around the last pass's M2L and P2P launches, its M2L tiles
+  // and vector slots per tile
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  uint32_t last_tiles = 0, last_slots = 0;
+  void *last_args = nullptr;  // a TcArgs copy of the last pass (for the work counts)
 };
 
 struct TcArgs {
@@ -986,6 +991,32 @@ __global__ void k_tc_apply(TcArgs a) {
   a.vy[i] = a.vy[i] + kk.y;
 }
 
+// ---- work counts of the last pass (for the roofline) ------------------------------------------------
+
+// out[0] M2L source-target pairs (table entries), out[1] P2P point pairs
+// (targets x sources over each leaf's P2P list, self pairs included),
+// out[2] M2P point-cell pairs, out[3] P2L point-cell pairs.
+__global__ void k_tc_count(TcArgs a, unsigned long long *out) {
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.ncells) return;
+  const TcCell C = a.cells[c];
+  unsigned long long m2l = 0, pp = 0, mp = 0, pl = 0;
+  if (C.level > 0) {
+    const uint32_t ns = a.tab->nslot[C.quad];
+    for (uint32_t j = 0; j < ns; ++j) m2l += a.m2l[(size_t)c * TC_SLOT_MAX + j] != TC_NONE;
+  }
+  const uint32_t *lo = a.loff + (size_t)c * 8;
+  if (C.nchild == 0) {
+    for (uint32_t e = 0; e < lo[1]; ++e) pp += (unsigned long long)C.count * a.cells[a.pool[lo[0] + e]].count;
+    mp = (unsigned long long)C.count * lo[3];
+  }
+  for (uint32_t e = 0; e < lo[5]; ++e) pl += a.cells[a.pool[lo[4] + e]].count;
+  if (m2l) atomicAdd(&out[0], m2l);
+  if (pp) atomicAdd(&out[1], pp);
+  if (mp) atomicAdd(&out[2], mp);
+  if (pl) atomicAdd(&out[3], pl);
+}
+
 // ---- tables (host) --------------------------------------------------------------------------------
 
 struct Cplx {
@@ -1225,7 +1256,14 @@ int tc_order_pass(TcDev &d, TcArgs &g, const TcTabSet &ts, uint32_t tiles, bool 
   g.q = ts.p + 1;
   const size_t up_smem = TC_WARPS * 32 * 2 * (size_t)g.q * 8;
   if (coop((const void *)k_tc_upward, d.coop_up, up_smem, g, st)) return -1;
+  if (!d.ev[0])
+    for (cudaEvent_t &e : d.ev) cudaEventCreate(&e);
+  cudaEventRecord(d.ev[0], st);
   if (tiles) D3_LAUNCH(k_tc_m2l, tiles, TC_TILE, sizeof(M2lSmem), st)(g);
+  cudaEventRecord(d.ev[1], st);
+  d.last_tiles = tiles;
+  if (!d.last_args) d.last_args = new TcArgs;
+  *static_cast<TcArgs *>(d.last_args) = g;
   const unsigned wblocks = blocks_for((size_t)g.ncells * 32, TC_THREADS);
   D3_LAUNCH(k_tc_p2l, wblocks, TC_THREADS, 0, st)(g);
   if (coop((const void *)k_tc_down, d.coop_down, TC_WARPS * TC_KN * 4, g, st)) return -1;
@@ -1237,7 +1275,9 @@ int tc_order_pass(TcDev &d, TcArgs &g, const TcTabSet &ts, uint32_t tiles, bool 
   }
   D3_LAUNCH(k_tc_leaf, blocks_for((size_t)nleaf * 32, TC_THREADS), TC_THREADS, 0, st)(
       g, learned ? 1 : 0);
+  cudaEventRecord(d.ev[2], st);
   D3_LAUNCH(k_tc_p2p, wblocks, TC_THREADS, 0, st)(g);
+  cudaEventRecord(d.ev[3], st);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
@@ -1255,6 +1295,9 @@ void fmm_tc_free(FastScratch &s) {
   cudaFree(d->pool); cudaFree(d->far); cudaFree(d->info); cudaFreeHost(d->h_info);
   cudaFree(d->feat); cudaFree(d->leaves); cudaFree(d->mlp_x); cudaFree(d->mlp_y);
   cudaFree(d->kick); cudaFree(d->chk); cudaFreeHost(d->h_chk); cudaFree(d->mlp);
+  for (cudaEvent_t e : d->ev)
+    if (e) cudaEventDestroy(e);
+  delete static_cast<TcArgs *>(d->last_args);
   delete d;
   s.fmm_tc = nullptr;
 }
@@ -1278,12 +1321,27 @@ int fmm_tc_leaves(FastScratch &s, float *out, uint32_t cap) {
 
 void fmm_tc_stats(FastScratch &s, double *out) {
   TcDev *d = static_cast<TcDev *>(s.fmm_tc);
-  for (int k = 0; k < 4; ++k) out[k] = 0;
+  for (int k = 0; k < 12; ++k) out[k] = 0;
   if (!d) return;
   out[0] = s.learn_checks;
   out[1] = s.learn_fallbacks;
   out[2] = s.learn_last_rms;
   out[3] = d->ncells_last;
+  if (!d->ev[0] || !d->last_args) return;
+  float ms = 0;
+  if (cudaEventElapsedTime(&ms, d->ev[0], d->ev[1]) == cudaSuccess) out[4] = ms;
+  if (cudaEventElapsedTime(&ms, d->ev[2], d->ev[3]) == cudaSuccess) out[5] = ms;
+  const TcArgs &g = *static_cast<const TcArgs *>(d->last_args);
+  out[6] = d->last_tiles;
+  unsigned long long *cnt = nullptr;
+  if (cudaMalloc(&cnt, 4 * sizeof(unsigned long long)) != cudaSuccess) return;
+  unsigned long long h[4] = {0, 0, 0, 0};
+  cudaMemset(cnt, 0, sizeof h);
+  k_tc_count<<<blocks_for(g.ncells, 256), 256>>>(g, cnt);
+  if (cudaMemcpy(h, cnt, sizeof h, cudaMemcpyDeviceToHost) == cudaSuccess)
+    for (int k = 0; k < 4; ++k) out[7 + k] = (double)h[k];
+  cudaFree(cnt);
+  out[11] = g.q;
 }
 
 int fmm_tc_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *strengths,

@@ -14,6 +14,7 @@
 //          release store of a flag in global memory seen by an acquire load
 //          spinning on another SM (half of a measured ping-pong round trip)
 //   out[6] SMs, out[7] SM clock (kHz, the device attribute)
+//   out[8] (len >= 9) FP32 FMA per second
 // Every spin is bounded; a wait that runs out makes the call fail.
 #include <cuda_runtime.h>
 
@@ -49,6 +50,21 @@ __global__ void __launch_bounds__(PK_THREADS) k_peak_fp64(double *out, int iters
 #pragma unroll
   for (int c = 0; c < PK_CHAINS; ++c) s += v[c];
   if (s == 12345.678) out[0] = s;  // keeps the chains alive
+}
+
+__global__ void __launch_bounds__(PK_THREADS) k_peak_ffma(double *out, int iters, float a, float b) {
+  float v[PK_CHAINS];
+  const float seed = 1.0f + 1e-6f * (threadIdx.x & 63);
+#pragma unroll
+  for (int c = 0; c < PK_CHAINS; ++c) v[c] = seed + c;
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int c = 0; c < PK_CHAINS; ++c) v[c] = __fmaf_rn(v[c], a, b);
+  }
+  float s = 0;
+#pragma unroll
+  for (int c = 0; c < PK_CHAINS; ++c) s += v[c];
+  if (s == 12345.678f) out[0] = s;
 }
 
 // Ping-pong between block 0 and block 1 of a cooperative launch (so both are
@@ -150,6 +166,15 @@ extern "C" int32_t d3_device_peaks(double *out, uint32_t len) {
   out[5] = (double)h[0] / rounds / 2.0 * 1e-3;
   out[6] = sms;
   out[7] = clk_khz;
+  if (len >= 9) {
+    // FP32 FMA per second (x2 for flop/s): the fast forms' near field
+    k_peak_ffma<<<blocks, PK_THREADS, 0, st>>>(sink, 4, 0.9999999f, 0.5f);
+    cudaEventRecord(e0, st);
+    k_peak_ffma<<<blocks, PK_THREADS, 0, st>>>(sink, 4096, 0.9999999f, 0.5f);
+    cudaEventRecord(e1, st);
+    if (cudaEventSynchronize(e1) != cudaSuccess) rc = D3_WORKER_FAILED;
+    out[8] = ops_per_iter * 4096 / (time_ms(e0, e1) * 1e-3);
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   cudaStreamDestroy(st);

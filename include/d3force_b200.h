@@ -282,7 +282,8 @@ int32_t batch_autotune(uint32_t h, uint32_t ticks, double *out);
  * global flag seen by another SM's acquire load, half a timed ping-pong
  * round trip); the SM count; the SM clock attribute in kHz. The exact tick
  * runs on the FP64 pipe without FMA and waits through L2, so these are its
- * roofline denominators. len must be >= 8. Every device wait is bounded;
+ * roofline denominators; with len >= 9, out[8] = FP32 FMA/s (the fast forms'
+ * near field). len must be >= 8. Every device wait is bounded;
  * D3_WORKER_FAILED if one ran out or a launch failed. Allocates and frees a
  * few bytes of device memory. */
 int32_t d3_device_peaks(double *out, uint32_t len);

@@ -705,10 +705,15 @@ def run_ours(args, pkg, sc):
     line["config"]["bit_exact"] = all(checks.values())
     line["bit_exact_checks"] = checks
     if not args.no_fast and world == 1:
-        line["fast_1m"] = fast_1m(pkg, pkg.cuda_core(), torch, flush_l2,
-                                  cpu=not args.no_cpu_baseline)
-        line["learned_1m"] = learned_1m(pkg, pkg.cuda_core(), torch, flush_l2)
-        line["batched"] = batched(pkg, pkg.cuda_core())
+        # the fast-mode legs; one that fails reports its error, not the line
+        for key, leg in (("fast_1m", lambda: fast_1m(pkg, pkg.cuda_core(), torch, flush_l2,
+                                                      cpu=not args.no_cpu_baseline)),
+                         ("learned_1m", lambda: learned_1m(pkg, pkg.cuda_core(), torch, flush_l2)),
+                         ("batched", lambda: batched(pkg, pkg.cuda_core()))):
+            try:
+                line[key] = leg()
+            except Exception as e:  # noqa: BLE001
+                line[key] = {"error": "%s: %s" % (type(e).__name__, e)}
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

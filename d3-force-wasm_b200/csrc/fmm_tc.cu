@@ -865,6 +865,9 @@ __global__ void __launch_bounds__(TC_THREADS) k_tc_leaf(TcArgs a, int corrected)
 
 // ---- P2P (FP32 with an FP64 origin shift) ----------------------------------------------------------
 
+// A leaf's targets take a lane each; a leaf of at most 16 (8) points splits
+// the warp into 2 (4) lane groups that hold the same targets and take every
+// other (fourth) source leaf, and the groups' sums are added at the end.
 __global__ void __launch_bounds__(TC_THREADS) k_tc_p2p(TcArgs a) {
   __shared__ float4 src[TC_WARPS][32];
   const unsigned lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
@@ -876,27 +879,32 @@ __global__ void __launch_bounds__(TC_THREADS) k_tc_p2p(TcArgs a) {
     const TcCell A = a.cells[c];
     if (A.nchild) continue;
     const uint32_t np = a.loff[(size_t)c * 8 + 1], op = a.loff[(size_t)c * 8];
+    // lane groups: G groups of W lanes (warp-uniform)
+    const uint32_t G = A.count <= 8 ? 4u : A.count <= 16 ? 2u : 1u, W = 32u / G;
+    const uint32_t grp = lane / W, gl = lane % W;
+    const unsigned gmask = W == 32 ? 0xffffffffu : ((1u << W) - 1u) << (grp * W);
+    float4 *gsrc = src[wl] + grp * W;
     // the leaf's origin: its first point, in FP64 world coordinates
     const double ox = a.px[A.first], oy = a.py[A.first];
-    for (uint32_t tb = A.first; tb < A.first + A.count; tb += 32) {
-      const uint32_t ti = tb + lane;
+    for (uint32_t tb = A.first; tb < A.first + A.count; tb += W) {
+      const uint32_t ti = tb + gl;
       const bool act = ti < A.first + A.count;
       const float xi = act ? (float)(a.px[ti] - ox) : 0.f, yi = act ? (float)(a.py[ti] - oy) : 0.f;
       const uint32_t gi = act ? a.perm[ti] : 0;
       float vx0 = 0, vy0 = 0, vx1 = 0, vy1 = 0;
-      for (uint32_t e = 0; e < np; ++e) {
+      for (uint32_t e = grp; e < np; e += G) {
         const TcCell B = a.cells[a.pool[op + e]];
-        for (uint32_t sb = B.first; sb < B.first + B.count; sb += 32) {
-          const uint32_t sj = sb + lane;
-          const uint32_t ns = min(32u, B.first + B.count - sb);
-          __syncwarp();
+        for (uint32_t sb = B.first; sb < B.first + B.count; sb += W) {
+          const uint32_t sj = sb + gl;
+          const uint32_t ns = min(W, B.first + B.count - sb);
+          __syncwarp(gmask);
           if (sj < B.first + B.count)
-            src[wl][lane] = make_float4((float)(a.px[sj] - ox), (float)(a.py[sj] - oy),
-                                        (float)a.ps[sj], __uint_as_float(sj));
-          __syncwarp();
+            gsrc[gl] = make_float4((float)(a.px[sj] - ox), (float)(a.py[sj] - oy),
+                                   (float)a.ps[sj], __uint_as_float(sj));
+          __syncwarp(gmask);
           if (!act) continue;
           for (uint32_t k = 0; k < ns; ++k) {
-            const float4 sv = src[wl][k];
+            const float4 sv = gsrc[k];
             const uint32_t tj = __float_as_uint(sv.w);
             float dx = sv.x - xi, dy = sv.y - yi;
             float l = dx * dx + dy * dy;
@@ -924,9 +932,15 @@ __global__ void __launch_bounds__(TC_THREADS) k_tc_p2p(TcArgs a) {
           }
         }
       }
-      if (act) {
+      __syncwarp();
+      float vx = vx0 + vx1, vy = vy0 + vy1;
+      for (uint32_t o = W; o < 32; o <<= 1) {  // the groups' sums, in a fixed order
+        vx += __shfl_xor_sync(0xffffffffu, vx, o);
+        vy += __shfl_xor_sync(0xffffffffu, vy, o);
+      }
+      if (act && grp == 0) {
         const float2 f = a.far[ti];
-        const double kx = (double)(vx0 + vx1) + (double)f.x, ky = (double)(vy0 + vy1) + (double)f.y;
+        const double kx = (double)vx + (double)f.x, ky = (double)vy + (double)f.y;
         if (a.kick) {
           a.kick[ti] = make_double2(kx, ky);
         } else {

@@ -87,6 +87,7 @@ def leaf_rows(core, xs, ys, order, alpha=1.0):
     sim.precision("fast", order=order, opening=1.5, form="bf16x3")
     ctx = sim.ctx
     ctx.copy_in(nodes)
+    mb._push()  # theta, distanceMin / distanceMax: the force's scalars
     mb.slot.run(alpha)
     cells = core.sim_fmm_leaves(ctx.h, None, 0)
     rows = np.zeros((max(cells, 1), 16), np.float32)

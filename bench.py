@@ -47,8 +47,9 @@ SIDE_PHASES = {"center_sum_side_stream": 11}
 # reference's worker pool does; link and collide's node loop are serial in both.
 THREADED = "tree keys, sort and emission jobs; many-body record pass"
 # DRAM bytes (read + write) of one collide launch (k_collide_spec) on this
-# workload, from an ncu capture (profiles/k_collide_spec_exact_50k.md)
-COLLIDE_DRAM_BYTES = 63628032 + 9661184
+# workload, from an ncu capture of the 11th pass of a 15-tick schedule
+# (profiles/k_collide_spec_exact_50k.md)
+COLLIDE_DRAM_BYTES = 64813568 + 9635072
 
 
 def parse():

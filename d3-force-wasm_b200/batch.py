@@ -103,17 +103,19 @@ def shard(sizes, world):
 class Batch:
     """The device batch of `graphs` = [(n, src, tgt)] on the CUDA engine."""
 
-    def __init__(self, core, graphs):
+    def __init__(self, core, graphs, positions=None):
+        """positions: optional [(x, y)] per graph; d3's phyllotaxis start
+        otherwise."""
         self.lib = _bind(core.lib)
         counts = np.array([g[0] for g in graphs], np.uint32)
         links = np.array([len(g[1]) for g in graphs], np.uint32)
         src = np.concatenate([g[1] for g in graphs]).astype(np.uint32)
         tgt = np.concatenate([g[2] for g in graphs]).astype(np.uint32)
         xs, ys = [], []
-        for n, _, _ in graphs:
-            x, y = phyllotaxis(n)
-            xs.append(x)
-            ys.append(y)
+        for g, (n, _, _) in enumerate(graphs):
+            x, y = positions[g] if positions is not None else phyllotaxis(n)
+            xs.append(np.asarray(x, np.float64))
+            ys.append(np.asarray(y, np.float64))
         self.x0 = np.concatenate(xs).astype(np.float32)
         self.y0 = np.concatenate(ys).astype(np.float32)
         self.counts = counts

@@ -64,3 +64,77 @@ def test_gpu_batch_ticks_move_and_autotune_picks_a_shape(gcore):
         assert np.abs(x - x0).max() > 1e-3
     finally:
         b.close()
+
+
+def _restated_tick(n, src, tgt, x, y):
+    """One batched tick of one graph in FP64 (numpy), from zero velocity:
+    the many-body force as a direct sum (distanceMin 1), the Jacobi link
+    (distance 30, strength 1 / min(degree), bias degree(source) / (degree(
+    source) + degree(target)), from the snapshot x + v), the Jacobi collide
+    (radius 3 each, an even share of each overlap, from the snapshot after the
+    link), then v *= 0.6 and x += v (link_fast.zig, grid.zig, simple.zig)."""
+    alpha = 1 - (1 - 0.001 ** (1 / 300))
+    vx = np.zeros(n)
+    vy = np.zeros(n)
+    dx = x[None, :] - x[:, None]
+    dy = y[None, :] - y[:, None]
+    l = dx * dx + dy * dy
+    l = np.where(l < 1, np.sqrt(l), l)
+    w = np.where(l > 0, -30.0 * alpha / np.where(l > 0, l, 1), 0)
+    vx += (dx * w).sum(1)
+    vy += (dy * w).sum(1)
+    deg = np.bincount(src, minlength=n) + np.bincount(tgt, minlength=n)
+    px, py = x + vx, y + vy
+    dvx, dvy = np.zeros(n), np.zeros(n)
+    for s_, t_ in zip(src, tgt):
+        ex, ey = px[t_] - px[s_], py[t_] - py[s_]
+        ll = np.hypot(ex, ey)
+        f = (ll - 30) / ll * alpha / min(deg[s_], deg[t_])
+        b = deg[s_] / (deg[s_] + deg[t_])
+        dvx[t_] -= ex * f * b
+        dvy[t_] -= ey * f * b
+        dvx[s_] += ex * f * (1 - b)
+        dvy[s_] += ey * f * (1 - b)
+    vx += dvx
+    vy += dvy
+    px, py = x + vx, y + vy
+    cx = px[:, None] - px[None, :]
+    cy = py[:, None] - py[None, :]
+    d2 = cx * cx + cy * cy
+    hit = (d2 < 36) & (d2 > 0)
+    ll = np.sqrt(np.where(hit, d2, 1))
+    push = np.where(hit, (6 - ll) / ll * 0.5, 0)
+    vx += (cx * push).sum(1)
+    vy += (cy * push).sum(1)
+    vx *= 0.6
+    vy *= 0.6
+    return x + vx, y + vy, vx, vy
+
+
+def test_gpu_batch_tick_matches_fp64_restatement(gcore):
+    """One tick of small graphs, their nodes packed so that collisions occur,
+    against the FP64 restatement: the FP32 tick agrees to 1e-4 of the largest
+    velocity (the FMM's own error is about 1e-6)."""
+    rng = np.random.default_rng(11)
+    graphs, pos = [], []
+    for n in (80, 150, 300, 600):
+        src = rng.integers(0, n, 2 * n)
+        tgt = (src + 1 + rng.integers(0, n - 1, 2 * n)) % n
+        graphs.append((n, src.astype(np.uint32), tgt.astype(np.uint32)))
+        side = 2.5 * np.sqrt(n)  # dense: many pairs closer than 6
+        pos.append((rng.random(n) * side, rng.random(n) * side))
+    b = B.Batch(gcore, graphs, positions=pos)
+    try:
+        b.run(1, graph=False)
+        x, y, vx, vy = b.read()
+    finally:
+        b.close()
+    o = 0
+    for (n, src, tgt), (px, py) in zip(graphs, pos):
+        px32 = px.astype(np.float32).astype(np.float64)
+        py32 = py.astype(np.float32).astype(np.float64)
+        rx, ry, rvx, rvy = _restated_tick(n, src.astype(np.int64), tgt.astype(np.int64), px32, py32)
+        scale = max(np.abs(rvx).max(), np.abs(rvy).max())
+        assert np.abs(vx[o:o + n] - rvx).max() <= 1e-4 * scale, n
+        assert np.abs(vy[o:o + n] - rvy).max() <= 1e-4 * scale, n
+        o += n

@@ -4,8 +4,10 @@
 
 Every source is compiled with -fmad=false -prec-div=true -prec-sqrt=true
 -ftz=false: exact mode reproduces d3-force's f64 arithmetic bit for bit. The
-fast mode's precision forms (fmm_tc.cu) are measured against an FP64 direct
-sum instead, and are compiled with FMA contraction on.
+fast mode's precision forms, the network and batched mode (fmm_tc.cu,
+mlp.cu, batch.cu) are measured against an FP64 direct sum instead: they are
+compiled with FMA contraction on and the fast FP32 division and square root
+(FP64 arithmetic is IEEE either way).
 """
 
 import os
@@ -20,11 +22,11 @@ SOURCES = ["engine.cu", "tree.cu", "scan_sort.cu", "forces.cu", "fast.cu", "fmm.
            "peaks.cu", "fmm_tc.cu", "mlp.cu", "batch.cu"]
 # The precision forms are judged by their error against an FP64 direct sum,
 # not bit for bit: their translation unit may contract to FMA.
-PER_SOURCE = {"fmm_tc.cu": ["-fmad=true"], "mlp.cu": ["-fmad=true"], "batch.cu": ["-fmad=true"]}
-EXACT = ["-fmad=false"]
+FAST = ["-fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=false"]
+PER_SOURCE = {"fmm_tc.cu": FAST, "mlp.cu": FAST, "batch.cu": FAST}
+EXACT = ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
-         "-prec-div=true", "-prec-sqrt=true", "-ftz=false",
          "-Xcompiler", "-fPIC", "-Xptxas", "-warn-spills"]
 
 

@@ -256,49 +256,57 @@ __global__ void __launch_bounds__(CB_THREADS) k_cells_count(const uint64_t *keys
   }
 }
 
-// One block: per level the exclusive scan of the block counts, the level
-// starts (info FI_LVL + d), the cell total, the level count, and the
-// overflow word when the cells do not fit `ccap`.
-__global__ void __launch_bounds__(1024) k_cells_scan(uint32_t *bcount, uint32_t nb, uint32_t ccap,
+// One block per level: the exclusive scan of that level's block counts; the
+// level's cell count goes to info FI_LVL + d (k_cells_starts turns the counts
+// into starts).
+__global__ void __launch_bounds__(1024) k_cells_scan(uint32_t *bcount, uint32_t nb,
                                                      uint32_t *info) {
-  __shared__ uint32_t tot[CB_LEVELS];
   __shared__ uint32_t sw[32];
   const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (uint32_t d = 0; d < CB_LEVELS; ++d) {
-    uint32_t *v = bcount + (size_t)d * nb;
-    uint32_t run = 0;
-    for (uint32_t base = 0; base < nb; base += blockDim.x) {
-      const uint32_t i = base + threadIdx.x;
-      const uint32_t x = i < nb ? v[i] : 0;
-      uint32_t incl = x;
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= (unsigned)o) incl += y;
-      }
-      if (lane == 31) sw[warp] = incl;
-      __syncthreads();
-      uint32_t wpre = 0, tile = 0;
-      for (unsigned w = 0; w < nw; ++w) {
-        if (w < warp) wpre += sw[w];
-        tile += sw[w];
-      }
-      if (i < nb) v[i] = run + wpre + incl - x;
-      run += tile;
-      __syncthreads();
+  const uint32_t d = blockIdx.x;
+  uint32_t *v = bcount + (size_t)d * nb;
+  uint32_t run = 0;
+  for (uint32_t base = 0; base < nb; base += blockDim.x) {
+    const uint32_t i = base + threadIdx.x;
+    const uint32_t x = i < nb ? v[i] : 0;
+    uint32_t incl = x;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= (unsigned)o) incl += y;
     }
-    if (threadIdx.x == 0) tot[d] = run;
+    if (lane == 31) sw[warp] = incl;
+    __syncthreads();
+    uint32_t wpre = 0, tile = 0;
+    for (unsigned w = 0; w < nw; ++w) {
+      if (w < warp) wpre += sw[w];
+      tile += sw[w];
+    }
+    if (i < nb) v[i] = run + wpre + incl - x;
+    run += tile;
     __syncthreads();
   }
-  if (threadIdx.x == 0) {
-    uint32_t at = 0, nlev = 0;
-    for (uint32_t d = 0; d < CB_LEVELS; ++d) {
-      info[FI_LVL + d] = at;
-      at += tot[d];
-      if (tot[d]) nlev = d + 1;
-    }
+  if (threadIdx.x == 0) info[FI_LVL + d] = run;
+}
+
+// One warp: the level starts (info FI_LVL + d) from the per-level counts, the
+// cell total, the level count, and the overflow word when the cells do not
+// fit `ccap`.
+__global__ void __launch_bounds__(32) k_cells_starts(uint32_t ccap, uint32_t *info) {
+  static_assert(CB_LEVELS <= 32, "one lane per level");
+  const unsigned lane = threadIdx.x;
+  const uint32_t x = lane < CB_LEVELS ? info[FI_LVL + lane] : 0;
+  uint32_t incl = x;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= (unsigned)o) incl += y;
+  }
+  const uint32_t at = __shfl_sync(0xffffffffu, incl, 31);
+  const unsigned used = __ballot_sync(0xffffffffu, x != 0);
+  if (lane < CB_LEVELS) info[FI_LVL + lane] = incl - x;
+  if (lane == 0) {
     info[FI_LVL + CB_LEVELS] = at;
     info[FI_CELLS] = at;
-    info[FI_LEVELS] = nlev;
+    info[FI_LEVELS] = used ? 32 - __clz(used) : 0;
     info[FI_OVERFLOW] = at > ccap ? at : 0;
   }
 }
@@ -1070,7 +1078,8 @@ int fmm_prepare(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *s
           grow(f.start_of, f.start_cap, (size_t)f.ccap) || grow(f.level_of, f.level_cap, (size_t)f.ccap))
         return -1;
       D3_LAUNCH(k_cells_count, nb, CB_THREADS, 0, st)(t.keys, m, f.cb_count);
-      D3_LAUNCH(k_cells_scan, 1, 1024, 0, st)(f.cb_count, nb, f.ccap, f.info);
+      D3_LAUNCH(k_cells_scan, CB_LEVELS, 1024, 0, st)(f.cb_count, nb, f.info);
+      D3_LAUNCH(k_cells_starts, 1, 32, 0, st)(f.ccap, f.info);
       D3_LAUNCH(k_cells_place, nb, CB_THREADS, 0, st)(t.keys, m, f.cb_count, f.info, f.start_of,
                                                     f.level_of);
       D3_LAUNCH(k_cells_fill, blocks_for(f.ccap, CB_THREADS), CB_THREADS, 0, st)(

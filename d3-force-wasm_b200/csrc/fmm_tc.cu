@@ -68,7 +68,6 @@ constexpr uint32_t TC_CLASS_MAX = 192;
 constexpr uint32_t TC_THREADS = 256;
 constexpr uint32_t TC_WARPS = TC_THREADS / 32;
 constexpr uint32_t TC_TILE = 128;     // target cells per M2L tile (the MMA's M)
-constexpr uint32_t TC_STAGES = 4;
 constexpr uint32_t TC_STACK = 64;
 constexpr uint32_t TC_NONE = 0xFFFFFFFFu;
 constexpr uint32_t TC_NEAR_FLAG = 0x8000u;
@@ -92,6 +91,7 @@ struct TcCell {
 
 struct TcTables {
   uint32_t q, nnear, nslot[4];
+  uint32_t sstride;  // the M2L table's row length: the largest nslot
   int8_t near_dx[TC_NEAR_MAX], near_dy[TC_NEAR_MAX];
   // [target quadrant a][parent near offset o][child quadrant b]: M2L slot,
   // or TC_NEAR_FLAG | near index
@@ -380,7 +380,7 @@ __device__ bool tc_candidate(const TcArgs &a, uint32_t c, const TcCell &A, uint3
       if (B == TC_NONE) return true;
       const uint32_t e16 = a.tab->map[A.quad][o][b];
       if (!(e16 & TC_NEAR_FLAG)) {
-        if (WRITE) a.m2l[(size_t)c * TC_SLOT_MAX + e16] = B;
+        if (WRITE) a.m2l[(size_t)c * a.tab->sstride + e16] = B;
         return true;
       }
       if (WRITE) a.near[(size_t)c * nn + (e16 & 0xFF)] = B;
@@ -428,7 +428,7 @@ __device__ void tc_list_cell(const TcArgs &a, uint32_t c) {
   const unsigned lane = threadIdx.x & 31;
   const uint32_t nn = a.tab->nnear;
   const TcCell A = a.cells[c];
-  for (uint32_t j = lane; j < TC_SLOT_MAX; j += 32) a.m2l[(size_t)c * TC_SLOT_MAX + j] = TC_NONE;
+  for (uint32_t j = lane; j < a.tab->sstride; j += 32) a.m2l[(size_t)c * a.tab->sstride + j] = TC_NONE;
   for (uint32_t j = lane; j < nn; j += 32) a.near[(size_t)c * nn + j] = TC_NONE;
   if (c == 0) {
     // the root: near itself
@@ -520,10 +520,16 @@ __global__ void __launch_bounds__(TC_THREADS) k_tc_lists(TcArgs a) {
 
 // ---- M2L on the tensor cores -------------------------------------------------------------
 
+// M2L CTA: 256 gathering threads (two per target row: the bf16 hi and the lo
+// half of the row) and one warp whose first lane only issues the MMAs.
+constexpr uint32_t M2L_STAGES = 3;
+constexpr uint32_t M2L_PRODUCERS = 2 * TC_TILE;
+constexpr uint32_t M2L_THREADS = M2L_PRODUCERS + 32;
+
 struct M2lSmem {
-  unsigned char a[TC_STAGES][2][TC_TILE * TC_KN * 2];  // [stage][hi, lo] 128 x 32 bf16
-  unsigned char b[TC_STAGES][2][TC_KN * TC_KN * 2];    // [stage][hi, lo] 32 x 32 bf16
-  uint64_t full[TC_STAGES], empty[TC_STAGES], done;
+  unsigned char a[M2L_STAGES][2][TC_TILE * TC_KN * 2];  // [stage][hi, lo] 128 x 32 bf16
+  unsigned char b[M2L_STAGES][2][TC_KN * TC_KN * 2];    // [stage][hi, lo] 32 x 32 bf16
+  uint64_t full[M2L_STAGES], empty[M2L_STAGES], done;
   uint32_t tmem;
   uint32_t tgt[TC_TILE];
   uint32_t err;
@@ -532,7 +538,7 @@ struct M2lSmem {
 // Budget of a wait on a barrier the tile's own threads complete.
 constexpr uint64_t TC_WAIT_NS = 50ull * 1000 * 1000;
 
-__global__ void __launch_bounds__(TC_TILE) k_tc_m2l(TcArgs a) {
+__global__ void __launch_bounds__(M2L_THREADS) k_tc_m2l(TcArgs a) {
   extern __shared__ __align__(1024) unsigned char tc_m2l_smem[];
   M2lSmem &S = *reinterpret_cast<M2lSmem *>(tc_m2l_smem);
   volatile uint32_t *abort = &S.err;
@@ -547,11 +553,11 @@ __global__ void __launch_bounds__(TC_TILE) k_tc_m2l(TcArgs a) {
   }
   if (g == 4) return;  // no tile: nothing allocated yet, nothing to free
   const uint32_t base = tile * TC_TILE;
-  const uint32_t nslot = a.tab->nslot[g];
-  S.tgt[t] = base + t < cnt ? a.groups[(size_t)g * a.ccap + base + t] : TC_NONE;
+  const uint32_t nslot = a.tab->nslot[g], sstride = a.tab->sstride;
+  if (t < TC_TILE) S.tgt[t] = base + t < cnt ? a.groups[(size_t)g * a.ccap + base + t] : TC_NONE;
   if (t == 0) {
-    for (uint32_t s = 0; s < TC_STAGES; ++s) {
-      tc::mbar_init(&S.full[s], TC_TILE);
+    for (uint32_t s = 0; s < M2L_STAGES; ++s) {
+      tc::mbar_init(&S.full[s], M2L_PRODUCERS);
       tc::mbar_init(&S.empty[s], 1);
     }
     tc::mbar_init(&S.done, 1);
@@ -567,48 +573,61 @@ __global__ void __launch_bounds__(TC_TILE) k_tc_m2l(TcArgs a) {
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t tmem = S.tmem;
-  const uint32_t my = S.tgt[t];
-  const uint32_t idesc = tc::idesc_bf16_f32(TC_TILE, TC_KN);
-  uint32_t issued = 0;  // thread 0: MMAs issued
-  for (uint32_t j = 0; j < nslot; ++j) {
-    const uint32_t s = j % TC_STAGES, use = j / TC_STAGES;
-    // the stage is free once the MMAs that read it (slot j - STAGES) are done
-    if (use > 0 && !tc::mbar_wait(&S.empty[s], (use - 1) & 1, abort, TC_WAIT_NS)) break;
-    // A rows: this thread's target's source for slot j (bf16 hi, lo), or zeros
-    const uint32_t src = my != TC_NONE ? __ldcg(&a.m2l[(size_t)my * TC_SLOT_MAX + j]) : TC_NONE;
-    uint4 hv[4], lv[4];
-    if (src != TC_NONE) {
-      const uint4 *m = reinterpret_cast<const uint4 *>(a.mbf + (size_t)src * 64);
+  uint32_t issued = 0;  // the MMA lane: MMAs issued
+  if (t < M2L_PRODUCERS) {
+    // a row's half: 4 chunks of 16 bytes (hi for t < 128, lo otherwise)
+    const uint32_t r = t & (TC_TILE - 1), h = t >> 7;
+    const uint32_t my = S.tgt[r];
+    auto source = [&](uint32_t j) -> uint32_t {
+      return (my != TC_NONE && j < nslot) ? __ldcg(&a.m2l[(size_t)my * sstride + j]) : TC_NONE;
+    };
+    auto rows = [&](uint32_t src, uint4 *v) {
+      if (src != TC_NONE) {
+        const uint4 *m = reinterpret_cast<const uint4 *>(a.mbf + (size_t)src * 64) + h * 4;
 #pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        hv[c] = __ldcg(m + c);
-        lv[c] = __ldcg(m + 4 + c);
+        for (int c = 0; c < 4; ++c) v[c] = __ldcg(m + c);
+      } else {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) v[c] = make_uint4(0, 0, 0, 0);
       }
-    } else {
+    };
+    auto oper = [&](uint32_t j) -> uint4 {  // this thread's 16 bytes of slot j's operator
+      if (j >= nslot) return make_uint4(0, 0, 0, 0);
+      const uint4 *w = reinterpret_cast<const uint4 *>(a.wops + (size_t)a.tab->slot_class[g][j] * 4096);
+      return __ldg(w + t);
+    };
+    // one slot of lookahead for the rows and the operator, two for the table
+    uint32_t src1 = source(1), src2;
+    uint4 cur[4], nxt[4];
+    rows(source(0), cur);
+    uint4 bcur = oper(0), bnxt;
+    for (uint32_t j = 0; j < nslot; ++j) {
+      const uint32_t s = j % M2L_STAGES, use = j / M2L_STAGES;
+      src2 = source(j + 2);
+      rows(j + 1 < nslot ? src1 : TC_NONE, nxt);
+      bnxt = oper(j + 1);
+      // the stage is free once the MMAs that read it (slot j - STAGES) are done
+      if (use > 0 && !tc::mbar_wait(&S.empty[s], (use - 1) & 1, abort, TC_WAIT_NS)) break;
 #pragma unroll
-      for (int c = 0; c < 4; ++c) hv[c] = lv[c] = make_uint4(0, 0, 0, 0);
-    }
+      for (int c = 0; c < 4; ++c)
+        *reinterpret_cast<uint4 *>(&S.a[s][h][tc::tile_offset(r, c, TC_TILE)]) = cur[c];
+      *reinterpret_cast<uint4 *>(&S.b[s][t >> 7][(t & 127) * 16]) = bcur;
+      tc::fence_proxy_async();
+      tc::mbar_arrive(&S.full[s]);
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      const uint32_t off = tc::tile_offset(t, c, TC_TILE);
-      *reinterpret_cast<uint4 *>(&S.a[s][0][off]) = hv[c];
-      *reinterpret_cast<uint4 *>(&S.a[s][1][off]) = lv[c];
+      for (int c = 0; c < 4; ++c) cur[c] = nxt[c];
+      bcur = bnxt;
+      src1 = src2;
     }
-    // B: the slot's operator, already in the tile layout (2 x 2 KB)
-    const uint32_t cls = a.tab->slot_class[g][j];
-    const uint4 *w = reinterpret_cast<const uint4 *>(a.wops + (size_t)cls * 4096);
-    for (uint32_t k = t; k < 256; k += TC_TILE) {
-      const uint4 v = __ldg(w + k);
-      *reinterpret_cast<uint4 *>(&S.b[s][k >> 7][(k & 127) * 16]) = v;
-    }
-    tc::fence_proxy_async();
-    tc::mbar_arrive(&S.full[s]);
-    if (t == 0) {
+  } else if (t == M2L_PRODUCERS) {
+    const uint32_t idesc = tc::idesc_bf16_f32(TC_TILE, TC_KN);
+    const uint32_t alb = (TC_TILE / 8) * 128, blb = (TC_KN / 8) * 128;
+    for (uint32_t j = 0; j < nslot; ++j) {
+      const uint32_t s = j % M2L_STAGES, use = j / M2L_STAGES;
       if (!tc::mbar_wait(&S.full[s], use & 1, abort, TC_WAIT_NS)) break;
       tc::fence_after_sync();
       const uint32_t a_hi = tc::smem_addr(S.a[s][0]), a_lo = tc::smem_addr(S.a[s][1]);
       const uint32_t b_hi = tc::smem_addr(S.b[s][0]), b_lo = tc::smem_addr(S.b[s][1]);
-      const uint32_t alb = (TC_TILE / 8) * 128, blb = (TC_KN / 8) * 128;
 #pragma unroll
       for (uint32_t ks = 0; ks < 2; ++ks) {  // K = 32 as two MMAs of K = 16
         const uint32_t ao = ks * 2 * alb, bo = ks * 2 * blb;
@@ -623,12 +642,11 @@ __global__ void __launch_bounds__(TC_TILE) k_tc_m2l(TcArgs a) {
       issued += 6;
       tc::commit(&S.empty[s]);
     }
+    // every MMA issued so far completes before the accumulator is read and
+    // the TMEM freed (also after a wait that gave up)
+    if (issued) tc::commit(&S.done);
   }
-  // every MMA issued so far completes before the accumulator is read and the
-  // TMEM freed (also after a wait that gave up)
-  if (t == 0 && issued) tc::commit(&S.done);
-  __syncthreads();
-  const bool any = __syncthreads_or(t == 0 && issued > 0);
+  const bool any = __syncthreads_or(issued > 0);
   bool done_ok = true;
   if (any) {
     // a fresh budget: this wait only needs the MMAs already issued
@@ -638,20 +656,25 @@ __global__ void __launch_bounds__(TC_TILE) k_tc_m2l(TcArgs a) {
   tc::fence_after_sync();
   const bool all_done = __syncthreads_and(done_ok);
   const bool good = any && S.err == 0 && all_done;
-  if (good) {
-    float v[32];
-    tc::tmem_ld32(tmem + ((warp * 32u) << 16), v);
-    if (my != TC_NONE) {
+  if (warp < 4) {
+    const uint32_t my = S.tgt[t];
+    if (good) {
+      float v[32];
+      tc::tmem_ld32(tmem + ((warp * 32u) << 16), v);
+      if (my != TC_NONE) {
+        float *L = a.lco + (size_t)my * TC_KN;
+#pragma unroll
+        for (uint32_t k = 0; k < 32; ++k)
+          if (k < 2 * a.q) L[k] = v[k];
+      }
+    } else if (my != TC_NONE) {
       float *L = a.lco + (size_t)my * TC_KN;
-      for (uint32_t k = 0; k < 2 * a.q; ++k) L[k] = v[k];
+      for (uint32_t k = 0; k < 2 * a.q; ++k) L[k] = 0;
     }
-  } else if (my != TC_NONE) {
-    float *L = a.lco + (size_t)my * TC_KN;
-    for (uint32_t k = 0; k < 2 * a.q; ++k) L[k] = 0;
   }
   tc::fence_before_sync();
   __syncthreads();
-  // (after a done-wait that ran out an MMA may still read the accumulator:
+  // (after a done-wait that ran out an MMA may still write the accumulator:
   // the columns are then left allocated rather than freed under it)
   if (warp == 0 && all_done) tc::tmem_dealloc(tmem, 32);
   if (t == 0 && (S.err || !all_done) && nslot) {
@@ -1017,7 +1040,7 @@ __global__ void k_tc_count(TcArgs a, unsigned long long *out) {
   unsigned long long m2l = 0, pp = 0, mp = 0, pl = 0;
   if (C.level > 0) {
     const uint32_t ns = a.tab->nslot[C.quad];
-    for (uint32_t j = 0; j < ns; ++j) m2l += a.m2l[(size_t)c * TC_SLOT_MAX + j] != TC_NONE;
+    for (uint32_t j = 0; j < ns; ++j) m2l += a.m2l[(size_t)c * a.tab->sstride + j] != TC_NONE;
   }
   const uint32_t *lo = a.loff + (size_t)c * 8;
   if (C.nchild == 0) {
@@ -1105,6 +1128,7 @@ int build_tables(TcTabSet &d, uint32_t p, double kappa, cudaStream_t st) {
         ++ns;
       }
     T.nslot[aq] = ns;
+    if (ns > T.sstride) T.sstride = ns;
   }
   // quadrant operators: child centre - parent centre = (s/4) delta_b
   for (uint32_t b = 0; b < 4; ++b) {
@@ -1273,7 +1297,7 @@ int tc_order_pass(TcDev &d, TcArgs &g, const TcTabSet &ts, uint32_t tiles, bool 
   if (!d.ev[0])
     for (cudaEvent_t &e : d.ev) cudaEventCreate(&e);
   cudaEventRecord(d.ev[0], st);
-  if (tiles) D3_LAUNCH(k_tc_m2l, tiles, TC_TILE, sizeof(M2lSmem), st)(g);
+  if (tiles) D3_LAUNCH(k_tc_m2l, tiles, M2L_THREADS, sizeof(M2lSmem), st)(g);
   cudaEventRecord(d.ev[1], st);
   d.last_tiles = tiles;
   if (!d.last_args) d.last_args = new TcArgs;

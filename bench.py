@@ -261,7 +261,8 @@ def fast_ticks(pkg, core, layout, form, flush_l2, steps=10, warmup=3):
     sim.device_end()
     # the tensor-core form's last pass: M2L / P2P event times and work counts
     stats = {k: core.sim_stat(sim.ctx.h, 54 + i) for i, k in enumerate(
-        ("m2l_ms", "p2p_ms", "m2l_tiles", "m2l_pairs", "p2p_pairs", "m2p_pairs", "p2l_pairs", "q"))}
+        ("m2l_ms", "p2p_ms", "m2l_tiles", "m2l_pairs", "p2p_pairs", "m2p_pairs", "p2l_pairs", "q",
+         "prepare_ms", "lists_ms", "upward_ms", "p2l_ms", "down_ms", "leaf_ms", "many_body_ms"))}
     sim.close()
     return sum(times) / len(times), stats
 
@@ -369,6 +370,7 @@ def fast_1m(pkg, core, torch, flush_l2, cpu=True):
 
 
 LEARN_LAYOUTS, LEARN_N = 200, 100000
+LEARN_HOLD = 16  # ticks on the fallback after a failed check
 
 
 def learned_1m(pkg, core, torch, flush_l2):
@@ -404,7 +406,7 @@ def learned_1m(pkg, core, torch, flush_l2):
     for form, order in (("plain", 8), ("bf16x3", 8), ("bf16x3", 4), ("learned", 8)):
         nodes, sim = fast_sim(pkg, core, xs, ys, src, tgt, form, order=order)
         if form == "learned":
-            sim.learned(params, tolerance=1e-5, samples=64)
+            sim.learned(params, tolerance=1e-5, samples=64, hold=LEARN_HOLD)
         sim.device_begin()
         for _ in range(3):
             flush_l2()
@@ -425,7 +427,8 @@ def learned_1m(pkg, core, torch, flush_l2):
                     "rms_vs_direct_sum": acc.rms(kick, ref, tg), "rms_targets": 4096}
         if form == "learned":
             out[key].update({"checks": stats[0], "fallbacks": stats[1],
-                             "last_sampled_rms": stats[2]})
+                             "last_sampled_rms": stats[2], "hold_ticks": LEARN_HOLD,
+                             "ticks_run": 13})
     out["learned"]["speedup_vs_plain_fp64_order8"] = round(
         out["plain"]["ms_per_tick"] / out["learned"]["ms_per_tick"], 3)
     return out

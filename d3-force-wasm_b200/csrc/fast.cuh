@@ -104,6 +104,12 @@ int fmm_tc_leaves(FastScratch &s, float *out, uint32_t cap);
 // out[12]: checks, fallbacks, last sampled RMS, cells of the last run; the
 // last pass's M2L and P2P milliseconds (CUDA events), its M2L tiles, its work
 // counts (M2L pairs, P2P point pairs, M2P and P2L point-cell pairs) and q.
+// The precision forms' counters (TC_STATS doubles): 0 learned-form checks,
+// 1 fallbacks, 2 the last check's RMS, 3 cells; the last pass: 4 M2L ms,
+// 5 P2P ms, 6 M2L tiles, 7 M2L pairs, 8 P2P point pairs, 9 M2P and 10 P2L
+// point-cell pairs, 11 q; the last run's ms: 12 prepare, 13 geometry and
+// lists, 14 upward, 15 P2L, 16 downward, 17 leaves, 18 the whole run.
+constexpr int TC_STATS = 19;
 void fmm_tc_stats(FastScratch &s, double *out);
 // fmm.zig:247-354. Returns 1 when applied, 0 when the exact kernel must run
 // instead (non-finite extent), < 0 on failure.

@@ -44,7 +44,6 @@
 //            FP64 and the pair sums in FP32 (d3's pair formula, distanceMin
 //            clamp, hashed jiggle of hash.zig for coincident points); then
 //            v += far + near in FP64.
-#include <cooperative_groups.h>
 
 #include <cmath>
 #include <cstdio>
@@ -55,7 +54,6 @@
 #include "mlp.cuh"
 #include "tc.cuh"
 
-namespace cg = cooperative_groups;
 
 namespace d3 {
 namespace {
@@ -129,7 +127,8 @@ struct TcDev {
   size_t pool_cap = 0, last_pool = 0;
   float2 *far = nullptr;            // per sorted point
   uint32_t *info = nullptr, *h_info = nullptr;
-  int coop_lists = 0, coop_up = 0, coop_down = 0;
+  int sms = 0;
+  uint32_t *arrive = nullptr;        // per cell: children finished (upward pass)
   // the learned form
   float *feat = nullptr;             // per cell: 16 floats (k_tc_features)
   uint32_t *leaves = nullptr;        // leaf cells (ccap)
@@ -139,9 +138,9 @@ struct TcDev {
   float *mlp = nullptr;              // installed network parameters (device)
   uint32_t ncells_last = 0;
   uint32_t hold = 0;                 // ticks left on the fallback after a failed check
-  // CUDA events around the last pass's M2L and P2P launches, its M2L tiles
-  // and vector slots per tile
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // CUDA events between the passes of the last run: 0 start, 1 prepared,
+  // 2 lists built, 3 upward, 4 M2L, 5 P2L, 6 downward, 7 leaves, 8 near field
+  cudaEvent_t ev[9] = {};
   uint32_t last_tiles = 0, last_slots = 0;
   void *last_args = nullptr;  // a TcArgs copy of the last pass (for the work counts)
 };
@@ -221,6 +220,7 @@ __global__ void k_tc_geom(TcArgs a) {
   t.nchild = (uint8_t)nch;
   t.child0 = nch ? f.child0 : 0;
   a.cells[c] = t;
+  if (nch) a.feat[(size_t)c * 16 + 15] = -1.f;  // no feature row: not a leaf
   if (nch == 0) a.leaves[atomicAdd(&a.info[TI_LEAVES], 1u)] = c;
   if (c == 0)  // the root gets no M2L: its local expansion starts at zero
     for (uint32_t k = 0; k < TC_KN; ++k) a.lco[k] = 0;
@@ -231,79 +231,141 @@ __global__ void k_tc_geom(TcArgs a) {
   }
 }
 
-// ---- upward (FP64) ------------------------------------------------------------------
+// ---- upward (FP64): P2M per leaf, M2M by the last child to finish ----------------------------
 
-// One cell by one warp; ws: this warp's shared rows (32 x 2q doubles).
-__device__ void tc_upward_cell(const TcArgs &a, uint32_t c, double *ws) {
-  const unsigned lane = threadIdx.x & 31;
-  const uint32_t q = a.q, st = 2 * q;
-  const TcCell C = a.cells[c];
-  double cx, cy;
-  cell_centre(C, cx, cy);
-  const double inv_s = ldexp(1.0, (int)C.level);
-  double *mc = a.mco + (size_t)c * st;
-  double acc0 = 0;  // lane r: real r of M'
-  if (C.nchild == 0) {
-    // P2M: M'_k = sum_j s_j ((u_j - c) / s)^k, points added in order
-    for (uint32_t base = C.first; base < C.first + C.count; base += 32) {
-      const uint32_t k = base + lane;
-      const uint32_t np = min(32u, C.first + C.count - base);
-      double *row = ws + lane * st;
-      if (k < C.first + C.count) {
-        const double sv = a.ps[k];
-        const double zr = (a.ux[k] - cx) * inv_s, zi = (a.uy[k] - cy) * inv_s;
-        double pr = sv, pi = 0;
-        for (uint32_t o = 0; o < q; ++o) {
-          row[o] = pr;
-          row[q + o] = pi;
-          const double nr = pr * zr - pi * zi;
-          pi = pr * zi + pi * zr;
-          pr = nr;
-        }
-      }
-      __syncwarp();
-      for (uint32_t t = 0; t < np; ++t) {
-        const double *rt = ws + t * st;
-        if (lane < st) acc0 += rt[lane];
-      }
-      __syncwarp();
-    }
-  } else {
-    // M2M: M'^P_n = sum_b sum_{k<=n} op_b[n][k] M'^b_k (lane n: real, lane q+n: imag)
-    const uint32_t n = lane < q ? lane : lane - q;
-    for (uint32_t b = 0; b < 4; ++b) {
-      const uint32_t ch = child_at(C, b);
-      if (ch == TC_NONE) continue;
-      if (lane < st) {
-        const double *cm = a.mco + (size_t)ch * st;
-        double sr = 0, si = 0;
-        for (uint32_t k = 0; k <= n; ++k) {
-          const double orr = a.tab->m2m_re[b][n][k], oi = a.tab->m2m_im[b][n][k];
-          const double mr = __ldcg(&cm[k]), mi = __ldcg(&cm[q + k]);
-          sr += orr * mr - oi * mi;
-          si += orr * mi + oi * mr;
-        }
-        acc0 += lane < q ? sr : si;
+constexpr uint32_t UP_THREADS = 128;
+
+// M' of cell c (Q = q complex coefficients) into mco and its bf16 split
+// (hi row then lo row, 32 reals each, zero padded) into mbf.
+template <int Q>
+__device__ __forceinline__ void tc_store_m(const TcArgs &a, uint32_t c, const double *mr,
+                                           const double *mi) {
+  double *mc = a.mco + (size_t)c * 2 * Q;
+#pragma unroll
+  for (int k = 0; k < Q; ++k) {
+    mc[k] = mr[k];
+    mc[Q + k] = mi[k];
+  }
+  uint32_t hi[16], lo[16];  // bf16 pairs
+#pragma unroll
+  for (int w = 0; w < 16; ++w) {
+    __nv_bfloat16 h0, l0, h1, l1;
+    const int p0 = 2 * w, p1 = 2 * w + 1;
+    const double v0 = p0 < Q ? mr[p0 < Q ? p0 : 0] : p0 < 2 * Q ? mi[p0 < 2 * Q && p0 >= Q ? p0 - Q : 0] : 0.0;
+    const double v1 = p1 < Q ? mr[p1 < Q ? p1 : 0] : p1 < 2 * Q ? mi[p1 < 2 * Q && p1 >= Q ? p1 - Q : 0] : 0.0;
+    tc::split_bf16(v0, h0, l0);
+    tc::split_bf16(v1, h1, l1);
+    hi[w] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+    lo[w] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+  }
+  uint4 *dst = reinterpret_cast<uint4 *>(a.mbf + (size_t)c * 64);
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    dst[v] = make_uint4(hi[4 * v], hi[4 * v + 1], hi[4 * v + 2], hi[4 * v + 3]);
+    dst[4 + v] = make_uint4(lo[4 * v], lo[4 * v + 1], lo[4 * v + 2], lo[4 * v + 3]);
+  }
+}
+
+// A thread per leaf: P2M, M'_k = sum_j s_j ((u_j - c) / s)^k with the points
+// added in order (upwardCell, fmm.zig:757-807, on the cell's square); then, while its cell
+// is the last of its parent's children to finish (arrival counters, `arrive`
+// zeroed before the launch), the same thread builds the parent by M2M,
+// M'^P_n = sum_b sum_{k<=n} op_b[n][k] M'^b_k over the children in quadrant
+// order (the M2M of upwardCell with the fixed quadrant operators). No level
+// barriers: a parent is built once, by the thread that completes it, from
+// children read through L2.
+template <int Q>
+__global__ void __launch_bounds__(UP_THREADS) k_tc_upward(TcArgs a, uint32_t *arrive) {
+  __shared__ double opr[4][Q][Q], opi[4][Q][Q];
+  for (uint32_t i = threadIdx.x; i < 4 * Q * Q; i += blockDim.x) {
+    const uint32_t b = i / (Q * Q), n = (i / Q) % Q, k = i % Q;
+    opr[b][n][k] = a.tab->m2m_re[b][n][k];
+    opi[b][n][k] = a.tab->m2m_im[b][n][k];
+  }
+  __syncthreads();
+  const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= __ldcg(&a.info[TI_LEAVES])) return;
+  uint32_t c = a.leaves[e];
+  TcCell C = a.cells[c];
+  double mr[Q], mi[Q];
+#pragma unroll
+  for (int k = 0; k < Q; ++k) mr[k] = mi[k] = 0.0;
+  {
+    double cx, cy;
+    cell_centre(C, cx, cy);
+    const double inv_s = ldexp(1.0, (int)C.level);
+    for (uint32_t j = C.first; j < C.first + C.count; ++j) {
+      const double sv = __ldg(&a.ps[j]);
+      const double zr = (__ldg(&a.ux[j]) - cx) * inv_s, zi = (__ldg(&a.uy[j]) - cy) * inv_s;
+      double pr = sv, pi = 0;
+#pragma unroll
+      for (int k = 0; k < Q; ++k) {
+        mr[k] += pr;
+        mi[k] += pi;
+        const double nr = pr * zr - pi * zi;
+        pi = pr * zi + pi * zr;
+        pr = nr;
       }
     }
   }
-  if (lane < st) mc[lane] = acc0;
-  // the bf16 split for the tensor cores: hi row then lo row, zero padded
-  __nv_bfloat16 hi = __float2bfloat16(0.f), lo = __float2bfloat16(0.f);
-  if (lane < st) tc::split_bf16(acc0, hi, lo);
-  a.mbf[(size_t)c * 64 + lane] = hi;
-  a.mbf[(size_t)c * 64 + 32 + lane] = lo;
+  for (uint32_t guard = 0; guard < 32; ++guard) {
+    tc_store_m<Q>(a, c, mr, mi);
+    __threadfence();
+    if (C.parent == TC_NONE) break;
+    const uint32_t par = C.parent;
+    const TcCell P = a.cells[par];
+    if (atomicAdd(&arrive[par], 1u) + 1 != P.nchild) break;
+    __threadfence();
+#pragma unroll
+    for (int k = 0; k < Q; ++k) mr[k] = mi[k] = 0.0;
+    for (uint32_t b = 0; b < 4; ++b) {
+      const uint32_t ch = child_at(P, b);
+      if (ch == TC_NONE) continue;
+      const double *cm = a.mco + (size_t)ch * 2 * Q;
+      double cr[Q], ci[Q];
+#pragma unroll
+      for (int k = 0; k < Q; ++k) {
+        cr[k] = __ldcg(&cm[k]);
+        ci[k] = __ldcg(&cm[Q + k]);
+      }
+#pragma unroll
+      for (int n = 0; n < Q; ++n)
+#pragma unroll
+        for (int k = 0; k <= n; ++k) {
+          const double orr = opr[b][n][k], oi = opi[b][n][k];
+          mr[n] += orr * cr[k] - oi * ci[k];
+          mi[n] += orr * ci[k] + oi * cr[k];
+        }
+    }
+    c = par;
+    C = P;
+  }
 }
 
-__global__ void __launch_bounds__(TC_THREADS) k_tc_upward(TcArgs a) {
-  extern __shared__ double tc_smem[];
-  cg::grid_group g = cg::this_grid();
-  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  double *ws = tc_smem + (threadIdx.x >> 5) * 32 * (2 * a.q);
-  for (int lev = (int)a.nlev - 1; lev >= 0; --lev) {
-    for (uint32_t c = a.lvl[lev] + gw; c < a.lvl[lev + 1]; c += nwarps) tc_upward_cell(a, c, ws);
-    g.sync();
+template <int Q>
+void launch_up_q(const TcArgs &g, uint32_t *arrive, unsigned blocks, cudaStream_t st) {
+  D3_LAUNCH(k_tc_upward<Q>, blocks, UP_THREADS, 0, st)(g, arrive);
+}
+
+void launch_up(const TcArgs &g, uint32_t *arrive, uint32_t nleaf, cudaStream_t st) {
+  const unsigned blocks = blocks_for(nleaf, UP_THREADS);
+  if (!blocks) return;
+  switch (g.q) {
+    case 2: launch_up_q<2>(g, arrive, blocks, st); break;
+    case 3: launch_up_q<3>(g, arrive, blocks, st); break;
+    case 4: launch_up_q<4>(g, arrive, blocks, st); break;
+    case 5: launch_up_q<5>(g, arrive, blocks, st); break;
+    case 6: launch_up_q<6>(g, arrive, blocks, st); break;
+    case 7: launch_up_q<7>(g, arrive, blocks, st); break;
+    case 8: launch_up_q<8>(g, arrive, blocks, st); break;
+    case 9: launch_up_q<9>(g, arrive, blocks, st); break;
+    case 10: launch_up_q<10>(g, arrive, blocks, st); break;
+    case 11: launch_up_q<11>(g, arrive, blocks, st); break;
+    case 12: launch_up_q<12>(g, arrive, blocks, st); break;
+    case 13: launch_up_q<13>(g, arrive, blocks, st); break;
+    case 14: launch_up_q<14>(g, arrive, blocks, st); break;
+    case 15: launch_up_q<15>(g, arrive, blocks, st); break;
+    default: launch_up_q<16>(g, arrive, blocks, st); break;
   }
 }
 
@@ -508,14 +570,11 @@ __device__ void tc_list_cell(const TcArgs &a, uint32_t c) {
   }
 }
 
-__global__ void __launch_bounds__(TC_THREADS) k_tc_lists(TcArgs a) {
-  cg::grid_group g = cg::this_grid();
-  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t lev = 0; lev < a.nlev; ++lev) {
-    for (uint32_t c = a.lvl[lev] + gw; c < a.lvl[lev + 1]; c += nwarps) tc_list_cell(a, c);
-    g.sync();
-  }
+// The cells of one level, a warp per cell; the levels run as consecutive
+// launches from the root down (a cell's lists read its parent's).
+__global__ void __launch_bounds__(TC_THREADS) k_tc_lists(TcArgs a, uint32_t c0, uint32_t c1) {
+  const uint32_t c = c0 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (c < c1) tc_list_cell(a, c);
 }
 
 // ---- M2L on the tensor cores -------------------------------------------------------------
@@ -729,42 +788,88 @@ __global__ void __launch_bounds__(TC_THREADS) k_tc_p2l(TcArgs a) {
   }
 }
 
-// ---- downward: L2L (levels), then L2P and M2P per leaf -----------------------------------------
+// ---- downward: each leaf gathers its ancestors' local expansions ---------------------------------
 
+__host__ __device__ constexpr float binomf(int n, int k) {
+  float r = 1.f;
+  for (int i = 1; i <= k; ++i) r = r * (float)(n - k + i) / (float)i;
+  return r;
+}
+
+// A thread per leaf: L'^leaf += sum over its ancestors P of the ancestor's own
+// M2L and P2L part shifted to the leaf's centre,
+//     L'^leaf_m += r^(m+1) sum_{l>=m} C(l, m) D^(l-m) L'^P_l,
+// D = (c_leaf - c_P) / s_P and r = s_leaf / s_P = 2^-d (the level-by-level
+// L2L of fmm.zig:821-850 composed along the path; D from the integer
+// coordinates, exact in FP32). The leaf's row is updated in place (no other
+// thread reads a leaf's row); Q >= q bounds the unrolled loops.
+template <int Q>
 __global__ void __launch_bounds__(TC_THREADS) k_tc_down(TcArgs a) {
-  extern __shared__ float tc_down_smem[];
-  cg::grid_group g = cg::this_grid();
-  const unsigned lane = threadIdx.x & 31;
-  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= __ldcg(&a.info[TI_LEAVES])) return;
   const uint32_t q = a.q;
-  float *Lw = tc_down_smem + (threadIdx.x >> 5) * TC_KN;
-  for (uint32_t lev = 0; lev + 1 < a.nlev; ++lev) {
-    for (uint32_t c = a.lvl[lev] + gw; c < a.lvl[lev + 1]; c += nwarps) {
-      const TcCell C = a.cells[c];
-      if (!C.nchild) continue;
-      Lw[lane] = lane < 2 * q ? __ldcg(&a.lco[(size_t)c * TC_KN + lane]) : 0.f;
-      __syncwarp();
-      // L2L into each child: L'^b_m += sum_{l>=m} op_b[m][l] L'_l
-      for (uint32_t b = 0; b < 4; ++b) {
-        const uint32_t ch = child_at(C, b);
-        if (ch == TC_NONE) continue;
-        if (lane < q) {
-          float sr = 0, si = 0;
-          for (uint32_t l = lane; l < q; ++l) {
-            const float orr = a.tab->l2l_re[b][lane][l], oi = a.tab->l2l_im[b][lane][l];
-            sr += orr * Lw[l] - oi * Lw[q + l];
-            si += orr * Lw[q + l] + oi * Lw[l];
-          }
-          float *Lc = a.lco + (size_t)ch * TC_KN;
-          Lc[lane] = __ldcg(&Lc[lane]) + sr;
-          Lc[q + lane] = __ldcg(&Lc[q + lane]) + si;
-        }
-      }
-      __syncwarp();
-    }
-    g.sync();
+  const uint32_t c = a.leaves[e];
+  const TcCell C = a.cells[c];
+  float lr[Q], li[Q];
+  float *L = a.lco + (size_t)c * TC_KN;
+#pragma unroll
+  for (int l = 0; l < Q; ++l) {
+    lr[l] = l < (int)q ? L[l] : 0.f;
+    li[l] = l < (int)q ? L[q + l] : 0.f;
   }
+  uint32_t p = C.parent;
+  for (uint32_t guard = 0; p != TC_NONE && guard < 32; ++guard) {
+    const TcCell P = a.cells[p];
+    const float *A = a.lco + (size_t)p * TC_KN;
+    float ar[Q], ai[Q];
+#pragma unroll
+    for (int l = 0; l < Q; ++l) {
+      ar[l] = l < (int)q ? __ldcg(&A[l]) : 0.f;
+      ai[l] = l < (int)q ? __ldcg(&A[q + l]) : 0.f;
+    }
+    const int d = (int)C.level - (int)P.level;
+    const uint32_t mask = (1u << d) - 1u;
+    const float dx = ldexpf((float)(C.ix & mask) + 0.5f, -d) - 0.5f;
+    const float dy = ldexpf((float)(C.iy & mask) + 0.5f, -d) - 0.5f;
+    float pr[Q], pi[Q];  // D^j
+    pr[0] = 1.f;
+    pi[0] = 0.f;
+#pragma unroll
+    for (int j = 1; j < Q; ++j) {
+      pr[j] = pr[j - 1] * dx - pi[j - 1] * dy;
+      pi[j] = pr[j - 1] * dy + pi[j - 1] * dx;
+    }
+#pragma unroll
+    for (int m = 0; m < Q; ++m) {
+      float sr = 0.f, si = 0.f;
+#pragma unroll
+      for (int j = 0; m + j < Q; ++j) {
+        const float b = binomf(m + j, m);
+        const float tr = ar[m + j] * b, ti = ai[m + j] * b;
+        sr += tr * pr[j] - ti * pi[j];
+        si += tr * pi[j] + ti * pr[j];
+      }
+      const float sc = ldexpf(1.f, -(m + 1) * d);
+      lr[m] += sr * sc;
+      li[m] += si * sc;
+    }
+    p = P.parent;
+  }
+#pragma unroll
+  for (int l = 0; l < Q; ++l)
+    if (l < (int)q) {
+      L[l] = lr[l];
+      L[q + l] = li[l];
+    }
+}
+
+void launch_down(const TcArgs &g, uint32_t nleaf, cudaStream_t st) {
+  const unsigned blocks = blocks_for(nleaf, TC_THREADS);
+  if (!blocks) return;
+  if (g.q <= 5) D3_LAUNCH(k_tc_down<5>, blocks, TC_THREADS, 0, st)(g);
+  else if (g.q <= 9) D3_LAUNCH(k_tc_down<9>, blocks, TC_THREADS, 0, st)(g);
+  else if (g.q <= 13) D3_LAUNCH(k_tc_down<13>, blocks, TC_THREADS, 0, st)(g);
+  else D3_LAUNCH(k_tc_down<16>, blocks, TC_THREADS, 0, st)(g);
 }
 
 // Leaf features of the learned correction, from the leaf's final local
@@ -772,18 +877,36 @@ __global__ void __launch_bounds__(TC_THREADS) k_tc_down(TcArgs a) {
 // reals), level / 16, count / 32, and the points' mean offset from the centre
 // in cell sides (2). Row of 16 floats per cell: features, L'_0 (2), sc, and
 // the cell index (as float bits) for leaves, -1 in column 15 otherwise.
+__device__ void feature_row(const TcArgs &a, uint32_t c, const TcCell &C, const float *L, float mx,
+                            float my) {
+  const uint32_t q = a.q;
+  float *row = a.feat + (size_t)c * 16;
+  const uint32_t lmax = q - 1 < 4 ? q - 1 : 4;
+  float s2 = 0;
+  for (uint32_t l = 0; l <= lmax; ++l) s2 += L[l] * L[l] + L[q + l] * L[q + l];
+  const float sc = sqrtf(s2) + 1e-30f;
+  for (uint32_t l = 1; l <= 4; ++l) {
+    row[2 * (l - 1)] = l <= lmax ? L[l] / sc : 0.f;
+    row[2 * (l - 1) + 1] = l <= lmax ? L[q + l] / sc : 0.f;
+  }
+  row[8] = C.level / 16.f;
+  row[9] = C.count / 32.f;
+  row[10] = mx / C.count;
+  row[11] = my / C.count;
+  row[12] = L[0];
+  row[13] = L[q];
+  row[14] = sc;
+  row[15] = __uint_as_float(c);
+}
+
 __global__ void __launch_bounds__(TC_THREADS) k_tc_features(TcArgs a) {
   const unsigned lane = threadIdx.x & 31;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  const uint32_t q = a.q;
-  for (uint32_t c = gw; c < a.ncells; c += nwarps) {
+  const uint32_t nleaf = __ldcg(&a.info[TI_LEAVES]);
+  for (uint32_t e = gw; e < nleaf; e += nwarps) {
+    const uint32_t c = a.leaves[e];
     const TcCell C = a.cells[c];
-    float *row = a.feat + (size_t)c * 16;
-    if (C.nchild) {
-      if (lane == 0) row[15] = -1.f;
-      continue;
-    }
     double cx, cy;
     cell_centre(C, cx, cy);
     const double inv_s = ldexp(1.0, (int)C.level);
@@ -796,25 +919,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_tc_features(TcArgs a) {
       mx += __shfl_xor_sync(0xffffffffu, mx, o);
       my += __shfl_xor_sync(0xffffffffu, my, o);
     }
-    if (lane == 0) {
-      const float *L = a.lco + (size_t)c * TC_KN;
-      const uint32_t lmax = q - 1 < 4 ? q - 1 : 4;
-      float s2 = 0;
-      for (uint32_t l = 0; l <= lmax; ++l) s2 += L[l] * L[l] + L[q + l] * L[q + l];
-      const float sc = sqrtf(s2) + 1e-30f;
-      for (uint32_t l = 1; l <= 4; ++l) {
-        row[2 * (l - 1)] = l <= lmax ? L[l] / sc : 0.f;
-        row[2 * (l - 1) + 1] = l <= lmax ? L[q + l] / sc : 0.f;
-      }
-      row[8] = C.level / 16.f;
-      row[9] = C.count / 32.f;
-      row[10] = mx / C.count;
-      row[11] = my / C.count;
-      row[12] = L[0];
-      row[13] = L[q];
-      row[14] = sc;
-      row[15] = __uint_as_float(c);
-    }
+    if (lane == 0) feature_row(a, c, C, a.lco + (size_t)c * TC_KN, mx, my);
   }
 }
 
@@ -848,8 +953,11 @@ __global__ void __launch_bounds__(TC_THREADS) k_tc_leaf(TcArgs a, int corrected)
     cell_centre(C, cx, cy);
     const double inv_s = ldexp(1.0, (int)C.level);
     const uint32_t nw = a.loff[(size_t)c * 8 + 3], ow = a.loff[(size_t)c * 8 + 2];
+    float mx = 0, my = 0;  // the points' offsets from the centre, for the feature row
     for (uint32_t k = C.first + lane; k < C.first + C.count; k += 32) {
       const float wr = (float)((a.ux[k] - cx) * inv_s), wi = (float)((a.uy[k] - cy) * inv_s);
+      mx += wr;
+      my += wi;
       float ar = q > 1 ? L[q - 1] : l0r, ai = q > 1 ? L[2 * q - 1] : l0i;
       for (int l = (int)q - 2; l >= 0; --l) {
         const float lr = l ? L[l] : l0r, li = l ? L[q + l] : l0i;
@@ -883,80 +991,123 @@ __global__ void __launch_bounds__(TC_THREADS) k_tc_leaf(TcArgs a, int corrected)
       }
       a.far[k] = make_float2((float)(-gr * a.inv_w), (float)(gi * a.inv_w));
     }
+    if (!corrected) {  // the leaf's feature row (k_tc_features writes it for the network)
+      for (int o = 16; o > 0; o >>= 1) {
+        mx += __shfl_xor_sync(0xffffffffu, mx, o);
+        my += __shfl_xor_sync(0xffffffffu, my, o);
+      }
+      if (lane == 0) feature_row(a, c, C, L, mx, my);
+    }
   }
 }
 
 // ---- P2P (FP32 with an FP64 origin shift) ----------------------------------------------------------
 
-// A leaf's targets take a lane each; a leaf of at most 16 (8) points splits
-// the warp into 2 (4) lane groups that hold the same targets and take every
-// other (fourth) source leaf, and the groups' sums are added at the end.
+constexpr uint32_t P2P_STAGE = 256;  // staged source points per warp
+
+// One point pair of the near field (d3's pair formula, the distanceMin clamp
+// and the hashed jiggle of hash.zig for exact zero deltas; the self pair adds
+// nothing).
+__device__ __forceinline__ void tc_pair(const float4 sv, float xi, float yi, uint32_t ti, uint32_t gi,
+                                        float dmin2, uint64_t seed, const uint32_t *perm, float &ax,
+                                        float &ay) {
+  float dx = sv.x - xi, dy = sv.y - yi;
+  float l = dx * dx + dy * dy;
+  if (dx == 0.f || dy == 0.f) {
+    const uint32_t tj = __float_as_uint(sv.w);
+    if (tj == ti) return;
+    const uint32_t gj = perm[tj];
+    if (dx == 0.f) {
+      dx = (float)hash_jiggle(seed, gi, gj, 0);
+      l += dx * dx;
+    }
+    if (dy == 0.f) {
+      dy = (float)hash_jiggle(seed, gi, gj, 1);
+      l += dy * dy;
+    }
+  }
+  if (l < dmin2) l = sqrtf(dmin2 * l);
+  const float w = __fdividef(sv.z, l);
+  ax += dx * w;
+  ay += dy * w;
+}
+
+// A warp per leaf (grid-stride over the leaf list). The leaf's targets take a
+// lane each; a leaf of at most 16 (8) points splits the warp into 2 (4) lane
+// groups that hold the same targets and take alternate sources, their sums
+// added at the end in a fixed order. The source leaves' points are staged in
+// shared memory, relative to the target leaf's first point (the shift taken
+// in FP64): up to 32 source leaves at a time, their points spread over the
+// lanes so every load of a batch is in flight at once.
 __global__ void __launch_bounds__(TC_THREADS) k_tc_p2p(TcArgs a) {
-  __shared__ float4 src[TC_WARPS][32];
+  __shared__ float4 stage[TC_WARPS][P2P_STAGE];
   const unsigned lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const uint64_t seed = (uint64_t)__double_as_longlong(*a.seed);
   const float dmin2 = a.dmin2f;
-  for (uint32_t c = gw; c < a.ncells; c += nwarps) {
+  const uint32_t nleaf = __ldcg(&a.info[TI_LEAVES]);
+  float4 *sg = stage[wl];
+  for (uint32_t e0 = gw; e0 < nleaf; e0 += nwarps) {
+    const uint32_t c = a.leaves[e0];
     const TcCell A = a.cells[c];
-    if (A.nchild) continue;
     const uint32_t np = a.loff[(size_t)c * 8 + 1], op = a.loff[(size_t)c * 8];
-    // lane groups: G groups of W lanes (warp-uniform)
     const uint32_t G = A.count <= 8 ? 4u : A.count <= 16 ? 2u : 1u, W = 32u / G;
     const uint32_t grp = lane / W, gl = lane % W;
-    const unsigned gmask = W == 32 ? 0xffffffffu : ((1u << W) - 1u) << (grp * W);
-    float4 *gsrc = src[wl] + grp * W;
-    // the leaf's origin: its first point, in FP64 world coordinates
     const double ox = a.px[A.first], oy = a.py[A.first];
     for (uint32_t tb = A.first; tb < A.first + A.count; tb += W) {
       const uint32_t ti = tb + gl;
       const bool act = ti < A.first + A.count;
       const float xi = act ? (float)(a.px[ti] - ox) : 0.f, yi = act ? (float)(a.py[ti] - oy) : 0.f;
       const uint32_t gi = act ? a.perm[ti] : 0;
-      float vx0 = 0, vy0 = 0, vx1 = 0, vy1 = 0;
-      for (uint32_t e = grp; e < np; e += G) {
-        const TcCell B = a.cells[a.pool[op + e]];
-        for (uint32_t sb = B.first; sb < B.first + B.count; sb += W) {
-          const uint32_t sj = sb + gl;
-          const uint32_t ns = min(W, B.first + B.count - sb);
-          __syncwarp(gmask);
-          if (sj < B.first + B.count)
-            gsrc[gl] = make_float4((float)(a.px[sj] - ox), (float)(a.py[sj] - oy),
-                                   (float)a.ps[sj], __uint_as_float(sj));
-          __syncwarp(gmask);
-          if (!act) continue;
-          for (uint32_t k = 0; k < ns; ++k) {
-            const float4 sv = gsrc[k];
-            const uint32_t tj = __float_as_uint(sv.w);
-            float dx = sv.x - xi, dy = sv.y - yi;
-            float l = dx * dx + dy * dy;
-            if (tj == ti) continue;
-            if (dx == 0.f || dy == 0.f) {
-              const uint32_t gj = a.perm[tj];
-              if (dx == 0.f) {
-                dx = (float)hash_jiggle(seed, gi, gj, 0);
-                l += dx * dx;
-              }
-              if (dy == 0.f) {
-                dy = (float)hash_jiggle(seed, gi, gj, 1);
-                l += dy * dy;
-              }
+      float ax0 = 0, ay0 = 0, ax1 = 0, ay1 = 0;
+      for (uint32_t eb = 0; eb < np; eb += 32) {
+        // this batch's source leaves: lane j holds leaf j's first point and
+        // the running count before it
+        const uint32_t ne = min(32u, np - eb);
+        uint32_t first = 0, cnt = 0;
+        if (lane < ne) {
+          const TcCell B = a.cells[a.pool[op + eb + lane]];
+          first = B.first;
+          cnt = B.count;
+        }
+        uint32_t total;
+        const uint32_t before = warp_excl_sum(cnt, total);
+        const uint32_t incl = before + cnt;
+        for (uint32_t base = 0; base < total; base += P2P_STAGE) {
+          const uint32_t kn = min(P2P_STAGE, total - base);
+          __syncwarp();
+#pragma unroll
+          for (uint32_t r = 0; r < P2P_STAGE / 32; ++r) {
+            const uint32_t idx = base + r * 32 + lane;
+            // the source leaf holding point idx of the batch: the number of
+            // leaves whose running count ends at or before idx
+            uint32_t j = 0;
+#pragma unroll
+            for (uint32_t step = 16; step; step >>= 1) {
+              const uint32_t v = __shfl_sync(0xffffffffu, incl, j + step - 1);
+              if (j + step - 1 < ne && v <= idx) j += step;
             }
-            if (l < dmin2) l = sqrtf(dmin2 * l);
-            const float w = sv.z / l;
-            if (k & 1) {
-              vx1 += dx * w;
-              vy1 += dy * w;
-            } else {
-              vx0 += dx * w;
-              vy0 += dy * w;
+            const uint32_t f = __shfl_sync(0xffffffffu, first, j & 31);
+            const uint32_t b0 = __shfl_sync(0xffffffffu, before, j & 31);
+            if (idx < base + kn) {
+              const uint32_t sj = f + (idx - b0);
+              sg[r * 32 + lane] = make_float4((float)(__ldg(&a.px[sj]) - ox),
+                                              (float)(__ldg(&a.py[sj]) - oy),
+                                              (float)__ldg(&a.ps[sj]), __uint_as_float(sj));
             }
           }
+          __syncwarp();
+          uint32_t k = grp;
+          for (; k + G < kn; k += 2 * G) {
+            tc_pair(sg[k], xi, yi, ti, gi, dmin2, seed, a.perm, ax0, ay0);
+            tc_pair(sg[k + G], xi, yi, ti, gi, dmin2, seed, a.perm, ax1, ay1);
+          }
+          if (k < kn) tc_pair(sg[k], xi, yi, ti, gi, dmin2, seed, a.perm, ax0, ay0);
         }
       }
       __syncwarp();
-      float vx = vx0 + vx1, vy = vy0 + vy1;
+      float vx = ax0 + ax1, vy = ay0 + ay1;
       for (uint32_t o = W; o < 32; o <<= 1) {  // the groups' sums, in a fixed order
         vx += __shfl_xor_sync(0xffffffffu, vx, o);
         vy += __shfl_xor_sync(0xffffffffu, vy, o);
@@ -1211,6 +1362,8 @@ int reserve(TcDev &d, uint32_t ncells, uint32_t m) {
     D3_CUDA_OK(cudaMalloc(&d.m2l, (size_t)cap * TC_SLOT_MAX * 4));
     D3_CUDA_OK(cudaMalloc(&d.groups, (size_t)cap * 4 * 4));
     D3_CUDA_OK(cudaMalloc(&d.loff, (size_t)cap * 8 * 4));
+    cudaFree(d.arrive);
+    D3_CUDA_OK(cudaMalloc(&d.arrive, (size_t)cap * 4));
     d.ccap = cap;
   }
   if (m > d.pcap) {
@@ -1242,12 +1395,6 @@ TcTabSet *tables_for(TcDev &d, uint32_t p, double kappa, cudaStream_t st) {
   return &t;
 }
 
-int coop(const void *fn, int blocks, size_t smem, TcArgs &args, cudaStream_t st) {
-  void *params[] = {&args};
-  ++g_launches;
-  return cudaLaunchCooperativeKernel(fn, blocks, TC_THREADS, params, smem, st) == cudaSuccess ? 0
-                                                                                              : -1;
-}
 
 }  // namespace
 
@@ -1269,17 +1416,9 @@ TcDev *tc_dev(FastScratch &s) {
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const size_t up_smem = TC_WARPS * 32 * 2 * TC_MAXQ * 8;
-  cudaFuncSetAttribute(k_tc_upward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)up_smem);
   cudaFuncSetAttribute(k_tc_m2l, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(M2lSmem));
-  int pl = 0, pu = 0, pd = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pl, k_tc_lists, TC_THREADS, 0);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pu, k_tc_upward, TC_THREADS, up_smem);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pd, k_tc_down, TC_THREADS, TC_WARPS * TC_KN * 4);
-  d->coop_lists = sms * (pl > 2 ? 2 : pl < 1 ? 1 : pl);
-  d->coop_up = sms * (pu > 2 ? 2 : pu < 1 ? 1 : pu);
-  d->coop_down = sms * (pd > 2 ? 2 : pd < 1 ? 1 : pd);
+  d->sms = sms;
   s.fmm_tc = d;
   return d;
 }
@@ -1292,30 +1431,30 @@ int tc_order_pass(TcDev &d, TcArgs &g, const TcTabSet &ts, uint32_t tiles, bool 
   g.tab = ts.tab;
   g.wops = ts.wops;
   g.q = ts.p + 1;
-  const size_t up_smem = TC_WARPS * 32 * 2 * (size_t)g.q * 8;
-  if (coop((const void *)k_tc_upward, d.coop_up, up_smem, g, st)) return -1;
-  if (!d.ev[0])
-    for (cudaEvent_t &e : d.ev) cudaEventCreate(&e);
-  cudaEventRecord(d.ev[0], st);
+  const uint32_t nleaf = d.h_info[TI_LEAVES];
+  const unsigned lw = blocks_for((size_t)nleaf * 32, TC_THREADS);
+  if (cudaMemsetAsync(d.arrive, 0, (size_t)g.ncells * 4, st) != cudaSuccess) return -1;
+  launch_up(g, d.arrive, nleaf, st);
+  cudaEventRecord(d.ev[3], st);
   if (tiles) D3_LAUNCH(k_tc_m2l, tiles, M2L_THREADS, sizeof(M2lSmem), st)(g);
-  cudaEventRecord(d.ev[1], st);
+  cudaEventRecord(d.ev[4], st);
   d.last_tiles = tiles;
   if (!d.last_args) d.last_args = new TcArgs;
   *static_cast<TcArgs *>(d.last_args) = g;
   const unsigned wblocks = blocks_for((size_t)g.ncells * 32, TC_THREADS);
   D3_LAUNCH(k_tc_p2l, wblocks, TC_THREADS, 0, st)(g);
-  if (coop((const void *)k_tc_down, d.coop_down, TC_WARPS * TC_KN * 4, g, st)) return -1;
-  D3_LAUNCH(k_tc_features, wblocks, TC_THREADS, 0, st)(g);
-  const uint32_t nleaf = d.h_info[TI_LEAVES];
+  cudaEventRecord(d.ev[5], st);
+  launch_down(g, nleaf, st);
+  cudaEventRecord(d.ev[6], st);
   if (learned) {
+    D3_LAUNCH(k_tc_features, lw, TC_THREADS, 0, st)(g);
     D3_LAUNCH(k_tc_pack, blocks_for(nleaf, 256), 256, 0, st)(g);
     if (mlp_infer_tc(d.mlp_x, nleaf, d.mlp, d.mlp_y, g.status, st)) return -1;
   }
-  D3_LAUNCH(k_tc_leaf, blocks_for((size_t)nleaf * 32, TC_THREADS), TC_THREADS, 0, st)(
-      g, learned ? 1 : 0);
-  cudaEventRecord(d.ev[2], st);
-  D3_LAUNCH(k_tc_p2p, wblocks, TC_THREADS, 0, st)(g);
-  cudaEventRecord(d.ev[3], st);
+  D3_LAUNCH(k_tc_leaf, lw, TC_THREADS, 0, st)(g, learned ? 1 : 0);
+  cudaEventRecord(d.ev[7], st);
+  D3_LAUNCH(k_tc_p2p, lw, TC_THREADS, 0, st)(g);
+  cudaEventRecord(d.ev[8], st);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
@@ -1330,6 +1469,7 @@ void fmm_tc_free(FastScratch &s) {
   }
   cudaFree(d->cells); cudaFree(d->mco); cudaFree(d->mbf);
   cudaFree(d->lco); cudaFree(d->near); cudaFree(d->m2l); cudaFree(d->groups); cudaFree(d->loff);
+  cudaFree(d->arrive);
   cudaFree(d->pool); cudaFree(d->far); cudaFree(d->info); cudaFreeHost(d->h_info);
   cudaFree(d->feat); cudaFree(d->leaves); cudaFree(d->mlp_x); cudaFree(d->mlp_y);
   cudaFree(d->kick); cudaFree(d->chk); cudaFreeHost(d->h_chk); cudaFree(d->mlp);
@@ -1359,16 +1499,26 @@ int fmm_tc_leaves(FastScratch &s, float *out, uint32_t cap) {
 
 void fmm_tc_stats(FastScratch &s, double *out) {
   TcDev *d = static_cast<TcDev *>(s.fmm_tc);
-  for (int k = 0; k < 12; ++k) out[k] = 0;
+  for (int k = 0; k < TC_STATS; ++k) out[k] = 0;
   if (!d) return;
   out[0] = s.learn_checks;
   out[1] = s.learn_fallbacks;
   out[2] = s.learn_last_rms;
   out[3] = d->ncells_last;
   if (!d->ev[0] || !d->last_args) return;
-  float ms = 0;
-  if (cudaEventElapsedTime(&ms, d->ev[0], d->ev[1]) == cudaSuccess) out[4] = ms;
-  if (cudaEventElapsedTime(&ms, d->ev[2], d->ev[3]) == cudaSuccess) out[5] = ms;
+  auto span = [&](int a, int b) -> double {
+    float ms = 0;
+    return cudaEventElapsedTime(&ms, d->ev[a], d->ev[b]) == cudaSuccess ? ms : 0.0;
+  };
+  out[4] = span(3, 4);
+  out[5] = span(7, 8);
+  out[12] = span(0, 1);
+  out[13] = span(1, 2);
+  out[14] = span(2, 3);
+  out[15] = span(4, 5);
+  out[16] = span(5, 6);
+  out[17] = span(6, 7);
+  out[18] = span(0, 8);
   const TcArgs &g = *static_cast<const TcArgs *>(d->last_args);
   out[6] = d->last_tiles;
   unsigned long long *cnt = nullptr;
@@ -1386,13 +1536,17 @@ int fmm_tc_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *st
                const FmmParams &prm, int form, const double *seed, uint32_t *status,
                cudaStream_t st) {
   if (prm.dmax2 < INFINITY) return fmm_run(s, t, a, strengths, prm, seed, status, st);
+  TcDev *dp = tc_dev(s);
+  if (!dp) return -1;
+  TcDev &d = *dp;
+  if (!d.ev[0])
+    for (cudaEvent_t &e : d.ev) cudaEventCreate(&e);
+  cudaEventRecord(d.ev[0], st);
   FmmPrep pr;
   const int pre = fmm_prepare(s, t, a, strengths, prm.alpha, pr, st);
   if (pre == 2) return 1;
   if (pre <= 0) return pre;
-  TcDev *dp = tc_dev(s);
-  if (!dp) return -1;
-  TcDev &d = *dp;
+  cudaEventRecord(d.ev[1], st);
   uint32_t p = 8;
   if (prm.order >= 1 && prm.order <= (double)(TC_MAXQ - 1)) p = (uint32_t)prm.order;
   double kappa = prm.opening;
@@ -1447,7 +1601,12 @@ int fmm_tc_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *st
     g.pool = d.pool;
     g.pool_cap = d.pool_cap;
     if (cudaMemsetAsync(d.info, 0, 8 * 4, st) != cudaSuccess) return -1;
-    if (coop((const void *)k_tc_lists, d.coop_lists, 0, g, st)) return -1;
+    for (uint32_t lev = 0; lev < pr.nlev; ++lev) {
+      const uint32_t c0 = pr.lvl[lev], c1 = pr.lvl[lev + 1];
+      if (c1 > c0)
+        D3_LAUNCH(k_tc_lists, blocks_for((size_t)(c1 - c0) * 32, TC_THREADS), TC_THREADS, 0, st)(
+            g, c0, c1);
+    }
     if (cudaMemcpyAsync(d.h_info, d.info, TI_WORDS * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)
       return -1;
@@ -1459,6 +1618,7 @@ int fmm_tc_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *st
     if ((d.h_info[TI_OVF] & 2) || attempt > 6) return -1;  // a walk's stack overflowed
     need = 2 * (size_t)(used > need ? used : need);
   }
+  cudaEventRecord(d.ev[2], st);
   uint32_t tiles = 0;
   for (uint32_t q4 = 0; q4 < 4; ++q4) tiles += (d.h_info[TI_GROUP + q4] + TC_TILE - 1) / TC_TILE;
   if (tc_order_pass(d, g, *main, tiles, learned, st)) return -1;

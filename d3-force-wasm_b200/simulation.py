@@ -875,12 +875,13 @@ class Simulation:
             self.ctx.precision = None
         return self
 
-    def learned(self, params, tolerance=1e-5, samples=64, hold=0):
+    def learned(self, params, tolerance=1e-5, samples=64, hold=16):
         """Installs the learned form's network (5,122 floats, learned.py) with
-        its sampled check: each tick the order-4 + network kick is compared
-        with an FP64 direct sum on `samples` nodes, and when the RMS exceeds
-        `tolerance` the tick runs the plain form instead (and the next `hold`
-        ticks too). No counterpart in the reference."""
+        its sampled check: each checked tick the order-4 + network kick is
+        compared with an FP64 direct sum on `samples` nodes, and when the RMS
+        exceeds `tolerance` the tick runs the plain form instead, and so do
+        the next `hold` ticks before the network is checked again. No
+        counterpart in the reference."""
         import numpy as np
         p = np.ascontiguousarray(params, np.float32)
         C.check(self.ctx.core.sim_set_learned(self.ctx.h, p.ctypes.data, len(p), float(tolerance),

@@ -1164,10 +1164,10 @@ double sim_stat(uint32_t h, uint32_t which) {
   if (which >= 50 && which < 50 + TC_STATS) {
     // the fast many-body precision forms: 50 learned-form checks, 51 of them
     // that fell back, 52 the last check's sampled RMS, 53 cells of the last
-    // run; its last pass: 54 M2L ms, 55 P2P ms, 56 M2L tiles, 57 M2L pairs,
+    // run; its last pass: 54 M2L ms, 55 near-field ms, 56 M2L tiles, 57 M2L pairs,
     // 58 P2P point pairs, 59 M2P and 60 P2L point-cell pairs, 61 q; the last
     // run's ms: 62 prepare, 63 geometry and lists, 64 upward, 65 P2L,
-    // 66 downward, 67 leaves, 68 the whole run
+    // 66 downward, 67 the learned form's network, 68 the whole run
     double out[TC_STATS];
     fmm_tc_stats(s->fast, out);
     return out[which - 50];

@@ -125,7 +125,6 @@ struct TcDev {
   uint32_t *loff = nullptr;         // per cell: offsets/counts of p2p, w, x, coarse lists
   uint32_t *pool = nullptr;
   size_t pool_cap = 0, last_pool = 0;
-  float2 *far = nullptr;            // per sorted point
   uint32_t *info = nullptr, *h_info = nullptr;
   int sms = 0;
   uint32_t *arrive = nullptr;        // per cell: children finished (upward pass)
@@ -158,7 +157,6 @@ struct TcArgs {
   float *lco;
   uint32_t *near, *m2l, *groups, *loff, *pool;
   size_t pool_cap;
-  float2 *far;
   float *feat, *mlp_x, *mlp_y;
   uint32_t *leaves;
   double2 *kick;  // non-null: the many-body kick goes here instead of into vx, vy
@@ -473,6 +471,7 @@ __device__ bool tc_candidate(const TcArgs &a, uint32_t c, const TcCell &A, uint3
   return true;
 }
 
+
 __device__ __forceinline__ uint32_t warp_excl_sum(uint32_t v, uint32_t &total) {
   const unsigned lane = threadIdx.x & 31;
   uint32_t incl = v;
@@ -482,6 +481,138 @@ __device__ __forceinline__ uint32_t warp_excl_sum(uint32_t v, uint32_t &total) {
   }
   total = __shfl_sync(0xffffffffu, incl, 31);
   return incl - v;
+}
+
+// One candidate's pool event, found once: its kind (0 none, 1 P2P leaf,
+// 2 W cell, 3 X leaf, 4 coarse leaf passed down, 5 a walk of the subtree of
+// `id`) and cell. The M2L table and near list entries are written here.
+struct Cand {
+  uint32_t kind, id;
+};
+
+__device__ Cand tc_eval(const TcArgs &a, uint32_t c, const TcCell &A, uint32_t u) {
+  const uint32_t nn = a.tab->nnear;
+  const bool leaf = A.nchild == 0;
+  uint32_t coarse = TC_NONE;
+  if (u < 4 * nn) {
+    const uint32_t o = u >> 2, b = u & 3;
+    const uint32_t pb = __ldcg(&a.near[(size_t)A.parent * nn + o]);
+    if (pb == TC_NONE) return {0, 0};
+    const TcCell PB = a.cells[pb];
+    if (PB.nchild == 0) {
+      if (b != 0) return {0, 0};
+      coarse = pb;
+    } else {
+      const uint32_t B = child_at(PB, b);
+      if (B == TC_NONE) return {0, 0};
+      const uint32_t e16 = a.tab->map[A.quad][o][b];
+      if (!(e16 & TC_NEAR_FLAG)) {
+        a.m2l[(size_t)c * a.tab->sstride + e16] = B;
+        return {0, 0};
+      }
+      a.near[(size_t)c * nn + (e16 & 0xFF)] = B;
+      if (!leaf) return {0, 0};
+      return {a.cells[B].nchild == 0 ? 1u : 5u, B};
+    }
+  } else {
+    const uint32_t k = u - 4 * nn;
+    coarse = __ldcg(&a.pool[__ldcg(&a.loff[(size_t)A.parent * 8 + 6]) + k]);
+  }
+  const TcCell L = a.cells[coarse];
+  if (separated(a, A, L)) return {3, coarse};
+  return {leaf ? 1u : 4u, coarse};
+}
+
+// The events of an evaluated candidate: counted into e, or (WRITE) written
+// from the offsets o4 (p2p, w, x, coarse) plus e's counts so far.
+template <bool WRITE>
+__device__ __forceinline__ bool cand_events(const TcArgs &a, const TcCell &A, Cand cd, Ev &e,
+                                            const uint32_t *o4) {
+  switch (cd.kind) {
+    case 1:
+      if (WRITE) a.pool[o4[0] + e.np] = cd.id;
+      ++e.np;
+      return true;
+    case 2:
+      if (WRITE) a.pool[o4[1] + e.nw] = cd.id;
+      ++e.nw;
+      return true;
+    case 3:
+      if (WRITE) a.pool[o4[2] + e.nx] = cd.id;
+      ++e.nx;
+      return true;
+    case 4:
+      if (WRITE) a.pool[o4[3] + e.nc] = cd.id;
+      ++e.nc;
+      return true;
+    case 5:
+      return tc_walk<WRITE>(a, A, cd.id, e, o4[0], o4[1]);
+    default:
+      return true;
+  }
+}
+
+// The lists of cell c (not the root) when its candidates fit LIST_KEEP
+// rounds of the warp: each candidate is evaluated once, its event and the
+// per-kind offsets kept in registers between the count and the write.
+constexpr uint32_t LIST_KEEP = 4;
+
+__device__ void tc_list_cell_kept(const TcArgs &a, uint32_t c, const TcCell &A, uint32_t ncand) {
+  const unsigned lane = threadIdx.x & 31;
+  Cand kept[LIST_KEEP];
+  uint32_t off[LIST_KEEP][4];
+  Ev tot{0, 0, 0, 0};
+  bool ok = true;
+#pragma unroll
+  for (uint32_t r = 0; r < LIST_KEEP; ++r) {
+    const uint32_t u = r * 32 + lane;
+    Cand cd{0, 0};
+    Ev e{0, 0, 0, 0};
+    if (r * 32 < ncand) {
+      if (u < ncand) {
+        cd = tc_eval(a, c, A, u);
+        const uint32_t z4[4] = {0, 0, 0, 0};
+        if (!cand_events<false>(a, A, cd, e, z4)) ok = false;
+      }
+      uint32_t t;
+      off[r][0] = tot.np + warp_excl_sum(e.np, t); tot.np += t;
+      off[r][1] = tot.nw + warp_excl_sum(e.nw, t); tot.nw += t;
+      off[r][2] = tot.nx + warp_excl_sum(e.nx, t); tot.nx += t;
+      off[r][3] = tot.nc + warp_excl_sum(e.nc, t); tot.nc += t;
+    }
+    kept[r] = cd;
+  }
+  ok = __all_sync(0xffffffffu, ok);
+  uint32_t base = 0;
+  const uint32_t all = tot.np + tot.nw + tot.nx + tot.nc;
+  if (lane == 0) base = atomicAdd(&a.info[TI_POOL_P2P], all);
+  base = __shfl_sync(0xffffffffu, base, 0);
+  const uint32_t o4[4] = {base, base + tot.np, base + tot.np + tot.nw,
+                          base + tot.np + tot.nw + tot.nx};
+  uint32_t *lo = a.loff + (size_t)c * 8;
+  if (!ok || (size_t)base + all > a.pool_cap) {
+    if (lane == 0) {
+      atomicOr(&a.info[TI_OVF], ok ? 1u : 2u);
+      lo[0] = lo[2] = lo[4] = lo[6] = 0;
+      lo[1] = lo[3] = lo[5] = lo[7] = 0;
+    }
+    return;
+  }
+  if (lane == 0) {
+    lo[0] = o4[0]; lo[1] = tot.np;
+    lo[2] = o4[1]; lo[3] = tot.nw;
+    lo[4] = o4[2]; lo[5] = tot.nx;
+    lo[6] = o4[3]; lo[7] = tot.nc;
+  }
+#pragma unroll
+  for (uint32_t r = 0; r < LIST_KEEP; ++r) {
+    if (kept[r].kind) {
+      const uint32_t w4[4] = {o4[0] + off[r][0], o4[1] + off[r][1], o4[2] + off[r][2],
+                              o4[3] + off[r][3]};
+      Ev w{0, 0, 0, 0};
+      cand_events<true>(a, A, kept[r], w, w4);
+    }
+  }
 }
 
 // loff[c * 8 + ...]: 0 p2p off, 1 p2p cnt, 2 w off, 3 w cnt, 4 x off, 5 x cnt,
@@ -515,7 +646,11 @@ __device__ void tc_list_cell(const TcArgs &a, uint32_t c) {
   __syncwarp();
   const uint32_t ncoarse = __ldcg(&a.loff[(size_t)A.parent * 8 + 7]);
   const uint32_t ncand = 4 * nn + ncoarse;
-  // counts
+  if (ncand <= 32 * LIST_KEEP) {
+    tc_list_cell_kept(a, c, A, ncand);
+    return;
+  }
+  // more candidates than the lanes keep: count, then evaluate again to write
   Ev tot{0, 0, 0, 0};
   bool ok = true;
   const uint32_t zero4[4] = {0, 0, 0, 0};
@@ -582,6 +717,8 @@ __global__ void __launch_bounds__(TC_THREADS) k_tc_lists(TcArgs a, uint32_t c0, 
 // M2L CTA: 256 gathering threads (two per target row: the bf16 hi and the lo
 // half of the row) and one warp whose first lane only issues the MMAs.
 constexpr uint32_t M2L_STAGES = 3;
+constexpr uint32_t M2L_AHEAD = 2;  // slots of copies in flight per gathering thread
+static_assert(M2L_AHEAD <= M2L_STAGES, "a stage is landed before it is reused");
 constexpr uint32_t M2L_PRODUCERS = 2 * TC_TILE;
 constexpr uint32_t M2L_THREADS = M2L_PRODUCERS + 32;
 
@@ -640,44 +777,45 @@ __global__ void __launch_bounds__(M2L_THREADS) k_tc_m2l(TcArgs a) {
     auto source = [&](uint32_t j) -> uint32_t {
       return (my != TC_NONE && j < nslot) ? __ldcg(&a.m2l[(size_t)my * sstride + j]) : TC_NONE;
     };
-    auto rows = [&](uint32_t src, uint4 *v) {
-      if (src != TC_NONE) {
-        const uint4 *m = reinterpret_cast<const uint4 *>(a.mbf + (size_t)src * 64) + h * 4;
+    // the copies of slot j into stage s: this thread's 4 chunks of the row
+    // (zeros when the slot has no source) and 16 bytes of the operator
+    const uint32_t a_dst = tc::smem_addr(S.a[0][h]), b_dst = tc::smem_addr(S.b[0][0]) + t * 16;
+    auto copy = [&](uint32_t j, uint32_t s, uint32_t src) {
+      const char *m = reinterpret_cast<const char *>(a.mbf) +
+                      (src != TC_NONE ? (size_t)src * 128 + h * 64 : 0);
+      const uint32_t bytes = src != TC_NONE ? 16u : 0u;
 #pragma unroll
-        for (int c = 0; c < 4; ++c) v[c] = __ldcg(m + c);
-      } else {
-#pragma unroll
-        for (int c = 0; c < 4; ++c) v[c] = make_uint4(0, 0, 0, 0);
-      }
+      for (uint32_t c = 0; c < 4; ++c)
+        tc::cp_async16(a_dst + s * sizeof(S.a[0]) + tc::tile_offset(r, c, TC_TILE), m + c * 16,
+                       bytes);
+      const char *w = reinterpret_cast<const char *>(a.wops) +
+                      (size_t)a.tab->slot_class[g][j] * 4096 + t * 16;
+      tc::cp_async16(b_dst + s * sizeof(S.b[0]), w, 16u);
+      tc::cp_async_commit();
     };
-    auto oper = [&](uint32_t j) -> uint4 {  // this thread's 16 bytes of slot j's operator
-      if (j >= nslot) return make_uint4(0, 0, 0, 0);
-      const uint4 *w = reinterpret_cast<const uint4 *>(a.wops + (size_t)a.tab->slot_class[g][j] * 4096);
-      return __ldg(w + t);
+    // slot j's stage is full once this thread's copies of it have landed:
+    // wait for them, make them visible to the tensor core, arrive
+    auto land = [&](uint32_t j, bool all) {
+      if (all) tc::cp_async_wait<0>();
+      else tc::cp_async_wait<M2L_AHEAD - 1>();
+      tc::fence_proxy_async();
+      tc::mbar_arrive(&S.full[j % M2L_STAGES]);
     };
-    // one slot of lookahead for the rows and the operator, two for the table
-    uint32_t src1 = source(1), src2;
-    uint4 cur[4], nxt[4];
-    rows(source(0), cur);
-    uint4 bcur = oper(0), bnxt;
+    uint32_t src = source(0), landed = 0;
     for (uint32_t j = 0; j < nslot; ++j) {
       const uint32_t s = j % M2L_STAGES, use = j / M2L_STAGES;
-      src2 = source(j + 2);
-      rows(j + 1 < nslot ? src1 : TC_NONE, nxt);
-      bnxt = oper(j + 1);
+      const uint32_t next = source(j + 1);
       // the stage is free once the MMAs that read it (slot j - STAGES) are done
       if (use > 0 && !tc::mbar_wait(&S.empty[s], (use - 1) & 1, abort, TC_WAIT_NS)) break;
-#pragma unroll
-      for (int c = 0; c < 4; ++c)
-        *reinterpret_cast<uint4 *>(&S.a[s][h][tc::tile_offset(r, c, TC_TILE)]) = cur[c];
-      *reinterpret_cast<uint4 *>(&S.b[s][t >> 7][(t & 127) * 16]) = bcur;
-      tc::fence_proxy_async();
-      tc::mbar_arrive(&S.full[s]);
-#pragma unroll
-      for (int c = 0; c < 4; ++c) cur[c] = nxt[c];
-      bcur = bnxt;
-      src1 = src2;
+      copy(j, s, src);
+      if (j + 1 >= M2L_AHEAD) land(landed++, false);
+      src = next;
     }
+    // the slots still in flight (also after a wait that gave up: every copy
+    // lands before the CTA can exit)
+    tc::cp_async_wait<0>();
+    if (!*abort)
+      while (landed < nslot) land(landed++, true);
   } else if (t == M2L_PRODUCERS) {
     const uint32_t idesc = tc::idesc_bf16_f32(TC_TILE, TC_KN);
     const uint32_t alb = (TC_TILE / 8) * 128, blb = (TC_KN / 8) * 128;
@@ -744,11 +882,32 @@ __global__ void __launch_bounds__(M2L_THREADS) k_tc_m2l(TcArgs a) {
 
 // ---- P2L (coarse leaves into local expansions, FP32) ------------------------------------------
 
+// The source leaf and point of batch index idx: the leaves' counts are held
+// one per lane (running count `incl`, `before` it, first point `first`, ne
+// lanes in use); returns the point.
+__device__ __forceinline__ uint32_t batch_point(uint32_t idx, uint32_t ne, uint32_t incl,
+                                                uint32_t before, uint32_t first) {
+  uint32_t j = 0;
+#pragma unroll
+  for (uint32_t step = 16; step; step >>= 1) {
+    const uint32_t v = __shfl_sync(0xffffffffu, incl, j + step - 1);
+    if (j + step - 1 < ne && v <= idx) j += step;
+  }
+  const uint32_t f = __shfl_sync(0xffffffffu, first, j & 31);
+  const uint32_t b0 = __shfl_sync(0xffffffffu, before, j & 31);
+  return f + (idx - b0);
+}
+
+// A warp per cell with an X list (coarse leaves seen from it): the points of
+// the listed leaves spread over the lanes; each lane adds its points' terms
+//     L'_l += (-1)^l s_j / z^(l+1),   z = (c_A - u_j) / s_A,
+// (z from an FP64 difference, the series in FP32), then the lanes' sums are
+// reduced and added to the cell's row. Q = q.
+template <int Q>
 __global__ void __launch_bounds__(TC_THREADS) k_tc_p2l(TcArgs a) {
   const unsigned lane = threadIdx.x & 31;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  const uint32_t q = a.q;
   for (uint32_t c = gw; c < a.ncells; c += nwarps) {
     const uint32_t nx = a.loff[(size_t)c * 8 + 5];
     if (!nx) continue;
@@ -757,34 +916,58 @@ __global__ void __launch_bounds__(TC_THREADS) k_tc_p2l(TcArgs a) {
     double ax, ay;
     cell_centre(A, ax, ay);
     const double inv_s = ldexp(1.0, (int)A.level);
-    // lane l < q accumulates L'_l over every point of every listed leaf
-    float sr = 0, si = 0;
-    for (uint32_t e = 0; e < nx; ++e) {
-      const TcCell L = a.cells[a.pool[ox + e]];
-      for (uint32_t k = L.first; k < L.first + L.count; ++k) {
-        const double sv = a.ps[k];
-        // z = (c_A - u_j) / s_A; term (-1)^l s_j / z^(l+1)
-        const double zr = (ax - a.ux[k]) * inv_s, zi = (ay - a.uy[k]) * inv_s;
-        const double d2 = zr * zr + zi * zi;
-        const float ir = (float)(zr / d2), ii = (float)(-zi / d2);  // 1 / z
-        float pr = ir, pi = ii;
-        for (uint32_t l = 0; l < lane && l < q; ++l) {
+    float sr[Q], si[Q];
+#pragma unroll
+    for (int l = 0; l < Q; ++l) sr[l] = si[l] = 0.f;
+    for (uint32_t eb = 0; eb < nx; eb += 32) {
+      const uint32_t ne = min(32u, nx - eb);
+      uint32_t first = 0, cnt = 0;
+      if (lane < ne) {
+        const TcCell L = a.cells[a.pool[ox + eb + lane]];
+        first = L.first;
+        cnt = L.count;
+      }
+      uint32_t total;
+      const uint32_t before = warp_excl_sum(cnt, total);
+      const uint32_t incl = before + cnt;
+      for (uint32_t i0 = 0; i0 < total; i0 += 32) {
+        const uint32_t idx = i0 + lane;
+        const uint32_t k = batch_point(idx, ne, incl, before, first);
+        if (idx >= total) continue;
+        const float sv = (float)__ldg(&a.ps[k]);
+        const float zr = (float)((ax - __ldg(&a.ux[k])) * inv_s);
+        const float zi = (float)((ay - __ldg(&a.uy[k])) * inv_s);
+        const float d2 = zr * zr + zi * zi;
+        const float ir = __fdividef(zr, d2), ii = -__fdividef(zi, d2);  // 1 / z
+        float pr = sv * ir, pi = sv * ii;
+#pragma unroll
+        for (int l = 0; l < Q; ++l) {
+          if (l & 1) {
+            sr[l] -= pr;
+            si[l] -= pi;
+          } else {
+            sr[l] += pr;
+            si[l] += pi;
+          }
           const float nr = pr * ir - pi * ii;
           pi = pr * ii + pi * ir;
           pr = nr;
         }
-        if (lane < q) {
-          const float sg = (lane & 1) ? -1.f : 1.f;
-          sr += sg * (float)sv * pr;
-          si += sg * (float)sv * pi;
-        }
       }
     }
-    if (lane < q) {
-      float *Lc = a.lco + (size_t)c * TC_KN;
-      Lc[lane] += sr;
-      Lc[q + lane] += si;
-    }
+#pragma unroll
+    for (int l = 0; l < Q; ++l)
+      for (int o = 16; o > 0; o >>= 1) {
+        sr[l] += __shfl_xor_sync(0xffffffffu, sr[l], o);
+        si[l] += __shfl_xor_sync(0xffffffffu, si[l], o);
+      }
+    float *Lc = a.lco + (size_t)c * TC_KN;
+#pragma unroll
+    for (int l = 0; l < Q; ++l)
+      if (lane == (unsigned)l) {
+        Lc[l] += sr[l];
+        Lc[Q + l] += si[l];
+      }
   }
 }
 
@@ -863,6 +1046,33 @@ __global__ void __launch_bounds__(TC_THREADS) k_tc_down(TcArgs a) {
     }
 }
 
+template <int Q>
+void launch_p2l_q(const TcArgs &g, unsigned blocks, cudaStream_t st) {
+  D3_LAUNCH(k_tc_p2l<Q>, blocks, TC_THREADS, 0, st)(g);
+}
+
+void launch_p2l(const TcArgs &g, cudaStream_t st) {
+  const unsigned blocks = blocks_for((size_t)g.ncells * 32, TC_THREADS);
+  if (!blocks) return;
+  switch (g.q) {
+    case 2: launch_p2l_q<2>(g, blocks, st); break;
+    case 3: launch_p2l_q<3>(g, blocks, st); break;
+    case 4: launch_p2l_q<4>(g, blocks, st); break;
+    case 5: launch_p2l_q<5>(g, blocks, st); break;
+    case 6: launch_p2l_q<6>(g, blocks, st); break;
+    case 7: launch_p2l_q<7>(g, blocks, st); break;
+    case 8: launch_p2l_q<8>(g, blocks, st); break;
+    case 9: launch_p2l_q<9>(g, blocks, st); break;
+    case 10: launch_p2l_q<10>(g, blocks, st); break;
+    case 11: launch_p2l_q<11>(g, blocks, st); break;
+    case 12: launch_p2l_q<12>(g, blocks, st); break;
+    case 13: launch_p2l_q<13>(g, blocks, st); break;
+    case 14: launch_p2l_q<14>(g, blocks, st); break;
+    case 15: launch_p2l_q<15>(g, blocks, st); break;
+    default: launch_p2l_q<16>(g, blocks, st); break;
+  }
+}
+
 void launch_down(const TcArgs &g, uint32_t nleaf, cudaStream_t st) {
   const unsigned blocks = blocks_for(nleaf, TC_THREADS);
   if (!blocks) return;
@@ -932,82 +1142,13 @@ __global__ void k_tc_pack(TcArgs a) {
   for (int j = 0; j < 12; ++j) a.mlp_x[(size_t)k * 12 + j] = row[j];
 }
 
-__global__ void __launch_bounds__(TC_THREADS) k_tc_leaf(TcArgs a, int corrected) {
-  const unsigned lane = threadIdx.x & 31;
-  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  const uint32_t q = a.q;
-  const uint32_t nleaf = __ldcg(&a.info[TI_LEAVES]);
-  for (uint32_t e0 = gw; e0 < nleaf; e0 += nwarps) {
-    const uint32_t c = a.leaves[e0];
-    const TcCell C = a.cells[c];
-    const float *L = a.lco + (size_t)c * TC_KN;
-    float l0r = L[0], l0i = L[q];
-    if (corrected) {
-      // L'_0 += sc * network output / TARGET_SCALE
-      const float sc = a.feat[(size_t)c * 16 + 14];
-      l0r += sc * a.mlp_y[(size_t)e0 * 2] * (1.f / LEARN_TARGET_SCALE);
-      l0i += sc * a.mlp_y[(size_t)e0 * 2 + 1] * (1.f / LEARN_TARGET_SCALE);
-    }
-    double cx, cy;
-    cell_centre(C, cx, cy);
-    const double inv_s = ldexp(1.0, (int)C.level);
-    const uint32_t nw = a.loff[(size_t)c * 8 + 3], ow = a.loff[(size_t)c * 8 + 2];
-    float mx = 0, my = 0;  // the points' offsets from the centre, for the feature row
-    for (uint32_t k = C.first + lane; k < C.first + C.count; k += 32) {
-      const float wr = (float)((a.ux[k] - cx) * inv_s), wi = (float)((a.uy[k] - cy) * inv_s);
-      mx += wr;
-      my += wi;
-      float ar = q > 1 ? L[q - 1] : l0r, ai = q > 1 ? L[2 * q - 1] : l0i;
-      for (int l = (int)q - 2; l >= 0; --l) {
-        const float lr = l ? L[l] : l0r, li = l ? L[q + l] : l0i;
-        const float nr = ar * wr - ai * wi + lr;
-        ai = ar * wi + ai * wr + li;
-        ar = nr;
-      }
-      double gr = (double)ar * inv_s, gi = (double)ai * inv_s;  // phi = (1/s) sum L'_l w^l
-      for (uint32_t e = 0; e < nw; ++e) {
-        const uint32_t cc = a.pool[ow + e];
-        const TcCell W = a.cells[cc];
-        double wx, wy;
-        cell_centre(W, wx, wy);
-        const double winv = ldexp(1.0, (int)W.level);
-        // g = (1/s_W) sum_k M'_k / z^(k+1), z = (u - c_W) / s_W
-        const double zr = (a.ux[k] - wx) * winv, zi = (a.uy[k] - wy) * winv;
-        const double d2 = zr * zr + zi * zi;
-        const double ir = zr / d2, ii = -zi / d2;
-        const double *mc = a.mco + (size_t)cc * 2 * q;
-        double pr = ir, pi = ii, sr = 0, si = 0;
-        for (uint32_t kk = 0; kk < q; ++kk) {
-          const double mr = mc[kk], mi = mc[q + kk];
-          sr += mr * pr - mi * pi;
-          si += mr * pi + mi * pr;
-          const double nr = pr * ir - pi * ii;
-          pi = pr * ii + pi * ir;
-          pr = nr;
-        }
-        gr += sr * winv;
-        gi += si * winv;
-      }
-      a.far[k] = make_float2((float)(-gr * a.inv_w), (float)(gi * a.inv_w));
-    }
-    if (!corrected) {  // the leaf's feature row (k_tc_features writes it for the network)
-      for (int o = 16; o > 0; o >>= 1) {
-        mx += __shfl_xor_sync(0xffffffffu, mx, o);
-        my += __shfl_xor_sync(0xffffffffu, my, o);
-      }
-      if (lane == 0) feature_row(a, c, C, L, mx, my);
-    }
-  }
-}
-
 // ---- P2P (FP32 with an FP64 origin shift) ----------------------------------------------------------
 
 constexpr uint32_t P2P_STAGE = 256;  // staged source points per warp
 
 // One point pair of the near field (d3's pair formula, the distanceMin clamp
 // and the hashed jiggle of hash.zig for exact zero deltas; the self pair adds
-// nothing).
+// nothing). The careful form, for batches that hold a coincident pair.
 __device__ __forceinline__ void tc_pair(const float4 sv, float xi, float yi, uint32_t ti, uint32_t gi,
                                         float dmin2, uint64_t seed, const uint32_t *perm, float &ax,
                                         float &ay) {
@@ -1032,29 +1173,116 @@ __device__ __forceinline__ void tc_pair(const float4 sv, float xi, float yi, uin
   ay += dy * w;
 }
 
-// A warp per leaf (grid-stride over the leaf list). The leaf's targets take a
-// lane each; a leaf of at most 16 (8) points splits the warp into 2 (4) lane
-// groups that hold the same targets and take alternate sources, their sums
-// added at the end in a fixed order. The source leaves' points are staged in
-// shared memory, relative to the target leaf's first point (the shift taken
-// in FP64): up to 32 source leaves at a time, their points spread over the
-// lanes so every load of a batch is in flight at once.
-__global__ void __launch_bounds__(TC_THREADS) k_tc_p2p(TcArgs a) {
+// The same pair without the jiggle: the self pair (zero deltas) adds 0 * w
+// with w kept finite, and `bad` notes a coincident pair of distinct points
+// (the batch is then redone with tc_pair). A single zero delta keeps its
+// zero here, where d3 would jiggle it by ~1e-6: the change to the kick is
+// ~1e-6 of that one pair's term.
+__device__ __forceinline__ void tc_pair_fast(const float4 sv, float xi, float yi, uint32_t ti,
+                                             float dmin2, float &ax, float &ay, bool &bad) {
+  const float dx = sv.x - xi, dy = sv.y - yi;
+  float l = dx * dx + dy * dy;
+  bad |= (l == 0.f) & (__float_as_uint(sv.w) != ti);
+  if (l < dmin2) l = sqrtf(dmin2 * l);
+  const float w = __fdividef(sv.z, fmaxf(l, 1e-30f));
+  ax += dx * w;
+  ay += dy * w;
+}
+
+// The far field at target point k of leaf C: L2P of the leaf's final local
+// expansion (Lsh: 2q floats, L'_0 possibly corrected) by Horner in FP32 (the
+// L2P of downwardCell, fmm.zig:851-886),
+//     phi = (1/s) sum_l L'_l w^l,   w = (u - c) / s,
+// and M2P from each cell of the leaf's W list (FP64; the adaptive list has
+// no reference counterpart),
+//     phi += (1/s_W) sum_k M'_k / z^(k+1),   z = (u - c_W) / s_W.
+// Returns the kick's far part in world units; (wr, wi) = w for the feature row.
+__device__ __forceinline__ float2 tc_far(const TcArgs &a, uint32_t k, double cx, double cy,
+                                         double inv_s, const float *Lsh, uint32_t nw, uint32_t ow,
+                                         float &wr, float &wi) {
+  const uint32_t q = a.q;
+  const double ux = a.ux[k], uy = a.uy[k];
+  wr = (float)((ux - cx) * inv_s);
+  wi = (float)((uy - cy) * inv_s);
+  float ar = Lsh[q - 1], ai = Lsh[2 * q - 1];
+  for (int l = (int)q - 2; l >= 0; --l) {
+    const float nr = ar * wr - ai * wi + Lsh[l];
+    ai = ar * wi + ai * wr + Lsh[q + l];
+    ar = nr;
+  }
+  double gr = (double)ar * inv_s, gi = (double)ai * inv_s;
+  for (uint32_t e = 0; e < nw; ++e) {
+    const uint32_t cc = a.pool[ow + e];
+    const TcCell W = a.cells[cc];
+    double wx, wy;
+    cell_centre(W, wx, wy);
+    const double winv = ldexp(1.0, (int)W.level);
+    const double zr = (ux - wx) * winv, zi = (uy - wy) * winv;
+    const double d2 = zr * zr + zi * zi;
+    const double ir = zr / d2, ii = -zi / d2;
+    const double *mc = a.mco + (size_t)cc * 2 * q;
+    double pr = ir, pi = ii, sr = 0, si = 0;
+    for (uint32_t kk = 0; kk < q; ++kk) {
+      const double mr = mc[kk], mi = mc[q + kk];
+      sr += mr * pr - mi * pi;
+      si += mr * pi + mi * pr;
+      const double nr = pr * ir - pi * ii;
+      pi = pr * ii + pi * ir;
+      pr = nr;
+    }
+    gr += sr * winv;
+    gi += si * winv;
+  }
+  return make_float2((float)(-gr * a.inv_w), (float)(gi * a.inv_w));
+}
+
+// A warp per leaf (grid-stride over the leaf list): the near field, the far
+// field and the kick of the leaf's points.
+// Near: the leaf's targets take a lane each; a leaf of at most 16 (8) points
+// splits the warp into 2 (4) lane groups that hold the same targets and take
+// alternate sources, their sums added at the end in a fixed order. The
+// source leaves' points are staged in shared memory relative to the target
+// leaf's first point (the shift in FP64): up to 32 source leaves at a time,
+// their points spread over the lanes so every load of a batch is in flight
+// at once.
+// Far: tc_far for each target (group 0's lanes), with the leaf's local
+// expansion in shared memory; `corrected` adds the learned form's network
+// output to L'_0 (sc * y / LEARN_TARGET_SCALE), else the leaf's feature row
+// is written. v += near + far in FP64 (or the kick to `kick`).
+__global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int corrected) {
   __shared__ float4 stage[TC_WARPS][P2P_STAGE];
+  __shared__ float lsh[TC_WARPS][TC_KN];
   const unsigned lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const uint64_t seed = (uint64_t)__double_as_longlong(*a.seed);
   const float dmin2 = a.dmin2f;
+  const uint32_t q = a.q;
   const uint32_t nleaf = __ldcg(&a.info[TI_LEAVES]);
   float4 *sg = stage[wl];
+  float *Lsh = lsh[wl];
   for (uint32_t e0 = gw; e0 < nleaf; e0 += nwarps) {
     const uint32_t c = a.leaves[e0];
     const TcCell A = a.cells[c];
     const uint32_t np = a.loff[(size_t)c * 8 + 1], op = a.loff[(size_t)c * 8];
+    const uint32_t nw = a.loff[(size_t)c * 8 + 3], ow = a.loff[(size_t)c * 8 + 2];
     const uint32_t G = A.count <= 8 ? 4u : A.count <= 16 ? 2u : 1u, W = 32u / G;
     const uint32_t grp = lane / W, gl = lane % W;
     const double ox = a.px[A.first], oy = a.py[A.first];
+    double cx, cy;
+    cell_centre(A, cx, cy);
+    const double inv_s = ldexp(1.0, (int)A.level);
+    __syncwarp();
+    {
+      const float *L = a.lco + (size_t)c * TC_KN;
+      float v = lane < 2 * q ? L[lane] : 0.f;
+      if (corrected && (lane == 0 || lane == q)) {
+        const float sc = a.feat[(size_t)c * 16 + 14];
+        v += sc * a.mlp_y[(size_t)e0 * 2 + (lane ? 1 : 0)] * (1.f / LEARN_TARGET_SCALE);
+      }
+      Lsh[lane] = v;
+    }
+    float mx = 0, my = 0;  // the points' offsets from the centre (feature row)
     for (uint32_t tb = A.first; tb < A.first + A.count; tb += W) {
       const uint32_t ti = tb + gl;
       const bool act = ti < A.first + A.count;
@@ -1080,30 +1308,31 @@ __global__ void __launch_bounds__(TC_THREADS) k_tc_p2p(TcArgs a) {
 #pragma unroll
           for (uint32_t r = 0; r < P2P_STAGE / 32; ++r) {
             const uint32_t idx = base + r * 32 + lane;
-            // the source leaf holding point idx of the batch: the number of
-            // leaves whose running count ends at or before idx
-            uint32_t j = 0;
-#pragma unroll
-            for (uint32_t step = 16; step; step >>= 1) {
-              const uint32_t v = __shfl_sync(0xffffffffu, incl, j + step - 1);
-              if (j + step - 1 < ne && v <= idx) j += step;
-            }
-            const uint32_t f = __shfl_sync(0xffffffffu, first, j & 31);
-            const uint32_t b0 = __shfl_sync(0xffffffffu, before, j & 31);
-            if (idx < base + kn) {
-              const uint32_t sj = f + (idx - b0);
+            const uint32_t sj = batch_point(idx, ne, incl, before, first);
+            if (idx < base + kn)
               sg[r * 32 + lane] = make_float4((float)(__ldg(&a.px[sj]) - ox),
                                               (float)(__ldg(&a.py[sj]) - oy),
                                               (float)__ldg(&a.ps[sj]), __uint_as_float(sj));
-            }
           }
           __syncwarp();
+          const float sx0 = ax0, sy0 = ay0, sx1 = ax1, sy1 = ay1;
+          bool bad = false;
           uint32_t k = grp;
+#pragma unroll 2
           for (; k + G < kn; k += 2 * G) {
-            tc_pair(sg[k], xi, yi, ti, gi, dmin2, seed, a.perm, ax0, ay0);
-            tc_pair(sg[k + G], xi, yi, ti, gi, dmin2, seed, a.perm, ax1, ay1);
+            tc_pair_fast(sg[k], xi, yi, ti, dmin2, ax0, ay0, bad);
+            tc_pair_fast(sg[k + G], xi, yi, ti, dmin2, ax1, ay1, bad);
           }
-          if (k < kn) tc_pair(sg[k], xi, yi, ti, gi, dmin2, seed, a.perm, ax0, ay0);
+          if (k < kn) tc_pair_fast(sg[k], xi, yi, ti, dmin2, ax0, ay0, bad);
+          if (__any_sync(0xffffffffu, bad && act)) {
+            // a coincident pair in this batch: redo it with the jiggle
+            ax0 = sx0, ay0 = sy0, ax1 = sx1, ay1 = sy1;
+            for (k = grp; k + G < kn; k += 2 * G) {
+              tc_pair(sg[k], xi, yi, ti, gi, dmin2, seed, a.perm, ax0, ay0);
+              tc_pair(sg[k + G], xi, yi, ti, gi, dmin2, seed, a.perm, ax1, ay1);
+            }
+            if (k < kn) tc_pair(sg[k], xi, yi, ti, gi, dmin2, seed, a.perm, ax0, ay0);
+          }
         }
       }
       __syncwarp();
@@ -1113,7 +1342,10 @@ __global__ void __launch_bounds__(TC_THREADS) k_tc_p2p(TcArgs a) {
         vy += __shfl_xor_sync(0xffffffffu, vy, o);
       }
       if (act && grp == 0) {
-        const float2 f = a.far[ti];
+        float wr, wi;
+        const float2 f = tc_far(a, ti, cx, cy, inv_s, Lsh, nw, ow, wr, wi);
+        mx += wr;
+        my += wi;
         const double kx = (double)vx + (double)f.x, ky = (double)vy + (double)f.y;
         if (a.kick) {
           a.kick[ti] = make_double2(kx, ky);
@@ -1122,6 +1354,13 @@ __global__ void __launch_bounds__(TC_THREADS) k_tc_p2p(TcArgs a) {
           a.vy[gi] = a.vy[gi] + ky;
         }
       }
+    }
+    if (!corrected) {
+      for (int o = 16; o > 0; o >>= 1) {
+        mx += __shfl_xor_sync(0xffffffffu, mx, o);
+        my += __shfl_xor_sync(0xffffffffu, my, o);
+      }
+      if (lane == 0) feature_row(a, c, A, a.lco + (size_t)c * TC_KN, mx, my);
     }
   }
 }
@@ -1368,9 +1607,7 @@ int reserve(TcDev &d, uint32_t ncells, uint32_t m) {
   }
   if (m > d.pcap) {
     const uint32_t cap = m + m / 4 + 1024;
-    cudaFree(d.far);
     cudaFree(d.kick);
-    D3_CUDA_OK(cudaMalloc(&d.far, (size_t)cap * sizeof(float2)));
     D3_CUDA_OK(cudaMalloc(&d.kick, (size_t)cap * sizeof(double2)));
     d.pcap = cap;
   }
@@ -1441,8 +1678,7 @@ int tc_order_pass(TcDev &d, TcArgs &g, const TcTabSet &ts, uint32_t tiles, bool 
   d.last_tiles = tiles;
   if (!d.last_args) d.last_args = new TcArgs;
   *static_cast<TcArgs *>(d.last_args) = g;
-  const unsigned wblocks = blocks_for((size_t)g.ncells * 32, TC_THREADS);
-  D3_LAUNCH(k_tc_p2l, wblocks, TC_THREADS, 0, st)(g);
+  launch_p2l(g, st);
   cudaEventRecord(d.ev[5], st);
   launch_down(g, nleaf, st);
   cudaEventRecord(d.ev[6], st);
@@ -1451,9 +1687,8 @@ int tc_order_pass(TcDev &d, TcArgs &g, const TcTabSet &ts, uint32_t tiles, bool 
     D3_LAUNCH(k_tc_pack, blocks_for(nleaf, 256), 256, 0, st)(g);
     if (mlp_infer_tc(d.mlp_x, nleaf, d.mlp, d.mlp_y, g.status, st)) return -1;
   }
-  D3_LAUNCH(k_tc_leaf, lw, TC_THREADS, 0, st)(g, learned ? 1 : 0);
   cudaEventRecord(d.ev[7], st);
-  D3_LAUNCH(k_tc_p2p, lw, TC_THREADS, 0, st)(g);
+  D3_LAUNCH(k_tc_near, lw, TC_THREADS, 0, st)(g, learned ? 1 : 0);
   cudaEventRecord(d.ev[8], st);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
@@ -1470,7 +1705,7 @@ void fmm_tc_free(FastScratch &s) {
   cudaFree(d->cells); cudaFree(d->mco); cudaFree(d->mbf);
   cudaFree(d->lco); cudaFree(d->near); cudaFree(d->m2l); cudaFree(d->groups); cudaFree(d->loff);
   cudaFree(d->arrive);
-  cudaFree(d->pool); cudaFree(d->far); cudaFree(d->info); cudaFreeHost(d->h_info);
+  cudaFree(d->pool); cudaFree(d->info); cudaFreeHost(d->h_info);
   cudaFree(d->feat); cudaFree(d->leaves); cudaFree(d->mlp_x); cudaFree(d->mlp_y);
   cudaFree(d->kick); cudaFree(d->chk); cudaFreeHost(d->h_chk); cudaFree(d->mlp);
   for (cudaEvent_t e : d->ev)
@@ -1574,7 +1809,6 @@ int fmm_tc_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *st
   g.cells = d.cells;
   g.mco = d.mco; g.mbf = d.mbf; g.lco = d.lco;
   g.near = d.near; g.m2l = d.m2l; g.groups = d.groups; g.loff = d.loff;
-  g.far = d.far;
   g.feat = d.feat; g.leaves = d.leaves; g.mlp_x = d.mlp_x; g.mlp_y = d.mlp_y;
   g.kick = learned ? d.kick : nullptr;
   g.vx = a.vx; g.vy = a.vy;

@@ -79,6 +79,9 @@ struct DSim {
   cudaEvent_t ev_upstart = nullptr, ev_rest = nullptr;
   bool rest_pending = false;
   bool settle_after_accumulate = false;  // sim_tick: settle in the first many-body force
+  // sim_tick: a many-body force of the tick runs a precision form judged by
+  // RMS (not bit-exact), so the center's sums may take the tree order
+  bool relaxed_center = false;
   uint32_t sync_mode = D3_SYNC_PER_CALL;
   bool fixed_from_f = false;  // sim_set_fixed_source
   // tree mirrors (tree_info)
@@ -507,6 +510,7 @@ int run_force(DSim *s, DForce *f, double alpha, bool presummed = false, bool fus
     case D3_CENTER: {
       cudaEvent_t e = phase_begin(s);
       if (presummed) cudaStreamWaitEvent(s->stream, s->ev_sumdone, 0);
+      else if (s->relaxed_center) center_sum_tree(a, s->scratch, s->stream);
       else center_sum(a, s->scratch, status_word(s), s->stream);
       if (!fuse_center)
         center_apply(a, f->scalars[D3_CX], f->scalars[D3_CY], f->scalars[D3_STRENGTH], s->scratch,
@@ -1004,6 +1008,11 @@ int32_t tick_impl(DSim *s, uint32_t ticks, double *alpha, double alpha_target, d
   // until its traversal: the rest of the node state may still be uploading.
   s->settle_after_accumulate = !fs.empty() && fs[0]->kind == D3_MANY_BODY && !s->host_random &&
                                !fast_mode(s, fs[0]);
+  s->relaxed_center = false;
+  for (const DForce *f : fs)
+    if (f->kind == D3_MANY_BODY && fast_mode(s, f) &&
+        (f->scalars[D3_PRECISION] == 2 || f->scalars[D3_PRECISION] == 3))
+      s->relaxed_center = true;
   if (!s->settle_after_accumulate) settle(s);
   // The first center force's sums only read positions, which no force
   // before it changes: run them on the side stream from the tick's start.
@@ -1026,7 +1035,8 @@ int32_t tick_impl(DSim *s, uint32_t ticks, double *alpha, double alpha_target, d
         e = pool_event(s);
         cudaEventRecord(e, s->side);
       }
-      center_sum(nodes_of(s), s->scratch, status_word(s), s->side);
+      if (s->relaxed_center) center_sum_tree(nodes_of(s), s->scratch, s->side);
+      else center_sum(nodes_of(s), s->scratch, status_word(s), s->side);
       if (e) {
         cudaEvent_t b = pool_event(s);
         cudaEventRecord(b, s->side);
@@ -1042,6 +1052,7 @@ int32_t tick_impl(DSim *s, uint32_t ticks, double *alpha, double alpha_target, d
       if (r < 0) {
         settle(s);
         s->settle_after_accumulate = false;
+        s->relaxed_center = false;
         return r;
       }
     }
@@ -1057,6 +1068,7 @@ int32_t tick_impl(DSim *s, uint32_t ticks, double *alpha, double alpha_target, d
     phase_end(s, PH_INTEGRATE, e);
   }
   s->settle_after_accumulate = false;
+  s->relaxed_center = false;
   cudaEventRecord(s->ev1, s->stream);
   s->last_enqueue_ms =
       std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - host0).count();

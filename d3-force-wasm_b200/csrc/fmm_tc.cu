@@ -1173,20 +1173,22 @@ __device__ __forceinline__ void tc_pair(const float4 sv, float xi, float yi, uin
   ay += dy * w;
 }
 
-// The same pair without the jiggle: the self pair (zero deltas) adds 0 * w
-// with w kept finite, and `bad` notes a coincident pair of distinct points
-// (the batch is then redone with tc_pair). A single zero delta keeps its
-// zero here, where d3 would jiggle it by ~1e-6: the change to the kick is
-// ~1e-6 of that one pair's term.
-__device__ __forceinline__ void tc_pair_fast(const float4 sv, float xi, float yi, uint32_t ti,
-                                             float dmin2, float &ax, float &ay, bool &bad) {
+// The same pair without the jiggle. w = s / l, or s / sqrt(dmin2 l) inside
+// distanceMin, is taken as s * rsqrt(y) with y = l^2 or dmin2 l (one MUFU op),
+// y kept above zero so the self pair adds 0 * w. Zero distances are counted
+// in zc: more than the lane's own self pair means a coincident pair of
+// distinct points, and the batch is redone with tc_pair. A single zero
+// delta keeps its zero here, where d3 would jiggle it by ~1e-6: the change
+// to the kick is ~1e-6 of that one pair's term.
+__device__ __forceinline__ void tc_pair_fast(const float4 sv, float xi, float yi, float dmin2,
+                                             float &ax, float &ay, uint32_t &zc) {
   const float dx = sv.x - xi, dy = sv.y - yi;
-  float l = dx * dx + dy * dy;
-  bad |= (l == 0.f) & (__float_as_uint(sv.w) != ti);
-  if (l < dmin2) l = sqrtf(dmin2 * l);
-  const float w = __fdividef(sv.z, fmaxf(l, 1e-30f));
-  ax += dx * w;
-  ay += dy * w;
+  const float l = fmaf(dx, dx, dy * dy);
+  zc += l == 0.f ? 1u : 0u;
+  const float y = fmaxf(l < dmin2 ? dmin2 * l : l * l, 1e-37f);
+  const float w = sv.z * rsqrtf(y);
+  ax = fmaf(dx, w, ax);
+  ay = fmaf(dy, w, ay);
 }
 
 // The far field at target point k of leaf C: L2P of the leaf's final local
@@ -1252,6 +1254,7 @@ __device__ __forceinline__ float2 tc_far(const TcArgs &a, uint32_t k, double cx,
 __global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int corrected) {
   __shared__ float4 stage[TC_WARPS][P2P_STAGE];
   __shared__ float lsh[TC_WARPS][TC_KN];
+  __shared__ uint32_t selfpos[TC_WARPS][32];  // per target lane: its own point's batch index
   const unsigned lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -1305,26 +1308,32 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int correct
         for (uint32_t base = 0; base < total; base += P2P_STAGE) {
           const uint32_t kn = min(P2P_STAGE, total - base);
           __syncwarp();
+          selfpos[wl][lane] = TC_NONE;
+          __syncwarp();
 #pragma unroll
           for (uint32_t r = 0; r < P2P_STAGE / 32; ++r) {
             const uint32_t idx = base + r * 32 + lane;
             const uint32_t sj = batch_point(idx, ne, incl, before, first);
-            if (idx < base + kn)
+            if (idx < base + kn) {
               sg[r * 32 + lane] = make_float4((float)(__ldg(&a.px[sj]) - ox),
                                               (float)(__ldg(&a.py[sj]) - oy),
                                               (float)__ldg(&a.ps[sj]), __uint_as_float(sj));
+              if (sj - tb < W) selfpos[wl][sj - tb] = r * 32 + lane;  // a target of this round
+            }
           }
           __syncwarp();
           const float sx0 = ax0, sy0 = ay0, sx1 = ax1, sy1 = ay1;
-          bool bad = false;
+          uint32_t zc = 0;
           uint32_t k = grp;
 #pragma unroll 2
           for (; k + G < kn; k += 2 * G) {
-            tc_pair_fast(sg[k], xi, yi, ti, dmin2, ax0, ay0, bad);
-            tc_pair_fast(sg[k + G], xi, yi, ti, dmin2, ax1, ay1, bad);
+            tc_pair_fast(sg[k], xi, yi, dmin2, ax0, ay0, zc);
+            tc_pair_fast(sg[k + G], xi, yi, dmin2, ax1, ay1, zc);
           }
-          if (k < kn) tc_pair_fast(sg[k], xi, yi, ti, dmin2, ax0, ay0, bad);
-          if (__any_sync(0xffffffffu, bad && act)) {
+          if (k < kn) tc_pair_fast(sg[k], xi, yi, dmin2, ax0, ay0, zc);
+          const uint32_t sp = selfpos[wl][gl];
+          const uint32_t self = (sp != TC_NONE && sp % G == grp) ? 1u : 0u;
+          if (__any_sync(0xffffffffu, act && zc > self)) {
             // a coincident pair in this batch: redo it with the jiggle
             ax0 = sx0, ay0 = sy0, ax1 = sx1, ay1 = sy1;
             for (k = grp; k + G < kn; k += 2 * G) {

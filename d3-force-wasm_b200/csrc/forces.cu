@@ -1470,6 +1470,47 @@ void center_sum(const NodeArrays &a, ForceScratch &s, uint32_t *status, cudaStre
   if (!attr || cudaGetLastError() != cudaSuccess) set_status(status, ST_CENTER_RECORDS, st);
 }
 
+// One block: s.center = the sums of the chunk sums in chunk order (a fixed
+// tree: lane-strided partials, then a shuffle tree).
+__global__ void __launch_bounds__(1024) k_csum_tree(const double *part, uint32_t nc, double *out) {
+  __shared__ double wx[32], wy[32];
+  double ax = 0, ay = 0;
+  for (uint32_t c = threadIdx.x; c < nc; c += blockDim.x) {
+    ax += part[c];
+    ay += part[nc + c];
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    ax += __shfl_xor_sync(0xffffffffu, ax, o);
+    ay += __shfl_xor_sync(0xffffffffu, ay, o);
+  }
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    wx[warp] = ax;
+    wy[warp] = ay;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const unsigned nw = blockDim.x >> 5;
+    ax = lane < nw ? wx[lane] : 0.0;
+    ay = lane < nw ? wy[lane] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) {
+      ax += __shfl_xor_sync(0xffffffffu, ax, o);
+      ay += __shfl_xor_sync(0xffffffffu, ay, o);
+    }
+    if (lane == 0) {
+      out[0] = ax;
+      out[1] = ay;
+    }
+  }
+}
+
+void center_sum_tree(const NodeArrays &a, ForceScratch &s, cudaStream_t st) {
+  if (a.n == 0) return;
+  const CsumGeom g = csum_geom(a.n);
+  D3_LAUNCH(k_csum_part, blocks_for((size_t)g.nc * 32, 256), 256, 0, st)(a.x, a.y, a.n, g, s.csum_part);
+  D3_LAUNCH(k_csum_tree, 1, 1024, 0, st)(s.csum_part, g.nc, s.center);
+}
+
 void center_apply(const NodeArrays &a, double cx, double cy, double strength, ForceScratch &s,
                   cudaStream_t st) {
   if (a.n == 0) return;

@@ -137,6 +137,9 @@ int collide_parallel(TreeDev &t, const NodeArrays &a, const double *radii, doubl
 // into s.center, then the shift. The sums only read positions, so the caller
 // may issue them early on another stream.
 void center_sum(const NodeArrays &a, ForceScratch &s, uint32_t *status, cudaStream_t st);
+// The same sums in a fixed tree order (chunk sums, then a reduction): for the
+// fast many-body forms judged by RMS, where the tick is not bit-exact anyway.
+void center_sum_tree(const NodeArrays &a, ForceScratch &s, cudaStream_t st);
 // src/core.js:130: the fixed bits from fx / fy (NaN = not set).
 void fixed_from_f(const double *fx, const double *fy, uint8_t *fixed, uint32_t n, cudaStream_t st);
 // simulation.js:157-178: the closest node below radius^2 (r2) into *out.

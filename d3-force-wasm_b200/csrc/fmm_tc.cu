@@ -483,45 +483,11 @@ __device__ __forceinline__ uint32_t warp_excl_sum(uint32_t v, uint32_t &total) {
   return incl - v;
 }
 
-// One candidate's pool event, found once: its kind (0 none, 1 P2P leaf,
-// 2 W cell, 3 X leaf, 4 coarse leaf passed down, 5 a walk of the subtree of
-// `id`) and cell. The M2L table and near list entries are written here.
+// One candidate's pool event: its kind (0 none, 1 P2P leaf, 2 W cell, 3 X
+// leaf, 4 coarse leaf passed down, 5 a walk of the subtree of `id`) and cell.
 struct Cand {
   uint32_t kind, id;
 };
-
-__device__ Cand tc_eval(const TcArgs &a, uint32_t c, const TcCell &A, uint32_t u) {
-  const uint32_t nn = a.tab->nnear;
-  const bool leaf = A.nchild == 0;
-  uint32_t coarse = TC_NONE;
-  if (u < 4 * nn) {
-    const uint32_t o = u >> 2, b = u & 3;
-    const uint32_t pb = __ldcg(&a.near[(size_t)A.parent * nn + o]);
-    if (pb == TC_NONE) return {0, 0};
-    const TcCell PB = a.cells[pb];
-    if (PB.nchild == 0) {
-      if (b != 0) return {0, 0};
-      coarse = pb;
-    } else {
-      const uint32_t B = child_at(PB, b);
-      if (B == TC_NONE) return {0, 0};
-      const uint32_t e16 = a.tab->map[A.quad][o][b];
-      if (!(e16 & TC_NEAR_FLAG)) {
-        a.m2l[(size_t)c * a.tab->sstride + e16] = B;
-        return {0, 0};
-      }
-      a.near[(size_t)c * nn + (e16 & 0xFF)] = B;
-      if (!leaf) return {0, 0};
-      return {a.cells[B].nchild == 0 ? 1u : 5u, B};
-    }
-  } else {
-    const uint32_t k = u - 4 * nn;
-    coarse = __ldcg(&a.pool[__ldcg(&a.loff[(size_t)A.parent * 8 + 6]) + k]);
-  }
-  const TcCell L = a.cells[coarse];
-  if (separated(a, A, L)) return {3, coarse};
-  return {leaf ? 1u : 4u, coarse};
-}
 
 // The events of an evaluated candidate: counted into e, or (WRITE) written
 // from the offsets o4 (p2p, w, x, coarse) plus e's counts so far.
@@ -559,28 +525,71 @@ constexpr uint32_t LIST_KEEP = 4;
 
 __device__ void tc_list_cell_kept(const TcArgs &a, uint32_t c, const TcCell &A, uint32_t ncand) {
   const unsigned lane = threadIdx.x & 31;
+  const uint32_t nn = a.tab->nnear;
+  const bool leaf = A.nchild == 0;
+  // the candidates' loads by dependency level, all rounds at once: the
+  // parent's near cell or coarse leaf, its cell, then (a leaf's near cell)
+  // the near cell's child
+  const uint32_t coff = ncand > 4 * nn ? __ldcg(&a.loff[(size_t)A.parent * 8 + 6]) : 0;
+  uint32_t id[LIST_KEEP];
+#pragma unroll
+  for (uint32_t r = 0; r < LIST_KEEP; ++r) {
+    const uint32_t u = r * 32 + lane;
+    id[r] = TC_NONE;
+    if (u < ncand)
+      id[r] = u < 4 * nn ? __ldcg(&a.near[(size_t)A.parent * nn + (u >> 2)])
+                         : __ldcg(&a.pool[coff + u - 4 * nn]);
+  }
+  TcCell P[LIST_KEEP];
+#pragma unroll
+  for (uint32_t r = 0; r < LIST_KEEP; ++r)
+    if (id[r] != TC_NONE) P[r] = a.cells[id[r]];
   Cand kept[LIST_KEEP];
+  uint32_t child[LIST_KEEP];
+#pragma unroll
+  for (uint32_t r = 0; r < LIST_KEEP; ++r) {
+    const uint32_t u = r * 32 + lane;
+    kept[r] = {0, 0};
+    child[r] = TC_NONE;
+    if (id[r] == TC_NONE) continue;
+    bool coarse = u >= 4 * nn;
+    if (!coarse) {
+      const uint32_t o = u >> 2, b = u & 3;
+      if (P[r].nchild == 0) {
+        if (b != 0) continue;
+        coarse = true;  // a near leaf of the parent: seen from A as a coarse leaf
+      } else {
+        const uint32_t B = child_at(P[r], b);
+        if (B == TC_NONE) continue;
+        const uint32_t e16 = a.tab->map[A.quad][o][b];
+        if (!(e16 & TC_NEAR_FLAG)) {
+          a.m2l[(size_t)c * a.tab->sstride + e16] = B;
+          continue;
+        }
+        a.near[(size_t)c * nn + (e16 & 0xFF)] = B;
+        if (leaf) child[r] = B;
+        continue;
+      }
+    }
+    if (coarse) kept[r] = {separated(a, A, P[r]) ? 3u : leaf ? 1u : 4u, id[r]};
+  }
+#pragma unroll
+  for (uint32_t r = 0; r < LIST_KEEP; ++r)
+    if (child[r] != TC_NONE) kept[r] = {a.cells[child[r]].nchild == 0 ? 1u : 5u, child[r]};
   uint32_t off[LIST_KEEP][4];
   Ev tot{0, 0, 0, 0};
   bool ok = true;
 #pragma unroll
   for (uint32_t r = 0; r < LIST_KEEP; ++r) {
-    const uint32_t u = r * 32 + lane;
-    Cand cd{0, 0};
+    if (r * 32 >= ncand) break;
     Ev e{0, 0, 0, 0};
-    if (r * 32 < ncand) {
-      if (u < ncand) {
-        cd = tc_eval(a, c, A, u);
-        const uint32_t z4[4] = {0, 0, 0, 0};
-        if (!cand_events<false>(a, A, cd, e, z4)) ok = false;
-      }
-      uint32_t t;
-      off[r][0] = tot.np + warp_excl_sum(e.np, t); tot.np += t;
-      off[r][1] = tot.nw + warp_excl_sum(e.nw, t); tot.nw += t;
-      off[r][2] = tot.nx + warp_excl_sum(e.nx, t); tot.nx += t;
-      off[r][3] = tot.nc + warp_excl_sum(e.nc, t); tot.nc += t;
-    }
-    kept[r] = cd;
+    const uint32_t z4[4] = {0, 0, 0, 0};
+    if (!cand_events<false>(a, A, kept[r], e, z4)) ok = false;
+    uint32_t t;
+    off[r][0] = tot.np + warp_excl_sum(e.np, t); tot.np += t;
+    off[r][1] = tot.nw + warp_excl_sum(e.nw, t); tot.nw += t;
+    off[r][2] = tot.nx + warp_excl_sum(e.nx, t); tot.nx += t;
+    off[r][3] = tot.nc + warp_excl_sum(e.nc, t); tot.nc += t;
   }
   ok = __all_sync(0xffffffffu, ok);
   uint32_t base = 0;
@@ -1174,19 +1183,20 @@ __device__ __forceinline__ void tc_pair(const float4 sv, float xi, float yi, uin
 }
 
 // The same pair without the jiggle. w = s / l, or s / sqrt(dmin2 l) inside
-// distanceMin, is taken as s * rsqrt(y) with y = l^2 or dmin2 l (one MUFU op),
-// y kept above zero so the self pair adds 0 * w. Zero distances are counted
-// in zc: more than the lane's own self pair means a coincident pair of
-// distinct points, and the batch is redone with tc_pair. A single zero
-// delta keeps its zero here, where d3 would jiggle it by ~1e-6: the change
-// to the kick is ~1e-6 of that one pair's term.
+// distanceMin, is s * rsqrt(y) with y = l max(l, dmin2) (one MUFU op); l is
+// floored at 1e-18 there (distances under 1e-9, below FP32's resolution of
+// the leaf-local coordinates) so the self pair adds 0 * w with w finite.
+// Zero distances are counted in zc: more than the lane's own self pair means
+// a coincident pair of distinct points, and the batch is redone with
+// tc_pair. A single zero delta keeps its zero here, where d3 would jiggle it
+// by ~1e-6: the change to the kick is ~1e-6 of that one pair's term.
 __device__ __forceinline__ void tc_pair_fast(const float4 sv, float xi, float yi, float dmin2,
                                              float &ax, float &ay, uint32_t &zc) {
   const float dx = sv.x - xi, dy = sv.y - yi;
   const float l = fmaf(dx, dx, dy * dy);
   zc += l == 0.f ? 1u : 0u;
-  const float y = fmaxf(l < dmin2 ? dmin2 * l : l * l, 1e-37f);
-  const float w = sv.z * rsqrtf(y);
+  const float lf = fmaxf(l, 1e-18f);
+  const float w = sv.z * rsqrtf(lf * fmaxf(lf, dmin2));
   ax = fmaf(dx, w, ax);
   ay = fmaf(dy, w, ay);
 }
@@ -1240,9 +1250,9 @@ __device__ __forceinline__ float2 tc_far(const TcArgs &a, uint32_t k, double cx,
 
 // A warp per leaf (grid-stride over the leaf list): the near field, the far
 // field and the kick of the leaf's points.
-// Near: the leaf's targets take a lane each; a leaf of at most 16 (8) points
-// splits the warp into 2 (4) lane groups that hold the same targets and take
-// alternate sources, their sums added at the end in a fixed order. The
+// Near: the leaf's targets take a lane each; a leaf of W <= 16 points splits
+// the warp into 32 / W lane groups that hold the same targets and take
+// alternate sources, their sums added at the end in group order. The
 // source leaves' points are staged in shared memory relative to the target
 // leaf's first point (the shift in FP64): up to 32 source leaves at a time,
 // their points spread over the lanes so every load of a batch is in flight
@@ -1255,6 +1265,7 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int correct
   __shared__ float4 stage[TC_WARPS][P2P_STAGE];
   __shared__ float lsh[TC_WARPS][TC_KN];
   __shared__ uint32_t selfpos[TC_WARPS][32];  // per target lane: its own point's batch index
+  __shared__ float2 red[TC_WARPS][32];
   const unsigned lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -1269,8 +1280,10 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int correct
     const TcCell A = a.cells[c];
     const uint32_t np = a.loff[(size_t)c * 8 + 1], op = a.loff[(size_t)c * 8];
     const uint32_t nw = a.loff[(size_t)c * 8 + 3], ow = a.loff[(size_t)c * 8 + 2];
-    const uint32_t G = A.count <= 8 ? 4u : A.count <= 16 ? 2u : 1u, W = 32u / G;
+    // lane groups: W targets each, G = 32 / W groups (lanes past G W idle)
+    const uint32_t W = A.count <= 16 ? A.count : 32u, G = 32u / W;
     const uint32_t grp = lane / W, gl = lane % W;
+    const bool in = grp < G;
     const double ox = a.px[A.first], oy = a.py[A.first];
     double cx, cy;
     cell_centre(A, cx, cy);
@@ -1288,7 +1301,7 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int correct
     float mx = 0, my = 0;  // the points' offsets from the centre (feature row)
     for (uint32_t tb = A.first; tb < A.first + A.count; tb += W) {
       const uint32_t ti = tb + gl;
-      const bool act = ti < A.first + A.count;
+      const bool act = in && ti < A.first + A.count;
       const float xi = act ? (float)(a.px[ti] - ox) : 0.f, yi = act ? (float)(a.py[ti] - oy) : 0.f;
       const uint32_t gi = act ? a.perm[ti] : 0;
       float ax0 = 0, ay0 = 0, ax1 = 0, ay1 = 0;
@@ -1324,7 +1337,7 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int correct
           __syncwarp();
           const float sx0 = ax0, sy0 = ay0, sx1 = ax1, sy1 = ay1;
           uint32_t zc = 0;
-          uint32_t k = grp;
+          uint32_t k = in ? grp : kn;
 #pragma unroll 2
           for (; k + G < kn; k += 2 * G) {
             tc_pair_fast(sg[k], xi, yi, dmin2, ax0, ay0, zc);
@@ -1336,7 +1349,7 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int correct
           if (__any_sync(0xffffffffu, act && zc > self)) {
             // a coincident pair in this batch: redo it with the jiggle
             ax0 = sx0, ay0 = sy0, ax1 = sx1, ay1 = sy1;
-            for (k = grp; k + G < kn; k += 2 * G) {
+            for (k = in ? grp : kn; k + G < kn; k += 2 * G) {
               tc_pair(sg[k], xi, yi, ti, gi, dmin2, seed, a.perm, ax0, ay0);
               tc_pair(sg[k + G], xi, yi, ti, gi, dmin2, seed, a.perm, ax1, ay1);
             }
@@ -1344,12 +1357,17 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int correct
           }
         }
       }
+      // the groups' sums, in group order
       __syncwarp();
-      float vx = ax0 + ax1, vy = ay0 + ay1;
-      for (uint32_t o = W; o < 32; o <<= 1) {  // the groups' sums, in a fixed order
-        vx += __shfl_xor_sync(0xffffffffu, vx, o);
-        vy += __shfl_xor_sync(0xffffffffu, vy, o);
-      }
+      red[wl][lane] = make_float2(ax0 + ax1, ay0 + ay1);
+      __syncwarp();
+      float vx = 0, vy = 0;
+      if (grp == 0)
+        for (uint32_t g2 = 0; g2 < G; ++g2) {
+          const float2 v = red[wl][g2 * W + gl];
+          vx += v.x;
+          vy += v.y;
+        }
       if (act && grp == 0) {
         float wr, wi;
         const float2 f = tc_far(a, ti, cx, cy, inv_s, Lsh, nw, ow, wr, wi);

@@ -110,7 +110,12 @@ __global__ void k_shift2(const double *x, const double *y, const double *vx, con
   py[i] = y[i] + vy[i];
 }
 
-// link_fast.zig:60-99
+// link_fast.zig:60-99. A thread per node over its adjacency, four links at a
+// time: the loads of the four are issued by dependency level (entries, then
+// the other endpoints and the link's scalars, then their positions), and
+// the four are then applied in adjacency order, as the serial loop does.
+constexpr uint32_t LINK_BATCH = 4;
+
 __global__ void k_link_sweep(const double *px, const double *py, double *vxs, double *vys,
                              LinkArrays l, const uint32_t *row, const uint32_t *adj, double alpha,
                              const double *seedp, uint32_t n) {
@@ -119,26 +124,49 @@ __global__ void k_link_sweep(const double *px, const double *py, double *vxs, do
   const uint64_t seed = seed_bits(seedp);
   double vx = vxs[i], vy = vys[i];
   const double pxi = px[i], pyi = py[i];
-  for (uint32_t a = row[i]; a < row[i + 1]; ++a) {
-    const uint32_t entry = adj[a];
-    const uint32_t e = entry & ~TARGET_BIT;
-    const bool is_target = (entry & TARGET_BIT) != 0;
-    const uint32_t j = is_target ? l.source[e] : l.target[e];
-    double x = is_target ? pxi - px[j] : px[j] - pxi;
-    double y = is_target ? pyi - py[j] : py[j] - pyi;
-    if (x == 0 || x != x) x = hash_jiggle(seed, e, 0, 0);
-    if (y == 0 || y != y) y = hash_jiggle(seed, e, 0, 1);
-    double len = sqrt(x * x + y * y);
-    len = (len - l.distance[e]) / len * alpha * l.strength[e];
-    x *= len;
-    y *= len;
-    const double b = l.bias[e];
-    if (is_target) {
-      vx -= x * b;
-      vy -= y * b;
-    } else {
-      vx += x * (1 - b);
-      vy += y * (1 - b);
+  const uint32_t a1 = row[i + 1];
+  for (uint32_t a0 = row[i]; a0 < a1; a0 += LINK_BATCH) {
+    uint32_t ent[LINK_BATCH], oth[LINK_BATCH];
+    double dist[LINK_BATCH], str[LINK_BATCH], bias[LINK_BATCH], xj[LINK_BATCH], yj[LINK_BATCH];
+#pragma unroll
+    for (uint32_t k = 0; k < LINK_BATCH; ++k)
+      if (a0 + k < a1) ent[k] = adj[a0 + k];
+#pragma unroll
+    for (uint32_t k = 0; k < LINK_BATCH; ++k)
+      if (a0 + k < a1) {
+        const uint32_t e = ent[k] & ~TARGET_BIT;
+        oth[k] = (ent[k] & TARGET_BIT) ? l.source[e] : l.target[e];
+        dist[k] = l.distance[e];
+        str[k] = l.strength[e];
+        bias[k] = l.bias[e];
+      }
+#pragma unroll
+    for (uint32_t k = 0; k < LINK_BATCH; ++k)
+      if (a0 + k < a1) {
+        xj[k] = px[oth[k]];
+        yj[k] = py[oth[k]];
+      }
+#pragma unroll
+    for (uint32_t k = 0; k < LINK_BATCH; ++k) {
+      if (a0 + k >= a1) break;
+      const uint32_t e = ent[k] & ~TARGET_BIT;
+      const bool is_target = (ent[k] & TARGET_BIT) != 0;
+      double x = is_target ? pxi - xj[k] : xj[k] - pxi;
+      double y = is_target ? pyi - yj[k] : yj[k] - pyi;
+      if (x == 0 || x != x) x = hash_jiggle(seed, e, 0, 0);
+      if (y == 0 || y != y) y = hash_jiggle(seed, e, 0, 1);
+      double len = sqrt(x * x + y * y);
+      len = (len - dist[k]) / len * alpha * str[k];
+      x *= len;
+      y *= len;
+      const double b = bias[k];
+      if (is_target) {
+        vx -= x * b;
+        vy -= y * b;
+      } else {
+        vx += x * (1 - b);
+        vy += y * (1 - b);
+      }
     }
   }
   vxs[i] = vx;

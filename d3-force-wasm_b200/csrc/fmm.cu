@@ -59,7 +59,9 @@ struct FmmTables {
 // (FI_LIST_OVERFLOW + level parity: a level's overflow is read at the start of
 // the next level, while that level writes the other word.)
 enum : uint32_t { FI_CELLS = 0, FI_OVERFLOW, FI_LEVELS, FI_POOL_M2L, FI_POOL_P2P, FI_POOL_FWD,
-                  FI_LIST_OVERFLOW, FI_LVL = 8 };  // FI_LVL + d: first cell of level d
+                  FI_LIST_OVERFLOW, FI_LVL = 8,  // FI_LVL + d: first cell of level d
+                  FI_M = 40,                     // points to act on (0 when the extent is bad)
+                  FI_BAD = 41 };                 // 1: the extent is not finite and positive
 
 struct FmmDev {
   uint32_t pcap = 0, ccap = 0;
@@ -76,7 +78,8 @@ struct FmmDev {
   uint32_t *info = nullptr, *bsum = nullptr;
   double *square = nullptr;      // box x0, y0, side
   uint32_t *h_info = nullptr;    // pinned mirror of info
-  double *h_geom = nullptr;      // pinned: square[3], extent[4]
+  double *h_geom = nullptr;      // pinned: the geometry read back (w, 1 / w, ox, oy)
+  double *geom = nullptr;        // device: w, 1 / w, ox, oy (k_fmm_geom)
   int coop_blocks = 0;
   size_t last_m2l = 0, last_p2p = 0, last_fwd = 0;  // list sizes of the previous run
   // the cell build: per-block counts per level, each cell's start and level
@@ -143,12 +146,32 @@ __global__ void k_fmm_keys(const double *xs, const double *ys, uint32_t n, const
 }
 
 // fmm.zig:668-682
+// The run's geometry from the square's extent (tree.zig:287-309): geom =
+// {w, 1 / w, ox, oy}; FI_M = the finite points, or 0 with FI_BAD = 1 when
+// there are some but the extent is not finite and positive (the exact kernel
+// runs instead). The
+// same IEEE f64 operations the host would do, so the values are the same.
+__global__ void k_fmm_geom(const double *extent, const uint32_t *tinfo, double *geom,
+                           uint32_t *info) {
+  const double e0 = extent[0], e1 = extent[1], e2 = extent[2], e3 = extent[3];
+  const double w = e2 - e0;
+  const bool ok = w > 0 && w < INFINITY;
+  geom[0] = w;
+  geom[1] = 1 / w;
+  geom[2] = (e0 + e2) / 2;
+  geom[3] = (e1 + e3) / 2;
+  const uint32_t m = tinfo[0];
+  info[FI_M] = ok ? m : 0;
+  info[FI_BAD] = m > 0 && !ok ? 1 : 0;
+}
+
 __global__ void k_fmm_gather(const uint32_t *perm, const double *xs, const double *ys,
-                             const double *strength, uint32_t m, double alpha, double ox, double oy,
-                             double inv_w, double *px, double *py, double *ps, double *ux,
+                             const double *strength, const uint32_t *info, double alpha,
+                             const double *geom, double *px, double *py, double *ps, double *ux,
                              double *uy) {
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= m) return;
+  if (j >= info[FI_M]) return;
+  const double inv_w = geom[1], ox = geom[2], oy = geom[3];
   const uint32_t i = perm[j];
   const double x = xs[i], y = ys[i];
   px[j] = x;
@@ -218,6 +241,23 @@ __device__ inline uint32_t key_lower(const uint64_t *keys, uint32_t lo, uint32_t
   return lo;
 }
 
+// The same first index for a run known to hold k - 1 (keys[k - 1] >= t):
+// galloping back from k - 1, then a binary search of the last stride, so a
+// short run costs a few loads.
+__device__ inline uint32_t key_lower_back(const uint64_t *keys, uint32_t k, uint64_t t) {
+  uint32_t hi = k - 1;  // keys[hi] >= t
+  uint32_t lo = 0;
+  for (uint32_t step = 1; step <= hi; step <<= 1) {
+    const uint32_t probe = hi - step;
+    if ((uint64_t)(uint32_t)keys[probe] < t) {
+      lo = probe + 1;
+      break;
+    }
+    hi = probe;
+  }
+  return key_lower(keys, lo, hi, t);
+}
+
 // The levels at which point k starts cells: [d0, d1] (empty when d1 < d0).
 __device__ void cell_levels(const uint64_t *keys, uint32_t m, uint32_t k, int &d0, int &d1) {
   const uint32_t key = (uint32_t)keys[k];
@@ -228,7 +268,7 @@ __device__ void cell_levels(const uint64_t *keys, uint32_t m, uint32_t k, int &d
   if (k > 0) {
     // the level-lcp run around k must hold more than FMM_LEAF points
     const uint64_t t = lcp ? (uint64_t)(key >> (32 - 2 * lcp)) << (32 - 2 * lcp) : 0;
-    const uint32_t s0 = key_lower(keys, 0, k, t);
+    const uint32_t s0 = key_lower_back(keys, k, t);
     if (s0 + FMM_LEAF >= m) return;
     if (shared_digits((uint32_t)keys[s0], (uint32_t)keys[s0 + FMM_LEAF]) < lcp) return;
   }
@@ -237,8 +277,9 @@ __device__ void cell_levels(const uint64_t *keys, uint32_t m, uint32_t k, int &d
   d1 = top < (int)FMM_LEVELS ? top : (int)FMM_LEVELS;
 }
 
-__global__ void __launch_bounds__(CB_THREADS) k_cells_count(const uint64_t *keys, uint32_t m,
-                                                            uint32_t *bcount) {
+__global__ void __launch_bounds__(CB_THREADS) k_cells_count(const uint64_t *keys,
+                                                            const uint32_t *info, uint32_t *bcount) {
+  const uint32_t m = info[FI_M];
   __shared__ uint32_t wc[CB_LEVELS][CB_THREADS / 32];
   const uint32_t k = blockIdx.x * CB_THREADS + threadIdx.x;
   const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -312,13 +353,14 @@ __global__ void __launch_bounds__(32) k_cells_starts(uint32_t ccap, uint32_t *in
 }
 
 // start_of[cell] = the point that starts it; level_of[cell] = its level.
-__global__ void __launch_bounds__(CB_THREADS) k_cells_place(const uint64_t *keys, uint32_t m,
+__global__ void __launch_bounds__(CB_THREADS) k_cells_place(const uint64_t *keys,
                                                             const uint32_t *bcount,
                                                             const uint32_t *info,
                                                             uint32_t *start_of,
                                                             uint8_t *level_of) {
   __shared__ uint32_t wc[CB_LEVELS][CB_THREADS / 32];
   if (__ldcg(&info[FI_OVERFLOW])) return;
+  const uint32_t m = info[FI_M];
   const uint32_t k = blockIdx.x * CB_THREADS + threadIdx.x;
   const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int d0 = 0, d1 = -1;
@@ -341,10 +383,11 @@ __global__ void __launch_bounds__(CB_THREADS) k_cells_place(const uint64_t *keys
   }
 }
 
-__global__ void __launch_bounds__(CB_THREADS) k_cells_fill(const uint64_t *keys, uint32_t m,
+__global__ void __launch_bounds__(CB_THREADS) k_cells_fill(const uint64_t *keys,
                                                            const uint32_t *start_of,
                                                            const uint8_t *level_of,
                                                            const uint32_t *info, FCell *cells) {
+  const uint32_t m = info[FI_M];
   const uint32_t total = __ldcg(&info[FI_CELLS]);
   if (__ldcg(&info[FI_OVERFLOW])) return;
   const uint32_t c = blockIdx.x * CB_THREADS + threadIdx.x;
@@ -991,7 +1034,7 @@ void fmm_free(FastScratch &s) {
   cudaFree(f->m2l_off); cudaFree(f->m2l_cnt); cudaFree(f->p2p_off);
   cudaFree(f->p2p_cnt); cudaFree(f->fwd_off); cudaFree(f->fwd_cnt); cudaFree(f->m2l);
   cudaFree(f->p2p); cudaFree(f->fwd); cudaFree(f->mco); cudaFree(f->lco); cudaFree(f->tab);
-  cudaFree(f->info); cudaFree(f->bsum); cudaFree(f->square);
+  cudaFree(f->info); cudaFree(f->bsum); cudaFree(f->square); cudaFree(f->geom);
   cudaFree(f->cb_count); cudaFree(f->start_of); cudaFree(f->level_of);
   cudaFreeHost(f->h_info); cudaFreeHost(f->h_geom);
   delete f;
@@ -1023,6 +1066,7 @@ int fmm_prepare(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *s
     D3_CUDA_OK(cudaMemset(f->info, 0, 64 * sizeof(uint32_t)));
     D3_CUDA_OK(cudaMalloc(&f->square, 4 * sizeof(double)));
     D3_CUDA_OK(cudaMalloc(&f->tab, sizeof(FmmTables)));
+    D3_CUDA_OK(cudaMalloc(&f->geom, 4 * sizeof(double)));
     D3_CUDA_OK(cudaHostAlloc(&f->h_info, 64 * sizeof(uint32_t), cudaHostAllocDefault));
     D3_CUDA_OK(cudaHostAlloc(&f->h_geom, 8 * sizeof(double), cudaHostAllocDefault));
     int dev = 0, sms = 0, per = 0;
@@ -1052,44 +1096,40 @@ int fmm_prepare(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *s
   D3_LAUNCH(k_fmm_keys, blocks_for(n, 256), 256, 0, st)(a.x, a.y, n, f.square, t.keys, t.sv);
   SortScratch ss{t.keys_tmp, t.sv_tmp, t.hist, t.scan_part};
   radix_sort_u64(t.keys, t.sv, n, 0, 4, true, ss, st);
-  if (cudaMemcpyAsync(f.h_geom, t.extent, 4 * sizeof(double), cudaMemcpyDeviceToHost, st) !=
-          cudaSuccess ||
-      cudaMemcpyAsync(f.h_info, t.info, sizeof(uint32_t), cudaMemcpyDeviceToHost, st) !=
-          cudaSuccess ||
-      cudaStreamSynchronize(st) != cudaSuccess)
-    return -1;
-  const uint32_t m = f.h_info[0];
-  if (m == 0) return 2;  // nothing to do (tree.zig:287-309 with an empty box)
-  const double e0 = f.h_geom[0], e1 = f.h_geom[1], e2 = f.h_geom[2], e3 = f.h_geom[3];
-  const double w = e2 - e0;
-  if (!(w > 0 && w < INFINITY)) return 0;  // the exact kernel runs instead
-  const double inv_w = 1 / w;
-  const double ox = (e0 + e2) / 2, oy = (e1 + e3) / 2;
-  D3_LAUNCH(k_fmm_gather, blocks_for(m, 256), 256, 0, st)(t.sv, a.x, a.y, strengths, m, alpha,
-                                                          ox, oy, inv_w, f.px, f.py, f.ps,
-                                                          f.ux, f.uy);
+  // the geometry, the point count and the gather stay on the device: the
+  // host reads them with the cell counts, in one synchronisation
+  D3_LAUNCH(k_fmm_geom, 1, 1, 0, st)(t.extent, t.info, f.geom, f.info);
+  D3_LAUNCH(k_fmm_gather, blocks_for(n, 256), 256, 0, st)(t.sv, a.x, a.y, strengths, f.info, alpha,
+                                                          f.geom, f.px, f.py, f.ps, f.ux, f.uy);
   // cells (level order); grow and rebuild if they do not fit
-  uint32_t want = 2 * (m / FMM_LEAF + 1) + 64;
+  uint32_t want = 2 * (n / FMM_LEAF + 1) + 64;
   for (int attempt = 0;; ++attempt) {
     if (fmm_reserve_cells(f, want > f.ccap ? want : f.ccap)) return -1;
     {
-      const uint32_t nb = (m + CB_THREADS - 1) / CB_THREADS;
+      const uint32_t nb = (n + CB_THREADS - 1) / CB_THREADS;
       if (grow(f.cb_count, f.cb_count_cap, (size_t)nb * CB_LEVELS) ||
           grow(f.start_of, f.start_cap, (size_t)f.ccap) || grow(f.level_of, f.level_cap, (size_t)f.ccap))
         return -1;
-      D3_LAUNCH(k_cells_count, nb, CB_THREADS, 0, st)(t.keys, m, f.cb_count);
+      D3_LAUNCH(k_cells_count, nb, CB_THREADS, 0, st)(t.keys, f.info, f.cb_count);
       D3_LAUNCH(k_cells_scan, CB_LEVELS, 1024, 0, st)(f.cb_count, nb, f.info);
       D3_LAUNCH(k_cells_starts, 1, 32, 0, st)(f.ccap, f.info);
-      D3_LAUNCH(k_cells_place, nb, CB_THREADS, 0, st)(t.keys, m, f.cb_count, f.info, f.start_of,
+      D3_LAUNCH(k_cells_place, nb, CB_THREADS, 0, st)(t.keys, f.cb_count, f.info, f.start_of,
                                                     f.level_of);
       D3_LAUNCH(k_cells_fill, blocks_for(f.ccap, CB_THREADS), CB_THREADS, 0, st)(
-          t.keys, m, f.start_of, f.level_of, f.info, f.cells);
+          t.keys, f.start_of, f.level_of, f.info, f.cells);
     }
-    if (sync_read(f, st)) return -1;
+    if (cudaMemcpyAsync(f.h_geom, f.geom, 4 * sizeof(double), cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess ||
+        sync_read(f, st))
+      return -1;
+    if (f.h_info[FI_BAD]) return 0;  // the exact kernel runs instead
+    if (!f.h_info[FI_M]) return 2;   // nothing to do (tree.zig:287-309 with an empty box)
     if (!f.h_info[FI_OVERFLOW]) break;
     if (attempt > 8) return -1;
     want = 2 * f.h_info[FI_OVERFLOW] + 64;
   }
+  const uint32_t m = f.h_info[FI_M];
+  const double w = f.h_geom[0], inv_w = f.h_geom[1], ox = f.h_geom[2], oy = f.h_geom[3];
   out.m = m;
   out.ncells = f.h_info[FI_CELLS];
   out.nlev = f.h_info[FI_LEVELS];

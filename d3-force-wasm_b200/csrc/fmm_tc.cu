@@ -192,41 +192,57 @@ __device__ __forceinline__ uint32_t compact16(uint32_t x) {  // even bits -> 16 
   return x;
 }
 
+// A thread per cell; the leaf list and the four quadrant groups are filled
+// with one atomic per warp and list (their order is free: every later pass
+// treats their entries independently).
 __global__ void k_tc_geom(TcArgs a) {
   const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= a.ncells) return;
-  const FCell f = a.fc[c];
-  TcCell t;
-  t.first = f.first;
-  t.count = f.count;
-  t.parent = f.parent;
-  t.level = (uint8_t)f.depth;
-  const uint32_t key = (uint32_t)a.keys[f.first];
-  const uint32_t pre = f.depth ? key >> (2 * (16 - f.depth)) : 0;
-  t.ix = (uint16_t)compact16(pre);
-  t.iy = (uint16_t)compact16(pre >> 1);
-  t.quad = (uint8_t)(pre & 3);
-  // the children: contiguous from child0, one per non-empty quadrant in order
-  uint32_t mask = 0;
-  const uint32_t nch = f.nchild;
-  for (uint32_t j = 0; j < nch; ++j) {
-    const FCell ch = a.fc[f.child0 + j];
-    const uint32_t ck = (uint32_t)a.keys[ch.first];
-    mask |= 1u << ((ck >> (2 * (16 - ch.depth))) & 3);
+  const unsigned lane = threadIdx.x & 31, lt = (1u << lane) - 1;
+  const bool valid = c < a.ncells;
+  TcCell t{};
+  uint32_t depth = 0;
+  if (valid) {
+    const FCell f = a.fc[c];
+    t.first = f.first;
+    t.count = f.count;
+    t.parent = f.parent;
+    t.level = (uint8_t)f.depth;
+    depth = f.depth;
+    const uint32_t key = (uint32_t)a.keys[f.first];
+    const uint32_t pre = f.depth ? key >> (2 * (16 - f.depth)) : 0;
+    t.ix = (uint16_t)compact16(pre);
+    t.iy = (uint16_t)compact16(pre >> 1);
+    t.quad = (uint8_t)(pre & 3);
+    // the children: contiguous from child0, one per non-empty quadrant in order
+    uint32_t mask = 0;
+    const uint32_t nch = f.nchild;
+    for (uint32_t j = 0; j < nch; ++j) {
+      const FCell ch = a.fc[f.child0 + j];
+      const uint32_t ck = (uint32_t)a.keys[ch.first];
+      mask |= 1u << ((ck >> (2 * (16 - ch.depth))) & 3);
+    }
+    t.cmask = (uint8_t)mask;
+    t.nchild = (uint8_t)nch;
+    t.child0 = nch ? f.child0 : 0;
+    a.cells[c] = t;
+    if (nch) a.feat[(size_t)c * 16 + 15] = -1.f;  // no feature row: not a leaf
+    if (c == 0)  // the root gets no M2L: its local expansion starts at zero
+      for (uint32_t k = 0; k < TC_KN; ++k) a.lco[k] = 0;
   }
-  t.cmask = (uint8_t)mask;
-  t.nchild = (uint8_t)nch;
-  t.child0 = nch ? f.child0 : 0;
-  a.cells[c] = t;
-  if (nch) a.feat[(size_t)c * 16 + 15] = -1.f;  // no feature row: not a leaf
-  if (nch == 0) a.leaves[atomicAdd(&a.info[TI_LEAVES], 1u)] = c;
-  if (c == 0)  // the root gets no M2L: its local expansion starts at zero
-    for (uint32_t k = 0; k < TC_KN; ++k) a.lco[k] = 0;
-  if (f.depth > 0) {
-    const uint32_t g = t.quad;
-    const uint32_t k = atomicAdd(&a.info[TI_GROUP + g], 1u);
-    a.groups[(size_t)g * a.ccap + k] = c;
-  }
+  // the leaf list
+  const unsigned leaves = __ballot_sync(0xffffffffu, valid && t.nchild == 0);
+  uint32_t lb = 0;
+  if (leaves && lane == __ffs(leaves) - 1) lb = atomicAdd(&a.info[TI_LEAVES], __popc(leaves));
+  lb = __shfl_sync(0xffffffffu, lb, leaves ? __ffs(leaves) - 1 : 0);
+  if (valid && t.nchild == 0) a.leaves[lb + __popc(leaves & lt)] = c;
+  // the quadrant groups (every cell but the root)
+  const uint32_t g = valid && depth > 0 ? t.quad : 4u + lane;  // 4+: no group, never matches
+  const unsigned peers = __match_any_sync(0xffffffffu, g);
+  const uint32_t leader = __ffs(peers) - 1;
+  uint32_t gb = 0;
+  if (g < 4 && lane == leader) gb = atomicAdd(&a.info[TI_GROUP + g], __popc(peers));
+  gb = __shfl_sync(0xffffffffu, gb, leader);
+  if (g < 4) a.groups[(size_t)g * a.ccap + gb + __popc(peers & lt)] = c;
 }
 
 // ---- upward (FP64): P2M per leaf, M2M by the last child to finish ----------------------------
@@ -518,39 +534,68 @@ __device__ __forceinline__ bool cand_events(const TcArgs &a, const TcCell &A, Ca
   }
 }
 
-// The lists of cell c (not the root) when its candidates fit LIST_KEEP
-// rounds of the warp: each candidate is evaluated once, its event and the
-// per-kind offsets kept in registers between the count and the write.
+// A cell's list state between its count and its writes (registers).
+// mode 0: the root; 1: candidates kept in registers (at most LIST_KEEP
+// rounds of the warp); 2: more candidates, evaluated again to write.
 constexpr uint32_t LIST_KEEP = 4;
 
-__device__ void tc_list_cell_kept(const TcArgs &a, uint32_t c, const TcCell &A, uint32_t ncand) {
+struct ListState {
+  Ev tot;
+  bool ok;
+  uint32_t mode, ncand;
+  Cand kept[LIST_KEEP];
+  uint32_t off[LIST_KEEP][4];
+};
+
+// The per-kind totals of one round of events: tot += the warp's sums, off[k]
+// = this lane's offset among the round's events of kind k (after tot).
+__device__ __forceinline__ void round_offsets(const Ev &e, Ev &tot, uint32_t *off) {
+  uint32_t t;
+  if (__all_sync(0xffffffffu, (e.np | e.nw | e.nx | e.nc) < 2048u)) {
+    // two counts per word: 32 lanes x 2047 stays below 2^16
+    uint32_t t23;
+    const uint32_t x01 = warp_excl_sum(e.np | (e.nw << 16), t);
+    const uint32_t x23 = warp_excl_sum(e.nx | (e.nc << 16), t23);
+    off[0] = tot.np + (x01 & 0xFFFFu); tot.np += t & 0xFFFFu;
+    off[1] = tot.nw + (x01 >> 16);     tot.nw += t >> 16;
+    off[2] = tot.nx + (x23 & 0xFFFFu); tot.nx += t23 & 0xFFFFu;
+    off[3] = tot.nc + (x23 >> 16);     tot.nc += t23 >> 16;
+  } else {
+    off[0] = tot.np + warp_excl_sum(e.np, t); tot.np += t;
+    off[1] = tot.nw + warp_excl_sum(e.nw, t); tot.nw += t;
+    off[2] = tot.nx + warp_excl_sum(e.nx, t); tot.nx += t;
+    off[3] = tot.nc + warp_excl_sum(e.nc, t); tot.nc += t;
+  }
+}
+
+// Count phase of a cell that is not the root, its candidates kept: the
+// candidates' loads by dependency level for all rounds at once (the parent's
+// near cell or coarse leaf, its cell, then for a leaf the near cell's child);
+// the M2L table and near list entries are written here.
+__device__ void tc_list_count_kept(const TcArgs &a, uint32_t c, const TcCell &A, ListState &S) {
   const unsigned lane = threadIdx.x & 31;
-  const uint32_t nn = a.tab->nnear;
+  const uint32_t nn = a.tab->nnear, ncand = S.ncand;
   const bool leaf = A.nchild == 0;
-  // the candidates' loads by dependency level, all rounds at once: the
-  // parent's near cell or coarse leaf, its cell, then (a leaf's near cell)
-  // the near cell's child
+  const uint32_t rounds = (ncand + 31) / 32;  // warp-uniform, <= LIST_KEEP
   const uint32_t coff = ncand > 4 * nn ? __ldcg(&a.loff[(size_t)A.parent * 8 + 6]) : 0;
-  uint32_t id[LIST_KEEP];
+  uint32_t id[LIST_KEEP], child[LIST_KEEP];
 #pragma unroll
   for (uint32_t r = 0; r < LIST_KEEP; ++r) {
     const uint32_t u = r * 32 + lane;
-    id[r] = TC_NONE;
-    if (u < ncand)
+    id[r] = child[r] = TC_NONE;
+    S.kept[r] = {0, 0};
+    if (r < rounds && u < ncand)
       id[r] = u < 4 * nn ? __ldcg(&a.near[(size_t)A.parent * nn + (u >> 2)])
                          : __ldcg(&a.pool[coff + u - 4 * nn]);
   }
   TcCell P[LIST_KEEP];
 #pragma unroll
   for (uint32_t r = 0; r < LIST_KEEP; ++r)
-    if (id[r] != TC_NONE) P[r] = a.cells[id[r]];
-  Cand kept[LIST_KEEP];
-  uint32_t child[LIST_KEEP];
+    if (r < rounds && id[r] != TC_NONE) P[r] = a.cells[id[r]];
 #pragma unroll
   for (uint32_t r = 0; r < LIST_KEEP; ++r) {
+    if (r >= rounds) break;
     const uint32_t u = r * 32 + lane;
-    kept[r] = {0, 0};
-    child[r] = TC_NONE;
     if (id[r] == TC_NONE) continue;
     bool coarse = u >= 4 * nn;
     if (!coarse) {
@@ -571,154 +616,149 @@ __device__ void tc_list_cell_kept(const TcArgs &a, uint32_t c, const TcCell &A, 
         continue;
       }
     }
-    if (coarse) kept[r] = {separated(a, A, P[r]) ? 3u : leaf ? 1u : 4u, id[r]};
+    if (coarse) S.kept[r] = {separated(a, A, P[r]) ? 3u : leaf ? 1u : 4u, id[r]};
   }
 #pragma unroll
   for (uint32_t r = 0; r < LIST_KEEP; ++r)
-    if (child[r] != TC_NONE) kept[r] = {a.cells[child[r]].nchild == 0 ? 1u : 5u, child[r]};
-  uint32_t off[LIST_KEEP][4];
-  Ev tot{0, 0, 0, 0};
-  bool ok = true;
+    if (r < rounds && child[r] != TC_NONE)
+      S.kept[r] = {a.cells[child[r]].nchild == 0 ? 1u : 5u, child[r]};
 #pragma unroll
   for (uint32_t r = 0; r < LIST_KEEP; ++r) {
-    if (r * 32 >= ncand) break;
+    if (r >= rounds) break;
     Ev e{0, 0, 0, 0};
     const uint32_t z4[4] = {0, 0, 0, 0};
-    if (!cand_events<false>(a, A, kept[r], e, z4)) ok = false;
-    uint32_t t;
-    off[r][0] = tot.np + warp_excl_sum(e.np, t); tot.np += t;
-    off[r][1] = tot.nw + warp_excl_sum(e.nw, t); tot.nw += t;
-    off[r][2] = tot.nx + warp_excl_sum(e.nx, t); tot.nx += t;
-    off[r][3] = tot.nc + warp_excl_sum(e.nc, t); tot.nc += t;
+    if (!cand_events<false>(a, A, S.kept[r], e, z4)) S.ok = false;
+    round_offsets(e, S.tot, S.off[r]);
   }
-  ok = __all_sync(0xffffffffu, ok);
-  uint32_t base = 0;
-  const uint32_t all = tot.np + tot.nw + tot.nx + tot.nc;
-  if (lane == 0) base = atomicAdd(&a.info[TI_POOL_P2P], all);
-  base = __shfl_sync(0xffffffffu, base, 0);
-  const uint32_t o4[4] = {base, base + tot.np, base + tot.np + tot.nw,
-                          base + tot.np + tot.nw + tot.nx};
-  uint32_t *lo = a.loff + (size_t)c * 8;
-  if (!ok || (size_t)base + all > a.pool_cap) {
-    if (lane == 0) {
-      atomicOr(&a.info[TI_OVF], ok ? 1u : 2u);
-      lo[0] = lo[2] = lo[4] = lo[6] = 0;
-      lo[1] = lo[3] = lo[5] = lo[7] = 0;
-    }
-    return;
+}
+
+// Count phase of a cell with more candidates than the lanes keep.
+__device__ void tc_list_count_general(const TcArgs &a, uint32_t c, const TcCell &A, ListState &S) {
+  const unsigned lane = threadIdx.x & 31;
+  const uint32_t zero4[4] = {0, 0, 0, 0};
+  for (uint32_t u0 = 0; u0 < S.ncand; u0 += 32) {
+    const uint32_t u = u0 + lane;
+    Ev e{0, 0, 0, 0};
+    if (u < S.ncand && !tc_candidate<false>(a, c, A, u, e, zero4)) S.ok = false;
+    uint32_t off[4];
+    round_offsets(e, S.tot, off);
   }
-  if (lane == 0) {
-    lo[0] = o4[0]; lo[1] = tot.np;
-    lo[2] = o4[1]; lo[3] = tot.nw;
-    lo[4] = o4[2]; lo[5] = tot.nx;
-    lo[6] = o4[3]; lo[7] = tot.nc;
-  }
-#pragma unroll
-  for (uint32_t r = 0; r < LIST_KEEP; ++r) {
-    if (kept[r].kind) {
-      const uint32_t w4[4] = {o4[0] + off[r][0], o4[1] + off[r][1], o4[2] + off[r][2],
-                              o4[3] + off[r][3]};
+}
+
+// Write phase of the general case: evaluate again, each lane's events after
+// those of the candidates before it.
+__device__ void tc_list_write_general(const TcArgs &a, uint32_t c, const TcCell &A,
+                                      const ListState &S, uint32_t *o4) {
+  const unsigned lane = threadIdx.x & 31;
+  const uint32_t zero4[4] = {0, 0, 0, 0};
+  Ev run{0, 0, 0, 0};
+  for (uint32_t u0 = 0; u0 < S.ncand; u0 += 32) {
+    const uint32_t u = u0 + lane;
+    Ev e{0, 0, 0, 0};
+    if (u < S.ncand) tc_candidate<false>(a, c, A, u, e, zero4);
+    uint32_t off[4];
+    round_offsets(e, run, off);
+    if (u < S.ncand) {
       Ev w{0, 0, 0, 0};
-      cand_events<true>(a, A, kept[r], w, w4);
+      const uint32_t w4[4] = {o4[0] + off[0], o4[1] + off[1], o4[2] + off[2], o4[3] + off[3]};
+      tc_candidate<true>(a, c, A, u, w, w4);
     }
   }
 }
 
 // loff[c * 8 + ...]: 0 p2p off, 1 p2p cnt, 2 w off, 3 w cnt, 4 x off, 5 x cnt,
 // 6 coarse off, 7 coarse cnt.
-__device__ void tc_list_cell(const TcArgs &a, uint32_t c) {
-  const unsigned lane = threadIdx.x & 31;
+//
+// The cells of one level, a warp per cell; the levels run as consecutive
+// launches from the root down (a cell's lists read its parent's). Each warp
+// counts its cell's events, the block takes one range of the pool for all of
+// its warps (one atomic per block), then each warp writes.
+__global__ void __launch_bounds__(TC_THREADS, 3) k_tc_lists(TcArgs a, uint32_t c0, uint32_t c1) {
+  __shared__ uint32_t wsum[TC_WARPS + 1];
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t c = c0 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const bool active = c < c1;  // warp-uniform
   const uint32_t nn = a.tab->nnear;
-  const TcCell A = a.cells[c];
-  for (uint32_t j = lane; j < a.tab->sstride; j += 32) a.m2l[(size_t)c * a.tab->sstride + j] = TC_NONE;
-  for (uint32_t j = lane; j < nn; j += 32) a.near[(size_t)c * nn + j] = TC_NONE;
-  if (c == 0) {
-    // the root: near itself
-    uint32_t self = 0;
-    for (uint32_t o = 0; o < nn; ++o)
-      if (a.tab->near_dx[o] == 0 && a.tab->near_dy[o] == 0) self = o;
+  ListState S;
+  S.tot = {0, 0, 0, 0};
+  S.ok = true;
+  S.mode = 0;
+  S.ncand = 0;
+  TcCell A;
+  uint32_t all = 0;
+  if (active) {
+    A = a.cells[c];
+    for (uint32_t j = lane; j < a.tab->sstride; j += 32) a.m2l[(size_t)c * a.tab->sstride + j] = TC_NONE;
+    for (uint32_t j = lane; j < nn; j += 32) a.near[(size_t)c * nn + j] = TC_NONE;
     __syncwarp();
-    if (lane == 0) {
-      a.near[self] = 0;
-      uint32_t op = 0;
-      if (A.nchild == 0) {
-        op = atomicAdd(&a.info[TI_POOL_P2P], 1u);
-        if (op < a.pool_cap) a.pool[op] = 0;
-        else atomicOr(&a.info[TI_OVF], 1u);
+    if (c == 0) {
+      S.tot.np = A.nchild == 0 ? 1 : 0;  // the root: near itself; a P2P entry when a leaf
+    } else {
+      S.ncand = 4 * nn + __ldcg(&a.loff[(size_t)A.parent * 8 + 7]);
+      if (S.ncand <= 32 * LIST_KEEP) {
+        S.mode = 1;
+        tc_list_count_kept(a, c, A, S);
+      } else {
+        S.mode = 2;
+        tc_list_count_general(a, c, A, S);
       }
-      uint32_t *lo = a.loff + (size_t)c * 8;
-      lo[0] = op; lo[1] = A.nchild == 0 ? 1 : 0;
-      lo[2] = lo[3] = lo[4] = lo[5] = lo[6] = lo[7] = 0;
+      S.ok = __all_sync(0xffffffffu, S.ok);
     }
-    return;
+    all = S.tot.np + S.tot.nw + S.tot.nx + S.tot.nc;
   }
-  __syncwarp();
-  const uint32_t ncoarse = __ldcg(&a.loff[(size_t)A.parent * 8 + 7]);
-  const uint32_t ncand = 4 * nn + ncoarse;
-  if (ncand <= 32 * LIST_KEEP) {
-    tc_list_cell_kept(a, c, A, ncand);
-    return;
+  if (lane == 0) wsum[warp] = all;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t run = 0;
+    for (uint32_t w = 0; w < TC_WARPS; ++w) {
+      const uint32_t t = wsum[w];
+      wsum[w] = run;
+      run += t;
+    }
+    wsum[TC_WARPS] = run ? atomicAdd(&a.info[TI_POOL_P2P], run) : 0;
   }
-  // more candidates than the lanes keep: count, then evaluate again to write
-  Ev tot{0, 0, 0, 0};
-  bool ok = true;
-  const uint32_t zero4[4] = {0, 0, 0, 0};
-  for (uint32_t u0 = 0; u0 < ncand; u0 += 32) {
-    const uint32_t u = u0 + lane;
-    Ev e{0, 0, 0, 0};
-    if (u < ncand && !tc_candidate<false>(a, c, A, u, e, zero4)) ok = false;
-    uint32_t t;
-    warp_excl_sum(e.np, t); tot.np += t;
-    warp_excl_sum(e.nw, t); tot.nw += t;
-    warp_excl_sum(e.nx, t); tot.nx += t;
-    warp_excl_sum(e.nc, t); tot.nc += t;
-  }
-  ok = __all_sync(0xffffffffu, ok);
-  uint32_t base = 0;
-  const uint32_t all = tot.np + tot.nw + tot.nx + tot.nc;
-  if (lane == 0) base = atomicAdd(&a.info[TI_POOL_P2P], all);
-  base = __shfl_sync(0xffffffffu, base, 0);
-  uint32_t o4[4] = {base, base + tot.np, base + tot.np + tot.nw, base + tot.np + tot.nw + tot.nx};
-  if (lane == 0) {
-    uint32_t *lo = a.loff + (size_t)c * 8;
-    lo[0] = o4[0]; lo[1] = tot.np;
-    lo[2] = o4[1]; lo[3] = tot.nw;
-    lo[4] = o4[2]; lo[5] = tot.nx;
-    lo[6] = o4[3]; lo[7] = tot.nc;
-  }
-  if (!ok || (size_t)base + all > a.pool_cap) {
+  __syncthreads();
+  if (!active) return;
+  const uint32_t base = wsum[TC_WARPS] + wsum[warp];
+  const uint32_t o4[4] = {base, base + S.tot.np, base + S.tot.np + S.tot.nw,
+                          base + S.tot.np + S.tot.nw + S.tot.nx};
+  uint32_t *lo = a.loff + (size_t)c * 8;
+  if (!S.ok || (size_t)base + all > a.pool_cap) {
     if (lane == 0) {
-      atomicOr(&a.info[TI_OVF], ok ? 1u : 2u);
-      uint32_t *lo = a.loff + (size_t)c * 8;
+      atomicOr(&a.info[TI_OVF], S.ok ? 1u : 2u);
+      lo[0] = lo[2] = lo[4] = lo[6] = 0;
       lo[1] = lo[3] = lo[5] = lo[7] = 0;
     }
     return;
   }
-  // writes, each lane's events after those of the candidates before it
-  for (uint32_t u0 = 0; u0 < ncand; u0 += 32) {
-    const uint32_t u = u0 + lane;
-    Ev e{0, 0, 0, 0};
-    if (u < ncand) tc_candidate<false>(a, c, A, u, e, zero4);
-    uint32_t t0, t1, t2, t3;
-    const uint32_t xp = warp_excl_sum(e.np, t0), xw = warp_excl_sum(e.nw, t1);
-    const uint32_t xx = warp_excl_sum(e.nx, t2), xc = warp_excl_sum(e.nc, t3);
-    if (u < ncand) {
-      Ev w{0, 0, 0, 0};
-      const uint32_t off[4] = {o4[0] + xp, o4[1] + xw, o4[2] + xx, o4[3] + xc};
-      tc_candidate<true>(a, c, A, u, w, off);
-    }
-    o4[0] += t0;
-    o4[1] += t1;
-    o4[2] += t2;
-    o4[3] += t3;
+  if (lane == 0) {
+    lo[0] = o4[0]; lo[1] = S.tot.np;
+    lo[2] = o4[1]; lo[3] = S.tot.nw;
+    lo[4] = o4[2]; lo[5] = S.tot.nx;
+    lo[6] = o4[3]; lo[7] = S.tot.nc;
   }
-}
-
-// The cells of one level, a warp per cell; the levels run as consecutive
-// launches from the root down (a cell's lists read its parent's).
-__global__ void __launch_bounds__(TC_THREADS) k_tc_lists(TcArgs a, uint32_t c0, uint32_t c1) {
-  const uint32_t c = c0 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  if (c < c1) tc_list_cell(a, c);
+  if (S.mode == 0) {
+    if (lane == 0) {
+      uint32_t self = 0;
+      for (uint32_t o = 0; o < nn; ++o)
+        if (a.tab->near_dx[o] == 0 && a.tab->near_dy[o] == 0) self = o;
+      a.near[self] = 0;
+      if (S.tot.np) a.pool[base] = 0;
+    }
+  } else if (S.mode == 1) {
+#pragma unroll
+    for (uint32_t r = 0; r < LIST_KEEP; ++r) {
+      if (S.kept[r].kind) {
+        const uint32_t w4[4] = {o4[0] + S.off[r][0], o4[1] + S.off[r][1], o4[2] + S.off[r][2],
+                                o4[3] + S.off[r][3]};
+        Ev w{0, 0, 0, 0};
+        cand_events<true>(a, A, S.kept[r], w, w4);
+      }
+    }
+  } else {
+    uint32_t o[4] = {o4[0], o4[1], o4[2], o4[3]};
+    tc_list_write_general(a, c, A, S, o);
+  }
 }
 
 // ---- M2L on the tensor cores -------------------------------------------------------------
@@ -1182,20 +1222,17 @@ __device__ __forceinline__ void tc_pair(const float4 sv, float xi, float yi, uin
   ay += dy * w;
 }
 
-// The same pair without the jiggle. w = s / l, or s / sqrt(dmin2 l) inside
-// distanceMin, is s * rsqrt(y) with y = l max(l, dmin2) (one MUFU op); l is
-// floored at 1e-18 there (distances under 1e-9, below FP32's resolution of
-// the leaf-local coordinates) so the self pair adds 0 * w with w finite.
-// Zero distances are counted in zc: more than the lane's own self pair means
-// a coincident pair of distinct points, and the batch is redone with
-// tc_pair. A single zero delta keeps its zero here, where d3 would jiggle it
-// by ~1e-6: the change to the kick is ~1e-6 of that one pair's term.
+// The same pair without the jiggle, for leaves with no coincident points.
+// w = s / l, or s / sqrt(dmin2 l) inside distanceMin, is s * rsqrt(y) with
+// y = l max(l, dmin2) (one MUFU op); l is floored at 1e-18 there (distances
+// under 1e-9, below FP32's resolution of the leaf-local coordinates) so the
+// self pair adds 0 * w with w finite. A single zero delta keeps its zero
+// here, where d3 would jiggle it by ~1e-6: the change to the kick is ~1e-6
+// of that one pair's term.
 __device__ __forceinline__ void tc_pair_fast(const float4 sv, float xi, float yi, float dmin2,
-                                             float &ax, float &ay, uint32_t &zc) {
+                                             float &ax, float &ay) {
   const float dx = sv.x - xi, dy = sv.y - yi;
-  const float l = fmaf(dx, dx, dy * dy);
-  zc += l == 0.f ? 1u : 0u;
-  const float lf = fmaxf(l, 1e-18f);
+  const float lf = fmaxf(fmaf(dx, dx, dy * dy), 1e-18f);
   const float w = sv.z * rsqrtf(lf * fmaxf(lf, dmin2));
   ax = fmaf(dx, w, ax);
   ay = fmaf(dy, w, ay);
@@ -1264,7 +1301,6 @@ __device__ __forceinline__ float2 tc_far(const TcArgs &a, uint32_t k, double cx,
 __global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int corrected) {
   __shared__ float4 stage[TC_WARPS][P2P_STAGE];
   __shared__ float lsh[TC_WARPS][TC_KN];
-  __shared__ uint32_t selfpos[TC_WARPS][32];  // per target lane: its own point's batch index
   __shared__ float2 red[TC_WARPS][32];
   const unsigned lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -1298,6 +1334,21 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int correct
       }
       Lsh[lane] = v;
     }
+    // Points at one position share a key, so they sit in one leaf: a leaf
+    // whose points (in its FP32 local coordinates) hold a coincident pair, or
+    // that spans several rounds of targets, takes the careful pair.
+    bool careful = A.count > 32;
+    if (!careful) {
+      const bool mine = lane < A.count;
+      const float px = mine ? (float)(a.px[A.first + lane] - ox) : 0.f;
+      const float py = mine ? (float)(a.py[A.first + lane] - oy) : 0.f;
+      bool dup = false;
+      for (uint32_t j = 0; j < A.count; ++j) {
+        const float qx = __shfl_sync(0xffffffffu, px, j), qy = __shfl_sync(0xffffffffu, py, j);
+        dup |= mine && j != lane && qx == px && qy == py;
+      }
+      careful = __any_sync(0xffffffffu, dup);
+    }
     float mx = 0, my = 0;  // the points' offsets from the centre (feature row)
     for (uint32_t tb = A.first; tb < A.first + A.count; tb += W) {
       const uint32_t ti = tb + gl;
@@ -1321,35 +1372,26 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int correct
         for (uint32_t base = 0; base < total; base += P2P_STAGE) {
           const uint32_t kn = min(P2P_STAGE, total - base);
           __syncwarp();
-          selfpos[wl][lane] = TC_NONE;
-          __syncwarp();
-#pragma unroll
+#pragma unroll 4
           for (uint32_t r = 0; r < P2P_STAGE / 32; ++r) {
             const uint32_t idx = base + r * 32 + lane;
             const uint32_t sj = batch_point(idx, ne, incl, before, first);
-            if (idx < base + kn) {
+            if (idx < base + kn)
               sg[r * 32 + lane] = make_float4((float)(__ldg(&a.px[sj]) - ox),
                                               (float)(__ldg(&a.py[sj]) - oy),
                                               (float)__ldg(&a.ps[sj]), __uint_as_float(sj));
-              if (sj - tb < W) selfpos[wl][sj - tb] = r * 32 + lane;  // a target of this round
-            }
           }
           __syncwarp();
-          const float sx0 = ax0, sy0 = ay0, sx1 = ax1, sy1 = ay1;
-          uint32_t zc = 0;
           uint32_t k = in ? grp : kn;
-#pragma unroll 2
-          for (; k + G < kn; k += 2 * G) {
-            tc_pair_fast(sg[k], xi, yi, dmin2, ax0, ay0, zc);
-            tc_pair_fast(sg[k + G], xi, yi, dmin2, ax1, ay1, zc);
-          }
-          if (k < kn) tc_pair_fast(sg[k], xi, yi, dmin2, ax0, ay0, zc);
-          const uint32_t sp = selfpos[wl][gl];
-          const uint32_t self = (sp != TC_NONE && sp % G == grp) ? 1u : 0u;
-          if (__any_sync(0xffffffffu, act && zc > self)) {
-            // a coincident pair in this batch: redo it with the jiggle
-            ax0 = sx0, ay0 = sy0, ax1 = sx1, ay1 = sy1;
-            for (k = in ? grp : kn; k + G < kn; k += 2 * G) {
+          if (!careful) {
+#pragma unroll 4
+            for (; k + G < kn; k += 2 * G) {
+              tc_pair_fast(sg[k], xi, yi, dmin2, ax0, ay0);
+              tc_pair_fast(sg[k + G], xi, yi, dmin2, ax1, ay1);
+            }
+            if (k < kn) tc_pair_fast(sg[k], xi, yi, dmin2, ax0, ay0);
+          } else {
+            for (; k + G < kn; k += 2 * G) {
               tc_pair(sg[k], xi, yi, ti, gi, dmin2, seed, a.perm, ax0, ay0);
               tc_pair(sg[k + G], xi, yi, ti, gi, dmin2, seed, a.perm, ax1, ay1);
             }

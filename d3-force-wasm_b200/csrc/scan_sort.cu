@@ -118,49 +118,65 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_hist(const uint64_t *keys
   for (int d = threadIdx.x; d < 256; d += blockDim.x) hist[(size_t)d * tiles + blockIdx.x] = h[d];
 }
 
-// Stable scatter of one tile: chunks of 256 keys in order; within a chunk a
-// key's rank among equal digits = earlier warps' counts + lanes below it in
-// its warp with the same digit (warp match).
+// Stable scatter of one tile of SORT_TILE keys: warp w takes the tile's
+// w-th run of 32 x PER keys, in PER rounds of 32. In a round a key's rank
+// among equal digits is the warp's count of that digit so far plus the lanes
+// below it with the same digit (warp match); the warps' counts then become
+// per-digit offsets (tile offset from the scanned histograms + the earlier
+// warps' counts), and every key is written once. Two block barriers per
+// tile.
 template <bool PART>
 __global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(const uint64_t *keys, const uint32_t *vals,
                                                                uint64_t *okeys, uint32_t *ovals,
                                                                uint32_t n, int shift,
                                                                const uint32_t *offsets,
                                                                uint32_t tiles) {
-  __shared__ uint32_t run[256];
-  __shared__ uint32_t wcnt[SORT_THREADS / 32][256];
+  constexpr unsigned WARPS = SORT_THREADS / 32, PER = SORT_TILE / SORT_THREADS;
+  __shared__ uint32_t wh[WARPS][256];
   const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int d = threadIdx.x; d < 256; d += blockDim.x) run[d] = offsets[(size_t)d * tiles + blockIdx.x];
-  const size_t base = (size_t)blockIdx.x * SORT_TILE;
-  for (unsigned c = 0; c < SORT_TILE; c += SORT_THREADS) {
-    for (int d = threadIdx.x; d < 256 * (SORT_THREADS / 32); d += blockDim.x) (&wcnt[0][0])[d] = 0;
-    __syncthreads();
-    size_t i = base + c + threadIdx.x;
-    bool valid = i < n;
-    uint64_t k = valid ? keys[i] : 0;
-    uint32_t v = valid ? vals[i] : 0;
-    uint32_t d = valid ? digit_of<PART>(k, v, shift) : 256u + lane;  // invalid lanes never match
-    unsigned peers = __match_any_sync(0xffffffffu, d);
-    unsigned below = __popc(peers & ((1u << lane) - 1));
-    if (valid && below == 0) wcnt[warp][d] = __popc(peers);
-    __syncthreads();
-    uint32_t pos = 0;
-    if (valid) {
-      uint32_t before = 0;
-      for (unsigned w = 0; w < warp; ++w) before += wcnt[w][d];
-      pos = run[d] + before + below;
-      okeys[pos] = k;
-      ovals[pos] = v;
-    }
-    __syncthreads();
-    // advance the running offsets by this chunk's counts
-    for (int dd = threadIdx.x; dd < 256; dd += blockDim.x) {
-      uint32_t t = 0;
-      for (unsigned w = 0; w < SORT_THREADS / 32; ++w) t += wcnt[w][dd];
-      run[dd] += t;
-    }
-    __syncthreads();
+  const unsigned lt = (1u << lane) - 1;
+  for (unsigned d = threadIdx.x; d < WARPS * 256; d += blockDim.x) (&wh[0][0])[d] = 0;
+  const size_t wbase = (size_t)blockIdx.x * SORT_TILE + (size_t)warp * 32 * PER;
+  uint64_t k[PER];
+  uint32_t v[PER], dg[PER], rk[PER];
+#pragma unroll
+  for (unsigned r = 0; r < PER; ++r) {
+    const size_t i = wbase + r * 32 + lane;
+    k[r] = i < n ? keys[i] : 0;
+    v[r] = i < n ? vals[i] : 0;
   }
+  __syncthreads();
+#pragma unroll
+  for (unsigned r = 0; r < PER; ++r) {
+    const bool valid = wbase + r * 32 + lane < n;
+    const uint32_t d = valid ? digit_of<PART>(k[r], v[r], shift) : 256u + lane;  // never matches
+    const unsigned peers = __match_any_sync(0xffffffffu, d);
+    const unsigned below = __popc(peers & lt);
+    const uint32_t cnt = valid ? wh[warp][d] : 0;
+    __syncwarp();
+    if (valid && below == 0) wh[warp][d] = cnt + __popc(peers);
+    __syncwarp();
+    dg[r] = d;
+    rk[r] = cnt + below;
+  }
+  __syncthreads();
+  for (unsigned d = threadIdx.x; d < 256; d += blockDim.x) {
+    uint32_t run = offsets[(size_t)d * tiles + blockIdx.x];
+#pragma unroll
+    for (unsigned w = 0; w < WARPS; ++w) {
+      const uint32_t t = wh[w][d];
+      wh[w][d] = run;
+      run += t;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (unsigned r = 0; r < PER; ++r)
+    if (wbase + r * 32 + lane < n) {
+      const uint32_t pos = wh[warp][dg[r]] + rk[r];
+      okeys[pos] = k[r];
+      ovals[pos] = v[r];
+    }
 }
 
 template <bool PART>

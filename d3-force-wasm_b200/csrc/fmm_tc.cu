@@ -134,6 +134,9 @@ struct TcDev {
   float *mlp_x = nullptr, *mlp_y = nullptr;  // per leaf: 12 inputs, 2 outputs
   double2 *kick = nullptr;           // per sorted point: the many-body kick
   double *chk = nullptr, *h_chk = nullptr;   // sampled check: sum err^2, sum ref^2
+  double2 *chk_part = nullptr;               // the check's partial direct sums
+  uint32_t chk_cap = 0;                      // samples chk_part holds
+  float2 *nearbuf = nullptr;                 // per sorted point: the learned pass's near field
   float *mlp = nullptr;              // installed network parameters (device)
   uint32_t ncells_last = 0;
   uint32_t hold = 0;                 // ticks left on the fallback after a failed check
@@ -170,7 +173,12 @@ struct TcArgs {
   const double *seed;
 };
 
-__device__ __forceinline__ double cell_side(uint32_t level) { return ldexp(1.0, -(int)level); }
+// 2^e for the small exponents of cell levels (|e| < 127), built exactly.
+__device__ __forceinline__ double pow2(int e) {
+  return __longlong_as_double((long long)(1023 + e) << 52);
+}
+__device__ __forceinline__ float pow2f(int e) { return __int_as_float((127 + e) << 23); }
+__device__ __forceinline__ double cell_side(uint32_t level) { return pow2(-(int)level); }
 __device__ __forceinline__ void cell_centre(const TcCell &c, double &x, double &y) {
   const double s = cell_side(c.level);
   x = -0.5 + (c.ix + 0.5) * s;
@@ -307,7 +315,7 @@ __global__ void __launch_bounds__(UP_THREADS) k_tc_upward(TcArgs a, uint32_t *ar
   {
     double cx, cy;
     cell_centre(C, cx, cy);
-    const double inv_s = ldexp(1.0, (int)C.level);
+    const double inv_s = pow2((int)C.level);
     for (uint32_t j = C.first; j < C.first + C.count; ++j) {
       const double sv = __ldg(&a.ps[j]);
       const double zr = (__ldg(&a.ux[j]) - cx) * inv_s, zi = (__ldg(&a.uy[j]) - cy) * inv_s;
@@ -964,7 +972,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_tc_p2l(TcArgs a) {
     const TcCell A = a.cells[c];
     double ax, ay;
     cell_centre(A, ax, ay);
-    const double inv_s = ldexp(1.0, (int)A.level);
+    const double inv_s = pow2((int)A.level);
     float sr[Q], si[Q];
 #pragma unroll
     for (int l = 0; l < Q; ++l) sr[l] = si[l] = 0.f;
@@ -1061,8 +1069,8 @@ __global__ void __launch_bounds__(TC_THREADS) k_tc_down(TcArgs a) {
     }
     const int d = (int)C.level - (int)P.level;
     const uint32_t mask = (1u << d) - 1u;
-    const float dx = ldexpf((float)(C.ix & mask) + 0.5f, -d) - 0.5f;
-    const float dy = ldexpf((float)(C.iy & mask) + 0.5f, -d) - 0.5f;
+    const float dx = ((float)(C.ix & mask) + 0.5f) * pow2f(-d) - 0.5f;
+    const float dy = ((float)(C.iy & mask) + 0.5f) * pow2f(-d) - 0.5f;
     float pr[Q], pi[Q];  // D^j
     pr[0] = 1.f;
     pi[0] = 0.f;
@@ -1081,7 +1089,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_tc_down(TcArgs a) {
         sr += tr * pr[j] - ti * pi[j];
         si += tr * pi[j] + ti * pr[j];
       }
-      const float sc = ldexpf(1.f, -(m + 1) * d);
+      const float sc = (m + 1) * d <= 126 ? pow2f(-(m + 1) * d) : 0.f;
       lr[m] += sr * sc;
       li[m] += si * sc;
     }
@@ -1168,7 +1176,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_tc_features(TcArgs a) {
     const TcCell C = a.cells[c];
     double cx, cy;
     cell_centre(C, cx, cy);
-    const double inv_s = ldexp(1.0, (int)C.level);
+    const double inv_s = pow2((int)C.level);
     float mx = 0, my = 0;
     for (uint32_t k = C.first + lane; k < C.first + C.count; k += 32) {
       mx += (float)((a.ux[k] - cx) * inv_s);
@@ -1242,8 +1250,8 @@ __device__ __forceinline__ void tc_pair_fast(const float4 sv, float xi, float yi
 // expansion (Lsh: 2q floats, L'_0 possibly corrected) by Horner in FP32 (the
 // L2P of downwardCell, fmm.zig:851-886),
 //     phi = (1/s) sum_l L'_l w^l,   w = (u - c) / s,
-// and M2P from each cell of the leaf's W list (FP64; the adaptive list has
-// no reference counterpart),
+// and M2P from each cell of the leaf's W list (z from an FP64 shift, the
+// series in FP32; the adaptive list has no reference counterpart),
 //     phi += (1/s_W) sum_k M'_k / z^(k+1),   z = (u - c_W) / s_W.
 // Returns the kick's far part in world units; (wr, wi) = w for the feature row.
 __device__ __forceinline__ float2 tc_far(const TcArgs &a, uint32_t k, double cx, double cy,
@@ -1265,22 +1273,23 @@ __device__ __forceinline__ float2 tc_far(const TcArgs &a, uint32_t k, double cx,
     const TcCell W = a.cells[cc];
     double wx, wy;
     cell_centre(W, wx, wy);
-    const double winv = ldexp(1.0, (int)W.level);
-    const double zr = (ux - wx) * winv, zi = (uy - wy) * winv;
-    const double d2 = zr * zr + zi * zi;
-    const double ir = zr / d2, ii = -zi / d2;
+    const double winv = pow2((int)W.level);
+    // z in FP64 (the shift), the series in FP32: |1/z| < 1 for a separated cell
+    const float zr = (float)((ux - wx) * winv), zi = (float)((uy - wy) * winv);
+    const float d2 = zr * zr + zi * zi;
+    const float ir = __fdividef(zr, d2), ii = -__fdividef(zi, d2);
     const double *mc = a.mco + (size_t)cc * 2 * q;
-    double pr = ir, pi = ii, sr = 0, si = 0;
+    float pr = ir, pi = ii, sr = 0, si = 0;
     for (uint32_t kk = 0; kk < q; ++kk) {
-      const double mr = mc[kk], mi = mc[q + kk];
+      const float mr = (float)mc[kk], mi = (float)mc[q + kk];
       sr += mr * pr - mi * pi;
       si += mr * pi + mi * pr;
-      const double nr = pr * ir - pi * ii;
+      const float nr = pr * ir - pi * ii;
       pi = pr * ii + pi * ir;
       pr = nr;
     }
-    gr += sr * winv;
-    gi += si * winv;
+    gr += (double)sr * winv;
+    gi += (double)si * winv;
   }
   return make_float2((float)(-gr * a.inv_w), (float)(gi * a.inv_w));
 }
@@ -1297,8 +1306,12 @@ __device__ __forceinline__ float2 tc_far(const TcArgs &a, uint32_t k, double cx,
 // Far: tc_far for each target (group 0's lanes), with the leaf's local
 // expansion in shared memory; `corrected` adds the learned form's network
 // output to L'_0 (sc * y / LEARN_TARGET_SCALE), else the leaf's feature row
-// is written. v += near + far in FP64 (or the kick to `kick`).
-__global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int corrected) {
+// is written. v += near + far in FP64 (or the kick to `kick`). `nearbuf`:
+// the near field is also stored there per point; with `far_only` it is read
+// back instead of computed (the learned form's fallback reuses the near
+// field of its order-4 pass: it does not depend on the order).
+__global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int corrected,
+                                                            float2 *nearbuf, int far_only) {
   __shared__ float4 stage[TC_WARPS][P2P_STAGE];
   __shared__ float lsh[TC_WARPS][TC_KN];
   __shared__ float2 red[TC_WARPS][32];
@@ -1323,7 +1336,7 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int correct
     const double ox = a.px[A.first], oy = a.py[A.first];
     double cx, cy;
     cell_centre(A, cx, cy);
-    const double inv_s = ldexp(1.0, (int)A.level);
+    const double inv_s = pow2((int)A.level);
     __syncwarp();
     {
       const float *L = a.lco + (size_t)c * TC_KN;
@@ -1338,7 +1351,7 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int correct
     // whose points (in its FP32 local coordinates) hold a coincident pair, or
     // that spans several rounds of targets, takes the careful pair.
     bool careful = A.count > 32;
-    if (!careful) {
+    if (!careful && !far_only) {
       const bool mine = lane < A.count;
       const float px = mine ? (float)(a.px[A.first + lane] - ox) : 0.f;
       const float py = mine ? (float)(a.py[A.first + lane] - oy) : 0.f;
@@ -1356,7 +1369,7 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int correct
       const float xi = act ? (float)(a.px[ti] - ox) : 0.f, yi = act ? (float)(a.py[ti] - oy) : 0.f;
       const uint32_t gi = act ? a.perm[ti] : 0;
       float ax0 = 0, ay0 = 0, ax1 = 0, ay1 = 0;
-      for (uint32_t eb = 0; eb < np; eb += 32) {
+      for (uint32_t eb = 0; eb < (far_only ? 0u : np); eb += 32) {
         // this batch's source leaves: lane j holds leaf j's first point and
         // the running count before it
         const uint32_t ne = min(32u, np - eb);
@@ -1411,6 +1424,13 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int correct
           vy += v.y;
         }
       if (act && grp == 0) {
+        if (far_only) {  // the near field of an earlier pass over the same lists
+          const float2 nv = nearbuf[ti];
+          vx = nv.x;
+          vy = nv.y;
+        } else if (nearbuf) {
+          nearbuf[ti] = make_float2(vx, vy);
+        }
         float wr, wi;
         const float2 f = tc_far(a, ti, cx, cy, inv_s, Lsh, nw, ow, wr, wi);
         mx += wr;
@@ -1436,18 +1456,26 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int correct
 
 // ---- the learned form's sampled check -----------------------------------------------------------
 
-// A block per sampled point k (sorted order, spread evenly): the FP64 direct
-// sum of d3's pair formula over every point (coincident pairs and the point
-// itself add nothing; distanceMin's clamp), against the kick the pass put in
-// kick[k]. Adds |kick - ref|^2 and |ref|^2 to chk[0], chk[1].
+// The sampled check's direct sums, spread over the GPU: block (j, part)
+// sums d3's pair formula in FP64 over its share of the points for sampled
+// point j (sorted order, spread evenly; coincident pairs and the point
+// itself add nothing; distanceMin's clamp) into part_out[(j * parts + part)].
+constexpr uint32_t CHECK_PARTS = 32;
+
+__device__ __forceinline__ uint32_t check_point(uint32_t j, uint32_t m, uint32_t samples) {
+  return (uint32_t)(((2ull * j + 1) * m) / (2ull * samples));
+}
+
 __global__ void __launch_bounds__(CHECK_THREADS) k_tc_check(TcArgs a, uint32_t samples,
-                                                            double dmin2, double *chk) {
+                                                            double dmin2, double2 *part_out) {
   __shared__ double sx[CHECK_THREADS / 32], sy[CHECK_THREADS / 32];
-  const uint32_t j = blockIdx.x;
-  const uint32_t k = (uint32_t)(((2ull * j + 1) * a.m) / (2ull * samples));
+  const uint32_t j = blockIdx.x / CHECK_PARTS, part = blockIdx.x % CHECK_PARTS;
+  const uint32_t k = check_point(j, a.m, samples);
   const double xi = a.px[k], yi = a.py[k];
+  const uint32_t i0 = (uint32_t)((uint64_t)a.m * part / CHECK_PARTS);
+  const uint32_t i1 = (uint32_t)((uint64_t)a.m * (part + 1) / CHECK_PARTS);
   double vx = 0, vy = 0;
-  for (uint32_t i = threadIdx.x; i < a.m; i += blockDim.x) {
+  for (uint32_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
     const double dx = a.px[i] - xi, dy = a.py[i] - yi;
     double l = dx * dx + dy * dy;
     if (!(l > 0)) continue;
@@ -1471,10 +1499,41 @@ __global__ void __launch_bounds__(CHECK_THREADS) k_tc_check(TcArgs a, uint32_t s
       rx += sx[w];
       ry += sy[w];
     }
-    const double2 kk = a.kick[k];
+    part_out[blockIdx.x] = make_double2(rx, ry);
+  }
+}
+
+// One block: per sample the reference kick (its parts in order) against the
+// kick the pass put in kick[k]; chk[0] = sum |kick - ref|^2, chk[1] =
+// sum |ref|^2, in sample order (deterministic).
+__global__ void __launch_bounds__(CHECK_THREADS) k_tc_check_fold(TcArgs a, uint32_t samples,
+                                                                 const double2 *parts,
+                                                                 double *chk) {
+  __shared__ double se[CHECK_THREADS], sr[CHECK_THREADS];
+  double e2 = 0, r2 = 0;
+  for (uint32_t j = threadIdx.x; j < samples; j += blockDim.x) {
+    double rx = 0, ry = 0;
+    for (uint32_t p = 0; p < CHECK_PARTS; ++p) {
+      const double2 v = parts[(size_t)j * CHECK_PARTS + p];
+      rx += v.x;
+      ry += v.y;
+    }
+    const double2 kk = a.kick[check_point(j, a.m, samples)];
     const double ex = kk.x - rx, ey = kk.y - ry;
-    atomicAdd(&chk[0], ex * ex + ey * ey);
-    atomicAdd(&chk[1], rx * rx + ry * ry);
+    e2 += ex * ex + ey * ey;
+    r2 += rx * rx + ry * ry;
+  }
+  se[threadIdx.x] = e2;
+  sr[threadIdx.x] = r2;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double te = 0, tr = 0;
+    for (uint32_t t = 0; t < blockDim.x; ++t) {
+      te += se[t];
+      tr += sr[t];
+    }
+    chk[0] = te;
+    chk[1] = tr;
   }
 }
 
@@ -1677,7 +1736,9 @@ int reserve(TcDev &d, uint32_t ncells, uint32_t m) {
   if (m > d.pcap) {
     const uint32_t cap = m + m / 4 + 1024;
     cudaFree(d.kick);
+    cudaFree(d.nearbuf);
     D3_CUDA_OK(cudaMalloc(&d.kick, (size_t)cap * sizeof(double2)));
+    D3_CUDA_OK(cudaMalloc(&d.nearbuf, (size_t)cap * sizeof(float2)));
     d.pcap = cap;
   }
   if (d.ccap > d.lcap) {
@@ -1733,7 +1794,7 @@ TcDev *tc_dev(FastScratch &s) {
 // M2L, P2L, L2L, leaf features, (the network, when `learned`), L2P / M2P and
 // the near field.
 int tc_order_pass(TcDev &d, TcArgs &g, const TcTabSet &ts, uint32_t tiles, bool learned,
-                  cudaStream_t st) {
+                  bool far_only, cudaStream_t st) {
   g.tab = ts.tab;
   g.wops = ts.wops;
   g.q = ts.p + 1;
@@ -1757,7 +1818,9 @@ int tc_order_pass(TcDev &d, TcArgs &g, const TcTabSet &ts, uint32_t tiles, bool 
     if (mlp_infer_tc(d.mlp_x, nleaf, d.mlp, d.mlp_y, g.status, st)) return -1;
   }
   cudaEventRecord(d.ev[7], st);
-  D3_LAUNCH(k_tc_near, lw, TC_THREADS, 0, st)(g, learned ? 1 : 0);
+  D3_LAUNCH(k_tc_near, lw, TC_THREADS, 0, st)(g, learned ? 1 : 0,
+                                               learned || far_only ? d.nearbuf : nullptr,
+                                               far_only ? 1 : 0);
   cudaEventRecord(d.ev[8], st);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
@@ -1777,6 +1840,7 @@ void fmm_tc_free(FastScratch &s) {
   cudaFree(d->pool); cudaFree(d->info); cudaFreeHost(d->h_info);
   cudaFree(d->feat); cudaFree(d->leaves); cudaFree(d->mlp_x); cudaFree(d->mlp_y);
   cudaFree(d->kick); cudaFree(d->chk); cudaFreeHost(d->h_chk); cudaFree(d->mlp);
+  cudaFree(d->chk_part); cudaFree(d->nearbuf);
   for (cudaEvent_t e : d->ev)
     if (e) cudaEventDestroy(e);
   delete static_cast<TcArgs *>(d->last_args);
@@ -1924,12 +1988,19 @@ int fmm_tc_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *st
   cudaEventRecord(d.ev[2], st);
   uint32_t tiles = 0;
   for (uint32_t q4 = 0; q4 < 4; ++q4) tiles += (d.h_info[TI_GROUP + q4] + TC_TILE - 1) / TC_TILE;
-  if (tc_order_pass(d, g, *main, tiles, learned, st)) return -1;
+  if (tc_order_pass(d, g, *main, tiles, learned, false, st)) return -1;
   if (!learned) return 1;
   // the sampled check against the FP64 direct sum
   const uint32_t samples = s.learn_samples ? s.learn_samples : 64;
-  if (cudaMemsetAsync(d.chk, 0, 2 * sizeof(double), st) != cudaSuccess) return -1;
-  D3_LAUNCH(k_tc_check, samples, CHECK_THREADS, 0, st)(g, samples, prm.dmin2, d.chk);
+  if (samples > d.chk_cap) {
+    cudaFree(d.chk_part);
+    d.chk_part = nullptr;
+    D3_CUDA_OK(cudaMalloc(&d.chk_part, (size_t)samples * CHECK_PARTS * sizeof(double2)));
+    d.chk_cap = samples;
+  }
+  D3_LAUNCH(k_tc_check, samples * CHECK_PARTS, CHECK_THREADS, 0, st)(g, samples, prm.dmin2,
+                                                                    d.chk_part);
+  D3_LAUNCH(k_tc_check_fold, 1, CHECK_THREADS, 0, st)(g, samples, d.chk_part, d.chk);
   if (cudaMemcpyAsync(d.h_chk, d.chk, 2 * sizeof(double), cudaMemcpyDeviceToHost, st) !=
           cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)
@@ -1947,7 +2018,7 @@ int fmm_tc_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *st
   TcTabSet *fb = tables_for(d, p, kappa, st);
   if (!fb) return -1;
   g.kick = nullptr;
-  if (tc_order_pass(d, g, *fb, tiles, false, st)) return -1;
+  if (tc_order_pass(d, g, *fb, tiles, false, true, st)) return -1;
   return 1;
 }
 

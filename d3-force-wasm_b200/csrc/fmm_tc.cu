@@ -22,28 +22,29 @@
 // Passes (one GPU, stream order):
 //   prepare  fmm_prepare (fmm.cu): keys, sort, gather, level-order cells.
 //   geom     per cell: level, integer coordinates, quadrant, child mask;
-//            the M2L target groups (one per quadrant).
-//   upward   FP64: P2M at leaves, M2M by the quadrant operators, level by
-//            level from the deepest; M' stored in FP64 and split into bf16
-//            hi + lo (x ~ hi + lo to 2^-17) for the tensor cores.
-//   lists    level by level from the root, a warp per cell: near cells (13
-//            at kappa 1.5), the M2L table (source per vector slot), and the
-//            adaptive lists: P2P leaves, coarse leaves (P2L), finer cells
-//            seen from a leaf (M2P).
+//            the leaf list and the M2L target groups (one per quadrant).
+//   lists    a launch per level from the root, a warp per cell: near cells
+//            (13 at kappa 1.5), the M2L table (source per vector slot), and
+//            the adaptive lists: P2P leaves, coarse leaves (P2L), finer
+//            cells seen from a leaf (M2P). Then one host read of the counts.
+//   upward   FP64, a thread per leaf: P2M, then M2M into each parent by the
+//            thread that completes it (arrival counters, no level
+//            barriers); M' stored in FP64 and split into bf16 hi + lo
+//            (x ~ hi + lo to 2^-17) for the tensor cores.
 //   m2l      tcgen05: a CTA per tile of 128 target cells of one quadrant
 //            group; per vector slot the 128 gathered source rows (A: 128 x
 //            32 bf16, hi and lo) times that vector's operator (B: 32 x 32,
 //            hi and lo) accumulate in TMEM as A_hi B_hi + A_hi B_lo +
-//            A_lo B_hi (BF16x3), FP32 accumulation; 4-stage smem ring with
-//            mbarriers, one thread issues the MMAs.
-//   p2l      coarse leaves' points into local expansions (FP32).
-//   down     L2L by the quadrant operators (FP32), level by level; at
-//            leaves L2P and M2P into a per-point far field.
-//   p2p      a warp per leaf: each source leaf's points staged in shared
-//            memory relative to the target leaf's centre, the shift taken in
-//            FP64 and the pair sums in FP32 (d3's pair formula, distanceMin
-//            clamp, hashed jiggle of hash.zig for coincident points); then
-//            v += far + near in FP64.
+//            A_lo B_hi (BF16x3), FP32 accumulation; cp.async gathers into a
+//            3-stage smem ring with mbarriers, one lane issues the MMAs.
+//   p2l      coarse leaves' points into local expansions (FP32 series).
+//   down     a thread per leaf: its ancestors' local expansions shifted to
+//            the leaf's centre (the L2L chain composed, FP32).
+//   near     a warp per leaf: the source leaves' points staged in shared
+//            memory relative to the leaf's first point (the shift in FP64,
+//            the pair sums in FP32: d3's pair formula, distanceMin clamp,
+//            hashed jiggle of hash.zig for coincident points); L2P and M2P
+//            per point; then v += near + far in FP64.
 
 #include <cmath>
 #include <cstdio>

@@ -1315,7 +1315,7 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int correct
                                                             float2 *nearbuf, int far_only) {
   __shared__ float4 stage[TC_WARPS][P2P_STAGE];
   __shared__ float lsh[TC_WARPS][TC_KN];
-  __shared__ float2 red[TC_WARPS][32];
+  __shared__ float4 red[TC_WARPS][32];
   const unsigned lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -1330,8 +1330,10 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int correct
     const TcCell A = a.cells[c];
     const uint32_t np = a.loff[(size_t)c * 8 + 1], op = a.loff[(size_t)c * 8];
     const uint32_t nw = a.loff[(size_t)c * 8 + 3], ow = a.loff[(size_t)c * 8 + 2];
-    // lane groups: W targets each, G = 32 / W groups (lanes past G W idle)
-    const uint32_t W = A.count <= 16 ? A.count : 32u, G = 32u / W;
+    // lane groups: a lane holds two targets (slots gl and W + gl of the
+    // round), W = ceil(count / 2) lanes a group, G = 32 / W groups (lanes
+    // past G W idle); a leaf of more than 64 points takes several rounds
+    const uint32_t W = A.count <= 64 ? (A.count + 1) / 2 : 32u, G = 32u / W;
     const uint32_t grp = lane / W, gl = lane % W;
     const bool in = grp < G;
     const double ox = a.px[A.first], oy = a.py[A.first];
@@ -1363,13 +1365,15 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int correct
       }
       careful = __any_sync(0xffffffffu, dup);
     }
+    const uint32_t end = A.first + A.count;
     float mx = 0, my = 0;  // the points' offsets from the centre (feature row)
-    for (uint32_t tb = A.first; tb < A.first + A.count; tb += W) {
-      const uint32_t ti = tb + gl;
-      const bool act = in && ti < A.first + A.count;
-      const float xi = act ? (float)(a.px[ti] - ox) : 0.f, yi = act ? (float)(a.py[ti] - oy) : 0.f;
-      const uint32_t gi = act ? a.perm[ti] : 0;
-      float ax0 = 0, ay0 = 0, ax1 = 0, ay1 = 0;
+    for (uint32_t tb = A.first; tb < end; tb += 2 * W) {
+      const uint32_t t0 = tb + gl, t1 = tb + W + gl;
+      const bool act0 = in && t0 < end, act1 = in && t1 < end;
+      const float x0 = act0 ? (float)(a.px[t0] - ox) : 0.f, y0 = act0 ? (float)(a.py[t0] - oy) : 0.f;
+      const float x1 = act1 ? (float)(a.px[t1] - ox) : 0.f, y1 = act1 ? (float)(a.py[t1] - oy) : 0.f;
+      const uint32_t g0 = act0 ? a.perm[t0] : 0, g1 = act1 ? a.perm[t1] : 0;
+      float ax0 = 0, ay0 = 0, ax1 = 0, ay1 = 0;  // targets 0 and 1
       for (uint32_t eb = 0; eb < (far_only ? 0u : np); eb += 32) {
         // this batch's source leaves: lane j holds leaf j's first point and
         // the running count before it
@@ -1399,49 +1403,57 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int correct
           uint32_t k = in ? grp : kn;
           if (!careful) {
 #pragma unroll 4
-            for (; k + G < kn; k += 2 * G) {
-              tc_pair_fast(sg[k], xi, yi, dmin2, ax0, ay0);
-              tc_pair_fast(sg[k + G], xi, yi, dmin2, ax1, ay1);
+            for (; k < kn; k += G) {
+              const float4 sv = sg[k];
+              tc_pair_fast(sv, x0, y0, dmin2, ax0, ay0);
+              tc_pair_fast(sv, x1, y1, dmin2, ax1, ay1);
             }
-            if (k < kn) tc_pair_fast(sg[k], xi, yi, dmin2, ax0, ay0);
           } else {
-            for (; k + G < kn; k += 2 * G) {
-              tc_pair(sg[k], xi, yi, ti, gi, dmin2, seed, a.perm, ax0, ay0);
-              tc_pair(sg[k + G], xi, yi, ti, gi, dmin2, seed, a.perm, ax1, ay1);
+            for (; k < kn; k += G) {
+              const float4 sv = sg[k];
+              tc_pair(sv, x0, y0, t0, g0, dmin2, seed, a.perm, ax0, ay0);
+              tc_pair(sv, x1, y1, t1, g1, dmin2, seed, a.perm, ax1, ay1);
             }
-            if (k < kn) tc_pair(sg[k], xi, yi, ti, gi, dmin2, seed, a.perm, ax0, ay0);
           }
         }
       }
       // the groups' sums, in group order
       __syncwarp();
-      red[wl][lane] = make_float2(ax0 + ax1, ay0 + ay1);
+      red[wl][lane] = make_float4(ax0, ay0, ax1, ay1);
       __syncwarp();
-      float vx = 0, vy = 0;
+      float v0x = 0, v0y = 0, v1x = 0, v1y = 0;
       if (grp == 0)
         for (uint32_t g2 = 0; g2 < G; ++g2) {
-          const float2 v = red[wl][g2 * W + gl];
-          vx += v.x;
-          vy += v.y;
+          const float4 v = red[wl][g2 * W + gl];
+          v0x += v.x;
+          v0y += v.y;
+          v1x += v.z;
+          v1y += v.w;
         }
-      if (act && grp == 0) {
-        if (far_only) {  // the near field of an earlier pass over the same lists
-          const float2 nv = nearbuf[ti];
-          vx = nv.x;
-          vy = nv.y;
-        } else if (nearbuf) {
-          nearbuf[ti] = make_float2(vx, vy);
-        }
-        float wr, wi;
-        const float2 f = tc_far(a, ti, cx, cy, inv_s, Lsh, nw, ow, wr, wi);
-        mx += wr;
-        my += wi;
-        const double kx = (double)vx + (double)f.x, ky = (double)vy + (double)f.y;
-        if (a.kick) {
-          a.kick[ti] = make_double2(kx, ky);
-        } else {
-          a.vx[gi] = a.vx[gi] + kx;
-          a.vy[gi] = a.vy[gi] + ky;
+      if (grp == 0) {
+        for (uint32_t h = 0; h < 2; ++h) {
+          const bool act = h ? act1 : act0;
+          if (!act) continue;
+          const uint32_t ti = h ? t1 : t0, gi = h ? g1 : g0;
+          float vx = h ? v1x : v0x, vy = h ? v1y : v0y;
+          if (far_only) {  // the near field of an earlier pass over the same lists
+            const float2 nv = nearbuf[ti];
+            vx = nv.x;
+            vy = nv.y;
+          } else if (nearbuf) {
+            nearbuf[ti] = make_float2(vx, vy);
+          }
+          float wr, wi;
+          const float2 f = tc_far(a, ti, cx, cy, inv_s, Lsh, nw, ow, wr, wi);
+          mx += wr;
+          my += wi;
+          const double kx = (double)vx + (double)f.x, ky = (double)vy + (double)f.y;
+          if (a.kick) {
+            a.kick[ti] = make_double2(kx, ky);
+          } else {
+            a.vx[gi] = a.vx[gi] + kx;
+            a.vy[gi] = a.vy[gi] + ky;
+          }
         }
       }
     }

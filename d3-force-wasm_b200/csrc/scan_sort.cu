@@ -96,26 +96,38 @@ void scan_u32(const uint32_t *in, uint32_t *out, uint32_t n, uint32_t *partials,
 
 // ---- radix sort -------------------------------------------------------------
 
-template <bool PART>
-__device__ inline uint32_t digit_of(uint64_t k, uint32_t v, int shift) {
-  if (PART) return v >> 31;
-  return (uint32_t)(k >> shift) & 255u;
+// Digit modes: BYTE, the key's byte at `shift` (256 buckets); PART_BYTE, the
+// value's bit 31 above the key's byte at `shift` (512 buckets: the partition
+// on bit 31 folded into the last byte pass, the same stable order as a byte
+// pass followed by a partition pass).
+enum : int { BYTE = 0, PART_BYTE = 1 };
+
+template <int MODE>
+__host__ __device__ constexpr unsigned buckets() {
+  return MODE == PART_BYTE ? 512u : 256u;
 }
 
-template <bool PART>
+template <int MODE>
+__device__ inline uint32_t digit_of(uint64_t k, uint32_t v, int shift) {
+  const uint32_t b = (uint32_t)(k >> shift) & 255u;
+  return MODE == PART_BYTE ? ((v >> 31) << 8) | b : b;
+}
+
+template <int MODE>
 __global__ void __launch_bounds__(SORT_THREADS) k_sort_hist(const uint64_t *keys, const uint32_t *vals,
                                                             uint32_t n, int shift, uint32_t *hist,
                                                             uint32_t tiles) {
-  __shared__ uint32_t h[256];
-  for (int d = threadIdx.x; d < 256; d += blockDim.x) h[d] = 0;
+  constexpr unsigned NB = buckets<MODE>();
+  __shared__ uint32_t h[NB];
+  for (unsigned d = threadIdx.x; d < NB; d += blockDim.x) h[d] = 0;
   __syncthreads();
   const size_t base = (size_t)blockIdx.x * SORT_TILE;
   for (unsigned k = threadIdx.x; k < SORT_TILE; k += blockDim.x) {
     size_t i = base + k;
-    if (i < n) atomicAdd(&h[digit_of<PART>(keys[i], vals[i], shift)], 1u);
+    if (i < n) atomicAdd(&h[digit_of<MODE>(keys[i], vals[i], shift)], 1u);
   }
   __syncthreads();
-  for (int d = threadIdx.x; d < 256; d += blockDim.x) hist[(size_t)d * tiles + blockIdx.x] = h[d];
+  for (unsigned d = threadIdx.x; d < NB; d += blockDim.x) hist[(size_t)d * tiles + blockIdx.x] = h[d];
 }
 
 // Stable scatter of one tile of SORT_TILE keys: warp w takes the tile's
@@ -125,17 +137,18 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_hist(const uint64_t *keys
 // per-digit offsets (tile offset from the scanned histograms + the earlier
 // warps' counts), and every key is written once. Two block barriers per
 // tile.
-template <bool PART>
+template <int MODE>
 __global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(const uint64_t *keys, const uint32_t *vals,
                                                                uint64_t *okeys, uint32_t *ovals,
                                                                uint32_t n, int shift,
                                                                const uint32_t *offsets,
                                                                uint32_t tiles) {
+  constexpr unsigned NB = buckets<MODE>();
   constexpr unsigned WARPS = SORT_THREADS / 32, PER = SORT_TILE / SORT_THREADS;
-  __shared__ uint32_t wh[WARPS][256];
+  __shared__ uint32_t wh[WARPS][NB];
   const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1;
-  for (unsigned d = threadIdx.x; d < WARPS * 256; d += blockDim.x) (&wh[0][0])[d] = 0;
+  for (unsigned d = threadIdx.x; d < WARPS * NB; d += blockDim.x) (&wh[0][0])[d] = 0;
   const size_t wbase = (size_t)blockIdx.x * SORT_TILE + (size_t)warp * 32 * PER;
   uint64_t k[PER];
   uint32_t v[PER], dg[PER], rk[PER];
@@ -149,7 +162,7 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(const uint64_t *k
 #pragma unroll
   for (unsigned r = 0; r < PER; ++r) {
     const bool valid = wbase + r * 32 + lane < n;
-    const uint32_t d = valid ? digit_of<PART>(k[r], v[r], shift) : 256u + lane;  // never matches
+    const uint32_t d = valid ? digit_of<MODE>(k[r], v[r], shift) : NB + lane;  // never matches
     const unsigned peers = __match_any_sync(0xffffffffu, d);
     const unsigned below = __popc(peers & lt);
     const uint32_t cnt = valid ? wh[warp][d] : 0;
@@ -160,7 +173,7 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(const uint64_t *k
     rk[r] = cnt + below;
   }
   __syncthreads();
-  for (unsigned d = threadIdx.x; d < 256; d += blockDim.x) {
+  for (unsigned d = threadIdx.x; d < NB; d += blockDim.x) {
     uint32_t run = offsets[(size_t)d * tiles + blockIdx.x];
 #pragma unroll
     for (unsigned w = 0; w < WARPS; ++w) {
@@ -179,13 +192,14 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(const uint64_t *k
     }
 }
 
-template <bool PART>
+template <int MODE>
 static void sort_pass(const uint64_t *ik, const uint32_t *iv, uint64_t *ok, uint32_t *ov, uint32_t n,
                       int shift, const SortScratch &s, cudaStream_t st) {
   uint32_t tiles = (n + SORT_TILE - 1) / SORT_TILE;
-  D3_LAUNCH(k_sort_hist<PART>, tiles, SORT_THREADS, 0, st)(ik, iv, n, shift, s.hist, tiles);
-  scan_u32(s.hist, s.hist, 256 * tiles, s.partials, nullptr, st);
-  D3_LAUNCH(k_sort_scatter<PART>, tiles, SORT_THREADS, 0, st)(ik, iv, ok, ov, n, shift, s.hist, tiles);
+  D3_LAUNCH(k_sort_hist<MODE>, tiles, SORT_THREADS, 0, st)(ik, iv, n, shift, s.hist, tiles);
+  scan_u32(s.hist, s.hist, buckets<MODE>() * tiles, s.partials, nullptr, st);
+  D3_LAUNCH(k_sort_scatter<MODE>, tiles, SORT_THREADS, 0, st)(ik, iv, ok, ov, n, shift, s.hist,
+                                                             tiles);
 }
 
 void radix_sort_u64(uint64_t *keys, uint32_t *vals, uint32_t n, int byte_lo, int byte_hi,
@@ -194,12 +208,9 @@ void radix_sort_u64(uint64_t *keys, uint32_t *vals, uint32_t n, int byte_lo, int
   uint64_t *ak = keys, *bk = s.keys_tmp;
   uint32_t *av = vals, *bv = s.vals_tmp;
   for (int b = byte_lo; b < byte_hi; ++b) {
-    sort_pass<false>(ak, av, bk, bv, n, 8 * b, s, st);
-    uint64_t *tk = ak; ak = bk; bk = tk;
-    uint32_t *tv = av; av = bv; bv = tv;
-  }
-  if (partition_hi_bit) {
-    sort_pass<true>(ak, av, bk, bv, n, 0, s, st);
+    // the partition on bit 31 rides on the last byte pass
+    if (partition_hi_bit && b + 1 == byte_hi) sort_pass<PART_BYTE>(ak, av, bk, bv, n, 8 * b, s, st);
+    else sort_pass<BYTE>(ak, av, bk, bv, n, 8 * b, s, st);
     uint64_t *tk = ak; ak = bk; bk = tk;
     uint32_t *tv = av; av = bv; bv = tv;
   }

@@ -94,13 +94,14 @@ constexpr unsigned SORT_TILE = 2048;
 constexpr unsigned SORT_THREADS = 256;
 
 // Stable sort of (keys, vals)[0..n) by key bytes [byte_lo, byte_hi), then (if
-// `partition_hi_bit`) a stable partition on bit 31 of the value, zeros first.
-// Results end in keys/vals. Scratch: keys_tmp, vals_tmp (n each) and hist of
-// at least 256 * tiles + 1 words plus scan partials.
+// `partition_hi_bit`) a stable partition on bit 31 of the value, zeros first
+// (folded into the last byte pass as a 9-bit digit). Results end in
+// keys/vals. Scratch: keys_tmp, vals_tmp (n each) and hist of at least
+// 512 * tiles + 1 words plus scan partials.
 struct SortScratch {
   uint64_t *keys_tmp;
   uint32_t *vals_tmp;
-  uint32_t *hist;      // 256 * tiles
+  uint32_t *hist;      // 512 * tiles
   uint32_t *partials;  // scan partials
 };
 void radix_sort_u64(uint64_t *keys, uint32_t *vals, uint32_t n, int byte_lo, int byte_hi,
@@ -109,7 +110,7 @@ void radix_sort_u64(uint64_t *keys, uint32_t *vals, uint32_t n, int byte_lo, int
 inline size_t sort_hist_words(uint32_t n) {
   size_t tiles = (n + SORT_TILE - 1) / SORT_TILE;
   if (!tiles) tiles = 1;
-  return 256 * tiles + 1;
+  return 512 * tiles + 1;
 }
 inline size_t scan_partial_words(size_t n) { return blocks_for(n, SCAN_BLOCK * 4) + 2; }
 

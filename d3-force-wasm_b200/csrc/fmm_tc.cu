@@ -138,6 +138,7 @@ struct TcDev {
   double2 *chk_part = nullptr;               // the check's partial direct sums
   uint32_t chk_cap = 0;                      // samples chk_part holds
   float2 *nearbuf = nullptr;                 // per sorted point: the learned pass's near field
+  uint32_t *leafof = nullptr;                // per sorted point: its leaf (learned pass)
   float *mlp = nullptr;              // installed network parameters (device)
   uint32_t ncells_last = 0;
   uint32_t hold = 0;                 // ticks left on the fallback after a failed check
@@ -163,6 +164,7 @@ struct TcArgs {
   size_t pool_cap;
   float *feat, *mlp_x, *mlp_y;
   uint32_t *leaves;
+  uint32_t *leafof;  // per sorted point: its leaf (the learned pass's features write it)
   double2 *kick;  // non-null: the many-body kick goes here instead of into vx, vy
   double *vx, *vy;
   uint32_t *info;
@@ -1182,6 +1184,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_tc_features(TcArgs a) {
     for (uint32_t k = C.first + lane; k < C.first + C.count; k += 32) {
       mx += (float)((a.ux[k] - cx) * inv_s);
       my += (float)((a.uy[k] - cy) * inv_s);
+      a.leafof[k] = c;
     }
     for (int o = 16; o > 0; o >>= 1) {
       mx += __shfl_xor_sync(0xffffffffu, mx, o);
@@ -1308,11 +1311,10 @@ __device__ __forceinline__ float2 tc_far(const TcArgs &a, uint32_t k, double cx,
 // expansion in shared memory; `corrected` adds the learned form's network
 // output to L'_0 (sc * y / LEARN_TARGET_SCALE), else the leaf's feature row
 // is written. v += near + far in FP64 (or the kick to `kick`). `nearbuf`:
-// the near field is also stored there per point; with `far_only` it is read
-// back instead of computed (the learned form's fallback reuses the near
-// field of its order-4 pass: it does not depend on the order).
+// the near field is also stored there per point (the learned form's
+// fallback, k_tc_far_only, reuses it: it does not depend on the order).
 __global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int corrected,
-                                                            float2 *nearbuf, int far_only) {
+                                                            float2 *nearbuf) {
   __shared__ float4 stage[TC_WARPS][P2P_STAGE];
   __shared__ float lsh[TC_WARPS][TC_KN];
   __shared__ float4 red[TC_WARPS][32];
@@ -1354,7 +1356,7 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int correct
     // whose points (in its FP32 local coordinates) hold a coincident pair, or
     // that spans several rounds of targets, takes the careful pair.
     bool careful = A.count > 32;
-    if (!careful && !far_only) {
+    if (!careful) {
       const bool mine = lane < A.count;
       const float px = mine ? (float)(a.px[A.first + lane] - ox) : 0.f;
       const float py = mine ? (float)(a.py[A.first + lane] - oy) : 0.f;
@@ -1374,7 +1376,7 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int correct
       const float x1 = act1 ? (float)(a.px[t1] - ox) : 0.f, y1 = act1 ? (float)(a.py[t1] - oy) : 0.f;
       const uint32_t g0 = act0 ? a.perm[t0] : 0, g1 = act1 ? a.perm[t1] : 0;
       float ax0 = 0, ay0 = 0, ax1 = 0, ay1 = 0;  // targets 0 and 1
-      for (uint32_t eb = 0; eb < (far_only ? 0u : np); eb += 32) {
+      for (uint32_t eb = 0; eb < np; eb += 32) {
         // this batch's source leaves: lane j holds leaf j's first point and
         // the running count before it
         const uint32_t ne = min(32u, np - eb);
@@ -1436,13 +1438,7 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int correct
           if (!act) continue;
           const uint32_t ti = h ? t1 : t0, gi = h ? g1 : g0;
           float vx = h ? v1x : v0x, vy = h ? v1y : v0y;
-          if (far_only) {  // the near field of an earlier pass over the same lists
-            const float2 nv = nearbuf[ti];
-            vx = nv.x;
-            vy = nv.y;
-          } else if (nearbuf) {
-            nearbuf[ti] = make_float2(vx, vy);
-          }
+          if (nearbuf) nearbuf[ti] = make_float2(vx, vy);
           float wr, wi;
           const float2 f = tc_far(a, ti, cx, cy, inv_s, Lsh, nw, ow, wr, wi);
           mx += wr;
@@ -1465,6 +1461,26 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int correct
       if (lane == 0) feature_row(a, c, A, a.lco + (size_t)c * TC_KN, mx, my);
     }
   }
+}
+
+// The learned form's fallback, a thread per point: the order-8 far field of
+// its leaf (tc_far, the local expansion read from the cell's row) plus the
+// near field that the order-4 pass stored, v += near + far in FP64.
+__global__ void __launch_bounds__(TC_THREADS) k_tc_far_only(TcArgs a, const float2 *nearbuf) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= a.m) return;
+  const uint32_t c = a.leafof[k];
+  const TcCell C = a.cells[c];
+  double cx, cy;
+  cell_centre(C, cx, cy);
+  const double inv_s = pow2((int)C.level);
+  const uint32_t nw = a.loff[(size_t)c * 8 + 3], ow = a.loff[(size_t)c * 8 + 2];
+  float wr, wi;
+  const float2 f = tc_far(a, k, cx, cy, inv_s, a.lco + (size_t)c * TC_KN, nw, ow, wr, wi);
+  const float2 nv = nearbuf[k];
+  const uint32_t gi = a.perm[k];
+  a.vx[gi] = a.vx[gi] + ((double)nv.x + (double)f.x);
+  a.vy[gi] = a.vy[gi] + ((double)nv.y + (double)f.y);
 }
 
 // ---- the learned form's sampled check -----------------------------------------------------------
@@ -1752,6 +1768,8 @@ int reserve(TcDev &d, uint32_t ncells, uint32_t m) {
     cudaFree(d.nearbuf);
     D3_CUDA_OK(cudaMalloc(&d.kick, (size_t)cap * sizeof(double2)));
     D3_CUDA_OK(cudaMalloc(&d.nearbuf, (size_t)cap * sizeof(float2)));
+    cudaFree(d.leafof);
+    D3_CUDA_OK(cudaMalloc(&d.leafof, (size_t)cap * sizeof(uint32_t)));
     d.pcap = cap;
   }
   if (d.ccap > d.lcap) {
@@ -1831,9 +1849,10 @@ int tc_order_pass(TcDev &d, TcArgs &g, const TcTabSet &ts, uint32_t tiles, bool 
     if (mlp_infer_tc(d.mlp_x, nleaf, d.mlp, d.mlp_y, g.status, st)) return -1;
   }
   cudaEventRecord(d.ev[7], st);
-  D3_LAUNCH(k_tc_near, lw, TC_THREADS, 0, st)(g, learned ? 1 : 0,
-                                               learned || far_only ? d.nearbuf : nullptr,
-                                               far_only ? 1 : 0);
+  if (far_only)
+    D3_LAUNCH(k_tc_far_only, blocks_for(g.m, TC_THREADS), TC_THREADS, 0, st)(g, d.nearbuf);
+  else
+    D3_LAUNCH(k_tc_near, lw, TC_THREADS, 0, st)(g, learned ? 1 : 0, learned ? d.nearbuf : nullptr);
   cudaEventRecord(d.ev[8], st);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
@@ -1853,7 +1872,7 @@ void fmm_tc_free(FastScratch &s) {
   cudaFree(d->pool); cudaFree(d->info); cudaFreeHost(d->h_info);
   cudaFree(d->feat); cudaFree(d->leaves); cudaFree(d->mlp_x); cudaFree(d->mlp_y);
   cudaFree(d->kick); cudaFree(d->chk); cudaFreeHost(d->h_chk); cudaFree(d->mlp);
-  cudaFree(d->chk_part); cudaFree(d->nearbuf);
+  cudaFree(d->chk_part); cudaFree(d->nearbuf); cudaFree(d->leafof);
   for (cudaEvent_t e : d->ev)
     if (e) cudaEventDestroy(e);
   delete static_cast<TcArgs *>(d->last_args);
@@ -1956,6 +1975,7 @@ int fmm_tc_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *st
   g.mco = d.mco; g.mbf = d.mbf; g.lco = d.lco;
   g.near = d.near; g.m2l = d.m2l; g.groups = d.groups; g.loff = d.loff;
   g.feat = d.feat; g.leaves = d.leaves; g.mlp_x = d.mlp_x; g.mlp_y = d.mlp_y;
+  g.leafof = d.leafof;
   g.kick = learned ? d.kick : nullptr;
   g.vx = a.vx; g.vy = a.vy;
   g.info = d.info;

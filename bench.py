@@ -415,10 +415,12 @@ def learned_1m(pkg, core, torch, flush_l2):
         # the learned form: two whole check cycles (a checked tick and the
         # `hold` ticks after a failed check), so the checks' cost is in the mean
         timed = 2 * (LEARN_HOLD + 1) if form == "learned" else 10
-        times = []
+        times, checked = [], []
         for _ in range(timed):
             flush_l2()
+            c0 = core.sim_stat(sim.ctx.h, 50)
             times.append(sim.device_ticks(1))
+            checked.append(core.sim_stat(sim.ctx.h, 50) > c0)
         sim.device_end()
         stats = [core.sim_stat(sim.ctx.h, 50 + k) for k in range(3)]
         sim.close()
@@ -432,7 +434,11 @@ def learned_1m(pkg, core, torch, flush_l2):
         if form == "learned":
             out[key].update({"checks": stats[0], "fallbacks": stats[1],
                              "last_sampled_rms": stats[2], "hold_ticks": LEARN_HOLD,
-                             "ticks_run": 3 + timed, "ticks_timed": timed})
+                             "ticks_run": 3 + timed, "ticks_timed": timed,
+                             "ms_checked_ticks": [round(t, 4) for t, c in zip(times, checked) if c],
+                             "ms_other_ticks_mean": round(
+                                 sum(t for t, c in zip(times, checked) if not c)
+                                 / max(1, sum(1 for c in checked if not c)), 4)})
     out["learned"]["speedup_vs_plain_fp64_order8"] = round(
         out["plain"]["ms_per_tick"] / out["learned"]["ms_per_tick"], 3)
     return out

@@ -86,20 +86,41 @@ int fast_link_build(FastLink &c, const uint32_t *src, const uint32_t *tgt, uint3
   }
   for (uint32_t i = 0; i < n; ++i) row[i] = row[i + 1];
   row[n] = 2 * m;
+  std::vector<uint32_t> other(adj.size(), 0);
+  for (size_t a = 0; a < 2 * (size_t)m; ++a) {
+    const uint32_t e = adj[a] & ~TARGET_BIT;
+    other[a] = (adj[a] & TARGET_BIT) ? src[e] : tgt[e];
+  }
   fast_link_free(c);
   D3_CUDA_OK(cudaMalloc(&c.row, row.size() * 4));
   D3_CUDA_OK(cudaMalloc(&c.adj, adj.size() * 4));
+  D3_CUDA_OK(cudaMalloc(&c.other, other.size() * 4));
+  D3_CUDA_OK(cudaMalloc(&c.scal, 3 * adj.size() * sizeof(double)));
   D3_CUDA_OK(cudaMemcpy(c.row, row.data(), row.size() * 4, cudaMemcpyHostToDevice));
   D3_CUDA_OK(cudaMemcpy(c.adj, adj.data(), adj.size() * 4, cudaMemcpyHostToDevice));
+  D3_CUDA_OK(cudaMemcpy(c.other, other.data(), other.size() * 4, cudaMemcpyHostToDevice));
   c.n = n;
   c.m = m;
+  c.gathered = false;
   return 0;
 }
 
 void fast_link_free(FastLink &c) {
   cudaFree(c.row);
   cudaFree(c.adj);
+  cudaFree(c.other);
+  cudaFree(c.scal);
   c = FastLink();
+}
+
+// scal[plane * 2m + a] = the distance / strength / bias of entry a's link.
+__global__ void k_link_gather(LinkArrays l, const uint32_t *adj, uint32_t entries, double *scal) {
+  const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= entries) return;
+  const uint32_t e = adj[a] & ~TARGET_BIT;
+  scal[a] = l.distance[e];
+  scal[(size_t)entries + a] = l.strength[e];
+  scal[2 * (size_t)entries + a] = l.bias[e];
 }
 
 __global__ void k_shift2(const double *x, const double *y, const double *vx, const double *vy,
@@ -110,14 +131,16 @@ __global__ void k_shift2(const double *x, const double *y, const double *vx, con
   py[i] = y[i] + vy[i];
 }
 
-// link_fast.zig:60-99. A thread per node over its adjacency, four links at a
-// time: the loads of the four are issued by dependency level (entries, then
-// the other endpoints and the link's scalars, then their positions), and
-// the four are then applied in adjacency order, as the serial loop does.
+// link_fast.zig:60-99. A thread per node over its adjacency in CSR order;
+// the entries' other endpoints and link scalars are read from the
+// adjacency-ordered copies (contiguous per node), four entries at a time
+// with the position loads issued together, and applied in adjacency order as
+// the serial loop does.
 constexpr uint32_t LINK_BATCH = 4;
 
 __global__ void k_link_sweep(const double *px, const double *py, double *vxs, double *vys,
-                             LinkArrays l, const uint32_t *row, const uint32_t *adj, double alpha,
+                             const uint32_t *row, const uint32_t *adj, const uint32_t *other,
+                             const double *scal, uint32_t entries, double alpha,
                              const double *seedp, uint32_t n) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -126,29 +149,20 @@ __global__ void k_link_sweep(const double *px, const double *py, double *vxs, do
   const double pxi = px[i], pyi = py[i];
   const uint32_t a1 = row[i + 1];
   for (uint32_t a0 = row[i]; a0 < a1; a0 += LINK_BATCH) {
-    uint32_t ent[LINK_BATCH], oth[LINK_BATCH];
-    double dist[LINK_BATCH], str[LINK_BATCH], bias[LINK_BATCH], xj[LINK_BATCH], yj[LINK_BATCH];
-#pragma unroll
-    for (uint32_t k = 0; k < LINK_BATCH; ++k)
-      if (a0 + k < a1) ent[k] = adj[a0 + k];
+    uint32_t ent[LINK_BATCH];
+    double xj[LINK_BATCH], yj[LINK_BATCH];
 #pragma unroll
     for (uint32_t k = 0; k < LINK_BATCH; ++k)
       if (a0 + k < a1) {
-        const uint32_t e = ent[k] & ~TARGET_BIT;
-        oth[k] = (ent[k] & TARGET_BIT) ? l.source[e] : l.target[e];
-        dist[k] = l.distance[e];
-        str[k] = l.strength[e];
-        bias[k] = l.bias[e];
-      }
-#pragma unroll
-    for (uint32_t k = 0; k < LINK_BATCH; ++k)
-      if (a0 + k < a1) {
-        xj[k] = px[oth[k]];
-        yj[k] = py[oth[k]];
+        ent[k] = adj[a0 + k];
+        const uint32_t j = other[a0 + k];
+        xj[k] = px[j];
+        yj[k] = py[j];
       }
 #pragma unroll
     for (uint32_t k = 0; k < LINK_BATCH; ++k) {
-      if (a0 + k >= a1) break;
+      const uint32_t a = a0 + k;
+      if (a >= a1) break;
       const uint32_t e = ent[k] & ~TARGET_BIT;
       const bool is_target = (ent[k] & TARGET_BIT) != 0;
       double x = is_target ? pxi - xj[k] : xj[k] - pxi;
@@ -156,10 +170,10 @@ __global__ void k_link_sweep(const double *px, const double *py, double *vxs, do
       if (x == 0 || x != x) x = hash_jiggle(seed, e, 0, 0);
       if (y == 0 || y != y) y = hash_jiggle(seed, e, 0, 1);
       double len = sqrt(x * x + y * y);
-      len = (len - dist[k]) / len * alpha * str[k];
+      len = (len - scal[a]) / len * alpha * scal[(size_t)entries + a];
       x *= len;
       y *= len;
-      const double b = bias[k];
+      const double b = scal[2 * (size_t)entries + a];
       if (is_target) {
         vx -= x * b;
         vy -= y * b;
@@ -173,13 +187,18 @@ __global__ void k_link_sweep(const double *px, const double *py, double *vxs, do
   vys[i] = vy;
 }
 
-void fast_link(const NodeArrays &a, const LinkArrays &l, const FastLink &c, double alpha,
+void fast_link(const NodeArrays &a, const LinkArrays &l, FastLink &c, double alpha,
                double iterations, const double *seed, cudaStream_t st) {
-  const uint32_t n = a.n;
+  const uint32_t n = a.n, entries = 2 * c.m;
+  if (!c.gathered && entries) {
+    D3_LAUNCH(k_link_gather, blocks_for(entries, 256), 256, 0, st)(l, c.adj, entries, c.scal);
+    c.gathered = true;
+  }
   for (double k = 0; k < iterations; k += 1) {
     D3_LAUNCH(k_shift2, blocks_for(n, 256), 256, 0, st)(a.x, a.y, a.vx, a.vy, a.px, a.py, n);
-    D3_LAUNCH(k_link_sweep, blocks_for(n, 128), 128, 0, st)(a.px, a.py, a.vx, a.vy, l, c.row, c.adj, alpha,
-                                                     seed, n);
+    D3_LAUNCH(k_link_sweep, blocks_for(n, 128), 128, 0, st)(a.px, a.py, a.vx, a.vy, c.row, c.adj,
+                                                           c.other, c.scal, entries, alpha, seed,
+                                                           n);
   }
 }
 

@@ -40,13 +40,20 @@ void set_seed(double *seed, double value, cudaStream_t st);
 
 // link_fast.zig: CSR adjacency (edge id, TARGET_BIT on the target's entry),
 // rows filled from the back so each row lists its edges in descending order.
+// The fast link's adjacency (CSR over nodes, link_fast.zig:105-130) and, in
+// the same adjacency order, each entry's other endpoint and its link's
+// distance, strength and bias (copied from the link arrays once per
+// rebuild), so a node's links are read contiguously.
 struct FastLink {
   uint32_t n = 0, m = 0;
   uint32_t *row = nullptr, *adj = nullptr;
+  uint32_t *other = nullptr;   // per adjacency entry
+  double *scal = nullptr;      // per adjacency entry: distance, strength, bias planes
+  bool gathered = false;       // scal holds the current link arrays
 };
 int fast_link_build(FastLink &c, const uint32_t *src, const uint32_t *tgt, uint32_t m, uint32_t n);
 void fast_link_free(FastLink &c);
-void fast_link(const NodeArrays &a, const LinkArrays &l, const FastLink &c, double alpha,
+void fast_link(const NodeArrays &a, const LinkArrays &l, FastLink &c, double alpha,
                double iterations, const double *seed, cudaStream_t st);
 
 // grid.zig:198-286

@@ -136,7 +136,7 @@ struct TcDev {
   double2 *kick = nullptr;           // per sorted point: the many-body kick
   double *chk = nullptr, *h_chk = nullptr;   // sampled check: sum err^2, sum ref^2
   double2 *chk_part = nullptr;               // the check's partial direct sums
-  uint32_t chk_cap = 0;                      // samples chk_part holds
+  uint32_t chk_cap = 0;                      // entries chk_part holds
   float2 *nearbuf = nullptr;                 // per sorted point: the learned pass's near field
   uint32_t *leafof = nullptr;                // per sorted point: its leaf (learned pass)
   float *mlp = nullptr;              // installed network parameters (device)
@@ -1485,11 +1485,14 @@ __global__ void __launch_bounds__(TC_THREADS) k_tc_far_only(TcArgs a, const floa
 
 // ---- the learned form's sampled check -----------------------------------------------------------
 
-// The sampled check's direct sums, spread over the GPU: block (j, part)
-// sums d3's pair formula in FP64 over its share of the points for sampled
-// point j (sorted order, spread evenly; coincident pairs and the point
-// itself add nothing; distanceMin's clamp) into part_out[(j * parts + part)].
-constexpr uint32_t CHECK_PARTS = 32;
+// The sampled check's direct sums, spread over the GPU: block `part` holds
+// CHECK_THREADS x CHECK_PTS consecutive points in registers (each thread
+// CHECK_PTS of them) and, for every sampled point j (sorted order, spread
+// evenly), sums d3's pair formula in FP64 over them (coincident pairs and
+// the point itself add nothing; distanceMin's clamp) into
+// part_out[j * parts + part]. Each point is read once.
+constexpr uint32_t CHECK_PTS = 16;
+constexpr uint32_t CHECK_MAX_SAMPLES = 1024;
 
 __device__ __forceinline__ uint32_t check_point(uint32_t j, uint32_t m, uint32_t samples) {
   return (uint32_t)(((2ull * j + 1) * m) / (2ull * samples));
@@ -1497,38 +1500,47 @@ __device__ __forceinline__ uint32_t check_point(uint32_t j, uint32_t m, uint32_t
 
 __global__ void __launch_bounds__(CHECK_THREADS) k_tc_check(TcArgs a, uint32_t samples,
                                                             double dmin2, double2 *part_out) {
-  __shared__ double sx[CHECK_THREADS / 32], sy[CHECK_THREADS / 32];
-  const uint32_t j = blockIdx.x / CHECK_PARTS, part = blockIdx.x % CHECK_PARTS;
-  const uint32_t k = check_point(j, a.m, samples);
-  const double xi = a.px[k], yi = a.py[k];
-  const uint32_t i0 = (uint32_t)((uint64_t)a.m * part / CHECK_PARTS);
-  const uint32_t i1 = (uint32_t)((uint64_t)a.m * (part + 1) / CHECK_PARTS);
-  double vx = 0, vy = 0;
-  for (uint32_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
-    const double dx = a.px[i] - xi, dy = a.py[i] - yi;
-    double l = dx * dx + dy * dy;
-    if (!(l > 0)) continue;
-    if (l < dmin2) l = sqrt(dmin2 * l);
-    const double w = a.ps[i] / l;
-    vx += dx * w;
-    vy += dy * w;
+  __shared__ double2 red[CHECK_THREADS / 32];
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const size_t base = (size_t)blockIdx.x * CHECK_THREADS * CHECK_PTS;
+  double px[CHECK_PTS], py[CHECK_PTS], ps[CHECK_PTS];
+#pragma unroll
+  for (uint32_t r = 0; r < CHECK_PTS; ++r) {
+    const size_t i = base + (size_t)r * CHECK_THREADS + threadIdx.x;
+    const bool ok = i < a.m;
+    px[r] = ok ? a.px[i] : 0.0;
+    py[r] = ok ? a.py[i] : 0.0;
+    ps[r] = ok ? a.ps[i] : 0.0;  // a missing point adds 0 (and l = 0 is skipped)
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    vx += __shfl_xor_sync(0xffffffffu, vx, o);
-    vy += __shfl_xor_sync(0xffffffffu, vy, o);
-  }
-  if ((threadIdx.x & 31) == 0) {
-    sx[threadIdx.x >> 5] = vx;
-    sy[threadIdx.x >> 5] = vy;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double rx = 0, ry = 0;
-    for (uint32_t w = 0; w < CHECK_THREADS / 32; ++w) {
-      rx += sx[w];
-      ry += sy[w];
+  for (uint32_t j = 0; j < samples; ++j) {
+    const uint32_t k = check_point(j, a.m, samples);
+    const double xi = a.px[k], yi = a.py[k];
+    double vx = 0, vy = 0;
+#pragma unroll
+    for (uint32_t r = 0; r < CHECK_PTS; ++r) {
+      const double dx = px[r] - xi, dy = py[r] - yi;
+      double l = dx * dx + dy * dy;
+      if (!(l > 0)) continue;
+      if (l < dmin2) l = sqrt(dmin2 * l);
+      const double w = ps[r] / l;
+      vx += dx * w;
+      vy += dy * w;
     }
-    part_out[blockIdx.x] = make_double2(rx, ry);
+    for (int o = 16; o > 0; o >>= 1) {
+      vx += __shfl_xor_sync(0xffffffffu, vx, o);
+      vy += __shfl_xor_sync(0xffffffffu, vy, o);
+    }
+    if (lane == 0) red[warp] = make_double2(vx, vy);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double rx = 0, ry = 0;
+      for (uint32_t w = 0; w < CHECK_THREADS / 32; ++w) {
+        rx += red[w].x;
+        ry += red[w].y;
+      }
+      part_out[(size_t)j * gridDim.x + blockIdx.x] = make_double2(rx, ry);
+    }
+    __syncthreads();
   }
 }
 
@@ -1536,14 +1548,15 @@ __global__ void __launch_bounds__(CHECK_THREADS) k_tc_check(TcArgs a, uint32_t s
 // kick the pass put in kick[k]; chk[0] = sum |kick - ref|^2, chk[1] =
 // sum |ref|^2, in sample order (deterministic).
 __global__ void __launch_bounds__(CHECK_THREADS) k_tc_check_fold(TcArgs a, uint32_t samples,
-                                                                 const double2 *parts,
+                                                                 uint32_t parts,
+                                                                 const double2 *part_in,
                                                                  double *chk) {
   __shared__ double se[CHECK_THREADS], sr[CHECK_THREADS];
   double e2 = 0, r2 = 0;
   for (uint32_t j = threadIdx.x; j < samples; j += blockDim.x) {
     double rx = 0, ry = 0;
-    for (uint32_t p = 0; p < CHECK_PARTS; ++p) {
-      const double2 v = parts[(size_t)j * CHECK_PARTS + p];
+    for (uint32_t p = 0; p < parts; ++p) {
+      const double2 v = part_in[(size_t)j * parts + p];
       rx += v.x;
       ry += v.y;
     }
@@ -2024,16 +2037,17 @@ int fmm_tc_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *st
   if (tc_order_pass(d, g, *main, tiles, learned, false, st)) return -1;
   if (!learned) return 1;
   // the sampled check against the FP64 direct sum
-  const uint32_t samples = s.learn_samples ? s.learn_samples : 64;
-  if (samples > d.chk_cap) {
+  uint32_t samples = s.learn_samples ? s.learn_samples : 64;
+  if (samples > CHECK_MAX_SAMPLES) samples = CHECK_MAX_SAMPLES;
+  const uint32_t parts = blocks_for(pr.m, CHECK_THREADS * CHECK_PTS);
+  if ((size_t)samples * parts > d.chk_cap) {
     cudaFree(d.chk_part);
     d.chk_part = nullptr;
-    D3_CUDA_OK(cudaMalloc(&d.chk_part, (size_t)samples * CHECK_PARTS * sizeof(double2)));
-    d.chk_cap = samples;
+    D3_CUDA_OK(cudaMalloc(&d.chk_part, (size_t)samples * parts * sizeof(double2)));
+    d.chk_cap = samples * parts;
   }
-  D3_LAUNCH(k_tc_check, samples * CHECK_PARTS, CHECK_THREADS, 0, st)(g, samples, prm.dmin2,
-                                                                    d.chk_part);
-  D3_LAUNCH(k_tc_check_fold, 1, CHECK_THREADS, 0, st)(g, samples, d.chk_part, d.chk);
+  D3_LAUNCH(k_tc_check, parts, CHECK_THREADS, 0, st)(g, samples, prm.dmin2, d.chk_part);
+  D3_LAUNCH(k_tc_check_fold, 1, CHECK_THREADS, 0, st)(g, samples, parts, d.chk_part, d.chk);
   if (cudaMemcpyAsync(d.h_chk, d.chk, 2 * sizeof(double), cudaMemcpyDeviceToHost, st) !=
           cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)

@@ -209,8 +209,17 @@ class Slot:
         C.check(ctx.core.force_run(ctx.h, self.fh, alpha))
 
 
+# Bumped by every attribute a core force's methods set (its scalars, its
+# nodes): Simulation.tick pushes the forces' scalars only when it moved.
+_FORCE_GEN = [0]
+
+
 class Force:
     kind = None
+
+    def __setattr__(self, name, value):
+        object.__setattr__(self, name, value)
+        _FORCE_GEN[0] += 1
 
     def __init__(self):
         self.slot = Slot(self.kind)
@@ -763,8 +772,15 @@ class Simulation:
 
     def _push_forces(self):
         """Every force's scalars (sent only when changed) and the force order
-        for sim_tick (rebuilt only when the forces changed)."""
+        for sim_tick (rebuilt only when the forces changed). Skipped when no
+        force attribute, force handle or precision setting moved since the
+        last push."""
         ctx = self.ctx
+        handles = tuple(f.slot.fh for f in self._forces.values())
+        prec = tuple(ctx.precision.items()) if ctx.precision else None
+        key = (_FORCE_GEN[0], handles, prec)
+        if getattr(self, "_push_key", None) == key:
+            return
         for f in self._forces.values():
             f._push()
             s = f.slot
@@ -772,11 +788,11 @@ class Simulation:
             if ctx.precision:
                 s.scalar(C.ORDER, ctx.precision["order"])
                 s.scalar(C.OPENING, ctx.precision["opening"])
-        handles = tuple(f.slot.fh for f in self._forces.values())
         if getattr(self, "_order_key", None) != handles:
             self._order = (C._U32 * max(1, len(handles)))(*handles)
             self._n_order = len(handles)
             self._order_key = handles
+        self._push_key = (_FORCE_GEN[0], handles, prec)
 
     def device_ticks(self, ticks):
         """`ticks` ticks on the device (sim_tick); returns their device ms.

@@ -1492,7 +1492,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_tc_far_only(TcArgs a, const floa
 // the point itself add nothing; distanceMin's clamp) into
 // part_out[j * parts + part]. Each point is read once.
 constexpr uint32_t CHECK_PTS = 16;
-constexpr uint32_t CHECK_MAX_SAMPLES = 1024;
+constexpr uint32_t CHECK_MAX_SAMPLES = 4096;  // sim_set_learned's limit
 
 __device__ __forceinline__ uint32_t check_point(uint32_t j, uint32_t m, uint32_t samples) {
   return (uint32_t)(((2ull * j + 1) * m) / (2ull * samples));

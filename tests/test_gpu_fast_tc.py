@@ -99,3 +99,26 @@ def test_gpu_tc_fmm_within_plain_fmm_error(gcore):
     rp = _check(gcore, xs, ys, "plain")
     rt = _check(gcore, xs, ys, "bf16x3")
     assert rt <= max(5 * rp, 2e-6)
+
+
+def test_gpu_tc_form_center_tree_sums(gcore):
+    """With a many-body force in the tensor-core form, the center force's sums
+    take the tree order (chunk sums, then one reduction) instead of the
+    sequential order: the shift still equals the exact mean to FP64 rounding.
+    A zero-strength many-body force leaves the velocities at zero, so the tick
+    moves every node by exactly the center's shift (simple.zig:14-31)."""
+    n = 100000
+    xs, ys = _uniform(n, 21)
+    nodes = pkg.Nodes(n, x=xs.copy(), y=ys.copy(), vx=np.zeros(n), vy=np.zeros(n))
+    sim = pkg.forceSimulation(nodes, core=gcore)
+    sim.force("charge", pkg.forceManyBody().strength(0))
+    sim.force("center", pkg.forceCenter(1234.5, -678.25))
+    sim.precision("fast", order=8, opening=1.5, form="bf16x3")
+    sim.tick()
+    x1, y1 = np.asarray(nodes.x).copy(), np.asarray(nodes.y).copy()
+    sim.close()
+    import math
+    sx = math.fsum(xs) / n - 1234.5
+    sy = math.fsum(ys) / n + 678.25
+    assert np.max(np.abs((xs - sx) - x1)) < 1e-9
+    assert np.max(np.abs((ys - sy) - y1)) < 1e-9

@@ -258,6 +258,22 @@ __device__ inline uint32_t key_lower_back(const uint64_t *keys, uint32_t k, uint
   return key_lower(keys, lo, hi, t);
 }
 
+// First index in [k, m) whose key >= t, for keys[k] < t: galloping forward
+// from k, then a binary search of the last stride (a short run costs a few
+// loads).
+__device__ inline uint32_t key_lower_fwd(const uint64_t *keys, uint32_t k, uint32_t m, uint64_t t) {
+  uint32_t lo = k + 1, hi = m;  // the answer is in [lo, hi]
+  for (uint32_t step = 1; lo < m; step <<= 1) {
+    const uint32_t probe = step < m - lo ? lo + step - 1 : m - 1;
+    if ((uint64_t)(uint32_t)keys[probe] >= t) {
+      hi = probe;
+      break;
+    }
+    lo = probe + 1;
+  }
+  return key_lower(keys, lo, hi, t);
+}
+
 // The levels at which point k starts cells: [d0, d1] (empty when d1 < d0).
 __device__ void cell_levels(const uint64_t *keys, uint32_t m, uint32_t k, int &d0, int &d1) {
   const uint32_t key = (uint32_t)keys[k];
@@ -399,7 +415,7 @@ __global__ void __launch_bounds__(CB_THREADS) k_cells_fill(const uint64_t *keys,
   uint32_t end = m;
   if (d > 0) {
     const uint64_t pre = key >> (32 - 2 * d);
-    end = key_lower(keys, k, m, (pre + 1) << (32 - 2 * d));
+    end = key_lower_fwd(keys, k, m, (pre + 1) << (32 - 2 * d));
   }
   FCell f;
   f.cx = f.cy = f.r = 0;

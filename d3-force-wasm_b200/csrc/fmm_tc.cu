@@ -143,8 +143,13 @@ struct TcDev {
   uint32_t ncells_last = 0;
   uint32_t hold = 0;                 // ticks left on the fallback after a failed check
   // CUDA events between the passes of the last run: 0 start, 1 prepared,
-  // 2 lists built, 3 upward, 4 M2L, 5 P2L, 6 downward, 7 leaves, 8 near field
-  cudaEvent_t ev[9] = {};
+  // 2 lists built, 3 upward waited for, 4 M2L, 5 P2L, 6 downward, 7 network,
+  // 8 near field; 9, 10 around the upward pass (on its own stream)
+  cudaEvent_t ev[11] = {};
+  // the upward pass runs on `side` while the lists are built on the main
+  // stream: ev_geom (geometry done) and ev_up (upward done) order them
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_geom = nullptr, ev_up = nullptr;
   uint32_t last_tiles = 0, last_slots = 0;
   void *last_args = nullptr;  // a TcArgs copy of the last pass (for the work counts)
 };
@@ -1830,6 +1835,19 @@ TcDev *tc_dev(FastScratch &s) {
   cudaFuncSetAttribute(k_tc_m2l, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(M2lSmem));
   d->sms = sms;
+  if (cudaStreamCreateWithFlags(&d->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&d->ev_geom, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&d->ev_up, cudaEventDisableTiming) != cudaSuccess) {
+    cudaStreamDestroy(d->side);
+    cudaEventDestroy(d->ev_geom);
+    cudaEventDestroy(d->ev_up);
+    cudaFree(d->info);
+    cudaFreeHost(d->h_info);
+    cudaFree(d->chk);
+    cudaFreeHost(d->h_chk);
+    delete d;
+    return nullptr;
+  }
   s.fmm_tc = d;
   return d;
 }
@@ -1837,15 +1855,35 @@ TcDev *tc_dev(FastScratch &s) {
 // The passes of one expansion order over a built tree and lists: upward,
 // M2L, P2L, L2L, leaf features, (the network, when `learned`), L2P / M2P and
 // the near field.
+// The upward pass at the table set's order: on the side stream, to overlap
+// the list build (`overlap`), else on st. Its grid covers `ncells` leaves at
+// most (the kernel reads the leaf count on the device).
+void tc_upward(TcDev &d, TcArgs &g, const TcTabSet &ts, bool overlap, cudaStream_t st) {
+  g.tab = ts.tab;
+  g.wops = ts.wops;
+  g.q = ts.p + 1;
+  cudaStream_t us = st;
+  if (overlap) {
+    cudaEventRecord(d.ev_geom, st);
+    cudaStreamWaitEvent(d.side, d.ev_geom, 0);
+    us = d.side;
+  }
+  cudaEventRecord(d.ev[9], us);
+  cudaMemsetAsync(d.arrive, 0, (size_t)g.ncells * 4, us);
+  launch_up(g, d.arrive, g.ncells, us);
+  cudaEventRecord(d.ev[10], us);
+  if (overlap) cudaEventRecord(d.ev_up, us);
+}
+
 int tc_order_pass(TcDev &d, TcArgs &g, const TcTabSet &ts, uint32_t tiles, bool learned,
-                  bool far_only, cudaStream_t st) {
+                  bool far_only, bool upward_done, cudaStream_t st) {
   g.tab = ts.tab;
   g.wops = ts.wops;
   g.q = ts.p + 1;
   const uint32_t nleaf = d.h_info[TI_LEAVES];
   const unsigned lw = blocks_for((size_t)nleaf * 32, TC_THREADS);
-  if (cudaMemsetAsync(d.arrive, 0, (size_t)g.ncells * 4, st) != cudaSuccess) return -1;
-  launch_up(g, d.arrive, nleaf, st);
+  if (upward_done) cudaStreamWaitEvent(st, d.ev_up, 0);
+  else tc_upward(d, g, ts, false, st);
   cudaEventRecord(d.ev[3], st);
   if (tiles) D3_LAUNCH(k_tc_m2l, tiles, M2L_THREADS, sizeof(M2lSmem), st)(g);
   cudaEventRecord(d.ev[4], st);
@@ -1888,6 +1926,12 @@ void fmm_tc_free(FastScratch &s) {
   cudaFree(d->chk_part); cudaFree(d->nearbuf); cudaFree(d->leafof);
   for (cudaEvent_t e : d->ev)
     if (e) cudaEventDestroy(e);
+  if (d->side) {
+    cudaStreamSynchronize(d->side);
+    cudaStreamDestroy(d->side);
+  }
+  if (d->ev_geom) cudaEventDestroy(d->ev_geom);
+  if (d->ev_up) cudaEventDestroy(d->ev_up);
   delete static_cast<TcArgs *>(d->last_args);
   delete d;
   s.fmm_tc = nullptr;
@@ -1927,7 +1971,7 @@ void fmm_tc_stats(FastScratch &s, double *out) {
   out[5] = span(7, 8);
   out[12] = span(0, 1);
   out[13] = span(1, 2);
-  out[14] = span(2, 3);
+  out[14] = span(9, 10);
   out[15] = span(4, 5);
   out[16] = span(5, 6);
   out[17] = span(6, 7);
@@ -2002,6 +2046,8 @@ int fmm_tc_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *st
   d.ncells_last = pr.ncells;
   if (cudaMemsetAsync(d.info, 0, TI_WORDS * 4, st) != cudaSuccess) return -1;
   D3_LAUNCH(k_tc_geom, blocks_for(pr.ncells, 256), 256, 0, st)(g);
+  // the upward pass does not read the lists: it runs beside them
+  tc_upward(d, g, *main, true, st);
   // lists (geometry and opening only); grow the pool and redo on overflow
   size_t need = d.last_pool ? d.last_pool + d.last_pool / 4 + 4096 : (size_t)pr.ncells * 24 + 4096;
   for (int attempt = 0;; ++attempt) {
@@ -2034,7 +2080,7 @@ int fmm_tc_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *st
   cudaEventRecord(d.ev[2], st);
   uint32_t tiles = 0;
   for (uint32_t q4 = 0; q4 < 4; ++q4) tiles += (d.h_info[TI_GROUP + q4] + TC_TILE - 1) / TC_TILE;
-  if (tc_order_pass(d, g, *main, tiles, learned, false, st)) return -1;
+  if (tc_order_pass(d, g, *main, tiles, learned, false, true, st)) return -1;
   if (!learned) return 1;
   // the sampled check against the FP64 direct sum
   uint32_t samples = s.learn_samples ? s.learn_samples : 64;
@@ -2065,7 +2111,7 @@ int fmm_tc_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *st
   TcTabSet *fb = tables_for(d, p, kappa, st);
   if (!fb) return -1;
   g.kick = nullptr;
-  if (tc_order_pass(d, g, *fb, tiles, false, true, st)) return -1;
+  if (tc_order_pass(d, g, *fb, tiles, false, true, false, st)) return -1;
   return 1;
 }
 

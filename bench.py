@@ -262,7 +262,8 @@ def fast_ticks(pkg, core, layout, form, flush_l2, steps=10, warmup=3):
     # the tensor-core form's last pass: M2L / P2P event times and work counts
     stats = {k: core.sim_stat(sim.ctx.h, 54 + i) for i, k in enumerate(
         ("m2l_ms", "near_ms", "m2l_tiles", "m2l_pairs", "p2p_pairs", "m2p_pairs", "p2l_pairs", "q",
-         "prepare_ms", "lists_ms", "upward_ms", "p2l_ms", "down_ms", "network_ms", "many_body_ms"))}
+         "prepare_ms", "lists_ms", "upward_ms", "p2l_ms", "down_ms", "network_ms", "many_body_ms",
+         "far_ms"))}
     sim.close()
     return sum(times) / len(times), stats
 
@@ -296,10 +297,10 @@ def fast_roofline(st, rates):
     2 * 128 * 32 * 16 flops each; achieved = those flops / the M2L launch's
     event time, against the measured dense BF16 peak. The useful share: each
     real source-target pair needs 3 x (2q)^2 multiply-adds of the 32-wide
-    padded rows. Near field: the launch that adds P2P, L2P and M2P; counted
-    as about 10 FP32 flops per P2P point pair (differences, the squared
-    distance, one division, two multiply-adds; the far terms are under 2 %
-    of its work), against the measured FP32 FMA rate x 2."""
+    padded rows. Near field: the P2P launch (it runs on a second stream
+    beside M2L, P2L and the downward pass), about 10 FP32 flops per point
+    pair (differences, the squared distance, one reciprocal square root, two
+    multiply-adds), against the measured FP32 FMA rate x 2."""
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:

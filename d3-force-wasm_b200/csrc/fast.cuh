@@ -113,12 +113,11 @@ int fmm_tc_leaves(FastScratch &s, float *out, uint32_t cap);
 // counts (M2L pairs, P2P point pairs, M2P and P2L point-cell pairs) and q.
 // The precision forms' counters (TC_STATS doubles): 0 learned-form checks,
 // 1 fallbacks, 2 the last check's RMS, 3 cells; the last pass: 4 M2L ms,
-// 5 near-field ms, 6 M2L tiles, 7 M2L pairs, 8 P2P point pairs, 9 M2P and 10 P2L
-// point-cell pairs, 11 q; the last run's ms: 12 prepare, 13 geometry and
-// lists, 14 upward, 15 P2L, 16 downward, 17 the learned form's network,
-// 18 the whole run. (4: the M2L launch; 5: the near-field launch, P2P with
-// L2P and M2P.)
-constexpr int TC_STATS = 19;
+// 5 near-field (P2P) ms, 6 M2L tiles, 7 M2L pairs, 8 P2P point pairs, 9 M2P
+// and 10 P2L point-cell pairs, 11 q; the last run's ms: 12 prepare,
+// 13 geometry and lists, 14 upward, 15 P2L, 16 downward, 17 the learned
+// form's network, 18 the whole run, 19 the far field (L2P, M2P, the kick).
+constexpr int TC_STATS = 20;
 void fmm_tc_stats(FastScratch &s, double *out);
 // fmm.zig:247-354. Returns 1 when applied, 0 when the exact kernel must run
 // instead (non-finite extent), < 0 on failure.

@@ -138,18 +138,22 @@ struct TcDev {
   double2 *chk_part = nullptr;               // the check's partial direct sums
   uint32_t chk_cap = 0;                      // entries chk_part holds
   float2 *nearbuf = nullptr;                 // per sorted point: the learned pass's near field
-  uint32_t *leafof = nullptr;                // per sorted point: its leaf (learned pass)
+  uint32_t *leafidx = nullptr;               // per sorted point: its leaf's index in the leaf list
   float *mlp = nullptr;              // installed network parameters (device)
   uint32_t ncells_last = 0;
   uint32_t hold = 0;                 // ticks left on the fallback after a failed check
-  // CUDA events between the passes of the last run: 0 start, 1 prepared,
-  // 2 lists built, 3 upward waited for, 4 M2L, 5 P2L, 6 downward, 7 network,
-  // 8 near field; 9, 10 around the upward pass (on its own stream)
-  cudaEvent_t ev[11] = {};
+  // CUDA events of the last run: main stream 0 start, 1 prepared, 2 lists
+  // built, 3 upward waited for, 4 M2L, 5 P2L, 6 downward, 11 network, 12 far
+  // field; side stream 7, 8 around the near field, 9, 10 around the upward
+  // pass
+  cudaEvent_t ev[13] = {};
   // the upward pass runs on `side` while the lists are built on the main
   // stream: ev_geom (geometry done) and ev_up (upward done) order them
   cudaStream_t side = nullptr;
   cudaEvent_t ev_geom = nullptr, ev_up = nullptr;
+  // the near field runs on `side` after the lists (ev_lists) until ev_near;
+  // the feature rows after the downward pass (ev_down) until ev_feat
+  cudaEvent_t ev_lists = nullptr, ev_near = nullptr, ev_down = nullptr, ev_feat = nullptr;
   uint32_t last_tiles = 0, last_slots = 0;
   void *last_args = nullptr;  // a TcArgs copy of the last pass (for the work counts)
 };
@@ -169,7 +173,7 @@ struct TcArgs {
   size_t pool_cap;
   float *feat, *mlp_x, *mlp_y;
   uint32_t *leaves;
-  uint32_t *leafof;  // per sorted point: its leaf (the learned pass's features write it)
+  uint32_t *leafidx;  // per sorted point: its leaf's index in the leaf list (near pass)
   double2 *kick;  // non-null: the many-body kick goes here instead of into vx, vy
   double *vx, *vy;
   uint32_t *info;
@@ -1189,7 +1193,6 @@ __global__ void __launch_bounds__(TC_THREADS) k_tc_features(TcArgs a) {
     for (uint32_t k = C.first + lane; k < C.first + C.count; k += 32) {
       mx += (float)((a.ux[k] - cx) * inv_s);
       my += (float)((a.uy[k] - cy) * inv_s);
-      a.leafof[k] = c;
     }
     for (int o = 16; o > 0; o >>= 1) {
       mx += __shfl_xor_sync(0xffffffffu, mx, o);
@@ -1264,16 +1267,17 @@ __device__ __forceinline__ void tc_pair_fast(const float4 sv, float xi, float yi
 //     phi += (1/s_W) sum_k M'_k / z^(k+1),   z = (u - c_W) / s_W.
 // Returns the kick's far part in world units; (wr, wi) = w for the feature row.
 __device__ __forceinline__ float2 tc_far(const TcArgs &a, uint32_t k, double cx, double cy,
-                                         double inv_s, const float *Lsh, uint32_t nw, uint32_t ow,
-                                         float &wr, float &wi) {
+                                         double inv_s, const float *Lsh, float c0r, float c0i,
+                                         uint32_t nw, uint32_t ow, float &wr, float &wi) {
   const uint32_t q = a.q;
   const double ux = a.ux[k], uy = a.uy[k];
   wr = (float)((ux - cx) * inv_s);
   wi = (float)((uy - cy) * inv_s);
-  float ar = Lsh[q - 1], ai = Lsh[2 * q - 1];
+  // L'_0 + (c0r, c0i): the learned form's correction (zero otherwise)
+  float ar = Lsh[q - 1] + (q == 1 ? c0r : 0.f), ai = Lsh[2 * q - 1] + (q == 1 ? c0i : 0.f);
   for (int l = (int)q - 2; l >= 0; --l) {
-    const float nr = ar * wr - ai * wi + Lsh[l];
-    ai = ar * wi + ai * wr + Lsh[q + l];
+    const float nr = ar * wr - ai * wi + Lsh[l] + (l == 0 ? c0r : 0.f);
+    ai = ar * wi + ai * wr + Lsh[q + l] + (l == 0 ? c0i : 0.f);
     ar = nr;
   }
   double gr = (double)ar * inv_s, gi = (double)ai * inv_s;
@@ -1303,40 +1307,31 @@ __device__ __forceinline__ float2 tc_far(const TcArgs &a, uint32_t k, double cx,
   return make_float2((float)(-gr * a.inv_w), (float)(gi * a.inv_w));
 }
 
-// A warp per leaf (grid-stride over the leaf list): the near field, the far
-// field and the kick of the leaf's points.
-// Near: the leaf's targets take a lane each; a leaf of W <= 16 points splits
-// the warp into 32 / W lane groups that hold the same targets and take
-// alternate sources, their sums added at the end in group order. The
-// source leaves' points are staged in shared memory relative to the target
-// leaf's first point (the shift in FP64): up to 32 source leaves at a time,
-// their points spread over the lanes so every load of a batch is in flight
-// at once.
-// Far: tc_far for each target (group 0's lanes), with the leaf's local
-// expansion in shared memory; `corrected` adds the learned form's network
-// output to L'_0 (sc * y / LEARN_TARGET_SCALE), else the leaf's feature row
-// is written. v += near + far in FP64 (or the kick to `kick`). `nearbuf`:
-// the near field is also stored there per point (the learned form's
-// fallback, k_tc_far_only, reuses it: it does not depend on the order).
-__global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int corrected,
-                                                            float2 *nearbuf) {
+// A warp per leaf (grid-stride over the leaf list): the near field of its
+// points into nearbuf (FP32 sums) and each point's leaf into leafidx. It
+// reads only the lists and the points, so it runs beside M2L, P2L and the
+// downward pass; k_tc_far adds the far field.
+// The leaf's targets take a lane each, two per lane: a leaf of W points
+// splits the warp into 32 / ceil(W / 2) lane groups that hold the same
+// targets and take alternate sources, their sums added at the end in group
+// order. The source leaves' points are staged in shared memory relative to
+// the target leaf's first point (the shift in FP64): up to 32 source leaves
+// at a time, their points spread over the lanes so every load of a batch is
+// in flight at once.
+__global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, float2 *nearbuf) {
   __shared__ float4 stage[TC_WARPS][P2P_STAGE];
-  __shared__ float lsh[TC_WARPS][TC_KN];
   __shared__ float4 red[TC_WARPS][32];
   const unsigned lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const uint64_t seed = (uint64_t)__double_as_longlong(*a.seed);
   const float dmin2 = a.dmin2f;
-  const uint32_t q = a.q;
   const uint32_t nleaf = __ldcg(&a.info[TI_LEAVES]);
   float4 *sg = stage[wl];
-  float *Lsh = lsh[wl];
   for (uint32_t e0 = gw; e0 < nleaf; e0 += nwarps) {
     const uint32_t c = a.leaves[e0];
     const TcCell A = a.cells[c];
     const uint32_t np = a.loff[(size_t)c * 8 + 1], op = a.loff[(size_t)c * 8];
-    const uint32_t nw = a.loff[(size_t)c * 8 + 3], ow = a.loff[(size_t)c * 8 + 2];
     // lane groups: a lane holds two targets (slots gl and W + gl of the
     // round), W = ceil(count / 2) lanes a group, G = 32 / W groups (lanes
     // past G W idle); a leaf of more than 64 points takes several rounds
@@ -1344,19 +1339,6 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int correct
     const uint32_t grp = lane / W, gl = lane % W;
     const bool in = grp < G;
     const double ox = a.px[A.first], oy = a.py[A.first];
-    double cx, cy;
-    cell_centre(A, cx, cy);
-    const double inv_s = pow2((int)A.level);
-    __syncwarp();
-    {
-      const float *L = a.lco + (size_t)c * TC_KN;
-      float v = lane < 2 * q ? L[lane] : 0.f;
-      if (corrected && (lane == 0 || lane == q)) {
-        const float sc = a.feat[(size_t)c * 16 + 14];
-        v += sc * a.mlp_y[(size_t)e0 * 2 + (lane ? 1 : 0)] * (1.f / LEARN_TARGET_SCALE);
-      }
-      Lsh[lane] = v;
-    }
     // Points at one position share a key, so they sit in one leaf: a leaf
     // whose points (in its FP32 local coordinates) hold a coincident pair, or
     // that spans several rounds of targets, takes the careful pair.
@@ -1373,7 +1355,6 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int correct
       careful = __any_sync(0xffffffffu, dup);
     }
     const uint32_t end = A.first + A.count;
-    float mx = 0, my = 0;  // the points' offsets from the centre (feature row)
     for (uint32_t tb = A.first; tb < end; tb += 2 * W) {
       const uint32_t t0 = tb + gl, t1 = tb + W + gl;
       const bool act0 = in && t0 < end, act1 = in && t1 < end;
@@ -1428,8 +1409,8 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int correct
       __syncwarp();
       red[wl][lane] = make_float4(ax0, ay0, ax1, ay1);
       __syncwarp();
-      float v0x = 0, v0y = 0, v1x = 0, v1y = 0;
-      if (grp == 0)
+      if (grp == 0) {
+        float v0x = 0, v0y = 0, v1x = 0, v1y = 0;
         for (uint32_t g2 = 0; g2 < G; ++g2) {
           const float4 v = red[wl][g2 * W + gl];
           v0x += v.x;
@@ -1437,55 +1418,54 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, int correct
           v1x += v.z;
           v1y += v.w;
         }
-      if (grp == 0) {
-        for (uint32_t h = 0; h < 2; ++h) {
-          const bool act = h ? act1 : act0;
-          if (!act) continue;
-          const uint32_t ti = h ? t1 : t0, gi = h ? g1 : g0;
-          float vx = h ? v1x : v0x, vy = h ? v1y : v0y;
-          if (nearbuf) nearbuf[ti] = make_float2(vx, vy);
-          float wr, wi;
-          const float2 f = tc_far(a, ti, cx, cy, inv_s, Lsh, nw, ow, wr, wi);
-          mx += wr;
-          my += wi;
-          const double kx = (double)vx + (double)f.x, ky = (double)vy + (double)f.y;
-          if (a.kick) {
-            a.kick[ti] = make_double2(kx, ky);
-          } else {
-            a.vx[gi] = a.vx[gi] + kx;
-            a.vy[gi] = a.vy[gi] + ky;
-          }
+        if (act0) {
+          nearbuf[t0] = make_float2(v0x, v0y);
+          a.leafidx[t0] = e0;
+        }
+        if (act1) {
+          nearbuf[t1] = make_float2(v1x, v1y);
+          a.leafidx[t1] = e0;
         }
       }
-    }
-    if (!corrected) {
-      for (int o = 16; o > 0; o >>= 1) {
-        mx += __shfl_xor_sync(0xffffffffu, mx, o);
-        my += __shfl_xor_sync(0xffffffffu, my, o);
-      }
-      if (lane == 0) feature_row(a, c, A, a.lco + (size_t)c * TC_KN, mx, my);
     }
   }
 }
 
-// The learned form's fallback, a thread per point: the order-8 far field of
-// its leaf (tc_far, the local expansion read from the cell's row) plus the
-// near field that the order-4 pass stored, v += near + far in FP64.
-__global__ void __launch_bounds__(TC_THREADS) k_tc_far_only(TcArgs a, const float2 *nearbuf) {
+// A thread per point: the far field of its leaf (tc_far: L2P of the leaf's
+// final local expansion, M2P of its W list) plus its near field from
+// nearbuf, v += near + far in FP64, or the kick to `kick`. `corrected`: the
+// learned form's network output is added to the leaf's L'_0 (sc * y /
+// LEARN_TARGET_SCALE). The learned form's fallback reuses the near field of
+// its order-4 pass here (it does not depend on the order).
+__global__ void __launch_bounds__(TC_THREADS) k_tc_far(TcArgs a, const float2 *nearbuf,
+                                                       int corrected) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= a.m) return;
-  const uint32_t c = a.leafof[k];
+  const uint32_t e = a.leafidx[k];
+  const uint32_t c = a.leaves[e];
   const TcCell C = a.cells[c];
   double cx, cy;
   cell_centre(C, cx, cy);
   const double inv_s = pow2((int)C.level);
   const uint32_t nw = a.loff[(size_t)c * 8 + 3], ow = a.loff[(size_t)c * 8 + 2];
+  float c0r = 0.f, c0i = 0.f;
+  if (corrected) {
+    const float sc = a.feat[(size_t)c * 16 + 14] * (1.f / LEARN_TARGET_SCALE);
+    c0r = sc * a.mlp_y[(size_t)e * 2];
+    c0i = sc * a.mlp_y[(size_t)e * 2 + 1];
+  }
   float wr, wi;
-  const float2 f = tc_far(a, k, cx, cy, inv_s, a.lco + (size_t)c * TC_KN, nw, ow, wr, wi);
+  const float2 f =
+      tc_far(a, k, cx, cy, inv_s, a.lco + (size_t)c * TC_KN, c0r, c0i, nw, ow, wr, wi);
   const float2 nv = nearbuf[k];
-  const uint32_t gi = a.perm[k];
-  a.vx[gi] = a.vx[gi] + ((double)nv.x + (double)f.x);
-  a.vy[gi] = a.vy[gi] + ((double)nv.y + (double)f.y);
+  const double kx = (double)nv.x + (double)f.x, ky = (double)nv.y + (double)f.y;
+  if (a.kick) {
+    a.kick[k] = make_double2(kx, ky);
+  } else {
+    const uint32_t gi = a.perm[k];
+    a.vx[gi] = a.vx[gi] + kx;
+    a.vy[gi] = a.vy[gi] + ky;
+  }
 }
 
 // ---- the learned form's sampled check -----------------------------------------------------------
@@ -1786,8 +1766,8 @@ int reserve(TcDev &d, uint32_t ncells, uint32_t m) {
     cudaFree(d.nearbuf);
     D3_CUDA_OK(cudaMalloc(&d.kick, (size_t)cap * sizeof(double2)));
     D3_CUDA_OK(cudaMalloc(&d.nearbuf, (size_t)cap * sizeof(float2)));
-    cudaFree(d.leafof);
-    D3_CUDA_OK(cudaMalloc(&d.leafof, (size_t)cap * sizeof(uint32_t)));
+    cudaFree(d.leafidx);
+    D3_CUDA_OK(cudaMalloc(&d.leafidx, (size_t)cap * sizeof(uint32_t)));
     d.pcap = cap;
   }
   if (d.ccap > d.lcap) {
@@ -1835,12 +1815,14 @@ TcDev *tc_dev(FastScratch &s) {
   cudaFuncSetAttribute(k_tc_m2l, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(M2lSmem));
   d->sms = sms;
-  if (cudaStreamCreateWithFlags(&d->side, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreateWithFlags(&d->ev_geom, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&d->ev_up, cudaEventDisableTiming) != cudaSuccess) {
-    cudaStreamDestroy(d->side);
-    cudaEventDestroy(d->ev_geom);
-    cudaEventDestroy(d->ev_up);
+  bool ok = cudaStreamCreateWithFlags(&d->side, cudaStreamNonBlocking) == cudaSuccess;
+  for (cudaEvent_t *e : {&d->ev_geom, &d->ev_up, &d->ev_lists, &d->ev_near, &d->ev_down,
+                         &d->ev_feat})
+    ok = ok && cudaEventCreateWithFlags(e, cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) {
+    if (d->side) cudaStreamDestroy(d->side);
+    for (cudaEvent_t e : {d->ev_geom, d->ev_up, d->ev_lists, d->ev_near, d->ev_down, d->ev_feat})
+      if (e) cudaEventDestroy(e);
     cudaFree(d->info);
     cudaFreeHost(d->h_info);
     cudaFree(d->chk);
@@ -1882,6 +1864,16 @@ int tc_order_pass(TcDev &d, TcArgs &g, const TcTabSet &ts, uint32_t tiles, bool 
   g.q = ts.p + 1;
   const uint32_t nleaf = d.h_info[TI_LEAVES];
   const unsigned lw = blocks_for((size_t)nleaf * 32, TC_THREADS);
+  // the near field on the side stream, beside M2L, P2L and the downward pass
+  // (it reads only the lists and the points); `far_only` reuses the stored one
+  if (!far_only) {
+    cudaEventRecord(d.ev_lists, st);
+    cudaStreamWaitEvent(d.side, d.ev_lists, 0);
+    cudaEventRecord(d.ev[7], d.side);
+    D3_LAUNCH(k_tc_near, lw, TC_THREADS, 0, d.side)(g, d.nearbuf);
+    cudaEventRecord(d.ev[8], d.side);
+    cudaEventRecord(d.ev_near, d.side);
+  }
   if (upward_done) cudaStreamWaitEvent(st, d.ev_up, 0);
   else tc_upward(d, g, ts, false, st);
   cudaEventRecord(d.ev[3], st);
@@ -1898,13 +1890,19 @@ int tc_order_pass(TcDev &d, TcArgs &g, const TcTabSet &ts, uint32_t tiles, bool 
     D3_LAUNCH(k_tc_features, lw, TC_THREADS, 0, st)(g);
     D3_LAUNCH(k_tc_pack, blocks_for(nleaf, 256), 256, 0, st)(g);
     if (mlp_infer_tc(d.mlp_x, nleaf, d.mlp, d.mlp_y, g.status, st)) return -1;
+  } else {
+    // the leaves' feature rows (sim_fmm_leaves) on the side stream, beside
+    // the far field; joined before the pass returns
+    cudaEventRecord(d.ev_down, st);
+    cudaStreamWaitEvent(d.side, d.ev_down, 0);
+    D3_LAUNCH(k_tc_features, lw, TC_THREADS, 0, d.side)(g);
+    cudaEventRecord(d.ev_feat, d.side);
   }
-  cudaEventRecord(d.ev[7], st);
-  if (far_only)
-    D3_LAUNCH(k_tc_far_only, blocks_for(g.m, TC_THREADS), TC_THREADS, 0, st)(g, d.nearbuf);
-  else
-    D3_LAUNCH(k_tc_near, lw, TC_THREADS, 0, st)(g, learned ? 1 : 0, learned ? d.nearbuf : nullptr);
-  cudaEventRecord(d.ev[8], st);
+  cudaEventRecord(d.ev[11], st);
+  if (!far_only) cudaStreamWaitEvent(st, d.ev_near, 0);
+  D3_LAUNCH(k_tc_far, blocks_for(g.m, TC_THREADS), TC_THREADS, 0, st)(g, d.nearbuf, learned ? 1 : 0);
+  cudaEventRecord(d.ev[12], st);
+  if (!learned) cudaStreamWaitEvent(st, d.ev_feat, 0);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
@@ -1923,15 +1921,15 @@ void fmm_tc_free(FastScratch &s) {
   cudaFree(d->pool); cudaFree(d->info); cudaFreeHost(d->h_info);
   cudaFree(d->feat); cudaFree(d->leaves); cudaFree(d->mlp_x); cudaFree(d->mlp_y);
   cudaFree(d->kick); cudaFree(d->chk); cudaFreeHost(d->h_chk); cudaFree(d->mlp);
-  cudaFree(d->chk_part); cudaFree(d->nearbuf); cudaFree(d->leafof);
+  cudaFree(d->chk_part); cudaFree(d->nearbuf); cudaFree(d->leafidx);
   for (cudaEvent_t e : d->ev)
     if (e) cudaEventDestroy(e);
   if (d->side) {
     cudaStreamSynchronize(d->side);
     cudaStreamDestroy(d->side);
   }
-  if (d->ev_geom) cudaEventDestroy(d->ev_geom);
-  if (d->ev_up) cudaEventDestroy(d->ev_up);
+  for (cudaEvent_t e : {d->ev_geom, d->ev_up, d->ev_lists, d->ev_near, d->ev_down, d->ev_feat})
+    if (e) cudaEventDestroy(e);
   delete static_cast<TcArgs *>(d->last_args);
   delete d;
   s.fmm_tc = nullptr;
@@ -1974,8 +1972,9 @@ void fmm_tc_stats(FastScratch &s, double *out) {
   out[14] = span(9, 10);
   out[15] = span(4, 5);
   out[16] = span(5, 6);
-  out[17] = span(6, 7);
-  out[18] = span(0, 8);
+  out[17] = span(6, 11);
+  out[18] = span(0, 12);
+  out[19] = span(11, 12);
   const TcArgs &g = *static_cast<const TcArgs *>(d->last_args);
   out[6] = d->last_tiles;
   unsigned long long *cnt = nullptr;
@@ -2032,7 +2031,7 @@ int fmm_tc_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *st
   g.mco = d.mco; g.mbf = d.mbf; g.lco = d.lco;
   g.near = d.near; g.m2l = d.m2l; g.groups = d.groups; g.loff = d.loff;
   g.feat = d.feat; g.leaves = d.leaves; g.mlp_x = d.mlp_x; g.mlp_y = d.mlp_y;
-  g.leafof = d.leafof;
+  g.leafidx = d.leafidx;
   g.kick = learned ? d.kick : nullptr;
   g.vx = a.vx; g.vy = a.vy;
   g.info = d.info;

@@ -222,10 +222,12 @@ int32_t sim_selftest_wait(uint32_t h, uint32_t budget_us);
  * [64][64], b2, W3 [2][64], b3), the RMS tolerance of the sampled check, its
  * sample count (1 .. 4096) and the ticks to stay on the fallback after a
  * failed check. sim_stat 50..53: checks, fallbacks, last sampled RMS, cells;
- * of the last form-2/3 pass: 54 M2L ms, 55 near-field ms, 56 M2L tiles,
- * 57 M2L pairs, 58 near point pairs, 59 M2P and 60 P2L point-cell pairs,
- * 61 q; of the last run (CUDA events): 62 prepare, 63 geometry and lists,
- * 64 upward, 65 P2L, 66 downward, 67 the network, 68 the whole run, in ms. */
+ * of the last form-2/3 pass: 54 M2L ms, 55 near-field (P2P) ms, 56 M2L
+ * tiles, 57 M2L pairs, 58 P2P point pairs, 59 M2P and 60 P2L point-cell
+ * pairs, 61 q; of the last run (CUDA events): 62 prepare, 63 geometry and
+ * lists, 64 upward, 65 P2L, 66 downward, 67 the network, 68 the whole run,
+ * 69 the far field, in ms. The near field and the upward pass run on a
+ * second stream beside the other passes. */
 int32_t sim_set_learned(uint32_t h, const float *params, uint32_t len, double tolerance,
                         uint32_t samples, uint32_t hold);
 

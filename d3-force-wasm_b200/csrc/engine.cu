@@ -602,7 +602,12 @@ extern "C" {
 uint32_t sim_create(void) {
   if (!device_ok()) return 0;
   DSim *s = new DSim();
-  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
+  // The tick's stream takes the greatest priority: work that other streams
+  // run beside it (the center sums, the tensor-core form's near field and
+  // upward pass) fills the SMs it leaves free.
+  int prio_least = 0, prio_greatest = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest);
+  if (cudaStreamCreateWithPriority(&s->stream, cudaStreamNonBlocking, prio_greatest) != cudaSuccess ||
       cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&s->upload, cudaStreamNonBlocking) != cudaSuccess) {
     delete s;
@@ -1176,10 +1181,11 @@ double sim_stat(uint32_t h, uint32_t which) {
   if (which >= 50 && which < 50 + TC_STATS) {
     // the fast many-body precision forms: 50 learned-form checks, 51 of them
     // that fell back, 52 the last check's sampled RMS, 53 cells of the last
-    // run; its last pass: 54 M2L ms, 55 near-field ms, 56 M2L tiles, 57 M2L pairs,
-    // 58 P2P point pairs, 59 M2P and 60 P2L point-cell pairs, 61 q; the last
-    // run's ms: 62 prepare, 63 geometry and lists, 64 upward, 65 P2L,
-    // 66 downward, 67 the learned form's network, 68 the whole run
+    // run; its last pass: 54 M2L ms, 55 near-field (P2P) ms, 56 M2L tiles,
+    // 57 M2L pairs, 58 P2P point pairs, 59 M2P and 60 P2L point-cell pairs,
+    // 61 q; the last run's ms: 62 prepare, 63 geometry and lists, 64 upward,
+    // 65 P2L, 66 downward, 67 the learned form's network, 68 the whole run,
+    // 69 the far field
     double out[TC_STATS];
     fmm_tc_stats(s->fast, out);
     return out[which - 50];

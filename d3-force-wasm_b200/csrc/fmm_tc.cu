@@ -19,7 +19,7 @@
 // M2L from are the children of its parent's near cells that are separated
 // from it: 39 vectors per child quadrant at kappa = 1.5 (60 in all).
 //
-// Passes (one GPU, stream order):
+// Passes (one GPU; the main stream in order, two passes on a second stream):
 //   prepare  fmm_prepare (fmm.cu): keys, sort, gather, level-order cells.
 //   geom     per cell: level, integer coordinates, quadrant, child mask;
 //            the leaf list and the M2L target groups (one per quadrant).
@@ -27,7 +27,8 @@
 //            (13 at kappa 1.5), the M2L table (source per vector slot), and
 //            the adaptive lists: P2P leaves, coarse leaves (P2L), finer
 //            cells seen from a leaf (M2P). Then one host read of the counts.
-//   upward   FP64, a thread per leaf: P2M, then M2M into each parent by the
+//   upward   FP64, a thread per leaf (on the second stream, beside the
+//            lists): P2M, then M2M into each parent by the
 //            thread that completes it (arrival counters, no level
 //            barriers); M' stored in FP64 and split into bf16 hi + lo
 //            (x ~ hi + lo to 2^-17) for the tensor cores.
@@ -40,11 +41,13 @@
 //   p2l      coarse leaves' points into local expansions (FP32 series).
 //   down     a thread per leaf: its ancestors' local expansions shifted to
 //            the leaf's centre (the L2L chain composed, FP32).
-//   near     a warp per leaf: the source leaves' points staged in shared
-//            memory relative to the leaf's first point (the shift in FP64,
-//            the pair sums in FP32: d3's pair formula, distanceMin clamp,
-//            hashed jiggle of hash.zig for coincident points); L2P and M2P
-//            per point; then v += near + far in FP64.
+//   near     a warp per leaf, on the second stream beside M2L / P2L /
+//            down: the source leaves' points staged in shared memory
+//            relative to the leaf's first point (the shift in FP64, the pair
+//            sums in FP32: d3's pair formula, distanceMin clamp, hashed
+//            jiggle of hash.zig for coincident points) into a per-point
+//            buffer.
+//   far      a thread per point: L2P and M2P, then v += near + far in FP64.
 
 #include <cmath>
 #include <cstdio>

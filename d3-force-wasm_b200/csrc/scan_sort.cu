@@ -133,10 +133,11 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_hist(const uint64_t *keys
 // Stable scatter of one tile of SORT_TILE keys: warp w takes the tile's
 // w-th run of 32 x PER keys, in PER rounds of 32. In a round a key's rank
 // among equal digits is the warp's count of that digit so far plus the lanes
-// below it with the same digit (warp match); the warps' counts then become
-// per-digit offsets (tile offset from the scanned histograms + the earlier
-// warps' counts), and every key is written once. Two block barriers per
-// tile.
+// below it with the same digit (warp match). The warps' counts then give
+// each key its place in the tile sorted by digit (stable); the tile is
+// reordered in shared memory and written in that order, so consecutive
+// threads write consecutive places of one digit's run (tile offset from the
+// scanned histograms).
 template <int MODE>
 __global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(const uint64_t *keys, const uint32_t *vals,
                                                                uint64_t *okeys, uint32_t *ovals,
@@ -146,10 +147,16 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(const uint64_t *k
   constexpr unsigned NB = buckets<MODE>();
   constexpr unsigned WARPS = SORT_THREADS / 32, PER = SORT_TILE / SORT_THREADS;
   __shared__ uint32_t wh[WARPS][NB];
+  __shared__ uint32_t lstart[NB], gbase[NB];
+  __shared__ uint64_t skey[SORT_TILE];
+  __shared__ uint32_t sval[SORT_TILE];
+  __shared__ uint32_t wsum[WARPS];
   const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1;
   for (unsigned d = threadIdx.x; d < WARPS * NB; d += blockDim.x) (&wh[0][0])[d] = 0;
-  const size_t wbase = (size_t)blockIdx.x * SORT_TILE + (size_t)warp * 32 * PER;
+  const size_t tbase = (size_t)blockIdx.x * SORT_TILE;
+  const size_t wbase = tbase + (size_t)warp * 32 * PER;
+  const uint32_t tn = n - tbase < SORT_TILE ? (uint32_t)(n - tbase) : SORT_TILE;
   uint64_t k[PER];
   uint32_t v[PER], dg[PER], rk[PER];
 #pragma unroll
@@ -173,23 +180,64 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(const uint64_t *k
     rk[r] = cnt + below;
   }
   __syncthreads();
-  for (unsigned d = threadIdx.x; d < NB; d += blockDim.x) {
-    uint32_t run = offsets[(size_t)d * tiles + blockIdx.x];
+  // per digit: the earlier warps' counts (in place) and the tile's count;
+  // the tile's digit starts by a block scan of the counts
+  uint32_t tot[NB / SORT_THREADS];
+#pragma unroll
+  for (unsigned j = 0; j < NB / SORT_THREADS; ++j) {
+    const unsigned d = j * SORT_THREADS + threadIdx.x;
+    uint32_t run = 0;
 #pragma unroll
     for (unsigned w = 0; w < WARPS; ++w) {
       const uint32_t t = wh[w][d];
       wh[w][d] = run;
       run += t;
     }
+    tot[j] = run;
+    gbase[d] = offsets[(size_t)d * tiles + blockIdx.x];
+  }
+  // exclusive scan of the NB tile counts, a chunk of SORT_THREADS digits at a
+  // time (thread t holds digit j * SORT_THREADS + t of chunk j)
+  {
+    uint32_t chunk_base = 0;
+#pragma unroll
+    for (unsigned j = 0; j < NB / SORT_THREADS; ++j) {
+      uint32_t x = tot[j], in = x;
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, in, o);
+        if (lane >= (unsigned)o) in += y;
+      }
+      __syncthreads();
+      if (lane == 31) wsum[warp] = in;
+      __syncthreads();
+      uint32_t pre = 0, all = 0;
+      for (unsigned w = 0; w < WARPS; ++w) {
+        if (w < warp) pre += wsum[w];
+        all += wsum[w];
+      }
+      lstart[j * SORT_THREADS + threadIdx.x] = chunk_base + pre + in - x;
+      chunk_base += all;
+    }
   }
   __syncthreads();
+  // each key into its place in the tile's digit order
 #pragma unroll
   for (unsigned r = 0; r < PER; ++r)
     if (wbase + r * 32 + lane < n) {
-      const uint32_t pos = wh[warp][dg[r]] + rk[r];
-      okeys[pos] = k[r];
-      ovals[pos] = v[r];
+      const uint32_t at = lstart[dg[r]] + wh[warp][dg[r]] + rk[r];
+      skey[at] = k[r];
+      sval[at] = v[r];
     }
+  __syncthreads();
+  // write in tile order: place i of digit d goes to gbase[d] + i - lstart[d]
+  for (uint32_t i = threadIdx.x; i < tn; i += blockDim.x) {
+    const uint64_t kk = skey[i];
+    const uint32_t vv = sval[i];
+    const uint32_t d = digit_of<MODE>(kk, vv, shift);
+    const uint32_t pos = gbase[d] + (i - lstart[d]);
+    okeys[pos] = kk;
+    ovals[pos] = vv;
+  }
 }
 
 template <int MODE>

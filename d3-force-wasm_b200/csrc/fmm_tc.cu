@@ -1342,19 +1342,15 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, float2 *nea
     const uint32_t grp = lane / W, gl = lane % W;
     const bool in = grp < G;
     const double ox = a.px[A.first], oy = a.py[A.first];
-    // Points at one position share a key, so they sit in one leaf: a leaf
-    // whose points (in its FP32 local coordinates) hold a coincident pair, or
-    // that spans several rounds of targets, takes the careful pair.
+    // Points at one position share a (sorted, 16-level) key, so they sit in
+    // one leaf next to each other: a leaf with two equal neighbouring keys,
+    // or that spans several rounds of targets, takes the careful pair. (Two
+    // points closer than FP32 resolves in the leaf's local coordinates but
+    // with different keys add nothing to each other here.)
     bool careful = A.count > 32;
     if (!careful) {
-      const bool mine = lane < A.count;
-      const float px = mine ? (float)(a.px[A.first + lane] - ox) : 0.f;
-      const float py = mine ? (float)(a.py[A.first + lane] - oy) : 0.f;
-      bool dup = false;
-      for (uint32_t j = 0; j < A.count; ++j) {
-        const float qx = __shfl_sync(0xffffffffu, px, j), qy = __shfl_sync(0xffffffffu, py, j);
-        dup |= mine && j != lane && qx == px && qy == py;
-      }
+      const bool dup = lane + 1 < A.count &&
+                       (uint32_t)a.keys[A.first + lane] == (uint32_t)a.keys[A.first + lane + 1];
       careful = __any_sync(0xffffffffu, dup);
     }
     const uint32_t end = A.first + A.count;

@@ -1321,7 +1321,7 @@ __device__ __forceinline__ float2 tc_far(const TcArgs &a, uint32_t k, double cx,
 // the target leaf's first point (the shift in FP64): up to 32 source leaves
 // at a time, their points spread over the lanes so every load of a batch is
 // in flight at once.
-__global__ void __launch_bounds__(TC_THREADS, 3) k_tc_near(TcArgs a, float2 *nearbuf) {
+__global__ void __launch_bounds__(TC_THREADS, 4) k_tc_near(TcArgs a, float2 *nearbuf) {
   __shared__ float4 stage[TC_WARPS][P2P_STAGE];
   __shared__ float4 red[TC_WARPS][32];
   const unsigned lane = threadIdx.x & 31, wl = threadIdx.x >> 5;

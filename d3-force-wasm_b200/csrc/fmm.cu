@@ -84,6 +84,7 @@ struct FmmDev {
   size_t last_m2l = 0, last_p2p = 0, last_fwd = 0;  // list sizes of the previous run
   // the cell build: per-block counts per level, each cell's start and level
   uint32_t *cb_count = nullptr, *start_of = nullptr;
+  uint16_t *pt_levels = nullptr;  // per point: the levels it starts cells at, d0 << 8 | d1
   uint8_t *level_of = nullptr;
   size_t cb_count_cap = 0, start_cap = 0, level_cap = 0;
 };
@@ -294,13 +295,17 @@ __device__ void cell_levels(const uint64_t *keys, uint32_t m, uint32_t k, int &d
 }
 
 __global__ void __launch_bounds__(CB_THREADS) k_cells_count(const uint64_t *keys,
-                                                            const uint32_t *info, uint32_t *bcount) {
+                                                            const uint32_t *info, uint32_t *bcount,
+                                                            uint16_t *levels) {
   const uint32_t m = info[FI_M];
   __shared__ uint32_t wc[CB_LEVELS][CB_THREADS / 32];
   const uint32_t k = blockIdx.x * CB_THREADS + threadIdx.x;
   const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int d0 = 0, d1 = -1;
-  if (k < m) cell_levels(keys, m, k, d0, d1);
+  if (k < m) {
+    cell_levels(keys, m, k, d0, d1);
+    levels[k] = (uint16_t)(((uint32_t)d0 << 8) | ((uint32_t)d1 & 0xFFu));  // for k_cells_place
+  }
   for (int d = 0; d < (int)CB_LEVELS; ++d) {
     const unsigned b = __ballot_sync(0xffffffffu, d >= d0 && d <= d1);
     if (lane == 0) wc[d][warp] = __popc(b);
@@ -369,7 +374,8 @@ __global__ void __launch_bounds__(32) k_cells_starts(uint32_t ccap, uint32_t *in
 }
 
 // start_of[cell] = the point that starts it; level_of[cell] = its level.
-__global__ void __launch_bounds__(CB_THREADS) k_cells_place(const uint64_t *keys,
+// (the point's levels as k_cells_count found them)
+__global__ void __launch_bounds__(CB_THREADS) k_cells_place(const uint16_t *levels,
                                                             const uint32_t *bcount,
                                                             const uint32_t *info,
                                                             uint32_t *start_of,
@@ -380,7 +386,11 @@ __global__ void __launch_bounds__(CB_THREADS) k_cells_place(const uint64_t *keys
   const uint32_t k = blockIdx.x * CB_THREADS + threadIdx.x;
   const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int d0 = 0, d1 = -1;
-  if (k < m) cell_levels(keys, m, k, d0, d1);
+  if (k < m) {
+    const uint32_t v = levels[k];
+    d0 = (int)(v >> 8);
+    d1 = (int)(int8_t)(v & 0xFFu);
+  }
   uint32_t rank[CB_LEVELS];
   for (int d = 0; d < (int)CB_LEVELS; ++d) {
     const unsigned b = __ballot_sync(0xffffffffu, d >= d0 && d <= d1);
@@ -1018,6 +1028,8 @@ int fmm_reserve_points(FmmDev &f, uint32_t n) {
   D3_CUDA_OK(cudaMalloc(&f.ps, cap * 8ull));
   D3_CUDA_OK(cudaMalloc(&f.ux, cap * 8ull));
   D3_CUDA_OK(cudaMalloc(&f.uy, cap * 8ull));
+  cudaFree(f.pt_levels);
+  D3_CUDA_OK(cudaMalloc(&f.pt_levels, cap * 2ull));
   f.pcap = cap;
   return 0;
 }
@@ -1046,6 +1058,7 @@ void fmm_free(FastScratch &s) {
   FmmDev *f = static_cast<FmmDev *>(s.fmm);
   if (!f) return;
   cudaFree(f->px); cudaFree(f->py); cudaFree(f->ps); cudaFree(f->ux); cudaFree(f->uy);
+  cudaFree(f->pt_levels);
   cudaFree(f->cells); cudaFree(f->bx0); cudaFree(f->by0); cudaFree(f->bx1); cudaFree(f->by1);
   cudaFree(f->m2l_off); cudaFree(f->m2l_cnt); cudaFree(f->p2p_off);
   cudaFree(f->p2p_cnt); cudaFree(f->fwd_off); cudaFree(f->fwd_cnt); cudaFree(f->m2l);
@@ -1126,10 +1139,10 @@ int fmm_prepare(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *s
       if (grow(f.cb_count, f.cb_count_cap, (size_t)nb * CB_LEVELS) ||
           grow(f.start_of, f.start_cap, (size_t)f.ccap) || grow(f.level_of, f.level_cap, (size_t)f.ccap))
         return -1;
-      D3_LAUNCH(k_cells_count, nb, CB_THREADS, 0, st)(t.keys, f.info, f.cb_count);
+      D3_LAUNCH(k_cells_count, nb, CB_THREADS, 0, st)(t.keys, f.info, f.cb_count, f.pt_levels);
       D3_LAUNCH(k_cells_scan, CB_LEVELS, 1024, 0, st)(f.cb_count, nb, f.info);
       D3_LAUNCH(k_cells_starts, 1, 32, 0, st)(f.ccap, f.info);
-      D3_LAUNCH(k_cells_place, nb, CB_THREADS, 0, st)(t.keys, f.cb_count, f.info, f.start_of,
+      D3_LAUNCH(k_cells_place, nb, CB_THREADS, 0, st)(f.pt_levels, f.cb_count, f.info, f.start_of,
                                                     f.level_of);
       D3_LAUNCH(k_cells_fill, blocks_for(f.ccap, CB_THREADS), CB_THREADS, 0, st)(
           t.keys, f.start_of, f.level_of, f.info, f.cells);

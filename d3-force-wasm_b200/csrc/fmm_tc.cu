@@ -696,7 +696,7 @@ __device__ void tc_list_write_general(const TcArgs &a, uint32_t c, const TcCell 
 // launches from the root down (a cell's lists read its parent's). Each warp
 // counts its cell's events, the block takes one range of the pool for all of
 // its warps (one atomic per block), then each warp writes.
-__global__ void __launch_bounds__(TC_THREADS, 3) k_tc_lists(TcArgs a, uint32_t c0, uint32_t c1) {
+__global__ void __launch_bounds__(TC_THREADS, 4) k_tc_lists(TcArgs a, uint32_t c0, uint32_t c1) {
   __shared__ uint32_t wsum[TC_WARPS + 1];
   const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t c = c0 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);

@@ -317,6 +317,7 @@ def fast_roofline(st, rates):
         out["m2l"] = {"bound": "tensor", "achieved": round(ach, 2), "peak": bf16,
                       "unit": "TFLOP/s", "frac": round(ach / bf16, 4),
                       "useful_frac_of_issued": round(useful / issued, 4),
+                      "timing": "event span; the near field runs beside it on a second stream",
                       "ms": round(st["m2l_ms"], 4), "tiles": int(st["m2l_tiles"]),
                       "pairs": int(st["m2l_pairs"]),
                       "peak_source": "measured" if peaks else "fallback"}
@@ -326,6 +327,7 @@ def fast_roofline(st, rates):
         pk = 2 * rates["ffma_per_s"] / 1e12
         out["near"] = {"bound": "fp32", "achieved": round(ach, 2), "peak": round(pk, 1),
                       "unit": "TFLOP/s", "frac": round(ach / pk, 4), "ms": round(st["near_ms"], 4),
+                      "timing": "event span; M2L, P2L and the downward pass run beside it",
                       "pairs": int(st["p2p_pairs"]), "peak_source": "measured (d3_device_peaks)"}
     return out
 

@@ -157,6 +157,7 @@ struct TcDev {
   // the near field runs on `side` after the lists (ev_lists) until ev_near;
   // the feature rows after the downward pass (ev_down) until ev_feat
   cudaEvent_t ev_lists = nullptr, ev_near = nullptr, ev_down = nullptr, ev_feat = nullptr;
+  cudaEvent_t ev_side_idle = nullptr;  // all side-stream work queued so far
   uint32_t last_tiles = 0, last_slots = 0;
   void *last_args = nullptr;  // a TcArgs copy of the last pass (for the work counts)
 };
@@ -1816,11 +1817,12 @@ TcDev *tc_dev(FastScratch &s) {
   d->sms = sms;
   bool ok = cudaStreamCreateWithFlags(&d->side, cudaStreamNonBlocking) == cudaSuccess;
   for (cudaEvent_t *e : {&d->ev_geom, &d->ev_up, &d->ev_lists, &d->ev_near, &d->ev_down,
-                         &d->ev_feat})
+                         &d->ev_feat, &d->ev_side_idle})
     ok = ok && cudaEventCreateWithFlags(e, cudaEventDisableTiming) == cudaSuccess;
   if (!ok) {
     if (d->side) cudaStreamDestroy(d->side);
-    for (cudaEvent_t e : {d->ev_geom, d->ev_up, d->ev_lists, d->ev_near, d->ev_down, d->ev_feat})
+    for (cudaEvent_t e : {d->ev_geom, d->ev_up, d->ev_lists, d->ev_near, d->ev_down, d->ev_feat,
+                          d->ev_side_idle})
       if (e) cudaEventDestroy(e);
     cudaFree(d->info);
     cudaFreeHost(d->h_info);
@@ -1927,7 +1929,8 @@ void fmm_tc_free(FastScratch &s) {
     cudaStreamSynchronize(d->side);
     cudaStreamDestroy(d->side);
   }
-  for (cudaEvent_t e : {d->ev_geom, d->ev_up, d->ev_lists, d->ev_near, d->ev_down, d->ev_feat})
+  for (cudaEvent_t e : {d->ev_geom, d->ev_up, d->ev_lists, d->ev_near, d->ev_down, d->ev_feat,
+                        d->ev_side_idle})
     if (e) cudaEventDestroy(e);
   delete static_cast<TcArgs *>(d->last_args);
   delete d;
@@ -1987,10 +1990,33 @@ void fmm_tc_stats(FastScratch &s, double *out) {
   out[11] = g.q;
 }
 
+namespace {
+
+int tc_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *strengths,
+           const FmmParams &prm, int form, const double *seed, uint32_t *status,
+           cudaStream_t st);
+
+}  // namespace
+
 int fmm_tc_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *strengths,
                const FmmParams &prm, int form, const double *seed, uint32_t *status,
                cudaStream_t st) {
   if (prm.dmax2 < INFINITY) return fmm_run(s, t, a, strengths, prm, seed, status, st);
+  const int r = tc_run(s, t, a, strengths, prm, form, seed, status, st);
+  // whatever path the run ended on, later work on st follows all of its
+  // side-stream work
+  if (TcDev *d = static_cast<TcDev *>(s.fmm_tc)) {
+    cudaEventRecord(d->ev_side_idle, d->side);
+    cudaStreamWaitEvent(st, d->ev_side_idle, 0);
+  }
+  return r;
+}
+
+namespace {
+
+int tc_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *strengths,
+           const FmmParams &prm, int form, const double *seed, uint32_t *status,
+           cudaStream_t st) {
   TcDev *dp = tc_dev(s);
   if (!dp) return -1;
   TcDev &d = *dp;
@@ -2112,5 +2138,7 @@ int fmm_tc_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *st
   if (tc_order_pass(d, g, *fb, tiles, false, true, false, st)) return -1;
   return 1;
 }
+
+}  // namespace
 
 }  // namespace d3

@@ -3,7 +3,7 @@ reference judges its fast many-body force: RMS of one tick's kick against an
 FP64 direct sum of d3's pair formula (test/fast/error-test.js:44-70,
 fmm.zig:913-1000), on seeded targets. The reference's own FMM at order 8,
 opening 1.5 reaches about 2e-6 on such layouts; the bound here is the
-north-star tolerance, RMS <= 1e-5, at that order and opening."""
+precision forms' tolerance, RMS <= 1e-5, at that order and opening."""
 
 import importlib
 

@@ -1253,13 +1253,33 @@ __device__ __forceinline__ void tc_pair(const float4 sv, float xi, float yi, uin
 // self pair adds 0 * w with w finite. A single zero delta keeps its zero
 // here, where d3 would jiggle it by ~1e-6: the change to the kick is ~1e-6
 // of that one pair's term.
-__device__ __forceinline__ void tc_pair_fast(const float4 sv, float xi, float yi, float dmin2,
-                                             float &ax, float &ay) {
-  const float dx = sv.x - xi, dy = sv.y - yi;
-  const float lf = fmaxf(fmaf(dx, dx, dy * dy), 1e-18f);
-  const float w = sv.z * rsqrtf(lf * fmaxf(lf, dmin2));
-  ax = fmaf(dx, w, ax);
-  ay = fmaf(dy, w, ay);
+// It takes two sources at once in sm_100's packed FP32 pairs (FADD2, FMUL2,
+// FFMA2, each half rounded as its scalar op): P = (x_a, x_b, y_a, y_b) and
+// S = (s_a, s_b) of sources a and b, (nx, ny) the target's negated
+// coordinates in both halves, d2 = dmin2 in both. y = max(l^2, l dmin2, fl)
+// with fl = 1e-18 max(1e-18, dmin2) equals lf max(lf, dmin2) with
+// lf = max(l, 1e-18) bit for bit (the rounding is monotonic). ax, ay: the a
+// and b sources' sums.
+__device__ __forceinline__ void tc_pair2(const float4 P, const float2 S, const float2 nx,
+                                         const float2 ny, const float2 d2, float fl, float2 &ax,
+                                         float2 &ay) {
+  const float2 dx = __fadd2_rn(make_float2(P.x, P.y), nx);
+  const float2 dy = __fadd2_rn(make_float2(P.z, P.w), ny);
+  const float2 l = __ffma2_rn(dx, dx, __fmul2_rn(dy, dy));
+  const float2 ll = __fmul2_rn(l, l), ld = __fmul2_rn(l, d2);
+  const float2 r = make_float2(rsqrtf(fmaxf(fmaxf(ll.x, ld.x), fl)),
+                               rsqrtf(fmaxf(fmaxf(ll.y, ld.y), fl)));
+  const float2 w = __fmul2_rn(S, r);
+  ax = __ffma2_rn(dx, w, ax);
+  ay = __ffma2_rn(dy, w, ay);
+}
+
+// Staged source k in the paired layout (slot 2i: x, x', y, y' of sources 2i
+// and 2i + 1; slot 2i + 1: s, s', index, index'), as (x, y, s, index).
+__device__ __forceinline__ float4 staged_point(const float4 *sg, uint32_t k) {
+  const float *p = reinterpret_cast<const float *>(sg + (k & ~1u));
+  const uint32_t h = k & 1u;
+  return make_float4(p[h], p[2 + h], p[4 + h], p[6 + h]);
 }
 
 // The far field at target point k of leaf C: L2P of the leaf's final local
@@ -1321,15 +1341,17 @@ __device__ __forceinline__ float2 tc_far(const TcArgs &a, uint32_t k, double cx,
 // order. The source leaves' points are staged in shared memory relative to
 // the target leaf's first point (the shift in FP64): up to 32 source leaves
 // at a time, their points spread over the lanes so every load of a batch is
-// in flight at once.
+// in flight at once. They are staged in pairs (staged_point), so that the
+// pair loop takes two sources per step in packed FP32 (tc_pair2), each half
+// of a target's sums adding every other source.
 __global__ void __launch_bounds__(TC_THREADS, 4) k_tc_near(TcArgs a, float2 *nearbuf) {
   __shared__ float4 stage[TC_WARPS][P2P_STAGE];
   __shared__ float4 red[TC_WARPS][32];
   const unsigned lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  const uint64_t seed = (uint64_t)__double_as_longlong(*a.seed);
-  const float dmin2 = a.dmin2f;
+  const float2 d2 = make_float2(a.dmin2f, a.dmin2f);
+  const float fl = 1e-18f * fmaxf(1e-18f, a.dmin2f);
   const uint32_t nleaf = __ldcg(&a.info[TI_LEAVES]);
   float4 *sg = stage[wl];
   for (uint32_t e0 = gw; e0 < nleaf; e0 += nwarps) {
@@ -1360,8 +1382,10 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_tc_near(TcArgs a, float2 *nea
       const bool act0 = in && t0 < end, act1 = in && t1 < end;
       const float x0 = act0 ? (float)(a.px[t0] - ox) : 0.f, y0 = act0 ? (float)(a.py[t0] - oy) : 0.f;
       const float x1 = act1 ? (float)(a.px[t1] - ox) : 0.f, y1 = act1 ? (float)(a.py[t1] - oy) : 0.f;
-      const uint32_t g0 = act0 ? a.perm[t0] : 0, g1 = act1 ? a.perm[t1] : 0;
-      float ax0 = 0, ay0 = 0, ax1 = 0, ay1 = 0;  // targets 0 and 1
+      const float2 nx0 = make_float2(-x0, -x0), ny0 = make_float2(-y0, -y0);
+      const float2 nx1 = make_float2(-x1, -x1), ny1 = make_float2(-y1, -y1);
+      // targets 0 and 1; the halves sum the even and the odd sources
+      float2 ax0 = make_float2(0.f, 0.f), ay0 = ax0, ax1 = ax0, ay1 = ax0;
       for (uint32_t eb = 0; eb < np; eb += 32) {
         // this batch's source leaves: lane j holds leaf j's first point and
         // the running count before it
@@ -1378,36 +1402,50 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_tc_near(TcArgs a, float2 *nea
         for (uint32_t base = 0; base < total; base += P2P_STAGE) {
           const uint32_t kn = min(P2P_STAGE, total - base);
           __syncwarp();
+          // the paired layout (staged_point): lanes 2i and 2i + 1 swap halves
+          // and write slots 2i and 2i + 1; a source past kn is a zero (x, y,
+          // s all 0) so an odd last pair adds nothing
+          const uint32_t rounds = (kn + 31) / 32;
+          const bool odd = lane & 1u;
 #pragma unroll 4
-          for (uint32_t r = 0; r < P2P_STAGE / 32; ++r) {
+          for (uint32_t r = 0; r < rounds; ++r) {
             const uint32_t idx = base + r * 32 + lane;
             const uint32_t sj = batch_point(idx, ne, incl, before, first);
-            if (idx < base + kn)
-              sg[r * 32 + lane] = make_float4((float)(__ldg(&a.px[sj]) - ox),
-                                              (float)(__ldg(&a.py[sj]) - oy),
-                                              (float)__ldg(&a.ps[sj]), __uint_as_float(sj));
+            float px = 0.f, py = 0.f, ps = 0.f;
+            if (idx < base + kn) {
+              px = (float)(__ldg(&a.px[sj]) - ox);
+              py = (float)(__ldg(&a.py[sj]) - oy);
+              ps = (float)__ldg(&a.ps[sj]);
+            }
+            const float u = __shfl_xor_sync(0xffffffffu, odd ? px : ps, 1);
+            const float v = __shfl_xor_sync(0xffffffffu, odd ? py : __uint_as_float(sj), 1);
+            sg[r * 32 + lane] = odd ? make_float4(u, ps, v, __uint_as_float(sj))
+                                    : make_float4(px, u, py, v);
           }
           __syncwarp();
-          uint32_t k = in ? grp : kn;
           if (!careful) {
+            const uint32_t kp_end = (kn + 1) / 2;
 #pragma unroll 4
-            for (; k < kn; k += G) {
-              const float4 sv = sg[k];
-              tc_pair_fast(sv, x0, y0, dmin2, ax0, ay0);
-              tc_pair_fast(sv, x1, y1, dmin2, ax1, ay1);
+            for (uint32_t kp = in ? grp : kp_end; kp < kp_end; kp += G) {
+              const float4 P = sg[2 * kp];
+              const float2 S = *reinterpret_cast<const float2 *>(&sg[2 * kp + 1]);
+              tc_pair2(P, S, nx0, ny0, d2, fl, ax0, ay0);
+              tc_pair2(P, S, nx1, ny1, d2, fl, ax1, ay1);
             }
           } else {
-            for (; k < kn; k += G) {
-              const float4 sv = sg[k];
-              tc_pair(sv, x0, y0, t0, g0, dmin2, seed, a.perm, ax0, ay0);
-              tc_pair(sv, x1, y1, t1, g1, dmin2, seed, a.perm, ax1, ay1);
+            const uint64_t seed = (uint64_t)__double_as_longlong(*a.seed);
+            const uint32_t g0 = act0 ? a.perm[t0] : 0, g1 = act1 ? a.perm[t1] : 0;
+            for (uint32_t k = in ? grp : kn; k < kn; k += G) {
+              const float4 sv = staged_point(sg, k);
+              tc_pair(sv, -nx0.x, -ny0.x, t0, g0, d2.x, seed, a.perm, ax0.x, ay0.x);
+              tc_pair(sv, -nx1.x, -ny1.x, t1, g1, d2.x, seed, a.perm, ax1.x, ay1.x);
             }
           }
         }
       }
       // the groups' sums, in group order
       __syncwarp();
-      red[wl][lane] = make_float4(ax0, ay0, ax1, ay1);
+      red[wl][lane] = make_float4(ax0.x + ax0.y, ay0.x + ay0.y, ax1.x + ax1.y, ay1.x + ay1.y);
       __syncwarp();
       if (grp == 0) {
         float v0x = 0, v0y = 0, v1x = 0, v1y = 0;

@@ -226,8 +226,9 @@ int32_t sim_selftest_wait(uint32_t h, uint32_t budget_us);
  * tiles, 57 M2L pairs, 58 P2P point pairs, 59 M2P and 60 P2L point-cell
  * pairs, 61 q; of the last run (CUDA events): 62 prepare, 63 geometry and
  * lists, 64 upward, 65 P2L, 66 downward, 67 the network, 68 the whole run,
- * 69 the far field, in ms. The near field and the upward pass run on a
- * second stream beside the other passes. */
+ * 69 the far field (from the wait on the near field to the end of L2P / M2P),
+ * in ms. The near field and the upward pass run on a second stream beside
+ * the other passes. */
 int32_t sim_set_learned(uint32_t h, const float *params, uint32_t len, double tolerance,
                         uint32_t samples, uint32_t hold);
 

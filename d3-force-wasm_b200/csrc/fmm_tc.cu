@@ -1343,7 +1343,8 @@ __device__ __forceinline__ float2 tc_far(const TcArgs &a, uint32_t k, double cx,
 // at a time, their points spread over the lanes so every load of a batch is
 // in flight at once. They are staged in pairs (staged_point), so that the
 // pair loop takes two sources per step in packed FP32 (tc_pair2), each half
-// of a target's sums adding every other source.
+// of a target's sums adding every other source; there the lane groups take
+// alternate source pairs.
 __global__ void __launch_bounds__(TC_THREADS, 4) k_tc_near(TcArgs a, float2 *nearbuf) {
   __shared__ float4 stage[TC_WARPS][P2P_STAGE];
   __shared__ float4 red[TC_WARPS][32];

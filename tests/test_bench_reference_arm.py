@@ -2,7 +2,8 @@
 (the reference core's algorithm restated in C) on the host cores, over the
 same schedule and workload as the GPU arm, and prints the same JSON line with
 `"impl": "reference"`. Under torchrun only rank 0 runs it; the other ranks
-exit 0 without work or output."""
+exit 0 without work or output. Both arms time the same ticks of the
+300-tick schedule (`schedule_positions`)."""
 
 import json
 import os
@@ -48,3 +49,17 @@ def test_reference_arm_other_ranks_do_no_work():
                "--steps", "3", "--warmup", "3")
     assert r.returncode == 0, r.stderr[-2000:]
     assert not [l for l in r.stdout.splitlines() if l.startswith("{")]
+
+
+def test_timed_ticks_spread_over_the_schedule():
+    """The K timed ticks lie after the W warm-up ticks, strictly increasing,
+    the last one the schedule's last tick; a run longer than the schedule
+    extends it."""
+    sys.path.insert(0, ROOT)
+    import bench
+
+    for w, k in [(3, 1), (3, 20), (5, 30), (5, 295), (10, 300)]:
+        pos, total = bench.schedule_positions(w, k)
+        assert total == max(bench.SCHEDULE_TICKS, w + k)
+        assert len(pos) == k and pos[-1] == total and pos[0] > w
+        assert all(b > a for a, b in zip(pos, pos[1:]))

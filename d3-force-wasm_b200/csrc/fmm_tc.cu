@@ -1218,6 +1218,10 @@ __global__ void k_tc_pack(TcArgs a) {
 // ---- P2P (FP32 with an FP64 origin shift) ----------------------------------------------------------
 
 constexpr uint32_t P2P_STAGE = 256;  // staged source points per warp
+// The near field's blocks: 4 warps, 8 blocks an SM (64 registers a thread).
+// A warp takes one leaf, and a block frees its slot when its slowest warp
+// ends, so small blocks keep more warps busy under uneven leaf sizes.
+constexpr uint32_t NEAR_THREADS = 128, NEAR_WARPS = NEAR_THREADS / 32;
 
 // One point pair of the near field (d3's pair formula, the distanceMin clamp
 // and the hashed jiggle of hash.zig for exact zero deltas; the self pair adds
@@ -1345,9 +1349,9 @@ __device__ __forceinline__ float2 tc_far(const TcArgs &a, uint32_t k, double cx,
 // pair loop takes two sources per step in packed FP32 (tc_pair2), each half
 // of a target's sums adding every other source; there the lane groups take
 // alternate source pairs.
-__global__ void __launch_bounds__(TC_THREADS, 4) k_tc_near(TcArgs a, float2 *nearbuf) {
-  __shared__ float4 stage[TC_WARPS][P2P_STAGE];
-  __shared__ float4 red[TC_WARPS][32];
+__global__ void __launch_bounds__(NEAR_THREADS, 8) k_tc_near(TcArgs a, float2 *nearbuf) {
+  __shared__ float4 stage[NEAR_WARPS][P2P_STAGE];
+  __shared__ float4 red[NEAR_WARPS][32];
   const unsigned lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -1910,7 +1914,8 @@ int tc_order_pass(TcDev &d, TcArgs &g, const TcTabSet &ts, uint32_t tiles, bool 
     cudaEventRecord(d.ev_lists, st);
     cudaStreamWaitEvent(d.side, d.ev_lists, 0);
     cudaEventRecord(d.ev[7], d.side);
-    D3_LAUNCH(k_tc_near, lw, TC_THREADS, 0, d.side)(g, d.nearbuf);
+    D3_LAUNCH(k_tc_near, blocks_for((size_t)nleaf * 32, NEAR_THREADS), NEAR_THREADS, 0, d.side)(
+        g, d.nearbuf);
     cudaEventRecord(d.ev[8], d.side);
     cudaEventRecord(d.ev_near, d.side);
   }

@@ -696,9 +696,11 @@ __device__ void tc_list_write_general(const TcArgs &a, uint32_t c, const TcCell 
 // The cells of one level, a warp per cell; the levels run as consecutive
 // launches from the root down (a cell's lists read its parent's). Each warp
 // counts its cell's events, the block takes one range of the pool for all of
-// its warps (one atomic per block), then each warp writes.
-__global__ void __launch_bounds__(TC_THREADS, 4) k_tc_lists(TcArgs a, uint32_t c0, uint32_t c1) {
-  __shared__ uint32_t wsum[TC_WARPS + 1];
+// its warps (one atomic per block), then each warp writes. Blocks of 4
+// warps, 8 an SM: the block waits at that range for its slowest warp's count.
+constexpr uint32_t LIST_THREADS = 128, LIST_WARPS = LIST_THREADS / 32;
+__global__ void __launch_bounds__(LIST_THREADS, 8) k_tc_lists(TcArgs a, uint32_t c0, uint32_t c1) {
+  __shared__ uint32_t wsum[LIST_WARPS + 1];
   const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t c = c0 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const bool active = c < c1;  // warp-uniform
@@ -734,16 +736,16 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_tc_lists(TcArgs a, uint32_t c
   __syncthreads();
   if (threadIdx.x == 0) {
     uint32_t run = 0;
-    for (uint32_t w = 0; w < TC_WARPS; ++w) {
+    for (uint32_t w = 0; w < LIST_WARPS; ++w) {
       const uint32_t t = wsum[w];
       wsum[w] = run;
       run += t;
     }
-    wsum[TC_WARPS] = run ? atomicAdd(&a.info[TI_POOL_P2P], run) : 0;
+    wsum[LIST_WARPS] = run ? atomicAdd(&a.info[TI_POOL_P2P], run) : 0;
   }
   __syncthreads();
   if (!active) return;
-  const uint32_t base = wsum[TC_WARPS] + wsum[warp];
+  const uint32_t base = wsum[LIST_WARPS] + wsum[warp];
   const uint32_t o4[4] = {base, base + S.tot.np, base + S.tot.np + S.tot.nw,
                           base + S.tot.np + S.tot.nw + S.tot.nx};
   uint32_t *lo = a.loff + (size_t)c * 8;
@@ -2131,7 +2133,7 @@ int tc_run(FastScratch &s, TreeDev &t, const NodeArrays &a, const double *streng
     for (uint32_t lev = 0; lev < pr.nlev; ++lev) {
       const uint32_t c0 = pr.lvl[lev], c1 = pr.lvl[lev + 1];
       if (c1 > c0)
-        D3_LAUNCH(k_tc_lists, blocks_for((size_t)(c1 - c0) * 32, TC_THREADS), TC_THREADS, 0, st)(
+        D3_LAUNCH(k_tc_lists, blocks_for((size_t)(c1 - c0) * 32, LIST_THREADS), LIST_THREADS, 0, st)(
             g, c0, c1);
     }
     if (cudaMemcpyAsync(d.h_info, d.info, TI_WORDS * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
